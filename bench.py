@@ -1,0 +1,303 @@
+"""Benchmark of the graph-construction hot path (one JSON line on stdout).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload: one synthetic assembly at binning scale — 100 genomes, 50,000 large
+contigs (~420 Mbp), S = 20 coverage samples, --sketch-m 500, --max-edges 200
+(the reference's fused N > 25000 path with the mutual filter and the
+abundance-first prune).  A step is one full pass of the hot path over it:
+2-bit packing, canonical 4-mer counting + GC-norm weights, ProbMinHash
+registers, b0, unit rank rows, all-pairs compare with per-row top-200, the
+calibration, the mutual filter and the edge weights.  Metric: contig pairs
+scored per second, N(N-1)/2 per step per assembly.
+
+* ``value``: inputs resident in HBM when the timed region starts (ASCII
+  sequences + coverage, 420 MB > 126 MB L2, so no flush is needed).
+* ``e2e``: the same step through the public C ABI call ``rbg_bin_graph`` with
+  host buffers: pinned host -> device copies of the inputs and the device ->
+  host read of the edge arrays inside the timed region.
+* multi-GPU: each rank processes its own assembly of the same size (weak
+  scaling over independent assemblies, no collective on the data path).
+* ``--impl reference``: RabbitBin's own CPU code (oracle/_ref, compiled from
+  the reference sources) on a bounded sample of the same workload with all
+  host cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(workload="binning-scale assembly: 100 genomes, 50000 contigs, S=20, "
+                         "sketch-m 500, max-edges 200, fused path + mutual filter",
+                n_genomes=100, n_contigs=50000, samples=20, sketch_m=500, max_edges=200,
+                inputs_exceed_l2=True, seed=1)
+METRIC = "contig-pairs scored/s"
+UNIT = "pairs/s"
+
+
+def _env_rank():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index):
+        self.index, self.rows, self.proc = index, [], None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.3)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for n, v in zip(names, r[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+def _assembly(seed):
+    from rabbitbin_b200.synth import make_assembly
+    w = WORKLOAD
+    return make_assembly(w["n_genomes"], w["n_contigs"], w["samples"], seed=seed)
+
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+    from rabbitbin_b200 import api
+
+    rank, world, local = _env_rank()
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    asm = _assembly(WORKLOAD["seed"] + rank)
+    buf, offs = asm.concat()
+    n = asm.n
+    pairs = n * (n - 1) // 2
+    params = api.default_params(m=WORKLOAD["sketch_m"], max_edges=WORKLOAD["max_edges"])
+    ctx = api.Context(local)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    # ── device-resident value ───────────────────────────────────────────────
+    ctx.stage(buf, offs, asm.depth)
+    for _ in range(args.warmup):
+        ctx.run_resident(params)
+    ext = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    timings = []
+    barrier()
+    with ClockSampler(local) as clk:
+        start.record(ext)
+        for _ in range(args.steps):
+            timings.append(ctx.run_resident(params))
+        end.record(ext)
+        barrier()
+    ms = start.elapsed_time(end) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * pairs / (ms / 1000.0)
+
+    # ── end to end through rbg_bin_graph with pinned host inputs ────────────
+    pin_seq = torch.empty(len(buf), dtype=torch.uint8, pin_memory=True)
+    pin_seq.numpy()[:] = np.frombuffer(buf, dtype=np.uint8)
+    pin_depth = torch.empty(asm.depth.shape, dtype=torch.float32, pin_memory=True)
+    pin_depth.numpy()[:] = asm.depth
+    seq_ptr = pin_seq.numpy().ctypes.data_as(__import__("ctypes").c_char_p)
+    ctx.bin_graph(seq_ptr, offs, pin_depth.numpy(), params)          # warm
+    barrier()
+    t0 = time.perf_counter()
+    e2e_edges = 0
+    for _ in range(args.steps):
+        g = ctx.bin_graph(seq_ptr, offs, pin_depth.numpy(), params)
+        e2e_edges = len(g["src"])
+    barrier()
+    e2e_ms = (time.perf_counter() - t0) * 1000.0 / args.steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+
+    last = timings[-1]
+    peaks, peak_src = _peaks()
+    clocks = clk.summary()
+    # dominant kernel: the all-pairs pass (abundance test on every ordered pair,
+    # register compare on the survivors); FP32 FMA/ADD pipe bound
+    ap_ms = last["allpairs_ms"]
+    S = WORKLOAD["samples"]
+    flops = last["pairs_prefiltered"] * (2 * S + 15)        # S FMAs + 15-add reduction tree
+    sm_mhz = clocks["sm_mhz"] or peaks.get("sm_max_mhz", 1965.0)
+    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12       # TFLOP/s at the sampled clock
+    achieved = flops / (ap_ms / 1000.0) / 1e12 if ap_ms > 0 else 0.0
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u8/u32 register codes, f64 sketch, f32 abundance",
+        "data": "synthetic (seeded order-3 Markov genomes, lognormal coverage)",
+        "config": dict(WORKLOAD, parallelism=f"{world} independent assemblies"),
+        "e2e": {"value": world * pairs / (e2e_ms / 1000.0), "unit": UNIT,
+                "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": int(len(buf) + offs.nbytes + asm.depth.nbytes),
+                "d2h_bytes_per_step": int(e2e_edges * 16)},
+        "stages_ms": {k: round(v, 4) for k, v in last.items() if k.endswith("_ms")},
+        "pairs_prefiltered": last["pairs_prefiltered"],
+        "pairs_compared": last["pairs_compared"],
+        "gpu_launches": int(last["kernel_launches"]) * args.steps,
+        "roofline": {"bound": "fp32-alu", "kernel": "k_allpairs",
+                     "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                     "frac": achieved / fp32_peak if fp32_peak else None,
+                     "peak_source": "nominal 148 SM x 128 FP32 lanes x 2 at the sampled SM clock "
+                                    f"(no measured FP32 peak; HBM/bf16 peaks are {peak_src})",
+                     "traffic": None},
+        "clocks": clocks,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(asm, seconds=args.cpu_seconds)
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result))
+
+
+def cpu_baseline(asm, seconds=20.0):
+    """RabbitBin's own CPU code on a bounded sample of the workload."""
+    import oracle
+    lib = oracle.ref()
+    kind = "reference"
+    if lib is None:
+        lib, kind = oracle.restated(), "port"
+    cores = os.cpu_count() or 1
+    n = min(asm.n, 12000)
+    buf, offs = asm.concat()
+    sub_offs = offs[:n + 1]
+    t0 = time.perf_counter()
+    w = lib.build_winners(buf[:int(sub_offs[-1])], sub_offs, nthreads=cores)
+    p = oracle.default_params(n, 500, asm.n_samples, force_path=2, nthreads=cores)
+    lib.run_graph(p, w, asm.depth[:n])
+    dt = time.perf_counter() - t0
+    pairs = n * (n - 1) // 2
+    return {"value": pairs / dt, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"first {n} contigs of the workload (sketch + fused graph + weights), "
+                      f"{dt:.1f} s"}
+
+
+def run_reference(args):
+    rank, world, _ = _env_rank()
+    if rank != 0:
+        return
+    import oracle
+    lib = oracle.ref()
+    kind = "reference"
+    if lib is None:
+        lib, kind = oracle.restated(), "port"
+    asm = _assembly(WORKLOAD["seed"])
+    cores = os.cpu_count() or 1
+    n = min(asm.n, args.ref_contigs)
+    buf, offs = asm.concat()
+    sub_offs = offs[:n + 1]
+    sbuf = buf[:int(sub_offs[-1])]
+
+    def step():
+        w = lib.build_winners(sbuf, sub_offs, nthreads=cores)
+        p = oracle.default_params(n, 500, asm.n_samples, force_path=2, nthreads=cores)
+        lib.run_graph(p, w, asm.depth[:n])
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    ms = (time.perf_counter() - t0) * 1000.0 / args.steps
+    pairs = n * (n - 1) // 2
+    value = pairs / (ms / 1000.0)
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "impl": "reference",
+        "dtype": "u16 winners, f64 sketch, f32 abundance", "data": "synthetic",
+        "config": dict(WORKLOAD, reference_sample_contigs=n),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": f"first {n} contigs of the workload per step"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--ref-contigs", type=int, default=12000)
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,165 @@
+/*
+ * rabbitbin_b200 — C ABI of the B200 graph-construction hot path of RabbitBin.
+ *
+ * The reference has no plugin or FFI layer: its seams are C++ functions inside
+ * one translation unit.  Each entry point below replaces one of them, keeps its
+ * argument meaning, and adds only what a device boundary needs (a context that
+ * owns the CUDA stream and device buffers, batching over contigs, an int status).
+ *
+ *   rbg_build_pmh_winners  ← build_pmh_winners            src/rabbitbin.cpp:1436-1589
+ *                            (called per contig at :2164, :4375, :4854-4863)
+ *   rbg_pack_win16         ← fold_win16 + pack loop       src/rabbitbin.cpp:249-253, :4934-4952
+ *   rbg_estimate_pmh_baseline ← estimate_pmh_baseline     src/rabbitbin.cpp:1340-1369, :4958-4965
+ *   rbg_build_graph        ← calibrate_sim_cutoff + build_similarity_graph (N <= 25000)
+ *                            src/impl/rb_graph.cpp:1362-1384, :199-220, :7-72
+ *                            gen_fused_calib_graph (N > 25000)  src/impl/rb_graph.cpp:501-1356
+ *                            dispatched as at src/rabbitbin.cpp:5035-5054, followed by
+ *                            the edge-weight loop src/rabbitbin.cpp:5482-5509
+ *                            (depth_edge_term :930-970) on the same device state
+ *   rbg_bin_graph          ← the whole hot path of rb_cmd_bin (sketch loop :4817-4882,
+ *                            pack, b0, unit rows :4972-4988, graph, edge weights)
+ *                            from sequences + coverage, without host round trips
+ *
+ * Conventions: all buffers are caller-owned host memory unless a name says
+ * "device"; sizes are element counts; every function returns RBG_OK (0) or a
+ * negative status and never throws.  rbg_last_error(ctx) describes the last
+ * failure on that context.  Calls on one context are serialised; different
+ * contexts may be used from different host threads.
+ */
+#ifndef RABBITBIN_B200_H
+#define RABBITBIN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  RBG_OK = 0,
+  RBG_ERR_ARG = -1,        /* bad argument (reference: cerr + return 1)          */
+  RBG_ERR_NOMEM = -2,      /* device or host allocation failed / over budget     */
+  RBG_ERR_CUDA = -3,       /* CUDA runtime error                                 */
+  RBG_ERR_UNSUPPORTED = -4,/* option value this build does not implement         */
+  RBG_ERR_TIMEOUT = -5     /* a bounded device wait gave up                      */
+};
+
+/* Options of `rabbitbin bin` and the hot-path RABBIT_* variables, with the
+ * reference defaults (src/rabbitbin.cpp:3339-3445, :4660-4705). */
+typedef struct rbg_params {
+  int32_t k;              /* RABBIT_PMHK (4); 1..4 supported                       */
+  int32_t m;              /* --sketch-m (500); 2..4096                             */
+  uint64_t pmh_seed;      /* g_pmh_seed (42)                                       */
+  int32_t gc_norm;        /* RABBIT_GC_NORM (1); 0 and 1 supported                 */
+  int32_t win_bits;       /* RABBIT_WIN_BITS (16) or 32                            */
+  double gc_norm_cap;     /* RABBIT_GC_NORM_CAP (20)                               */
+  int32_t max_edges;      /* --max-edges (200)                                     */
+  int32_t mutual;         /* RABBIT_MUTUAL_KNN (1)                                 */
+  int32_t base_on;        /* RABBIT_PMH_BASE (1)                                   */
+  uint32_t seed;          /* --seed, the srand() seed of the calibration (1)       */
+  int32_t force_path;     /* 0: N > 25000 -> fused path as the reference; 1 small; 2 fused */
+  int32_t abdfirst;       /* 1 unless RABBIT_NO_ABDFIRST is set                    */
+  double coverage;        /* --max-posterior / 100 (0.95)                          */
+  double min_edge;        /* --min-edge-score / 100 (0.70)                         */
+  double w_comp;          /* RABBIT_W_COMP, < 0 = auto (S <= 2 -> 1, else 0)       */
+  double min_cv;          /* --min-coverage (1.0)                                  */
+  double neg_thr;         /* RABBIT_NEG_DEPTH (-0.3)                               */
+  int32_t depth_sim;      /* RABBIT_DEPTH_SIM: 0 corr, 1 wjac, 2 fuse (2)          */
+  int32_t depth_fuse;     /* RABBIT_DEPTH_FUSE: 0 geo-mean, 1 min, 2 product (1)   */
+  int32_t wjac_norm;      /* RABBIT_DEPTH_WJAC_NORM (1)                            */
+  int32_t fp_contract;    /* 1: arithmetic of the reference's release build, where
+                             GCC contracts a*b+c into FMA; 0: -ffp-contract=off   */
+  double wjac_cut;        /* RABBIT_DEPTH_WJAC_CUT (0)                             */
+  int32_t wjac_gate;      /* RABBIT_DEPTH_WJAC_GATE (0)                            */
+  int32_t reserved;
+} rbg_params;
+
+/* Graph + edge weights (the reference Graph's from/to/sComp/edgeScore,
+ * src/rabbitbin.h:264-301), sorted by (from, to).  Arrays are allocated by the
+ * library; release them with rbg_free_graph. */
+typedef struct rbg_graph {
+  int64_t n_edges;
+  uint32_t *from;
+  uint32_t *to;
+  float *scomp;           /* composition similarity sComp                          */
+  float *score;           /* edgeScore                                             */
+  double b0;              /* g_pmh_baseline                                        */
+  double sim_cutoff;      /* simCutoff as the reference returns it (x1000 units)   */
+  int32_t path;           /* 1 small-N path, 2 fused large-N path                  */
+  int32_t reserved;
+} rbg_graph;
+
+/* Per-stage device time of the last rbg_bin_graph / rbg_run_resident call. */
+typedef struct rbg_timing {
+  float pack_ms, count_ms, sketch_ms, unit_ms, b0_ms, allpairs_ms, finalize_ms,
+        emit_ms, weight_ms, total_ms;
+  int64_t pairs_prefiltered;   /* ordered pairs through the abundance test      */
+  int64_t pairs_compared;      /* ordered pairs through the register compare    */
+  int32_t kernel_launches;     /* kernels launched by the call                  */
+  int32_t reserved;
+} rbg_timing;
+
+typedef struct rbg_ctx rbg_ctx;
+
+/* Fill *p with the reference defaults. */
+int rbg_default_params(rbg_params *p);
+
+/* Create a context on CUDA device `device` (owns a stream and device buffers). */
+int rbg_create(int device, rbg_ctx **out);
+int rbg_destroy(rbg_ctx *ctx);
+const char *rbg_last_error(rbg_ctx *ctx);
+/* cudaStream_t of the context, as void*, for callers that time or order work. */
+void *rbg_stream(rbg_ctx *ctx);
+
+/* build_pmh_winners for n contigs.  seqcat holds the ASCII sequences back to
+ * back, contig r = seqcat[offsets[r], offsets[r+1]).  out_winners32 (n*m) gets
+ * the 64->32-bit folded winner rows (src/rabbitbin.cpp:1582-1588). */
+int rbg_build_pmh_winners(rbg_ctx *ctx, const rbg_params *p, const char *seqcat,
+                          const int64_t *offsets, int64_t n,
+                          uint32_t *out_winners32);
+
+/* fold_win16 over `count` folded winners (src/rabbitbin.cpp:249-253). */
+int rbg_pack_win16(rbg_ctx *ctx, const uint32_t *in, int64_t count, uint16_t *out);
+
+/* estimate_pmh_baseline over n winner rows of width p->m; `winners` is
+ * uint16_t[n*m] when win_bits == 16, else uint32_t[n*m]. */
+int rbg_estimate_pmh_baseline(rbg_ctx *ctx, const rbg_params *p,
+                              const void *winners, int32_t win_bits, int64_t n,
+                              double *out_b0);
+
+/* Graph + edge weights from folded 32-bit winner rows (n*m) and the raw
+ * coverage means depth (n*S floats, S = 0 for no depth file). */
+int rbg_build_graph(rbg_ctx *ctx, const rbg_params *p, const uint32_t *winners32,
+                    int64_t n, const float *depth, int32_t S, rbg_graph *out);
+
+/* The whole hot path: sequences + coverage -> graph with edge weights. */
+int rbg_bin_graph(rbg_ctx *ctx, const rbg_params *p, const char *seqcat,
+                  const int64_t *offsets, int64_t n, const float *depth,
+                  int32_t S, rbg_graph *out);
+
+/* Device-resident form used by batching, serving and the benchmark: stage the
+ * inputs once (host -> device), run the hot path on them any number of times,
+ * then fetch the graph (device -> host). */
+int rbg_stage(rbg_ctx *ctx, const char *seqcat, const int64_t *offsets,
+              int64_t n, const float *depth, int32_t S);
+int rbg_run_resident(rbg_ctx *ctx, const rbg_params *p, rbg_timing *timing);
+int rbg_fetch_graph(rbg_ctx *ctx, rbg_graph *out);
+
+int rbg_free_graph(rbg_graph *g);
+
+/* Introspection (host only, no device needed): the ProbMinHash element streams
+ * the sketch kernel reduces over for one configuration.  For every canonical
+ * k-mer e (ascending code canon_codes[e]) and register r, U[e*m + r] is the
+ * weight-free value e offers to r (the offer is (1/w) * U) and W32[e*m + r]
+ * the folded winner it leaves there.  Call with null arrays to read *n_elems.
+ * Replaces nothing in the reference: ProbMinHash4 (src/probmh.cpp:634-686)
+ * draws these values inline for each element of each contig. */
+int rbg_pmh_stream_tables(int32_t k, int32_t m, uint64_t pmh_seed, int32_t fp_contract,
+                          int32_t *n_elems, int32_t *canon_codes, double *U, uint32_t *W32);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RABBITBIN_B200_H */

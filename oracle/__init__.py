@@ -1,0 +1,147 @@
+"""ctypes bindings of the oracle libraries (test infrastructure only).
+
+Only tests/, the smoke check and bench.py's CPU-baseline leg import this
+package.  ``ref()`` is RabbitBin's own code compiled from the reference tree
+(see build.py); ``restated()`` is the plain CPU restatement in rb_oracle.cpp.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import build as _build
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+class RefParams(C.Structure):
+    _fields_ = [("n", C.c_int64), ("m", C.c_int32), ("S", C.c_int32),
+                ("win_bits", C.c_int32), ("max_edges", C.c_int32),
+                ("mutual", C.c_int32), ("base_on", C.c_int32),
+                ("nthreads", C.c_int32), ("seed", C.c_uint32),
+                ("force_path", C.c_int32), ("coverage", C.c_double),
+                ("min_edge", C.c_double), ("w_comp", C.c_double),
+                ("min_cv", C.c_double), ("neg_thr", C.c_double),
+                ("depth_sim", C.c_int32), ("depth_fuse", C.c_int32),
+                ("wjac_norm", C.c_int32), ("no_abdfirst", C.c_int32)]
+
+
+class RefOut(C.Structure):
+    _fields_ = [("b0", C.c_double), ("sim_cutoff", C.c_double),
+                ("n_edges", C.c_int64),
+                ("from_", C.POINTER(C.c_uint32)), ("to", C.POINTER(C.c_uint32)),
+                ("scomp", C.POINTER(C.c_float)), ("score", C.POINTER(C.c_float))]
+
+
+def default_params(n, m=500, S=0, **kw):
+    p = RefParams(n=n, m=m, S=S, win_bits=16, max_edges=200, mutual=1,
+                  base_on=1, nthreads=os.cpu_count() or 1, seed=1, force_path=0,
+                  coverage=0.95, min_edge=0.70, w_comp=-1.0, min_cv=1.0,
+                  neg_thr=-0.3, depth_sim=2, depth_fuse=1, wjac_norm=1, no_abdfirst=0)
+    if "abdfirst" in kw:
+        kw["no_abdfirst"] = 0 if kw.pop("abdfirst") else 1
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def _ptr(a, t):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+class _Lib:
+    """Common wrappers over the harness / restatement entry points."""
+
+    def __init__(self, path, prefix):
+        self.lib = C.CDLL(path)
+        self.path = path
+        L, p = self.lib, prefix
+        self._bw = getattr(L, p + "build_winners")
+        self._bw.restype = None
+        self._bw.argtypes = [C.c_char_p, C.POINTER(C.c_int64), C.c_int64, C.c_int,
+                             C.c_uint32, C.c_uint64, C.c_int, C.c_double,
+                             C.POINTER(C.c_uint32), C.c_int]
+        self._rg = getattr(L, p + "run_graph")
+        self._rg.restype = C.c_int
+        self._rg.argtypes = [C.POINTER(RefParams), C.POINTER(C.c_uint32),
+                             C.POINTER(C.c_float), C.POINTER(C.c_float),
+                             C.POINTER(RefOut)]
+        self._free = getattr(L, p + "free")
+        self._free.argtypes = [C.c_void_p]
+        self._pe = getattr(L, p + "pmh_elements")
+        self._pe.restype = None
+        self._pe.argtypes = [C.POINTER(C.c_uint64), C.POINTER(C.c_double), C.c_int64,
+                             C.c_uint32, C.c_uint64, C.POINTER(C.c_double),
+                             C.POINTER(C.c_uint64)]
+        self._ud = getattr(L, p + "unit_dot_f")
+        self._ud.restype = C.c_float
+        self._ud.argtypes = [C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_uint32]
+
+    def build_winners(self, seqcat, offsets, k=4, m=500, seed=42, gc_norm=1,
+                      gc_cap=20.0, nthreads=None):
+        n = len(offsets) - 1
+        out = np.zeros((n, m), dtype=np.uint32)
+        offs = np.ascontiguousarray(offsets, dtype=np.int64)
+        self._bw(seqcat, _ptr(offs, C.c_int64), n, k, m, seed, gc_norm, gc_cap,
+                 _ptr(out, C.c_uint32), nthreads or os.cpu_count() or 1)
+        return out
+
+    def run_graph(self, params, winners32, depth):
+        n, S = params.n, params.S
+        w = np.ascontiguousarray(winners32, dtype=np.uint32)
+        d = np.ascontiguousarray(depth, dtype=np.float32).reshape(n, max(S, 0))
+        unit = np.zeros((n, max(S, 1)), dtype=np.float32)
+        out = RefOut()
+        rc = self._rg(C.byref(params), _ptr(w, C.c_uint32), _ptr(d, C.c_float),
+                      _ptr(unit, C.c_float), C.byref(out))
+        if rc != 0:
+            raise RuntimeError(f"oracle run_graph failed: {rc}")
+        ne = out.n_edges
+        res = dict(b0=out.b0, sim_cutoff=out.sim_cutoff,
+                   src=np.ctypeslib.as_array(out.from_, (ne,)).copy() if ne else np.zeros(0, np.uint32),
+                   dst=np.ctypeslib.as_array(out.to, (ne,)).copy() if ne else np.zeros(0, np.uint32),
+                   scomp=np.ctypeslib.as_array(out.scomp, (ne,)).copy() if ne else np.zeros(0, np.float32),
+                   score=np.ctypeslib.as_array(out.score, (ne,)).copy() if ne else np.zeros(0, np.float32),
+                   unit=unit[:, :S] if S > 1 else None)
+        for ptr in (out.from_, out.to, out.scomp, out.score):
+            self._free(C.cast(ptr, C.c_void_p))
+        return res
+
+    def pmh_elements(self, keys, weights, m=500, seed=42):
+        keys = np.ascontiguousarray(keys, dtype=np.uint64)
+        w = np.ascontiguousarray(weights, dtype=np.float64)
+        regs = np.zeros(m, dtype=np.float64)
+        win = np.zeros(m, dtype=np.uint64)
+        self._pe(_ptr(keys, C.c_uint64), _ptr(w, C.c_double), len(keys), m, seed,
+                 _ptr(regs, C.c_double), _ptr(win, C.c_uint64))
+        return regs, win
+
+    def unit_dot_f(self, a, b):
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        b = np.ascontiguousarray(b, dtype=np.float32)
+        return float(self._ud(_ptr(a, C.c_float), _ptr(b, C.c_float), len(a)))
+
+
+_cache = {}
+
+
+def ref():
+    """RabbitBin's own hot-path code (None when not built and not buildable)."""
+    if "ref" not in _cache:
+        path = _build.build_ref()
+        _cache["ref"] = _Lib(path, "ref_") if path and os.path.exists(path) else None
+    return _cache["ref"]
+
+
+def restated():
+    """The CPU restatement of the hot path (always available)."""
+    if "orc" not in _cache:
+        _cache["orc"] = _Lib(_build.build_oracle(), "orc_")
+    return _cache["orc"]
+
+
+def sorted_edges(res):
+    """Edge set sorted by (src, dst): the reference emits rows in thread order."""
+    order = np.lexsort((res["dst"], res["src"]))
+    return (res["src"][order], res["dst"][order], res["scomp"][order],
+            res["score"][order])

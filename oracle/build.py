@@ -1,0 +1,101 @@
+"""Build recipe for the oracle libraries (test infrastructure only).
+
+Two host libraries come out of this script:
+
+* ``oracle/_build/librboracle.so`` — the CPU restatement in ``oracle/rb_oracle.cpp``
+  (committed source, always buildable).
+* ``oracle/_ref/librbref.so`` — RabbitBin's own hot-path code, compiled from the
+  reference tree where it lies.  ``src/probmh.cpp`` is compiled whole; the
+  functions that live inside the (unbuildable, Boost/libdeflate-dependent)
+  ``src/rabbitbin.cpp`` TU and the graph module ``src/impl/rb_graph.cpp`` are cut
+  out by line range into ``oracle/_ref/frag/`` at build time and #included by
+  ``oracle/ref_shim.cpp``.  Nothing from the reference tree is committed; the
+  ``_ref`` folder is git-ignored and travels to the GPU box prebuilt.
+
+Both are compiled with the reference's release flags
+(``src/CMakeLists.txt:211-253``: ``-O3 -march=native -funroll-loops -fopenmp``),
+with ``-march=x86-64-v4`` (AVX-512F/BW/DQ/VL) in place of ``native`` so the
+prebuilt library runs on any AVX-512 host and follows the AVX-512 code paths of
+the reference on every machine.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF = os.environ.get("RABBITBIN_REFERENCE", "/root/reference")
+REF_SRC = os.path.join(REF, "src")
+FLAGS = ["-std=c++17", "-O3", "-march=x86-64-v4", "-funroll-loops", "-fopenmp",
+         "-fPIC", "-shared", "-w"]
+
+# (fragment name, reference file, first line, last line)
+FRAGMENTS = [
+    ("frag_random_unique.inc", "rabbitbin.h", 330, 341),
+    ("frag_compare_edge.inc", "rabbitbin.h", 418, 429),
+    ("frag_fold16.inc", "rabbitbin.cpp", 249, 253),
+    ("frag_depth_terms.inc", "rabbitbin.cpp", 685, 970),
+    ("frag_pmh_sim.inc", "rabbitbin.cpp", 1194, 1426),
+    ("frag_build_winners.inc", "rabbitbin.cpp", 1436, 1589),
+    ("frag_anynz.inc", "impl/rb_abundance.cpp", 94, 114),
+    ("frag_graph_allpairs.inc", "impl/rb_graph.cpp", 7, 72),
+    ("frag_calib_converge.inc", "impl/rb_graph.cpp", 390, 415),
+    ("frag_fused_graph.inc", "impl/rb_graph.cpp", 489, 1356),
+    ("frag_calibrate.inc", "impl/rb_graph.cpp", 1362, 1384),
+]
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
+        raise RuntimeError("oracle build failed")
+
+
+def _stale(out, deps):
+    if not os.path.exists(out):
+        return True
+    t = os.path.getmtime(out)
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build_oracle():
+    """Compile the restatement oracle into oracle/_build/librboracle.so."""
+    out_dir = os.path.join(HERE, "_build")
+    os.makedirs(out_dir, exist_ok=True)
+    out = os.path.join(out_dir, "librboracle.so")
+    src = os.path.join(HERE, "rb_oracle.cpp")
+    if _stale(out, [src, __file__]):
+        _run(["g++"] + FLAGS + [src, "-o", out])
+    return out
+
+
+def build_ref():
+    """Compile the reference harness into oracle/_ref/librbref.so.
+
+    Returns the path, or None when the reference tree is absent (GPU box: the
+    prebuilt library travels with the snapshot instead)."""
+    out_dir = os.path.join(HERE, "_ref")
+    out = os.path.join(out_dir, "librbref.so")
+    if not os.path.isdir(REF_SRC):
+        return out if os.path.exists(out) else None
+    frag_dir = os.path.join(out_dir, "frag")
+    os.makedirs(frag_dir, exist_ok=True)
+    for name, rel, a, b in FRAGMENTS:
+        with open(os.path.join(REF_SRC, rel), encoding="utf-8") as f:
+            lines = f.readlines()
+        text = "".join(lines[a - 1:b])
+        path = os.path.join(frag_dir, name)
+        if not os.path.exists(path) or open(path, encoding="utf-8").read() != text:
+            with open(path, "w", encoding="utf-8") as f:
+                f.write(text)
+    shim = os.path.join(HERE, "ref_shim.cpp")
+    deps = [shim, __file__, os.path.join(REF_SRC, "probmh.cpp")]
+    if _stale(out, deps):
+        _run(["g++"] + FLAGS + ["-I", frag_dir, "-I", REF_SRC, shim,
+                                os.path.join(REF_SRC, "probmh.cpp"), "-o", out])
+    return out
+
+
+if __name__ == "__main__":
+    print(build_oracle())
+    print(build_ref())

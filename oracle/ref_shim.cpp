@@ -1,0 +1,380 @@
+// Reference harness: runs RabbitBin's own hot-path code on the host.
+//
+// TEST INFRASTRUCTURE ONLY.  This translation unit is the checker, never the
+// product: only tests/, the smoke check and bench.py's CPU-baseline leg load
+// the library it builds (oracle/_ref/librbref.so).
+//
+// The full `rabbitbin` binary cannot be built here (it needs Boost >= 1.66
+// headers and libdeflate).  oracle/build.py therefore compiles the hot-path
+// functions where they lie in the reference tree:
+//   * src/probmh.cpp (whole file, unchanged) + src/probmh.h, src/hash_int.h,
+//     src/rabbit_sketch.h, src/ranker.h, src/tile.h (headers, unchanged);
+//   * line ranges of src/rabbitbin.cpp, src/rabbitbin.h, src/impl/rb_graph.cpp
+//     and src/impl/rb_abundance.cpp, cut out verbatim into oracle/_ref/frag/
+//     at build time (never committed) and #included below.
+// What this file adds is only the surrounding declarations those functions
+// read (globals with the reference's names and defaults, a row-major stand-in
+// for the ublas depth matrix, logging stubs) and the glue that the reference
+// keeps inline in rb_cmd_bin (the winner pack loop src/rabbitbin.cpp:4934-4952,
+// b0 setup :4958-4965, colnorm :4792-4809, rank loop :4867-4874, unit rows
+// :4972-4988, graph dispatch :5035-5054, edge-weight loop :5482-5509).
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <climits>
+#include <cmath>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <immintrin.h>
+#include <limits>
+#include <memory>
+#include <numeric>
+#include <queue>
+#include <random>
+#include <string>
+#include <unordered_set>
+#include <utility>
+#include <vector>
+#include <omp.h>
+
+#include "probmh.h"
+#include "rabbit_sketch.h"
+#include "ranker.h"
+#include "tile.h"
+#include "ProgressTracker.h"
+
+// ── typedefs the fragments use (src/rabbitbin.h:71-102, :207, :213, :261-262) ──
+typedef double Distance;
+typedef double Similarity;
+typedef float StoredDistance;
+typedef std::pair<size_t, StoredDistance> Edge;
+typedef std::unordered_set<size_t> ContigSet;
+using GraphNodeId = uint32_t;
+using GraphEdgeId = uint32_t;
+
+// Data contract of the reference graph (src/rabbitbin.h:264-301), reduced to
+// the members the hot path touches.
+struct Graph {
+  size_t n;
+  std::vector<GraphNodeId> from, to;
+  std::vector<StoredDistance> sComp, edgeScore;
+  explicit Graph(size_t num_nodes) : n(num_nodes) {}
+  size_t getEdgeCount() { return from.size(); }
+};
+
+// Row-major float matrix standing in for boost::numeric::ublas::matrix<float>.
+struct RowMajorMatrix {
+  std::vector<float> v;
+  size_t cols = 0;
+  float &operator()(size_t r, size_t c) { return v[r * cols + c]; }
+  float operator()(size_t r, size_t c) const { return v[r * cols + c]; }
+};
+
+// ── globals read by the fragments, reference names and defaults ─────────────
+static bool verbose = false;
+static std::string depth_file;               // non-empty <=> depth input given
+static size_t numThreads = 1;
+static Similarity min_edge_weight = 0.70;
+static Distance minCV = 1.0;
+static size_t maxEdges = 200;
+static size_t nobs = 0;
+static size_t num_depth_samples = 0;
+static uint32_t sketch_size = 500;
+static uint32_t sketch_bits = 1;
+static RowMajorMatrix depth_matrix;
+static const size_t RB_SIM_FLOOR = 50;
+
+static int g_depth_sim = 2;
+static int g_depth_fuse = 1;
+static double g_depth_wjac_cut = 0.0;
+static bool g_depth_wjac_gate = false;
+static std::vector<float> g_depth_raw;
+static std::vector<double> g_depth_colnorm;
+static std::vector<float> g_depth_unit;
+static std::vector<float> g_snv_traj;
+static std::vector<char> g_snv_traj_have;
+static bool g_snv_edge = false;
+static double g_snv_edge_lo = 0.10;
+static bool g_dual_conj = false;
+static std::vector<float> g_depth_unit_blk;
+
+static std::vector<uint64_t> g_sig_flat;
+static uint32_t g_sig_nw = 0, g_sig_np = 0, g_sig_m = 0;
+static bool g_pmh_mode = true;
+static uint32_t g_pmh_m = 0;
+static std::vector<uint32_t> g_win_flat;
+static std::vector<uint64_t> g_win64_flat;
+static std::vector<uint16_t> g_win16;
+static int g_win_bits = 32;
+static bool g_pmh_base_on = true;
+static double g_pmh_baseline = 0.0;
+static double g_inv_pmh_m = 0.0;
+static double g_inv_one_minus_b0 = 1.0;
+static double g_w_comp = 0.5;
+static bool g_mutual_knn = true;
+static double g_neg_depth_thr = -0.3;
+static int g_gc_norm = 1;
+static double g_gc_norm_cap = 20.0;
+static bool g_exact_cos_cmp = false;
+static std::vector<float> g_k4cosine_flat;
+static std::vector<uint8_t> g_anynz;
+
+static void verbose_message(const char *, ...) {}
+static double getUsedPhysMem() { return 0.0; }
+static double getTotalPhysMem() { return 0.0; }
+static inline void numa_interleave_buffer(void *, size_t) {}
+static const char *rb_getenv(const char *key) {
+  const char *e = getenv(key);
+  return (e && e[0]) ? e : nullptr;
+}
+// Unused branches of the fragments (OPH signatures, Welford correlation).
+static inline double jaccard_raw(const uint64_t *, const uint64_t *, uint32_t,
+                                 uint32_t, uint32_t) { abort(); }
+double cal_depth_corr(size_t, size_t, bool = false, bool = false) { abort(); }
+
+#pragma omp declare reduction (merge_graphnode : std::vector<GraphNodeId> : omp_out.insert(omp_out.end(), omp_in.begin(), omp_in.end()) )
+#pragma omp declare reduction (merge_storeddist : std::vector<StoredDistance> : omp_out.insert(omp_out.end(), omp_in.begin(), omp_in.end()) )
+
+// ── reference code, verbatim line ranges (see oracle/build.py) ───────────────
+#include "frag_random_unique.inc"   // src/rabbitbin.h:330-341
+#include "frag_compare_edge.inc"    // src/rabbitbin.h:418-429
+#include "frag_fold16.inc"          // src/rabbitbin.cpp:249-253
+#include "frag_depth_terms.inc"     // src/rabbitbin.cpp:685-970
+#include "frag_pmh_sim.inc"         // src/rabbitbin.cpp:1194-1426
+#include "frag_build_winners.inc"   // src/rabbitbin.cpp:1436-1589
+#include "frag_anynz.inc"           // src/impl/rb_abundance.cpp:94-114
+#include "frag_graph_allpairs.inc"  // src/impl/rb_graph.cpp:7-72
+#include "frag_calib_converge.inc"  // src/impl/rb_graph.cpp:390-415
+#include "frag_fused_graph.inc"     // src/impl/rb_graph.cpp:480-1356
+#include "frag_calibrate.inc"       // src/impl/rb_graph.cpp:1362-1384
+
+// ═════════════════════════════════════════════════════════════════════════════
+// C entry points used by the tests and the CPU baseline.
+// ═════════════════════════════════════════════════════════════════════════════
+extern "C" {
+
+// Winner rows for n contigs (concatenated ASCII, offsets[n+1]), the parallel
+// sketch loop of src/rabbitbin.cpp:4849-4865 (one thread-local scratch each).
+void ref_build_winners(const char *seqcat, const int64_t *offsets, int64_t n,
+                       int k, uint32_t m, uint64_t seed, int gc_norm,
+                       double gc_cap, uint32_t *out32, int nthreads) {
+  g_gc_norm = gc_norm;
+  g_gc_norm_cap = gc_cap;
+  if (nthreads < 1) nthreads = 1;
+#pragma omp parallel num_threads(nthreads)
+  {
+    std::vector<uint64_t> scratch;
+#pragma omp for schedule(dynamic, 8)
+    for (int64_t r = 0; r < n; ++r)
+      build_pmh_winners(seqcat + offsets[r], (size_t)(offsets[r + 1] - offsets[r]),
+                        k, m, seed, out32 + (size_t)r * m, scratch);
+  }
+}
+
+void ref_fold16(const uint32_t *in, uint16_t *out, int64_t n) {
+  for (int64_t t = 0; t < n; ++t) out[t] = fold_win16(in[t]);
+}
+
+// Parameters of one graph + edge-weight run (the rb_cmd_bin globals).
+struct RefParams {
+  int64_t n;            // large contigs
+  int32_t m;            // --sketch-m
+  int32_t S;            // depth samples (0 = no depth file)
+  int32_t win_bits;     // 16 (default) or 32
+  int32_t max_edges;    // --max-edges
+  int32_t mutual;       // RABBIT_MUTUAL_KNN
+  int32_t base_on;      // RABBIT_PMH_BASE
+  int32_t nthreads;
+  uint32_t seed;        // --seed (srand)
+  int32_t force_path;   // 0 auto, 1 small-N, 2 fused large-N
+  double coverage;      // --max-posterior / 100
+  double min_edge;      // --min-edge-score / 100
+  double w_comp;        // < 0: auto_w_comp(S)
+  double min_cv;        // --min-coverage
+  double neg_thr;       // RABBIT_NEG_DEPTH
+  int32_t depth_sim;    // RABBIT_DEPTH_SIM
+  int32_t depth_fuse;   // RABBIT_DEPTH_FUSE
+  int32_t wjac_norm;    // RABBIT_DEPTH_WJAC_NORM
+  int32_t no_abdfirst;  // RABBIT_NO_ABDFIRST set
+};
+
+struct RefOut {
+  double b0;
+  double sim_cutoff;    // simCutoff (x1000 units, as returned by the reference)
+  int64_t n_edges;
+  uint32_t *from, *to;  // malloc'd, caller frees with ref_free
+  float *scomp, *score;
+};
+
+void ref_free(void *p) { free(p); }
+
+// Runs pack -> b0 -> ranks/unit rows -> graph -> edge weights exactly as
+// rb_cmd_bin does for a PMH run; winners32 holds the build_pmh_winners rows.
+// unit_out (n*S floats, may be null) receives g_depth_unit.
+int ref_run_graph(const RefParams *p, const uint32_t *winners32,
+                  const float *depth_raw, float *unit_out, RefOut *out) {
+  nobs = (size_t)p->n;
+  g_pmh_m = (uint32_t)p->m;
+  sketch_size = g_pmh_m;
+  g_inv_pmh_m = (g_pmh_m > 0) ? (1.0 / (double)g_pmh_m) : 0.0;
+  num_depth_samples = (size_t)(p->S > 0 ? p->S : 0);
+  depth_file = p->S > 0 ? "depth.tsv" : "";
+  maxEdges = (size_t)p->max_edges;
+  g_mutual_knn = p->mutual != 0;
+  g_pmh_base_on = p->base_on != 0;
+  numThreads = (size_t)(p->nthreads > 0 ? p->nthreads : 1);
+  min_edge_weight = p->min_edge;
+  minCV = p->min_cv;
+  g_neg_depth_thr = p->neg_thr;
+  g_depth_sim = p->depth_sim;
+  g_depth_fuse = p->depth_fuse;
+  // src/rabbitbin.cpp:4670-4673 (auto_w_comp: S<=2 -> 1, else 0)
+  g_w_comp = (p->w_comp < 0.0) ? (num_depth_samples <= 2 ? 1.0 : 0.0) : p->w_comp;
+  const size_t S = num_depth_samples;
+
+  // depth_matrix rows in FASTA order; raw snapshot + column norm
+  // (src/rabbitbin.cpp:4792-4809).
+  depth_matrix.cols = S;
+  depth_matrix.v.assign(depth_raw, depth_raw + nobs * S);
+  g_depth_raw.clear();
+  g_depth_colnorm.clear();
+  if (g_depth_sim >= 1 && S > 1) {
+    g_depth_raw.assign(depth_raw, depth_raw + nobs * S);
+    if (p->wjac_norm) {
+      g_depth_colnorm.assign(S, 1.0);
+      for (size_t i = 0; i < S; ++i) {
+        double s = 0.0;
+        for (size_t r = 0; r < nobs; ++r) s += g_depth_raw[r * S + i];
+        double mean = s / std::max<size_t>(nobs, 1);
+        g_depth_colnorm[i] = (mean > 1e-12) ? 1.0 / mean : 0.0;
+      }
+    }
+  }
+  // In-place Spearman rank per row (src/rabbitbin.cpp:4867-4874).
+  if (S > 1) {
+    std::vector<float> rowMat(S);
+    for (size_t r = 0; r < nobs; ++r) {
+      for (size_t k = 0; k < S; ++k) rowMat[k] = depth_matrix(r, k);
+      rank(rowMat, rowMat);
+      for (size_t k = 0; k < S; ++k) depth_matrix(r, k) = rowMat[k];
+    }
+  }
+  g_anynz.clear();
+  build_anynz_cache();
+
+  // 16-bit pack (src/rabbitbin.cpp:4934-4952).
+  g_win_flat.assign(winners32, winners32 + nobs * g_pmh_m);
+  g_win16.clear();
+  g_win_bits = 32;
+  if (p->win_bits == 16 && !g_win_flat.empty()) {
+    g_win16.resize(g_win_flat.size());
+    for (size_t t = 0; t < g_win_flat.size(); ++t) g_win16[t] = fold_win16(g_win_flat[t]);
+    g_win_bits = 16;
+    std::vector<uint32_t>().swap(g_win_flat);
+  }
+  // b0 (src/rabbitbin.cpp:4958-4965).
+  g_pmh_baseline = 0.0;
+  g_inv_one_minus_b0 = 1.0;
+  if (g_pmh_base_on) {
+    g_pmh_baseline = estimate_pmh_baseline(nobs);
+    g_inv_one_minus_b0 = (g_pmh_baseline < 1.0) ? (1.0 / (1.0 - g_pmh_baseline)) : 1.0;
+  }
+  // Unit rank rows (src/rabbitbin.cpp:4972-4988).
+  g_depth_unit.clear();
+  if (S > 1) {
+    g_depth_unit.assign(nobs * S, 0.0f);
+    for (size_t r = 0; r < nobs; ++r) {
+      double mean = 0.0;
+      for (size_t k = 0; k < S; ++k) mean += depth_matrix(r, k);
+      mean /= (double)S;
+      double ss = 0.0;
+      for (size_t k = 0; k < S; ++k) { double d = (double)depth_matrix(r, k) - mean; ss += d * d; }
+      if (ss > 0.0) {
+        const double inv = 1.0 / std::sqrt(ss);
+        float *u = g_depth_unit.data() + r * S;
+        for (size_t k = 0; k < S; ++k)
+          u[k] = (float)(((double)depth_matrix(r, k) - mean) * inv);
+      }
+    }
+    if (unit_out) std::copy(g_depth_unit.begin(), g_depth_unit.end(), unit_out);
+  }
+
+  // Graph (src/rabbitbin.cpp:5035-5054).
+  if (p->no_abdfirst) setenv("RABBIT_NO_ABDFIRST", "1", 1);
+  else unsetenv("RABBIT_NO_ABDFIRST");
+  srand(p->seed);
+  Graph g(nobs);
+  double simCutoff = 0.0;
+  const bool fused = (p->force_path == 2) || (p->force_path == 0 && nobs > 25000);
+  if (fused) {
+    simCutoff = gen_fused_calib_graph(g, p->coverage);
+  } else {
+    simCutoff = (double)calibrate_sim_cutoff(p->coverage, true);
+    build_graph_allpairs(g, simCutoff / 1000.);
+  }
+
+  // Edge weights, default fixed-cutoff branch (src/rabbitbin.cpp:5482-5509
+  // and the no-depth branch :5532-5536).  The GFA sentinel never occurs here.
+  const size_t ne = g.getEdgeCount();
+  g.edgeScore.assign(ne, 0.0f);
+  if (S > 0) {
+    for (size_t e = 0; e < ne; ++e) {
+      size_t i = g.from[e], j = g.to[e];
+      if (S <= 1) {
+        g.edgeScore[e] = (StoredDistance)(double)g.sComp[e];
+      } else {
+        bool depth_ok;
+        double dterm = depth_edge_term(i, j, depth_ok);
+        if (!depth_ok) { g.edgeScore[e] = 0.0f; continue; }
+        double sComp_v = g.sComp[e];
+        double min_edge_weight_v = min_edge_weight;
+        double w = g_w_comp * sComp_v + (1.0 - g_w_comp) * dterm;
+        if (!std::isfinite(w) || w < min_edge_weight_v) w = 0.0;
+        g.edgeScore[e] = (StoredDistance)w;
+      }
+    }
+  } else {
+    for (size_t e = 0; e < ne; ++e) {
+      float s = g.sComp[e];
+      if (s < min_edge_weight) s = 0.0f;
+      g.edgeScore[e] = s;
+    }
+  }
+
+  out->b0 = g_pmh_baseline;
+  out->sim_cutoff = simCutoff;
+  out->n_edges = (int64_t)ne;
+  out->from = (uint32_t *)malloc(sizeof(uint32_t) * (ne + 1));
+  out->to = (uint32_t *)malloc(sizeof(uint32_t) * (ne + 1));
+  out->scomp = (float *)malloc(sizeof(float) * (ne + 1));
+  out->score = (float *)malloc(sizeof(float) * (ne + 1));
+  for (size_t e = 0; e < ne; ++e) {
+    out->from[e] = g.from[e];
+    out->to[e] = g.to[e];
+    out->scomp[e] = g.sComp[e];
+    out->score[e] = g.edgeScore[e];
+  }
+  return 0;
+}
+
+// Float dot of two unit rows exactly as the abundance-first prune computes it.
+float ref_unit_dot_f(const float *a, const float *b, uint32_t S) {
+  return unit_dot_f(a, b, S);
+}
+
+// Full ProbMinHash4 state for one weighted element list (addHash order), for
+// kernel-level parity of registers and winners.
+void ref_pmh_elements(const uint64_t *keys, const double *weights, int64_t ne,
+                      uint32_t m, uint64_t seed, double *regs_out,
+                      uint64_t *winners_out) {
+  Sketch::ProbMinHash4 pmh(m, 4, seed);
+  for (int64_t t = 0; t < ne; ++t) pmh.addHash(keys[t], weights[t]);
+  const double *r = pmh.getRegisters();
+  const uint64_t *w = pmh.getWinners();
+  for (uint32_t t = 0; t < m; ++t) { regs_out[t] = r[t]; winners_out[t] = w[t]; }
+}
+
+}  // extern "C"

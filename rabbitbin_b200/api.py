@@ -1,0 +1,241 @@
+"""Python binding of the C ABI in include/rabbitbin_b200.h (ctypes).
+
+The product is the CUDA library ``librabbitbin_b200.so`` built in-tree by
+``rabbitbin_b200.build``; this module only marshals host arrays.  There is no
+CPU fallback: without a CUDA device every compute call raises ``RbgError``.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "librabbitbin_b200.so")
+
+RBG_OK = 0
+_STATUS = {-1: "bad argument", -2: "out of memory", -3: "CUDA error",
+           -4: "unsupported option", -5: "device wait timed out"}
+
+
+class RbgError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{_STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Params(C.Structure):
+    """rbg_params: `rabbitbin bin` options and hot-path RABBIT_* settings."""
+    _fields_ = [("k", C.c_int32), ("m", C.c_int32), ("pmh_seed", C.c_uint64),
+                ("gc_norm", C.c_int32), ("win_bits", C.c_int32),
+                ("gc_norm_cap", C.c_double), ("max_edges", C.c_int32),
+                ("mutual", C.c_int32), ("base_on", C.c_int32), ("seed", C.c_uint32),
+                ("force_path", C.c_int32), ("abdfirst", C.c_int32),
+                ("coverage", C.c_double), ("min_edge", C.c_double),
+                ("w_comp", C.c_double), ("min_cv", C.c_double), ("neg_thr", C.c_double),
+                ("depth_sim", C.c_int32), ("depth_fuse", C.c_int32),
+                ("wjac_norm", C.c_int32), ("fp_contract", C.c_int32),
+                ("wjac_cut", C.c_double), ("wjac_gate", C.c_int32), ("reserved", C.c_int32)]
+
+
+class Graph(C.Structure):
+    _fields_ = [("n_edges", C.c_int64), ("from_", C.POINTER(C.c_uint32)),
+                ("to", C.POINTER(C.c_uint32)), ("scomp", C.POINTER(C.c_float)),
+                ("score", C.POINTER(C.c_float)), ("b0", C.c_double),
+                ("sim_cutoff", C.c_double), ("path", C.c_int32), ("reserved", C.c_int32)]
+
+
+class Timing(C.Structure):
+    _fields_ = [(n, C.c_float) for n in ("pack_ms", "count_ms", "sketch_ms", "unit_ms",
+                                        "b0_ms", "allpairs_ms", "finalize_ms", "emit_ms",
+                                        "weight_ms", "total_ms")] + \
+               [("pairs_prefiltered", C.c_int64), ("pairs_compared", C.c_int64),
+                ("kernel_launches", C.c_int32), ("reserved", C.c_int32)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_ if n != "reserved"}
+
+
+_lib = None
+
+
+def lib():
+    """Load the in-tree library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RbgError(-4, f"{LIB_PATH} is missing; run python -m rabbitbin_b200.build")
+    L = C.CDLL(LIB_PATH)
+    P = C.POINTER
+    vp, i64p = C.c_void_p, P(C.c_int64)
+    sig = {
+        "rbg_default_params": ([P(Params)], C.c_int),
+        "rbg_create": ([C.c_int, P(vp)], C.c_int),
+        "rbg_destroy": ([vp], C.c_int),
+        "rbg_last_error": ([vp], C.c_char_p),
+        "rbg_stream": ([vp], vp),
+        "rbg_build_pmh_winners": ([vp, P(Params), C.c_char_p, i64p, C.c_int64,
+                                   P(C.c_uint32)], C.c_int),
+        "rbg_pack_win16": ([vp, P(C.c_uint32), C.c_int64, P(C.c_uint16)], C.c_int),
+        "rbg_estimate_pmh_baseline": ([vp, P(Params), vp, C.c_int32, C.c_int64,
+                                       P(C.c_double)], C.c_int),
+        "rbg_build_graph": ([vp, P(Params), P(C.c_uint32), C.c_int64, P(C.c_float),
+                             C.c_int32, P(Graph)], C.c_int),
+        "rbg_bin_graph": ([vp, P(Params), C.c_char_p, i64p, C.c_int64, P(C.c_float),
+                           C.c_int32, P(Graph)], C.c_int),
+        "rbg_stage": ([vp, C.c_char_p, i64p, C.c_int64, P(C.c_float), C.c_int32], C.c_int),
+        "rbg_run_resident": ([vp, P(Params), P(Timing)], C.c_int),
+        "rbg_fetch_graph": ([vp, P(Graph)], C.c_int),
+        "rbg_free_graph": ([P(Graph)], C.c_int),
+        "rbg_pmh_stream_tables": ([C.c_int32, C.c_int32, C.c_uint64, C.c_int32,
+                                   P(C.c_int32), P(C.c_int32), P(C.c_double),
+                                   P(C.c_uint32)], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes, f.restype = args, res
+    _lib = L
+    return L
+
+
+def exported_symbols():
+    """Entry points declared in include/rabbitbin_b200.h."""
+    hdr = os.path.join(os.path.dirname(_HERE), "include", "rabbitbin_b200.h")
+    import re
+    return sorted(set(re.findall(r"\b(rbg_[a-z0-9_]+)\s*\(", open(hdr).read())))
+
+
+def default_params(**kw):
+    p = Params()
+    lib().rbg_default_params(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def _p(a, t):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+def stream_tables(k=4, m=500, pmh_seed=42, fp_contract=1):
+    """(canonical codes, U [E, m] float64, W32 [E, m] uint32) of one configuration."""
+    L = lib()
+    ne = C.c_int32()
+    rc = L.rbg_pmh_stream_tables(k, m, pmh_seed, fp_contract, C.byref(ne), None, None, None)
+    if rc != RBG_OK:
+        raise RbgError(rc, "stream tables")
+    E = ne.value
+    codes = np.zeros(E, np.int32)
+    U = np.zeros((E, m), np.float64)
+    W = np.zeros((E, m), np.uint32)
+    rc = L.rbg_pmh_stream_tables(k, m, pmh_seed, fp_contract, C.byref(ne), _p(codes, C.c_int32),
+                                 _p(U, C.c_double), _p(W, C.c_uint32))
+    if rc != RBG_OK:
+        raise RbgError(rc, "stream tables")
+    return codes, U, W
+
+
+def _graph_dict(g):
+    ne = g.n_edges
+    take = (lambda ptr, dt: np.ctypeslib.as_array(ptr, (ne,)).astype(dt, copy=True)
+            if ne else np.zeros(0, dt))
+    return dict(src=take(g.from_, np.uint32), dst=take(g.to, np.uint32),
+                scomp=take(g.scomp, np.float32), score=take(g.score, np.float32),
+                b0=g.b0, sim_cutoff=g.sim_cutoff, path=g.path)
+
+
+class Context:
+    """One device context (stream + device buffers), like the reference's
+    per-thread sketch pool but on a GPU."""
+
+    def __init__(self, device=0):
+        self._L = lib()
+        h = C.c_void_p()
+        rc = self._L.rbg_create(device, C.byref(h))
+        if rc != RBG_OK:
+            raise RbgError(rc, f"cannot create a context on device {device}")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.rbg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc != RBG_OK:
+            raise RbgError(rc, f"{what}: {self._L.rbg_last_error(self._h).decode()}")
+
+    @property
+    def stream(self):
+        return self._L.rbg_stream(self._h)
+
+    def build_pmh_winners(self, seqcat, offsets, params=None):
+        p = params or default_params()
+        offs = np.ascontiguousarray(offsets, np.int64)
+        n = len(offs) - 1
+        out = np.zeros((n, p.m), np.uint32)
+        self._check(self._L.rbg_build_pmh_winners(self._h, C.byref(p), seqcat, _p(offs, C.c_int64),
+                                                  n, _p(out, C.c_uint32)), "build_pmh_winners")
+        return out
+
+    def pack_win16(self, w32):
+        w = np.ascontiguousarray(w32, np.uint32)
+        out = np.zeros(w.shape, np.uint16)
+        self._check(self._L.rbg_pack_win16(self._h, _p(w, C.c_uint32), w.size, _p(out, C.c_uint16)),
+                    "pack_win16")
+        return out
+
+    def estimate_pmh_baseline(self, winners, params=None):
+        p = params or default_params()
+        w = np.ascontiguousarray(winners)
+        bits = 16 if w.dtype == np.uint16 else 32
+        b0 = C.c_double()
+        self._check(self._L.rbg_estimate_pmh_baseline(self._h, C.byref(p), w.ctypes.data, bits,
+                                                      w.shape[0], C.byref(b0)), "estimate_pmh_baseline")
+        return b0.value
+
+    def _graph_call(self, fn, *args):
+        g = Graph()
+        self._check(fn(*args, C.byref(g)), fn.__name__)
+        try:
+            return _graph_dict(g)
+        finally:
+            self._L.rbg_free_graph(C.byref(g))
+
+    def build_graph(self, winners32, depth, params=None):
+        p = params or default_params()
+        w = np.ascontiguousarray(winners32, np.uint32)
+        n = w.shape[0]
+        d = np.ascontiguousarray(depth, np.float32).reshape(n, -1)
+        return self._graph_call(self._L.rbg_build_graph, self._h, C.byref(p), _p(w, C.c_uint32), n,
+                                _p(d, C.c_float), d.shape[1])
+
+    def bin_graph(self, seqcat, offsets, depth, params=None):
+        p = params or default_params()
+        offs = np.ascontiguousarray(offsets, np.int64)
+        n = len(offs) - 1
+        d = np.ascontiguousarray(depth, np.float32).reshape(n, -1)
+        return self._graph_call(self._L.rbg_bin_graph, self._h, C.byref(p), seqcat,
+                                _p(offs, C.c_int64), n, _p(d, C.c_float), d.shape[1])
+
+    def stage(self, seqcat, offsets, depth):
+        offs = np.ascontiguousarray(offsets, np.int64)
+        n = len(offs) - 1
+        d = np.ascontiguousarray(depth, np.float32).reshape(n, -1)
+        self._check(self._L.rbg_stage(self._h, seqcat, _p(offs, C.c_int64), n, _p(d, C.c_float),
+                                      d.shape[1]), "stage")
+
+    def run_resident(self, params=None):
+        p = params or default_params()
+        t = Timing()
+        self._check(self._L.rbg_run_resident(self._h, C.byref(p), C.byref(t)), "run_resident")
+        return t.as_dict()
+
+    def fetch_graph(self):
+        return self._graph_call(self._L.rbg_fetch_graph, self._h)

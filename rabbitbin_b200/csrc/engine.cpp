@@ -1,0 +1,816 @@
+// Host engine: device buffers, the orchestration of the hot path, the host
+// steps that stay sequential by definition (b0 sampling with mt19937_64, the
+// rand()-driven cutoff calibration), and the C ABI of include/rabbitbin_b200.h.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <functional>
+#include <mutex>
+#include <numeric>
+#include <random>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "rbg_internal.h"
+
+namespace rbg {
+void launch_fold16(const uint32_t *in, int64_t n, uint16_t *out, cudaStream_t s);
+void launch_raw_pair_counts(const void *win, int bits, int m, const int64_t *pairs, int np,
+                            uint32_t *out, cudaStream_t s);
+void launch_codes_from_winners(const uint32_t *w32, int64_t n, int m, int mpad, int use16,
+                               const uint32_t *vals, const uint8_t *codes, const int32_t *nvals,
+                               uint8_t *A, uint8_t *B, int *bad, cudaStream_t s);
+}  // namespace rbg
+
+namespace {
+
+using namespace rbg;
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+#define CK(x)                                                                     \
+  do {                                                                            \
+    cudaError_t e_ = (x);                                                         \
+    if (e_ != cudaSuccess)                                                        \
+      throw Error(e_ == cudaErrorMemoryAllocation ? RBG_ERR_NOMEM : RBG_ERR_CUDA, \
+                  std::string(#x) + ": " + cudaGetErrorString(e_));               \
+  } while (0)
+
+// A growable device allocation.
+struct DBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  template <typename T> T *as() const { return (T *)p; }
+  void ensure(size_t bytes) {
+    if (bytes <= cap) return;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    const size_t want = std::max<size_t>(bytes, 256);
+    CK(cudaMalloc(&p, want));
+    cap = want;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+// Pinned host staging buffer.
+struct HBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  void ensure(size_t bytes) {
+    if (bytes <= cap) return;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    CK(cudaMallocHost(&p, std::max<size_t>(bytes, 256)));
+    cap = std::max<size_t>(bytes, 256);
+  }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+inline int mpad_of(int m) { return (m + 15) & ~15; }
+
+// random_unique (src/rabbitbin.h:330-341): partial Fisher-Yates with rand().
+void rand_prefix_shuffle(std::vector<size_t> &v, size_t count) {
+  size_t left = v.size();
+  size_t b = 0;
+  while (count--) {
+    const size_t r = b + (size_t)rand() % left;
+    std::swap(v[b], v[r]);
+    ++b;
+    --left;
+  }
+}
+
+// calib_converge (src/impl/rb_graph.cpp:390-415): walk the cutoff p (x1000)
+// down in rand()-sized steps until the connected fraction reaches coverage.
+size_t converge_cutoff(const std::vector<double> &maxsim, double coverage) {
+  const size_t n = maxsim.size();
+  size_t p = 999, pp = 1000;
+  double cov = 0, pcov = 0;
+  for (; p > 50;) {
+    const double cutoff = (double)p / 1000.;
+    size_t on = 0;
+    for (size_t i = 0; i < n; ++i)
+      if (maxsim[i] >= cutoff) on++;
+    cov = (double)on / (double)n;
+    if (cov >= coverage) {
+      if (cov - coverage > coverage - pcov) { p = pp; cov = pcov; }
+      break;
+    }
+    pp = p;
+    pcov = cov;
+    if (p > 990) p -= rand() % 3 + 1;
+    else if (p > 900) p -= rand() % 3 + 3;
+    else p -= rand() % 3 + 9;
+  }
+  return p;
+}
+
+struct Tables {
+  std::shared_ptr<const PmhTables> t;
+  int win_bits = 16;
+  DBuf U, codeA, W32, rank;
+  DBuf dict_vals, dict_codes, dict_n;   // per-column sorted dictionaries
+  bool dict_ready = false;
+};
+
+}  // namespace
+
+struct rbg_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  std::mutex mu;
+  // staged inputs
+  int64_t n = 0, nbases = 0;
+  int S = 0;
+  std::vector<int64_t> h_offsets;
+  DBuf ascii, offsets, depth;
+  // sketch state
+  DBuf packed, nmask, elem_idx, elem_winv, elem_cnt, codesA, codesB, winners32;
+  // graph state
+  DBuf unit, anynz, colnorm, svbits, topk, topk_cnt, maxc_cand, maxc_all, stats;
+  DBuf pairs, pair_out, nbr, nbr_sv, nbr_cnt, row_edges;
+  DBuf e_from, e_to, e_scomp, e_score, badflag, tmp;
+  HBuf pin;
+  int64_t n_edges = 0;
+  double b0 = 0.0, sim_cutoff = 0.0;
+  int path = 0;
+  bool graph_ready = false;
+  // tables (one configuration cached)
+  std::unique_ptr<Tables> tables;
+  int tab_k = -1, tab_m = -1, tab_contract = -1, tab_bits = -1;
+  uint64_t tab_seed = 0;
+  cudaEvent_t ev[12];
+  int launches = 0;
+};
+
+namespace {
+
+void validate(const rbg_params *p) {
+  if (!p) throw Error(RBG_ERR_ARG, "null params");
+  if (p->k < 1 || p->k > 4) throw Error(RBG_ERR_UNSUPPORTED, "k must be in 1..4");
+  if (p->m < 2 || p->m > kMaxM) throw Error(RBG_ERR_ARG, "m must be in 2..4096");
+  if (p->win_bits != 16 && p->win_bits != 32) throw Error(RBG_ERR_ARG, "win_bits must be 16 or 32");
+  if (p->gc_norm != 0 && p->gc_norm != 1) throw Error(RBG_ERR_UNSUPPORTED, "gc_norm must be 0 or 1");
+  if (p->max_edges < 1 || p->max_edges > 480) throw Error(RBG_ERR_UNSUPPORTED, "max_edges must be in 1..480");
+  if (!(p->coverage > 0.0 && p->coverage < 1.0)) throw Error(RBG_ERR_ARG, "coverage must be in (0,1)");
+}
+
+Tables &tables_for(rbg_ctx *c, const rbg_params *p) {
+  if (c->tables && c->tab_k == p->k && c->tab_m == p->m && c->tab_seed == p->pmh_seed &&
+      c->tab_contract == (p->fp_contract != 0) && c->tab_bits == p->win_bits)
+    return *c->tables;
+  auto T = std::make_unique<Tables>();
+  T->t = pmh_tables(p->k, p->m, p->pmh_seed, p->fp_contract != 0);
+  T->win_bits = p->win_bits;
+  const PmhTables &t = *T->t;
+  const size_t EM = (size_t)t.n_elems * t.m;
+  T->U.ensure(EM * sizeof(double));
+  T->codeA.ensure(EM);
+  T->W32.ensure(EM * sizeof(uint32_t));
+  std::vector<int16_t> rk(t.rank_of_code.begin(), t.rank_of_code.end());
+  T->rank.ensure(rk.size() * sizeof(int16_t));
+  CK(cudaMemcpyAsync(T->U.p, t.U.data(), EM * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(T->codeA.p, p->win_bits == 16 ? t.code16.data() : t.code32.data(), EM,
+                     cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(T->W32.p, t.W32.data(), EM * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(T->rank.p, rk.data(), rk.size() * sizeof(int16_t), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->tables = std::move(T);
+  c->tab_k = p->k; c->tab_m = p->m; c->tab_seed = p->pmh_seed;
+  c->tab_contract = p->fp_contract != 0; c->tab_bits = p->win_bits;
+  return *c->tables;
+}
+
+void stage(rbg_ctx *c, const char *seqcat, const int64_t *offsets, int64_t n,
+           const float *depth, int S) {
+  if (n < 0 || (n > 0 && (!offsets || !seqcat))) throw Error(RBG_ERR_ARG, "bad sequence arguments");
+  if (S < 0 || S > kMaxS) throw Error(RBG_ERR_UNSUPPORTED, "S must be in 0..64");
+  if (S > 0 && n > 0 && !depth) throw Error(RBG_ERR_ARG, "depth is null");
+  if (n > 0 && offsets[0] != 0) throw Error(RBG_ERR_ARG, "offsets[0] must be 0");
+  for (int64_t i = 0; i < n; ++i)
+    if (offsets[i + 1] < offsets[i]) throw Error(RBG_ERR_ARG, "offsets must be non-decreasing");
+  c->n = n;
+  c->S = S;
+  c->nbases = n > 0 ? offsets[n] : 0;
+  c->h_offsets.assign(offsets, offsets + n + 1);
+  c->graph_ready = false;
+  const size_t abytes = (size_t)((c->nbases + 15) / 16) * 16 + 16;
+  c->ascii.ensure(abytes);
+  c->offsets.ensure((n + 1) * sizeof(int64_t));
+  c->depth.ensure(std::max<size_t>(1, (size_t)n * S) * sizeof(float));
+  CK(cudaMemsetAsync(c->ascii.p, 0, abytes, c->stream));
+  if (c->nbases)
+    CK(cudaMemcpyAsync(c->ascii.p, seqcat, (size_t)c->nbases, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->offsets.p, offsets, (n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
+  if (S > 0 && n > 0)
+    CK(cudaMemcpyAsync(c->depth.p, depth, (size_t)n * S * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+}
+
+// Sketch stage: pack, count + weights, register minimum.
+void run_sketch(rbg_ctx *c, const rbg_params *p, bool want_winners) {
+  Tables &T = tables_for(c, p);
+  const int64_t n = c->n;
+  const int m = p->m, mpad = mpad_of(p->m);
+  const int64_t nwords = (c->nbases + 15) / 16 + 1;
+  c->packed.ensure(nwords * 4);
+  c->nmask.ensure((nwords / 2 + 2) * 4);
+  c->elem_idx.ensure(std::max<int64_t>(n, 1) * kMaxElems);
+  c->elem_winv.ensure(std::max<int64_t>(n, 1) * kMaxElems * sizeof(double));
+  c->elem_cnt.ensure(std::max<int64_t>(n, 1) * sizeof(int32_t));
+  c->codesA.ensure(std::max<int64_t>(n, 1) * mpad);
+  c->codesB.ensure(std::max<int64_t>(n, 1) * mpad);
+  if (want_winners) c->winners32.ensure(std::max<int64_t>(n, 1) * m * sizeof(uint32_t));
+  CK(cudaEventRecord(c->ev[0], c->stream));
+  launch_pack(c->ascii.as<char>(), c->nbases, c->packed.as<uint32_t>(), c->nmask.as<uint32_t>(),
+              c->stream);
+  c->launches += c->nbases ? 1 : 0;
+  CK(cudaEventRecord(c->ev[1], c->stream));
+  SketchArgs a;
+  a.packed = c->packed.as<uint32_t>();
+  a.nmask = c->nmask.as<uint32_t>();
+  a.offsets = c->offsets.as<int64_t>();
+  a.n = n;
+  a.k = p->k;
+  a.m = m;
+  a.gc_norm = p->gc_norm;
+  a.gc_cap = p->gc_norm_cap;
+  a.n_elems = T.t->n_elems;
+  a.rank_of_code = T.rank.as<int16_t>();
+  a.elem_idx = c->elem_idx.as<uint8_t>();
+  a.elem_winv = c->elem_winv.as<double>();
+  a.elem_cnt = c->elem_cnt.as<int32_t>();
+  a.U = T.U.as<double>();
+  a.codeA = T.codeA.as<uint8_t>();
+  a.W32 = T.W32.as<uint32_t>();
+  a.codesA = c->codesA.as<uint8_t>();
+  a.codesB = c->codesB.as<uint8_t>();
+  a.winners32 = want_winners ? c->winners32.as<uint32_t>() : nullptr;
+  a.mpad = mpad;
+  launch_count(a, c->stream);
+  CK(cudaEventRecord(c->ev[2], c->stream));
+  launch_minreduce(a, c->stream);
+  CK(cudaEventRecord(c->ev[3], c->stream));
+  c->launches += n ? 2 : 0;
+  CK(cudaGetLastError());
+}
+
+// b0: median raw match fraction over 30000 mt19937_64 draws
+// (estimate_pmh_baseline, src/rabbitbin.cpp:1340-1369).
+double estimate_b0(rbg_ctx *c, int64_t n, int m, const std::function<void(const int64_t *, int, uint32_t *)> &count) {
+  if (n < 4) return 0.0;
+  const size_t NP = 30000;
+  std::mt19937_64 rng(0x9E3779B97F4A7C15ULL);
+  std::uniform_int_distribution<size_t> uni(0, (size_t)n - 1);
+  std::vector<int64_t> pr;
+  pr.reserve(2 * NP);
+  for (size_t s = 0; s < NP; ++s) {
+    const size_t i = uni(rng), j = uni(rng);
+    if (i == j) continue;
+    pr.push_back((int64_t)i);
+    pr.push_back((int64_t)j);
+  }
+  const int np = (int)(pr.size() / 2);
+  if (np == 0) return 0.0;
+  std::vector<uint32_t> cnt(np);
+  count(pr.data(), np, cnt.data());
+  const double inv_m = 1.0 / (double)m;
+  std::vector<float> vals(np);
+  for (int q = 0; q < np; ++q) vals[q] = (float)((double)cnt[q] * inv_m);
+  std::nth_element(vals.begin(), vals.begin() + vals.size() / 2, vals.end());
+  return (double)vals[vals.size() / 2];
+}
+
+void count_pairs_codes(rbg_ctx *c, int mpad, int m, const int64_t *pr, int np, uint32_t *out) {
+  c->pairs.ensure((size_t)np * 2 * sizeof(int64_t));
+  c->pair_out.ensure((size_t)np * sizeof(uint32_t));
+  CK(cudaMemcpyAsync(c->pairs.p, pr, (size_t)np * 2 * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
+  launch_pair_counts(c->codesA.as<uint8_t>(), c->codesB.as<uint8_t>(), mpad, m,
+                     c->pairs.as<int64_t>(), np, c->pair_out.as<uint32_t>(), c->stream);
+  c->launches++;
+  CK(cudaMemcpyAsync(out, c->pair_out.p, (size_t)np * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+}
+
+// Graph + edge weights on the codes already in c->codesA/B and the staged depth.
+void run_graph(rbg_ctx *c, const rbg_params *p) {
+  const int64_t n = c->n;
+  const int m = p->m, mpad = mpad_of(m), S = c->S, K = p->max_edges;
+  const int64_t n1 = std::max<int64_t>(n, 1);
+  c->unit.ensure(n1 * std::max(S, 1) * sizeof(float));
+  c->anynz.ensure(n1);
+  c->colnorm.ensure(std::max(S, 1) * sizeof(double));
+  c->svbits.ensure((m + 1) * sizeof(uint32_t));
+  c->topk.ensure(n1 * K * sizeof(uint64_t));
+  c->topk_cnt.ensure(n1 * sizeof(int32_t));
+  c->maxc_cand.ensure(n1 * sizeof(uint32_t));
+  c->maxc_all.ensure(n1 * sizeof(uint32_t));
+  c->stats.ensure(2 * sizeof(unsigned long long));
+
+  const double w_comp = (p->w_comp < 0.0) ? (S <= 2 ? 1.0 : 0.0) : p->w_comp;
+  GraphArgs g;
+  g.n = n; g.m = m; g.mpad = mpad; g.S = S; g.K = K;
+  g.codesA = c->codesA.as<uint8_t>();
+  g.codesB = c->codesB.as<uint8_t>();
+  g.depth_raw = c->depth.as<float>();
+  g.unit = c->unit.as<float>();
+  g.anynz = c->anynz.as<uint8_t>();
+  g.colnorm = c->colnorm.as<double>();
+  g.min_cv = (float)p->min_cv;
+  g.min_cv_d = p->min_cv;
+  g.has_depth = S > 0;
+  g.wjac_norm = p->wjac_norm;
+  launch_unit_rows(g, c->stream);
+  c->launches += n ? 1 : 0;
+  const bool need_colnorm = p->depth_sim >= 1 && S > 1 && p->wjac_norm;
+  if (need_colnorm) { launch_colnorm(g, c->stream); c->launches++; }
+  CK(cudaEventRecord(c->ev[4], c->stream));
+
+  // b0 on the codes (equal codes <=> equal winners of the chosen width)
+  c->b0 = 0.0;
+  if (p->base_on) {
+    c->b0 = estimate_b0(c, n, m, [&](const int64_t *pr, int np, uint32_t *out) {
+      count_pairs_codes(c, mpad, m, pr, np, out);
+    });
+  }
+  std::vector<double> sv_d;
+  std::vector<float> sv_f;
+  sv_table(m, p->base_on != 0, c->b0, sv_d, sv_f);
+  std::vector<uint32_t> sv_bits(m + 1);
+  std::memcpy(sv_bits.data(), sv_f.data(), (m + 1) * sizeof(uint32_t));
+  CK(cudaMemcpyAsync(c->svbits.p, sv_bits.data(), (m + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                     c->stream));
+  CK(cudaEventRecord(c->ev[5], c->stream));
+
+  const bool fused = (p->force_path == 2) || (p->force_path == 0 && n > 25000);
+  if (fused && n <= 2500) throw Error(RBG_ERR_ARG, "the fused path samples 2500 contigs; need n > 2500");
+  c->path = fused ? 2 : 1;
+  g.small_path = fused ? 0 : 1;
+  const bool abdfirst = fused && p->abdfirst && S > 1 && w_comp < 1.0 && w_comp < p->min_edge;
+  const double abd_corr_min = abdfirst ? (p->min_edge - w_comp) / (1.0 - w_comp) : -2.0;
+  g.prefilter = abdfirst ? 1 : 0;
+  g.prefilter_eps = (float)(abd_corr_min - 1e-4);
+  g.sv_bits = c->svbits.as<uint32_t>();
+  g.topk = c->topk.as<uint64_t>();
+  g.topk_cnt = c->topk_cnt.as<int32_t>();
+  g.maxcnt_cand = c->maxc_cand.as<uint32_t>();
+  g.maxcnt_all = c->maxc_all.as<uint32_t>();
+  g.stats = c->stats.as<unsigned long long>();
+  CK(cudaMemsetAsync(c->stats.p, 0, 2 * sizeof(unsigned long long), c->stream));
+  launch_allpairs(g, c->stream);
+  c->launches += n ? 1 : 0;
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(c->ev[6], c->stream));
+
+  // calibration on the host (rand() sequence of the reference)
+  std::vector<uint32_t> maxc(n1, 0);
+  CK(cudaMemcpyAsync(maxc.data(), fused ? c->maxc_cand.p : c->maxc_all.p, n * sizeof(uint32_t),
+                     cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  srand(p->seed);
+  double simCutoff;
+  if (!fused) {
+    std::vector<size_t> idx(n);
+    std::iota(idx.begin(), idx.end(), 0);
+    rand_prefix_shuffle(idx, (size_t)n);
+    std::vector<double> maxsim(n);
+    for (int64_t i = 0; i < n; ++i) maxsim[i] = sv_d[maxc[idx[i]]];
+    simCutoff = (double)converge_cutoff(maxsim, p->coverage);
+  } else {
+    const size_t NR = 10, SAMP = 2500;
+    std::vector<std::vector<size_t>> idxs(NR, std::vector<size_t>(n));
+    for (size_t r = 0; r < NR; ++r) {
+      std::iota(idxs[r].begin(), idxs[r].end(), 0);
+      rand_prefix_shuffle(idxs[r], SAMP);
+    }
+    std::vector<int8_t> sround(n, -1);
+    std::vector<size_t> slocal(n, 0);
+    for (int r = (int)NR - 1; r >= 0; --r)
+      for (size_t li = 0; li < SAMP; ++li) {
+        sround[idxs[r][li]] = (int8_t)r;
+        slocal[idxs[r][li]] = li;
+      }
+    std::vector<std::vector<float>> ms(NR, std::vector<float>(SAMP, 0.f));
+    for (int64_t ci = 0; ci < n; ++ci)
+      if (sround[ci] >= 0) {
+        const float v = sv_f[maxc[ci]];
+        float &slot = ms[sround[ci]][slocal[ci]];
+        if (v > slot) slot = v;
+      }
+    double sum_p = 0;
+    for (size_t r = 0; r < NR; ++r) {
+      std::vector<double> sub(SAMP);
+      for (size_t li = 0; li < SAMP; ++li) sub[li] = (double)ms[r][li];
+      double mp = (double)converge_cutoff(sub, p->coverage);
+      if (mp < 51.0) mp = 50.0;
+      sum_p += mp;
+      if (r == 1 && sum_p / 2 < 51.0) { sum_p = 500.0; break; }
+    }
+    simCutoff = sum_p / (double)NR;
+  }
+  c->sim_cutoff = simCutoff;
+  CK(cudaEventRecord(c->ev[7], c->stream));
+
+  // neighbour lists, edges
+  c->nbr.ensure(n1 * K * sizeof(uint32_t));
+  c->nbr_sv.ensure(n1 * K * sizeof(float));
+  c->nbr_cnt.ensure(n1 * sizeof(int32_t));
+  c->row_edges.ensure((n1 + 1) * sizeof(int32_t));
+  EmitArgs e;
+  e.n = n; e.K = K; e.mutual = p->mutual; e.small_path = fused ? 0 : 1;
+  e.topk = g.topk; e.topk_cnt = g.topk_cnt;
+  e.cutoff = simCutoff / 1000.;
+  e.nbr_sorted = c->nbr.as<uint32_t>();
+  e.nbr_sv = c->nbr_sv.as<float>();
+  e.nbr_cnt = c->nbr_cnt.as<int32_t>();
+  e.row_edges = c->row_edges.as<int32_t>();
+  launch_sort_rows(e, c->stream);
+  launch_count_edges(e, c->stream);
+  c->launches += n ? 3 : 0;
+  int32_t ne = 0;
+  if (n > 0) {
+    CK(cudaMemcpyAsync(&ne, c->row_edges.as<int32_t>() + n, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  c->n_edges = ne;
+  const size_t ne1 = std::max<int64_t>(ne, 1);
+  c->e_from.ensure(ne1 * 4);
+  c->e_to.ensure(ne1 * 4);
+  c->e_scomp.ensure(ne1 * 4);
+  c->e_score.ensure(ne1 * 4);
+  e.from = c->e_from.as<uint32_t>();
+  e.to = c->e_to.as<uint32_t>();
+  e.scomp = c->e_scomp.as<float>();
+  launch_write_edges(e, c->stream);
+  c->launches += n ? 1 : 0;
+  CK(cudaEventRecord(c->ev[8], c->stream));
+
+  WeightArgs w;
+  w.n_edges = ne;
+  w.S = S;
+  w.from = e.from; w.to = e.to; w.scomp = e.scomp;
+  w.score = c->e_score.as<float>();
+  w.unit = c->unit.as<float>();
+  w.depth_raw = c->depth.as<float>();
+  w.colnorm = need_colnorm ? c->colnorm.as<double>() : nullptr;
+  w.w_comp = w_comp;
+  w.min_edge = p->min_edge;
+  w.neg_thr = p->neg_thr;
+  w.wjac_cut = p->wjac_cut;
+  w.depth_sim = p->depth_sim;
+  w.depth_fuse = p->depth_fuse;
+  w.wjac_gate = p->wjac_gate;
+  w.contract = p->fp_contract;
+  launch_edge_weights(w, c->stream);
+  c->launches += ne ? 1 : 0;
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(c->ev[9], c->stream));
+  c->graph_ready = true;
+}
+
+void fetch(rbg_ctx *c, rbg_graph *out) {
+  if (!out) throw Error(RBG_ERR_ARG, "null graph");
+  if (!c->graph_ready) throw Error(RBG_ERR_ARG, "no graph has been built on this context");
+  std::memset(out, 0, sizeof(*out));
+  const size_t ne = (size_t)c->n_edges;
+  out->n_edges = (int64_t)ne;
+  out->b0 = c->b0;
+  out->sim_cutoff = c->sim_cutoff;
+  out->path = c->path;
+  const size_t nb = std::max<size_t>(ne, 1) * 4;
+  out->from = (uint32_t *)malloc(nb);
+  out->to = (uint32_t *)malloc(nb);
+  out->scomp = (float *)malloc(nb);
+  out->score = (float *)malloc(nb);
+  if (!out->from || !out->to || !out->scomp || !out->score) {
+    rbg_free_graph(out);
+    throw Error(RBG_ERR_NOMEM, "host allocation of the edge arrays failed");
+  }
+  if (ne) {
+    CK(cudaMemcpyAsync(out->from, c->e_from.p, ne * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(out->to, c->e_to.p, ne * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(out->scomp, c->e_scomp.p, ne * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(out->score, c->e_score.p, ne * 4, cudaMemcpyDeviceToHost, c->stream));
+  }
+  CK(cudaStreamSynchronize(c->stream));
+}
+
+// Map externally produced 32-bit winner rows onto register codes.
+void codes_from_winners(rbg_ctx *c, const rbg_params *p, const uint32_t *w32, int64_t n) {
+  Tables &T = tables_for(c, p);
+  const PmhTables &t = *T.t;
+  const int m = p->m, mpad = mpad_of(m);
+  if (!T.dict_ready) {
+    std::vector<uint32_t> vals((size_t)m * kMaxElems, 0);
+    std::vector<uint8_t> codes((size_t)m * kMaxElems, 0);
+    std::vector<int32_t> nv(m, 0);
+    const std::vector<uint8_t> &cd = p->win_bits == 16 ? t.code16 : t.code32;
+    for (int r = 0; r < m; ++r) {
+      std::vector<std::pair<uint32_t, uint8_t>> col;
+      for (int e = 0; e < t.n_elems; ++e) {
+        const size_t q = (size_t)e * m + r;
+        const uint32_t v = p->win_bits == 16 ? (uint32_t)t.W16[q] : t.W32[q];
+        if (v) col.emplace_back(v, cd[q]);
+      }
+      std::sort(col.begin(), col.end());
+      col.erase(std::unique(col.begin(), col.end()), col.end());
+      nv[r] = (int32_t)col.size();
+      for (size_t q = 0; q < col.size(); ++q) {
+        vals[(size_t)r * kMaxElems + q] = col[q].first;
+        codes[(size_t)r * kMaxElems + q] = col[q].second;
+      }
+    }
+    T.dict_vals.ensure(vals.size() * 4);
+    T.dict_codes.ensure(codes.size());
+    T.dict_n.ensure(nv.size() * 4);
+    CK(cudaMemcpyAsync(T.dict_vals.p, vals.data(), vals.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(T.dict_codes.p, codes.data(), codes.size(), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(T.dict_n.p, nv.data(), nv.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    T.dict_ready = true;
+  }
+  const int64_t n1 = std::max<int64_t>(n, 1);
+  c->winners32.ensure(n1 * m * 4);
+  c->codesA.ensure(n1 * mpad);
+  c->codesB.ensure(n1 * mpad);
+  c->badflag.ensure(sizeof(int));
+  CK(cudaMemsetAsync(c->badflag.p, 0, sizeof(int), c->stream));
+  if (n) CK(cudaMemcpyAsync(c->winners32.p, w32, (size_t)n * m * 4, cudaMemcpyHostToDevice, c->stream));
+  launch_codes_from_winners(c->winners32.as<uint32_t>(), n, m, mpad, p->win_bits == 16,
+                            T.dict_vals.as<uint32_t>(), T.dict_codes.as<uint8_t>(),
+                            T.dict_n.as<int32_t>(), c->codesA.as<uint8_t>(), c->codesB.as<uint8_t>(),
+                            c->badflag.as<int>(), c->stream);
+  int bad = 0;
+  CK(cudaMemcpyAsync(&bad, c->badflag.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (bad) throw Error(RBG_ERR_ARG, "winner rows do not come from this sketch configuration (k, m, seed)");
+}
+
+template <typename F>
+int guarded(rbg_ctx *c, F &&f) {
+  if (!c) return RBG_ERR_ARG;
+  std::lock_guard<std::mutex> lk(c->mu);
+  try {
+    CK(cudaSetDevice(c->device));
+    f();
+    c->err.clear();
+    return RBG_OK;
+  } catch (const Error &e) {
+    c->err = e.what();
+    return e.code;
+  } catch (const std::bad_alloc &) {
+    c->err = "host allocation failed";
+    return RBG_ERR_NOMEM;
+  } catch (const std::exception &e) {
+    c->err = e.what();
+    return RBG_ERR_CUDA;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int rbg_default_params(rbg_params *p) {
+  if (!p) return RBG_ERR_ARG;
+  std::memset(p, 0, sizeof(*p));
+  p->k = 4;
+  p->m = 500;
+  p->pmh_seed = 42;
+  p->gc_norm = 1;
+  p->win_bits = 16;
+  p->gc_norm_cap = 20.0;
+  p->max_edges = 200;
+  p->mutual = 1;
+  p->base_on = 1;
+  p->seed = 1;
+  p->force_path = 0;
+  p->abdfirst = 1;
+  p->coverage = 0.95;
+  p->min_edge = 0.70;
+  p->w_comp = -1.0;
+  p->min_cv = 1.0;
+  p->neg_thr = -0.3;
+  p->depth_sim = 2;
+  p->depth_fuse = 1;
+  p->wjac_norm = 1;
+  p->fp_contract = 1;
+  p->wjac_cut = 0.0;
+  p->wjac_gate = 0;
+  return RBG_OK;
+}
+
+int rbg_create(int device, rbg_ctx **out) {
+  if (!out) return RBG_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return RBG_ERR_CUDA;
+  if (device < 0 || device >= ndev) return RBG_ERR_ARG;
+  auto *c = new (std::nothrow) rbg_ctx();
+  if (!c) return RBG_ERR_NOMEM;
+  c->device = device;
+  if (cudaSetDevice(device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return RBG_ERR_CUDA;
+  }
+  for (auto &e : c->ev) cudaEventCreate(&e);
+  *out = c;
+  return RBG_OK;
+}
+
+int rbg_destroy(rbg_ctx *c) {
+  if (!c) return RBG_ERR_ARG;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  DBuf *bufs[] = {&c->ascii, &c->offsets, &c->depth, &c->packed, &c->nmask, &c->elem_idx,
+                  &c->elem_winv, &c->elem_cnt, &c->codesA, &c->codesB, &c->winners32, &c->unit,
+                  &c->anynz, &c->colnorm, &c->svbits, &c->topk, &c->topk_cnt, &c->maxc_cand,
+                  &c->maxc_all, &c->stats, &c->pairs, &c->pair_out, &c->nbr, &c->nbr_sv,
+                  &c->nbr_cnt, &c->row_edges, &c->e_from, &c->e_to, &c->e_scomp, &c->e_score,
+                  &c->badflag, &c->tmp};
+  for (DBuf *b : bufs) b->release();
+  if (c->tables) {
+    c->tables->U.release(); c->tables->codeA.release(); c->tables->W32.release();
+    c->tables->rank.release(); c->tables->dict_vals.release(); c->tables->dict_codes.release();
+    c->tables->dict_n.release();
+  }
+  c->pin.release();
+  for (auto &e : c->ev) cudaEventDestroy(e);
+  cudaStreamDestroy(c->stream);
+  delete c;
+  return RBG_OK;
+}
+
+const char *rbg_last_error(rbg_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+void *rbg_stream(rbg_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int rbg_build_pmh_winners(rbg_ctx *c, const rbg_params *p, const char *seqcat,
+                          const int64_t *offsets, int64_t n, uint32_t *out) {
+  return guarded(c, [&] {
+    validate(p);
+    if (!out && n > 0) throw Error(RBG_ERR_ARG, "null output");
+    stage(c, seqcat, offsets, n, nullptr, 0);
+    run_sketch(c, p, true);
+    if (n) CK(cudaMemcpyAsync(out, c->winners32.p, (size_t)n * p->m * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int rbg_pack_win16(rbg_ctx *c, const uint32_t *in, int64_t count, uint16_t *out) {
+  return guarded(c, [&] {
+    if (count < 0 || (count > 0 && (!in || !out))) throw Error(RBG_ERR_ARG, "bad arguments");
+    if (count == 0) return;
+    c->winners32.ensure(count * 4);
+    c->tmp.ensure(count * 2);
+    CK(cudaMemcpyAsync(c->winners32.p, in, count * 4, cudaMemcpyHostToDevice, c->stream));
+    launch_fold16(c->winners32.as<uint32_t>(), count, c->tmp.as<uint16_t>(), c->stream);
+    CK(cudaMemcpyAsync(out, c->tmp.p, count * 2, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int rbg_estimate_pmh_baseline(rbg_ctx *c, const rbg_params *p, const void *winners,
+                              int32_t win_bits, int64_t n, double *b0) {
+  return guarded(c, [&] {
+    validate(p);
+    if (!b0 || (n > 0 && !winners) || (win_bits != 16 && win_bits != 32))
+      throw Error(RBG_ERR_ARG, "bad arguments");
+    const int m = p->m;
+    const size_t bytes = (size_t)n * m * (win_bits / 8);
+    c->tmp.ensure(std::max<size_t>(bytes, 4));
+    if (bytes) CK(cudaMemcpyAsync(c->tmp.p, winners, bytes, cudaMemcpyHostToDevice, c->stream));
+    *b0 = estimate_b0(c, n, m, [&](const int64_t *pr, int np, uint32_t *o) {
+      c->pairs.ensure((size_t)np * 16);
+      c->pair_out.ensure((size_t)np * 4);
+      CK(cudaMemcpyAsync(c->pairs.p, pr, (size_t)np * 16, cudaMemcpyHostToDevice, c->stream));
+      launch_raw_pair_counts(c->tmp.p, win_bits, m, c->pairs.as<int64_t>(), np,
+                             c->pair_out.as<uint32_t>(), c->stream);
+      CK(cudaMemcpyAsync(o, c->pair_out.p, (size_t)np * 4, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+    });
+  });
+}
+
+int rbg_build_graph(rbg_ctx *c, const rbg_params *p, const uint32_t *winners32, int64_t n,
+                    const float *depth, int32_t S, rbg_graph *out) {
+  return guarded(c, [&] {
+    validate(p);
+    if (n < 0 || (n > 0 && !winners32) || !out) throw Error(RBG_ERR_ARG, "bad arguments");
+    if (S < 0 || S > kMaxS) throw Error(RBG_ERR_UNSUPPORTED, "S must be in 0..64");
+    c->n = n;
+    c->S = S;
+    c->depth.ensure(std::max<size_t>(1, (size_t)n * S) * sizeof(float));
+    if (S > 0 && n > 0) {
+      if (!depth) throw Error(RBG_ERR_ARG, "depth is null");
+      CK(cudaMemcpyAsync(c->depth.p, depth, (size_t)n * S * 4, cudaMemcpyHostToDevice, c->stream));
+    }
+    codes_from_winners(c, p, winners32, n);
+    run_graph(c, p);
+    fetch(c, out);
+  });
+}
+
+int rbg_bin_graph(rbg_ctx *c, const rbg_params *p, const char *seqcat, const int64_t *offsets,
+                  int64_t n, const float *depth, int32_t S, rbg_graph *out) {
+  return guarded(c, [&] {
+    validate(p);
+    stage(c, seqcat, offsets, n, depth, S);
+    run_sketch(c, p, false);
+    run_graph(c, p);
+    fetch(c, out);
+  });
+}
+
+int rbg_stage(rbg_ctx *c, const char *seqcat, const int64_t *offsets, int64_t n,
+              const float *depth, int32_t S) {
+  return guarded(c, [&] {
+    stage(c, seqcat, offsets, n, depth, S);
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int rbg_run_resident(rbg_ctx *c, const rbg_params *p, rbg_timing *t) {
+  return guarded(c, [&] {
+    validate(p);
+    c->launches = 0;
+    run_sketch(c, p, false);
+    run_graph(c, p);
+    CK(cudaStreamSynchronize(c->stream));
+    if (t) {
+      std::memset(t, 0, sizeof(*t));
+      auto el = [&](int a, int b) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev[a], c->ev[b]);
+        return ms;
+      };
+      t->pack_ms = el(0, 1);
+      t->count_ms = el(1, 2);
+      t->sketch_ms = el(2, 3);
+      t->unit_ms = el(3, 4);
+      t->b0_ms = el(4, 5);
+      t->allpairs_ms = el(5, 6);
+      t->finalize_ms = el(6, 7);
+      t->emit_ms = el(7, 8);
+      t->weight_ms = el(8, 9);
+      t->total_ms = el(0, 9);
+      unsigned long long st[2] = {0, 0};
+      CK(cudaMemcpy(st, c->stats.p, sizeof(st), cudaMemcpyDeviceToHost));
+      t->pairs_prefiltered = (int64_t)st[0];
+      t->pairs_compared = (int64_t)st[1];
+      t->kernel_launches = c->launches;
+    }
+  });
+}
+
+int rbg_fetch_graph(rbg_ctx *c, rbg_graph *out) {
+  return guarded(c, [&] { fetch(c, out); });
+}
+
+int rbg_pmh_stream_tables(int32_t k, int32_t m, uint64_t seed, int32_t contract, int32_t *n_elems,
+                          int32_t *codes, double *U, uint32_t *W32) {
+  if (k < 1 || k > 4 || m < 2 || m > kMaxM || !n_elems) return RBG_ERR_ARG;
+  try {
+    auto t = pmh_tables(k, m, seed, contract != 0);
+    *n_elems = t->n_elems;
+    if (codes) std::copy(t->canon_codes.begin(), t->canon_codes.end(), codes);
+    if (U) std::copy(t->U.begin(), t->U.end(), U);
+    if (W32) std::copy(t->W32.begin(), t->W32.end(), W32);
+    return RBG_OK;
+  } catch (...) {
+    return RBG_ERR_NOMEM;
+  }
+}
+
+int rbg_free_graph(rbg_graph *g) {
+  if (!g) return RBG_ERR_ARG;
+  free(g->from);
+  free(g->to);
+  free(g->scomp);
+  free(g->score);
+  g->from = g->to = nullptr;
+  g->scomp = g->score = nullptr;
+  g->n_edges = 0;
+  return RBG_OK;
+}
+
+}  // extern "C"

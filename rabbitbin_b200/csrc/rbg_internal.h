@@ -1,0 +1,143 @@
+// Internal declarations shared by the host engine and the CUDA kernels.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/rabbitbin_b200.h"
+
+namespace rbg {
+
+// Largest element universe handled with 8-bit register codes: the canonical
+// k-mers of k <= 4 (136 for k = 4).
+constexpr int kMaxElems = 136;
+constexpr int kMaxM = 4096;
+constexpr int kMaxS = 64;          // coverage samples held in registers
+constexpr int kRowsPerCta = 32;    // rows of one all-pairs CTA (one per lane)
+
+// ── PMH element streams (host, pmh_streams.cpp) ─────────────────────────────
+// For one sketch configuration (k, m, seed, arithmetic mode) every canonical
+// k-mer e has a fixed ProbMinHash stream: the register it visits at each step
+// and the weight-independent part U of the value it offers there
+// (hv = (1/w) * U).  Tables are indexed [e][register].
+struct PmhTables {
+  int k = 0, m = 0, n_elems = 0, contract = 1;
+  uint64_t seed = 0;
+  std::vector<int> canon_codes;        // ascending canonical codes, size n_elems
+  std::vector<int> rank_of_code;       // 4^k -> element index or -1
+  std::vector<double> U;               // [n_elems][m]
+  std::vector<uint64_t> W64;           // [n_elems][m] winner (RNG state)
+  std::vector<uint32_t> W32;           // folded h ^ (h >> 32)
+  std::vector<uint16_t> W16;           // fold_win16(W32)
+  std::vector<uint8_t> code16;         // 8-bit code of W16 per column (0 = unset)
+  std::vector<uint8_t> code32;         // 8-bit code of W32 per column (0 = unset)
+};
+
+// Builds (or returns the cached) tables for (k, m, seed, contract).
+std::shared_ptr<const PmhTables> pmh_tables(int k, int m, uint64_t seed, int contract);
+
+// The reference's similarity of a winner-match count, as a float and its
+// double (pmh_sv_from_count, src/rabbitbin.cpp:1297-1305).
+void sv_table(int m, bool base_on, double b0, std::vector<double> &sv_d,
+              std::vector<float> &sv_f);
+
+// ── kernel launchers (kernels_*.cu) ─────────────────────────────────────────
+struct SketchArgs {
+  // input: 2-bit packed bases (16 per word, first base in the top bits) and
+  // invalid-base mask (1 bit per base), covering the concatenated contigs
+  const uint32_t *packed = nullptr;
+  const uint32_t *nmask = nullptr;
+  const int64_t *offsets = nullptr;    // [n+1] base offsets
+  int64_t n = 0;
+  int k = 4, m = 500, gc_norm = 1, n_elems = 136;
+  double gc_cap = 20.0;
+  const int16_t *rank_of_code = nullptr;  // [4^k]
+  // per-contig element lists
+  uint8_t *elem_idx = nullptr;         // [n][kMaxElems]
+  double *elem_winv = nullptr;         // [n][kMaxElems]
+  int32_t *elem_cnt = nullptr;         // [n]
+  // tables
+  const double *U = nullptr;           // [E][m]
+  const uint8_t *codeA = nullptr;      // [E][m]
+  const uint32_t *W32 = nullptr;       // [E][m]
+  // outputs
+  uint8_t *codesA = nullptr;           // [n][mpad]  (0 = unset)
+  uint8_t *codesB = nullptr;           // [n][mpad]  (0xFF = unset)
+  uint32_t *winners32 = nullptr;       // [n][m], optional
+  int mpad = 512;                      // row stride of the code arrays (bytes)
+};
+
+void launch_pack(const char *ascii, int64_t nbases, uint32_t *packed, uint32_t *nmask,
+                 cudaStream_t s);
+void launch_count(const SketchArgs &a, cudaStream_t s);
+void launch_minreduce(const SketchArgs &a, cudaStream_t s);
+
+struct GraphArgs {
+  int64_t n = 0;
+  int m = 500, mpad = 512, S = 0, K = 200;
+  const uint8_t *codesA = nullptr, *codesB = nullptr;
+  const float *depth_raw = nullptr;    // [n][S]
+  float *unit = nullptr;               // [n][S] centred + L2-normalised ranks
+  uint8_t *anynz = nullptr;            // [n]
+  double *colnorm = nullptr;           // [S]
+  float min_cv = 1.0f;
+  double min_cv_d = 1.0;
+  int has_depth = 0;
+  int wjac_norm = 1;
+  // all-pairs
+  int small_path = 0;                  // N <= 25000 path: maxima over all j != i
+  int prefilter = 0;                   // abundance-first prune on
+  float prefilter_eps = 0.f;           // (float)(abd_corr_min - 1e-4)
+  const uint32_t *sv_bits = nullptr;   // [m+1] float bits of the similarity
+  uint64_t *topk = nullptr;            // [n][K] keys, descending
+  int32_t *topk_cnt = nullptr;         // [n]
+  uint32_t *maxcnt_cand = nullptr;     // [n] over candidates
+  uint32_t *maxcnt_all = nullptr;      // [n] over all j != i
+  unsigned long long *stats = nullptr; // [2] prefiltered, compared
+};
+
+void launch_unit_rows(const GraphArgs &g, cudaStream_t s);
+void launch_colnorm(const GraphArgs &g, cudaStream_t s);
+void launch_pair_counts(const uint8_t *codesA, const uint8_t *codesB, int mpad, int m,
+                        const int64_t *pairs, int npairs, uint32_t *out, cudaStream_t s);
+void launch_allpairs(const GraphArgs &g, cudaStream_t s);
+int allpairs_cap(int K);
+
+struct EmitArgs {
+  int64_t n = 0;
+  int K = 200, mutual = 1, small_path = 0;
+  const uint64_t *topk = nullptr;
+  const int32_t *topk_cnt = nullptr;
+  double cutoff = 0.0;
+  uint32_t *nbr_sorted = nullptr;      // [n][K] ids of kept neighbours, ascending
+  float *nbr_sv = nullptr;             // [n][K]
+  int32_t *nbr_cnt = nullptr;          // [n]
+  int32_t *row_edges = nullptr;        // [n+1] edges per row, then exclusive scan
+  uint32_t *from = nullptr, *to = nullptr;
+  float *scomp = nullptr;
+};
+
+void launch_sort_rows(const EmitArgs &e, cudaStream_t s);
+void launch_count_edges(const EmitArgs &e, cudaStream_t s);
+void launch_write_edges(const EmitArgs &e, cudaStream_t s);
+
+struct WeightArgs {
+  int64_t n_edges = 0;
+  int S = 0;
+  const uint32_t *from = nullptr, *to = nullptr;
+  const float *scomp = nullptr;
+  float *score = nullptr;
+  const float *unit = nullptr;
+  const float *depth_raw = nullptr;
+  const double *colnorm = nullptr;     // null = no column normalisation
+  double w_comp = 0.0, min_edge = 0.7, neg_thr = -0.3, wjac_cut = 0.0;
+  int depth_sim = 2, depth_fuse = 1, wjac_gate = 0, contract = 1;
+};
+
+void launch_edge_weights(const WeightArgs &w, cudaStream_t s);
+
+}  // namespace rbg

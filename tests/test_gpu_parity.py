@@ -1,0 +1,174 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU oracle.
+
+Registers, winner rows, b0, calibrated cutoffs, top-N derived edge sets and
+sComp are compared bit-exactly; edge weights exactly against the reference-
+order oracle and within 1e-6 absolute of an FP64 recomputation.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from rabbitbin_b200 import api
+from rabbitbin_b200.synth import make_assembly
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP64 = 1e-6   # edge weights vs the FP64 recomputation
+
+
+def _concat(seqs):
+    offs = np.zeros(len(seqs) + 1, np.int64)
+    offs[1:] = np.cumsum([len(s) for s in seqs])
+    return b"".join(seqs), offs
+
+
+def _edge_cases():
+    rng = np.random.default_rng(11)
+    rnd = lambda n: bytes(rng.choice(list(b"ACGT"), size=n))
+    return [
+        b"",                          # empty contig
+        b"ACG",                       # shorter than k
+        b"ACGT",                      # exactly one k-mer (palindrome)
+        b"NNNNNNNNNNNNNNNNNNNN",      # no valid base
+        b"AAAAAAAAAAAAAAAAAAAAAAAAAAAAAAAA",   # homopolymer
+        b"ACGT" * 100,                # palindromic 4-mers
+        rnd(3000).lower(),            # lower case
+        rnd(500) + b"N" + rnd(500) + b"NN" + rnd(3) + b"N" + rnd(700),  # N resets
+        rnd(2501),
+        bytes(rng.choice(list(b"ACGTNRYacgtn-"), size=4000)),         # IUPAC / gaps
+        rnd(17) + b"X" * 5 + rnd(33),
+    ]
+
+
+@pytest.mark.parametrize("m", [2, 3, 17, 250, 500, 1000])
+def test_winners_bit_exact(gpu_ctx, orc, m):
+    asm = make_assembly(8, 150, 0, seed=100 + m, n_frac=0.01)
+    seqs = _edge_cases() + asm.seqs
+    buf, offs = _concat(seqs)
+    p = api.default_params(m=m)
+    got = gpu_ctx.build_pmh_winners(buf, offs, p)
+    want = orc.build_winners(buf, offs, m=m)
+    assert got.shape == want.shape
+    bad = np.argwhere(got != want)
+    assert bad.size == 0, f"{len(bad)} registers differ, first {bad[:5]}"
+
+
+@pytest.mark.parametrize("k,gc", [(1, 1), (2, 1), (3, 1), (4, 0), (4, 1)])
+def test_winners_k_and_gcnorm(gpu_ctx, orc, k, gc):
+    asm = make_assembly(5, 80, 0, seed=7 * k + gc)
+    buf, offs = _concat(_edge_cases() + asm.seqs)
+    p = api.default_params(k=k, gc_norm=gc)
+    got = gpu_ctx.build_pmh_winners(buf, offs, p)
+    want = orc.build_winners(buf, offs, k=k, gc_norm=gc)
+    assert np.array_equal(got, want)
+
+
+def test_winners_against_reference(gpu_ctx, ref_lib):
+    asm = make_assembly(10, 300, 0, seed=5, n_frac=0.01)
+    buf, offs = _concat(_edge_cases() + asm.seqs)
+    got = gpu_ctx.build_pmh_winners(buf, offs)
+    assert np.array_equal(got, ref_lib.build_winners(buf, offs))
+
+
+def test_pack_win16(gpu_ctx, orc):
+    rng = np.random.default_rng(3)
+    w = rng.integers(0, 2**32, size=100000, dtype=np.uint64).astype(np.uint32)
+    w[:100] = 0
+    w[100:200] = 0x00010001   # folds to 0 -> 1
+    got = gpu_ctx.pack_win16(w)
+    h = (w ^ (w >> 16)).astype(np.uint16)
+    want = np.where(w == 0, 0, np.where(h == 0, 1, h)).astype(np.uint16)
+    assert np.array_equal(got, want)
+
+
+def _fp64_weights(asm, res, wc):
+    """Edge weights recomputed in FP64 from the oracle's unit rows."""
+    S = asm.n_samples
+    if S <= 1:
+        return None
+    unit = res["unit"].astype(np.float64)
+    d = asm.depth.astype(np.float64)
+    cn = d.mean(axis=0)
+    cn = np.where(cn > 1e-12, 1.0 / cn, 0.0)
+    i, j = res["src"].astype(np.int64), res["dst"].astype(np.int64)
+    rho = (unit[i] * unit[j]).sum(axis=1)
+    x, y = d[i] * cn, d[j] * cn
+    wj = np.minimum(x, y).sum(axis=1) / np.maximum(np.maximum(x, y).sum(axis=1), 1e-300)
+    wj = np.clip(wj, 0, 1)
+    dterm = np.minimum(np.maximum(rho, 0), wj)
+    w = wc * res["scomp"].astype(np.float64) + (1 - wc) * dterm
+    w[(rho < -0.3) | (w < 0.70)] = 0.0
+    return w
+
+
+def _graph_case(gpu_ctx, orc, G, N, S, seed, **kw):
+    asm = make_assembly(G, N, S, seed=seed, absent_frac=0.1 if S > 2 else 0.0)
+    buf, offs = asm.concat()
+    w = orc.build_winners(buf, offs)
+    op = oracle.default_params(asm.n, 500, S, **kw)
+    want = orc.run_graph(op, w, asm.depth)
+    gp = api.default_params(**kw)
+    got = gpu_ctx.bin_graph(buf, offs, asm.depth, gp)
+    assert got["b0"] == want["b0"]
+    assert got["sim_cutoff"] == want["sim_cutoff"]
+    ws, wd, wsc, wsw = oracle.sorted_edges(want)
+    assert np.array_equal(got["src"], ws) and np.array_equal(got["dst"], wd), \
+        f"edge sets differ: {len(got['src'])} vs {len(ws)}"
+    assert np.array_equal(got["scomp"], wsc)
+    assert np.array_equal(got["score"], wsw)
+    fp = _fp64_weights(asm, dict(want, src=ws, dst=wd, scomp=wsc), 0.0 if S > 2 else 1.0)
+    if fp is not None and S > 2:
+        agree = (fp > 0) == (wsw > 0)
+        err = np.abs(fp[agree] - wsw[agree].astype(np.float64))
+        assert err.size == 0 or err.max() <= TOL_FP64
+    return got
+
+
+@pytest.mark.parametrize("S", [0, 1, 2, 5])
+def test_graph_small_path(gpu_ctx, orc, S):
+    g = _graph_case(gpu_ctx, orc, 20, 2000, S, seed=40 + S)
+    assert g["path"] == 1
+
+
+@pytest.mark.parametrize("S,extra", [(3, {}), (10, {}), (20, {}), (30, {}), (40, {}),
+                                     (1, {}), (2, {}), (5, {"mutual": 0}),
+                                     (20, {"win_bits": 32}), (10, {"abdfirst": 0})])
+def test_graph_fused_path(gpu_ctx, orc, S, extra):
+    g = _graph_case(gpu_ctx, orc, 30, 4000, S, seed=60 + S, force_path=2, **extra)
+    assert g["path"] == 2
+
+
+def test_build_graph_from_reference_winners(gpu_ctx, ref_lib):
+    asm = make_assembly(20, 3000, 10, seed=9, absent_frac=0.1)
+    buf, offs = asm.concat()
+    w = ref_lib.build_winners(buf, offs)
+    p = oracle.default_params(asm.n, 500, 10, force_path=2)
+    want = ref_lib.run_graph(p, w, asm.depth)
+    got = gpu_ctx.build_graph(w, asm.depth, api.default_params(force_path=2))
+    ws, wd, wsc, wsw = oracle.sorted_edges(want)
+    assert got["b0"] == want["b0"] and got["sim_cutoff"] == want["sim_cutoff"]
+    assert np.array_equal(got["src"], ws) and np.array_equal(got["dst"], wd)
+    assert np.array_equal(got["scomp"], wsc) and np.array_equal(got["score"], wsw)
+
+
+def test_estimate_b0(gpu_ctx, ref_lib):
+    asm = make_assembly(15, 1500, 0, seed=21)
+    buf, offs = asm.concat()
+    w = ref_lib.build_winners(buf, offs)
+    p = oracle.default_params(asm.n, 500, 0)
+    want = ref_lib.run_graph(p, w, np.zeros((asm.n, 0), np.float32))["b0"]
+    w16 = gpu_ctx.pack_win16(w)
+    assert gpu_ctx.estimate_pmh_baseline(w16) == want
+
+
+def test_same_alone_and_repeated(gpu_ctx, orc):
+    """Device buffers are reused across calls: results do not depend on history."""
+    a = make_assembly(10, 800, 5, seed=31)
+    b = make_assembly(12, 1200, 10, seed=32)
+    ba, oa = a.concat()
+    bb, ob = b.concat()
+    first = gpu_ctx.bin_graph(ba, oa, a.depth)
+    gpu_ctx.bin_graph(bb, ob, b.depth, api.default_params(force_path=2 if b.n > 2500 else 0))
+    again = gpu_ctx.bin_graph(ba, oa, a.depth)
+    for k in ("src", "dst", "scomp", "score"):
+        assert np.array_equal(first[k], again[k])
