@@ -113,6 +113,16 @@ def _assembly(seed):
     return make_assembly(w["n_genomes"], w["n_contigs"], w["samples"], seed=seed)
 
 
+def _apply_size(args):
+    """--contigs/--samples shrink the workload (profiling cases only)."""
+    if args.contigs:
+        WORKLOAD["n_contigs"] = args.contigs
+        WORKLOAD["workload"] = (f"reduced assembly for profiling: {WORKLOAD['n_genomes']} genomes, "
+                                f"{args.contigs} contigs, S={args.samples or WORKLOAD['samples']}")
+    if args.samples:
+        WORKLOAD["samples"] = args.samples
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
@@ -157,6 +167,22 @@ def run_b200(args):
     value = world * pairs / (ms / 1000.0)
 
     # ── end to end through rbg_bin_graph with pinned host inputs ────────────
+    e2e_ms, e2e_edges = float("nan"), 0
+    if args.no_e2e:
+        pin_seq = None
+    else:
+        e2e_ms, e2e_edges = _e2e(args, ctx, buf, offs, asm, params, barrier, world, dev)
+    result_e2e = None if args.no_e2e else {
+        "value": world * pairs / (e2e_ms / 1000.0), "unit": UNIT, "ms_per_step": e2e_ms,
+        "h2d_bytes_per_step": int(len(buf) + offs.nbytes + asm.depth.nbytes),
+        "d2h_bytes_per_step": int(e2e_edges * 16)}
+    last = timings[-1]
+    return _finish(args, ctx, asm, timings, last, ms, value, result_e2e, clk, world, rank, dev)
+
+
+def _e2e(args, ctx, buf, offs, asm, params, barrier, world, dev):
+    import torch
+    import torch.distributed as dist
     pin_seq = torch.empty(len(buf), dtype=torch.uint8, pin_memory=True)
     pin_seq.numpy()[:] = np.frombuffer(buf, dtype=np.uint8)
     pin_depth = torch.empty(asm.depth.shape, dtype=torch.float32, pin_memory=True)
@@ -175,8 +201,11 @@ def run_b200(args):
         t = torch.tensor([e2e_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
+    return e2e_ms, e2e_edges
 
-    last = timings[-1]
+
+def _finish(args, ctx, asm, timings, last, ms, value, result_e2e, clk, world, rank, dev):
+    import torch.distributed as dist
     peaks, peak_src = _peaks()
     clocks = clk.summary()
     # dominant kernel: the all-pairs pass (abundance test on every ordered pair,
@@ -194,10 +223,7 @@ def run_b200(args):
         "dtype": "u8/u32 register codes, f64 sketch, f32 abundance",
         "data": "synthetic (seeded order-3 Markov genomes, lognormal coverage)",
         "config": dict(WORKLOAD, parallelism=f"{world} independent assemblies"),
-        "e2e": {"value": world * pairs / (e2e_ms / 1000.0), "unit": UNIT,
-                "ms_per_step": e2e_ms,
-                "h2d_bytes_per_step": int(len(buf) + offs.nbytes + asm.depth.nbytes),
-                "d2h_bytes_per_step": int(e2e_edges * 16)},
+        "e2e": result_e2e,
         "stages_ms": {k: round(v, 4) for k, v in last.items() if k.endswith("_ms")},
         "pairs_prefiltered": last["pairs_prefiltered"],
         "pairs_compared": last["pairs_compared"],
@@ -292,7 +318,11 @@ def main():
     ap.add_argument("--ref-contigs", type=int, default=12000)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--contigs", type=int, default=0, help="profiling: fewer contigs")
+    ap.add_argument("--samples", type=int, default=0, help="profiling: other S")
     args = ap.parse_args()
+    _apply_size(args)
     if args.impl == "reference":
         run_reference(args)
     else:

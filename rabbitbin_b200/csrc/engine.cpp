@@ -146,7 +146,7 @@ struct rbg_ctx {
   DBuf packed, nmask, elem_idx, elem_winv, elem_cnt, codesA, codesB, winners32;
   // graph state
   DBuf unit, anynz, colnorm, svbits, topk, topk_cnt, maxc_cand, maxc_all, stats;
-  DBuf pairs, pair_out, nbr, nbr_sv, nbr_cnt, row_edges;
+  DBuf pairs, pair_out, nbr, nbr_sv, nbr_cnt, row_edges, cand_buf;
   DBuf e_from, e_to, e_scomp, e_score, badflag, tmp;
   HBuf pin;
   int64_t n_edges = 0;
@@ -169,7 +169,7 @@ void validate(const rbg_params *p) {
   if (p->m < 2 || p->m > kMaxM) throw Error(RBG_ERR_ARG, "m must be in 2..4096");
   if (p->win_bits != 16 && p->win_bits != 32) throw Error(RBG_ERR_ARG, "win_bits must be 16 or 32");
   if (p->gc_norm != 0 && p->gc_norm != 1) throw Error(RBG_ERR_UNSUPPORTED, "gc_norm must be 0 or 1");
-  if (p->max_edges < 1 || p->max_edges > 480) throw Error(RBG_ERR_UNSUPPORTED, "max_edges must be in 1..480");
+  if (p->max_edges < 1 || p->max_edges > 448) throw Error(RBG_ERR_UNSUPPORTED, "max_edges must be in 1..448");
   if (!(p->coverage > 0.0 && p->coverage < 1.0)) throw Error(RBG_ERR_ARG, "coverage must be in (0,1)");
 }
 
@@ -205,6 +205,7 @@ void stage(rbg_ctx *c, const char *seqcat, const int64_t *offsets, int64_t n,
   if (S < 0 || S > kMaxS) throw Error(RBG_ERR_UNSUPPORTED, "S must be in 0..64");
   if (S > 0 && n > 0 && !depth) throw Error(RBG_ERR_ARG, "depth is null");
   if (n > 0 && offsets[0] != 0) throw Error(RBG_ERR_ARG, "offsets[0] must be 0");
+  if (n >= (1 << 27)) throw Error(RBG_ERR_UNSUPPORTED, "at most 2^27 - 1 contigs per assembly");
   for (int64_t i = 0; i < n; ++i)
     if (offsets[i + 1] < offsets[i]) throw Error(RBG_ERR_ARG, "offsets must be non-decreasing");
   c->n = n;
@@ -314,7 +315,8 @@ void run_graph(rbg_ctx *c, const rbg_params *p) {
   const int64_t n = c->n;
   const int m = p->m, mpad = mpad_of(m), S = c->S, K = p->max_edges;
   const int64_t n1 = std::max<int64_t>(n, 1);
-  c->unit.ensure(n1 * std::max(S, 1) * sizeof(float));
+  const int Su = (std::max(S, 1) + 3) & ~3;
+  c->unit.ensure(n1 * Su * sizeof(float));
   c->anynz.ensure(n1);
   c->colnorm.ensure(std::max(S, 1) * sizeof(double));
   c->svbits.ensure((m + 1) * sizeof(uint32_t));
@@ -326,7 +328,7 @@ void run_graph(rbg_ctx *c, const rbg_params *p) {
 
   const double w_comp = (p->w_comp < 0.0) ? (S <= 2 ? 1.0 : 0.0) : p->w_comp;
   GraphArgs g;
-  g.n = n; g.m = m; g.mpad = mpad; g.S = S; g.K = K;
+  g.n = n; g.m = m; g.mpad = mpad; g.S = S; g.K = K; g.Su = Su;
   g.codesA = c->codesA.as<uint8_t>();
   g.codesB = c->codesB.as<uint8_t>();
   g.depth_raw = c->depth.as<float>();
@@ -374,7 +376,8 @@ void run_graph(rbg_ctx *c, const rbg_params *p) {
   g.maxcnt_all = c->maxc_all.as<uint32_t>();
   g.stats = c->stats.as<unsigned long long>();
   CK(cudaMemsetAsync(c->stats.p, 0, 2 * sizeof(unsigned long long), c->stream));
-  launch_allpairs(g, c->stream);
+  c->cand_buf.ensure((size_t)((n + 127) / 128 * 128) * allpairs_cap(K) * sizeof(uint64_t));
+  launch_allpairs(g, c->cand_buf.as<uint64_t>(), c->stream);
   c->launches += n ? 1 : 0;
   CK(cudaGetLastError());
   CK(cudaEventRecord(c->ev[6], c->stream));
@@ -469,6 +472,7 @@ void run_graph(rbg_ctx *c, const rbg_params *p) {
   w.from = e.from; w.to = e.to; w.scomp = e.scomp;
   w.score = c->e_score.as<float>();
   w.unit = c->unit.as<float>();
+  w.Su = Su;
   w.depth_raw = c->depth.as<float>();
   w.colnorm = need_colnorm ? c->colnorm.as<double>() : nullptr;
   w.w_comp = w_comp;
@@ -646,7 +650,7 @@ int rbg_destroy(rbg_ctx *c) {
                   &c->anynz, &c->colnorm, &c->svbits, &c->topk, &c->topk_cnt, &c->maxc_cand,
                   &c->maxc_all, &c->stats, &c->pairs, &c->pair_out, &c->nbr, &c->nbr_sv,
                   &c->nbr_cnt, &c->row_edges, &c->e_from, &c->e_to, &c->e_scomp, &c->e_score,
-                  &c->badflag, &c->tmp};
+                  &c->badflag, &c->tmp, &c->cand_buf};
   for (DBuf *b : bufs) b->release();
   if (c->tables) {
     c->tables->U.release(); c->tables->codeA.release(); c->tables->W32.release();

@@ -48,7 +48,7 @@ __global__ void k_unit_rows(GraphArgs g) {
     const double d = __dsub_rn((double)rk[k], mean);
     ss = __dadd_rn(ss, __dmul_rn(d, d));
   }
-  float *u = g.unit + r * S;
+  float *u = g.unit + r * g.Su;
   if (ss > 0.0) {
     const double inv = 1.0 / __dsqrt_rn(ss);
     for (int k = 0; k < S; ++k)
@@ -56,17 +56,29 @@ __global__ void k_unit_rows(GraphArgs g) {
   } else {
     for (int k = 0; k < S; ++k) u[k] = 0.0f;
   }
+  for (int k = S; k < g.Su; ++k) u[k] = 0.0f;
 }
 
 // Column norms of the raw depths, summed in row order
-// (src/rabbitbin.cpp:4800-4806).
+// (src/rabbitbin.cpp:4800-4806): one CTA stages row chunks in shared memory
+// with coalesced loads; thread i < S adds its column sequentially.
 __global__ void k_colnorm(GraphArgs g) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= g.S) return;
+  constexpr int CH = 128;
+  __shared__ float chunk[CH * kMaxS];
+  const int S = g.S, i = threadIdx.x;
   double s = 0.0;
-  for (int64_t r = 0; r < g.n; ++r) s = __dadd_rn(s, (double)g.depth_raw[r * g.S + i]);
-  const double mean = s / (double)(g.n > 1 ? g.n : 1);
-  g.colnorm[i] = (mean > 1e-12) ? 1.0 / mean : 0.0;
+  for (int64_t r0 = 0; r0 < g.n; r0 += CH) {
+    const int rows = (int)((g.n - r0) < CH ? (g.n - r0) : CH);
+    __syncthreads();
+    for (int q = threadIdx.x; q < rows * S; q += blockDim.x) chunk[q] = g.depth_raw[r0 * S + q];
+    __syncthreads();
+    if (i < S)
+      for (int r = 0; r < rows; ++r) s = __dadd_rn(s, (double)chunk[r * S + i]);
+  }
+  if (i < S) {
+    const double mean = s / (double)(g.n > 1 ? g.n : 1);
+    g.colnorm[i] = (mean > 1e-12) ? 1.0 / mean : 0.0;
+  }
 }
 
 // Number of registers where two 8-bit code words agree (A side: 0 = unset,
@@ -87,42 +99,6 @@ __global__ void k_pair_counts(const uint8_t *__restrict__ A, const uint8_t *__re
   uint32_t c = 0;
   for (int w = 0; w < mpad / 4; ++w) c += match4(__ldg(a + w), __ldg(b + w));
   out[p] = c;
-}
-
-// unit_dot_f (src/rabbitbin.cpp:754-796) on an AVX-512 host: element t goes to
-// lane t % 16 of accumulator acc1 when it lies in the second half of a full
-// 32-element block, else of acc0; the masked tail joins acc0; the lanes are
-// then reduced as _mm512_reduce_add_ps does (halves of 8, 4, 2, 1).
-template <int SMAX>
-__device__ __forceinline__ float unit_dot_avx512(const float (&a)[SMAX], const float *b,
-                                                 int S) {
-  float acc0[16], acc1[16];
-#pragma unroll
-  for (int l = 0; l < 16; ++l) { acc0[l] = 0.f; acc1[l] = 0.f; }
-  const int lim32 = S & ~31;
-#pragma unroll
-  for (int t = 0; t < SMAX; ++t) {
-    if (t < S) {
-      if ((t & 16) && t < lim32) acc1[t & 15] = __fmaf_rn(a[t], b[t], acc1[t & 15]);
-      else acc0[t & 15] = __fmaf_rn(a[t], b[t], acc0[t & 15]);
-    }
-  }
-  float v[16];
-  if (lim32 > 0) {
-#pragma unroll
-    for (int l = 0; l < 16; ++l) v[l] = __fadd_rn(acc0[l], acc1[l]);
-  } else {
-    // acc1 is all zeros: acc0 + 0 only differs in the sign of a zero lane
-#pragma unroll
-    for (int l = 0; l < 16; ++l) v[l] = acc0[l];
-  }
-#pragma unroll
-  for (int l = 0; l < 8; ++l) v[l] = __fadd_rn(v[l], v[l + 8]);
-#pragma unroll
-  for (int l = 0; l < 4; ++l) v[l] = __fadd_rn(v[l], v[l + 4]);
-  v[0] = __fadd_rn(v[0], v[2]);
-  v[1] = __fadd_rn(v[1], v[3]);
-  return __fadd_rn(v[0], v[1]);
 }
 
 // Bitonic sort, descending, of `len` (power of two) keys in shared memory by
@@ -148,158 +124,6 @@ __device__ __forceinline__ int pow2_at_least(int x) {
   int p = 1;
   while (p < x) p <<= 1;
   return p;
-}
-
-constexpr int kWarps = 8;       // warps per all-pairs CTA
-constexpr int kColsPerWarp = 2; // columns a warp handles between CTA syncs
-constexpr int kColWords = 8;    // column code words a lane keeps in registers
-
-// Compact one row's candidate buffer: keep the K best keys (descending) and
-// move the admission threshold up to the K-th best.
-__device__ void compact_row(uint64_t *buf, int &cnt, uint64_t &thr, int K, int cap) {
-  const int lane = threadIdx.x & 31;
-  const int len = pow2_at_least(cnt > 1 ? cnt : 2);
-  for (int i = cnt + lane; i < len; i += 32) buf[i] = 0;
-  __syncwarp();
-  warp_sort_desc(buf, len);
-  if (cnt >= K) {
-    thr = buf[K - 1];
-    cnt = K;
-  }
-  __syncwarp();
-}
-
-// All-pairs pass over full rows.  CTA = 32 rows (lane = row) x 8 warps that
-// walk the columns; per (row, column) pair: is_nz, the abundance-first float
-// test, the register-match count (warp-cooperative, only for surviving pairs),
-// the per-row maximum count and admission of the (similarity, id) key into the
-// row's top-K buffer.  Sampled-row calibration and both graph paths are served
-// from the per-row maxima and top-K lists this pass leaves behind.
-template <int SMAX>
-__global__ void __launch_bounds__(kWarps * 32)
-k_allpairs(GraphArgs g, int cap, int small_path) {
-  extern __shared__ uint64_t sh[];
-  uint64_t *buf = sh;                                     // [32][cap]
-  uint64_t *thr = buf + (size_t)kRowsPerCta * cap;        // [32]
-  int *bcnt = (int *)(thr + kRowsPerCta);                 // [32]
-  uint32_t *maxc = (uint32_t *)(bcnt + kRowsPerCta);      // [32]
-  uint32_t *maxa = maxc + kRowsPerCta;                    // [32]
-  int *need = (int *)(maxa + kRowsPerCta);                // [1]
-  uint32_t *rowA = (uint32_t *)(need + 4);                // [32][mpad/4]
-
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int64_t row0 = (int64_t)blockIdx.x * kRowsPerCta;
-  const int64_t row = row0 + lane;
-  const bool vrow = row < g.n;
-  const int mw = g.mpad >> 2;
-  const int S = g.S;
-  const int K = g.K;
-
-  for (int i = threadIdx.x; i < kRowsPerCta; i += blockDim.x) {
-    thr[i] = 0; bcnt[i] = 0; maxc[i] = 0; maxa[i] = 0;
-  }
-  for (int i = threadIdx.x; i < kRowsPerCta * mw; i += blockDim.x) {
-    const int r = i / mw, w = i - r * mw;
-    rowA[i] = (row0 + r < g.n) ? __ldg((const uint32_t *)(g.codesA + (row0 + r) * g.mpad) + w) : 0u;
-  }
-  float ur[SMAX];
-#pragma unroll
-  for (int t = 0; t < SMAX; ++t) ur[t] = (vrow && t < S && g.prefilter) ? g.unit[row * S + t] : 0.f;
-  const uint8_t nz_row = vrow ? g.anynz[row] : 0;
-  __syncthreads();
-
-  uint32_t my_maxc = 0, my_maxa = 0;
-  unsigned long long n_pref = 0, n_cmp = 0;
-  const int64_t step = (int64_t)kWarps * kColsPerWarp;
-  for (int64_t j0 = 0; j0 < g.n; j0 += step) {
-    for (int q = 0; q < kColsPerWarp; ++q) {
-      const int64_t j = j0 + warp * kColsPerWarp + q;
-      if (j >= g.n) break;
-      const bool other = vrow && j != row;
-      bool cand = other && (nz_row | __ldg(g.anynz + j));
-      if (cand && g.prefilter) {
-        float ub[SMAX];
-        const float *uj = g.unit + j * S;
-#pragma unroll
-        for (int t = 0; t < SMAX; ++t) ub[t] = (t < S) ? __ldg(uj + t) : 0.f;
-        const float c = unit_dot_avx512<SMAX>(ur, ub, S);
-        ++n_pref;
-        if (c < g.prefilter_eps) cand = false;
-      }
-      const bool count_it = small_path ? other : cand;
-      uint32_t mask = __ballot_sync(FULL, count_it);
-      if (mask == 0) continue;
-      n_cmp += (count_it ? 1 : 0);
-      // column j's B codes: lane holds words lane, lane+32, ...
-      const uint32_t *cb = (const uint32_t *)(g.codesB + j * g.mpad);
-      uint32_t colw[kColWords];
-#pragma unroll
-      for (int t = 0; t < kColWords; ++t) {
-        const int w = lane + 32 * t;
-        colw[t] = (w < mw) ? __ldg(cb + w) : 0xFFFFFFFFu;
-      }
-      uint32_t cnt = 0;
-      while (mask) {
-        const int r = __ffs(mask) - 1;
-        mask &= mask - 1;
-        const uint32_t *ra = rowA + r * mw;
-        uint32_t part = 0;
-#pragma unroll
-        for (int t = 0; t < kColWords; ++t) {
-          const int w = lane + 32 * t;
-          if (w < mw) part += match4(ra[w], colw[t]);
-        }
-        for (int w = lane + 32 * kColWords; w < mw; w += 32)
-          part += match4(ra[w], __ldg(cb + w));
-        const uint32_t tot = __reduce_add_sync(FULL, part);
-        if (lane == r) cnt = tot;
-      }
-      if (count_it) {
-        if (small_path) my_maxa = cnt > my_maxa ? cnt : my_maxa;
-        if (cand) {
-          my_maxc = cnt > my_maxc ? cnt : my_maxc;
-          const uint64_t key = ((uint64_t)__ldg(g.sv_bits + cnt) << 32) |
-                               (uint64_t)(~(uint32_t)j);
-          if (key > thr[lane]) {
-            const int p = atomicAdd(&bcnt[lane], 1);
-            buf[(size_t)lane * cap + p] = key;
-          }
-        }
-      }
-    }
-    __syncthreads();
-    // compact rows whose buffers could overflow before the next sync
-    for (int r = warp; r < kRowsPerCta; r += kWarps) {
-      int c = bcnt[r];
-      if (c > cap - (int)step) {
-        uint64_t t = thr[r];
-        compact_row(buf + (size_t)r * cap, c, t, K, cap);
-        if (lane == 0) { bcnt[r] = c; thr[r] = t; }
-      }
-    }
-    __syncthreads();
-  }
-  atomicMax(&maxc[lane], my_maxc);
-  atomicMax(&maxa[lane], my_maxa);
-  if (g.stats) {
-    if (n_pref) atomicAdd(g.stats, n_pref);
-    if (n_cmp) atomicAdd(g.stats + 1, n_cmp);
-  }
-  __syncthreads();
-  for (int r = warp; r < kRowsPerCta; r += kWarps) {
-    const int64_t gr = row0 + r;
-    if (gr >= g.n) continue;
-    int c = bcnt[r];
-    uint64_t t = thr[r];
-    compact_row(buf + (size_t)r * cap, c, t, K, cap);
-    const int keep = c < K ? c : K;
-    for (int i = lane; i < keep; i += 32) g.topk[gr * K + i] = buf[(size_t)r * cap + i];
-    if (lane == 0) {
-      g.topk_cnt[gr] = keep;
-      g.maxcnt_cand[gr] = maxc[r];
-      g.maxcnt_all[gr] = maxa[r];
-    }
-  }
 }
 
 // ── neighbour lists: cut by the calibrated threshold, sorted by id ──────────
@@ -467,13 +291,13 @@ __global__ void k_edge_weights(WeightArgs w) {
     else if (w.wjac_cut > 0.0 && wj < w.wjac_cut) ok = false;
     else {
       if (w.wjac_gate && w.neg_thr > -0.99) {
-        const double corr = depth_corr(w.unit + i * S, w.unit + j * S, S);
+        const double corr = depth_corr(w.unit + i * w.Su, w.unit + j * w.Su, S);
         if (isfinite(corr) && corr < w.neg_thr) ok = false;
       }
       dterm = wj < 0.0 ? 0.0 : (wj > 1.0 ? 1.0 : wj);
     }
   } else {
-    const double corr = depth_corr(w.unit + i * S, w.unit + j * S, S);
+    const double corr = depth_corr(w.unit + i * w.Su, w.unit + j * w.Su, S);
     if (!isfinite(corr)) ok = false;
     else if (w.neg_thr > -0.99 && corr < w.neg_thr) ok = false;
     else {
@@ -508,7 +332,7 @@ void launch_unit_rows(const GraphArgs &g, cudaStream_t s) {
 
 void launch_colnorm(const GraphArgs &g, cudaStream_t s) {
   if (g.S == 0) return;
-  k_colnorm<<<1, 64, 0, s>>>(g);
+  k_colnorm<<<1, 256, 0, s>>>(g);
 }
 
 void launch_pair_counts(const uint8_t *A, const uint8_t *B, int mpad, int m,
@@ -516,34 +340,6 @@ void launch_pair_counts(const uint8_t *A, const uint8_t *B, int mpad, int m,
   (void)m;
   if (np == 0) return;
   k_pair_counts<<<(np + 127) / 128, 128, 0, s>>>(A, B, mpad, pairs, np, out);
-}
-
-static size_t allpairs_smem(int cap, int mpad) {
-  return (size_t)kRowsPerCta * cap * 8 + kRowsPerCta * 8 + kRowsPerCta * 4 * 3 + 16 +
-         (size_t)kRowsPerCta * mpad;
-}
-
-int allpairs_cap(int K) {
-  int c = 1;
-  while (c < K + 2 * kWarps * kColsPerWarp) c <<= 1;
-  return c;
-}
-
-void launch_allpairs(const GraphArgs &g, cudaStream_t s) {
-  if (g.n == 0) return;
-  const int cap = allpairs_cap(g.K);
-  const size_t smem = allpairs_smem(cap, g.mpad);
-  const unsigned grid = (unsigned)((g.n + kRowsPerCta - 1) / kRowsPerCta);
-  if (g.S <= 16) {
-    cudaFuncSetAttribute(k_allpairs<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_allpairs<16><<<grid, kWarps * 32, smem, s>>>(g, cap, g.small_path);
-  } else if (g.S <= 32) {
-    cudaFuncSetAttribute(k_allpairs<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_allpairs<32><<<grid, kWarps * 32, smem, s>>>(g, cap, g.small_path);
-  } else {
-    cudaFuncSetAttribute(k_allpairs<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_allpairs<64><<<grid, kWarps * 32, smem, s>>>(g, cap, g.small_path);
-  }
 }
 
 void launch_sort_rows(const EmitArgs &e, cudaStream_t s) {

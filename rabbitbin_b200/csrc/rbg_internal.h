@@ -79,9 +79,10 @@ void launch_minreduce(const SketchArgs &a, cudaStream_t s);
 struct GraphArgs {
   int64_t n = 0;
   int m = 500, mpad = 512, S = 0, K = 200;
+  int Su = 4;                          // row stride of `unit` (S rounded up to 4)
   const uint8_t *codesA = nullptr, *codesB = nullptr;
   const float *depth_raw = nullptr;    // [n][S]
-  float *unit = nullptr;               // [n][S] centred + L2-normalised ranks
+  float *unit = nullptr;               // [n][Su] centred + L2-normalised ranks, 0-padded
   uint8_t *anynz = nullptr;            // [n]
   double *colnorm = nullptr;           // [S]
   float min_cv = 1.0f;
@@ -104,7 +105,7 @@ void launch_unit_rows(const GraphArgs &g, cudaStream_t s);
 void launch_colnorm(const GraphArgs &g, cudaStream_t s);
 void launch_pair_counts(const uint8_t *codesA, const uint8_t *codesB, int mpad, int m,
                         const int64_t *pairs, int npairs, uint32_t *out, cudaStream_t s);
-void launch_allpairs(const GraphArgs &g, cudaStream_t s);
+void launch_allpairs(const GraphArgs &g, uint64_t *gbuf, cudaStream_t s);
 int allpairs_cap(int K);
 
 struct EmitArgs {
@@ -131,7 +132,8 @@ struct WeightArgs {
   const uint32_t *from = nullptr, *to = nullptr;
   const float *scomp = nullptr;
   float *score = nullptr;
-  const float *unit = nullptr;
+  const float *unit = nullptr;         // [n][Su]
+  int Su = 4;
   const float *depth_raw = nullptr;
   const double *colnorm = nullptr;     // null = no column normalisation
   double w_comp = 0.0, min_edge = 0.7, neg_thr = -0.3, wjac_cut = 0.0;

@@ -172,3 +172,30 @@ def test_same_alone_and_repeated(gpu_ctx, orc):
     again = gpu_ctx.bin_graph(ba, oa, a.depth)
     for k in ("src", "dst", "scomp", "score"):
         assert np.array_equal(first[k], again[k])
+
+
+def test_against_golden_fixtures(gpu_ctx):
+    """Outputs of RabbitBin's own code, committed as fixtures (no reference tree
+    is needed at run time)."""
+    import os
+    gdir = os.path.join(os.path.dirname(__file__), "golden")
+    files = sorted(f for f in os.listdir(gdir) if f.endswith(".npz"))
+    assert files
+    for f in files:
+        z = np.load(os.path.join(gdir, f))
+        seqcat, offs, m = z["seqcat"].tobytes(), z["offsets"], int(z["m"])
+        w = gpu_ctx.build_pmh_winners(seqcat, offs, api.default_params(m=m))
+        assert np.array_equal(w, z["winners32"]), f
+        if "src" in z.files:
+            p = api.default_params(m=m, force_path=int(z["force_path"]))
+            g = gpu_ctx.bin_graph(seqcat, offs, z["depth"], p)
+            assert g["b0"] == float(z["b0"]) and g["sim_cutoff"] == float(z["sim_cutoff"]), f
+            assert np.array_equal(g["src"], z["src"]) and np.array_equal(g["dst"], z["dst"]), f
+            assert np.array_equal(g["scomp"], z["scomp"]), f
+            assert np.array_equal(g["score"], z["score"]), f
+
+
+@pytest.mark.parametrize("N,S,fp", [(2599, 7, 2), (2601, 33, 2), (3001, 2, 2), (1999, 4, 1)])
+def test_graph_ragged_sizes(gpu_ctx, orc, N, S, fp):
+    """Row/column counts that leave partial CTA tiles."""
+    _graph_case(gpu_ctx, orc, 25, N, S, seed=N, force_path=fp)
