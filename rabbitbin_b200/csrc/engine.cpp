@@ -12,6 +12,7 @@
 #include <numeric>
 #include <random>
 #include <stdexcept>
+#include <unordered_map>
 #include <string>
 #include <vector>
 
@@ -85,29 +86,19 @@ struct HBuf {
 
 inline int mpad_of(int m) { return (m + 15) & ~15; }
 
-// random_unique (src/rabbitbin.h:330-341): partial Fisher-Yates with rand().
-void rand_prefix_shuffle(std::vector<size_t> &v, size_t count) {
-  size_t left = v.size();
-  size_t b = 0;
-  while (count--) {
-    const size_t r = b + (size_t)rand() % left;
-    std::swap(v[b], v[r]);
-    ++b;
-    --left;
-  }
-}
-
 // calib_converge (src/impl/rb_graph.cpp:390-415): walk the cutoff p (x1000)
 // down in rand()-sized steps until the connected fraction reaches coverage.
+// The count of maxsim >= cutoff comes from a sorted copy (same counts, same
+// rand() calls).
 size_t converge_cutoff(const std::vector<double> &maxsim, double coverage) {
   const size_t n = maxsim.size();
+  std::vector<double> sorted(maxsim);
+  std::sort(sorted.begin(), sorted.end());
   size_t p = 999, pp = 1000;
   double cov = 0, pcov = 0;
   for (; p > 50;) {
     const double cutoff = (double)p / 1000.;
-    size_t on = 0;
-    for (size_t i = 0; i < n; ++i)
-      if (maxsim[i] >= cutoff) on++;
+    const size_t on = n - (size_t)(std::lower_bound(sorted.begin(), sorted.end(), cutoff) - sorted.begin());
     cov = (double)on / (double)n;
     if (cov >= coverage) {
       if (cov - coverage > coverage - pcov) { p = pp; cov = pcov; }
@@ -120,6 +111,27 @@ size_t converge_cutoff(const std::vector<double> &maxsim, double coverage) {
     else p -= rand() % 3 + 9;
   }
   return p;
+}
+
+// random_unique (src/rabbitbin.h:330-341), a partial Fisher-Yates driven by
+// rand(): the first `count` entries it leaves in iota(n), without
+// materialising the n-entry vector (positions touched are tracked lazily).
+// `val`/`stamp` are scratch of n entries reused across calls (stamp marks the
+// positions this call has written).
+std::vector<size_t> rand_prefix_of_iota(size_t n, size_t count, std::vector<size_t> &val,
+                                        std::vector<uint32_t> &stamp, uint32_t cur) {
+  auto at = [&](size_t i) { return stamp[i] == cur ? val[i] : i; };
+  auto put = [&](size_t i, size_t v) { val[i] = v; stamp[i] = cur; };
+  std::vector<size_t> out(count);
+  size_t left = n;
+  for (size_t b = 0; b < count; ++b, --left) {
+    const size_t r = b + (size_t)rand() % left;
+    const size_t vb = at(b), vr = at(r);
+    put(r, vb);
+    put(b, vr);
+    out[b] = vr;
+  }
+  return out;
 }
 
 struct Tables {
@@ -146,8 +158,8 @@ struct rbg_ctx {
   DBuf packed, nmask, elem_idx, elem_winv, elem_cnt, codesA, codesB, winners32;
   // graph state
   DBuf unit, anynz, colnorm, svbits, topk, topk_cnt, maxc_cand, maxc_all, stats;
-  DBuf pairs, pair_out, nbr, nbr_sv, nbr_cnt, row_edges, cand_buf;
-  DBuf e_from, e_to, e_scomp, e_score, badflag, tmp;
+  DBuf pairs, pair_out, nbr, nbr_sv, nbr_cnt, row_edges, cand_buf, cand_cnt;
+  DBuf e_from, e_to, e_scomp, e_score, badflag, tmp, colacc;
   HBuf pin;
   int64_t n_edges = 0;
   double b0 = 0.0, sim_cutoff = 0.0;
@@ -158,6 +170,9 @@ struct rbg_ctx {
   int tab_k = -1, tab_m = -1, tab_contract = -1, tab_bits = -1;
   uint64_t tab_seed = 0;
   cudaEvent_t ev[12];
+  cudaStream_t aux = nullptr;            // depth preparation, overlapped with the sketch
+  cudaEvent_t ev_in = nullptr, ev_aux = nullptr, ev_a0 = nullptr, ev_a1 = nullptr;
+  bool prep_done = false;
   int launches = 0;
 };
 
@@ -225,6 +240,42 @@ void stage(rbg_ctx *c, const char *seqcat, const int64_t *offsets, int64_t n,
     CK(cudaMemcpyAsync(c->depth.p, depth, (size_t)n * S * sizeof(float), cudaMemcpyHostToDevice, c->stream));
 }
 
+bool need_colnorm(const rbg_params *p, int S) { return p->depth_sim >= 1 && S > 1 && p->wjac_norm; }
+
+// Unit rank rows, anynz and column norms on the auxiliary stream: they depend
+// only on the coverage table, so they overlap the sketch kernels.
+void prep_depth(rbg_ctx *c, const rbg_params *p) {
+  const int64_t n = c->n, n1 = std::max<int64_t>(n, 1);
+  const int S = c->S;
+  const int Su = (std::max(S, 1) + 3) & ~3;
+  c->unit.ensure(n1 * Su * sizeof(float));
+  c->anynz.ensure(n1);
+  c->colnorm.ensure(std::max(S, 1) * sizeof(double));
+  GraphArgs g;
+  g.n = n; g.S = S; g.Su = Su;
+  g.depth_raw = c->depth.as<float>();
+  g.unit = c->unit.as<float>();
+  g.anynz = c->anynz.as<uint8_t>();
+  g.colnorm = c->colnorm.as<double>();
+  g.min_cv = (float)p->min_cv;
+  g.min_cv_d = p->min_cv;
+  g.has_depth = S > 0;
+  g.wjac_norm = p->wjac_norm;
+  CK(cudaEventRecord(c->ev_in, c->stream));
+  CK(cudaStreamWaitEvent(c->aux, c->ev_in, 0));
+  CK(cudaEventRecord(c->ev_a0, c->aux));
+  launch_unit_rows(g, c->aux);
+  c->launches += n ? 1 : 0;
+  if (need_colnorm(p, S)) {
+    c->colacc.ensure(3 * sizeof(double) * std::max(S, 1));
+    launch_colnorm(g, c->colacc.as<double>(), c->aux);
+    c->launches += 2;
+  }
+  CK(cudaEventRecord(c->ev_a1, c->aux));
+  CK(cudaEventRecord(c->ev_aux, c->aux));
+  c->prep_done = true;
+}
+
 // Sketch stage: pack, count + weights, register minimum.
 void run_sketch(rbg_ctx *c, const rbg_params *p, bool want_winners) {
   Tables &T = tables_for(c, p);
@@ -233,13 +284,13 @@ void run_sketch(rbg_ctx *c, const rbg_params *p, bool want_winners) {
   const int64_t nwords = (c->nbases + 15) / 16 + 1;
   c->packed.ensure(nwords * 4);
   c->nmask.ensure((nwords / 2 + 2) * 4);
-  c->elem_idx.ensure(std::max<int64_t>(n, 1) * kMaxElems);
-  c->elem_winv.ensure(std::max<int64_t>(n, 1) * kMaxElems * sizeof(double));
+  c->elem_winv.ensure(std::max<int64_t>(n, 1) * T.t->n_elems * sizeof(double));
   c->elem_cnt.ensure(std::max<int64_t>(n, 1) * sizeof(int32_t));
   c->codesA.ensure(std::max<int64_t>(n, 1) * mpad);
   c->codesB.ensure(std::max<int64_t>(n, 1) * mpad);
   if (want_winners) c->winners32.ensure(std::max<int64_t>(n, 1) * m * sizeof(uint32_t));
   CK(cudaEventRecord(c->ev[0], c->stream));
+  prep_depth(c, p);
   launch_pack(c->ascii.as<char>(), c->nbases, c->packed.as<uint32_t>(), c->nmask.as<uint32_t>(),
               c->stream);
   c->launches += c->nbases ? 1 : 0;
@@ -255,7 +306,6 @@ void run_sketch(rbg_ctx *c, const rbg_params *p, bool want_winners) {
   a.gc_cap = p->gc_norm_cap;
   a.n_elems = T.t->n_elems;
   a.rank_of_code = T.rank.as<int16_t>();
-  a.elem_idx = c->elem_idx.as<uint8_t>();
   a.elem_winv = c->elem_winv.as<double>();
   a.elem_cnt = c->elem_cnt.as<int32_t>();
   a.U = T.U.as<double>();
@@ -316,9 +366,6 @@ void run_graph(rbg_ctx *c, const rbg_params *p) {
   const int m = p->m, mpad = mpad_of(m), S = c->S, K = p->max_edges;
   const int64_t n1 = std::max<int64_t>(n, 1);
   const int Su = (std::max(S, 1) + 3) & ~3;
-  c->unit.ensure(n1 * Su * sizeof(float));
-  c->anynz.ensure(n1);
-  c->colnorm.ensure(std::max(S, 1) * sizeof(double));
   c->svbits.ensure((m + 1) * sizeof(uint32_t));
   c->topk.ensure(n1 * K * sizeof(uint64_t));
   c->topk_cnt.ensure(n1 * sizeof(int32_t));
@@ -327,6 +374,7 @@ void run_graph(rbg_ctx *c, const rbg_params *p) {
   c->stats.ensure(2 * sizeof(unsigned long long));
 
   const double w_comp = (p->w_comp < 0.0) ? (S <= 2 ? 1.0 : 0.0) : p->w_comp;
+  if (!c->prep_done) prep_depth(c, p);
   GraphArgs g;
   g.n = n; g.m = m; g.mpad = mpad; g.S = S; g.K = K; g.Su = Su;
   g.codesA = c->codesA.as<uint8_t>();
@@ -335,14 +383,9 @@ void run_graph(rbg_ctx *c, const rbg_params *p) {
   g.unit = c->unit.as<float>();
   g.anynz = c->anynz.as<uint8_t>();
   g.colnorm = c->colnorm.as<double>();
-  g.min_cv = (float)p->min_cv;
-  g.min_cv_d = p->min_cv;
   g.has_depth = S > 0;
   g.wjac_norm = p->wjac_norm;
-  launch_unit_rows(g, c->stream);
-  c->launches += n ? 1 : 0;
-  const bool need_colnorm = p->depth_sim >= 1 && S > 1 && p->wjac_norm;
-  if (need_colnorm) { launch_colnorm(g, c->stream); c->launches++; }
+  const bool use_colnorm = need_colnorm(p, S);
   CK(cudaEventRecord(c->ev[4], c->stream));
 
   // b0 on the codes (equal codes <=> equal winners of the chosen width)
@@ -376,8 +419,16 @@ void run_graph(rbg_ctx *c, const rbg_params *p) {
   g.maxcnt_all = c->maxc_all.as<uint32_t>();
   g.stats = c->stats.as<unsigned long long>();
   CK(cudaMemsetAsync(c->stats.p, 0, 2 * sizeof(unsigned long long), c->stream));
-  c->cand_buf.ensure((size_t)((n + 127) / 128 * 128) * allpairs_cap(K) * sizeof(uint64_t));
-  launch_allpairs(g, c->cand_buf.as<uint64_t>(), c->stream);
+  CK(cudaStreamWaitEvent(c->stream, c->ev_aux, 0));   // unit rows, anynz, column norms
+  c->prep_done = false;
+  {
+    const size_t slots = (size_t)((n + 31) / 32) * allpairs_slices(n, K) * 32;
+    c->cand_buf.ensure(slots * allpairs_cap(K) * sizeof(uint64_t));
+    c->cand_cnt.ensure(slots * sizeof(int32_t));
+    CK(cudaMemsetAsync(c->maxc_cand.p, 0, n1 * sizeof(uint32_t), c->stream));
+    CK(cudaMemsetAsync(c->maxc_all.p, 0, n1 * sizeof(uint32_t), c->stream));
+  }
+  launch_allpairs(g, c->cand_buf.as<uint64_t>(), c->cand_cnt.as<int32_t>(), c->stream);
   c->launches += n ? 1 : 0;
   CK(cudaGetLastError());
   CK(cudaEventRecord(c->ev[6], c->stream));
@@ -390,19 +441,19 @@ void run_graph(rbg_ctx *c, const rbg_params *p) {
   srand(p->seed);
   double simCutoff;
   if (!fused) {
-    std::vector<size_t> idx(n);
-    std::iota(idx.begin(), idx.end(), 0);
-    rand_prefix_shuffle(idx, (size_t)n);
+    // random_unique over all n contigs: only its rand() calls matter here,
+    // the maxima are counted, not ordered
+    for (int64_t left = n; left > 0; --left) (void)(rand() % left);
     std::vector<double> maxsim(n);
-    for (int64_t i = 0; i < n; ++i) maxsim[i] = sv_d[maxc[idx[i]]];
+    for (int64_t i = 0; i < n; ++i) maxsim[i] = sv_d[maxc[i]];
     simCutoff = (double)converge_cutoff(maxsim, p->coverage);
   } else {
     const size_t NR = 10, SAMP = 2500;
-    std::vector<std::vector<size_t>> idxs(NR, std::vector<size_t>(n));
-    for (size_t r = 0; r < NR; ++r) {
-      std::iota(idxs[r].begin(), idxs[r].end(), 0);
-      rand_prefix_shuffle(idxs[r], SAMP);
-    }
+    std::vector<std::vector<size_t>> idxs(NR);
+    std::vector<size_t> val((size_t)n);
+    std::vector<uint32_t> stamp((size_t)n, 0);
+    for (size_t r = 0; r < NR; ++r)
+      idxs[r] = rand_prefix_of_iota((size_t)n, SAMP, val, stamp, (uint32_t)(r + 1));
     std::vector<int8_t> sround(n, -1);
     std::vector<size_t> slocal(n, 0);
     for (int r = (int)NR - 1; r >= 0; --r)
@@ -474,7 +525,7 @@ void run_graph(rbg_ctx *c, const rbg_params *p) {
   w.unit = c->unit.as<float>();
   w.Su = Su;
   w.depth_raw = c->depth.as<float>();
-  w.colnorm = need_colnorm ? c->colnorm.as<double>() : nullptr;
+  w.colnorm = use_colnorm ? c->colnorm.as<double>() : nullptr;
   w.w_comp = w_comp;
   w.min_edge = p->min_edge;
   w.neg_thr = p->neg_thr;
@@ -637,6 +688,15 @@ int rbg_create(int device, rbg_ctx **out) {
     return RBG_ERR_CUDA;
   }
   for (auto &e : c->ev) cudaEventCreate(&e);
+  if (cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return RBG_ERR_CUDA;
+  }
+  cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&c->ev_aux, cudaEventDisableTiming);
+  cudaEventCreate(&c->ev_a0);
+  cudaEventCreate(&c->ev_a1);
   *out = c;
   return RBG_OK;
 }
@@ -650,7 +710,7 @@ int rbg_destroy(rbg_ctx *c) {
                   &c->anynz, &c->colnorm, &c->svbits, &c->topk, &c->topk_cnt, &c->maxc_cand,
                   &c->maxc_all, &c->stats, &c->pairs, &c->pair_out, &c->nbr, &c->nbr_sv,
                   &c->nbr_cnt, &c->row_edges, &c->e_from, &c->e_to, &c->e_scomp, &c->e_score,
-                  &c->badflag, &c->tmp, &c->cand_buf};
+                  &c->badflag, &c->tmp, &c->cand_buf, &c->cand_cnt, &c->colacc};
   for (DBuf *b : bufs) b->release();
   if (c->tables) {
     c->tables->U.release(); c->tables->codeA.release(); c->tables->W32.release();
@@ -659,6 +719,9 @@ int rbg_destroy(rbg_ctx *c) {
   }
   c->pin.release();
   for (auto &e : c->ev) cudaEventDestroy(e);
+  cudaStreamSynchronize(c->aux);
+  for (cudaEvent_t e : {c->ev_in, c->ev_aux, c->ev_a0, c->ev_a1}) cudaEventDestroy(e);
+  cudaStreamDestroy(c->aux);
   cudaStreamDestroy(c->stream);
   delete c;
   return RBG_OK;
@@ -675,6 +738,7 @@ int rbg_build_pmh_winners(rbg_ctx *c, const rbg_params *p, const char *seqcat,
     if (!out && n > 0) throw Error(RBG_ERR_ARG, "null output");
     stage(c, seqcat, offsets, n, nullptr, 0);
     run_sketch(c, p, true);
+    c->prep_done = false;
     if (n) CK(cudaMemcpyAsync(out, c->winners32.p, (size_t)n * p->m * 4, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
   });
@@ -729,6 +793,7 @@ int rbg_build_graph(rbg_ctx *c, const rbg_params *p, const uint32_t *winners32, 
       CK(cudaMemcpyAsync(c->depth.p, depth, (size_t)n * S * 4, cudaMemcpyHostToDevice, c->stream));
     }
     codes_from_winners(c, p, winners32, n);
+    c->prep_done = false;                    // coverage changed: prepare it again
     run_graph(c, p);
     fetch(c, out);
   });
@@ -770,7 +835,11 @@ int rbg_run_resident(rbg_ctx *c, const rbg_params *p, rbg_timing *t) {
       t->pack_ms = el(0, 1);
       t->count_ms = el(1, 2);
       t->sketch_ms = el(2, 3);
-      t->unit_ms = el(3, 4);
+      {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev_a0, c->ev_a1);
+        t->unit_ms = ms;
+      }
       t->b0_ms = el(4, 5);
       t->allpairs_ms = el(5, 6);
       t->finalize_ms = el(6, 7);

@@ -21,6 +21,7 @@
 //    at a time, lane = survivor.
 //
 // Compiled with -fmad=false; __fmaf_rn marks every fused operation.
+#include <algorithm>
 #include <cstdint>
 
 #include "rbg_internal.h"
@@ -32,6 +33,7 @@ constexpr unsigned FULL = 0xffffffffu;
 constexpr int kWarps = 4;         // warps per CTA (independent)
 constexpr int kCapW = 16;         // candidate buffer <= 32 * kCapW keys per row
 constexpr int kQ = 64;            // survivor queue entries per warp
+constexpr int kTC = 32;           // sparse: columns per staged tile
 
 __device__ __forceinline__ uint32_t eq_bytes(uint32_t a, uint32_t b) {
   const uint32_t x = a ^ b;
@@ -104,6 +106,14 @@ __device__ uint64_t select_topk(uint64_t *buf, int cnt, int K) {
   return P;
 }
 
+// 16-byte asynchronous global->shared copies (per lane), and their groups.
+__device__ __forceinline__ void cp16(void *dst, const void *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
 struct Warp {
   uint64_t *gbuf;     // [32 rows][cap] candidate keys of this warp's rows
   int *cnt;           // smem [32]
@@ -162,53 +172,66 @@ __device__ __forceinline__ void count_batch(const GraphArgs &g, Warp &w, const i
 
 template <int SMAX, bool SPARSE>
 __global__ void __launch_bounds__(kWarps * 32)
-k_allpairs(GraphArgs g, uint64_t *gbuf, int cap, float lo, float hi) {
+k_allpairs(GraphArgs g, uint64_t *gbuf, int32_t *gcnt, int cap, int P, float lo, float hi) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t n = g.n;
-  const int64_t row0 = ((int64_t)blockIdx.x * kWarps + warp) * 32;
+  const int64_t row0 = (int64_t)blockIdx.x * 32;
   const int64_t row = row0 + lane;
   const bool vrow = row < n;
   const int S = g.S, Su = g.Su;
   const int mw = g.mpad >> 2;
   const int mwq = ((mw + 27) & ~31) + 4;           // = 4 mod 32 words: conflict-free LDS.128
+  const int slice = blockIdx.y * kWarps + warp;     // column slice of this warp
+  const int64_t jb = n * slice / P, je = n * (slice + 1) / P;
 
-  // per-warp shared state
-  unsigned char *ws = smem + (size_t)warp * (SPARSE ? 1024 : (1024 + 32 * mwq * 4));
+  // shared: per-warp state, then (dense) the 32 row-code rows of the block
+  unsigned char *ws = smem + (size_t)warp * 1024;
   uint64_t *thr = (uint64_t *)ws;                  // [32]
   int *cnt = (int *)(thr + 32);                    // [32]
   uint32_t *mxc = (uint32_t *)(cnt + 32);          // [32]
-  uint32_t *mxa = mxc + 32;                        // [32]
-  int *q = (int *)(mxa + 32);                      // [kQ]
-  uint32_t *sA = (uint32_t *)(ws + 1024);          // dense: [32][mwq] row codes
+  int *q = (int *)(mxc + 32);                      // [kQ]
+  uint32_t *sA = (uint32_t *)(smem + (size_t)kWarps * 1024);   // dense: [32][mwq]
 
   thr[lane] = 0;
   cnt[lane] = 0;
   mxc[lane] = 0;
-  mxa[lane] = 0;
-  Warp w{gbuf + (size_t)(row0 < n ? row0 : 0) * cap, cnt, thr, mxc, cap, g.K};
+  const size_t bufrow = ((size_t)blockIdx.x * P + slice) * 32;  // first buffer row of the warp
+  Warp w{gbuf + bufrow * cap, cnt, thr, mxc, cap, g.K};
   const uint8_t nz_row = vrow ? g.anynz[row] : 0;
-  unsigned long long n_pref = 0, n_cmp = 0;
-  __syncwarp();
+  unsigned n_pref = 0, n_cmp = 0;
+  uint32_t mx_a = 0, mx_c = 0;
 
   if (!SPARSE) {
-    for (int i = lane; i < 32 * (mw >> 2); i += 32) {
+    for (int i = threadIdx.x; i < 32 * (mw >> 2); i += blockDim.x) {
       const int r = i / (mw >> 2), t = i - r * (mw >> 2);
       uint4 v = make_uint4(0, 0, 0, 0);
       if (row0 + r < n) v = __ldg((const uint4 *)(g.codesA + (row0 + r) * g.mpad) + t);
       *(uint4 *)(sA + r * mwq + 4 * t) = v;
     }
-    __syncwarp();
+    __syncthreads();
     const uint32_t *ra = sA + lane * mwq;
-    uint32_t mx_a = 0, mx_c = 0;
     const int m4 = mw >> 2;
-    for (int64_t j0 = 0; j0 < n; j0 += 4) {
-      const int64_t j1 = j0 + 1 < n ? j0 + 1 : j0, j2 = j0 + 2 < n ? j0 + 2 : j0,
-                    j3 = j0 + 3 < n ? j0 + 3 : j0;
-      const uint4 *c0 = (const uint4 *)(g.codesB + j0 * g.mpad);
-      const uint4 *c1 = (const uint4 *)(g.codesB + j1 * g.mpad);
-      const uint4 *c2 = (const uint4 *)(g.codesB + j2 * g.mpad);
-      const uint4 *c3 = (const uint4 *)(g.codesB + j3 * g.mpad);
+    // per-warp ring: 2 stages x 4 columns of B codes
+    uint4 *ring = (uint4 *)(smem + (size_t)kWarps * 1024 + 32 * (size_t)mwq * 4) +
+                  (size_t)warp * 2 * 4 * m4;
+    auto stage_cols = [&](int st, int64_t j0) {
+      uint4 *dst = ring + (size_t)st * 4 * m4;
+      for (int i = lane; i < 4 * m4; i += 32) {
+        const int u = i / m4, t = i - u * m4;
+        const int64_t j = j0 + u < je ? j0 + u : j0;
+        cp16(dst + i, (const uint4 *)(g.codesB + j * g.mpad) + t);
+      }
+      cp_commit();
+    };
+    if (jb < je) stage_cols(0, jb);
+    int st = 0;
+    for (int64_t j0 = jb; j0 < je; j0 += 4, st ^= 1) {
+      if (j0 + 4 < je) stage_cols(st ^ 1, j0 + 4); else cp_commit();
+      cp_wait1();
+      __syncwarp();
+      const uint4 *c0 = ring + (size_t)st * 4 * m4;
+      const uint4 *c1 = c0 + m4, *c2 = c1 + m4, *c3 = c2 + m4;
       uint32_t cntq[4] = {0, 0, 0, 0};
       for (int t0 = 0; t0 < m4; t0 += 63) {
         const int t1 = t0 + 63 < m4 ? t0 + 63 : m4;
@@ -216,8 +239,7 @@ k_allpairs(GraphArgs g, uint64_t *gbuf, int cap, float lo, float hi) {
 #pragma unroll 2
         for (int t = t0; t < t1; ++t) {
           const uint4 a = *(const uint4 *)(ra + 4 * t);
-          const uint4 b0 = __ldg(c0 + t), b1 = __ldg(c1 + t), b2 = __ldg(c2 + t),
-                      b3 = __ldg(c3 + t);
+          const uint4 b0 = c0[t], b1 = c1[t], b2 = c2[t], b3 = c3[t];
           a0 += eq_bytes(a.x, b0.x) + eq_bytes(a.y, b0.y) + eq_bytes(a.z, b0.z) + eq_bytes(a.w, b0.w);
           a1 += eq_bytes(a.x, b1.x) + eq_bytes(a.y, b1.y) + eq_bytes(a.z, b1.z) + eq_bytes(a.w, b1.w);
           a2 += eq_bytes(a.x, b2.x) + eq_bytes(a.y, b2.y) + eq_bytes(a.z, b2.z) + eq_bytes(a.w, b2.w);
@@ -228,11 +250,12 @@ k_allpairs(GraphArgs g, uint64_t *gbuf, int cap, float lo, float hi) {
         cntq[2] += byte_sum(a2);
         cntq[3] += byte_sum(a3);
       }
+      __syncwarp();
 #pragma unroll
       for (int t = 0; t < 4; ++t) {
         const int64_t j = j0 + t;
-        const bool other = vrow && j < n && j != row;
-        const bool cand = other && (nz_row | __ldg(g.anynz + (j < n ? j : 0)));
+        const bool other = vrow && j < je && j != row;
+        const bool cand = other && (nz_row | __ldg(g.anynz + (j < je ? j : jb)));
         const uint32_t c = cntq[t];
         if (other && c > mx_a) mx_a = c;
         if (cand && c > mx_c) mx_c = c;
@@ -245,85 +268,171 @@ k_allpairs(GraphArgs g, uint64_t *gbuf, int cap, float lo, float hi) {
       __syncwarp();
       compact_full_rows(w, cap - 4);
     }
-    mxa[lane] = mx_a;
-    mxc[lane] = mx_c;
   } else {
     float ur[SMAX];
 #pragma unroll
     for (int t = 0; t < SMAX; ++t) ur[t] = (vrow && t < Su) ? g.unit[row * Su + t] : 0.f;
     int qn = 0;
-    for (int64_t j = 0; j < n; ++j) {
-      const bool other = vrow && j != row;
-      const bool cand = other && (nz_row | __ldg(g.anynz + j));
-      const float4 *uj = (const float4 *)(g.unit + j * Su);
-      float c1 = 0.f;
+    // per-warp ring: 2 stages x kTC columns of unit rows
+    float *ring = (float *)(smem + (size_t)kWarps * 1024) + (size_t)warp * 2 * kTC * Su;
+    auto stage_cols = [&](int st, int64_t jt) {
+      const int nc = (int)(je - jt < kTC ? je - jt : kTC);
+      float *dst = ring + (size_t)st * kTC * Su;
+      const float *src = g.unit + jt * Su;
+      for (int i = lane; i < nc * (Su >> 2); i += 32) cp16(dst + 4 * i, src + 4 * i);
+      cp_commit();
+    };
+    if (jb < je) stage_cols(0, jb);
+    int st = 0;
+    for (int64_t jt = jb; jt < je; jt += kTC, st ^= 1) {
+      if (jt + kTC < je) stage_cols(st ^ 1, jt + kTC); else cp_commit();
+      const int nc = (int)(je - jt < kTC ? je - jt : kTC);
+      const unsigned nzm = __ballot_sync(FULL, lane < nc && __ldg(g.anynz + jt + (lane < nc ? lane : 0)));
+      cp_wait1();
+      __syncwarp();
+      const float *tile = ring + (size_t)st * kTC * Su;
+      for (int c0 = 0; c0 < nc; c0 += 4) {
+        float c1[4] = {0.f, 0.f, 0.f, 0.f};
+        bool cand[4];
 #pragma unroll
-      for (int t4 = 0; t4 < SMAX; t4 += 4) {
-        if (t4 < Su) {
-          const float4 v = __ldg(uj + (t4 >> 2));
-          c1 = __fmaf_rn(ur[t4 + 0], v.x, c1);
-          c1 = __fmaf_rn(ur[t4 + 1], v.y, c1);
-          c1 = __fmaf_rn(ur[t4 + 2], v.z, c1);
-          c1 = __fmaf_rn(ur[t4 + 3], v.w, c1);
+        for (int u = 0; u < 4; ++u) {
+          const int c = c0 + u;
+          const int64_t j = jt + c;
+          cand[u] = vrow && c < nc && j != row && (nz_row | ((nzm >> c) & 1u));
+        }
+#pragma unroll
+        for (int t4 = 0; t4 < SMAX; t4 += 4) {
+          if (t4 < Su) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const int c = c0 + u < nc ? c0 + u : c0;
+              const float4 v = *(const float4 *)(tile + c * Su + t4);
+              c1[u] = __fmaf_rn(ur[t4 + 0], v.x, c1[u]);
+              c1[u] = __fmaf_rn(ur[t4 + 1], v.y, c1[u]);
+              c1[u] = __fmaf_rn(ur[t4 + 2], v.z, c1[u]);
+              c1[u] = __fmaf_rn(ur[t4 + 3], v.w, c1[u]);
+            }
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int64_t j = jt + c0 + u;
+          n_pref += cand[u];
+          bool pass = cand[u] && c1[u] >= hi;
+          const bool band = cand[u] && c1[u] >= lo && c1[u] < hi;
+          if (__any_sync(FULL, band)) {
+            if (band) pass = !(dot_avx512<SMAX>(ur, g.unit + j * Su, S) < g.prefilter_eps);
+          }
+          const unsigned m = __ballot_sync(FULL, pass);
+          if (m) {
+            if (pass) q[qn + __popc(m & ((1u << lane) - 1u))] = (int)(((unsigned)lane << 27) | (unsigned)j);
+            qn += __popc(m);
+            __syncwarp();
+            if (qn >= 32) {
+              count_batch(g, w, q, 32, row0);
+              n_cmp += 1;
+              if (lane + 32 < qn) q[lane] = q[lane + 32];
+              __syncwarp();
+              qn -= 32;
+            }
+          }
         }
       }
-      n_pref += cand;
-      bool pass = cand && c1 >= hi;
-      const bool band = cand && c1 >= lo && c1 < hi;
-      if (__any_sync(FULL, band)) {
-        if (band) pass = !(dot_avx512<SMAX>(ur, g.unit + j * Su, S) < g.prefilter_eps);
-      }
-      const unsigned m = __ballot_sync(FULL, pass);
-      if (m) {
-        if (pass) q[qn + __popc(m & ((1u << lane) - 1u))] = (int)(((unsigned)lane << 27) | (unsigned)j);
-        qn += __popc(m);
-        __syncwarp();
-        if (qn >= 32) {
-          count_batch(g, w, q, 32, row0);
-          n_cmp += 1;
-          if (lane + 32 < qn) q[lane] = q[lane + 32];
-          __syncwarp();
-          qn -= 32;
-        }
-      }
+      __syncwarp();
     }
     if (qn > 0) {
       n_cmp += lane < qn;
       count_batch(g, w, q, qn, row0);
     }
+    __syncwarp();
+    mx_c = mxc[lane];
   }
   if (g.stats) {
-    if (n_pref) atomicAdd(g.stats, n_pref);
-    if (n_cmp) atomicAdd(g.stats + 1, n_cmp);
+    const unsigned a = __reduce_add_sync(FULL, n_pref), b = __reduce_add_sync(FULL, n_cmp);
+    if (lane == 0) {
+      if (a) atomicAdd(g.stats, (unsigned long long)a);
+      if (b) atomicAdd(g.stats + 1, (unsigned long long)b);
+    }
   }
   __syncwarp();
-  // the K best of each row, written unsorted
+  // this slice's K best of each row stay in the buffer for the merge
   compact_full_rows(w, g.K);
+  gcnt[bufrow + lane] = cnt[lane];
   if (vrow) {
-    const int c = cnt[lane];
-    for (int i = 0; i < c; ++i) g.topk[row * g.K + i] = w.gbuf[(size_t)lane * cap + i];
-    g.topk_cnt[row] = c;
-    g.maxcnt_cand[row] = mxc[lane];
-    g.maxcnt_all[row] = mxa[lane];
+    if (mx_c) atomicMax(g.maxcnt_cand + row, mx_c);
+    if (mx_a) atomicMax(g.maxcnt_all + row, mx_a);
   }
 }
 
-size_t allpairs_smem(int mpad, bool sparse) {
+// Warp per row: the K best keys among the P slices' partial lists.
+__global__ void k_merge_topk(GraphArgs g, const uint64_t *gbuf, const int32_t *gcnt, int cap,
+                             int P) {
+  extern __shared__ uint64_t mk[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int64_t row = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
+  if (row >= g.n) return;
+  const int K = g.K;
+  uint64_t *keys = mk + (size_t)wib * P * K;
+  const int64_t rb = row >> 5, rl = row & 31;
+  int tot = 0;
+  for (int s = 0; s < P; ++s) {
+    const size_t br = ((size_t)rb * P + s) * 32 + rl;
+    const int c = gcnt[br];
+    for (int i = lane; i < c; i += 32) keys[tot + i] = gbuf[br * cap + i];
+    tot += c;
+  }
+  __syncwarp();
+  uint64_t Pk = 0;
+  if (tot > K) {
+    for (int bit = 63; bit >= 0; --bit) {
+      const uint64_t c = Pk | (1ull << bit);
+      int k = 0;
+      for (int i = lane; i < tot; i += 32) k += keys[i] >= c;
+      if ((int)__reduce_add_sync(FULL, (unsigned)k) >= K) Pk = c;
+    }
+  }
+  int out = 0;
+  for (int base = 0; base < tot; base += 32) {
+    const int i = base + lane;
+    const uint64_t v = i < tot ? keys[i] : 0ull;
+    const bool keep = i < tot && v >= Pk;
+    const unsigned m = __ballot_sync(FULL, keep);
+    if (keep) g.topk[row * K + out + __popc(m & ((1u << lane) - 1u))] = v;
+    out += __popc(m);
+  }
+  if (lane == 0) g.topk_cnt[row] = out;
+}
+
+size_t allpairs_smem(int mpad, int Su, bool sparse) {
   const int mw = mpad >> 2;
   const int mwq = ((mw + 27) & ~31) + 4;
-  return (size_t)kWarps * (sparse ? 1024 : (1024 + 32 * (size_t)mwq * 4));
+  if (sparse) return (size_t)kWarps * 1024 + (size_t)kWarps * 2 * kTC * Su * 4;
+  return (size_t)kWarps * 1024 + 32 * (size_t)mwq * 4 + (size_t)kWarps * 2 * 4 * mpad;
 }
 
 }  // namespace
 
 int allpairs_cap(int K) { return (K + 64 + 31) & ~31; }
 
-void launch_allpairs(const GraphArgs &g, uint64_t *gbuf, cudaStream_t s) {
+// Column slices per 32-row block: enough warps for several waves of the GPU,
+// each slice at least 64 columns; a multiple of the CTA's warp count.
+int allpairs_slices(int64_t n, int K) {
+  const int64_t blocks = (n + 31) / 32;
+  int64_t P = (4 * 148 * 48 + blocks - 1) / std::max<int64_t>(blocks, 1);
+  P = std::min<int64_t>(P, std::max<int64_t>(n / 64, 1));
+  P = std::max<int64_t>(P, 1);
+  const int pmax = std::max(kWarps, std::min(32, (6400 / std::max(K, 1)) / kWarps * kWarps));
+  P = std::min<int64_t>(P, pmax);
+  return (int)(((P + kWarps - 1) / kWarps) * kWarps);
+}
+
+void launch_allpairs(const GraphArgs &g, uint64_t *gbuf, int32_t *gcnt, cudaStream_t s) {
   if (g.n == 0) return;
   const int cap = allpairs_cap(g.K);
+  const int P = allpairs_slices(g.n, g.K);
   const bool sparse = g.prefilter != 0;
-  const size_t smem = allpairs_smem(g.mpad, sparse);
-  const unsigned grid = (unsigned)((g.n + kWarps * 32 - 1) / (kWarps * 32));
+  const size_t smem = allpairs_smem(g.mpad, g.Su, sparse);
+  const dim3 grid((unsigned)((g.n + 31) / 32), (unsigned)(P / kWarps));
   // band of the exact-safe prefilter: |chain - AVX-512 order| < delta
   const double eps = (double)g.prefilter_eps;
   const double delta = (double)(g.S + (g.S + 15) / 16 + 8) * ldexp(1.0, -23);
@@ -334,7 +443,7 @@ void launch_allpairs(const GraphArgs &g, uint64_t *gbuf, cudaStream_t s) {
   do {                                                                                       \
     cudaFuncSetAttribute(k_allpairs<SM, SP>, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
                          (int)smem);                                                         \
-    k_allpairs<SM, SP><<<grid, kWarps * 32, smem, s>>>(g, gbuf, cap, lo, hi);               \
+    k_allpairs<SM, SP><<<grid, kWarps * 32, smem, s>>>(g, gbuf, gcnt, cap, P, lo, hi);      \
   } while (0)
   if (sparse) {
     if (g.Su <= 16) RBG_LAUNCH(16, true);
@@ -344,6 +453,9 @@ void launch_allpairs(const GraphArgs &g, uint64_t *gbuf, cudaStream_t s) {
     RBG_LAUNCH(4, false);
   }
 #undef RBG_LAUNCH
+  const size_t msm = (size_t)P * g.K * sizeof(uint64_t);
+  cudaFuncSetAttribute(k_merge_topk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msm);
+  k_merge_topk<<<(unsigned)g.n, 32, msm, s>>>(g, gbuf, gcnt, cap, P);
 }
 
 }  // namespace rbg

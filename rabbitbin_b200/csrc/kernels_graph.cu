@@ -17,63 +17,123 @@ constexpr unsigned FULL = 0xffffffffu;
 
 // ── unit rank rows (src/rabbitbin.cpp:4867-4874 rank, :4972-4988 unit rows,
 //    src/ranker.h:55-66 average ranks, src/impl/rb_abundance.cpp:94-114 anynz)
+// Warp per row, lane = sample (two samples per lane when S > 32).  The average
+// rank of x_k is 1 + #{x_l < x_k} + (#{x_l == x_k} - 1) / 2, a half-integer, so
+// the reference's sequential double sums of ranks and of squared deviations
+// (multiples of 1/4, far below 2^53) are exact in any order: warp reductions
+// give the same mean and ss.
 __global__ void k_unit_rows(GraphArgs g) {
-  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (r >= g.n) return;
   const int S = g.S;
-  float x[kMaxS], rk[kMaxS];
-  for (int k = 0; k < S; ++k) x[k] = g.depth_raw[r * S + k];
-  uint8_t nz = 1;
+  const float *x = g.depth_raw + r * S;
+  const float x0 = lane < S ? x[lane] : 0.f;
+  const float x1 = lane + 32 < S ? x[lane + 32] : 0.f;
+  float rk0 = 0.f, rk1 = 0.f;
+  bool nz = !g.has_depth;
   if (g.has_depth) {
-    nz = 0;
     if (S > 1) {
-      for (int k = 0; k < S; ++k) {
-        int less = 0, eq = 0;
-        for (int l = 0; l < S; ++l) { less += x[l] < x[k]; eq += x[l] == x[k]; }
-        // average rank of a tie group starting at sorted position `less`
-        rk[k] = __fadd_rn((float)(2 * less + eq - 1) / 2.0f, 1.0f);
-        if ((double)rk[k] > g.min_cv_d) nz = 1;
+      int less0 = 0, eq0 = 0, less1 = 0, eq1 = 0;
+      for (int l = 0; l < S; ++l) {
+        const float xl = __shfl_sync(0xffffffffu, l < 32 ? x0 : x1, l & 31);
+        less0 += xl < x0; eq0 += xl == x0;
+        less1 += xl < x1; eq1 += xl == x1;
       }
+      rk0 = __fadd_rn((float)(2 * less0 + eq0 - 1) / 2.0f, 1.0f);
+      rk1 = __fadd_rn((float)(2 * less1 + eq1 - 1) / 2.0f, 1.0f);
+      nz = (lane < S && (double)rk0 > g.min_cv_d) || (lane + 32 < S && (double)rk1 > g.min_cv_d);
     } else {
-      for (int k = 0; k < S; ++k) if ((double)x[k] > g.min_cv_d) nz = 1;
+      nz = lane < S && (double)x0 > g.min_cv_d;
     }
+    nz = __any_sync(0xffffffffu, nz);
   }
-  g.anynz[r] = nz;
+  if (lane == 0) g.anynz[r] = nz ? 1 : 0;
   if (S <= 1) return;
-  double mean = 0.0;
-  for (int k = 0; k < S; ++k) mean = __dadd_rn(mean, (double)rk[k]);
-  mean = mean / (double)S;
-  double ss = 0.0;
-  for (int k = 0; k < S; ++k) {
-    const double d = __dsub_rn((double)rk[k], mean);
-    ss = __dadd_rn(ss, __dmul_rn(d, d));
-  }
+  double sum = (lane < S ? (double)rk0 : 0.0) + (lane + 32 < S ? (double)rk1 : 0.0);
+  for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  const double mean = sum / (double)S;
+  const double d0 = lane < S ? __dsub_rn((double)rk0, mean) : 0.0;
+  const double d1 = lane + 32 < S ? __dsub_rn((double)rk1, mean) : 0.0;
+  double ss = __dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1));
+  for (int o = 16; o; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
   float *u = g.unit + r * g.Su;
-  if (ss > 0.0) {
-    const double inv = 1.0 / __dsqrt_rn(ss);
-    for (int k = 0; k < S; ++k)
-      u[k] = __double2float_rn(__dmul_rn(__dsub_rn((double)rk[k], mean), inv));
-  } else {
-    for (int k = 0; k < S; ++k) u[k] = 0.0f;
-  }
-  for (int k = S; k < g.Su; ++k) u[k] = 0.0f;
+  const double inv = ss > 0.0 ? 1.0 / __dsqrt_rn(ss) : 0.0;
+  if (lane < g.Su) u[lane] = (lane < S && ss > 0.0) ? __double2float_rn(__dmul_rn(d0, inv)) : 0.0f;
+  if (lane + 32 < g.Su) u[lane + 32] = (lane + 32 < S && ss > 0.0) ? __double2float_rn(__dmul_rn(d1, inv)) : 0.0f;
 }
 
-// Column norms of the raw depths, summed in row order
-// (src/rabbitbin.cpp:4800-4806): one CTA stages row chunks in shared memory
-// with coalesced loads; thread i < S adds its column sequentially.
-__global__ void k_colnorm(GraphArgs g) {
+// Column norms of the raw depths (src/rabbitbin.cpp:4800-4806): the reference
+// sums each column in row order in double.  Fast path: if every value of a
+// column is an integer multiple of 2^E (E = lowest set bit over its non-zero
+// values) and sum|x| < 2^(52+E), every partial sum in any order is a multiple
+// of 2^E below 2^(53+E) and so exact; the parallel sum then equals the
+// sequential one.  Columns that fail the test are summed sequentially.
+__device__ __forceinline__ int low_bit_exp(float x) {
+  const uint32_t b = __float_as_uint(x) & 0x7FFFFFFFu;
+  const int e = (int)(b >> 23);
+  uint32_t mant = b & 0x7FFFFFu;
+  int base;
+  if (e == 0) base = -149;                       // subnormal: mant * 2^-149
+  else { mant |= 0x800000u; base = e - 150; }    // mant * 2^(e-150)
+  return base + __ffs(mant) - 1;
+}
+
+__global__ void k_colsum_fast(GraphArgs g, double *acc) {
+  // acc layout per column i: [0] sum, [1] sum |x|, [2] (int) min exponent
+  __shared__ double ssum[kMaxS], sabs[kMaxS];
+  __shared__ int semin[kMaxS];
+  const int S = g.S;
+  for (int i = threadIdx.x; i < S; i += blockDim.x) { ssum[i] = 0.0; sabs[i] = 0.0; semin[i] = 1 << 20; }
+  __syncthreads();
+  const int64_t total = g.n * S;
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const float x = g.depth_raw[q];
+    const int i = (int)(q % S);
+    if (x != 0.0f) {
+      atomicAdd(&ssum[i], (double)x);
+      atomicAdd(&sabs[i], fabs((double)x));
+      atomicMin(&semin[i], low_bit_exp(x));
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < S; i += blockDim.x) {
+    atomicAdd(&acc[3 * i], ssum[i]);
+    atomicAdd(&acc[3 * i + 1], sabs[i]);
+    atomicMin((int *)&acc[3 * i + 2], semin[i]);
+  }
+}
+
+__global__ void k_colnorm(GraphArgs g, const double *acc) {
   constexpr int CH = 128;
   __shared__ float chunk[CH * kMaxS];
+  __shared__ int need_seq;
   const int S = g.S, i = threadIdx.x;
+  bool exact = false;
   double s = 0.0;
-  for (int64_t r0 = 0; r0 < g.n; r0 += CH) {
-    const int rows = (int)((g.n - r0) < CH ? (g.n - r0) : CH);
-    __syncthreads();
-    for (int q = threadIdx.x; q < rows * S; q += blockDim.x) chunk[q] = g.depth_raw[r0 * S + q];
-    __syncthreads();
-    if (i < S)
-      for (int r = 0; r < rows; ++r) s = __dadd_rn(s, (double)chunk[r * S + i]);
+  if (i < S) {
+    const int emin = *(const int *)&acc[3 * i + 2];
+    const double sum_abs = acc[3 * i + 1];
+    exact = (emin >= (1 << 20)) ||                                  // all zero
+            (emin > -1000 && sum_abs < ldexp(1.0, 52 + emin));
+    s = emin >= (1 << 20) ? 0.0 : acc[3 * i];
+  }
+  if (threadIdx.x == 0) need_seq = 0;
+  __syncthreads();
+  if (i < S && !exact) atomicOr(&need_seq, 1);
+  __syncthreads();
+  if (need_seq) {
+    double sq = 0.0;
+    for (int64_t r0 = 0; r0 < g.n; r0 += CH) {
+      const int rows = (int)((g.n - r0) < CH ? (g.n - r0) : CH);
+      __syncthreads();
+      for (int q = threadIdx.x; q < rows * S; q += blockDim.x) chunk[q] = g.depth_raw[r0 * S + q];
+      __syncthreads();
+      if (i < S && !exact)
+        for (int r = 0; r < rows; ++r) sq = __dadd_rn(sq, (double)chunk[r * S + i]);
+    }
+    if (i < S && !exact) s = sq;
   }
   if (i < S) {
     const double mean = s / (double)(g.n > 1 ? g.n : 1);
@@ -327,12 +387,16 @@ __global__ void k_edge_weights(WeightArgs w) {
 
 void launch_unit_rows(const GraphArgs &g, cudaStream_t s) {
   if (g.n == 0) return;
-  k_unit_rows<<<(unsigned)((g.n + 127) / 128), 128, 0, s>>>(g);
+  k_unit_rows<<<(unsigned)((g.n + 7) / 8), 256, 0, s>>>(g);   // warp per row
 }
 
-void launch_colnorm(const GraphArgs &g, cudaStream_t s) {
+void launch_colnorm(const GraphArgs &g, double *acc, cudaStream_t s) {
   if (g.S == 0) return;
-  k_colnorm<<<1, 256, 0, s>>>(g);
+  // zeroed slots: the exponent minimum then starts at 0, a valid (conservative)
+  // lower bound of every column's lowest set bit once values below 1 appear
+  cudaMemsetAsync(acc, 0, 3 * sizeof(double) * g.S, s);
+  k_colsum_fast<<<296, 256, 0, s>>>(g, acc);
+  k_colnorm<<<1, 256, 0, s>>>(g, acc);
 }
 
 void launch_pair_counts(const uint8_t *A, const uint8_t *B, int mpad, int m,

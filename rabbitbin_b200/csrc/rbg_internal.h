@@ -56,10 +56,9 @@ struct SketchArgs {
   int k = 4, m = 500, gc_norm = 1, n_elems = 136;
   double gc_cap = 20.0;
   const int16_t *rank_of_code = nullptr;  // [4^k]
-  // per-contig element lists
-  uint8_t *elem_idx = nullptr;         // [n][kMaxElems]
-  double *elem_winv = nullptr;         // [n][kMaxElems]
-  int32_t *elem_cnt = nullptr;         // [n]
+  // per-contig element weights: 1/w of canonical k-mer e, +inf when absent
+  double *elem_winv = nullptr;         // [n][n_elems]
+  int32_t *elem_cnt = nullptr;         // [n] number of present elements
   // tables
   const double *U = nullptr;           // [E][m]
   const uint8_t *codeA = nullptr;      // [E][m]
@@ -102,10 +101,11 @@ struct GraphArgs {
 };
 
 void launch_unit_rows(const GraphArgs &g, cudaStream_t s);
-void launch_colnorm(const GraphArgs &g, cudaStream_t s);
+void launch_colnorm(const GraphArgs &g, double *acc, cudaStream_t s);
 void launch_pair_counts(const uint8_t *codesA, const uint8_t *codesB, int mpad, int m,
                         const int64_t *pairs, int npairs, uint32_t *out, cudaStream_t s);
-void launch_allpairs(const GraphArgs &g, uint64_t *gbuf, cudaStream_t s);
+void launch_allpairs(const GraphArgs &g, uint64_t *gbuf, int32_t *gcnt, cudaStream_t s);
+int allpairs_slices(int64_t n, int K);
 int allpairs_cap(int K);
 
 struct EmitArgs {

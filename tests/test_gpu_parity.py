@@ -199,3 +199,25 @@ def test_against_golden_fixtures(gpu_ctx):
 def test_graph_ragged_sizes(gpu_ctx, orc, N, S, fp):
     """Row/column counts that leave partial CTA tiles."""
     _graph_case(gpu_ctx, orc, 25, N, S, seed=N, force_path=fp)
+
+
+@pytest.mark.parametrize("kind", ["fractional", "wide_range"])
+def test_graph_nonint_depths(gpu_ctx, orc, kind):
+    """Coverage values that are not small integers: the column sums of the
+    weighted-Jaccard norm must still round exactly as the sequential sum."""
+    asm = make_assembly(20, 3000, 6, seed=77)
+    rng = np.random.default_rng(5)
+    d = asm.depth * rng.uniform(0.5, 1.5, size=asm.depth.shape).astype(np.float32)
+    if kind == "wide_range":
+        d[rng.random(d.shape) < 0.05] = np.float32(3e-30)
+        d[rng.random(d.shape) < 0.01] *= np.float32(1e12)
+    d = d.astype(np.float32)
+    buf, offs = asm.concat()
+    w = orc.build_winners(buf, offs)
+    for fp in (1, 2):
+        want = orc.run_graph(oracle.default_params(asm.n, 500, 6, force_path=fp), w, d)
+        got = gpu_ctx.bin_graph(buf, offs, d, api.default_params(force_path=fp))
+        s, dd, sc, sw = oracle.sorted_edges(want)
+        assert got["sim_cutoff"] == want["sim_cutoff"]
+        assert np.array_equal(got["src"], s) and np.array_equal(got["dst"], dd)
+        assert np.array_equal(got["scomp"], sc) and np.array_equal(got["score"], sw)
