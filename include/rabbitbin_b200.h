@@ -148,6 +148,26 @@ int rbg_fetch_graph(rbg_ctx *ctx, rbg_graph *out);
 
 int rbg_free_graph(rbg_graph *g);
 
+/* rbg_build_pmh_winners for callers that cannot allocate device memory (a host
+ * framework that owns the device heap through its own pool, a plugin inside
+ * another process's CUDA context with a fixed budget, a caller that must not
+ * synchronise on an allocation).  No counterpart in the reference: it is the
+ * same sketch, but inputs and outputs are caller-owned DEVICE buffers and every
+ * intermediate lives in one static 24 MiB device array that the library
+ * reserves on each GPU that loads it (held until exit).  seq_device is the
+ * concatenated ASCII (16-byte aligned, readable up to a multiple of 16 bytes),
+ * offsets_device the n+1 base offsets (offsets[0] == 0, offsets[n] == nbases),
+ * winners_device n*m folded 32-bit winner rows.  Requests needing more scratch
+ * than the array holds return RBG_ERR_ARG (message in errbuf) before any device
+ * work.  The first call on a device looks up the array's address: make it
+ * before any stream capture.  Calls share the array; calls that overlap on the
+ * GPU race.  `stream` is a cudaStream_t (null: the default stream); the call
+ * returns after the work has finished on it. */
+int rbg_build_pmh_winners_noalloc(const rbg_params *p, const char *seq_device,
+                                  const int64_t *offsets_device, int64_t n, int64_t nbases,
+                                  uint32_t *winners_device, void *stream, char *errbuf,
+                                  size_t errlen);
+
 /* Introspection (host only, no device needed): the ProbMinHash element streams
  * the sketch kernel reduces over for one configuration.  For every canonical
  * k-mer e (ascending code canon_codes[e]) and register r, U[e*m + r] is the

@@ -90,6 +90,8 @@ def lib():
         "rbg_pmh_stream_tables": ([C.c_int32, C.c_int32, C.c_uint64, C.c_int32,
                                    P(C.c_int32), P(C.c_int32), P(C.c_double),
                                    P(C.c_uint32)], C.c_int),
+        "rbg_build_pmh_winners_noalloc": ([P(Params), vp, vp, C.c_int64, C.c_int64, vp, vp,
+                                           C.c_char_p, C.c_size_t], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
