@@ -157,7 +157,7 @@ struct rbg_ctx {
   // sketch state
   DBuf packed, nmask, elem_idx, elem_winv, elem_cnt, codesA, codesB, winners32;
   // graph state
-  DBuf unit, anynz, colnorm, svbits, topk, topk_cnt, maxc_cand, maxc_all, stats;
+  DBuf unit, unit16, anynz, colnorm, svbits, topk, topk_cnt, maxc_cand, maxc_all, stats;
   DBuf pairs, pair_out, nbr, nbr_sv, nbr_cnt, row_edges, cand_buf, cand_cnt;
   DBuf e_from, e_to, e_scomp, e_score, badflag, tmp, colacc;
   HBuf pin;
@@ -240,6 +240,10 @@ void stage(rbg_ctx *c, const char *seqcat, const int64_t *offsets, int64_t n,
     CK(cudaMemcpyAsync(c->depth.p, depth, (size_t)n * S * sizeof(float), cudaMemcpyHostToDevice, c->stream));
 }
 
+// Row stride (halves) of the FP16 unit rows: 16, 32 or 64, the k extent of the
+// tensor-core prefilter variant that reads them.
+int unit16_stride(int S) { return S <= 16 ? 16 : (S <= 32 ? 32 : 64); }
+
 bool need_colnorm(const rbg_params *p, int S) { return p->depth_sim >= 1 && S > 1 && p->wjac_norm; }
 
 // Unit rank rows, anynz and column norms on the auxiliary stream: they depend
@@ -248,11 +252,14 @@ void prep_depth(rbg_ctx *c, const rbg_params *p) {
   const int64_t n = c->n, n1 = std::max<int64_t>(n, 1);
   const int S = c->S;
   const int Su = (std::max(S, 1) + 3) & ~3;
+  const int Kp = unit16_stride(S);
   c->unit.ensure(n1 * Su * sizeof(float));
+  c->unit16.ensure(n1 * Kp * sizeof(uint16_t));
   c->anynz.ensure(n1);
   c->colnorm.ensure(std::max(S, 1) * sizeof(double));
   GraphArgs g;
-  g.n = n; g.S = S; g.Su = Su;
+  g.n = n; g.S = S; g.Su = Su; g.Kp = Kp;
+  g.unit16 = c->unit16.as<uint16_t>();
   g.depth_raw = c->depth.as<float>();
   g.unit = c->unit.as<float>();
   g.anynz = c->anynz.as<uint8_t>();
@@ -381,6 +388,8 @@ void run_graph(rbg_ctx *c, const rbg_params *p) {
   g.codesB = c->codesB.as<uint8_t>();
   g.depth_raw = c->depth.as<float>();
   g.unit = c->unit.as<float>();
+  g.unit16 = c->unit16.as<uint16_t>();
+  g.Kp = unit16_stride(S);
   g.anynz = c->anynz.as<uint8_t>();
   g.colnorm = c->colnorm.as<double>();
   g.has_depth = S > 0;
@@ -710,7 +719,7 @@ int rbg_destroy(rbg_ctx *c) {
                   &c->anynz, &c->colnorm, &c->svbits, &c->topk, &c->topk_cnt, &c->maxc_cand,
                   &c->maxc_all, &c->stats, &c->pairs, &c->pair_out, &c->nbr, &c->nbr_sv,
                   &c->nbr_cnt, &c->row_edges, &c->e_from, &c->e_to, &c->e_scomp, &c->e_score,
-                  &c->badflag, &c->tmp, &c->cand_buf, &c->cand_cnt, &c->colacc};
+                  &c->badflag, &c->tmp, &c->cand_buf, &c->cand_cnt, &c->colacc, &c->unit16};
   for (DBuf *b : bufs) b->release();
   if (c->tables) {
     c->tables->U.release(); c->tables->codeA.release(); c->tables->W32.release();

@@ -23,6 +23,7 @@
 // Compiled with -fmad=false; __fmaf_rn marks every fused operation.
 #include <algorithm>
 #include <cstdint>
+#include <cuda_fp16.h>
 
 #include "rbg_internal.h"
 
@@ -364,6 +365,240 @@ k_allpairs(GraphArgs g, uint64_t *gbuf, int32_t *gcnt, int cap, int P, float lo,
   }
 }
 
+// ── sparse regime on the tensor cores ──────────────────────────────────────
+// The abundance prune is a threshold on U·Uᵀ.  A warp multiplies its 32 rows
+// (FP16 copies of the unit rank rows, A fragments kept in registers) with
+// 8-column tiles of its column slice (FP16, staged in shared memory, B
+// fragments by ldmatrix) using mma.sync m16n8k16 with FP32 accumulation.  For
+// unit rows, |c16 - c_ref| <= 2^-10·Σ|a_k b_k| + 2^-24·(|a|_1+|b|_1) + K·2^-22
+// + |c_ref - a·b| < 1.1e-3 (FP16 rounding of both inputs, accumulation,
+// the reference's own FP32 error), so every pair with c16 < eps - kTcDelta is
+// pruned exactly as the reference prunes it.  The rest are checked one per
+// lane: FP32 chain with its own band, then the AVX-512 order inside the band.
+constexpr float kTcDelta = 2.5e-3f;
+constexpr int kTCT = 64;          // columns per staged tile
+constexpr int kCQ = 512;          // check-queue ring entries per warp
+
+__device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0,
+                                         uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ void ldsm_x4(uint32_t (&r)[4], const void *p) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(a));
+}
+__device__ __forceinline__ void ldsm_x2(uint32_t &r0, uint32_t &r1, const void *p) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+  asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0,%1}, [%2];\n"
+               : "=r"(r0), "=r"(r1)
+               : "r"(a));
+}
+
+// Exact prune decision for up to 32 queued candidates (lane = candidate),
+// survivors appended to the counting queue.
+template <int SMAX>
+__device__ __forceinline__ void check_batch(const GraphArgs &g, Warp &w, const int *cq,
+                                            unsigned head, int nq, int64_t row0, int *q,
+                                            int &qn, float lo, float hi,
+                                            unsigned long long &n_cmp) {
+  const int lane = threadIdx.x & 31;
+  const bool act = lane < nq;
+  const unsigned e = act ? (unsigned)cq[(head + lane) & (kCQ - 1)] : 0u;
+  const int r = (int)(e >> 27);
+  const int64_t j = e & 0x07FFFFFFu;
+  const int64_t row = row0 + r;
+  bool pass = false;
+  if (act && j != row && (__ldg(g.anynz + row) | __ldg(g.anynz + j))) {
+    const int Su = g.Su;
+    const float4 *ua = (const float4 *)(g.unit + row * Su);
+    const float4 *ub = (const float4 *)(g.unit + j * Su);
+    float ur[SMAX];
+    float c1 = 0.f;
+#pragma unroll
+    for (int t4 = 0; t4 < SMAX; t4 += 4) {
+      if (t4 < Su) {
+        const float4 x = __ldg(ua + (t4 >> 2)), y = __ldg(ub + (t4 >> 2));
+        ur[t4] = x.x; ur[t4 + 1] = x.y; ur[t4 + 2] = x.z; ur[t4 + 3] = x.w;
+        c1 = __fmaf_rn(x.x, y.x, c1);
+        c1 = __fmaf_rn(x.y, y.y, c1);
+        c1 = __fmaf_rn(x.z, y.z, c1);
+        c1 = __fmaf_rn(x.w, y.w, c1);
+      } else {
+        ur[t4] = ur[t4 + 1] = ur[t4 + 2] = ur[t4 + 3] = 0.f;
+      }
+    }
+    if (c1 >= hi) pass = true;
+    else if (c1 >= lo) pass = !(dot_avx512<SMAX>(ur, g.unit + j * Su, g.S) < g.prefilter_eps);
+  }
+  const unsigned m = __ballot_sync(FULL, pass);
+  if (pass) q[qn + __popc(m & ((1u << lane) - 1u))] = (int)(((unsigned)r << 27) | (unsigned)j);
+  qn += __popc(m);
+  __syncwarp();
+  if (qn >= 32) {
+    count_batch(g, w, q, 32, row0);
+    n_cmp += 1;
+    if (lane + 32 < qn) q[lane] = q[lane + 32];
+    __syncwarp();
+    qn -= 32;
+  }
+}
+
+template <int KS, int SMAX>
+__global__ void __launch_bounds__(kWarps * 32)
+k_allpairs_tc(GraphArgs g, uint64_t *gbuf, int32_t *gcnt, int cap, int P, float lo, float hi,
+              float lo16) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gq = lane >> 2, tq = lane & 3;
+  const int64_t n = g.n;
+  const int64_t row0 = (int64_t)blockIdx.x * 32;
+  const int slice = blockIdx.y * kWarps + warp;
+  const int64_t jb = n * slice / P, je = n * (slice + 1) / P;
+  const int Kp = KS * 16;
+  const int cstride = Kp * 2 + 16;                 // bytes per staged column (conflict-free ldmatrix)
+
+  unsigned char *ws = smem + (size_t)warp * 1024;
+  uint64_t *thr = (uint64_t *)ws;
+  int *cnt = (int *)(thr + 32);
+  uint32_t *mxc = (uint32_t *)(cnt + 32);
+  int *q = (int *)(mxc + 32);                      // [kQ] survivors to count
+  int *cq = (int *)(smem + (size_t)kWarps * 1024) + (size_t)warp * kCQ;      // check ring
+  unsigned char *ring = smem + (size_t)kWarps * 1024 + (size_t)kWarps * kCQ * 4 +
+                        (size_t)warp * 2 * kTCT * cstride;
+  thr[lane] = 0;
+  cnt[lane] = 0;
+  mxc[lane] = 0;
+  const size_t bufrow = ((size_t)blockIdx.x * P + slice) * 32;
+  Warp w{gbuf + bufrow * cap, cnt, thr, mxc, cap, g.K};
+  unsigned long long n_pref = 0, n_cmp = 0;
+
+  // A fragments: rows mt*16 + gq (+8), k = ks*16 + 2*tq (+8)
+  uint32_t af[2][KS][4];
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt) {
+    const int64_t ra = row0 + mt * 16 + gq, rb = ra + 8;
+    const uint32_t *pa = (const uint32_t *)(g.unit16 + (ra < n ? ra : 0) * Kp);
+    const uint32_t *pb = (const uint32_t *)(g.unit16 + (rb < n ? rb : 0) * Kp);
+#pragma unroll
+    for (int ks = 0; ks < KS; ++ks) {
+      af[mt][ks][0] = ra < n ? __ldg(pa + ks * 8 + tq) : 0u;
+      af[mt][ks][1] = rb < n ? __ldg(pb + ks * 8 + tq) : 0u;
+      af[mt][ks][2] = ra < n ? __ldg(pa + ks * 8 + 4 + tq) : 0u;
+      af[mt][ks][3] = rb < n ? __ldg(pb + ks * 8 + 4 + tq) : 0u;
+    }
+  }
+  auto stage_cols = [&](int st, int64_t jt) {
+    const int nc = (int)(je - jt < kTCT ? je - jt : kTCT);
+    unsigned char *dst = ring + (size_t)st * kTCT * cstride;
+    const int per = Kp / 8;                        // 16-byte chunks per column
+    for (int i = lane; i < nc * per; i += 32) {
+      const int c = i / per, t = i - c * per;
+      cp16(dst + c * cstride + 16 * t, g.unit16 + (jt + c) * Kp + 8 * t);
+    }
+    cp_commit();
+  };
+  unsigned head = 0, tail = 0;                     // check ring
+  int qn = 0;
+  if (jb < je) stage_cols(0, jb);
+  int st = 0;
+  for (int64_t jt = jb; jt < je; jt += kTCT, st ^= 1) {
+    if (jt + kTCT < je) stage_cols(st ^ 1, jt + kTCT); else cp_commit();
+    const int nc = (int)(je - jt < kTCT ? je - jt : kTCT);
+    cp_wait1();
+    __syncwarp();
+    const unsigned char *tile = ring + (size_t)st * kTCT * cstride;
+    for (int c0 = 0; c0 < nc; c0 += 8) {
+      float acc[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+      // B fragments: ldmatrix rows = columns c0 + (lane & 7), k block by lane >> 3
+      const unsigned char *bp = tile + (c0 + (lane & 7)) * cstride;
+      if (KS == 1) {
+        uint32_t b0, b1;
+        ldsm_x2(b0, b1, bp + 16 * ((lane >> 3) & 1));
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) mma16816(acc[mt], af[mt][0], b0, b1);
+      } else {
+#pragma unroll
+        for (int kp = 0; kp < KS; kp += 2) {
+          uint32_t b[4];
+          ldsm_x4(b, bp + 16 * (2 * kp + (lane >> 3)));
+#pragma unroll
+          for (int mt = 0; mt < 2; ++mt) {
+            mma16816(acc[mt], af[mt][kp], b[0], b[1]);
+            mma16816(acc[mt], af[mt][kp + 1], b[2], b[3]);
+          }
+        }
+      }
+      // candidates: value i of m-tile mt -> row mt*16 + gq + 8*(i>>1), column c0 + 2*tq + (i&1)
+      unsigned mk = 0;
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int rr = mt * 16 + gq + 8 * (i >> 1);
+          const int cc = c0 + 2 * tq + (i & 1);
+          if (acc[mt][i] >= lo16 && cc < nc && row0 + rr < n) mk |= 1u << (mt * 4 + i);
+        }
+      n_pref += 8;
+      if (__any_sync(FULL, mk != 0)) {
+        const int cntl = __popc(mk);
+        int incl = cntl;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(FULL, incl, o);
+          if (lane >= o) incl += v;
+        }
+        const int total = __shfl_sync(FULL, incl, 31);
+        unsigned pos = tail + (unsigned)(incl - cntl);
+        while (mk) {
+          const int b = __ffs(mk) - 1;
+          mk &= mk - 1;
+          const int mt = b >> 2, i = b & 3;
+          const int rr = mt * 16 + gq + 8 * (i >> 1);
+          const int64_t jj = jt + c0 + 2 * tq + (i & 1);
+          cq[pos & (kCQ - 1)] = (int)(((unsigned)rr << 27) | (unsigned)jj);
+          ++pos;
+        }
+        tail += (unsigned)total;
+        __syncwarp();
+        while (tail - head >= 32) {
+          check_batch<SMAX>(g, w, cq, head, 32, row0, q, qn, lo, hi, n_cmp);
+          head += 32;
+        }
+      }
+    }
+    __syncwarp();
+  }
+  while (tail != head) {
+    const int nq = (int)(tail - head < 32 ? tail - head : 32);
+    check_batch<SMAX>(g, w, cq, head, nq, row0, q, qn, lo, hi, n_cmp);
+    head += (unsigned)nq;
+  }
+  if (qn > 0) {
+    n_cmp += lane < qn;
+    count_batch(g, w, q, qn, row0);
+  }
+  if (g.stats) {
+    const unsigned a = __reduce_add_sync(FULL, (unsigned)n_pref),
+                   b = __reduce_add_sync(FULL, (unsigned)n_cmp);
+    if (lane == 0) {
+      if (a) atomicAdd(g.stats, (unsigned long long)a);
+      if (b) atomicAdd(g.stats + 1, (unsigned long long)b);
+    }
+  }
+  __syncwarp();
+  compact_full_rows(w, g.K);
+  gcnt[bufrow + lane] = cnt[lane];
+  const int64_t row = row0 + lane;
+  if (row < n && mxc[lane]) atomicMax(g.maxcnt_cand + row, mxc[lane]);
+}
+
 // Warp per row: the K best keys among the P slices' partial lists.
 __global__ void k_merge_topk(GraphArgs g, const uint64_t *gbuf, const int32_t *gcnt, int cap,
                              int P) {
@@ -446,9 +681,20 @@ void launch_allpairs(const GraphArgs &g, uint64_t *gbuf, int32_t *gcnt, cudaStre
     k_allpairs<SM, SP><<<grid, kWarps * 32, smem, s>>>(g, gbuf, gcnt, cap, P, lo, hi);      \
   } while (0)
   if (sparse) {
-    if (g.Su <= 16) RBG_LAUNCH(16, true);
-    else if (g.Su <= 32) RBG_LAUNCH(32, true);
-    else RBG_LAUNCH(64, true);
+    const float lo16 = (float)(eps - (double)kTcDelta);
+    const size_t tsm = (size_t)kWarps * 1024 + (size_t)kWarps * kCQ * 4 +
+                       (size_t)kWarps * 2 * kTCT * (g.Kp * 2 + 16);
+#define RBG_TC(KS, SM)                                                                        \
+  do {                                                                                        \
+    cudaFuncSetAttribute(k_allpairs_tc<KS, SM>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
+                         (int)tsm);                                                           \
+    k_allpairs_tc<KS, SM><<<grid, kWarps * 32, tsm, s>>>(g, gbuf, gcnt, cap, P, lo, hi, lo16); \
+  } while (0)
+    // the FP16 rows are 16, 32 or 64 halves wide: exactly KS * 16
+    if (g.Kp == 16) RBG_TC(1, 16);
+    else if (g.Kp == 32) RBG_TC(2, 32);
+    else if (g.Kp == 64) RBG_TC(4, 64);
+#undef RBG_TC
   } else {
     RBG_LAUNCH(4, false);
   }

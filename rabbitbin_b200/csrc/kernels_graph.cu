@@ -7,6 +7,7 @@
 // code below calls __fmaf_rn / __fma_rn explicitly; everything else rounds
 // operation by operation exactly as the reference does.
 #include <cstdint>
+#include <cuda_fp16.h>
 
 #include "rbg_internal.h"
 
@@ -59,8 +60,15 @@ __global__ void k_unit_rows(GraphArgs g) {
   for (int o = 16; o; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
   float *u = g.unit + r * g.Su;
   const double inv = ss > 0.0 ? 1.0 / __dsqrt_rn(ss) : 0.0;
-  if (lane < g.Su) u[lane] = (lane < S && ss > 0.0) ? __double2float_rn(__dmul_rn(d0, inv)) : 0.0f;
-  if (lane + 32 < g.Su) u[lane + 32] = (lane + 32 < S && ss > 0.0) ? __double2float_rn(__dmul_rn(d1, inv)) : 0.0f;
+  const float f0 = (lane < S && ss > 0.0) ? __double2float_rn(__dmul_rn(d0, inv)) : 0.0f;
+  const float f1 = (lane + 32 < S && ss > 0.0) ? __double2float_rn(__dmul_rn(d1, inv)) : 0.0f;
+  if (lane < g.Su) u[lane] = f0;
+  if (lane + 32 < g.Su) u[lane + 32] = f1;
+  if (g.unit16) {
+    uint16_t *h = g.unit16 + r * g.Kp;
+    if (lane < g.Kp) h[lane] = __half_as_ushort(__float2half_rn(f0));
+    if (lane + 32 < g.Kp) h[lane + 32] = __half_as_ushort(__float2half_rn(f1));
+  }
 }
 
 // Column norms of the raw depths (src/rabbitbin.cpp:4800-4806): the reference

@@ -82,6 +82,8 @@ struct GraphArgs {
   const uint8_t *codesA = nullptr, *codesB = nullptr;
   const float *depth_raw = nullptr;    // [n][S]
   float *unit = nullptr;               // [n][Su] centred + L2-normalised ranks, 0-padded
+  uint16_t *unit16 = nullptr;          // [n][Kp] the same rows rounded to FP16 (tensor-core prefilter)
+  int Kp = 16;                         // row stride of unit16 (S rounded up to 16)
   uint8_t *anynz = nullptr;            // [n]
   double *colnorm = nullptr;           // [S]
   float min_cv = 1.0f;
