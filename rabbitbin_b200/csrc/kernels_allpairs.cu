@@ -171,6 +171,56 @@ __device__ __forceinline__ void count_batch(const GraphArgs &g, Warp &w, const i
   compact_full_rows(w, w.cap - 32);
 }
 
+// Register-match counts of up to 32 queued survivors, the warp working on one
+// survivor at a time: row codes from shared memory (sA, [32][mpad]) and column
+// codes as coalesced 16-byte loads, four survivors in flight.  Lane p ends
+// with survivor p's count and admits it.
+__device__ __forceinline__ void count_batch_coop(const GraphArgs &g, Warp &w, const int *q, int nq,
+                                                 const unsigned char *sA) {
+  const int lane = threadIdx.x & 31;
+  const int m16 = g.mpad >> 4;
+  uint32_t mine = 0;
+  for (int p = 0; p < nq; p += 4) {
+    const uint4 *ra[4], *cb[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const unsigned e = (unsigned)q[p + u < nq ? p + u : p];
+      ra[u] = (const uint4 *)(sA + (size_t)(e >> 27) * g.mpad);
+      cb[u] = (const uint4 *)(g.codesB + (int64_t)(e & 0x07FFFFFFu) * g.mpad);
+    }
+    uint32_t acc[4] = {0u, 0u, 0u, 0u};
+    for (int t = lane; t < m16; t += 32) {      // <= 8 steps: byte lanes stay below 256
+      uint4 b[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) b[u] = __ldg(cb[u] + t);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const uint4 a = ra[u][t];
+        acc[u] += eq_bytes(a.x, b[u].x) + eq_bytes(a.y, b[u].y) + eq_bytes(a.z, b[u].z) +
+                  eq_bytes(a.w, b[u].w);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const uint32_t c = __reduce_add_sync(FULL, byte_sum(acc[u]));
+      if (lane == p + u) mine = c;
+    }
+  }
+  if (lane < nq) {
+    const unsigned e = (unsigned)q[lane];
+    const int r = (int)(e >> 27);
+    const int64_t j = e & 0x07FFFFFFu;
+    atomicMax(&w.mxc[r], mine);
+    const uint64_t key = ((uint64_t)__ldg(g.sv_bits + mine) << 32) | (uint64_t)(~(uint32_t)j);
+    if (key > w.thr[r]) {
+      const int p = atomicAdd(&w.cnt[r], 1);
+      w.gbuf[(size_t)r * w.cap + p] = key;
+    }
+  }
+  __syncwarp();
+  compact_full_rows(w, w.cap - 32);
+}
+
 template <int SMAX, bool SPARSE>
 __global__ void __launch_bounds__(kWarps * 32)
 k_allpairs(GraphArgs g, uint64_t *gbuf, int32_t *gcnt, int cap, int P, float lo, float hi) {
@@ -376,7 +426,7 @@ k_allpairs(GraphArgs g, uint64_t *gbuf, int32_t *gcnt, int cap, int P, float lo,
 // pruned exactly as the reference prunes it.  The rest are checked one per
 // lane: FP32 chain with its own band, then the AVX-512 order inside the band.
 constexpr float kTcDelta = 2.5e-3f;
-constexpr int kTCT = 64;          // columns per staged tile
+constexpr int kTCT = 32;          // columns per staged tile
 constexpr int kCQ = 512;          // check-queue ring entries per warp
 
 __device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0,
@@ -407,7 +457,8 @@ template <int SMAX>
 __device__ __forceinline__ void check_batch(const GraphArgs &g, Warp &w, const int *cq,
                                             unsigned head, int nq, int64_t row0, int *q,
                                             int &qn, float lo, float hi,
-                                            unsigned long long &n_cmp) {
+                                            unsigned long long &n_cmp, const float *sU,
+                                            const unsigned char *sA) {
   const int lane = threadIdx.x & 31;
   const bool act = lane < nq;
   const unsigned e = act ? (unsigned)cq[(head + lane) & (kCQ - 1)] : 0u;
@@ -417,14 +468,14 @@ __device__ __forceinline__ void check_batch(const GraphArgs &g, Warp &w, const i
   bool pass = false;
   if (act && j != row && (__ldg(g.anynz + row) | __ldg(g.anynz + j))) {
     const int Su = g.Su;
-    const float4 *ua = (const float4 *)(g.unit + row * Su);
+    const float4 *ua = (const float4 *)(sU + r * Su);
     const float4 *ub = (const float4 *)(g.unit + j * Su);
     float ur[SMAX];
     float c1 = 0.f;
 #pragma unroll
     for (int t4 = 0; t4 < SMAX; t4 += 4) {
       if (t4 < Su) {
-        const float4 x = __ldg(ua + (t4 >> 2)), y = __ldg(ub + (t4 >> 2));
+        const float4 x = ua[t4 >> 2], y = __ldg(ub + (t4 >> 2));
         ur[t4] = x.x; ur[t4 + 1] = x.y; ur[t4 + 2] = x.z; ur[t4 + 3] = x.w;
         c1 = __fmaf_rn(x.x, y.x, c1);
         c1 = __fmaf_rn(x.y, y.y, c1);
@@ -442,7 +493,7 @@ __device__ __forceinline__ void check_batch(const GraphArgs &g, Warp &w, const i
   qn += __popc(m);
   __syncwarp();
   if (qn >= 32) {
-    count_batch(g, w, q, 32, row0);
+    count_batch_coop(g, w, q, 32, sA);
     n_cmp += 1;
     if (lane + 32 < qn) q[lane] = q[lane + 32];
     __syncwarp();
@@ -470,8 +521,27 @@ k_allpairs_tc(GraphArgs g, uint64_t *gbuf, int32_t *gcnt, int cap, int P, float 
   uint32_t *mxc = (uint32_t *)(cnt + 32);
   int *q = (int *)(mxc + 32);                      // [kQ] survivors to count
   int *cq = (int *)(smem + (size_t)kWarps * 1024) + (size_t)warp * kCQ;      // check ring
-  unsigned char *ring = smem + (size_t)kWarps * 1024 + (size_t)kWarps * kCQ * 4 +
-                        (size_t)warp * 2 * kTCT * cstride;
+  unsigned char *rings = smem + (size_t)kWarps * 1024 + (size_t)kWarps * kCQ * 4;
+  unsigned char *ring = rings + (size_t)warp * 2 * kTCT * cstride;
+  // the block's 32 rows: register codes [32][mpad] and unit rows [32][Su]
+  unsigned char *sA = rings + (size_t)kWarps * 2 * kTCT * cstride;
+  float *sU = (float *)(sA + (size_t)32 * g.mpad);
+  {
+    const int m16 = g.mpad >> 4, s4 = g.Su >> 2;
+    for (int i = threadIdx.x; i < 32 * m16; i += blockDim.x) {
+      const int r = i / m16, t = i - r * m16;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (row0 + r < n) v = __ldg((const uint4 *)(g.codesA + (row0 + r) * g.mpad) + t);
+      *((uint4 *)(sA + (size_t)r * g.mpad) + t) = v;
+    }
+    for (int i = threadIdx.x; i < 32 * s4; i += blockDim.x) {
+      const int r = i / s4, t = i - r * s4;
+      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (row0 + r < n) v = __ldg((const float4 *)(g.unit + (row0 + r) * g.Su) + t);
+      *((float4 *)(sU + (size_t)r * g.Su) + t) = v;
+    }
+    __syncthreads();
+  }
   thr[lane] = 0;
   cnt[lane] = 0;
   mxc[lane] = 0;
@@ -568,7 +638,7 @@ k_allpairs_tc(GraphArgs g, uint64_t *gbuf, int32_t *gcnt, int cap, int P, float 
         tail += (unsigned)total;
         __syncwarp();
         while (tail - head >= 32) {
-          check_batch<SMAX>(g, w, cq, head, 32, row0, q, qn, lo, hi, n_cmp);
+          check_batch<SMAX>(g, w, cq, head, 32, row0, q, qn, lo, hi, n_cmp, sU, sA);
           head += 32;
         }
       }
@@ -577,12 +647,12 @@ k_allpairs_tc(GraphArgs g, uint64_t *gbuf, int32_t *gcnt, int cap, int P, float 
   }
   while (tail != head) {
     const int nq = (int)(tail - head < 32 ? tail - head : 32);
-    check_batch<SMAX>(g, w, cq, head, nq, row0, q, qn, lo, hi, n_cmp);
+    check_batch<SMAX>(g, w, cq, head, nq, row0, q, qn, lo, hi, n_cmp, sU, sA);
     head += (unsigned)nq;
   }
   if (qn > 0) {
     n_cmp += lane < qn;
-    count_batch(g, w, q, qn, row0);
+    count_batch_coop(g, w, q, qn, sA);
   }
   if (g.stats) {
     const unsigned a = __reduce_add_sync(FULL, (unsigned)n_pref),
@@ -599,43 +669,45 @@ k_allpairs_tc(GraphArgs g, uint64_t *gbuf, int32_t *gcnt, int cap, int P, float 
   if (row < n && mxc[lane]) atomicMax(g.maxcnt_cand + row, mxc[lane]);
 }
 
-// Warp per row: the K best keys among the P slices' partial lists.
-__global__ void k_merge_topk(GraphArgs g, const uint64_t *gbuf, const int32_t *gcnt, int cap,
-                             int P) {
-  extern __shared__ uint64_t mk[];
+// Warp per row: the K best keys among the P slices' partial lists.  The lists
+// stream through a 512-key shared buffer per warp; whenever it fills, the
+// register radix select keeps its K best (K <= 448 leaves room to refill).
+constexpr int kMergeWarps = 8;
+constexpr int kMergeBuf = 32 * kCapW;       // 512 keys per warp
+
+__global__ void __launch_bounds__(kMergeWarps * 32)
+k_merge_topk(GraphArgs g, const uint64_t *gbuf, const int32_t *gcnt, int cap, int P) {
+  __shared__ uint64_t mk[kMergeWarps][kMergeBuf];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int64_t row = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
+  const int64_t row = (int64_t)blockIdx.x * kMergeWarps + wib;
   if (row >= g.n) return;
   const int K = g.K;
-  uint64_t *keys = mk + (size_t)wib * P * K;
+  uint64_t *keys = mk[wib];
   const int64_t rb = row >> 5, rl = row & 31;
-  int tot = 0;
+  const size_t br0 = (size_t)rb * P * 32 + rl;          // slice s: br0 + 32 s
+  const int cl = lane < P ? gcnt[br0 + (size_t)lane * 32] : 0;   // P <= 32
+  int fill = 0;
   for (int s = 0; s < P; ++s) {
-    const size_t br = ((size_t)rb * P + s) * 32 + rl;
-    const int c = gcnt[br];
-    for (int i = lane; i < c; i += 32) keys[tot + i] = gbuf[br * cap + i];
-    tot += c;
-  }
-  __syncwarp();
-  uint64_t Pk = 0;
-  if (tot > K) {
-    for (int bit = 63; bit >= 0; --bit) {
-      const uint64_t c = Pk | (1ull << bit);
-      int k = 0;
-      for (int i = lane; i < tot; i += 32) k += keys[i] >= c;
-      if ((int)__reduce_add_sync(FULL, (unsigned)k) >= K) Pk = c;
+    const int c = __shfl_sync(FULL, cl, s);
+    const uint64_t *src = gbuf + (br0 + (size_t)s * 32) * cap;
+    for (int i0 = 0; i0 < c;) {
+      const int take = min(c - i0, kMergeBuf - fill);
+      for (int i = lane; i < take; i += 32) keys[fill + i] = src[i0 + i];
+      fill += take;
+      i0 += take;
+      __syncwarp();
+      if (fill == kMergeBuf) {
+        select_topk(keys, fill, K);
+        fill = K;
+      }
     }
   }
-  int out = 0;
-  for (int base = 0; base < tot; base += 32) {
-    const int i = base + lane;
-    const uint64_t v = i < tot ? keys[i] : 0ull;
-    const bool keep = i < tot && v >= Pk;
-    const unsigned m = __ballot_sync(FULL, keep);
-    if (keep) g.topk[row * K + out + __popc(m & ((1u << lane) - 1u))] = v;
-    out += __popc(m);
+  if (fill > K) {
+    select_topk(keys, fill, K);
+    fill = K;
   }
-  if (lane == 0) g.topk_cnt[row] = out;
+  for (int i = lane; i < fill; i += 32) g.topk[row * K + i] = keys[i];
+  if (lane == 0) g.topk_cnt[row] = fill;
 }
 
 size_t allpairs_smem(int mpad, int Su, bool sparse) {
@@ -683,7 +755,8 @@ void launch_allpairs(const GraphArgs &g, uint64_t *gbuf, int32_t *gcnt, cudaStre
   if (sparse) {
     const float lo16 = (float)(eps - (double)kTcDelta);
     const size_t tsm = (size_t)kWarps * 1024 + (size_t)kWarps * kCQ * 4 +
-                       (size_t)kWarps * 2 * kTCT * (g.Kp * 2 + 16);
+                       (size_t)kWarps * 2 * kTCT * (g.Kp * 2 + 16) + (size_t)32 * g.mpad +
+                       (size_t)32 * g.Su * 4;
 #define RBG_TC(KS, SM)                                                                        \
   do {                                                                                        \
     cudaFuncSetAttribute(k_allpairs_tc<KS, SM>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
@@ -699,9 +772,8 @@ void launch_allpairs(const GraphArgs &g, uint64_t *gbuf, int32_t *gcnt, cudaStre
     RBG_LAUNCH(4, false);
   }
 #undef RBG_LAUNCH
-  const size_t msm = (size_t)P * g.K * sizeof(uint64_t);
-  cudaFuncSetAttribute(k_merge_topk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msm);
-  k_merge_topk<<<(unsigned)g.n, 32, msm, s>>>(g, gbuf, gcnt, cap, P);
+  k_merge_topk<<<(unsigned)((g.n + kMergeWarps - 1) / kMergeWarps), kMergeWarps * 32, 0, s>>>(
+      g, gbuf, gcnt, cap, P);
 }
 
 }  // namespace rbg
