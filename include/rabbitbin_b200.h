@@ -138,6 +138,44 @@ int rbg_bin_graph(rbg_ctx *ctx, const rbg_params *p, const char *seqcat,
                   const int64_t *offsets, int64_t n, const float *depth,
                   int32_t S, rbg_graph *out);
 
+/* ── batching: many assemblies per launch ─────────────────────────────────
+ * No counterpart in the reference, which bins one assembly per process
+ * (rb_cmd_bin, src/rabbitbin.cpp:4660-5622).  Each assembly's graph equals
+ * rbg_bin_graph on that assembly alone (same edges, same weights). */
+typedef struct rbg_assembly {
+  const char *seqcat;          /* host ASCII contigs back to back              */
+  const int64_t *offsets;      /* n + 1 offsets into seqcat, offsets[0] == 0   */
+  int64_t n;                   /* contigs                                      */
+  const float *depth;          /* n x S coverage means (NULL when S == 0)      */
+  int32_t S;                   /* coverage samples                             */
+  int32_t reserved;
+  const rbg_params *params;    /* NULL: the call's default parameters          */
+} rbg_assembly;
+
+typedef struct rbg_batch_stats {
+  float stage_ms;              /* host -> device copies of the inputs (device)  */
+  float graph_ms;              /* sketch, b0, all-pairs, merge (device)         */
+  float calib_ms;              /* cutoff calibration of every assembly (host)   */
+  float emit_ms;               /* edges + weights + copies back (device)        */
+  float total_ms;              /* the whole call (host clock)                   */
+  int32_t n_assemblies;
+  int32_t kernel_launches;     /* kernels in the call's launch sequence          */
+  int32_t graph_launches;      /* CUDA graph launches (0 with RBG_NO_GRAPHS set) */
+  int32_t reserved;
+  int64_t rows;                /* contigs over all assemblies                   */
+  int64_t pairs;               /* contig pairs scored, sum of n (n - 1) / 2     */
+  int64_t items;               /* all-pairs work items (32 rows x 4 slices)     */
+  int64_t edges;
+} rbg_batch_stats;
+
+/* Sketch and graph n_asm assemblies together: one pass of every kernel over
+ * all of them (persistent all-pairs kernels pull (assembly, row block)
+ * items from a device queue; each stage's launches form one CUDA graph) and
+ * one host round trip for all calibrations.  out[i] (n_asm entries) receives
+ * assembly i's graph; free each with rbg_free_graph.  `stats` may be NULL. */
+int rbg_bin_batch(rbg_ctx *ctx, const rbg_params *defaults, const rbg_assembly *asms,
+                  int32_t n_asm, rbg_graph *out, rbg_batch_stats *stats);
+
 /* Device-resident form used by batching, serving and the benchmark: stage the
  * inputs once (host -> device), run the hot path on them any number of times,
  * then fetch the graph (device -> host). */

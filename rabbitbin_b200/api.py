@@ -55,6 +55,25 @@ class Timing(C.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_ if n != "reserved"}
 
 
+class Assembly(C.Structure):
+    """rbg_assembly: one assembly of a batch (host arrays)."""
+    _fields_ = [("seqcat", C.c_char_p), ("offsets", C.POINTER(C.c_int64)), ("n", C.c_int64),
+                ("depth", C.POINTER(C.c_float)), ("S", C.c_int32), ("reserved", C.c_int32),
+                ("params", C.POINTER(Params))]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [(n, C.c_float) for n in ("stage_ms", "graph_ms", "calib_ms", "emit_ms",
+                                        "total_ms")] + \
+               [("n_assemblies", C.c_int32), ("kernel_launches", C.c_int32),
+                ("graph_launches", C.c_int32), ("reserved", C.c_int32),
+                ("rows", C.c_int64), ("pairs", C.c_int64), ("items", C.c_int64),
+                ("edges", C.c_int64)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_ if n != "reserved"}
+
+
 _lib = None
 
 
@@ -90,6 +109,8 @@ def lib():
         "rbg_pmh_stream_tables": ([C.c_int32, C.c_int32, C.c_uint64, C.c_int32,
                                    P(C.c_int32), P(C.c_int32), P(C.c_double),
                                    P(C.c_uint32)], C.c_int),
+        "rbg_bin_batch": ([vp, P(Params), P(Assembly), C.c_int32, P(Graph), P(BatchStats)],
+                          C.c_int),
         "rbg_build_pmh_winners_noalloc": ([P(Params), vp, vp, C.c_int64, C.c_int64, vp, vp,
                                            C.c_char_p, C.c_size_t], C.c_int),
     }
@@ -241,3 +262,38 @@ class Context:
 
     def fetch_graph(self):
         return self._graph_call(self._L.rbg_fetch_graph, self._h)
+
+    def bin_batch(self, assemblies, params=None):
+        """Graphs of many assemblies in one call (rbg_bin_batch).
+
+        `assemblies`: sequence of (seqcat, offsets, depth) or
+        (seqcat, offsets, depth, params); depth is n x S (S may be 0).
+        Returns (list of graph dicts in input order, stats dict)."""
+        dflt = params or default_params()
+        nb = len(assemblies)
+        arr = (Assembly * max(nb, 1))()
+        keep = []
+        for i, a in enumerate(assemblies):
+            seq, offs, depth = a[0], a[1], a[2]
+            p = a[3] if len(a) > 3 and a[3] is not None else None
+            offs = np.ascontiguousarray(offs, np.int64)
+            n = len(offs) - 1
+            dep = np.ascontiguousarray(depth, np.float32)
+            S = dep.shape[1] if dep.ndim == 2 else (dep.size // n if n > 0 else 0)
+            d = dep.reshape(n, S)
+            keep += [seq, offs, d, p]
+            arr[i].seqcat = seq
+            arr[i].offsets = _p(offs, C.c_int64)
+            arr[i].n = n
+            arr[i].depth = _p(d, C.c_float) if d.size else None
+            arr[i].S = S
+            arr[i].params = C.pointer(p) if p is not None else None
+        outs = (Graph * max(nb, 1))()
+        st = BatchStats()
+        self._check(self._L.rbg_bin_batch(self._h, C.byref(dflt), arr, nb, outs, C.byref(st)),
+                    "bin_batch")
+        try:
+            return [_graph_dict(outs[i]) for i in range(nb)], st.as_dict()
+        finally:
+            for i in range(nb):
+                self._L.rbg_free_graph(C.byref(outs[i]))

@@ -1,0 +1,679 @@
+// Batch engine: many assemblies sketched and graphed together.
+//
+// The assemblies of a call share one set of device buffers (rows of all
+// assemblies laid end to end) and one pass of each stage:
+//   pack (all bases) -> count (per k / GC-norm group) -> register minimum (per
+//   sketch-table group) -> unit rows + column norms -> b0 and similarity
+//   tables (on the device) -> persistent all-pairs kernels pulling
+//   (assembly, row block, slice group) items from a device counter, one per
+//   variant (dense / tensor-core KS) -> top-K merge
+// then one host round trip for the rand()-driven calibration of every
+// assembly (the maxima and b0 come back together), then neighbour lists, edge
+// counts and the batch-wide scan, one more round trip for the edge total, and
+// edge emission + weights.  The device part of each of the three segments is
+// captured into a CUDA graph; an instantiated graph is updated in place when
+// the next batch has the same launch topology.
+//
+// Each assembly's result equals rbg_bin_graph on that assembly alone: the
+// kernels are the single-assembly kernels behind a descriptor lookup, and
+// the host steps are the same functions with private rand() state.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <thread>
+
+#include "engine_internal.h"
+
+namespace rbg {
+namespace {
+
+constexpr int kVariants[4] = {0, 1, 2, 4};
+
+inline int vslot(int v) { return v == 0 ? 0 : (v == 1 ? 1 : (v == 2 ? 2 : 3)); }
+
+struct AsmPlan {
+  int orig = 0;
+  const rbg_params *p = nullptr;
+  const rbg_assembly *in = nullptr;
+  int64_t n = 0, nbases = 0;
+  int S = 0, Su = 4, Kp = 16, m = 500, mpad = 512, K = 200, E = 136;
+  bool fused = false, abdfirst = false;
+  double w_comp = 0.0;
+  int variant = 0, P = 4, cap = 288;
+  // offsets into the batch buffers (elements of each buffer's type)
+  int64_t row0 = 0, base0 = 0, dep0 = 0, code0 = 0, unit0 = 0, u16_0 = 0, col0 = 0, acc0 = 0;
+  int64_t sv0 = 0, topk0 = 0, gbuf0 = 0, gcnt0 = 0, pair0 = 0, winv0 = 0;
+  int np = 0;
+  std::shared_ptr<const std::vector<int32_t>> pairs;
+};
+
+// Slices per row block for an assembly of the batch: the batch's row blocks
+// already give the GPU its parallelism, so slices only bound the size of one
+// work item (32 rows x n*4/P columns), which bounds the tail of the
+// persistent kernel.
+int batch_slices(int64_t n, int K, int variant) {
+  const double target = variant == 0 ? 4.0e5 : 3.0e6;       // pairs per work item
+  int64_t P = (int64_t)std::ceil(4.0 * 32.0 * (double)n / target);
+  const int pmax = std::max(4, std::min(32, (6400 / std::max(K, 1)) / 4 * 4));
+  P = std::min<int64_t>(std::max<int64_t>(P, 4), pmax);
+  P = std::min<int64_t>(P, std::max<int64_t>(4, (n / 64) / 4 * 4));
+  return (int)((P + 3) / 4 * 4);
+}
+
+double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// A captured stream segment, instantiated once and updated in place while the
+// launch topology stays the same.
+struct GraphSlot {
+  cudaGraphExec_t exec = nullptr;
+  void run(cudaStream_t s, cudaGraph_t g, int &launches) {
+    if (exec) {
+      cudaGraphExecUpdateResultInfo info;
+      if (cudaGraphExecUpdate(exec, g, &info) != cudaSuccess) {
+        cudaGetLastError();
+        cudaGraphExecDestroy(exec);
+        exec = nullptr;
+      }
+    }
+    if (!exec) {
+      const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+      if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        exec = nullptr;
+        CK(e);
+      }
+    }
+    cudaGraphDestroy(g);
+    CK(cudaGraphLaunch(exec, s));
+    ++launches;
+  }
+};
+
+struct GraphCache {
+  GraphSlot seg[3];
+};
+
+std::mutex g_graph_mu;
+std::map<rbg_ctx *, std::unique_ptr<GraphCache>> g_graphs;
+
+GraphCache &graphs_of(rbg_ctx *c) {
+  std::lock_guard<std::mutex> lk(g_graph_mu);
+  auto &p = g_graphs[c];
+  if (!p) p = std::make_unique<GraphCache>();
+  return *p;
+}
+
+// Runs `body` (stream work on c->stream) directly or as a captured graph.
+template <typename F>
+void captured(rbg_ctx *c, int seg, bool use_graph, int &graph_launches, F &&body) {
+  if (!use_graph) {
+    body();
+    CK(cudaGetLastError());
+    return;
+  }
+  CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+  try {
+    body();
+  } catch (...) {
+    cudaGraph_t g = nullptr;
+    cudaStreamEndCapture(c->stream, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamEndCapture(c->stream, &g));
+  graphs_of(c).seg[seg].run(c->stream, g, graph_launches);
+}
+
+template <typename T>
+T *dptr(DBuf &b, int64_t off) { return b.as<T>() + off; }
+
+inline size_t up256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+}  // namespace
+
+void release_batch_graphs(rbg_ctx *c) {
+  std::lock_guard<std::mutex> lk(g_graph_mu);
+  auto it = g_graphs.find(c);
+  if (it == g_graphs.end()) return;
+  for (auto &s : it->second->seg)
+    if (s.exec) cudaGraphExecDestroy(s.exec);
+  g_graphs.erase(it);
+}
+
+namespace {
+
+// Layout of one batch: per-assembly plans in batch order (grouped by sketch
+// configuration) and the sizes of the shared buffers.
+struct BatchPlan {
+  std::vector<AsmPlan> P;              // caller order
+  std::vector<int> ord;                // batch position -> caller index
+  int64_t rows = 0, bases = 0, dep = 0, code = 0, unit = 0, u16 = 0, col = 0, acc = 0, sv = 0;
+  int64_t topk = 0, gbuf = 0, gcnt = 0, npairs = 0, winv = 0, pairs_scored = 0;
+  int max_m = 2, max_k = 1, max_s = 0;
+  const AsmPlan &at(int b) const { return P[ord[b]]; }
+};
+
+void plan_batch(const rbg_params *defaults, const rbg_assembly *asms, int nb, BatchPlan &L) {
+  L.P.assign(nb, AsmPlan());
+  for (int i = 0; i < nb; ++i) {
+    AsmPlan &a = L.P[i];
+    const rbg_assembly &x = asms[i];
+    a.orig = i;
+    a.in = &x;
+    a.p = x.params ? x.params : defaults;
+    validate_params(a.p);
+    const std::string who = "assembly " + std::to_string(i) + ": ";
+    if (x.n < 0 || (x.n > 0 && (!x.offsets || !x.seqcat)))
+      throw Error(RBG_ERR_ARG, who + "bad sequence arguments");
+    if (x.S < 0 || x.S > kMaxS) throw Error(RBG_ERR_UNSUPPORTED, who + "S must be in 0..64");
+    if (x.S > 0 && x.n > 0 && !x.depth) throw Error(RBG_ERR_ARG, who + "depth is null");
+    if (x.n >= (1 << 27)) throw Error(RBG_ERR_UNSUPPORTED, who + "at most 2^27 - 1 contigs");
+    if (x.n > 0 && x.offsets[0] != 0) throw Error(RBG_ERR_ARG, who + "offsets[0] must be 0");
+    for (int64_t q = 0; q < x.n; ++q)
+      if (x.offsets[q + 1] < x.offsets[q])
+        throw Error(RBG_ERR_ARG, who + "offsets must be non-decreasing");
+    a.n = x.n;
+    a.nbases = x.n > 0 ? x.offsets[x.n] : 0;
+    a.S = x.S;
+    a.Su = (std::max(a.S, 1) + 3) & ~3;
+    a.Kp = unit16_stride(a.S);
+    a.m = a.p->m;
+    a.mpad = mpad_of(a.m);
+    a.K = a.p->max_edges;
+    a.E = a.p->k == 4 ? 136 : (a.p->k == 3 ? 32 : (a.p->k == 2 ? 10 : 2));
+    a.w_comp = (a.p->w_comp < 0.0) ? (a.S <= 2 ? 1.0 : 0.0) : a.p->w_comp;
+    a.fused = (a.p->force_path == 2) || (a.p->force_path == 0 && a.n > 25000);
+    if (a.fused && a.n <= 2500)
+      throw Error(RBG_ERR_ARG, who + "the fused path samples 2500 contigs; need n > 2500");
+    a.abdfirst = a.fused && a.p->abdfirst && a.S > 1 && a.w_comp < 1.0 && a.w_comp < a.p->min_edge;
+    a.variant = a.abdfirst ? a.Kp / 16 : 0;
+    a.P = batch_slices(a.n, a.K, a.variant);
+    a.cap = allpairs_cap(a.K);
+  }
+  // group order: equal count configuration, then equal sketch tables
+  L.ord.resize(nb);
+  std::iota(L.ord.begin(), L.ord.end(), 0);
+  auto key = [&](int i) {
+    const rbg_params *p = L.P[i].p;
+    return std::make_tuple(p->k, p->gc_norm, p->gc_norm_cap, p->m, p->pmh_seed,
+                           p->fp_contract != 0, p->win_bits);
+  };
+  std::stable_sort(L.ord.begin(), L.ord.end(), [&](int x, int y) { return key(x) < key(y); });
+  for (int b = 0; b < nb; ++b) {
+    AsmPlan &a = L.P[L.ord[b]];
+    a.row0 = L.rows; L.rows += a.n;
+    a.base0 = L.bases; L.bases += a.nbases;
+    a.dep0 = L.dep; L.dep += a.n * a.S;
+    a.code0 = L.code; L.code += a.n * a.mpad;
+    a.unit0 = L.unit; L.unit += a.n * a.Su;
+    a.u16_0 = L.u16; L.u16 += a.n * a.Kp;
+    a.col0 = L.col; L.col += std::max(a.S, 1);
+    a.acc0 = L.acc; L.acc += 3 * std::max(a.S, 1);
+    a.sv0 = L.sv; L.sv += a.m + 1;
+    a.topk0 = L.topk; L.topk += a.n * a.K;
+    const int64_t nbk = (a.n + 31) / 32;
+    a.gbuf0 = L.gbuf; L.gbuf += nbk * a.P * 32 * a.cap;
+    a.gcnt0 = L.gcnt; L.gcnt += nbk * a.P * 32;
+    a.winv0 = L.winv; L.winv += a.n * a.E;
+    if (a.p->base_on) {
+      a.pairs = b0_pairs(a.n);
+      a.np = (int)(a.pairs->size() / 2);
+    }
+    a.pair0 = L.npairs; L.npairs += a.np;
+    L.max_m = std::max(L.max_m, a.m);
+    L.max_k = std::max(L.max_k, a.K);
+    L.max_s = std::max(L.max_s, a.S);
+    L.pairs_scored += a.n * (a.n - 1) / 2;
+  }
+  if ((double)L.rows * L.max_k >= 2147483647.0)
+    throw Error(RBG_ERR_UNSUPPORTED, "batch too large: rows x max_edges must stay below 2^31");
+}
+
+void ensure_buffers(BatchBufs &B, const BatchPlan &L, int nb) {
+  const int64_t rows1 = std::max<int64_t>(L.rows, 1);
+  const int64_t nwords = (L.bases + 15) / 16 + 1;
+  B.ascii.ensure((size_t)((L.bases + 15) / 16) * 16 + 16);
+  B.offsets.ensure((L.rows + 1) * sizeof(int64_t));
+  B.depth.ensure(std::max<int64_t>(L.dep, 1) * sizeof(float));
+  B.packed.ensure(nwords * 4);
+  B.nmask.ensure((nwords / 2 + 2) * 4);
+  B.winv.ensure(std::max<int64_t>(L.winv, 1) * sizeof(double));
+  B.ecnt.ensure(rows1 * sizeof(int32_t));
+  B.codesA.ensure(std::max<int64_t>(L.code, 16));
+  B.codesB.ensure(std::max<int64_t>(L.code, 16));
+  B.unit.ensure(std::max<int64_t>(L.unit, 4) * sizeof(float));
+  B.unit16.ensure(std::max<int64_t>(L.u16, 16) * sizeof(uint16_t));
+  B.anynz.ensure(rows1);
+  B.colnorm.ensure(L.col * sizeof(double));
+  B.colacc.ensure(L.acc * sizeof(double));
+  B.svbits.ensure(L.sv * sizeof(uint32_t));
+  B.topk.ensure(std::max<int64_t>(L.topk, 1) * sizeof(uint64_t));
+  B.topk_cnt.ensure(rows1 * sizeof(int32_t));
+  B.maxc_cand.ensure(rows1 * sizeof(uint32_t));
+  B.maxc_all.ensure(rows1 * sizeof(uint32_t));
+  B.stats.ensure(2 * sizeof(unsigned long long));
+  B.gbuf.ensure(std::max<int64_t>(L.gbuf, 1) * sizeof(uint64_t));
+  B.gcnt.ensure(std::max<int64_t>(L.gcnt, 1) * sizeof(int32_t));
+  B.pairs.ensure(std::max<int64_t>(L.npairs, 1) * 2 * sizeof(int32_t));
+  B.pair_cnt.ensure(std::max<int64_t>(L.npairs, 1) * sizeof(uint32_t));
+  B.b0.ensure(nb * sizeof(float));
+  B.nbr.ensure(std::max<int64_t>(L.topk, 1) * sizeof(uint32_t));
+  B.nbr_sv.ensure(std::max<int64_t>(L.topk, 1) * sizeof(float));
+  B.nbr_cnt.ensure(rows1 * sizeof(int32_t));
+  B.row_edges.ensure((L.rows + 1) * sizeof(int32_t));
+  B.edge0s.ensure((nb + 1) * sizeof(int64_t));
+  B.desc.ensure(nb * sizeof(BatchAsm));
+  B.row0s.ensure((nb + 1) * sizeof(int64_t));
+  B.pair0s.ensure((nb + 1) * sizeof(int64_t));
+  B.lists.ensure(4 * (nb + 1) * sizeof(int32_t));
+  B.item0s.ensure(4 * (nb + 1) * sizeof(int64_t));
+  B.queues.ensure(4 * sizeof(unsigned long long));
+  B.e_from.ensure(4); B.e_to.ensure(4); B.e_scomp.ensure(4); B.e_score.ensure(4);
+}
+
+// The device descriptor of the assembly at batch position b (edge arrays are
+// filled in once the edge total is known).
+BatchAsm describe(BatchBufs &B, const AsmPlan &a, int b) {
+  const rbg_params *p = a.p;
+  BatchAsm d;
+  GraphArgs &g = d.g;
+  g.n = a.n; g.m = a.m; g.mpad = a.mpad; g.S = a.S; g.K = a.K; g.Su = a.Su; g.Kp = a.Kp;
+  g.codesA = dptr<uint8_t>(B.codesA, a.code0);
+  g.codesB = dptr<uint8_t>(B.codesB, a.code0);
+  g.depth_raw = dptr<float>(B.depth, a.dep0);
+  g.unit = dptr<float>(B.unit, a.unit0);
+  g.unit16 = dptr<uint16_t>(B.unit16, a.u16_0);
+  g.anynz = dptr<uint8_t>(B.anynz, a.row0);
+  g.colnorm = dptr<double>(B.colnorm, a.col0);
+  g.min_cv = (float)p->min_cv;
+  g.min_cv_d = p->min_cv;
+  g.has_depth = a.S > 0;
+  g.wjac_norm = p->wjac_norm;
+  g.small_path = a.fused ? 0 : 1;
+  g.prefilter = a.abdfirst ? 1 : 0;
+  const double abd_corr_min = a.abdfirst ? (p->min_edge - a.w_comp) / (1.0 - a.w_comp) : -2.0;
+  g.prefilter_eps = (float)(abd_corr_min - 1e-4);
+  g.sv_bits = dptr<uint32_t>(B.svbits, a.sv0);
+  g.topk = dptr<uint64_t>(B.topk, a.topk0);
+  g.topk_cnt = dptr<int32_t>(B.topk_cnt, a.row0);
+  g.maxcnt_cand = dptr<uint32_t>(B.maxc_cand, a.row0);
+  g.maxcnt_all = dptr<uint32_t>(B.maxc_all, a.row0);
+  g.stats = B.stats.as<unsigned long long>();
+  d.row0 = a.row0;
+  d.gbuf = dptr<uint64_t>(B.gbuf, a.gbuf0);
+  d.gcnt = dptr<int32_t>(B.gcnt, a.gcnt0);
+  d.cap = a.cap;
+  d.P = a.P;
+  d.variant = a.variant;
+  prefilter_bands(a.S, g.prefilter_eps, &d.lo, &d.hi, &d.lo16);
+  d.colnorm_on = need_colnorm(p, a.S) ? 1 : 0;
+  d.colacc = dptr<double>(B.colacc, a.acc0);
+  d.base_on = p->base_on ? 1 : 0;
+  d.np = a.np;
+  d.pair0 = a.pair0;
+  d.b0 = dptr<float>(B.b0, b);
+  d.sv_out = dptr<uint32_t>(B.svbits, a.sv0);
+  EmitArgs &e = d.e;
+  e.n = a.n; e.K = a.K; e.mutual = p->mutual; e.small_path = a.fused ? 0 : 1;
+  e.topk = g.topk; e.topk_cnt = g.topk_cnt;
+  e.nbr_sorted = dptr<uint32_t>(B.nbr, a.topk0);
+  e.nbr_sv = dptr<float>(B.nbr_sv, a.topk0);
+  e.nbr_cnt = dptr<int32_t>(B.nbr_cnt, a.row0);
+  e.row_edges = dptr<int32_t>(B.row_edges, a.row0);
+  WeightArgs &w = d.w;
+  w.S = a.S;
+  w.unit = g.unit;
+  w.Su = a.Su;
+  w.depth_raw = g.depth_raw;
+  w.colnorm = d.colnorm_on ? g.colnorm : nullptr;
+  w.w_comp = a.w_comp;
+  w.min_edge = p->min_edge;
+  w.neg_thr = p->neg_thr;
+  w.wjac_cut = p->wjac_cut;
+  w.depth_sim = p->depth_sim;
+  w.depth_fuse = p->depth_fuse;
+  w.wjac_gate = p->wjac_gate;
+  w.contract = p->fp_contract;
+  return d;
+}
+
+// Work lists of the persistent all-pairs kernels, one per variant slot.
+struct Lists {
+  std::vector<int32_t> list[4];
+  std::vector<int64_t> item0[4];
+  size_t smem[4] = {0, 0, 0, 0};
+};
+
+// Pack, count (one launch per k / GC-norm run), register minimum (one per
+// sketch-table run); returns the number of kernel launches.
+int launch_sketch_groups(rbg_ctx *c, BatchBufs &B, const BatchPlan &L,
+                         const std::vector<Tables *> &tab, int nb) {
+  int launches = 0;
+  launch_pack(B.ascii.as<char>(), L.bases, B.packed.as<uint32_t>(), B.nmask.as<uint32_t>(),
+              c->stream);
+  launches += L.bases ? 1 : 0;
+  for (int b0 = 0; b0 < nb;) {
+    const rbg_params *p = L.at(b0).p;
+    int b1 = b0;
+    while (b1 < nb && L.at(b1).p->k == p->k && L.at(b1).p->gc_norm == p->gc_norm &&
+           L.at(b1).p->gc_norm_cap == p->gc_norm_cap)
+      ++b1;
+    const AsmPlan &f = L.at(b0);
+    const AsmPlan &l = L.at(b1 - 1);
+    SketchArgs a;
+    a.packed = B.packed.as<uint32_t>();
+    a.nmask = B.nmask.as<uint32_t>();
+    a.offsets = B.offsets.as<int64_t>() + f.row0;
+    a.n = l.row0 + l.n - f.row0;
+    a.k = p->k;
+    a.gc_norm = p->gc_norm;
+    a.gc_cap = p->gc_norm_cap;
+    a.n_elems = tab[b0]->t->n_elems;
+    a.rank_of_code = tab[b0]->rank.as<int16_t>();
+    a.elem_winv = B.winv.as<double>() + f.winv0;
+    a.elem_cnt = B.ecnt.as<int32_t>() + f.row0;
+    launch_count(a, c->stream);
+    launches += a.n ? 1 : 0;
+    for (int t0 = b0; t0 < b1;) {
+      int t1 = t0;
+      while (t1 < b1 && tab[t1] == tab[t0]) ++t1;
+      const AsmPlan &tf = L.at(t0);
+      const AsmPlan &tl = L.at(t1 - 1);
+      SketchArgs r = a;
+      r.offsets = B.offsets.as<int64_t>() + tf.row0;
+      r.n = tl.row0 + tl.n - tf.row0;
+      r.m = tf.m;
+      r.mpad = tf.mpad;
+      r.elem_winv = B.winv.as<double>() + tf.winv0;
+      r.elem_cnt = B.ecnt.as<int32_t>() + tf.row0;
+      r.U = tab[t0]->U.as<double>();
+      r.codeA = tab[t0]->codeA.as<uint8_t>();
+      r.W32 = tab[t0]->W32.as<uint32_t>();
+      r.codesA = B.codesA.as<uint8_t>() + tf.code0;
+      r.codesB = B.codesB.as<uint8_t>() + tf.code0;
+      r.winners32 = nullptr;
+      launch_minreduce(r, c->stream);
+      launches += r.n ? 1 : 0;
+      t0 = t1;
+    }
+    b0 = b1;
+  }
+  return launches;
+}
+
+// Depth rows, b0, all-pairs and merge for the whole batch.
+int launch_graph_stage(rbg_ctx *c, BatchBufs &B, const BatchPlan &L, const Lists &W, int nb) {
+  const BatchAsm *dD = B.desc.as<BatchAsm>();
+  const int64_t rows1 = std::max<int64_t>(L.rows, 1);
+  int launches = 0;
+  launch_unit_rows_batch(dD, B.row0s.as<int64_t>(), nb, L.rows, c->stream);
+  CK(cudaMemsetAsync(B.colacc.p, 0, L.acc * sizeof(double), c->stream));
+  launch_colnorm_batch(dD, nb, L.max_s, c->stream);
+  launch_b0_batch(dD, B.pair0s.as<int64_t>(), nb, L.npairs, B.pairs.as<int32_t>(),
+                  B.pair_cnt.as<uint32_t>(), L.max_m, c->stream);
+  launches += (L.rows ? 1 : 0) + (L.max_s > 1 ? 2 : 0) + (L.npairs ? 2 : 1);
+  CK(cudaMemsetAsync(B.maxc_cand.p, 0, rows1 * sizeof(uint32_t), c->stream));
+  CK(cudaMemsetAsync(B.maxc_all.p, 0, rows1 * sizeof(uint32_t), c->stream));
+  CK(cudaMemsetAsync(B.stats.p, 0, 2 * sizeof(unsigned long long), c->stream));
+  CK(cudaMemsetAsync(B.queues.p, 0, 4 * sizeof(unsigned long long), c->stream));
+  for (int v = 0; v < 4; ++v) {
+    if (W.list[v].empty()) continue;
+    launch_allpairs_batch(dD, kVariants[v], B.lists.as<int32_t>() + v * (nb + 1),
+                          B.item0s.as<int64_t>() + v * (nb + 1), (int)W.list[v].size(),
+                          W.item0[v].back(), W.smem[v], B.queues.as<unsigned long long>() + v,
+                          c->stream);
+    ++launches;
+  }
+  launch_merge_batch(dD, B.row0s.as<int64_t>(), nb, L.rows, c->stream);
+  launches += L.rows ? 1 : 0;
+  return launches;
+}
+
+// BATCH_BODY2
+}  // namespace
+
+void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms, int nb,
+               rbg_graph *out, rbg_batch_stats *st) {
+  const auto t_start = std::chrono::steady_clock::now();
+  if (nb < 0 || (nb > 0 && (!asms || !out))) throw Error(RBG_ERR_ARG, "bad batch arguments");
+  for (int i = 0; i < nb; ++i) std::memset(&out[i], 0, sizeof(out[i]));
+  rbg_batch_stats stats;
+  std::memset(&stats, 0, sizeof(stats));
+  stats.n_assemblies = nb;
+  if (nb == 0) {
+    if (st) *st = stats;
+    return;
+  }
+  if (!c->batch) c->batch = std::make_unique<BatchBufs>();
+  BatchBufs &B = *c->batch;
+  const bool use_graph = getenv("RBG_NO_GRAPHS") == nullptr;
+
+  BatchPlan L;
+  plan_batch(defaults, asms, nb, L);
+  const int64_t rows = L.rows, rows1 = std::max<int64_t>(rows, 1);
+  stats.rows = rows;
+  stats.pairs = L.pairs_scored;
+  ensure_buffers(B, L, nb);
+  std::vector<Tables *> tab(nb);
+  for (int b = 0; b < nb; ++b) {
+    const rbg_params *p = L.at(b).p;
+    auto k = std::make_tuple(p->k, p->m, p->pmh_seed, (int)(p->fp_contract != 0), p->win_bits);
+    auto &slot = B.tables[k];
+    if (!slot) slot = make_tables(p, c->stream);
+    tab[b] = slot.get();
+  }
+  std::vector<BatchAsm> D(nb);
+  Lists W;
+  for (int b = 0; b < nb; ++b) {
+    const AsmPlan &a = L.at(b);
+    D[b] = describe(B, a, b);
+    if (a.n > 0) {
+      const int vs = vslot(a.variant);
+      if (W.item0[vs].empty()) W.item0[vs].push_back(0);
+      W.list[vs].push_back(b);
+      W.item0[vs].push_back(W.item0[vs].back() + allpairs_items(a.n, a.P));
+      W.smem[vs] = std::max(W.smem[vs], allpairs_batch_smem(a.variant, a.mpad, a.Su));
+    }
+  }
+  for (int v = 0; v < 4; ++v) stats.items += W.item0[v].empty() ? 0 : W.item0[v].back();
+
+  // pinned staging: global offsets, b0 pairs, descriptors, index arrays
+  const size_t off_bytes = (rows + 1) * sizeof(int64_t);
+  const size_t pair_bytes = (size_t)L.npairs * 2 * sizeof(int32_t);
+  const size_t desc_bytes = (size_t)nb * sizeof(BatchAsm);
+  const size_t idx_bytes = 2 * (nb + 1) * sizeof(int64_t) + 4 * (nb + 1) * (sizeof(int32_t) + sizeof(int64_t));
+  B.hstage.ensure(up256(off_bytes) + up256(pair_bytes) + up256(desc_bytes) + up256(idx_bytes));
+  char *hs = B.hstage.as<char>();
+  int64_t *h_off = (int64_t *)hs;
+  int32_t *h_pairs = (int32_t *)(hs + up256(off_bytes));
+  BatchAsm *h_desc = (BatchAsm *)(hs + up256(off_bytes) + up256(pair_bytes));
+  int64_t *h_row0s = (int64_t *)(hs + up256(off_bytes) + up256(pair_bytes) + up256(desc_bytes));
+  int64_t *h_pair0s = h_row0s + (nb + 1);
+  int32_t *h_lists = (int32_t *)(h_pair0s + (nb + 1));
+  int64_t *h_item0s = (int64_t *)(h_lists + 4 * (nb + 1));
+  for (int b = 0; b < nb; ++b) {
+    const AsmPlan &a = L.at(b);
+    for (int64_t q = 0; q < a.n; ++q) h_off[a.row0 + q] = a.base0 + a.in->offsets[q];
+    if (a.np) std::memcpy(h_pairs + 2 * a.pair0, a.pairs->data(), (size_t)a.np * 2 * sizeof(int32_t));
+    h_row0s[b] = a.row0;
+    h_pair0s[b] = a.pair0;
+  }
+  h_off[rows] = L.bases;
+  h_row0s[nb] = rows;
+  h_pair0s[nb] = L.npairs;
+  std::memcpy(h_desc, D.data(), desc_bytes);
+  for (int v = 0; v < 4; ++v) {
+    std::copy(W.list[v].begin(), W.list[v].end(), h_lists + v * (nb + 1));
+    std::copy(W.item0[v].begin(), W.item0[v].end(), h_item0s + v * (nb + 1));
+  }
+
+  // ── inputs to the device ────────────────────────────────────────────────
+  cudaEvent_t ev0 = c->ev[0], ev1 = c->ev[1], ev2 = c->ev[2], ev3 = c->ev[3], ev4 = c->ev[4];
+  CK(cudaEventRecord(ev0, c->stream));
+  for (int b = 0; b < nb; ++b) {
+    const AsmPlan &a = L.at(b);
+    if (a.nbases)
+      CK(cudaMemcpyAsync(B.ascii.as<char>() + a.base0, a.in->seqcat, (size_t)a.nbases,
+                         cudaMemcpyHostToDevice, c->stream));
+    if (a.n && a.S)
+      CK(cudaMemcpyAsync(B.depth.as<float>() + a.dep0, a.in->depth,
+                         (size_t)a.n * a.S * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  }
+  const size_t abytes = (size_t)((L.bases + 15) / 16) * 16 + 16;
+  CK(cudaMemsetAsync(B.ascii.as<char>() + L.bases, 0, abytes - (size_t)L.bases, c->stream));
+  CK(cudaMemcpyAsync(B.offsets.p, h_off, off_bytes, cudaMemcpyHostToDevice, c->stream));
+  if (pair_bytes) CK(cudaMemcpyAsync(B.pairs.p, h_pairs, pair_bytes, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(B.desc.p, h_desc, desc_bytes, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(B.row0s.p, h_row0s, (nb + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(B.pair0s.p, h_pair0s, (nb + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(B.lists.p, h_lists, 4 * (nb + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(B.item0s.p, h_item0s, 4 * (nb + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaEventRecord(ev1, c->stream));
+
+  // ── segment 1: sketch, depth rows, b0, all-pairs, merge ────────────────
+  const size_t mx_bytes = up256(2 * rows1 * sizeof(uint32_t));
+  B.hout.ensure(mx_bytes + up256(nb * sizeof(float)) + up256((nb + 1) * sizeof(int64_t)));
+  uint32_t *h_maxc = B.hout.as<uint32_t>();
+  float *h_b0 = (float *)(B.hout.as<char>() + mx_bytes);
+  int64_t *h_edge0s = (int64_t *)(B.hout.as<char>() + mx_bytes + up256(nb * sizeof(float)));
+  int launches = 0;
+  captured(c, 0, use_graph, stats.graph_launches, [&] {
+    launches += launch_sketch_groups(c, B, L, tab, nb);
+    launches += launch_graph_stage(c, B, L, W, nb);
+    if (rows) {
+      CK(cudaMemcpyAsync(h_maxc, B.maxc_cand.p, rows * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                         c->stream));
+      CK(cudaMemcpyAsync(h_maxc + rows1, B.maxc_all.p, rows * sizeof(uint32_t),
+                         cudaMemcpyDeviceToHost, c->stream));
+    }
+    CK(cudaMemcpyAsync(h_b0, B.b0.p, nb * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  });
+  CK(cudaEventRecord(ev2, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+
+  // ── host calibration of every assembly ─────────────────────────────────
+  const auto t_cal = std::chrono::steady_clock::now();
+  std::vector<double> cut(nb, 0.0);
+  std::vector<float> b0f(h_b0, h_b0 + nb);
+  auto calibrate = [&](int b) {
+    const AsmPlan &a = L.at(b);
+    std::vector<double> sv_d;
+    std::vector<float> sv_f;
+    sv_table(a.m, a.p->base_on != 0, a.p->base_on ? (double)b0f[b] : 0.0, sv_d, sv_f);
+    const uint32_t *mc = (a.fused ? h_maxc : h_maxc + rows1) + a.row0;
+    cut[b] = calibrate_cutoff(mc, a.n, a.fused, a.m, sv_d, sv_f, a.p->coverage, a.p->seed);
+  };
+  {
+    const int nt = std::max(1, std::min<int>(nb, (int)std::thread::hardware_concurrency()));
+    if (nt <= 1 || nb < 4) {
+      for (int b = 0; b < nb; ++b) calibrate(b);
+    } else {
+      std::vector<std::thread> th;
+      std::atomic<int> next{0};
+      for (int t = 0; t < nt; ++t)
+        th.emplace_back([&] {
+          for (int b; (b = next.fetch_add(1)) < nb;) calibrate(b);
+        });
+      for (auto &t : th) t.join();
+    }
+  }
+  stats.calib_ms = (float)ms_since(t_cal);
+  for (int b = 0; b < nb; ++b) h_desc[b].e.cutoff = cut[b] / 1000.;
+
+  // ── segment 2: neighbour lists, edge counts, batch-wide scan ───────────
+  const BatchAsm *dD = B.desc.as<BatchAsm>();
+  captured(c, 1, use_graph, stats.graph_launches, [&] {
+    CK(cudaMemcpyAsync(B.desc.p, h_desc, desc_bytes, cudaMemcpyHostToDevice, c->stream));
+    launch_emit_batch(dD, B.row0s.as<int64_t>(), nb, rows, L.max_k, B.row_edges.as<int32_t>(),
+                      B.edge0s.as<int64_t>(), c->stream);
+    launches += (rows ? 2 : 0) + 2;
+    CK(cudaMemcpyAsync(h_edge0s, B.edge0s.p, (nb + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost,
+                       c->stream));
+  });
+  CK(cudaEventRecord(ev3, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  std::vector<int64_t> edge0v(h_edge0s, h_edge0s + nb + 1);
+  const int64_t E = edge0v[nb];
+  stats.edges = E;
+
+  // ── segment 3: edges and weights, then the copies back ─────────────────
+  const size_t E1 = (size_t)std::max<int64_t>(E, 1);
+  B.e_from.ensure(E1 * 4); B.e_to.ensure(E1 * 4); B.e_scomp.ensure(E1 * 4); B.e_score.ensure(E1 * 4);
+  for (int b = 0; b < nb; ++b) {
+    EmitArgs &e = h_desc[b].e;
+    e.from = B.e_from.as<uint32_t>(); e.to = B.e_to.as<uint32_t>(); e.scomp = B.e_scomp.as<float>();
+    WeightArgs &w = h_desc[b].w;
+    w.from = e.from; w.to = e.to; w.scomp = e.scomp; w.score = B.e_score.as<float>();
+    w.n_edges = edge0v[b + 1] - edge0v[b];
+  }
+  const size_t eb = up256(E1 * 4);
+  B.hedge.ensure(4 * eb);
+  char *hb = B.hedge.as<char>();
+  uint32_t *h_from = (uint32_t *)hb;
+  uint32_t *h_to = (uint32_t *)(hb + eb);
+  float *h_scomp = (float *)(hb + 2 * eb);
+  float *h_score = (float *)(hb + 3 * eb);
+  captured(c, 2, use_graph, stats.graph_launches, [&] {
+    CK(cudaMemcpyAsync(B.desc.p, h_desc, desc_bytes, cudaMemcpyHostToDevice, c->stream));
+    launch_write_edges_batch(dD, B.row0s.as<int64_t>(), nb, rows, c->stream);
+    launch_edge_weights_batch(dD, B.edge0s.as<int64_t>(), nb, E, c->stream);
+    launches += (rows ? 1 : 0) + (E ? 1 : 0);
+    if (E) {
+      CK(cudaMemcpyAsync(h_from, B.e_from.p, E * 4, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaMemcpyAsync(h_to, B.e_to.p, E * 4, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaMemcpyAsync(h_scomp, B.e_scomp.p, E * 4, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaMemcpyAsync(h_score, B.e_score.p, E * 4, cudaMemcpyDeviceToHost, c->stream));
+    }
+  });
+  CK(cudaEventRecord(ev4, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+
+  // ── results in the caller's order ──────────────────────────────────────
+  for (int b = 0; b < nb; ++b) {
+    const AsmPlan &a = L.at(b);
+    rbg_graph &g = out[a.orig];
+    const int64_t e0 = edge0v[b], ne = edge0v[b + 1] - e0;
+    g.n_edges = ne;
+    g.b0 = a.p->base_on ? (double)b0f[b] : 0.0;
+    g.sim_cutoff = cut[b];
+    g.path = a.fused ? 2 : 1;
+    const size_t bytes = (size_t)std::max<int64_t>(ne, 1) * 4;
+    g.from = (uint32_t *)malloc(bytes);
+    g.to = (uint32_t *)malloc(bytes);
+    g.scomp = (float *)malloc(bytes);
+    g.score = (float *)malloc(bytes);
+    if (!g.from || !g.to || !g.scomp || !g.score) {
+      for (int q = 0; q < nb; ++q) rbg_free_graph(&out[q]);
+      throw Error(RBG_ERR_NOMEM, "host allocation of the edge arrays failed");
+    }
+    if (ne) {
+      std::memcpy(g.from, h_from + e0, ne * 4);
+      std::memcpy(g.to, h_to + e0, ne * 4);
+      std::memcpy(g.scomp, h_scomp + e0, ne * 4);
+      std::memcpy(g.score, h_score + e0, ne * 4);
+    }
+  }
+  float t01 = 0, t12 = 0, t34 = 0;
+  cudaEventElapsedTime(&t01, ev0, ev1);
+  cudaEventElapsedTime(&t12, ev1, ev2);
+  cudaEventElapsedTime(&t34, ev3, ev4);
+  stats.stage_ms = t01;
+  stats.graph_ms = t12;
+  stats.emit_ms = t34;
+  stats.kernel_launches = launches;
+  stats.total_ms = (float)ms_since(t_start);
+  if (st) *st = stats;
+}
+
+}  // namespace rbg
+
+extern "C" int rbg_bin_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
+                             int32_t n_asm, rbg_graph *out, rbg_batch_stats *stats) {
+  return rbg::guarded(c, [&] { rbg::run_batch(c, defaults, asms, n_asm, out, stats); });
+}

@@ -16,7 +16,7 @@
 #include <string>
 #include <vector>
 
-#include "rbg_internal.h"
+#include "engine_internal.h"
 
 namespace rbg {
 void launch_fold16(const uint32_t *in, int64_t n, uint16_t *out, cudaStream_t s);
@@ -31,184 +31,14 @@ namespace {
 
 using namespace rbg;
 
-struct Error : std::runtime_error {
-  int code;
-  Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
-};
-
-#define CK(x)                                                                     \
-  do {                                                                            \
-    cudaError_t e_ = (x);                                                         \
-    if (e_ != cudaSuccess)                                                        \
-      throw Error(e_ == cudaErrorMemoryAllocation ? RBG_ERR_NOMEM : RBG_ERR_CUDA, \
-                  std::string(#x) + ": " + cudaGetErrorString(e_));               \
-  } while (0)
-
-// A growable device allocation.
-struct DBuf {
-  void *p = nullptr;
-  size_t cap = 0;
-  template <typename T> T *as() const { return (T *)p; }
-  void ensure(size_t bytes) {
-    if (bytes <= cap) return;
-    if (p) cudaFree(p);
-    p = nullptr;
-    cap = 0;
-    const size_t want = std::max<size_t>(bytes, 256);
-    CK(cudaMalloc(&p, want));
-    cap = want;
-  }
-  void release() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    cap = 0;
-  }
-};
-
-// Pinned host staging buffer.
-struct HBuf {
-  void *p = nullptr;
-  size_t cap = 0;
-  void ensure(size_t bytes) {
-    if (bytes <= cap) return;
-    if (p) cudaFreeHost(p);
-    p = nullptr;
-    cap = 0;
-    CK(cudaMallocHost(&p, std::max<size_t>(bytes, 256)));
-    cap = std::max<size_t>(bytes, 256);
-  }
-  void release() {
-    if (p) cudaFreeHost(p);
-    p = nullptr;
-    cap = 0;
-  }
-};
-
-inline int mpad_of(int m) { return (m + 15) & ~15; }
-
-// calib_converge (src/impl/rb_graph.cpp:390-415): walk the cutoff p (x1000)
-// down in rand()-sized steps until the connected fraction reaches coverage.
-// The count of maxsim >= cutoff comes from a sorted copy (same counts, same
-// rand() calls).
-size_t converge_cutoff(const std::vector<double> &maxsim, double coverage) {
-  const size_t n = maxsim.size();
-  std::vector<double> sorted(maxsim);
-  std::sort(sorted.begin(), sorted.end());
-  size_t p = 999, pp = 1000;
-  double cov = 0, pcov = 0;
-  for (; p > 50;) {
-    const double cutoff = (double)p / 1000.;
-    const size_t on = n - (size_t)(std::lower_bound(sorted.begin(), sorted.end(), cutoff) - sorted.begin());
-    cov = (double)on / (double)n;
-    if (cov >= coverage) {
-      if (cov - coverage > coverage - pcov) { p = pp; cov = pcov; }
-      break;
-    }
-    pp = p;
-    pcov = cov;
-    if (p > 990) p -= rand() % 3 + 1;
-    else if (p > 900) p -= rand() % 3 + 3;
-    else p -= rand() % 3 + 9;
-  }
-  return p;
-}
-
-// random_unique (src/rabbitbin.h:330-341), a partial Fisher-Yates driven by
-// rand(): the first `count` entries it leaves in iota(n), without
-// materialising the n-entry vector (positions touched are tracked lazily).
-// `val`/`stamp` are scratch of n entries reused across calls (stamp marks the
-// positions this call has written).
-std::vector<size_t> rand_prefix_of_iota(size_t n, size_t count, std::vector<size_t> &val,
-                                        std::vector<uint32_t> &stamp, uint32_t cur) {
-  auto at = [&](size_t i) { return stamp[i] == cur ? val[i] : i; };
-  auto put = [&](size_t i, size_t v) { val[i] = v; stamp[i] = cur; };
-  std::vector<size_t> out(count);
-  size_t left = n;
-  for (size_t b = 0; b < count; ++b, --left) {
-    const size_t r = b + (size_t)rand() % left;
-    const size_t vb = at(b), vr = at(r);
-    put(r, vb);
-    put(b, vr);
-    out[b] = vr;
-  }
-  return out;
-}
-
-struct Tables {
-  std::shared_ptr<const PmhTables> t;
-  int win_bits = 16;
-  DBuf U, codeA, W32, rank;
-  DBuf dict_vals, dict_codes, dict_n;   // per-column sorted dictionaries
-  bool dict_ready = false;
-};
-
-}  // namespace
-
-struct rbg_ctx {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  std::string err;
-  std::mutex mu;
-  // staged inputs
-  int64_t n = 0, nbases = 0;
-  int S = 0;
-  std::vector<int64_t> h_offsets;
-  DBuf ascii, offsets, depth;
-  // sketch state
-  DBuf packed, nmask, elem_idx, elem_winv, elem_cnt, codesA, codesB, winners32;
-  // graph state
-  DBuf unit, unit16, anynz, colnorm, svbits, topk, topk_cnt, maxc_cand, maxc_all, stats;
-  DBuf pairs, pair_out, nbr, nbr_sv, nbr_cnt, row_edges, cand_buf, cand_cnt;
-  DBuf e_from, e_to, e_scomp, e_score, badflag, tmp, colacc;
-  HBuf pin;
-  int64_t n_edges = 0;
-  double b0 = 0.0, sim_cutoff = 0.0;
-  int path = 0;
-  bool graph_ready = false;
-  // tables (one configuration cached)
-  std::unique_ptr<Tables> tables;
-  int tab_k = -1, tab_m = -1, tab_contract = -1, tab_bits = -1;
-  uint64_t tab_seed = 0;
-  cudaEvent_t ev[12];
-  cudaStream_t aux = nullptr;            // depth preparation, overlapped with the sketch
-  cudaEvent_t ev_in = nullptr, ev_aux = nullptr, ev_a0 = nullptr, ev_a1 = nullptr;
-  bool prep_done = false;
-  int launches = 0;
-};
-
-namespace {
-
-void validate(const rbg_params *p) {
-  if (!p) throw Error(RBG_ERR_ARG, "null params");
-  if (p->k < 1 || p->k > 4) throw Error(RBG_ERR_UNSUPPORTED, "k must be in 1..4");
-  if (p->m < 2 || p->m > kMaxM) throw Error(RBG_ERR_ARG, "m must be in 2..4096");
-  if (p->win_bits != 16 && p->win_bits != 32) throw Error(RBG_ERR_ARG, "win_bits must be 16 or 32");
-  if (p->gc_norm != 0 && p->gc_norm != 1) throw Error(RBG_ERR_UNSUPPORTED, "gc_norm must be 0 or 1");
-  if (p->max_edges < 1 || p->max_edges > 448) throw Error(RBG_ERR_UNSUPPORTED, "max_edges must be in 1..448");
-  if (!(p->coverage > 0.0 && p->coverage < 1.0)) throw Error(RBG_ERR_ARG, "coverage must be in (0,1)");
-}
+void validate(const rbg_params *p) { validate_params(p); }
 
 Tables &tables_for(rbg_ctx *c, const rbg_params *p) {
   if (c->tables && c->tab_k == p->k && c->tab_m == p->m && c->tab_seed == p->pmh_seed &&
       c->tab_contract == (p->fp_contract != 0) && c->tab_bits == p->win_bits)
     return *c->tables;
-  auto T = std::make_unique<Tables>();
-  T->t = pmh_tables(p->k, p->m, p->pmh_seed, p->fp_contract != 0);
-  T->win_bits = p->win_bits;
-  const PmhTables &t = *T->t;
-  const size_t EM = (size_t)t.n_elems * t.m;
-  T->U.ensure(EM * sizeof(double));
-  T->codeA.ensure(EM);
-  T->W32.ensure(EM * sizeof(uint32_t));
-  std::vector<int16_t> rk(t.rank_of_code.begin(), t.rank_of_code.end());
-  T->rank.ensure(rk.size() * sizeof(int16_t));
-  CK(cudaMemcpyAsync(T->U.p, t.U.data(), EM * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  CK(cudaMemcpyAsync(T->codeA.p, p->win_bits == 16 ? t.code16.data() : t.code32.data(), EM,
-                     cudaMemcpyHostToDevice, c->stream));
-  CK(cudaMemcpyAsync(T->W32.p, t.W32.data(), EM * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
-  CK(cudaMemcpyAsync(T->rank.p, rk.data(), rk.size() * sizeof(int16_t), cudaMemcpyHostToDevice, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  c->tables = std::move(T);
+  if (c->tables) c->tables->release();
+  c->tables = make_tables(p, c->stream);
   c->tab_k = p->k; c->tab_m = p->m; c->tab_seed = p->pmh_seed;
   c->tab_contract = p->fp_contract != 0; c->tab_bits = p->win_bits;
   return *c->tables;
@@ -239,12 +69,6 @@ void stage(rbg_ctx *c, const char *seqcat, const int64_t *offsets, int64_t n,
   if (S > 0 && n > 0)
     CK(cudaMemcpyAsync(c->depth.p, depth, (size_t)n * S * sizeof(float), cudaMemcpyHostToDevice, c->stream));
 }
-
-// Row stride (halves) of the FP16 unit rows: 16, 32 or 64, the k extent of the
-// tensor-core prefilter variant that reads them.
-int unit16_stride(int S) { return S <= 16 ? 16 : (S <= 32 ? 32 : 64); }
-
-bool need_colnorm(const rbg_params *p, int S) { return p->depth_sim >= 1 && S > 1 && p->wjac_norm; }
 
 // Unit rank rows, anynz and column norms on the auxiliary stream: they depend
 // only on the coverage table, so they overlap the sketch kernels.
@@ -333,20 +157,11 @@ void run_sketch(rbg_ctx *c, const rbg_params *p, bool want_winners) {
 // b0: median raw match fraction over 30000 mt19937_64 draws
 // (estimate_pmh_baseline, src/rabbitbin.cpp:1340-1369).
 double estimate_b0(rbg_ctx *c, int64_t n, int m, const std::function<void(const int64_t *, int, uint32_t *)> &count) {
-  if (n < 4) return 0.0;
-  const size_t NP = 30000;
-  std::mt19937_64 rng(0x9E3779B97F4A7C15ULL);
-  std::uniform_int_distribution<size_t> uni(0, (size_t)n - 1);
-  std::vector<int64_t> pr;
-  pr.reserve(2 * NP);
-  for (size_t s = 0; s < NP; ++s) {
-    const size_t i = uni(rng), j = uni(rng);
-    if (i == j) continue;
-    pr.push_back((int64_t)i);
-    pr.push_back((int64_t)j);
-  }
-  const int np = (int)(pr.size() / 2);
+  (void)c;
+  const auto prs = b0_pairs(n);
+  const int np = (int)(prs->size() / 2);
   if (np == 0) return 0.0;
+  std::vector<int64_t> pr(prs->begin(), prs->end());
   std::vector<uint32_t> cnt(np);
   count(pr.data(), np, cnt.data());
   const double inv_m = 1.0 / (double)m;
@@ -447,47 +262,7 @@ void run_graph(rbg_ctx *c, const rbg_params *p) {
   CK(cudaMemcpyAsync(maxc.data(), fused ? c->maxc_cand.p : c->maxc_all.p, n * sizeof(uint32_t),
                      cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  srand(p->seed);
-  double simCutoff;
-  if (!fused) {
-    // random_unique over all n contigs: only its rand() calls matter here,
-    // the maxima are counted, not ordered
-    for (int64_t left = n; left > 0; --left) (void)(rand() % left);
-    std::vector<double> maxsim(n);
-    for (int64_t i = 0; i < n; ++i) maxsim[i] = sv_d[maxc[i]];
-    simCutoff = (double)converge_cutoff(maxsim, p->coverage);
-  } else {
-    const size_t NR = 10, SAMP = 2500;
-    std::vector<std::vector<size_t>> idxs(NR);
-    std::vector<size_t> val((size_t)n);
-    std::vector<uint32_t> stamp((size_t)n, 0);
-    for (size_t r = 0; r < NR; ++r)
-      idxs[r] = rand_prefix_of_iota((size_t)n, SAMP, val, stamp, (uint32_t)(r + 1));
-    std::vector<int8_t> sround(n, -1);
-    std::vector<size_t> slocal(n, 0);
-    for (int r = (int)NR - 1; r >= 0; --r)
-      for (size_t li = 0; li < SAMP; ++li) {
-        sround[idxs[r][li]] = (int8_t)r;
-        slocal[idxs[r][li]] = li;
-      }
-    std::vector<std::vector<float>> ms(NR, std::vector<float>(SAMP, 0.f));
-    for (int64_t ci = 0; ci < n; ++ci)
-      if (sround[ci] >= 0) {
-        const float v = sv_f[maxc[ci]];
-        float &slot = ms[sround[ci]][slocal[ci]];
-        if (v > slot) slot = v;
-      }
-    double sum_p = 0;
-    for (size_t r = 0; r < NR; ++r) {
-      std::vector<double> sub(SAMP);
-      for (size_t li = 0; li < SAMP; ++li) sub[li] = (double)ms[r][li];
-      double mp = (double)converge_cutoff(sub, p->coverage);
-      if (mp < 51.0) mp = 50.0;
-      sum_p += mp;
-      if (r == 1 && sum_p / 2 < 51.0) { sum_p = 500.0; break; }
-    }
-    simCutoff = sum_p / (double)NR;
-  }
+  const double simCutoff = calibrate_cutoff(maxc.data(), n, fused, m, sv_d, sv_f, p->coverage, p->seed);
   c->sim_cutoff = simCutoff;
   CK(cudaEventRecord(c->ev[7], c->stream));
 
@@ -628,27 +403,6 @@ void codes_from_winners(rbg_ctx *c, const rbg_params *p, const uint32_t *w32, in
   if (bad) throw Error(RBG_ERR_ARG, "winner rows do not come from this sketch configuration (k, m, seed)");
 }
 
-template <typename F>
-int guarded(rbg_ctx *c, F &&f) {
-  if (!c) return RBG_ERR_ARG;
-  std::lock_guard<std::mutex> lk(c->mu);
-  try {
-    CK(cudaSetDevice(c->device));
-    f();
-    c->err.clear();
-    return RBG_OK;
-  } catch (const Error &e) {
-    c->err = e.what();
-    return e.code;
-  } catch (const std::bad_alloc &) {
-    c->err = "host allocation failed";
-    return RBG_ERR_NOMEM;
-  } catch (const std::exception &e) {
-    c->err = e.what();
-    return RBG_ERR_CUDA;
-  }
-}
-
 }  // namespace
 
 extern "C" {
@@ -721,11 +475,9 @@ int rbg_destroy(rbg_ctx *c) {
                   &c->nbr_cnt, &c->row_edges, &c->e_from, &c->e_to, &c->e_scomp, &c->e_score,
                   &c->badflag, &c->tmp, &c->cand_buf, &c->cand_cnt, &c->colacc, &c->unit16};
   for (DBuf *b : bufs) b->release();
-  if (c->tables) {
-    c->tables->U.release(); c->tables->codeA.release(); c->tables->W32.release();
-    c->tables->rank.release(); c->tables->dict_vals.release(); c->tables->dict_codes.release();
-    c->tables->dict_n.release();
-  }
+  if (c->tables) c->tables->release();
+  release_batch_graphs(c);
+  if (c->batch) c->batch->release();
   c->pin.release();
   for (auto &e : c->ev) cudaEventDestroy(e);
   cudaStreamSynchronize(c->aux);

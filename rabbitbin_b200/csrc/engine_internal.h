@@ -1,0 +1,226 @@
+// Host-side internals shared by the single-assembly engine (engine.cpp) and
+// the batch engine (batch.cpp): errors, device and pinned buffers, the
+// per-configuration table cache, the context, and the host steps of the
+// calibration.
+#pragma once
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "rbg_internal.h"
+
+struct rbg_ctx;
+
+namespace rbg {
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+#define CK(x)                                                                     \
+  do {                                                                            \
+    cudaError_t e_ = (x);                                                         \
+    if (e_ != cudaSuccess)                                                        \
+      throw ::rbg::Error(e_ == cudaErrorMemoryAllocation ? RBG_ERR_NOMEM : RBG_ERR_CUDA, \
+                         std::string(#x) + ": " + cudaGetErrorString(e_));        \
+  } while (0)
+
+// A growable device allocation.
+struct DBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  template <typename T> T *as() const { return (T *)p; }
+  void ensure(size_t bytes) {
+    if (bytes <= cap) return;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    const size_t want = bytes < 256 ? 256 : bytes;
+    CK(cudaMalloc(&p, want));
+    cap = want;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+// Pinned host staging buffer.
+struct HBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  template <typename T> T *as() const { return (T *)p; }
+  void ensure(size_t bytes) {
+    if (bytes <= cap) return;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    const size_t want = bytes < 256 ? 256 : bytes;
+    CK(cudaMallocHost(&p, want));
+    cap = want;
+  }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+inline int mpad_of(int m) { return (m + 15) & ~15; }
+
+// Row stride (halves) of the FP16 unit rows: 16, 32 or 64, the k extent of the
+// tensor-core prefilter variant that reads them.
+inline int unit16_stride(int S) { return S <= 16 ? 16 : (S <= 32 ? 32 : 64); }
+
+inline bool need_colnorm(const rbg_params *p, int S) {
+  return p->depth_sim >= 1 && S > 1 && p->wjac_norm;
+}
+
+// Device copy of one sketch configuration's tables.
+struct Tables {
+  std::shared_ptr<const PmhTables> t;
+  int win_bits = 16;
+  DBuf U, codeA, W32, rank;
+  DBuf dict_vals, dict_codes, dict_n;   // per-column sorted dictionaries
+  bool dict_ready = false;
+  void release() {
+    U.release(); codeA.release(); W32.release(); rank.release();
+    dict_vals.release(); dict_codes.release(); dict_n.release();
+  }
+};
+
+// Uploads (k, m, seed, contract, win_bits) tables to the device on `s`
+// (synchronised before returning).
+std::unique_ptr<Tables> make_tables(const rbg_params *p, cudaStream_t s);
+
+// Buffers of the batch engine (many assemblies per launch).
+struct BatchBufs {
+  DBuf ascii, offsets, depth, packed, nmask, winv, ecnt, codesA, codesB;
+  DBuf unit, unit16, anynz, colnorm, colacc, svbits, topk, topk_cnt, maxc_cand, maxc_all, stats;
+  DBuf gbuf, gcnt, pairs, pair_cnt, b0;
+  DBuf nbr, nbr_sv, nbr_cnt, row_edges, edge0s;
+  DBuf e_from, e_to, e_scomp, e_score;
+  DBuf desc, row0s, lists, item0s, queues, pair0s;
+  HBuf hstage, hout, hedge;
+  std::map<std::tuple<int, int, uint64_t, int, int>, std::unique_ptr<Tables>> tables;
+  void release() {
+    DBuf *all[] = {&ascii, &offsets, &depth, &packed, &nmask, &winv, &ecnt, &codesA, &codesB,
+                   &unit, &unit16, &anynz, &colnorm, &colacc, &svbits, &topk, &topk_cnt,
+                   &maxc_cand, &maxc_all, &stats, &gbuf, &gcnt, &pairs, &pair_cnt, &b0, &nbr,
+                   &nbr_sv, &nbr_cnt, &row_edges, &edge0s, &e_from, &e_to, &e_scomp, &e_score,
+                   &desc, &row0s, &lists, &item0s, &queues, &pair0s};
+    for (DBuf *b : all) b->release();
+    hstage.release();
+    hout.release();
+    hedge.release();
+    for (auto &kv : tables) kv.second->release();
+    tables.clear();
+  }
+};
+
+// glibc's rand() sequence of one seed (srand(seed); rand(); ...) on private
+// state, so concurrent calibrations do not share the process-wide generator.
+struct CRand {
+  random_data rd;
+  char state[128];
+  explicit CRand(unsigned seed) {
+    std::memset(&rd, 0, sizeof(rd));
+    std::memset(state, 0, sizeof(state));
+    initstate_r(seed, state, sizeof(state), &rd);
+  }
+  int operator()() {
+    int32_t r = 0;
+    random_r(&rd, &r);
+    return (int)r;
+  }
+};
+
+// The calibrated similarity cutoff (x1000) of one assembly from its per-row
+// maximum register-match counts (maxc over candidates for the fused path,
+// over all j != i for the small path) and its similarity tables:
+// calibrate_sim_cutoff (src/impl/rb_graph.cpp:1362-1384) for the small path,
+// the sampling rounds of gen_fused_calib_graph (:505-522, per-round converge
+// and mean) for the fused path.
+double calibrate_cutoff(const uint32_t *maxc, int64_t n, bool fused, int m,
+                        const std::vector<double> &sv_d, const std::vector<float> &sv_f,
+                        double coverage, unsigned seed);
+
+// b0 sampling pairs of an assembly of n contigs (estimate_pmh_baseline,
+// src/rabbitbin.cpp:1340-1369: mt19937_64 draws, i == j skipped), as local ids.
+std::shared_ptr<const std::vector<int32_t>> b0_pairs(int64_t n);
+
+void validate_params(const rbg_params *p);
+
+// Frees the CUDA graphs the batch engine keeps for a context.
+void release_batch_graphs(rbg_ctx *c);
+
+}  // namespace rbg
+
+struct rbg_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  std::mutex mu;
+  // staged inputs
+  int64_t n = 0, nbases = 0;
+  int S = 0;
+  std::vector<int64_t> h_offsets;
+  rbg::DBuf ascii, offsets, depth;
+  // sketch state
+  rbg::DBuf packed, nmask, elem_idx, elem_winv, elem_cnt, codesA, codesB, winners32;
+  // graph state
+  rbg::DBuf unit, unit16, anynz, colnorm, svbits, topk, topk_cnt, maxc_cand, maxc_all, stats;
+  rbg::DBuf pairs, pair_out, nbr, nbr_sv, nbr_cnt, row_edges, cand_buf, cand_cnt;
+  rbg::DBuf e_from, e_to, e_scomp, e_score, badflag, tmp, colacc;
+  rbg::HBuf pin;
+  int64_t n_edges = 0;
+  double b0 = 0.0, sim_cutoff = 0.0;
+  int path = 0;
+  bool graph_ready = false;
+  // tables (one configuration cached)
+  std::unique_ptr<rbg::Tables> tables;
+  int tab_k = -1, tab_m = -1, tab_contract = -1, tab_bits = -1;
+  uint64_t tab_seed = 0;
+  cudaEvent_t ev[12];
+  cudaStream_t aux = nullptr;            // depth preparation, overlapped with the sketch
+  cudaEvent_t ev_in = nullptr, ev_aux = nullptr, ev_a0 = nullptr, ev_a1 = nullptr;
+  bool prep_done = false;
+  int launches = 0;
+  // batch engine
+  std::unique_ptr<rbg::BatchBufs> batch;
+};
+
+namespace rbg {
+
+// Runs f under the context's lock with the context's device current and maps
+// exceptions onto status codes and the context's error string.
+template <typename F>
+int guarded(rbg_ctx *c, F &&f) {
+  if (!c) return RBG_ERR_ARG;
+  std::lock_guard<std::mutex> lk(c->mu);
+  try {
+    CK(cudaSetDevice(c->device));
+    f();
+    c->err.clear();
+    return RBG_OK;
+  } catch (const Error &e) {
+    c->err = e.what();
+    return e.code;
+  } catch (const std::bad_alloc &) {
+    c->err = "host allocation failed";
+    return RBG_ERR_NOMEM;
+  } catch (const std::exception &e) {
+    c->err = e.what();
+    return RBG_ERR_CUDA;
+  }
+}
+
+}  // namespace rbg

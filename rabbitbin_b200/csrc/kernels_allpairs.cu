@@ -1,24 +1,25 @@
 // All-pairs pass: per row top-K of (similarity, id) keys plus the row maxima
 // the calibration reads, over full rows (every ordered pair i != j).
 //
-// Layout: lane = row, a warp owns 32 rows and streams every column j in
-// order; column data (unit rank rows, 8-bit register codes) are read with
-// warp-uniform 128-bit loads that the SM's L1 serves to all warps walking the
-// same columns.  Nothing is shared across warps, so there is no CTA barrier.
-// Each row keeps its candidate keys in a private global buffer (L2-resident)
-// with the admission threshold and fill count in shared memory; when a buffer
-// fills, the owning warp selects the K best in registers (radix search of the
-// K-th largest key) and raises the threshold to it.
+// A work item is a block of 32 rows (lane = row) against kWarps column slices,
+// one warp per slice; the plain launch maps items to the grid, the batch form
+// runs a persistent kernel that pulls (assembly, row block, slice group)
+// items from a device counter.  Each row keeps its candidate keys in a
+// private global buffer per slice (L2-resident) with the admission threshold
+// and fill count in shared memory; when a buffer fills, the owning warp
+// selects the K best in registers (radix search of the K-th largest key) and
+// raises the threshold to it.  A merge pass then keeps the K best over the
+// slices.
 //
 // Two regimes:
 //  * dense (no abundance prune: the N <= 25000 path, S <= 2, RABBIT_NO_ABDFIRST):
 //    every pair's register-match count, 4 columns per step over 8-bit code
-//    words (row words from shared memory, column words uniform loads);
-//  * sparse (the abundance-first prune of the fused path): a single FP32 FMA
-//    chain decides the prune for almost every pair under a rigorous error bound
-//    against the AVX-512 order of unit_dot_f; pairs inside the bound's band
-//    evaluate that order exactly.  Survivors queue per warp and are counted 32
-//    at a time, lane = survivor.
+//    words (row words from shared memory, column words staged by cp.async);
+//  * sparse (the abundance-first prune of the fused path): tensor-core FP16
+//    products of the unit rows prune almost every pair under a rigorous error
+//    bound; the few left are decided by an FP32 chain with its own band and
+//    then the AVX-512 order of unit_dot_f exactly.  Survivors queue per warp
+//    and are counted by the whole warp, one survivor at a time.
 //
 // Compiled with -fmad=false; __fmaf_rn marks every fused operation.
 #include <algorithm>
@@ -33,8 +34,6 @@ namespace {
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int kWarps = 4;         // warps per CTA (independent)
 constexpr int kCapW = 16;         // candidate buffer <= 32 * kCapW keys per row
-constexpr int kQ = 64;            // survivor queue entries per warp
-constexpr int kTC = 32;           // sparse: columns per staged tile
 
 __device__ __forceinline__ uint32_t eq_bytes(uint32_t a, uint32_t b) {
   const uint32_t x = a ^ b;
@@ -136,41 +135,6 @@ __device__ __forceinline__ void compact_full_rows(Warp &w, int limit) {
   }
 }
 
-// Register-match counts of up to 32 queued survivors (lane = survivor); the
-// row codes and column codes both come through L1/L2.
-__device__ __forceinline__ void count_batch(const GraphArgs &g, Warp &w, const int *q, int nq,
-                                            int64_t row0) {
-  const int lane = threadIdx.x & 31;
-  const bool act = lane < nq;
-  const unsigned e = act ? (unsigned)q[lane] : 0u;
-  const int r = (int)(e >> 27);
-  const int64_t j = e & 0x07FFFFFFu;
-  if (act) {
-    const uint4 *ra = (const uint4 *)(g.codesA + (row0 + r) * g.mpad);
-    const uint4 *cb = (const uint4 *)(g.codesB + j * g.mpad);
-    const int m4 = g.mpad >> 4;
-    uint32_t cnt = 0;
-    for (int w0 = 0; w0 < m4; w0 += 63) {
-      const int w1 = (w0 + 63 < m4) ? w0 + 63 : m4;
-      uint32_t acc = 0;
-      for (int t = w0; t < w1; ++t) {
-        const uint4 a = __ldg(ra + t), b = __ldg(cb + t);
-        acc += eq_bytes(a.x, b.x) + eq_bytes(a.y, b.y) + eq_bytes(a.z, b.z) +
-               eq_bytes(a.w, b.w);
-      }
-      cnt += byte_sum(acc);
-    }
-    atomicMax(&w.mxc[r], cnt);
-    const uint64_t key = ((uint64_t)__ldg(g.sv_bits + cnt) << 32) | (uint64_t)(~(uint32_t)j);
-    if (key > w.thr[r]) {
-      const int p = atomicAdd(&w.cnt[r], 1);
-      w.gbuf[(size_t)r * w.cap + p] = key;
-    }
-  }
-  __syncwarp();
-  compact_full_rows(w, w.cap - 32);
-}
-
 // Register-match counts of up to 32 queued survivors, the warp working on one
 // survivor at a time: row codes from shared memory (sA, [32][mpad]) and column
 // codes as coalesced 16-byte loads, four survivors in flight.  Lane p ends
@@ -221,182 +185,101 @@ __device__ __forceinline__ void count_batch_coop(const GraphArgs &g, Warp &w, co
   compact_full_rows(w, w.cap - 32);
 }
 
-template <int SMAX, bool SPARSE>
-__global__ void __launch_bounds__(kWarps * 32)
-k_allpairs(GraphArgs g, uint64_t *gbuf, int32_t *gcnt, int cap, int P, float lo, float hi) {
-  extern __shared__ __align__(16) unsigned char smem[];
+// Dense regime: one work item = 32 rows (row block bx) x the column slices
+// kWarps*by .. kWarps*by+3, one warp per slice.
+__device__ __forceinline__ void dense_item(const GraphArgs &g, uint64_t *gbuf, int32_t *gcnt,
+                                           int cap, int P, int64_t bx, int by,
+                                           unsigned char *smem) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t n = g.n;
-  const int64_t row0 = (int64_t)blockIdx.x * 32;
+  const int64_t row0 = bx * 32;
   const int64_t row = row0 + lane;
   const bool vrow = row < n;
-  const int S = g.S, Su = g.Su;
   const int mw = g.mpad >> 2;
   const int mwq = ((mw + 27) & ~31) + 4;           // = 4 mod 32 words: conflict-free LDS.128
-  const int slice = blockIdx.y * kWarps + warp;     // column slice of this warp
+  const int slice = by * kWarps + warp;              // column slice of this warp
   const int64_t jb = n * slice / P, je = n * (slice + 1) / P;
 
-  // shared: per-warp state, then (dense) the 32 row-code rows of the block
+  // shared: per-warp state, then the 32 row-code rows of the block
   unsigned char *ws = smem + (size_t)warp * 1024;
   uint64_t *thr = (uint64_t *)ws;                  // [32]
   int *cnt = (int *)(thr + 32);                    // [32]
   uint32_t *mxc = (uint32_t *)(cnt + 32);          // [32]
-  int *q = (int *)(mxc + 32);                      // [kQ]
-  uint32_t *sA = (uint32_t *)(smem + (size_t)kWarps * 1024);   // dense: [32][mwq]
+  uint32_t *sA = (uint32_t *)(smem + (size_t)kWarps * 1024);   // [32][mwq]
 
   thr[lane] = 0;
   cnt[lane] = 0;
   mxc[lane] = 0;
-  const size_t bufrow = ((size_t)blockIdx.x * P + slice) * 32;  // first buffer row of the warp
+  const size_t bufrow = ((size_t)bx * P + slice) * 32;  // first buffer row of the warp
   Warp w{gbuf + bufrow * cap, cnt, thr, mxc, cap, g.K};
   const uint8_t nz_row = vrow ? g.anynz[row] : 0;
   unsigned n_pref = 0, n_cmp = 0;
   uint32_t mx_a = 0, mx_c = 0;
 
-  if (!SPARSE) {
-    for (int i = threadIdx.x; i < 32 * (mw >> 2); i += blockDim.x) {
-      const int r = i / (mw >> 2), t = i - r * (mw >> 2);
-      uint4 v = make_uint4(0, 0, 0, 0);
-      if (row0 + r < n) v = __ldg((const uint4 *)(g.codesA + (row0 + r) * g.mpad) + t);
-      *(uint4 *)(sA + r * mwq + 4 * t) = v;
+  for (int i = threadIdx.x; i < 32 * (mw >> 2); i += blockDim.x) {
+    const int r = i / (mw >> 2), t = i - r * (mw >> 2);
+    uint4 v = make_uint4(0, 0, 0, 0);
+    if (row0 + r < n) v = __ldg((const uint4 *)(g.codesA + (row0 + r) * g.mpad) + t);
+    *(uint4 *)(sA + r * mwq + 4 * t) = v;
+  }
+  __syncthreads();
+  const uint32_t *ra = sA + lane * mwq;
+  const int m4 = mw >> 2;
+  // per-warp ring: 2 stages x 4 columns of B codes
+  uint4 *ring = (uint4 *)(smem + (size_t)kWarps * 1024 + 32 * (size_t)mwq * 4) +
+                (size_t)warp * 2 * 4 * m4;
+  auto stage_cols = [&](int st, int64_t j0) {
+    uint4 *dst = ring + (size_t)st * 4 * m4;
+    for (int i = lane; i < 4 * m4; i += 32) {
+      const int u = i / m4, t = i - u * m4;
+      const int64_t j = j0 + u < je ? j0 + u : j0;
+      cp16(dst + i, (const uint4 *)(g.codesB + j * g.mpad) + t);
     }
-    __syncthreads();
-    const uint32_t *ra = sA + lane * mwq;
-    const int m4 = mw >> 2;
-    // per-warp ring: 2 stages x 4 columns of B codes
-    uint4 *ring = (uint4 *)(smem + (size_t)kWarps * 1024 + 32 * (size_t)mwq * 4) +
-                  (size_t)warp * 2 * 4 * m4;
-    auto stage_cols = [&](int st, int64_t j0) {
-      uint4 *dst = ring + (size_t)st * 4 * m4;
-      for (int i = lane; i < 4 * m4; i += 32) {
-        const int u = i / m4, t = i - u * m4;
-        const int64_t j = j0 + u < je ? j0 + u : j0;
-        cp16(dst + i, (const uint4 *)(g.codesB + j * g.mpad) + t);
-      }
-      cp_commit();
-    };
-    if (jb < je) stage_cols(0, jb);
-    int st = 0;
-    for (int64_t j0 = jb; j0 < je; j0 += 4, st ^= 1) {
-      if (j0 + 4 < je) stage_cols(st ^ 1, j0 + 4); else cp_commit();
-      cp_wait1();
-      __syncwarp();
-      const uint4 *c0 = ring + (size_t)st * 4 * m4;
-      const uint4 *c1 = c0 + m4, *c2 = c1 + m4, *c3 = c2 + m4;
-      uint32_t cntq[4] = {0, 0, 0, 0};
-      for (int t0 = 0; t0 < m4; t0 += 63) {
-        const int t1 = t0 + 63 < m4 ? t0 + 63 : m4;
-        uint32_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+    cp_commit();
+  };
+  if (jb < je) stage_cols(0, jb);
+  int st = 0;
+  for (int64_t j0 = jb; j0 < je; j0 += 4, st ^= 1) {
+    if (j0 + 4 < je) stage_cols(st ^ 1, j0 + 4); else cp_commit();
+    cp_wait1();
+    __syncwarp();
+    const uint4 *c0 = ring + (size_t)st * 4 * m4;
+    const uint4 *c1 = c0 + m4, *c2 = c1 + m4, *c3 = c2 + m4;
+    uint32_t cntq[4] = {0, 0, 0, 0};
+    for (int t0 = 0; t0 < m4; t0 += 63) {
+      const int t1 = t0 + 63 < m4 ? t0 + 63 : m4;
+      uint32_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
 #pragma unroll 2
-        for (int t = t0; t < t1; ++t) {
-          const uint4 a = *(const uint4 *)(ra + 4 * t);
-          const uint4 b0 = c0[t], b1 = c1[t], b2 = c2[t], b3 = c3[t];
-          a0 += eq_bytes(a.x, b0.x) + eq_bytes(a.y, b0.y) + eq_bytes(a.z, b0.z) + eq_bytes(a.w, b0.w);
-          a1 += eq_bytes(a.x, b1.x) + eq_bytes(a.y, b1.y) + eq_bytes(a.z, b1.z) + eq_bytes(a.w, b1.w);
-          a2 += eq_bytes(a.x, b2.x) + eq_bytes(a.y, b2.y) + eq_bytes(a.z, b2.z) + eq_bytes(a.w, b2.w);
-          a3 += eq_bytes(a.x, b3.x) + eq_bytes(a.y, b3.y) + eq_bytes(a.z, b3.z) + eq_bytes(a.w, b3.w);
-        }
-        cntq[0] += byte_sum(a0);
-        cntq[1] += byte_sum(a1);
-        cntq[2] += byte_sum(a2);
-        cntq[3] += byte_sum(a3);
+      for (int t = t0; t < t1; ++t) {
+        const uint4 a = *(const uint4 *)(ra + 4 * t);
+        const uint4 b0 = c0[t], b1 = c1[t], b2 = c2[t], b3 = c3[t];
+        a0 += eq_bytes(a.x, b0.x) + eq_bytes(a.y, b0.y) + eq_bytes(a.z, b0.z) + eq_bytes(a.w, b0.w);
+        a1 += eq_bytes(a.x, b1.x) + eq_bytes(a.y, b1.y) + eq_bytes(a.z, b1.z) + eq_bytes(a.w, b1.w);
+        a2 += eq_bytes(a.x, b2.x) + eq_bytes(a.y, b2.y) + eq_bytes(a.z, b2.z) + eq_bytes(a.w, b2.w);
+        a3 += eq_bytes(a.x, b3.x) + eq_bytes(a.y, b3.y) + eq_bytes(a.z, b3.z) + eq_bytes(a.w, b3.w);
       }
-      __syncwarp();
-#pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        const int64_t j = j0 + t;
-        const bool other = vrow && j < je && j != row;
-        const bool cand = other && (nz_row | __ldg(g.anynz + (j < je ? j : jb)));
-        const uint32_t c = cntq[t];
-        if (other && c > mx_a) mx_a = c;
-        if (cand && c > mx_c) mx_c = c;
-        n_cmp += other;
-        if (cand) {
-          const uint64_t key = ((uint64_t)__ldg(g.sv_bits + c) << 32) | (uint64_t)(~(uint32_t)j);
-          if (key > thr[lane]) w.gbuf[(size_t)lane * cap + cnt[lane]++] = key;
-        }
-      }
-      __syncwarp();
-      compact_full_rows(w, cap - 4);
-    }
-  } else {
-    float ur[SMAX];
-#pragma unroll
-    for (int t = 0; t < SMAX; ++t) ur[t] = (vrow && t < Su) ? g.unit[row * Su + t] : 0.f;
-    int qn = 0;
-    // per-warp ring: 2 stages x kTC columns of unit rows
-    float *ring = (float *)(smem + (size_t)kWarps * 1024) + (size_t)warp * 2 * kTC * Su;
-    auto stage_cols = [&](int st, int64_t jt) {
-      const int nc = (int)(je - jt < kTC ? je - jt : kTC);
-      float *dst = ring + (size_t)st * kTC * Su;
-      const float *src = g.unit + jt * Su;
-      for (int i = lane; i < nc * (Su >> 2); i += 32) cp16(dst + 4 * i, src + 4 * i);
-      cp_commit();
-    };
-    if (jb < je) stage_cols(0, jb);
-    int st = 0;
-    for (int64_t jt = jb; jt < je; jt += kTC, st ^= 1) {
-      if (jt + kTC < je) stage_cols(st ^ 1, jt + kTC); else cp_commit();
-      const int nc = (int)(je - jt < kTC ? je - jt : kTC);
-      const unsigned nzm = __ballot_sync(FULL, lane < nc && __ldg(g.anynz + jt + (lane < nc ? lane : 0)));
-      cp_wait1();
-      __syncwarp();
-      const float *tile = ring + (size_t)st * kTC * Su;
-      for (int c0 = 0; c0 < nc; c0 += 4) {
-        float c1[4] = {0.f, 0.f, 0.f, 0.f};
-        bool cand[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int c = c0 + u;
-          const int64_t j = jt + c;
-          cand[u] = vrow && c < nc && j != row && (nz_row | ((nzm >> c) & 1u));
-        }
-#pragma unroll
-        for (int t4 = 0; t4 < SMAX; t4 += 4) {
-          if (t4 < Su) {
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              const int c = c0 + u < nc ? c0 + u : c0;
-              const float4 v = *(const float4 *)(tile + c * Su + t4);
-              c1[u] = __fmaf_rn(ur[t4 + 0], v.x, c1[u]);
-              c1[u] = __fmaf_rn(ur[t4 + 1], v.y, c1[u]);
-              c1[u] = __fmaf_rn(ur[t4 + 2], v.z, c1[u]);
-              c1[u] = __fmaf_rn(ur[t4 + 3], v.w, c1[u]);
-            }
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int64_t j = jt + c0 + u;
-          n_pref += cand[u];
-          bool pass = cand[u] && c1[u] >= hi;
-          const bool band = cand[u] && c1[u] >= lo && c1[u] < hi;
-          if (__any_sync(FULL, band)) {
-            if (band) pass = !(dot_avx512<SMAX>(ur, g.unit + j * Su, S) < g.prefilter_eps);
-          }
-          const unsigned m = __ballot_sync(FULL, pass);
-          if (m) {
-            if (pass) q[qn + __popc(m & ((1u << lane) - 1u))] = (int)(((unsigned)lane << 27) | (unsigned)j);
-            qn += __popc(m);
-            __syncwarp();
-            if (qn >= 32) {
-              count_batch(g, w, q, 32, row0);
-              n_cmp += 1;
-              if (lane + 32 < qn) q[lane] = q[lane + 32];
-              __syncwarp();
-              qn -= 32;
-            }
-          }
-        }
-      }
-      __syncwarp();
-    }
-    if (qn > 0) {
-      n_cmp += lane < qn;
-      count_batch(g, w, q, qn, row0);
+      cntq[0] += byte_sum(a0);
+      cntq[1] += byte_sum(a1);
+      cntq[2] += byte_sum(a2);
+      cntq[3] += byte_sum(a3);
     }
     __syncwarp();
-    mx_c = mxc[lane];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int64_t j = j0 + t;
+      const bool other = vrow && j < je && j != row;
+      const bool cand = other && (nz_row | __ldg(g.anynz + (j < je ? j : jb)));
+      const uint32_t c = cntq[t];
+      if (other && c > mx_a) mx_a = c;
+      if (cand && c > mx_c) mx_c = c;
+      n_cmp += other;
+      if (cand) {
+        const uint64_t key = ((uint64_t)__ldg(g.sv_bits + c) << 32) | (uint64_t)(~(uint32_t)j);
+        if (key > thr[lane]) w.gbuf[(size_t)lane * cap + cnt[lane]++] = key;
+      }
+    }
+    __syncwarp();
+    compact_full_rows(w, cap - 4);
   }
   if (g.stats) {
     const unsigned a = __reduce_add_sync(FULL, n_pref), b = __reduce_add_sync(FULL, n_cmp);
@@ -413,6 +296,13 @@ k_allpairs(GraphArgs g, uint64_t *gbuf, int32_t *gcnt, int cap, int P, float lo,
     if (mx_c) atomicMax(g.maxcnt_cand + row, mx_c);
     if (mx_a) atomicMax(g.maxcnt_all + row, mx_a);
   }
+}
+
+template <int SMAX>
+__global__ void __launch_bounds__(kWarps * 32)
+k_allpairs(GraphArgs g, uint64_t *gbuf, int32_t *gcnt, int cap, int P) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  dense_item(g, gbuf, gcnt, cap, P, blockIdx.x, blockIdx.y, smem);
 }
 
 // ── sparse regime on the tensor cores ──────────────────────────────────────
@@ -502,15 +392,14 @@ __device__ __forceinline__ void check_batch(const GraphArgs &g, Warp &w, const i
 }
 
 template <int KS, int SMAX>
-__global__ void __launch_bounds__(kWarps * 32)
-k_allpairs_tc(GraphArgs g, uint64_t *gbuf, int32_t *gcnt, int cap, int P, float lo, float hi,
-              float lo16) {
-  extern __shared__ __align__(16) unsigned char smem[];
+__device__ __forceinline__ void tc_item(const GraphArgs &g, uint64_t *gbuf, int32_t *gcnt,
+                                        int cap, int P, float lo, float hi, float lo16,
+                                        int64_t bx, int by, unsigned char *smem) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gq = lane >> 2, tq = lane & 3;
   const int64_t n = g.n;
-  const int64_t row0 = (int64_t)blockIdx.x * 32;
-  const int slice = blockIdx.y * kWarps + warp;
+  const int64_t row0 = bx * 32;
+  const int slice = by * kWarps + warp;
   const int64_t jb = n * slice / P, je = n * (slice + 1) / P;
   const int Kp = KS * 16;
   const int cstride = Kp * 2 + 16;                 // bytes per staged column (conflict-free ldmatrix)
@@ -519,7 +408,7 @@ k_allpairs_tc(GraphArgs g, uint64_t *gbuf, int32_t *gcnt, int cap, int P, float 
   uint64_t *thr = (uint64_t *)ws;
   int *cnt = (int *)(thr + 32);
   uint32_t *mxc = (uint32_t *)(cnt + 32);
-  int *q = (int *)(mxc + 32);                      // [kQ] survivors to count
+  int *q = (int *)(mxc + 32);                      // [64] survivors to count
   int *cq = (int *)(smem + (size_t)kWarps * 1024) + (size_t)warp * kCQ;      // check ring
   unsigned char *rings = smem + (size_t)kWarps * 1024 + (size_t)kWarps * kCQ * 4;
   unsigned char *ring = rings + (size_t)warp * 2 * kTCT * cstride;
@@ -545,7 +434,7 @@ k_allpairs_tc(GraphArgs g, uint64_t *gbuf, int32_t *gcnt, int cap, int P, float 
   thr[lane] = 0;
   cnt[lane] = 0;
   mxc[lane] = 0;
-  const size_t bufrow = ((size_t)blockIdx.x * P + slice) * 32;
+  const size_t bufrow = ((size_t)bx * P + slice) * 32;
   Warp w{gbuf + bufrow * cap, cnt, thr, mxc, cap, g.K};
   unsigned long long n_pref = 0, n_cmp = 0;
 
@@ -669,20 +558,55 @@ k_allpairs_tc(GraphArgs g, uint64_t *gbuf, int32_t *gcnt, int cap, int P, float 
   if (row < n && mxc[lane]) atomicMax(g.maxcnt_cand + row, mxc[lane]);
 }
 
+template <int KS, int SMAX>
+__global__ void __launch_bounds__(kWarps * 32)
+k_allpairs_tc(GraphArgs g, uint64_t *gbuf, int32_t *gcnt, int cap, int P, float lo, float hi,
+              float lo16) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  tc_item<KS, SMAX>(g, gbuf, gcnt, cap, P, lo, hi, lo16, blockIdx.x, blockIdx.y, smem);
+}
+
+// Persistent form over a batch: CTAs pull (assembly, row block, slice group)
+// items from a device counter until the variant's items are exhausted.
+template <int KS, int SMAX>
+__global__ void __launch_bounds__(kWarps * 32)
+k_allpairs_batch(const BatchAsm *B, const int32_t *list, const int64_t *item0s, int nv,
+                 int64_t items, unsigned long long *next) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ long long s_item;
+  for (;;) {
+    __syncthreads();                     // the previous item is done with shared memory
+    if (threadIdx.x == 0) s_item = (long long)atomicAdd(next, 1ull);
+    __syncthreads();
+    const int64_t it = s_item;
+    if (it >= items) return;
+    int lo = 0, hi = nv - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(item0s + mid) <= it) lo = mid; else hi = mid - 1;
+    }
+    const BatchAsm &b = B[list[lo]];
+    const GraphArgs g = b.g;
+    const int G = b.P / kWarps;
+    const int64_t local = it - item0s[lo];
+    const int64_t bx = local / G;
+    const int by = (int)(local - bx * G);
+    if constexpr (KS == 0) dense_item(g, b.gbuf, b.gcnt, b.cap, b.P, bx, by, smem);
+    else tc_item<KS, SMAX>(g, b.gbuf, b.gcnt, b.cap, b.P, b.lo, b.hi, b.lo16, bx, by, smem);
+  }
+}
+
 // Warp per row: the K best keys among the P slices' partial lists.  The lists
 // stream through a 512-key shared buffer per warp; whenever it fills, the
 // register radix select keeps its K best (K <= 448 leaves room to refill).
 constexpr int kMergeWarps = 8;
 constexpr int kMergeBuf = 32 * kCapW;       // 512 keys per warp
 
-__global__ void __launch_bounds__(kMergeWarps * 32)
-k_merge_topk(GraphArgs g, const uint64_t *gbuf, const int32_t *gcnt, int cap, int P) {
-  __shared__ uint64_t mk[kMergeWarps][kMergeBuf];
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int64_t row = (int64_t)blockIdx.x * kMergeWarps + wib;
-  if (row >= g.n) return;
+__device__ __forceinline__ void merge_row(const GraphArgs &g, const uint64_t *gbuf,
+                                          const int32_t *gcnt, int cap, int P, int64_t row,
+                                          uint64_t *keys) {
+  const int lane = threadIdx.x & 31;
   const int K = g.K;
-  uint64_t *keys = mk[wib];
   const int64_t rb = row >> 5, rl = row & 31;
   const size_t br0 = (size_t)rb * P * 32 + rl;          // slice s: br0 + 32 s
   const int cl = lane < P ? gcnt[br0 + (size_t)lane * 32] : 0;   // P <= 32
@@ -710,11 +634,38 @@ k_merge_topk(GraphArgs g, const uint64_t *gbuf, const int32_t *gcnt, int cap, in
   if (lane == 0) g.topk_cnt[row] = fill;
 }
 
-size_t allpairs_smem(int mpad, int Su, bool sparse) {
+__global__ void __launch_bounds__(kMergeWarps * 32)
+k_merge_topk(GraphArgs g, const uint64_t *gbuf, const int32_t *gcnt, int cap, int P) {
+  __shared__ uint64_t mk[kMergeWarps][kMergeBuf];
+  const int wib = threadIdx.x >> 5;
+  const int64_t row = (int64_t)blockIdx.x * kMergeWarps + wib;
+  if (row < g.n) merge_row(g, gbuf, gcnt, cap, P, row, mk[wib]);
+}
+
+__global__ void __launch_bounds__(kMergeWarps * 32)
+k_merge_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows) {
+  __shared__ uint64_t mk[kMergeWarps][kMergeBuf];
+  const int wib = threadIdx.x >> 5;
+  const int64_t r = (int64_t)blockIdx.x * kMergeWarps + wib;
+  if (r >= rows) return;
+  int lo = 0, hi = nb - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(row0s + mid) <= r) lo = mid; else hi = mid - 1;
+  }
+  const BatchAsm &b = B[lo];
+  merge_row(b.g, b.gbuf, b.gcnt, b.cap, b.P, r - b.row0, mk[wib]);
+}
+
+size_t dense_smem(int mpad) {
   const int mw = mpad >> 2;
   const int mwq = ((mw + 27) & ~31) + 4;
-  if (sparse) return (size_t)kWarps * 1024 + (size_t)kWarps * 2 * kTC * Su * 4;
   return (size_t)kWarps * 1024 + 32 * (size_t)mwq * 4 + (size_t)kWarps * 2 * 4 * mpad;
+}
+
+size_t tc_smem(int KS, int mpad, int Su) {
+  return (size_t)kWarps * 1024 + (size_t)kWarps * kCQ * 4 +
+         (size_t)kWarps * 2 * kTCT * (KS * 16 * 2 + 16) + (size_t)32 * mpad + (size_t)32 * Su * 4;
 }
 
 }  // namespace
@@ -733,47 +684,85 @@ int allpairs_slices(int64_t n, int K) {
   return (int)(((P + kWarps - 1) / kWarps) * kWarps);
 }
 
+int64_t allpairs_items(int64_t n, int P) { return ((n + 31) / 32) * (P / kWarps); }
+
+size_t allpairs_batch_smem(int variant, int mpad, int Su) {
+  return variant == 0 ? dense_smem(mpad) : tc_smem(variant, mpad, Su);
+}
+
+void prefilter_bands(int S, float eps, float *lo, float *hi, float *lo16) {
+  // band of the exact-safe prefilter: |chain - AVX-512 order| < delta
+  const double e = (double)eps;
+  const double delta = (double)(S + (S + 15) / 16 + 8) * ldexp(1.0, -23);
+  float l = (float)(e - delta), h = (float)(e + delta);
+  if ((double)l > e - delta) l = nextafterf(l, -INFINITY);
+  if ((double)h < e + delta) h = nextafterf(h, INFINITY);
+  *lo = l;
+  *hi = h;
+  *lo16 = (float)(e - (double)kTcDelta);
+}
+
+int allpairs_variant(const GraphArgs &g) {
+  if (!g.prefilter) return 0;
+  return g.Kp == 16 ? 1 : (g.Kp == 32 ? 2 : 4);   // the FP16 rows are KS * 16 halves wide
+}
+
 void launch_allpairs(const GraphArgs &g, uint64_t *gbuf, int32_t *gcnt, cudaStream_t s) {
   if (g.n == 0) return;
   const int cap = allpairs_cap(g.K);
   const int P = allpairs_slices(g.n, g.K);
-  const bool sparse = g.prefilter != 0;
-  const size_t smem = allpairs_smem(g.mpad, g.Su, sparse);
   const dim3 grid((unsigned)((g.n + 31) / 32), (unsigned)(P / kWarps));
-  // band of the exact-safe prefilter: |chain - AVX-512 order| < delta
-  const double eps = (double)g.prefilter_eps;
-  const double delta = (double)(g.S + (g.S + 15) / 16 + 8) * ldexp(1.0, -23);
-  float lo = (float)(eps - delta), hi = (float)(eps + delta);
-  if ((double)lo > eps - delta) lo = nextafterf(lo, -INFINITY);
-  if ((double)hi < eps + delta) hi = nextafterf(hi, INFINITY);
-#define RBG_LAUNCH(SM, SP)                                                                   \
-  do {                                                                                       \
-    cudaFuncSetAttribute(k_allpairs<SM, SP>, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
-                         (int)smem);                                                         \
-    k_allpairs<SM, SP><<<grid, kWarps * 32, smem, s>>>(g, gbuf, gcnt, cap, P, lo, hi);      \
-  } while (0)
-  if (sparse) {
-    const float lo16 = (float)(eps - (double)kTcDelta);
-    const size_t tsm = (size_t)kWarps * 1024 + (size_t)kWarps * kCQ * 4 +
-                       (size_t)kWarps * 2 * kTCT * (g.Kp * 2 + 16) + (size_t)32 * g.mpad +
-                       (size_t)32 * g.Su * 4;
+  float lo, hi, lo16;
+  prefilter_bands(g.S, g.prefilter_eps, &lo, &hi, &lo16);
+  const int v = allpairs_variant(g);
+  const size_t smem = allpairs_batch_smem(v, g.mpad, g.Su);
 #define RBG_TC(KS, SM)                                                                        \
   do {                                                                                        \
     cudaFuncSetAttribute(k_allpairs_tc<KS, SM>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
-                         (int)tsm);                                                           \
-    k_allpairs_tc<KS, SM><<<grid, kWarps * 32, tsm, s>>>(g, gbuf, gcnt, cap, P, lo, hi, lo16); \
+                         (int)smem);                                                          \
+    k_allpairs_tc<KS, SM><<<grid, kWarps * 32, smem, s>>>(g, gbuf, gcnt, cap, P, lo, hi, lo16); \
   } while (0)
-    // the FP16 rows are 16, 32 or 64 halves wide: exactly KS * 16
-    if (g.Kp == 16) RBG_TC(1, 16);
-    else if (g.Kp == 32) RBG_TC(2, 32);
-    else if (g.Kp == 64) RBG_TC(4, 64);
-#undef RBG_TC
-  } else {
-    RBG_LAUNCH(4, false);
+  if (v == 1) RBG_TC(1, 16);
+  else if (v == 2) RBG_TC(2, 32);
+  else if (v == 4) RBG_TC(4, 64);
+  else {
+    cudaFuncSetAttribute(k_allpairs<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_allpairs<4><<<grid, kWarps * 32, smem, s>>>(g, gbuf, gcnt, cap, P);
   }
-#undef RBG_LAUNCH
+#undef RBG_TC
   k_merge_topk<<<(unsigned)((g.n + kMergeWarps - 1) / kMergeWarps), kMergeWarps * 32, 0, s>>>(
       g, gbuf, gcnt, cap, P);
+}
+
+void launch_allpairs_batch(const BatchAsm *B, int variant, const int32_t *list,
+                           const int64_t *item0s, int nv, int64_t items, size_t smem,
+                           unsigned long long *next, cudaStream_t s) {
+  if (items == 0 || nv == 0) return;
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+#define RBG_PB(KS, SM)                                                                         \
+  do {                                                                                         \
+    cudaFuncSetAttribute(k_allpairs_batch<KS, SM>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                         (int)smem);                                                           \
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_allpairs_batch<KS, SM>,           \
+                                                  kWarps * 32, smem);                          \
+    const int64_t grid = std::min<int64_t>(items, (int64_t)std::max(per_sm, 1) * sms);         \
+    k_allpairs_batch<KS, SM><<<(unsigned)grid, kWarps * 32, smem, s>>>(B, list, item0s, nv,    \
+                                                                       items, next);           \
+  } while (0)
+  if (variant == 1) RBG_PB(1, 16);
+  else if (variant == 2) RBG_PB(2, 32);
+  else if (variant == 4) RBG_PB(4, 64);
+  else RBG_PB(0, 4);
+#undef RBG_PB
+}
+
+void launch_merge_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows,
+                        cudaStream_t s) {
+  if (rows == 0) return;
+  k_merge_batch<<<(unsigned)((rows + kMergeWarps - 1) / kMergeWarps), kMergeWarps * 32, 0, s>>>(
+      B, row0s, nb, rows);
 }
 
 }  // namespace rbg

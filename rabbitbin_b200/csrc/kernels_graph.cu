@@ -16,6 +16,16 @@ namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
 
+// Last assembly a with starts[a] <= x (starts ascending, starts[0] = 0).
+__device__ __forceinline__ int find_asm(const int64_t *starts, int nb, int64_t x) {
+  int lo = 0, hi = nb - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(starts + mid) <= x) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
 // ── unit rank rows (src/rabbitbin.cpp:4867-4874 rank, :4972-4988 unit rows,
 //    src/ranker.h:55-66 average ranks, src/impl/rb_abundance.cpp:94-114 anynz)
 // Warp per row, lane = sample (two samples per lane when S > 32).  The average
@@ -23,10 +33,8 @@ constexpr unsigned FULL = 0xffffffffu;
 // the reference's sequential double sums of ranks and of squared deviations
 // (multiples of 1/4, far below 2^53) are exact in any order: warp reductions
 // give the same mean and ss.
-__global__ void k_unit_rows(GraphArgs g) {
+__device__ __forceinline__ void unit_row(const GraphArgs &g, int64_t r) {
   const int lane = threadIdx.x & 31;
-  const int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (r >= g.n) return;
   const int S = g.S;
   const float *x = g.depth_raw + r * S;
   const float x0 = lane < S ? x[lane] : 0.f;
@@ -71,6 +79,19 @@ __global__ void k_unit_rows(GraphArgs g) {
   }
 }
 
+__global__ void k_unit_rows(GraphArgs g) {
+  const int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (r >= g.n) return;
+  unit_row(g, r);
+}
+
+__global__ void k_unit_rows_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows) {
+  const int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (r >= rows) return;
+  const int a = find_asm(row0s, nb, r);
+  unit_row(B[a].g, r - B[a].row0);
+}
+
 // Column norms of the raw depths (src/rabbitbin.cpp:4800-4806): the reference
 // sums each column in row order in double.  Fast path: if every value of a
 // column is an integer multiple of 2^E (E = lowest set bit over its non-zero
@@ -87,7 +108,7 @@ __device__ __forceinline__ int low_bit_exp(float x) {
   return base + __ffs(mant) - 1;
 }
 
-__global__ void k_colsum_fast(GraphArgs g, double *acc) {
+__device__ __forceinline__ void colsum_fast(const GraphArgs &g, double *acc, int blk, int nblk) {
   // acc layout per column i: [0] sum, [1] sum |x|, [2] (int) min exponent
   __shared__ double ssum[kMaxS], sabs[kMaxS];
   __shared__ int semin[kMaxS];
@@ -95,8 +116,8 @@ __global__ void k_colsum_fast(GraphArgs g, double *acc) {
   for (int i = threadIdx.x; i < S; i += blockDim.x) { ssum[i] = 0.0; sabs[i] = 0.0; semin[i] = 1 << 20; }
   __syncthreads();
   const int64_t total = g.n * S;
-  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total;
-       q += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t q = (int64_t)blk * blockDim.x + threadIdx.x; q < total;
+       q += (int64_t)nblk * blockDim.x) {
     const float x = g.depth_raw[q];
     const int i = (int)(q % S);
     if (x != 0.0f) {
@@ -113,7 +134,14 @@ __global__ void k_colsum_fast(GraphArgs g, double *acc) {
   }
 }
 
-__global__ void k_colnorm(GraphArgs g, const double *acc) {
+__global__ void k_colsum_fast(GraphArgs g, double *acc) { colsum_fast(g, acc, blockIdx.x, gridDim.x); }
+
+__global__ void k_colsum_fast_batch(const BatchAsm *B) {
+  const BatchAsm &b = B[blockIdx.y];
+  if (b.colnorm_on && b.g.n > 0) colsum_fast(b.g, b.colacc, blockIdx.x, gridDim.x);
+}
+
+__device__ __forceinline__ void colnorm_body(const GraphArgs &g, const double *acc) {
   constexpr int CH = 128;
   __shared__ float chunk[CH * kMaxS];
   __shared__ int need_seq;
@@ -149,6 +177,13 @@ __global__ void k_colnorm(GraphArgs g, const double *acc) {
   }
 }
 
+__global__ void k_colnorm(GraphArgs g, const double *acc) { colnorm_body(g, acc); }
+
+__global__ void k_colnorm_batch(const BatchAsm *B) {
+  const BatchAsm &b = B[blockIdx.x];
+  if (b.colnorm_on && b.g.n > 0) colnorm_body(b.g, b.colacc);
+}
+
 // Number of registers where two 8-bit code words agree (A side: 0 = unset,
 // B side: 0xFF = unset, so unset never matches).
 __device__ __forceinline__ uint32_t match4(uint32_t a, uint32_t b) {
@@ -167,6 +202,62 @@ __global__ void k_pair_counts(const uint8_t *__restrict__ A, const uint8_t *__re
   uint32_t c = 0;
   for (int w = 0; w < mpad / 4; ++w) c += match4(__ldg(a + w), __ldg(b + w));
   out[p] = c;
+}
+
+// b0 of every assembly of a batch (estimate_pmh_baseline,
+// src/rabbitbin.cpp:1340-1369): register-match counts of its sampled pairs
+// (local ids), then the element at index np/2 of their sorted list from a
+// histogram of the counts (the float match fractions sort as the counts do),
+// then the similarity table of pmh_sv_from_count (:1297-1305).
+__global__ void k_pair_counts_batch(const BatchAsm *B, const int64_t *pair0s, int nb,
+                                    int64_t npairs, const int32_t *__restrict__ pairs,
+                                    uint32_t *__restrict__ out) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npairs) return;
+  const int a = find_asm(pair0s, nb, p);
+  const GraphArgs &g = B[a].g;
+  const uint32_t *x = (const uint32_t *)(g.codesA + (int64_t)pairs[2 * p] * g.mpad);
+  const uint32_t *y = (const uint32_t *)(g.codesB + (int64_t)pairs[2 * p + 1] * g.mpad);
+  uint32_t c = 0;
+  for (int w = 0; w < g.mpad / 4; ++w) c += match4(__ldg(x + w), __ldg(y + w));
+  out[p] = c;
+}
+
+__global__ void k_b0_batch(const BatchAsm *B, const uint32_t *__restrict__ counts) {
+  extern __shared__ int hist[];
+  __shared__ int med;
+  const BatchAsm &b = B[blockIdx.x];
+  const int m = b.g.m, np = b.np;
+  const bool on = b.base_on && np > 0;
+  if (on) {
+    for (int c = threadIdx.x; c <= m; c += blockDim.x) hist[c] = 0;
+    __syncthreads();
+    for (int q = threadIdx.x; q < np; q += blockDim.x) atomicAdd(&hist[counts[b.pair0 + q]], 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int cum = 0, c = 0;
+      for (; c < m; ++c) {
+        cum += hist[c];
+        if (cum > np / 2) break;
+      }
+      med = c;
+    }
+    __syncthreads();
+  }
+  const double inv_m = 1.0 / (double)m;
+  const float b0f = on ? (float)__dmul_rn((double)(uint32_t)med, inv_m) : 0.0f;
+  const double b0 = (double)b0f;
+  if (threadIdx.x == 0) *b.b0 = b0f;
+  const double inv1mb0 = (b0 < 1.0) ? 1.0 / __dsub_rn(1.0, b0) : 1.0;
+  for (int c = threadIdx.x; c <= m; c += blockDim.x) {
+    double j = __dmul_rn((double)(uint32_t)c, inv_m);
+    if (b.base_on && b0 > 0.0 && b0 < 1.0) {
+      j = __dmul_rn(__dsub_rn(j, b0), inv1mb0);
+      if (j < 0.0) j = 0.0;
+    }
+    if (j > 1.0 - 1e-6) j = 1.0 - 1e-6;
+    b.sv_out[c] = __float_as_uint((float)j);
+  }
 }
 
 // Bitonic sort, descending, of `len` (power of two) keys in shared memory by
@@ -188,21 +279,17 @@ __device__ void warp_sort_desc(uint64_t *keys, int len) {
   }
 }
 
-__device__ __forceinline__ int pow2_at_least(int x) {
+__host__ __device__ __forceinline__ int pow2_at_least(int x) {
   int p = 1;
   while (p < x) p <<= 1;
   return p;
 }
 
 // ── neighbour lists: cut by the calibrated threshold, sorted by id ──────────
-__global__ void k_sort_rows(EmitArgs e) {
-  extern __shared__ uint64_t shk[];
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int64_t i = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
-  if (i >= e.n) return;
+__device__ __forceinline__ void sort_row(const EmitArgs &e, int64_t i, uint64_t *keys) {
+  const int lane = threadIdx.x & 31;
   const int K = e.K;
   const int len = pow2_at_least(K > 32 ? K : 32);
-  uint64_t *keys = shk + (size_t)wib * len;
   const int c = e.topk_cnt[i];
   // keep sv > cutoff; re-key as (id, sv bits) so an ascending sort orders ids
   for (int q = lane; q < len; q += 32) {
@@ -231,6 +318,24 @@ __global__ void k_sort_rows(EmitArgs e) {
   if (lane == 0) e.nbr_cnt[i] = kept;
 }
 
+__global__ void k_sort_rows(EmitArgs e) {
+  extern __shared__ uint64_t shk[];
+  const int wib = threadIdx.x >> 5;
+  const int64_t i = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
+  if (i >= e.n) return;
+  sort_row(e, i, shk + (size_t)wib * pow2_at_least(e.K > 32 ? e.K : 32));
+}
+
+__global__ void k_sort_rows_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows,
+                                  int maxlen) {
+  extern __shared__ uint64_t shk[];
+  const int wib = threadIdx.x >> 5;
+  const int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
+  if (r >= rows) return;
+  const int a = find_asm(row0s, nb, r);
+  sort_row(B[a].e, r - B[a].row0, shk + (size_t)wib * maxlen);
+}
+
 __device__ __forceinline__ bool has_nbr(const uint32_t *ids, int cnt, uint32_t x) {
   int lo = 0, hi = cnt;
   while (lo < hi) {
@@ -242,9 +347,7 @@ __device__ __forceinline__ bool has_nbr(const uint32_t *ids, int cnt, uint32_t x
 
 // Edges of row i: (i, j) for kept neighbours j > i; with the mutual filter
 // (src/impl/rb_graph.cpp:1284-1348) i must also be a kept neighbour of j.
-__global__ void k_count_edges(EmitArgs e) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= e.n) return;
+__device__ __forceinline__ void count_edges_row(const EmitArgs &e, int64_t i) {
   const int c = e.nbr_cnt[i];
   const uint32_t *ids = e.nbr_sorted + i * e.K;
   int cnt = 0;
@@ -256,6 +359,23 @@ __global__ void k_count_edges(EmitArgs e) {
     ++cnt;
   }
   e.row_edges[i] = cnt;
+}
+
+__global__ void k_count_edges(EmitArgs e) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < e.n) count_edges_row(e, i);
+}
+
+__global__ void k_count_edges_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  const int a = find_asm(row0s, nb, r);
+  count_edges_row(B[a].e, r - B[a].row0);
+}
+
+// First edge of every assembly after the batch-wide scan of row_edges.
+__global__ void k_edge0s(const int64_t *row0s, int nb, const int32_t *row_edges, int64_t *edge0s) {
+  for (int a = threadIdx.x; a <= nb; a += blockDim.x) edge0s[a] = row_edges[row0s[a]];
 }
 
 __global__ void k_scan(int32_t *v, int64_t n) {
@@ -279,9 +399,7 @@ __global__ void k_scan(int32_t *v, int64_t n) {
   if (t == 1023) v[n] = (int32_t)part[1023];
 }
 
-__global__ void k_write_edges(EmitArgs e) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= e.n) return;
+__device__ __forceinline__ void write_edges_row(const EmitArgs &e, int64_t i) {
   const int c = e.nbr_cnt[i];
   const uint32_t *ids = e.nbr_sorted + i * e.K;
   int64_t o = e.row_edges[i];
@@ -295,6 +413,18 @@ __global__ void k_write_edges(EmitArgs e) {
     e.scomp[o] = e.nbr_sv[i * e.K + q];
     ++o;
   }
+}
+
+__global__ void k_write_edges(EmitArgs e) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < e.n) write_edges_row(e, i);
+}
+
+__global__ void k_write_edges_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  const int a = find_asm(row0s, nb, r);
+  write_edges_row(B[a].e, r - B[a].row0);
 }
 
 // ── edge weights (src/rabbitbin.cpp:5482-5509, depth_edge_term :930-970) ───
@@ -340,9 +470,7 @@ __device__ double depth_wjac(const float *a, const float *b, int S, const double
   return mn / mx;
 }
 
-__global__ void k_edge_weights(WeightArgs w) {
-  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= w.n_edges) return;
+__device__ __forceinline__ void edge_weight(const WeightArgs &w, int64_t e) {
   const float sc = w.scomp[e];
   if (w.S <= 0) {              // no depth file (src/rabbitbin.cpp:5532-5536)
     w.score[e] = (sc < w.min_edge) ? 0.0f : sc;
@@ -391,6 +519,17 @@ __global__ void k_edge_weights(WeightArgs w) {
   w.score[e] = (float)val;
 }
 
+__global__ void k_edge_weights(WeightArgs w) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < w.n_edges) edge_weight(w, e);
+}
+
+__global__ void k_edge_weights_batch(const BatchAsm *B, const int64_t *edge0s, int nb, int64_t edges) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= edges) return;
+  edge_weight(B[find_asm(edge0s, nb, e)].w, e);
+}
+
 }  // namespace
 
 void launch_unit_rows(const GraphArgs &g, cudaStream_t s) {
@@ -437,6 +576,52 @@ void launch_write_edges(const EmitArgs &e, cudaStream_t s) {
 void launch_edge_weights(const WeightArgs &w, cudaStream_t s) {
   if (w.n_edges == 0) return;
   k_edge_weights<<<(unsigned)((w.n_edges + 127) / 128), 128, 0, s>>>(w);
+}
+
+void launch_unit_rows_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows,
+                            cudaStream_t s) {
+  if (rows == 0) return;
+  k_unit_rows_batch<<<(unsigned)((rows + 7) / 8), 256, 0, s>>>(B, row0s, nb, rows);
+}
+
+void launch_colnorm_batch(const BatchAsm *B, int nb, int max_s, cudaStream_t s) {
+  if (nb == 0 || max_s <= 1) return;
+  k_colsum_fast_batch<<<dim3(64, (unsigned)nb), 256, 0, s>>>(B);
+  k_colnorm_batch<<<(unsigned)nb, 256, 0, s>>>(B);
+}
+
+void launch_b0_batch(const BatchAsm *B, const int64_t *pair0s, int nb, int64_t npairs,
+                     const int32_t *pairs, uint32_t *counts, int max_m, cudaStream_t s) {
+  if (nb == 0) return;
+  if (npairs > 0)
+    k_pair_counts_batch<<<(unsigned)((npairs + 127) / 128), 128, 0, s>>>(B, pair0s, nb, npairs,
+                                                                          pairs, counts);
+  k_b0_batch<<<(unsigned)nb, 256, (size_t)(max_m + 1) * sizeof(int), s>>>(B, counts);
+}
+
+void launch_emit_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows, int max_k,
+                       int32_t *row_edges, int64_t *edge0s, cudaStream_t s) {
+  if (rows > 0) {
+    const int len = pow2_at_least(max_k > 32 ? max_k : 32);
+    const int warps = 4;
+    k_sort_rows_batch<<<(unsigned)((rows + warps - 1) / warps), warps * 32,
+                        (size_t)warps * len * 8, s>>>(B, row0s, nb, rows, len);
+    k_count_edges_batch<<<(unsigned)((rows + 127) / 128), 128, 0, s>>>(B, row0s, nb, rows);
+  }
+  k_scan<<<1, 1024, 0, s>>>(row_edges, rows);
+  k_edge0s<<<1, 256, 0, s>>>(row0s, nb, row_edges, edge0s);
+}
+
+void launch_write_edges_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows,
+                              cudaStream_t s) {
+  if (rows == 0) return;
+  k_write_edges_batch<<<(unsigned)((rows + 127) / 128), 128, 0, s>>>(B, row0s, nb, rows);
+}
+
+void launch_edge_weights_batch(const BatchAsm *B, const int64_t *edge0s, int nb, int64_t edges,
+                               cudaStream_t s) {
+  if (edges == 0) return;
+  k_edge_weights_batch<<<(unsigned)((edges + 127) / 128), 128, 0, s>>>(B, edge0s, nb, edges);
 }
 
 }  // namespace rbg

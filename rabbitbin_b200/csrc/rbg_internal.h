@@ -144,4 +144,59 @@ struct WeightArgs {
 
 void launch_edge_weights(const WeightArgs &w, cudaStream_t s);
 
+// ── batches of assemblies (kernels over many assemblies in one launch) ─────
+// One assembly of a batch, held in device memory.  Every pointer in g, e and
+// w addresses that assembly's own rows (local ids 0..n-1); the edge arrays
+// e.from/to/scomp and w.from/to/scomp/score are the batch's global ones and
+// e.row_edges points at the assembly's first row of the batch-wide scan.
+struct BatchAsm {
+  GraphArgs g;
+  EmitArgs e;
+  WeightArgs w;
+  int64_t row0 = 0;                    // first row in the batch's row space
+  // all-pairs
+  uint64_t *gbuf = nullptr;            // candidate buffers [ceil(n/32)][P][32][cap]
+  int32_t *gcnt = nullptr;             // [ceil(n/32)][P][32]
+  int cap = 0, P = 0, variant = 0;     // variant: 0 dense, 1/2/4 tensor-core KS
+  float lo = 0.f, hi = 0.f, lo16 = 0.f;
+  // column norms
+  int colnorm_on = 0;
+  double *colacc = nullptr;            // [3 S]
+  // b0: register-match counts of this assembly's sampled pairs
+  int base_on = 0, np = 0;
+  int64_t pair0 = 0;                   // first pair in the batch's pair list
+  float *b0 = nullptr;                 // out: b0 of the assembly (float, as stored)
+  uint32_t *sv_out = nullptr;          // out: [m+1] similarity float bits (== g.sv_bits)
+};
+
+// Index helper arrays ("starts") are ascending int64 with starts[nb] = total;
+// a batch kernel maps a global index x to the last assembly a with
+// starts[a] <= x.
+void launch_unit_rows_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows,
+                            cudaStream_t s);
+void launch_colnorm_batch(const BatchAsm *B, int nb, int max_s, cudaStream_t s);
+void launch_b0_batch(const BatchAsm *B, const int64_t *pair0s, int nb, int64_t npairs,
+                     const int32_t *pairs, uint32_t *counts, int max_m, cudaStream_t s);
+// Persistent all-pairs over the assemblies list[0..nv) of one variant: work
+// item x of assembly list[k] is x - item0s[k] (row block, slice group); CTAs
+// pull items from *next (zeroed by the caller).
+void launch_allpairs_batch(const BatchAsm *B, int variant, const int32_t *list,
+                           const int64_t *item0s, int nv, int64_t items, size_t smem,
+                           unsigned long long *next, cudaStream_t s);
+void launch_merge_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows,
+                        cudaStream_t s);
+void launch_emit_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows, int max_k,
+                       int32_t *row_edges, int64_t *edge0s, cudaStream_t s);
+void launch_write_edges_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows,
+                              cudaStream_t s);
+void launch_edge_weights_batch(const BatchAsm *B, const int64_t *edge0s, int nb, int64_t edges,
+                               cudaStream_t s);
+// Work items of the all-pairs kernels for one assembly.
+int64_t allpairs_items(int64_t n, int P);
+size_t allpairs_batch_smem(int variant, int mpad, int Su);
+// 0 (dense) or the tensor-core prefilter's k-steps KS (1, 2, 4).
+int allpairs_variant(const GraphArgs &g);
+// lo/hi: band of the exact-safe FP32 chain; lo16: the tensor-core prune bound.
+void prefilter_bands(int S, float eps, float *lo, float *hi, float *lo16);
+
 }  // namespace rbg
