@@ -53,12 +53,14 @@ class Assembly:
 def _stationary(P):
     """Stationary distribution of the 64-context chain with rows P[ctx, b]."""
     T = np.zeros((64, 64))
-    for c in range(64):
-        for b in range(4):
-            T[c, ((c << 2) | b) & 63] += P[c, b]
-    pi = np.full(64, 1.0 / 64)
-    for _ in range(500):
-        pi = pi @ T
+    c = np.repeat(np.arange(64), 4)
+    np.add.at(T, (c, ((c << 2) | np.tile(np.arange(4), 64)) & 63), P.reshape(-1))
+    # pi (T - I) = 0 with sum(pi) = 1: one equation replaced by the normalisation
+    A = (T - np.eye(64)).T
+    A[-1, :] = 1.0
+    rhs = np.zeros(64)
+    rhs[-1] = 1.0
+    pi = np.linalg.solve(A, rhs)
     return pi / pi.sum()
 
 
@@ -116,7 +118,10 @@ def _chains(rng, tabs, genome_ids, lengths):
     cum = np.ascontiguousarray(np.cumsum(tabs, axis=2)[:, :, :3], dtype=np.float64)
     gid = np.ascontiguousarray(genome_ids, dtype=np.int32)
     seeds = rng.integers(0, 2**63, size=n, dtype=np.int64).astype(np.uint64)
-    out = np.zeros(int(offs[-1]), dtype=np.uint8)
+    # filled here, on one thread: the generator's threads would otherwise take
+    # the first-touch page faults of the whole buffer concurrently (slow)
+    out = np.empty(int(offs[-1]), dtype=np.uint8)
+    out.fill(0)
     P = ctypes.c_void_p
     _chain_so().synth_chains(P(cum.ctypes.data), P(gid.ctypes.data), P(offs.ctypes.data),
                              P(seeds.ctypes.data), ctypes.c_int64(n), P(out.ctypes.data))
