@@ -305,6 +305,7 @@ BatchAsm describe(BatchBufs &B, const AsmPlan &a, int b) {
   g.maxcnt_cand = dptr<uint32_t>(B.maxc_cand, a.row0);
   g.maxcnt_all = dptr<uint32_t>(B.maxc_all, a.row0);
   g.stats = B.stats.as<unsigned long long>();
+  g.key_floor = admission_floor();
   d.row0 = a.row0;
   d.gbuf = dptr<uint64_t>(B.gbuf, a.gbuf0);
   d.gcnt = dptr<int32_t>(B.gcnt, a.gcnt0);

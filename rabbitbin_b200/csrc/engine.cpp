@@ -242,6 +242,7 @@ void run_graph(rbg_ctx *c, const rbg_params *p) {
   g.maxcnt_cand = c->maxc_cand.as<uint32_t>();
   g.maxcnt_all = c->maxc_all.as<uint32_t>();
   g.stats = c->stats.as<unsigned long long>();
+  g.key_floor = admission_floor();
   CK(cudaMemsetAsync(c->stats.p, 0, 2 * sizeof(unsigned long long), c->stream));
   CK(cudaStreamWaitEvent(c->stream, c->ev_aux, 0));   // unit rows, anynz, column norms
   c->prep_done = false;

@@ -35,14 +35,22 @@ constexpr unsigned FULL = 0xffffffffu;
 constexpr int kWarps = 4;         // warps per CTA (independent)
 constexpr int kCapW = 16;         // candidate buffer <= 32 * kCapW keys per row
 
-__device__ __forceinline__ uint32_t eq_bytes(uint32_t a, uint32_t b) {
+// 0x80 in each byte where a and b agree, 0 elsewhere: the low seven bits of
+// each byte of a ^ b are tested by an add that cannot carry out of the byte,
+// the top bit directly.
+__device__ __forceinline__ uint32_t eq_mask(uint32_t a, uint32_t b) {
   const uint32_t x = a ^ b;
-  const uint32_t t = ((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | x;
-  return (~t & 0x80808080u) >> 7;      // 0x01 in each equal byte
+  const uint32_t t = (x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu;
+  return ~(t | x) & 0x80808080u;
 }
-__device__ __forceinline__ uint32_t byte_sum(uint32_t acc) {
-  const uint32_t t = (acc & 0x00FF00FFu) + ((acc >> 8) & 0x00FF00FFu);
-  return (t & 0xFFFFu) + (t >> 16);
+// acc + 128 x (number of equal bytes of two 16-byte blocks); the byte dot
+// product with 0x01010101 sums the masks on the FMA pipe, beside the ALU
+// work of the masks.
+__device__ __forceinline__ uint32_t eq16(const uint4 &a, const uint4 &b, uint32_t acc) {
+  acc = __dp4a(eq_mask(a.x, b.x), 0x01010101u, acc);
+  acc = __dp4a(eq_mask(a.y, b.y), 0x01010101u, acc);
+  acc = __dp4a(eq_mask(a.z, b.z), 0x01010101u, acc);
+  return __dp4a(eq_mask(a.w, b.w), 0x01010101u, acc);
 }
 
 // unit_dot_f (src/rabbitbin.cpp:754-796) as an AVX-512 build evaluates it:
@@ -152,21 +160,17 @@ __device__ __forceinline__ void count_batch_coop(const GraphArgs &g, Warp &w, co
       ra[u] = (const uint4 *)(sA + (size_t)(e >> 27) * g.mpad);
       cb[u] = (const uint4 *)(g.codesB + (int64_t)(e & 0x07FFFFFFu) * g.mpad);
     }
-    uint32_t acc[4] = {0u, 0u, 0u, 0u};
-    for (int t = lane; t < m16; t += 32) {      // <= 8 steps: byte lanes stay below 256
+    uint32_t acc[4] = {0u, 0u, 0u, 0u};         // 128 x matches
+    for (int t = lane; t < m16; t += 32) {
       uint4 b[4];
 #pragma unroll
       for (int u = 0; u < 4; ++u) b[u] = __ldg(cb[u] + t);
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const uint4 a = ra[u][t];
-        acc[u] += eq_bytes(a.x, b[u].x) + eq_bytes(a.y, b[u].y) + eq_bytes(a.z, b[u].z) +
-                  eq_bytes(a.w, b[u].w);
-      }
+      for (int u = 0; u < 4; ++u) acc[u] = eq16(ra[u][t], b[u], acc[u]);
     }
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
-      const uint32_t c = __reduce_add_sync(FULL, byte_sum(acc[u]));
+      const uint32_t c = __reduce_add_sync(FULL, acc[u]) >> 7;
       if (lane == p + u) mine = c;
     }
   }
@@ -207,7 +211,7 @@ __device__ __forceinline__ void dense_item(const GraphArgs &g, uint64_t *gbuf, i
   uint32_t *mxc = (uint32_t *)(cnt + 32);          // [32]
   uint32_t *sA = (uint32_t *)(smem + (size_t)kWarps * 1024);   // [32][mwq]
 
-  thr[lane] = 0;
+  thr[lane] = g.key_floor;
   cnt[lane] = 0;
   mxc[lane] = 0;
   const size_t bufrow = ((size_t)bx * P + slice) * 32;  // first buffer row of the warp
@@ -245,24 +249,16 @@ __device__ __forceinline__ void dense_item(const GraphArgs &g, uint64_t *gbuf, i
     __syncwarp();
     const uint4 *c0 = ring + (size_t)st * 4 * m4;
     const uint4 *c1 = c0 + m4, *c2 = c1 + m4, *c3 = c2 + m4;
-    uint32_t cntq[4] = {0, 0, 0, 0};
-    for (int t0 = 0; t0 < m4; t0 += 63) {
-      const int t1 = t0 + 63 < m4 ? t0 + 63 : m4;
-      uint32_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+    uint32_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;      // 128 x matches
 #pragma unroll 2
-      for (int t = t0; t < t1; ++t) {
-        const uint4 a = *(const uint4 *)(ra + 4 * t);
-        const uint4 b0 = c0[t], b1 = c1[t], b2 = c2[t], b3 = c3[t];
-        a0 += eq_bytes(a.x, b0.x) + eq_bytes(a.y, b0.y) + eq_bytes(a.z, b0.z) + eq_bytes(a.w, b0.w);
-        a1 += eq_bytes(a.x, b1.x) + eq_bytes(a.y, b1.y) + eq_bytes(a.z, b1.z) + eq_bytes(a.w, b1.w);
-        a2 += eq_bytes(a.x, b2.x) + eq_bytes(a.y, b2.y) + eq_bytes(a.z, b2.z) + eq_bytes(a.w, b2.w);
-        a3 += eq_bytes(a.x, b3.x) + eq_bytes(a.y, b3.y) + eq_bytes(a.z, b3.z) + eq_bytes(a.w, b3.w);
-      }
-      cntq[0] += byte_sum(a0);
-      cntq[1] += byte_sum(a1);
-      cntq[2] += byte_sum(a2);
-      cntq[3] += byte_sum(a3);
+    for (int t = 0; t < m4; ++t) {
+      const uint4 a = *(const uint4 *)(ra + 4 * t);
+      a0 = eq16(a, c0[t], a0);
+      a1 = eq16(a, c1[t], a1);
+      a2 = eq16(a, c2[t], a2);
+      a3 = eq16(a, c3[t], a3);
     }
+    const uint32_t cntq[4] = {a0 >> 7, a1 >> 7, a2 >> 7, a3 >> 7};
     __syncwarp();
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
@@ -431,7 +427,7 @@ __device__ __forceinline__ void tc_item(const GraphArgs &g, uint64_t *gbuf, int3
     }
     __syncthreads();
   }
-  thr[lane] = 0;
+  thr[lane] = g.key_floor;
   cnt[lane] = 0;
   mxc[lane] = 0;
   const size_t bufrow = ((size_t)bx * P + slice) * 32;

@@ -2,6 +2,7 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <cstring>
 #include <memory>
 #include <string>
 #include <vector>
@@ -100,7 +101,25 @@ struct GraphArgs {
   uint32_t *maxcnt_cand = nullptr;     // [n] over candidates
   uint32_t *maxcnt_all = nullptr;      // [n] over all j != i
   unsigned long long *stats = nullptr; // [2] prefiltered, compared
+  // Keys at or below key_floor are never admitted to a row's candidates
+  // (admission_floor()).
+  uint64_t key_floor = 0;
 };
+
+// The lowest key worth keeping: similarity 0.039 with the largest id bits.
+// The calibrated cutoff a graph is cut at is at least 0.040 (the small path's
+// walk stops at p <= 50 after a step of at most 11; the fused path clamps each
+// round to >= 50), and only keys with similarity above the cutoff become
+// edges.  The top-K of the keys above the floor, cut at the cutoff, is the
+// same set as the top-K of all keys cut at the cutoff, so rows skip every
+// pair that could not be an edge.  The row maxima the calibration reads are
+// taken before admission.
+inline uint64_t admission_floor() {
+  const float f = 0.039f;
+  uint32_t bits;
+  std::memcpy(&bits, &f, sizeof(bits));
+  return ((uint64_t)bits << 32) | 0xFFFFFFFFull;
+}
 
 void launch_unit_rows(const GraphArgs &g, cudaStream_t s);
 void launch_colnorm(const GraphArgs &g, double *acc, cudaStream_t s);
