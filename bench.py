@@ -41,6 +41,10 @@ WORKLOAD = dict(workload="binning-scale assembly: 100 genomes, 50000 contigs, S=
                 n_genomes=100, n_contigs=50000, samples=20, sketch_m=500, max_edges=200,
                 inputs_exceed_l2=True, seed=1)
 METRIC = "contig-pairs scored/s"
+# DRAM bytes (read + write) of the all-pairs kernel per ordered pair, from the
+# ncu capture of the 30,000-contig case (profiles/k_allpairs_tc_fused30k.txt),
+# scaled to a launch by its n^2 ordered pairs.
+ALLPAIRS_TRAFFIC_PER_PAIR = None
 UNIT = "pairs/s"
 
 
@@ -208,14 +212,23 @@ def _finish(args, ctx, asm, timings, last, ms, value, result_e2e, clk, world, ra
     import torch.distributed as dist
     peaks, peak_src = _peaks()
     clocks = clk.summary()
-    # dominant kernel: the all-pairs pass (abundance test on every ordered pair,
-    # register compare on the survivors); FP32 FMA/ADD pipe bound
+    n, S, m = asm.n, WORKLOAD["samples"], WORKLOAD["sketch_m"]
+    mpad = (m + 15) // 16 * 16
     ap_ms = last["allpairs_ms"]
-    S = WORKLOAD["samples"]
-    flops = last["pairs_prefiltered"] * (2 * S + 15)        # S FMAs + 15-add reduction tree
-    sm_mhz = clocks["sm_mhz"] or peaks.get("sm_max_mhz", 1965.0)
-    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12       # TFLOP/s at the sampled clock
+    # dominant kernel: the all-pairs pass.  Its tensor-core prefilter multiplies
+    # the FP16 unit rank rows of every ordered pair (2 S FLOPs per pair, n^2
+    # pairs per launch); the register compares of the survivors run on the
+    # integer pipe (pairs_compared x m byte compares).
+    flops = 2.0 * S * n * n
     achieved = flops / (ap_ms / 1000.0) / 1e12 if ap_ms > 0 else 0.0
+    peak = peaks.get("bf16_tflops", 1590.0)
+    traffic = (ALLPAIRS_TRAFFIC_PER_PAIR * n * n
+               if ALLPAIRS_TRAFFIC_PER_PAIR is not None and WORKLOAD["samples"] == 20 else None)
+    # sketch: ASCII read, 2-bit words + invalid mask written and read back,
+    # per-contig 1/w rows written and read, two code rows written
+    nbases = sum(len(q) for q in asm.seqs)
+    sk_ms = last["pack_ms"] + last["count_ms"] + last["sketch_ms"]
+    sk_bytes = nbases * (1.0 + 3.0 / 8.0 + 3.0 / 8.0) + n * (136 * 8 * 2 + 2 * mpad)
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -228,12 +241,22 @@ def _finish(args, ctx, asm, timings, last, ms, value, result_e2e, clk, world, ra
         "pairs_prefiltered": last["pairs_prefiltered"],
         "pairs_compared": last["pairs_compared"],
         "gpu_launches": int(last["kernel_launches"]) * args.steps,
-        "roofline": {"bound": "fp32-alu", "kernel": "k_allpairs",
-                     "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                     "frac": achieved / fp32_peak if fp32_peak else None,
-                     "peak_source": "nominal 148 SM x 128 FP32 lanes x 2 at the sampled SM clock "
-                                    f"(no measured FP32 peak; HBM/bf16 peaks are {peak_src})",
-                     "traffic": None},
+        "roofline": {"bound": "tensor", "kernel": "k_allpairs_tc (FP16 mma prefilter + survivor compare)",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak else None,
+                     "peak_source": f"bf16_tflops of MEASURED_PEAKS.json ({peak_src})",
+                     "work": "2*S*n^2 FLOPs per launch (FP16 products of every ordered pair)",
+                     "traffic": traffic},
+        "int_pipe": {"register_compares_per_s": last["pairs_compared"] * m / (ap_ms / 1000.0)
+                     if ap_ms > 0 else 0.0,
+                     "pairs_compared": last["pairs_compared"],
+                     "note": "ALU-pipe utilisation from ncu is in profiles/"},
+        "sketch": {"contigs_per_s": n / (sk_ms / 1000.0) if sk_ms > 0 else 0.0,
+                   "ms": sk_ms, "bytes": sk_bytes,
+                   "achieved_gbs": sk_bytes / (sk_ms / 1000.0) / 1e9 if sk_ms > 0 else 0.0,
+                   "hbm_peak_gbs": peaks.get("hbm_gbs", 6650.0),
+                   "frac_hbm": (sk_bytes / (sk_ms / 1000.0) / 1e9) / peaks.get("hbm_gbs", 6650.0)
+                   if sk_ms > 0 else 0.0},
         "clocks": clocks,
     }
     if rank == 0 and not args.no_cpu_baseline:
@@ -381,6 +404,116 @@ def run_batch_form(args):
     print(json.dumps(res))
 
 
+def _digest(g):
+    import hashlib
+    h = hashlib.blake2b(digest_size=16)
+    for k in ("src", "dst", "scomp", "score"):
+        h.update(np.ascontiguousarray(g[k]).tobytes())
+    h.update(np.float64([g["b0"], g["sim_cutoff"]]).tobytes())
+    return h.hexdigest()
+
+
+def _serve_trace(srv, pool, trace, warm):
+    """Replay an arrival trace [(t_s, pool index)] open-loop; per-request
+    (latency stats, digest) in trace order, and the time of the last result."""
+    import threading
+    for i in warm:                                    # tables, graphs, buffers
+        b, o, d, p = pool[i]
+        srv.wait(srv.submit(b, o, d, p), timeout=900.0)
+    ids = [None] * len(trace)
+    t0 = time.perf_counter()
+
+    def submitter():
+        for k, (t, i) in enumerate(trace):
+            dt = t0 + t - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            b, o, d, p = pool[i]
+            ids[k] = srv.submit(b, o, d, p)
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    out = []
+    for k in range(len(trace)):
+        while ids[k] is None:
+            time.sleep(0.001)
+        g, st = srv.wait(ids[k], timeout=900.0)
+        out.append((st, _digest(g)))
+    th.join()
+    return out, time.perf_counter() - t0
+
+
+def run_serve_form(args):
+    """Serving form: an open-loop Poisson stream of assemblies at a stated rate
+    through the request loop (rbg_server, requests folded into shared launches),
+    and the same trace through the plain per-request path."""
+    import torch
+    from rabbitbin_b200 import api
+    from rabbitbin_b200.workloads import iter_stream
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    pool, keep, sizes = [], [], []
+    for it in iter_stream(args.pool, seed=4, n_min=500, n_max=200000,
+                          s_choices=tuple(range(3, 31)), m_choices=(250, 500, 1000)):
+        buf, offs = it.asm.concat()
+        sizes.append(it.n)
+        it.asm.seqs = []
+        pin, ptr = _pin(buf)
+        del buf
+        keep.append(pin)
+        pool.append((ptr, offs, it.asm.depth, api.default_params(m=it.m, max_edges=200)))
+    gen_s = time.perf_counter() - t0
+    rng = np.random.default_rng(4)
+    trace, t = [], 0.0
+    while True:
+        t += float(rng.exponential(1.0 / args.rate))
+        if t >= args.duration:
+            break
+        trace.append((t, int(rng.integers(0, len(pool)))))
+    warm = [int(np.argmin(sizes)), int(np.argmax(sizes))]
+    modes = {}
+    for mode in ("batched", "plain"):
+        srv = api.Server(workers=1 if mode == "plain" else args.workers, plain=(mode == "plain"),
+                         hbm_budget=150 << 30, max_batch=64)
+        with ClockSampler(0) as clk:
+            res, wall = _serve_trace(srv, pool, trace, warm)
+        srv.close()
+        lat = np.array([st["latency_ms"] for st, _ in res])
+        contigs = sum(sizes[i] for _, i in trace)
+        # server-side span: first submit to last result of the trace
+        span = max(st["done_s"] for st, _ in res) - min(st["submit_s"] for st, _ in res)
+        modes[mode] = {
+            "graphs_per_s": len(trace) / span, "contigs_per_s": contigs / span,
+            "span_s": span,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "p999_ms": float(np.percentile(lat, 99.9)), "mean_ms": float(lat.mean()),
+            "mean_batch": float(np.mean([st["batch_size"] for st, _ in res])),
+            "max_batch": int(max(st["batch_size"] for st, _ in res)),
+            "wall_s": wall, "clocks": clk.summary(), "digests": [d for _, d in res]}
+    identical = modes["batched"]["digests"] == modes["plain"]["digests"]
+    for m in modes.values():
+        m.pop("digests")
+    b = modes["batched"]
+    res = {
+        "metric": f"served graphs/s (Poisson {args.rate:g} req/s)", "value": b["graphs_per_s"],
+        "unit": "graphs/s", "n_gpus": 1, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8/u32 register codes, f64 sketch, f32 abundance",
+        "data": "synthetic (seeded order-3 Markov genomes, lognormal coverage)",
+        "config": {"workload": f"open-loop Poisson arrivals at {args.rate:g} req/s for "
+                               f"{args.duration:g} s; assemblies from a pool of {len(pool)} drawn "
+                               "with contigs log-uniform [500, 2e5], S in 3..30, sketch-m in "
+                               "{250,500,1000}, max-edges 200; HBM budget 150 GB",
+                   "workers": args.workers,
+                   "requests": len(trace), "pool_contigs": sizes,
+                   "inputs": "pinned host memory, copies inside each request"},
+        "latency_ms": {"p50": b["p50_ms"], "p99": b["p99_ms"], "p999": b["p999_ms"]},
+        "batched": b, "plain": modes["plain"],
+        "graphs_per_s_vs_plain": b["graphs_per_s"] / modes["plain"]["graphs_per_s"],
+        "outputs_identical": bool(identical), "generate_s": gen_s,
+    }
+    print(json.dumps(res))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -393,15 +526,22 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--contigs", type=int, default=0, help="profiling: fewer contigs")
     ap.add_argument("--samples", type=int, default=0, help="profiling: other S")
-    ap.add_argument("--form", default="plain", choices=["plain", "batch"],
-                    help="plain: the binning-scale assembly; batch: a mixed stream per call")
+    ap.add_argument("--form", default="plain", choices=["plain", "batch", "serve"],
+                    help="plain: the binning-scale assembly; batch: a mixed stream per call; "
+                         "serve: a Poisson request stream through the request loop")
     ap.add_argument("--batch-size", type=int, default=64, help="batch form: assemblies")
+    ap.add_argument("--rate", type=float, default=20.0, help="serve form: requests per second")
+    ap.add_argument("--duration", type=float, default=10.0, help="serve form: seconds of arrivals")
+    ap.add_argument("--pool", type=int, default=32, help="serve form: distinct assemblies")
+    ap.add_argument("--workers", type=int, default=2, help="serve form: concurrent batches")
     args = ap.parse_args()
     _apply_size(args)
     if args.impl == "reference":
         run_reference(args)
     elif args.form == "batch":
         run_batch_form(args)
+    elif args.form == "serve":
+        run_serve_form(args)
     else:
         run_b200(args)
 

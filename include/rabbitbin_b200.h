@@ -176,6 +176,56 @@ typedef struct rbg_batch_stats {
 int rbg_bin_batch(rbg_ctx *ctx, const rbg_params *defaults, const rbg_assembly *asms,
                   int32_t n_asm, rbg_graph *out, rbg_batch_stats *stats);
 
+/* ── serving: a request loop over a stream of assemblies ──────────────────
+ * No counterpart in the reference.  Requests are queued on submit; worker
+ * threads (one device context each) take every queued request that fits
+ * their share of the HBM budget and run them as one batch (rbg_bin_batch),
+ * so requests that arrive while others are on the GPU are folded into the
+ * next launch, and the workers' batches overlap on the device.  Each result
+ * equals rbg_bin_graph on that assembly alone. */
+typedef struct rbg_server rbg_server;
+
+typedef struct rbg_server_config {
+  int32_t device;              /* CUDA device                                   */
+  int32_t workers;             /* concurrent batches (contexts); 0 -> 2         */
+  int64_t hbm_budget;          /* bytes of device memory for request state;
+                                  0 -> 150 GB, capped at the free memory        */
+  int32_t max_batch;           /* assemblies folded into one launch; 0 -> 64    */
+  int32_t plain;               /* 1: one rbg_bin_graph call per request, one
+                                  worker (the unbatched comparison path)        */
+  int64_t max_batch_pairs;     /* fold requests while the batch's contig pairs
+                                  stay below this (a larger request runs alone);
+                                  0 -> 2e9                                      */
+} rbg_server_config;
+
+typedef struct rbg_request_stats {
+  double queue_ms;             /* submit -> start of its batch                  */
+  double service_ms;           /* start of its batch -> result                  */
+  double latency_ms;           /* submit -> result                              */
+  int32_t batch_size;          /* assemblies in the batch it ran in             */
+  int32_t worker;
+  int64_t est_bytes;           /* device bytes reserved for it at admission     */
+  double submit_s;             /* submit time, seconds since rbg_server_create  */
+  double done_s;               /* result time, seconds since rbg_server_create  */
+} rbg_request_stats;
+
+int rbg_server_create(const rbg_server_config *cfg, const rbg_params *defaults,
+                      rbg_server **out);
+/* Queue one assembly.  The arrays a->seqcat, a->offsets and a->depth must stay
+ * valid until rbg_server_wait returns for this request; a->params (if set) is
+ * copied.  Validation errors are returned here. */
+int rbg_server_submit(rbg_server *srv, const rbg_assembly *a, int64_t *request_id);
+/* Wait up to timeout_s seconds (< 0: forever) for a request's graph.  Returns
+ * RBG_ERR_TIMEOUT if it is not done yet (it stays queued), else the request's
+ * status; on RBG_OK *out owns the edges (free with rbg_free_graph).  A request
+ * can be waited for once after it completes.  `stats` may be NULL. */
+int rbg_server_wait(rbg_server *srv, int64_t request_id, double timeout_s, rbg_graph *out,
+                    rbg_request_stats *stats);
+/* Last error message of the server (submit-time validation, device errors). */
+const char *rbg_server_last_error(rbg_server *srv);
+/* Stops accepting work, finishes queued requests, frees the contexts. */
+int rbg_server_destroy(rbg_server *srv);
+
 /* Device-resident form used by batching, serving and the benchmark: stage the
  * inputs once (host -> device), run the hot path on them any number of times,
  * then fetch the graph (device -> host). */

@@ -74,6 +74,20 @@ class BatchStats(C.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_ if n != "reserved"}
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("workers", C.c_int32), ("hbm_budget", C.c_int64),
+                ("max_batch", C.c_int32), ("plain", C.c_int32), ("max_batch_pairs", C.c_int64)]
+
+
+class RequestStats(C.Structure):
+    _fields_ = [("queue_ms", C.c_double), ("service_ms", C.c_double), ("latency_ms", C.c_double),
+                ("batch_size", C.c_int32), ("worker", C.c_int32), ("est_bytes", C.c_int64),
+                ("submit_s", C.c_double), ("done_s", C.c_double)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -111,6 +125,11 @@ def lib():
                                    P(C.c_uint32)], C.c_int),
         "rbg_bin_batch": ([vp, P(Params), P(Assembly), C.c_int32, P(Graph), P(BatchStats)],
                           C.c_int),
+        "rbg_server_create": ([P(ServerConfig), P(Params), P(vp)], C.c_int),
+        "rbg_server_submit": ([vp, P(Assembly), P(C.c_int64)], C.c_int),
+        "rbg_server_wait": ([vp, C.c_int64, C.c_double, P(Graph), P(RequestStats)], C.c_int),
+        "rbg_server_last_error": ([vp], C.c_char_p),
+        "rbg_server_destroy": ([vp], C.c_int),
         "rbg_build_pmh_winners_noalloc": ([P(Params), vp, vp, C.c_int64, C.c_int64, vp, vp,
                                            C.c_char_p, C.c_size_t], C.c_int),
     }
@@ -297,3 +316,70 @@ class Context:
         finally:
             for i in range(nb):
                 self._L.rbg_free_graph(C.byref(outs[i]))
+
+
+class Server:
+    """Request loop of the serving form (rbg_server_*): submit assemblies as
+    they arrive, wait for their graphs.  Arrays passed to submit are kept
+    alive here until their request has been waited for."""
+
+    def __init__(self, device=0, workers=2, hbm_budget=0, max_batch=64, plain=False,
+                 params=None, max_batch_pairs=0):
+        self._L = lib()
+        cfg = ServerConfig(device, workers, int(hbm_budget), max_batch, 1 if plain else 0,
+                           int(max_batch_pairs))
+        h = C.c_void_p()
+        p = params or default_params()
+        rc = self._L.rbg_server_create(C.byref(cfg), C.byref(p), C.byref(h))
+        if rc != RBG_OK:
+            raise RbgError(rc, "cannot create the server")
+        self._h = h
+        self._keep = {}
+
+    def _check(self, rc, what):
+        if rc != RBG_OK:
+            raise RbgError(rc, f"{what}: {self._L.rbg_server_last_error(self._h).decode()}")
+
+    def submit(self, seqcat, offsets, depth, params=None):
+        offs = np.ascontiguousarray(offsets, np.int64)
+        n = len(offs) - 1
+        dep = np.ascontiguousarray(depth, np.float32)
+        S = dep.shape[1] if dep.ndim == 2 else (dep.size // n if n > 0 else 0)
+        d = dep.reshape(n, S)
+        a = Assembly()
+        a.seqcat = seqcat
+        a.offsets = _p(offs, C.c_int64)
+        a.n = n
+        a.depth = _p(d, C.c_float) if d.size else None
+        a.S = S
+        a.params = C.pointer(params) if params is not None else None
+        rid = C.c_int64()
+        self._check(self._L.rbg_server_submit(self._h, C.byref(a), C.byref(rid)), "submit")
+        self._keep[rid.value] = (seqcat, offs, d, params)
+        return rid.value
+
+    def wait(self, rid, timeout=-1.0):
+        """(graph dict, stats dict); raises RbgError (code -5) on timeout."""
+        g = Graph()
+        st = RequestStats()
+        rc = self._L.rbg_server_wait(self._h, rid, float(timeout), C.byref(g), C.byref(st))
+        if rc == -5:
+            raise RbgError(rc, f"request {rid} not finished")
+        self._keep.pop(rid, None)
+        self._check(rc, f"request {rid}")
+        try:
+            return _graph_dict(g), st.as_dict()
+        finally:
+            self._L.rbg_free_graph(C.byref(g))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.rbg_server_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -137,6 +137,40 @@ inline size_t up256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 }  // namespace
 
+void validate_assembly(const rbg_assembly &x, const rbg_params *p, const std::string &who) {
+  validate_params(p);
+  if (x.n < 0 || (x.n > 0 && (!x.offsets || !x.seqcat)))
+    throw Error(RBG_ERR_ARG, who + "bad sequence arguments");
+  if (x.S < 0 || x.S > kMaxS) throw Error(RBG_ERR_UNSUPPORTED, who + "S must be in 0..64");
+  if (x.S > 0 && x.n > 0 && !x.depth) throw Error(RBG_ERR_ARG, who + "depth is null");
+  if (x.n >= (1 << 27)) throw Error(RBG_ERR_UNSUPPORTED, who + "at most 2^27 - 1 contigs");
+  if (x.n > 0 && x.offsets[0] != 0) throw Error(RBG_ERR_ARG, who + "offsets[0] must be 0");
+  for (int64_t q = 0; q < x.n; ++q)
+    if (x.offsets[q + 1] < x.offsets[q])
+      throw Error(RBG_ERR_ARG, who + "offsets must be non-decreasing");
+  const bool fused = (p->force_path == 2) || (p->force_path == 0 && x.n > 25000);
+  if (fused && x.n <= 2500)
+    throw Error(RBG_ERR_ARG, who + "the fused path samples 2500 contigs; need n > 2500");
+}
+
+int64_t batch_request_bytes(const rbg_params *p, int64_t n, int64_t nbases, int S) {
+  const int m = p->m, mpad = mpad_of(m), K = p->max_edges;
+  const int Su = (std::max(S, 1) + 3) & ~3, Kp = unit16_stride(S);
+  const int E = p->k == 4 ? 136 : (p->k == 3 ? 32 : (p->k == 2 ? 10 : 2));
+  const double w_comp = (p->w_comp < 0.0) ? (S <= 2 ? 1.0 : 0.0) : p->w_comp;
+  const bool fused = (p->force_path == 2) || (p->force_path == 0 && n > 25000);
+  const bool abd = fused && p->abdfirst && S > 1 && w_comp < 1.0 && w_comp < p->min_edge;
+  const int P = batch_slices(n, K, abd ? Kp / 16 : 0);
+  const int64_t cap = allpairs_cap(K);
+  int64_t b = nbases + nbases / 4 + nbases / 8 + 64;             // ASCII, 2-bit words, mask
+  b += n * (int64_t)(S * 4 + 8 + E * 8 + 4 + 2 * mpad + Su * 4 + Kp * 2 + 1);
+  b += n * (int64_t)K * (8 + 4 + 4) + n * 32;                    // top-K, neighbour lists
+  b += ((n + 31) / 32) * P * 32 * (cap * 8 + 4);                 // slice candidate buffers
+  b += n * (int64_t)K / 2 * 16;                                   // edge arrays (bound)
+  b += 30000 * 12 + (m + 1) * 4 + 4096;                          // b0 pairs, tables of sv
+  return b;
+}
+
 void release_batch_graphs(rbg_ctx *c) {
   std::lock_guard<std::mutex> lk(g_graph_mu);
   auto it = g_graphs.find(c);
@@ -167,17 +201,7 @@ void plan_batch(const rbg_params *defaults, const rbg_assembly *asms, int nb, Ba
     a.orig = i;
     a.in = &x;
     a.p = x.params ? x.params : defaults;
-    validate_params(a.p);
-    const std::string who = "assembly " + std::to_string(i) + ": ";
-    if (x.n < 0 || (x.n > 0 && (!x.offsets || !x.seqcat)))
-      throw Error(RBG_ERR_ARG, who + "bad sequence arguments");
-    if (x.S < 0 || x.S > kMaxS) throw Error(RBG_ERR_UNSUPPORTED, who + "S must be in 0..64");
-    if (x.S > 0 && x.n > 0 && !x.depth) throw Error(RBG_ERR_ARG, who + "depth is null");
-    if (x.n >= (1 << 27)) throw Error(RBG_ERR_UNSUPPORTED, who + "at most 2^27 - 1 contigs");
-    if (x.n > 0 && x.offsets[0] != 0) throw Error(RBG_ERR_ARG, who + "offsets[0] must be 0");
-    for (int64_t q = 0; q < x.n; ++q)
-      if (x.offsets[q + 1] < x.offsets[q])
-        throw Error(RBG_ERR_ARG, who + "offsets must be non-decreasing");
+    validate_assembly(x, a.p, "assembly " + std::to_string(i) + ": ");
     a.n = x.n;
     a.nbases = x.n > 0 ? x.offsets[x.n] : 0;
     a.S = x.S;
@@ -189,8 +213,6 @@ void plan_batch(const rbg_params *defaults, const rbg_assembly *asms, int nb, Ba
     a.E = a.p->k == 4 ? 136 : (a.p->k == 3 ? 32 : (a.p->k == 2 ? 10 : 2));
     a.w_comp = (a.p->w_comp < 0.0) ? (a.S <= 2 ? 1.0 : 0.0) : a.p->w_comp;
     a.fused = (a.p->force_path == 2) || (a.p->force_path == 0 && a.n > 25000);
-    if (a.fused && a.n <= 2500)
-      throw Error(RBG_ERR_ARG, who + "the fused path samples 2500 contigs; need n > 2500");
     a.abdfirst = a.fused && a.p->abdfirst && a.S > 1 && a.w_comp < 1.0 && a.w_comp < a.p->min_edge;
     a.variant = a.abdfirst ? a.Kp / 16 : 0;
     a.P = batch_slices(a.n, a.K, a.variant);

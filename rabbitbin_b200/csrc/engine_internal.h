@@ -32,17 +32,29 @@ struct Error : std::runtime_error {
                          std::string(#x) + ": " + cudaGetErrorString(e_));        \
   } while (0)
 
-// A growable device allocation.
+// A growable device allocation.  It grows by at least half its size, so a
+// stream of growing requests reallocates (cudaFree synchronises the device)
+// only a logarithmic number of times.
 struct DBuf {
   void *p = nullptr;
   size_t cap = 0;
   template <typename T> T *as() const { return (T *)p; }
   void ensure(size_t bytes) {
     if (bytes <= cap) return;
+    const size_t grown = cap + cap / 2;
     if (p) cudaFree(p);
     p = nullptr;
     cap = 0;
-    const size_t want = bytes < 256 ? 256 : bytes;
+    size_t want = bytes < 256 ? 256 : bytes;
+    if (grown > want) {
+      // fall back to the exact size when the grown one does not fit
+      if (cudaMalloc(&p, grown) == cudaSuccess) {
+        cap = grown;
+        return;
+      }
+      cudaGetLastError();
+      p = nullptr;
+    }
     CK(cudaMalloc(&p, want));
     cap = want;
   }
@@ -161,6 +173,13 @@ void validate_params(const rbg_params *p);
 
 // Frees the CUDA graphs the batch engine keeps for a context.
 void release_batch_graphs(rbg_ctx *c);
+
+// Device bytes the batch engine needs for one assembly (its share of every
+// batch buffer; a bound on the edge arrays).
+int64_t batch_request_bytes(const rbg_params *p, int64_t n, int64_t nbases, int S);
+
+// Validation of one assembly's arguments (the checks rbg_bin_batch makes).
+void validate_assembly(const rbg_assembly &x, const rbg_params *p, const std::string &who);
 
 }  // namespace rbg
 
