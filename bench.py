@@ -44,7 +44,7 @@ METRIC = "contig-pairs scored/s"
 # DRAM bytes (read + write) of the all-pairs kernel per ordered pair, from the
 # ncu capture of the 30,000-contig case (profiles/k_allpairs_tc_fused30k.txt),
 # scaled to a launch by its n^2 ordered pairs.
-ALLPAIRS_TRAFFIC_PER_PAIR = None
+ALLPAIRS_TRAFFIC_PER_PAIR = 0.147
 UNIT = "pairs/s"
 
 

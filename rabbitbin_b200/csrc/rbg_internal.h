@@ -108,9 +108,9 @@ struct GraphArgs {
 
 // The lowest key worth keeping: similarity 0.039 with the largest id bits.
 // The calibrated cutoff a graph is cut at is at least 0.040 (the small path's
-// walk stops at p <= 50 after a step of at most 11; the fused path clamps each
-// round to >= 50), and only keys with similarity above the cutoff become
-// edges.  The top-K of the keys above the floor, cut at the cutoff, is the
+// walk stops at p <= RB_SIM_FLOOR = 50 after a step of at most 11,
+// src/impl/rb_graph.cpp:395-415; the fused path clamps each round to >= 50,
+// :1248-1252), and only keys with similarity above the cutoff become edges.  The top-K of the keys above the floor, cut at the cutoff, is the
 // same set as the top-K of all keys cut at the cutoff, so rows skip every
 // pair that could not be an edge.  The row maxima the calibration reads are
 // taken before admission.
