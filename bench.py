@@ -48,11 +48,6 @@ ALLPAIRS_TRAFFIC_PER_PAIR = 0.147
 UNIT = "pairs/s"
 
 
-def _env_rank():
-    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
-            int(os.environ.get("LOCAL_RANK", "0")))
-
-
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
@@ -129,15 +124,14 @@ def _apply_size(args):
 
 def run_b200(args):
     import torch
-    import torch.distributed as dist
     from rabbitbin_b200 import api
 
-    rank, world, local = _env_rank()
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    from rabbitbin_b200 import shard
+    rank, world, local = shard.env_rank()
+    shard.init(world, "nccl")
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    asm = _assembly(WORKLOAD["seed"] + rank)
+    asm = _assembly(shard.shard_seed(WORKLOAD["seed"], rank))
     buf, offs = asm.concat()
     n = asm.n
     pairs = n * (n - 1) // 2
@@ -145,8 +139,7 @@ def run_b200(args):
     ctx = api.Context(local)
 
     def barrier():
-        if world > 1:
-            dist.barrier()
+        shard.barrier(world)
         torch.cuda.synchronize(dev)
 
     # ── device-resident value ───────────────────────────────────────────────
@@ -163,12 +156,8 @@ def run_b200(args):
             timings.append(ctx.run_resident(params))
         end.record(ext)
         barrier()
-    ms = start.elapsed_time(end) / args.steps
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * pairs / (ms / 1000.0)
+    ms = shard.max_over_ranks(start.elapsed_time(end) / args.steps, world, dev)
+    value = shard.whole_job_rate(pairs, world, ms / 1000.0)
 
     # ── end to end through rbg_bin_graph with pinned host inputs ────────────
     e2e_ms, e2e_edges = float("nan"), 0
@@ -186,7 +175,6 @@ def run_b200(args):
 
 def _e2e(args, ctx, buf, offs, asm, params, barrier, world, dev):
     import torch
-    import torch.distributed as dist
     pin_seq = torch.empty(len(buf), dtype=torch.uint8, pin_memory=True)
     pin_seq.numpy()[:] = np.frombuffer(buf, dtype=np.uint8)
     pin_depth = torch.empty(asm.depth.shape, dtype=torch.float32, pin_memory=True)
@@ -200,16 +188,12 @@ def _e2e(args, ctx, buf, offs, asm, params, barrier, world, dev):
         g = ctx.bin_graph(seq_ptr, offs, pin_depth.numpy(), params)
         e2e_edges = len(g["src"])
     barrier()
-    e2e_ms = (time.perf_counter() - t0) * 1000.0 / args.steps
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    from rabbitbin_b200 import shard
+    e2e_ms = shard.max_over_ranks((time.perf_counter() - t0) * 1000.0 / args.steps, world, dev)
     return e2e_ms, e2e_edges
 
 
 def _finish(args, ctx, asm, timings, last, ms, value, result_e2e, clk, world, rank, dev):
-    import torch.distributed as dist
     peaks, peak_src = _peaks()
     clocks = clk.summary()
     n, S, m = asm.n, WORKLOAD["samples"], WORKLOAD["sketch_m"]
@@ -262,9 +246,8 @@ def _finish(args, ctx, asm, timings, last, ms, value, result_e2e, clk, world, ra
     if rank == 0 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(asm, seconds=args.cpu_seconds)
     ctx.close()
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    from rabbitbin_b200 import shard
+    shard.finish(world)
     if rank == 0:
         print(json.dumps(result))
 
@@ -292,7 +275,8 @@ def cpu_baseline(asm, seconds=20.0):
 
 
 def run_reference(args):
-    rank, world, _ = _env_rank()
+    from rabbitbin_b200 import shard
+    rank, world, _ = shard.env_rank()
     if rank != 0:
         return
     import oracle
