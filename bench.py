@@ -106,10 +106,17 @@ def _peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
 
 
+LARGE = dict(workload="large single assembly: 300 genomes, 300000 contigs, S=30 with 10% of "
+                       "genomes absent per sample, sketch-m 500, max-edges 200, fused path",
+             n_genomes=300, n_contigs=300000, samples=30, sketch_m=500, max_edges=200,
+             inputs_exceed_l2=True, seed=3, absent_frac=0.1)
+
+
 def _assembly(seed):
     from rabbitbin_b200.synth import make_assembly
     w = WORKLOAD
-    return make_assembly(w["n_genomes"], w["n_contigs"], w["samples"], seed=seed)
+    return make_assembly(w["n_genomes"], w["n_contigs"], w["samples"], seed=seed,
+                         absent_frac=w.get("absent_frac", 0.0))
 
 
 def _apply_size(args):
@@ -514,11 +521,16 @@ def main():
                     help="plain: the binning-scale assembly; batch: a mixed stream per call; "
                          "serve: a Poisson request stream through the request loop")
     ap.add_argument("--batch-size", type=int, default=64, help="batch form: assemblies")
+    ap.add_argument("--config", default="binning", choices=["binning", "large"],
+                    help="binning: 50,000 contigs, S=20 (default); large: 300,000 contigs, S=30")
     ap.add_argument("--rate", type=float, default=20.0, help="serve form: requests per second")
     ap.add_argument("--duration", type=float, default=10.0, help="serve form: seconds of arrivals")
     ap.add_argument("--pool", type=int, default=32, help="serve form: distinct assemblies")
     ap.add_argument("--workers", type=int, default=2, help="serve form: concurrent batches")
     args = ap.parse_args()
+    if args.config == "large":
+        WORKLOAD.clear()
+        WORKLOAD.update(LARGE)
     _apply_size(args)
     if args.impl == "reference":
         run_reference(args)

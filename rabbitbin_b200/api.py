@@ -177,12 +177,42 @@ def stream_tables(k=4, m=500, pmh_seed=42, fp_contract=1):
     return codes, U, W
 
 
-def _graph_dict(g):
+class _GraphMem:
+    """Owns one rbg_graph's library-allocated arrays; frees them when the
+    last array viewing them is gone."""
+
+    def __init__(self, L, g):
+        self._L, self.g = L, g
+
+    def __del__(self):
+        try:
+            self._L.rbg_free_graph(C.byref(self.g))
+        except Exception:
+            pass
+
+
+class _View:
+    """Array interface over library memory, keeping its owner alive."""
+
+    def __init__(self, owner, addr, n, typestr):
+        self.owner = owner
+        self.__array_interface__ = {"shape": (n,), "typestr": typestr,
+                                    "data": (addr, False), "version": 3}
+
+
+def _graph_dict(L, g):
+    """The graph's arrays as numpy views of the library's buffers (no copy);
+    the buffers are released with rbg_free_graph when the views are gone."""
     ne = g.n_edges
-    take = (lambda ptr, dt: np.ctypeslib.as_array(ptr, (ne,)).astype(dt, copy=True)
-            if ne else np.zeros(0, dt))
-    return dict(src=take(g.from_, np.uint32), dst=take(g.to, np.uint32),
-                scomp=take(g.scomp, np.float32), score=take(g.score, np.float32),
+    owner = _GraphMem(L, g)
+
+    def view(ptr, typestr, dt):
+        if ne == 0:
+            return np.zeros(0, dt)
+        return np.asarray(_View(owner, C.cast(ptr, C.c_void_p).value, ne, typestr))
+
+    return dict(src=view(g.from_, "<u4", np.uint32), dst=view(g.to, "<u4", np.uint32),
+                scomp=view(g.scomp, "<f4", np.float32), score=view(g.score, "<f4", np.float32),
                 b0=g.b0, sim_cutoff=g.sim_cutoff, path=g.path)
 
 
@@ -245,10 +275,7 @@ class Context:
     def _graph_call(self, fn, *args):
         g = Graph()
         self._check(fn(*args, C.byref(g)), fn.__name__)
-        try:
-            return _graph_dict(g)
-        finally:
-            self._L.rbg_free_graph(C.byref(g))
+        return _graph_dict(self._L, g)
 
     def build_graph(self, winners32, depth, params=None):
         p = params or default_params()
@@ -311,11 +338,12 @@ class Context:
         st = BatchStats()
         self._check(self._L.rbg_bin_batch(self._h, C.byref(dflt), arr, nb, outs, C.byref(st)),
                     "bin_batch")
-        try:
-            return [_graph_dict(outs[i]) for i in range(nb)], st.as_dict()
-        finally:
-            for i in range(nb):
-                self._L.rbg_free_graph(C.byref(outs[i]))
+        graphs = []
+        for i in range(nb):
+            g = Graph()
+            C.pointer(g)[0] = outs[i]
+            graphs.append(_graph_dict(self._L, g))
+        return graphs, st.as_dict()
 
 
 class Server:
@@ -367,10 +395,7 @@ class Server:
             raise RbgError(rc, f"request {rid} not finished")
         self._keep.pop(rid, None)
         self._check(rc, f"request {rid}")
-        try:
-            return _graph_dict(g), st.as_dict()
-        finally:
-            self._L.rbg_free_graph(C.byref(g))
+        return _graph_dict(self._L, g), st.as_dict()
 
     def close(self):
         if getattr(self, "_h", None):

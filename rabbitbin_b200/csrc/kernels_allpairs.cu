@@ -35,6 +35,26 @@ constexpr unsigned FULL = 0xffffffffu;
 constexpr int kWarps = 4;         // warps per CTA (independent)
 constexpr int kCapW = 16;         // candidate buffer <= 32 * kCapW keys per row
 
+// One 16-byte shared-memory load (a single 128-bit access: lanes reading
+// consecutive 16-byte blocks take 4 wavefronts for the warp, where four 32-bit
+// loads of the same blocks would conflict 4-way each).  Volatile, so it stays
+// ordered after the cp.async waits and warp barriers around it.
+__device__ __forceinline__ uint4 lds128(const void *p) {
+  uint4 v;
+  const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+  asm volatile("ld.shared.v4.u32 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "r"(a));
+  return v;
+}
+
+// Row stride (floats) of the unit rows staged in shared memory: an odd number
+// of 16-byte units, so lanes gathering rows of random indices spread over all
+// eight 16-byte bank groups.
+__host__ __device__ __forceinline__ int su_stride(int Su) {
+  return ((Su >> 2) & 1) ? Su : Su + 4;
+}
+
 // 0x80 in each byte where a and b agree, 0 elsewhere: the low seven bits of
 // each byte of a ^ b are tested by an add that cannot carry out of the byte,
 // the top bit directly.
@@ -46,7 +66,7 @@ __device__ __forceinline__ uint32_t eq_mask(uint32_t a, uint32_t b) {
 // acc + 128 x (number of equal bytes of two 16-byte blocks); the byte dot
 // product with 0x01010101 sums the masks on the FMA pipe, beside the ALU
 // work of the masks.
-__device__ __forceinline__ uint32_t eq16(const uint4 &a, const uint4 &b, uint32_t acc) {
+__device__ __forceinline__ uint32_t eq16(const uint4 a, const uint4 b, uint32_t acc) {
   acc = __dp4a(eq_mask(a.x, b.x), 0x01010101u, acc);
   acc = __dp4a(eq_mask(a.y, b.y), 0x01010101u, acc);
   acc = __dp4a(eq_mask(a.z, b.z), 0x01010101u, acc);
@@ -166,7 +186,7 @@ __device__ __forceinline__ void count_batch_coop(const GraphArgs &g, Warp &w, co
 #pragma unroll
       for (int u = 0; u < 4; ++u) b[u] = __ldg(cb[u] + t);
 #pragma unroll
-      for (int u = 0; u < 4; ++u) acc[u] = eq16(ra[u][t], b[u], acc[u]);
+      for (int u = 0; u < 4; ++u) acc[u] = eq16(lds128(ra[u] + t), b[u], acc[u]);
     }
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
@@ -174,15 +194,25 @@ __device__ __forceinline__ void count_batch_coop(const GraphArgs &g, Warp &w, co
       if (lane == p + u) mine = c;
     }
   }
+  // Row maxima and admission.  The row state is this warp's own, so lanes of
+  // the same row combine in registers and one of them writes: no shared-memory
+  // atomics, which serialise when survivors share a row.
+  const unsigned act = __ballot_sync(FULL, lane < nq);
   if (lane < nq) {
     const unsigned e = (unsigned)q[lane];
     const int r = (int)(e >> 27);
     const int64_t j = e & 0x07FFFFFFu;
-    atomicMax(&w.mxc[r], mine);
+    const unsigned grp = __match_any_sync(act, r);
+    const uint32_t mx = __reduce_max_sync(grp, mine);
     const uint64_t key = ((uint64_t)__ldg(g.sv_bits + mine) << 32) | (uint64_t)(~(uint32_t)j);
-    if (key > w.thr[r]) {
-      const int p = atomicAdd(&w.cnt[r], 1);
-      w.gbuf[(size_t)r * w.cap + p] = key;
+    const bool adm = key > w.thr[r];
+    const unsigned ag = grp & __ballot_sync(act, adm);
+    const int base = w.cnt[r];
+    if (adm) w.gbuf[(size_t)r * w.cap + base + __popc(ag & ((1u << lane) - 1u))] = key;
+    __syncwarp(act);
+    if (lane == __ffs(grp) - 1) {
+      if (mx > w.mxc[r]) w.mxc[r] = mx;
+      w.cnt[r] = base + __popc(ag);
     }
   }
   __syncwarp();
@@ -252,11 +282,11 @@ __device__ __forceinline__ void dense_item(const GraphArgs &g, uint64_t *gbuf, i
     uint32_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;      // 128 x matches
 #pragma unroll 2
     for (int t = 0; t < m4; ++t) {
-      const uint4 a = *(const uint4 *)(ra + 4 * t);
-      a0 = eq16(a, c0[t], a0);
-      a1 = eq16(a, c1[t], a1);
-      a2 = eq16(a, c2[t], a2);
-      a3 = eq16(a, c3[t], a3);
+      const uint4 a = lds128(ra + 4 * t);
+      a0 = eq16(a, lds128(c0 + t), a0);
+      a1 = eq16(a, lds128(c1 + t), a1);
+      a2 = eq16(a, lds128(c2 + t), a2);
+      a3 = eq16(a, lds128(c3 + t), a3);
     }
     const uint32_t cntq[4] = {a0 >> 7, a1 >> 7, a2 >> 7, a3 >> 7};
     __syncwarp();
@@ -344,7 +374,7 @@ __device__ __forceinline__ void check_batch(const GraphArgs &g, Warp &w, const i
                                             unsigned head, int nq, int64_t row0, int *q,
                                             int &qn, float lo, float hi,
                                             unsigned long long &n_cmp, const float *sU,
-                                            const unsigned char *sA) {
+                                            int SuP, const unsigned char *sA) {
   const int lane = threadIdx.x & 31;
   const bool act = lane < nq;
   const unsigned e = act ? (unsigned)cq[(head + lane) & (kCQ - 1)] : 0u;
@@ -354,7 +384,7 @@ __device__ __forceinline__ void check_batch(const GraphArgs &g, Warp &w, const i
   bool pass = false;
   if (act && j != row && (__ldg(g.anynz + row) | __ldg(g.anynz + j))) {
     const int Su = g.Su;
-    const float4 *ua = (const float4 *)(sU + r * Su);
+    const float4 *ua = (const float4 *)(sU + r * SuP);
     const float4 *ub = (const float4 *)(g.unit + j * Su);
     float ur[SMAX];
     float c1 = 0.f;
@@ -411,6 +441,7 @@ __device__ __forceinline__ void tc_item(const GraphArgs &g, uint64_t *gbuf, int3
   // the block's 32 rows: register codes [32][mpad] and unit rows [32][Su]
   unsigned char *sA = rings + (size_t)kWarps * 2 * kTCT * cstride;
   float *sU = (float *)(sA + (size_t)32 * g.mpad);
+  const int SuP = su_stride(g.Su);
   {
     const int m16 = g.mpad >> 4, s4 = g.Su >> 2;
     for (int i = threadIdx.x; i < 32 * m16; i += blockDim.x) {
@@ -423,7 +454,7 @@ __device__ __forceinline__ void tc_item(const GraphArgs &g, uint64_t *gbuf, int3
       const int r = i / s4, t = i - r * s4;
       float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
       if (row0 + r < n) v = __ldg((const float4 *)(g.unit + (row0 + r) * g.Su) + t);
-      *((float4 *)(sU + (size_t)r * g.Su) + t) = v;
+      *((float4 *)(sU + (size_t)r * SuP) + t) = v;
     }
     __syncthreads();
   }
@@ -523,7 +554,7 @@ __device__ __forceinline__ void tc_item(const GraphArgs &g, uint64_t *gbuf, int3
         tail += (unsigned)total;
         __syncwarp();
         while (tail - head >= 32) {
-          check_batch<SMAX>(g, w, cq, head, 32, row0, q, qn, lo, hi, n_cmp, sU, sA);
+          check_batch<SMAX>(g, w, cq, head, 32, row0, q, qn, lo, hi, n_cmp, sU, SuP, sA);
           head += 32;
         }
       }
@@ -532,7 +563,7 @@ __device__ __forceinline__ void tc_item(const GraphArgs &g, uint64_t *gbuf, int3
   }
   while (tail != head) {
     const int nq = (int)(tail - head < 32 ? tail - head : 32);
-    check_batch<SMAX>(g, w, cq, head, nq, row0, q, qn, lo, hi, n_cmp, sU, sA);
+    check_batch<SMAX>(g, w, cq, head, nq, row0, q, qn, lo, hi, n_cmp, sU, SuP, sA);
     head += (unsigned)nq;
   }
   if (qn > 0) {
@@ -661,7 +692,8 @@ size_t dense_smem(int mpad) {
 
 size_t tc_smem(int KS, int mpad, int Su) {
   return (size_t)kWarps * 1024 + (size_t)kWarps * kCQ * 4 +
-         (size_t)kWarps * 2 * kTCT * (KS * 16 * 2 + 16) + (size_t)32 * mpad + (size_t)32 * Su * 4;
+         (size_t)kWarps * 2 * kTCT * (KS * 16 * 2 + 16) + (size_t)32 * mpad +
+         (size_t)32 * su_stride(Su) * 4;
 }
 
 }  // namespace
