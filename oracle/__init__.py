@@ -145,3 +145,59 @@ def sorted_edges(res):
     order = np.lexsort((res["dst"], res["src"]))
     return (res["src"][order], res["dst"][order], res["scomp"][order],
             res["score"][order])
+
+
+class _RefFasta(C.Structure):
+    _fields_ = [("num_seqs", C.c_int64), ("n_large", C.c_int64), ("n_small", C.c_int64),
+                ("names", C.c_void_p), ("name_off", C.POINTER(C.c_int64)),
+                ("seqcat", C.c_void_p), ("seq_off", C.POINTER(C.c_int64))]
+
+
+class _OrcFasta(C.Structure):
+    _fields_ = [("num_seqs", C.c_int64), ("n_large", C.c_int64), ("n_small", C.c_int64),
+                ("name_start", C.POINTER(C.c_int64)), ("name_len", C.POINTER(C.c_int32)),
+                ("seq", C.c_void_p), ("seq_off", C.POINTER(C.c_int64))]
+
+
+def _split(base, off, count):
+    return [C.string_at(base + off[i], off[i + 1] - off[i]) for i in range(count)]
+
+
+def parse_fasta_ref(path, min_contig=2500, min_small=1000, nthreads=4):
+    """RabbitBin's own parse_fasta_mmap_parallel on a file (None if the
+    harness is not built): {num_seqs, large: [(name, seq)], small: [...]}."""
+    lib = ref()
+    if lib is None:
+        return None
+    f = lib.lib.ref_parse_fasta
+    f.restype = C.c_int
+    f.argtypes = [C.c_char_p, C.c_int, C.c_int64, C.c_int64, C.POINTER(_RefFasta)]
+    out = _RefFasta()
+    if f(path.encode(), nthreads, min_contig, min_small, C.byref(out)) != 0:
+        raise RuntimeError("reference parser failed")
+    n = out.n_large + out.n_small
+    names = _split(out.names, out.name_off, n)
+    seqs = _split(out.seqcat, out.seq_off, n)
+    for p in (out.names, out.seqcat, C.cast(out.name_off, C.c_void_p).value,
+              C.cast(out.seq_off, C.c_void_p).value):
+        lib._free(p)
+    pairs = list(zip(names, seqs))
+    return {"num_seqs": out.num_seqs, "large": pairs[:out.n_large], "small": pairs[out.n_large:]}
+
+
+def parse_fasta_restated(data, min_contig=2500, min_small=1000):
+    """The restated parser on an in-memory file; same result shape."""
+    lib = restated()
+    f = lib.lib.orc_parse_fasta
+    f.restype = C.c_int
+    f.argtypes = [C.c_char_p, C.c_int64, C.c_int64, C.c_int64, C.POINTER(_OrcFasta)]
+    out = _OrcFasta()
+    f(data, len(data), min_contig, min_small, C.byref(out))
+    n = out.n_large + out.n_small
+    names = [data[out.name_start[i]:out.name_start[i] + out.name_len[i]] for i in range(n)]
+    seqs = _split(out.seq, out.seq_off, n)
+    for p in (out.seq, C.cast(out.name_start, C.c_void_p).value,
+              C.cast(out.name_len, C.c_void_p).value, C.cast(out.seq_off, C.c_void_p).value):
+        lib._free(p)
+    pairs = list(zip(names, seqs))
+    return {"num_seqs": out.num_seqs, "large": pairs[:out.n_large], "small": pairs[out.n_large:]}

@@ -36,6 +36,8 @@ FRAGMENTS = [
     ("frag_depth_terms.inc", "rabbitbin.cpp", 685, 970),
     ("frag_pmh_sim.inc", "rabbitbin.cpp", 1194, 1426),
     ("frag_build_winners.inc", "rabbitbin.cpp", 1436, 1589),
+    ("frag_contig_rec.inc", "rabbitbin.cpp", 1876, 1888),
+    ("frag_parse_fasta.inc", "rabbitbin.cpp", 1890, 2248),
     ("frag_anynz.inc", "impl/rb_abundance.cpp", 94, 114),
     ("frag_graph_allpairs.inc", "impl/rb_graph.cpp", 7, 72),
     ("frag_calib_converge.inc", "impl/rb_graph.cpp", 390, 415),

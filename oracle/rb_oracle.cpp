@@ -30,6 +30,7 @@
 #include <limits>
 #include <numeric>
 #include <random>
+#include <string>
 #include <vector>
 #include <omp.h>
 
@@ -604,6 +605,99 @@ void orc_pmh_elements(const uint64_t *keys, const double *w, int64_t ne, uint32_
   Sketch sk((int)m);
   for (int64_t t = 0; t < ne; ++t) sk.add(keys[t], w[t], seed);
   for (uint32_t r = 0; r < m; ++r) { regs[r] = sk.tree[sk.leaves + r]; win[r] = sk.win[r]; }
+}
+
+// ── FASTA ingest (parse_fasta_mmap_parallel, src/rabbitbin.cpp:1998-2196) ──
+// Sequential restatement over an in-memory file.  A record starts at the first
+// '>' of a line; its name is the run of bytes > ' ' after it; the header ends at
+// the next '\n' (a record without one is dropped, :2037-2038); the body runs to
+// the next record start.  A body whose bytes after its first '\n' are all '\n'
+// or '\r' is single-line: its first line minus one trailing '\r' (:2084-2096).
+// Otherwise every '\n'-separated segment minus one trailing '\r' is kept
+// (:2097-2117).  Records of length >= min_contig are large, >= min_small small,
+// the rest dropped (:2131-2136); num_seqs counts every record with a header line.
+// Output: large then small records, each in file order; name_start/name_len
+// index the input; sequences back to back in `seq` with offsets seq_off.
+struct OrcFasta {
+  int64_t num_seqs, n_large, n_small;
+  int64_t *name_start;
+  int32_t *name_len;
+  char *seq;
+  int64_t *seq_off;
+};
+
+int orc_parse_fasta(const char *buf, int64_t n, int64_t min_contig, int64_t min_small,
+                    OrcFasta *out) {
+  struct Rec { int64_t ns; int32_t nl; std::string s; };
+  std::vector<Rec> large, small;
+  int64_t nseq = 0, p = 0;
+  auto find = [&](int64_t from, char c) -> int64_t {
+    for (int64_t q = from; q < n; ++q) if (buf[q] == c) return q;
+    return -1;
+  };
+  while (p < n) {
+    const int64_t gt = find(p, '>');
+    if (gt < 0) break;
+    int64_t q = gt + 1;
+    const int64_t ns = q;
+    while (q < n && (uint8_t)buf[q] > ' ') ++q;
+    const int32_t nl_len = (int32_t)(q - ns);
+    const int64_t hnl = find(q, '\n');
+    if (hnl < 0) break;
+    const int64_t b0 = hnl + 1;
+    int64_t b1 = find(b0, '>');
+    if (b1 < 0) b1 = n;
+    std::string s;
+    int64_t first_nl = -1;
+    for (int64_t t = b0; t < b1; ++t) if (buf[t] == '\n') { first_nl = t; break; }
+    bool single = true;
+    if (first_nl >= 0)
+      for (int64_t t = first_nl + 1; t < b1; ++t)
+        if (buf[t] != '\n' && buf[t] != '\r') { single = false; break; }
+    if (single) {
+      int64_t e = first_nl >= 0 ? first_nl : b1;
+      if (e > b0 && buf[e - 1] == '\r') --e;
+      s.assign(buf + b0, buf + e);
+    } else {
+      int64_t seg = b0;
+      while (seg < b1) {
+        int64_t e = seg;
+        while (e < b1 && buf[e] != '\n') ++e;
+        int64_t l = e - seg;
+        if (l > 0 && buf[seg + l - 1] == '\r') --l;
+        s.append(buf + seg, buf + seg + l);
+        if (e >= b1) break;
+        seg = e + 1;
+      }
+    }
+    ++nseq;
+    const int64_t L = (int64_t)s.size();
+    if (L >= min_contig) large.push_back({ns, nl_len, std::move(s)});
+    else if (L >= min_small) small.push_back({ns, nl_len, std::move(s)});
+    p = b1;
+  }
+  const size_t cnt = large.size() + small.size();
+  size_t tot = 0;
+  for (auto &r : large) tot += r.s.size();
+  for (auto &r : small) tot += r.s.size();
+  out->num_seqs = nseq;
+  out->n_large = (int64_t)large.size();
+  out->n_small = (int64_t)small.size();
+  out->name_start = (int64_t *)malloc((cnt + 1) * sizeof(int64_t));
+  out->name_len = (int32_t *)malloc((cnt + 1) * sizeof(int32_t));
+  out->seq = (char *)malloc(tot + 1);
+  out->seq_off = (int64_t *)malloc((cnt + 1) * sizeof(int64_t));
+  size_t k = 0, o = 0;
+  out->seq_off[0] = 0;
+  for (auto *v : {&large, &small})
+    for (auto &r : *v) {
+      out->name_start[k] = r.ns;
+      out->name_len[k] = r.nl;
+      memcpy(out->seq + o, r.s.data(), r.s.size());
+      o += r.s.size();
+      out->seq_off[++k] = (int64_t)o;
+    }
+  return 0;
 }
 
 }  // extern "C"

@@ -39,6 +39,10 @@
 #include <utility>
 #include <vector>
 #include <omp.h>
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include "probmh.h"
 #include "rabbit_sketch.h"
@@ -145,6 +149,16 @@ double cal_depth_corr(size_t, size_t, bool = false, bool = false) { abort(); }
 #include "frag_depth_terms.inc"     // src/rabbitbin.cpp:685-970
 #include "frag_pmh_sim.inc"         // src/rabbitbin.cpp:1194-1426
 #include "frag_build_winners.inc"   // src/rabbitbin.cpp:1436-1589
+// globals and helpers the FASTA parser reads (src/rabbitbin.h:198-199 and the
+// rb_cmd_bin state); the TNF branch is never taken here (collect_tnf = false)
+static const char *g_fasta_mmap = nullptr;
+static size_t g_fasta_mmap_len = 0;
+static std::vector<std::string> g_seq_arenas;
+static bool g_idf_norm = false;
+static inline void rb_phase(const char *) {}
+static inline void rb_fill_tnf(const char *, size_t, float *) { abort(); }
+#include "frag_contig_rec.inc"      // src/rabbitbin.cpp:1876-1888
+#include "frag_parse_fasta.inc"     // src/rabbitbin.cpp:1890-2248
 #include "frag_anynz.inc"           // src/impl/rb_abundance.cpp:94-114
 #include "frag_graph_allpairs.inc"  // src/impl/rb_graph.cpp:7-72
 #include "frag_calib_converge.inc"  // src/impl/rb_graph.cpp:390-415
@@ -210,6 +224,61 @@ struct RefOut {
 };
 
 void ref_free(void *p) { free(p); }
+
+// parse_fasta_mmap_parallel (src/rabbitbin.cpp:1890-2248) on a file, as
+// rb_cmd_bin calls it for binning (full headers off, no streamed sketches, no
+// tiny or TNF collection).  Large then small contigs, each in file order:
+// names joined in `names` (offsets name_off[n+1]), sequences in `seqcat`
+// (offsets seq_off[n+1]); arrays malloc'd, free each with ref_free.
+struct RefFasta {
+  int64_t num_seqs, n_large, n_small;
+  char *names;
+  int64_t *name_off;
+  char *seqcat;
+  int64_t *seq_off;
+};
+
+int ref_parse_fasta(const char *path, int nthreads, int64_t min_contig, int64_t min_small,
+                    RefFasta *out) {
+  std::vector<ContigRec> large, small;
+  std::vector<std::pair<std::string, std::string>> tiny;
+  size_t nseq = 0;
+  if (!parse_fasta_mmap_parallel(path, nthreads, (size_t)min_contig, (size_t)min_small,
+                                 false, false, false, false, false, 500, 4, large, small,
+                                 tiny, nseq))
+    return -1;
+  std::vector<const ContigRec *> recs;
+  for (auto &r : large) recs.push_back(&r);
+  for (auto &r : small) recs.push_back(&r);
+  const size_t n = recs.size();
+  size_t nb = 0, sb = 0;
+  for (auto *r : recs) { nb += r->name.size(); sb += r->len; }
+  out->num_seqs = (int64_t)nseq;
+  out->n_large = (int64_t)large.size();
+  out->n_small = (int64_t)small.size();
+  out->names = (char *)malloc(nb + 1);
+  out->name_off = (int64_t *)malloc((n + 1) * sizeof(int64_t));
+  out->seqcat = (char *)malloc(sb + 1);
+  out->seq_off = (int64_t *)malloc((n + 1) * sizeof(int64_t));
+  size_t a = 0, b = 0;
+  out->name_off[0] = 0;
+  out->seq_off[0] = 0;
+  for (size_t i = 0; i < n; ++i) {
+    const ContigRec &r = *recs[i];
+    memcpy(out->names + a, r.name.data(), r.name.size());
+    a += r.name.size();
+    const char *s = r.seq_view_ptr ? r.seq_view_ptr : g_seq_arenas[r.arena_tid].data() + r.arena_off;
+    memcpy(out->seqcat + b, s, r.len);
+    b += r.len;
+    out->name_off[i + 1] = (int64_t)a;
+    out->seq_off[i + 1] = (int64_t)b;
+  }
+  if (g_fasta_mmap) munmap((void *)g_fasta_mmap, g_fasta_mmap_len);
+  g_fasta_mmap = nullptr;
+  g_fasta_mmap_len = 0;
+  g_seq_arenas.clear();
+  return 0;
+}
 
 // Runs pack -> b0 -> ranks/unit rows -> graph -> edge weights exactly as
 // rb_cmd_bin does for a PMH run; winners32 holds the build_pmh_winners rows.
