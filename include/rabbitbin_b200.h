@@ -138,6 +138,32 @@ int rbg_bin_graph(rbg_ctx *ctx, const rbg_params *p, const char *seqcat,
                   const int64_t *offsets, int64_t n, const float *depth,
                   int32_t S, rbg_graph *out);
 
+/* ── FASTA ingest on the device ───────────────────────────────────────────
+ * parse_fasta_mmap_parallel (src/rabbitbin.cpp:1890-2248) as rb_cmd_bin calls
+ * it for binning: records start at the first '>' of a line, names end at the
+ * first byte <= ' ', multi-line bodies lose their newlines and one '\r' per
+ * line, records of length >= min_contig are large, >= min_small_contig small,
+ * shorter ones dropped; num_seqs counts every record with a header line.
+ * Large and small contigs come back in file order, sequences back to back
+ * (offsets n + 1), names as byte ranges of the input.  Free with
+ * rbg_free_fasta. */
+typedef struct rbg_fasta {
+  int64_t num_seqs, n_large, n_small;
+  char *large_seq;  int64_t *large_off;  int64_t *large_name_start;  int32_t *large_name_len;
+  char *small_seq;  int64_t *small_off;  int64_t *small_name_start;  int32_t *small_name_len;
+} rbg_fasta;
+
+int rbg_parse_fasta(rbg_ctx *ctx, const char *fasta, int64_t nbytes, int64_t min_contig,
+                    int64_t min_small_contig, rbg_fasta *out);
+int rbg_free_fasta(rbg_fasta *f);
+
+/* The whole hot path from a FASTA file's bytes: the device parse, then the
+ * large contigs (>= min_contig) go straight into rbg_bin_graph's pipeline
+ * without a host round trip of the sequences.  depth: n_large x S coverage
+ * means of the large contigs in file order. */
+int rbg_bin_fasta(rbg_ctx *ctx, const rbg_params *p, const char *fasta, int64_t nbytes,
+                  int64_t min_contig, const float *depth, int32_t S, rbg_graph *out);
+
 /* ── batching: many assemblies per launch ─────────────────────────────────
  * No counterpart in the reference, which bins one assembly per process
  * (rb_cmd_bin, src/rabbitbin.cpp:4660-5622).  Each assembly's graph equals

@@ -74,6 +74,14 @@ class BatchStats(C.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_ if n != "reserved"}
 
 
+class Fasta(C.Structure):
+    _fields_ = [("num_seqs", C.c_int64), ("n_large", C.c_int64), ("n_small", C.c_int64),
+                ("large_seq", C.c_void_p), ("large_off", C.POINTER(C.c_int64)),
+                ("large_name_start", C.POINTER(C.c_int64)), ("large_name_len", C.POINTER(C.c_int32)),
+                ("small_seq", C.c_void_p), ("small_off", C.POINTER(C.c_int64)),
+                ("small_name_start", C.POINTER(C.c_int64)), ("small_name_len", C.POINTER(C.c_int32))]
+
+
 class ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("workers", C.c_int32), ("hbm_budget", C.c_int64),
                 ("max_batch", C.c_int32), ("plain", C.c_int32), ("max_batch_pairs", C.c_int64)]
@@ -125,6 +133,10 @@ def lib():
                                    P(C.c_uint32)], C.c_int),
         "rbg_bin_batch": ([vp, P(Params), P(Assembly), C.c_int32, P(Graph), P(BatchStats)],
                           C.c_int),
+        "rbg_parse_fasta": ([vp, C.c_char_p, C.c_int64, C.c_int64, C.c_int64, P(Fasta)], C.c_int),
+        "rbg_free_fasta": ([P(Fasta)], C.c_int),
+        "rbg_bin_fasta": ([vp, P(Params), C.c_char_p, C.c_int64, C.c_int64, P(C.c_float),
+                           C.c_int32, P(Graph)], C.c_int),
         "rbg_server_create": ([P(ServerConfig), P(Params), P(vp)], C.c_int),
         "rbg_server_submit": ([vp, P(Assembly), P(C.c_int64)], C.c_int),
         "rbg_server_wait": ([vp, C.c_int64, C.c_double, P(Graph), P(RequestStats)], C.c_int),
@@ -308,6 +320,38 @@ class Context:
 
     def fetch_graph(self):
         return self._graph_call(self._L.rbg_fetch_graph, self._h)
+
+    def parse_fasta(self, data, min_contig=2500, min_small_contig=1000):
+        """Device FASTA parse (rbg_parse_fasta) of the bytes `data`:
+        {num_seqs, large: (seqcat, offsets, names), small: (...)}."""
+        f = Fasta()
+        self._check(self._L.rbg_parse_fasta(self._h, data, len(data), min_contig,
+                                            min_small_contig, C.byref(f)), "parse_fasta")
+        try:
+            out = {"num_seqs": f.num_seqs}
+            for tag, n, seq, off, ns, nl in (
+                    ("large", f.n_large, f.large_seq, f.large_off, f.large_name_start,
+                     f.large_name_len),
+                    ("small", f.n_small, f.small_seq, f.small_off, f.small_name_start,
+                     f.small_name_len)):
+                offs = np.ctypeslib.as_array(off, (n + 1,)).copy()
+                seqcat = C.string_at(seq, int(offs[-1])) if offs[-1] else b""
+                names = [data[ns[i]:ns[i] + nl[i]] for i in range(n)]
+                out[tag] = (seqcat, offs, names)
+            return out
+        finally:
+            self._L.rbg_free_fasta(C.byref(f))
+
+    def bin_fasta(self, data, depth, min_contig=2500, params=None, nbytes=None):
+        """The hot path from FASTA bytes (rbg_bin_fasta); depth rows are the
+        large contigs in file order.  `data` is bytes, or a char pointer with
+        `nbytes` (e.g. pinned host memory)."""
+        p = params or default_params()
+        d = np.ascontiguousarray(depth, np.float32)
+        S = d.shape[1] if d.ndim == 2 else 0
+        n = len(data) if nbytes is None else nbytes
+        return self._graph_call(self._L.rbg_bin_fasta, self._h, C.byref(p), data, n,
+                                min_contig, _p(d, C.c_float) if d.size else None, S)
 
     def bin_batch(self, assemblies, params=None):
         """Graphs of many assemblies in one call (rbg_bin_batch).

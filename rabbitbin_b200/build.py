@@ -19,8 +19,8 @@ CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SRCS = ["kernels_sketch.cu", "kernels_graph.cu", "kernels_allpairs.cu", "kernels_util.cu",
-           "noalloc.cu"]
-CPP_SRCS = ["pmh_streams.cpp", "calib.cpp", "engine.cpp", "batch.cpp", "server.cpp"]
+           "noalloc.cu", "kernels_fasta.cu"]
+CPP_SRCS = ["pmh_streams.cpp", "calib.cpp", "engine.cpp", "batch.cpp", "server.cpp", "fasta.cpp"]
 HEADERS = ["rbg_internal.h", "../../include/rabbitbin_b200.h", "gen_zig_tables.py"]
 
 

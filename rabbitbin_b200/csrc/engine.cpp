@@ -70,6 +70,32 @@ void stage(rbg_ctx *c, const char *seqcat, const int64_t *offsets, int64_t n,
     CK(cudaMemcpyAsync(c->depth.p, depth, (size_t)n * S * sizeof(float), cudaMemcpyHostToDevice, c->stream));
 }
 
+// Inputs already on the device (the FASTA parser's output): sequences and
+// offsets are copied device to device, the coverage table from the host.
+void stage_device(rbg_ctx *c, const char *dseq, const int64_t *doffsets, int64_t n,
+                  int64_t nbases, const float *depth, int S) {
+  if (S < 0 || S > kMaxS) throw Error(RBG_ERR_UNSUPPORTED, "S must be in 0..64");
+  if (S > 0 && n > 0 && !depth) throw Error(RBG_ERR_ARG, "depth is null");
+  if (n >= (1 << 27)) throw Error(RBG_ERR_UNSUPPORTED, "at most 2^27 - 1 contigs per assembly");
+  c->n = n;
+  c->S = S;
+  c->nbases = nbases;
+  c->h_offsets.clear();
+  c->graph_ready = false;
+  const size_t abytes = (size_t)((nbases + 15) / 16) * 16 + 16;
+  c->ascii.ensure(abytes);
+  c->offsets.ensure((n + 1) * sizeof(int64_t));
+  c->depth.ensure(std::max<size_t>(1, (size_t)n * S) * sizeof(float));
+  CK(cudaMemsetAsync(c->ascii.p, 0, abytes, c->stream));
+  if (nbases)
+    CK(cudaMemcpyAsync(c->ascii.p, dseq, (size_t)nbases, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->offsets.p, doffsets, (n + 1) * sizeof(int64_t), cudaMemcpyDeviceToDevice,
+                     c->stream));
+  if (S > 0 && n > 0)
+    CK(cudaMemcpyAsync(c->depth.p, depth, (size_t)n * S * sizeof(float), cudaMemcpyHostToDevice,
+                       c->stream));
+}
+
 // Unit rank rows, anynz and column norms on the auxiliary stream: they depend
 // only on the coverage table, so they overlap the sketch kernels.
 void prep_depth(rbg_ctx *c, const rbg_params *p) {
@@ -479,6 +505,7 @@ int rbg_destroy(rbg_ctx *c) {
   if (c->tables) c->tables->release();
   release_batch_graphs(c);
   if (c->batch) c->batch->release();
+  if (c->fasta) c->fasta->release();
   c->pin.release();
   for (auto &e : c->ev) cudaEventDestroy(e);
   cudaStreamSynchronize(c->aux);
@@ -556,6 +583,21 @@ int rbg_build_graph(rbg_ctx *c, const rbg_params *p, const uint32_t *winners32, 
     }
     codes_from_winners(c, p, winners32, n);
     c->prep_done = false;                    // coverage changed: prepare it again
+    run_graph(c, p);
+    fetch(c, out);
+  });
+}
+
+int rbg_bin_fasta(rbg_ctx *c, const rbg_params *p, const char *fasta, int64_t nbytes,
+                  int64_t min_contig, const float *depth, int32_t S, rbg_graph *out) {
+  return guarded(c, [&] {
+    validate(p);
+    // small contigs are not needed here: a small threshold equal to the large
+    // one leaves that class empty
+    const FastaCounts k = fasta_parse(c, fasta, nbytes, min_contig, min_contig);
+    stage_device(c, c->fasta->seq[0].as<char>(), c->fasta->seq_off[0].as<int64_t>(), k.n[0],
+                 k.bytes[0], depth, S);
+    run_sketch(c, p, false);
     run_graph(c, p);
     fetch(c, out);
   });

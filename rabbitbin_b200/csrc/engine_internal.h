@@ -138,6 +138,25 @@ struct BatchBufs {
   }
 };
 
+// Buffers of the device FASTA parser.
+struct FastaBufs {
+  DBuf in, tile_nl, tile_gt, nl_base, gt_base, nl_pos, gt_pos, flag, rs, rec;
+  DBuf idx[2], off[2], seq[2], seq_off[2], name_start[2], name_len[2];
+  void release() {
+    DBuf *all[] = {&in, &tile_nl, &tile_gt, &nl_base, &gt_base, &nl_pos, &gt_pos, &flag, &rs,
+                   &rec, &idx[0], &idx[1], &off[0], &off[1], &seq[0], &seq[1], &seq_off[0],
+                   &seq_off[1], &name_start[0], &name_start[1], &name_len[0], &name_len[1]};
+    for (DBuf *b : all) b->release();
+  }
+};
+
+// Counts of one parse; the outputs are in FastaBufs: slot 0 large, 1 small
+// (seq: sequences back to back, seq_off: n+1 offsets, name_start / name_len:
+// name ranges in the input).
+struct FastaCounts {
+  int64_t num_seqs = 0, n[2] = {0, 0}, bytes[2] = {0, 0};
+};
+
 // glibc's rand() sequence of one seed (srand(seed); rand(); ...) on private
 // state, so concurrent calibrations do not share the process-wide generator.
 struct CRand {
@@ -170,6 +189,10 @@ double calibrate_cutoff(const uint32_t *maxc, int64_t n, bool fused, int m,
 std::shared_ptr<const std::vector<int32_t>> b0_pairs(int64_t n);
 
 void validate_params(const rbg_params *p);
+
+// Parses `F` bytes of FASTA (host memory) on the context's device.
+FastaCounts fasta_parse(rbg_ctx *c, const char *data, int64_t F, int64_t min_contig,
+                        int64_t min_small);
 
 // Frees the CUDA graphs the batch engine keeps for a context.
 void release_batch_graphs(rbg_ctx *c);
@@ -215,6 +238,8 @@ struct rbg_ctx {
   int launches = 0;
   // batch engine
   std::unique_ptr<rbg::BatchBufs> batch;
+  // FASTA ingest
+  std::unique_ptr<rbg::FastaBufs> fasta;
 };
 
 namespace rbg {

@@ -210,6 +210,36 @@ void launch_write_edges_batch(const BatchAsm *B, const int64_t *row0s, int nb, i
                               cudaStream_t s);
 void launch_edge_weights_batch(const BatchAsm *B, const int64_t *edge0s, int nb, int64_t edges,
                                cudaStream_t s);
+// ── FASTA ingest (kernels_fasta.cu) ────────────────────────────────────────
+// One record of a FASTA file on the device: its name range in the input, its
+// body [b0, b1) with body newlines nl_pos[nl0..nl1), its length after newline
+// removal, single-line flag and class (0 tiny, 1 small, 2 large, 3 no header
+// newline: dropped and not counted).
+struct FastaRec {
+  int64_t name_start, b0, b1, nl0, nl1, len;
+  int32_t name_len;
+  int8_t cls, single;
+};
+// Tile counts of '\n' and '>' and their exclusive scans (totals at [tiles]).
+void launch_fasta_positions(const uint8_t *in, int64_t F, int *tile_nl, int *tile_gt,
+                            int64_t *nl_base, int64_t *gt_base, cudaStream_t s);
+void launch_fasta_scatter(const uint8_t *in, int64_t F, const int64_t *nl_base,
+                          const int64_t *gt_base, int64_t *nl_pos, int64_t *gt_pos,
+                          cudaStream_t s);
+// flag[0..ngt] becomes the exclusive scan of record-start flags; rs the starts.
+void launch_fasta_starts(const int64_t *gt_pos, int64_t ngt, const int64_t *nl_pos, int64_t nnl,
+                         int64_t *flag, int64_t *rs, cudaStream_t s);
+void launch_fasta_records(const uint8_t *in, int64_t F, const int64_t *rs, int64_t nrs,
+                          const int64_t *nl_pos, int64_t nnl, int64_t min_contig,
+                          int64_t min_small, FastaRec *rec, cudaStream_t s);
+// Exclusive scans of class-c membership (output index) and length (byte
+// offset) over the records, totals at [nrs].
+void launch_fasta_class(const FastaRec *rec, int64_t nrs, int c, int64_t *flag, int64_t *bytes,
+                        cudaStream_t s);
+void launch_fasta_copy(const uint8_t *in, const FastaRec *rec, int64_t nrs, const int64_t *nl_pos,
+                       int c, const int64_t *idx, const int64_t *off, uint8_t *out,
+                       int64_t *out_off, int64_t *name_start, int32_t *name_len, cudaStream_t s);
+
 // Work items of the all-pairs kernels for one assembly.
 int64_t allpairs_items(int64_t n, int P);
 size_t allpairs_batch_smem(int variant, int mpad, int Su);
