@@ -8,6 +8,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <map>
 #include <mutex>
 #include <numeric>
 #include <random>
@@ -352,6 +353,57 @@ void run_graph(rbg_ctx *c, const rbg_params *p) {
   c->graph_ready = true;
 }
 
+// Pinned host blocks for graph results: the four edge arrays of one graph
+// share one block, which the device writes at DMA speed (pageable destinations
+// are slow and page-fault on first touch).  rbg_free_graph returns a block to
+// the pool; a few idle blocks are kept for reuse.
+struct PinnedPool {
+  std::mutex mu;
+  std::unordered_map<void *, size_t> live;
+  std::multimap<size_t, void *> idle;
+  size_t idle_bytes = 0;
+
+  void *take(size_t bytes) {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = idle.lower_bound(bytes);
+    if (it != idle.end() && it->first <= 2 * bytes + ((size_t)1 << 20)) {
+      void *p = it->second;
+      live[p] = it->first;
+      idle_bytes -= it->first;
+      idle.erase(it);
+      return p;
+    }
+    void *p = nullptr;
+    if (cudaHostAlloc(&p, bytes, cudaHostAllocPortable) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    live[p] = bytes;
+    return p;
+  }
+
+  bool give(void *p) {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = live.find(p);
+    if (it == live.end()) return false;
+    idle.emplace(it->second, p);
+    idle_bytes += it->second;
+    live.erase(it);
+    while (idle.size() > 8 || idle_bytes > ((size_t)2 << 30)) {
+      auto v = idle.begin();
+      idle_bytes -= v->first;
+      cudaFreeHost(v->second);
+      idle.erase(v);
+    }
+    return true;
+  }
+};
+
+PinnedPool &pinned_pool() {
+  static PinnedPool *pool = new PinnedPool();     // outlives every context
+  return *pool;
+}
+
 void fetch(rbg_ctx *c, rbg_graph *out) {
   if (!out) throw Error(RBG_ERR_ARG, "null graph");
   if (!c->graph_ready) throw Error(RBG_ERR_ARG, "no graph has been built on this context");
@@ -361,11 +413,19 @@ void fetch(rbg_ctx *c, rbg_graph *out) {
   out->b0 = c->b0;
   out->sim_cutoff = c->sim_cutoff;
   out->path = c->path;
-  const size_t nb = std::max<size_t>(ne, 1) * 4;
-  out->from = (uint32_t *)malloc(nb);
-  out->to = (uint32_t *)malloc(nb);
-  out->scomp = (float *)malloc(nb);
-  out->score = (float *)malloc(nb);
+  const size_t n1 = std::max<size_t>(ne, 1);
+  const size_t nb = n1 * 4;
+  if (void *blk = pinned_pool().take(4 * nb)) {
+    out->from = (uint32_t *)blk;
+    out->to = out->from + n1;
+    out->scomp = (float *)(out->to + n1);
+    out->score = out->scomp + n1;
+  } else {
+    out->from = (uint32_t *)malloc(nb);
+    out->to = (uint32_t *)malloc(nb);
+    out->scomp = (float *)malloc(nb);
+    out->score = (float *)malloc(nb);
+  }
   if (!out->from || !out->to || !out->scomp || !out->score) {
     rbg_free_graph(out);
     throw Error(RBG_ERR_NOMEM, "host allocation of the edge arrays failed");
@@ -680,10 +740,12 @@ int rbg_pmh_stream_tables(int32_t k, int32_t m, uint64_t seed, int32_t contract,
 
 int rbg_free_graph(rbg_graph *g) {
   if (!g) return RBG_ERR_ARG;
-  free(g->from);
-  free(g->to);
-  free(g->scomp);
-  free(g->score);
+  if (!(g->from && pinned_pool().give(g->from))) {     // one pinned block, or four mallocs
+    free(g->from);
+    free(g->to);
+    free(g->scomp);
+    free(g->score);
+  }
   g->from = g->to = nullptr;
   g->scomp = g->score = nullptr;
   g->n_edges = 0;
