@@ -45,8 +45,10 @@ Tables &tables_for(rbg_ctx *c, const rbg_params *p) {
   return *c->tables;
 }
 
-void stage(rbg_ctx *c, const char *seqcat, const int64_t *offsets, int64_t n,
-           const float *depth, int S) {
+// Checks, sizes, offsets and coverage to the device; the ASCII bases are
+// copied by the caller (whole, or in chunks behind the sketch).
+void stage_meta(rbg_ctx *c, const char *seqcat, const int64_t *offsets, int64_t n,
+                const float *depth, int S) {
   if (n < 0 || (n > 0 && (!offsets || !seqcat))) throw Error(RBG_ERR_ARG, "bad sequence arguments");
   if (S < 0 || S > kMaxS) throw Error(RBG_ERR_UNSUPPORTED, "S must be in 0..64");
   if (S > 0 && n > 0 && !depth) throw Error(RBG_ERR_ARG, "depth is null");
@@ -63,12 +65,19 @@ void stage(rbg_ctx *c, const char *seqcat, const int64_t *offsets, int64_t n,
   c->ascii.ensure(abytes);
   c->offsets.ensure((n + 1) * sizeof(int64_t));
   c->depth.ensure(std::max<size_t>(1, (size_t)n * S) * sizeof(float));
-  CK(cudaMemsetAsync(c->ascii.p, 0, abytes, c->stream));
-  if (c->nbases)
-    CK(cudaMemcpyAsync(c->ascii.p, seqcat, (size_t)c->nbases, cudaMemcpyHostToDevice, c->stream));
+  (void)abytes;
   CK(cudaMemcpyAsync(c->offsets.p, offsets, (n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
   if (S > 0 && n > 0)
     CK(cudaMemcpyAsync(c->depth.p, depth, (size_t)n * S * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+}
+
+void stage(rbg_ctx *c, const char *seqcat, const int64_t *offsets, int64_t n,
+           const float *depth, int S) {
+  stage_meta(c, seqcat, offsets, n, depth, S);
+  const size_t abytes = (size_t)((c->nbases + 15) / 16) * 16 + 16;
+  CK(cudaMemsetAsync(c->ascii.p, 0, abytes, c->stream));
+  if (c->nbases)
+    CK(cudaMemcpyAsync(c->ascii.p, seqcat, (size_t)c->nbases, cudaMemcpyHostToDevice, c->stream));
 }
 
 // Inputs already on the device (the FASTA parser's output): sequences and
@@ -135,6 +144,93 @@ void prep_depth(rbg_ctx *c, const rbg_params *p) {
 }
 
 // Sketch stage: pack, count + weights, register minimum.
+// Sketch buffers and the kernel arguments over all contigs.
+SketchArgs sketch_setup(rbg_ctx *c, const rbg_params *p, bool want_winners) {
+  Tables &T = tables_for(c, p);
+  const int64_t n = c->n;
+  const int m = p->m, mpad = mpad_of(p->m);
+  const int64_t nwords = (c->nbases + 15) / 16 + 1;
+  c->packed.ensure(nwords * 4);
+  c->nmask.ensure((nwords / 2 + 2) * 4);
+  c->elem_winv.ensure(std::max<int64_t>(n, 1) * T.t->n_elems * sizeof(double));
+  c->elem_cnt.ensure(std::max<int64_t>(n, 1) * sizeof(int32_t));
+  c->codesA.ensure(std::max<int64_t>(n, 1) * mpad);
+  c->codesB.ensure(std::max<int64_t>(n, 1) * mpad);
+  if (want_winners) c->winners32.ensure(std::max<int64_t>(n, 1) * m * sizeof(uint32_t));
+  SketchArgs a;
+  a.packed = c->packed.as<uint32_t>();
+  a.nmask = c->nmask.as<uint32_t>();
+  a.offsets = c->offsets.as<int64_t>();
+  a.n = n;
+  a.k = p->k;
+  a.m = m;
+  a.gc_norm = p->gc_norm;
+  a.gc_cap = p->gc_norm_cap;
+  a.n_elems = T.t->n_elems;
+  a.rank_of_code = T.rank.as<int16_t>();
+  a.elem_winv = c->elem_winv.as<double>();
+  a.elem_cnt = c->elem_cnt.as<int32_t>();
+  a.U = T.U.as<double>();
+  a.codeA = T.codeA.as<uint8_t>();
+  a.W32 = T.W32.as<uint32_t>();
+  a.codesA = c->codesA.as<uint8_t>();
+  a.codesB = c->codesB.as<uint8_t>();
+  a.winners32 = want_winners ? c->winners32.as<uint32_t>() : nullptr;
+  a.mpad = mpad;
+  return a;
+}
+
+// The host-input path of rbg_bin_graph: the ASCII copy runs in chunks on the
+// copy stream; each chunk's words are packed as it lands, and the contigs
+// whose words are all packed (e <= 16 * packed words) are counted and reduced
+// while the next chunks copy.
+void stage_sketch_chunked(rbg_ctx *c, const rbg_params *p, const char *seqcat,
+                          const int64_t *offsets, int64_t n, const float *depth, int S) {
+  stage_meta(c, seqcat, offsets, n, depth, S);
+  const SketchArgs all = sketch_setup(c, p, false);
+  const int64_t nb = c->nbases, nwords = (nb + 15) / 16;
+  const int E = all.n_elems, mpad = all.mpad;
+  CK(cudaEventRecord(c->ev[0], c->stream));
+  prep_depth(c, p);
+  CK(cudaEventRecord(c->ev_cin, c->stream));             // the buffers are free to overwrite
+  CK(cudaStreamWaitEvent(c->copy, c->ev_cin, 0));
+  const int G = nwords >= ((int64_t)kChunks << 16) ? kChunks : 1;
+  int64_t c0 = 0;
+  for (int g = 0; g < G; ++g) {
+    const int64_t w0 = (int64_t)g * nwords / G & ~(int64_t)1;
+    const int64_t w1 = g + 1 == G ? nwords : ((int64_t)(g + 1) * nwords / G & ~(int64_t)1);
+    const int64_t b0 = 16 * w0, b1 = std::min<int64_t>(16 * w1, nb);
+    if (b1 > b0)
+      CK(cudaMemcpyAsync(c->ascii.as<char>() + b0, seqcat + b0, (size_t)(b1 - b0),
+                         cudaMemcpyHostToDevice, c->copy));
+    CK(cudaEventRecord(c->ev_chunk[g], c->copy));
+    CK(cudaStreamWaitEvent(c->stream, c->ev_chunk[g], 0));
+    launch_pack_range(c->ascii.as<char>(), nb, w0, w1, c->packed.as<uint32_t>(),
+                      c->nmask.as<uint32_t>(), c->stream);
+    const int64_t c1 = g + 1 == G ? n
+                     : (int64_t)(std::upper_bound(offsets + 1, offsets + n + 1, 16 * w1) -
+                                 (offsets + 1));
+    if (c1 > c0) {
+      SketchArgs a = all;
+      a.offsets += c0;
+      a.n = c1 - c0;
+      a.elem_winv += c0 * E;
+      a.elem_cnt += c0;
+      a.codesA += c0 * mpad;
+      a.codesB += c0 * mpad;
+      launch_count(a, c->stream);
+      launch_minreduce(a, c->stream);
+      c->launches += 2;
+    }
+    c0 = c1;
+  }
+  c->launches += G;
+  CK(cudaEventRecord(c->ev[1], c->stream));
+  CK(cudaEventRecord(c->ev[2], c->stream));
+  CK(cudaEventRecord(c->ev[3], c->stream));
+  CK(cudaGetLastError());
+}
+
 void run_sketch(rbg_ctx *c, const rbg_params *p, bool want_winners) {
   Tables &T = tables_for(c, p);
   const int64_t n = c->n;
@@ -547,6 +643,14 @@ int rbg_create(int device, rbg_ctx **out) {
   cudaEventCreateWithFlags(&c->ev_aux, cudaEventDisableTiming);
   cudaEventCreate(&c->ev_a0);
   cudaEventCreate(&c->ev_a1);
+  if (cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaStreamDestroy(c->aux);
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return RBG_ERR_CUDA;
+  }
+  cudaEventCreateWithFlags(&c->ev_cin, cudaEventDisableTiming);
+  for (auto &e : c->ev_chunk) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   *out = c;
   return RBG_OK;
 }
@@ -569,7 +673,10 @@ int rbg_destroy(rbg_ctx *c) {
   c->pin.release();
   for (auto &e : c->ev) cudaEventDestroy(e);
   cudaStreamSynchronize(c->aux);
-  for (cudaEvent_t e : {c->ev_in, c->ev_aux, c->ev_a0, c->ev_a1}) cudaEventDestroy(e);
+  cudaStreamSynchronize(c->copy);
+  for (cudaEvent_t e : {c->ev_in, c->ev_aux, c->ev_a0, c->ev_a1, c->ev_cin}) cudaEventDestroy(e);
+  for (auto &e : c->ev_chunk) cudaEventDestroy(e);
+  cudaStreamDestroy(c->copy);
   cudaStreamDestroy(c->aux);
   cudaStreamDestroy(c->stream);
   delete c;
@@ -667,8 +774,7 @@ int rbg_bin_graph(rbg_ctx *c, const rbg_params *p, const char *seqcat, const int
                   int64_t n, const float *depth, int32_t S, rbg_graph *out) {
   return guarded(c, [&] {
     validate(p);
-    stage(c, seqcat, offsets, n, depth, S);
-    run_sketch(c, p, false);
+    stage_sketch_chunked(c, p, seqcat, offsets, n, depth, S);
     run_graph(c, p);
     fetch(c, out);
   });

@@ -88,6 +88,9 @@ struct HBuf {
 
 inline int mpad_of(int m) { return (m + 15) & ~15; }
 
+// Chunks of the host-to-device copy that rbg_bin_graph overlaps with the sketch.
+constexpr int kChunks = 8;
+
 // Row stride (halves) of the FP16 unit rows: 16, 32 or 64, the k extent of the
 // tensor-core prefilter variant that reads them.
 inline int unit16_stride(int S) { return S <= 16 ? 16 : (S <= 32 ? 32 : 64); }
@@ -236,6 +239,9 @@ struct rbg_ctx {
   cudaEvent_t ev_in = nullptr, ev_aux = nullptr, ev_a0 = nullptr, ev_a1 = nullptr;
   bool prep_done = false;
   int launches = 0;
+  // chunked input copy behind the sketch (rbg_bin_graph)
+  cudaStream_t copy = nullptr;
+  cudaEvent_t ev_cin = nullptr, ev_chunk[rbg::kChunks] = {};
   // batch engine
   std::unique_ptr<rbg::BatchBufs> batch;
   // FASTA ingest

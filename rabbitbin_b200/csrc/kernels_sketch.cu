@@ -28,10 +28,12 @@ __device__ __forceinline__ uint32_t enc_base(uint32_t c, uint32_t &bad) {
 // (first base in the top two bits) and 16 bits of the invalid mask; lane pairs
 // merge their halves into one 32-bit mask word.
 __global__ void k_pack(const uint4 *__restrict__ ascii, int64_t nbases, int64_t nwords,
-                       uint32_t *__restrict__ packed, uint32_t *__restrict__ nmask) {
-  const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+                       int64_t w_begin, int64_t w_end, uint32_t *__restrict__ packed,
+                       uint32_t *__restrict__ nmask) {
+  // w_begin is even, so lane pairs (2i, 2i+1) hold the word pairs of one mask word
+  const int64_t w = w_begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t word = 0, bad16 = 0;
-  if (w < nwords) {
+  if (w < w_end) {
     const uint4 v = ascii[w];
     const uint32_t q[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
@@ -47,7 +49,7 @@ __global__ void k_pack(const uint4 *__restrict__ ascii, int64_t nbases, int64_t 
     packed[w] = word;
   }
   const uint32_t other = __shfl_xor_sync(0xffffffffu, bad16, 1);
-  if (w < nwords && (threadIdx.x & 1) == 0) {
+  if (w < w_end && (threadIdx.x & 1) == 0) {
     const uint32_t m = (bad16 << 16) | ((w + 1 < nwords) ? other : 0xFFFFu);
     nmask[w >> 1] = m;
   }
@@ -263,11 +265,18 @@ __global__ void __launch_bounds__(128) k_minreduce(SketchArgs a) {
 
 void launch_pack(const char *ascii, int64_t nbases, uint32_t *packed, uint32_t *nmask,
                  cudaStream_t s) {
+  launch_pack_range(ascii, nbases, 0, (nbases + 15) / 16, packed, nmask, s);
+}
+
+void launch_pack_range(const char *ascii, int64_t nbases, int64_t w_begin, int64_t w_end,
+                       uint32_t *packed, uint32_t *nmask, cudaStream_t s) {
   const int64_t nwords = (nbases + 15) / 16;
-  if (nwords == 0) return;
+  if (w_end > nwords) w_end = nwords;
+  if (w_end <= w_begin) return;
   const int tb = 256;
-  const int64_t grid = (nwords + tb - 1) / tb;
-  k_pack<<<(unsigned)grid, tb, 0, s>>>((const uint4 *)ascii, nbases, nwords, packed, nmask);
+  const int64_t grid = (w_end - w_begin + tb - 1) / tb;
+  k_pack<<<(unsigned)grid, tb, 0, s>>>((const uint4 *)ascii, nbases, nwords, w_begin, w_end,
+                                      packed, nmask);
 }
 
 void launch_count(const SketchArgs &a, cudaStream_t s) {

@@ -73,6 +73,10 @@ struct SketchArgs {
 
 void launch_pack(const char *ascii, int64_t nbases, uint32_t *packed, uint32_t *nmask,
                  cudaStream_t s);
+// Words [w_begin, w_end) only (w_begin even): the packing of one chunk of a
+// copy that is still arriving.
+void launch_pack_range(const char *ascii, int64_t nbases, int64_t w_begin, int64_t w_end,
+                       uint32_t *packed, uint32_t *nmask, cudaStream_t s);
 void launch_count(const SketchArgs &a, cudaStream_t s);
 void launch_minreduce(const SketchArgs &a, cudaStream_t s);
 
