@@ -415,7 +415,8 @@ int launch_sketch_groups(rbg_ctx *c, BatchBufs &B, const BatchPlan &L,
       r.mpad = tf.mpad;
       r.elem_winv = B.winv.as<double>() + tf.winv0;
       r.elem_cnt = B.ecnt.as<int32_t>() + tf.row0;
-      r.U = tab[t0]->U.as<double>();
+      r.order = tab[t0]->order.as<RegOrder>();
+      r.UT = tab[t0]->UT.as<double>();
       r.codeA = tab[t0]->codeA.as<uint8_t>();
       r.W32 = tab[t0]->W32.as<uint32_t>();
       r.codesA = B.codesA.as<uint8_t>() + tf.code0;

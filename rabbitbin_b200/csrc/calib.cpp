@@ -160,12 +160,14 @@ std::unique_ptr<Tables> make_tables(const rbg_params *p, cudaStream_t s) {
   T->win_bits = p->win_bits;
   const PmhTables &t = *T->t;
   const size_t EM = (size_t)t.n_elems * t.m;
-  T->U.ensure(EM * sizeof(double));
+  T->order.ensure(EM * sizeof(RegOrder));
+  T->UT.ensure(EM * sizeof(double));
   T->codeA.ensure(EM);
   T->W32.ensure(EM * sizeof(uint32_t));
   std::vector<int16_t> rk(t.rank_of_code.begin(), t.rank_of_code.end());
   T->rank.ensure(rk.size() * sizeof(int16_t));
-  CK(cudaMemcpyAsync(T->U.p, t.U.data(), EM * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(T->order.p, t.order.data(), EM * sizeof(RegOrder), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(T->UT.p, t.UT.data(), EM * sizeof(double), cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(T->codeA.p, p->win_bits == 16 ? t.code16.data() : t.code32.data(), EM,
                      cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(T->W32.p, t.W32.data(), EM * sizeof(uint32_t), cudaMemcpyHostToDevice, s));

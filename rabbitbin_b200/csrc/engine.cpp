@@ -170,7 +170,8 @@ SketchArgs sketch_setup(rbg_ctx *c, const rbg_params *p, bool want_winners) {
   a.rank_of_code = T.rank.as<int16_t>();
   a.elem_winv = c->elem_winv.as<double>();
   a.elem_cnt = c->elem_cnt.as<int32_t>();
-  a.U = T.U.as<double>();
+  a.order = T.order.as<RegOrder>();
+  a.UT = T.UT.as<double>();
   a.codeA = T.codeA.as<uint8_t>();
   a.W32 = T.W32.as<uint32_t>();
   a.codesA = c->codesA.as<uint8_t>();
@@ -262,7 +263,8 @@ void run_sketch(rbg_ctx *c, const rbg_params *p, bool want_winners) {
   a.rank_of_code = T.rank.as<int16_t>();
   a.elem_winv = c->elem_winv.as<double>();
   a.elem_cnt = c->elem_cnt.as<int32_t>();
-  a.U = T.U.as<double>();
+  a.order = T.order.as<RegOrder>();
+  a.UT = T.UT.as<double>();
   a.codeA = T.codeA.as<uint8_t>();
   a.W32 = T.W32.as<uint32_t>();
   a.codesA = c->codesA.as<uint8_t>();

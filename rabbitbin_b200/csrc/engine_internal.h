@@ -103,11 +103,11 @@ inline bool need_colnorm(const rbg_params *p, int S) {
 struct Tables {
   std::shared_ptr<const PmhTables> t;
   int win_bits = 16;
-  DBuf U, codeA, W32, rank;
+  DBuf order, UT, codeA, W32, rank;
   DBuf dict_vals, dict_codes, dict_n;   // per-column sorted dictionaries
   bool dict_ready = false;
   void release() {
-    U.release(); codeA.release(); W32.release(); rank.release();
+    order.release(); UT.release(); codeA.release(); W32.release(); rank.release();
     dict_vals.release(); dict_codes.release(); dict_n.release();
   }
 };

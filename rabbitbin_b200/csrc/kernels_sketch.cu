@@ -197,67 +197,221 @@ __global__ void k_count(SketchArgs a) {
   if (lane == 0) a.elem_cnt[c] = pos;
 }
 
-// Register minimum, tiled for reuse of the stream table: a CTA owns a slice of
-// 32 registers (lane = register) and walks batches of 32 contigs (warp w holds
-// contigs 8w .. 8w+7 of the batch).  The slice U[:, r0:r0+32] and the batch's
-// dense 1/w table (+inf for absent elements, which then never win: inf*U is
-// inf or NaN, neither is < best) live in shared memory.  Elements are visited
-// in ascending order with a strict <, so ties keep the first-inserted element.
-constexpr int kMRegs = 32;      // registers per CTA
-constexpr int kMCon = 32;       // contigs per batch
-constexpr int kMBatches = 4;    // batches per CTA
+// Register minimum with an exact early exit.  The winner of register r for a
+// contig is the element e with the smallest rounded product h = (1/w_e) * U[e][r],
+// ties to the smallest e (the reference inserts elements in ascending order with
+// a strict <), so the result is the lexicographic minimum of (h, e).
+//
+// Per contig, the kMHeavy elements with the smallest 1/w are evaluated directly;
+// the others are bounded below by wb, the next smallest 1/w.  The elements of
+// register r are then visited in ascending U (table `order`, ties by e): once
+// round(wb * U_next) > best, no element left can reach best, since each remaining
+// element is either already evaluated or has 1/w >= wb and U >= U_next, and a
+// rounded product is monotonic in both factors.  Elements met again on the walk
+// change nothing.  Absent elements (1/w = +inf) give inf or NaN, never below or
+// equal to a finite best.
+//
+// A CTA holds 32 contigs (lane = contig) with their 1/w rows transposed in shared
+// memory ([E][32]: the per-step gather is conflict-free).  Each warp takes one
+// register at a time: the first 32 entries of its visiting order and its U row
+// (by element, table UT) are loaded into registers one register ahead, stored in
+// the warp's shared slot, and walked in lock step until every lane's bound has
+// passed (entries past 32 come straight from the table).  Winners go to a shared
+// tile and leave as 4-byte code words, padding columns included.
+constexpr int kMC = 32;          // contigs per CTA, one per lane
+constexpr int kMThreads = 256;
+constexpr int kMWarps = kMThreads / 32;
+constexpr int kMHeavy = 8;       // smallest-1/w elements evaluated directly
+constexpr int kMChunk = 256;     // registers per pass; a multiple of 16
+constexpr int kMWinStride = kMChunk + 4;
+constexpr int kMRec = 32;        // visiting-order entries staged per register (one per lane)
+constexpr int kMUcPerLane = (kMaxElems / 2 + 31) / 32;   // 16-byte chunks of a U row per lane
+static_assert(kMaxElems % 2 == 0 && kMaxElems <= 5 * 32, "U rows in 16-byte chunks, 5 values per lane");
 
-__global__ void __launch_bounds__(128) k_minreduce(SketchArgs a) {
-  extern __shared__ __align__(16) double msh[];
-  const int E = a.n_elems, m = a.m;
-  double *sU = msh;                               // [E][kMRegs]
-  double *sW = msh + (size_t)E * kMRegs;          // [kMCon][E]   1/w, +inf = absent
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int r0 = blockIdx.x * kMRegs;
-  const int r = r0 + lane;
-  for (int i = threadIdx.x; i < E * kMRegs; i += blockDim.x) {
-    const int e = i / kMRegs, rr = r0 + (i - e * kMRegs);
-    sU[i] = rr < m ? __ldg(a.U + (size_t)e * m + rr) : 0.0;
+__host__ __device__ constexpr size_t minreduce_smem(int E) {
+  return (size_t)E * kMC * sizeof(double)            // sW   [E][kMC]
+         + (size_t)kMHeavy * kMC * sizeof(double)     // sHw  [kMHeavy][kMC]
+         + (size_t)kMC * sizeof(double)               // sWb  [kMC]
+         + (size_t)kMWarps * kMRec * 16               // sRec [kMWarps][kMRec]
+         + (size_t)kMWarps * E * sizeof(double)       // sUc  [kMWarps][E]
+         + (size_t)kMHeavy * kMC                      // sHe  [kMHeavy][kMC]
+         + (size_t)kMC * kMWinStride;                 // sWin [kMC][kMWinStride]
+}
+
+__device__ __forceinline__ void lex_min(double h, int e, double &best, int &win) {
+  if (h < best || (h == best && e < win)) {
+    best = h;
+    win = e;
   }
+}
+
+__device__ __forceinline__ void cswap(uint64_t &a, int &ia, uint64_t &b, int &ib) {
+  if (b < a) {
+    const uint64_t t = a; a = b; b = t;
+    const int u = ia; ia = ib; ib = u;
+  }
+}
+
+// One register's staging data, loaded a register ahead: entry `lane` of the
+// visiting order and the lane's 16-byte chunks of the U row.
+struct MinStage {
+  double2 rec;
+  double2 uc[kMUcPerLane];
+};
+
+__device__ __forceinline__ void min_fetch(MinStage &st, const double2 *ord, const double2 *ut,
+                                          int r, int E, int lane) {
+  const int half = E >> 1;
+  st.rec = lane < E ? __ldg(ord + (size_t)r * E + lane) : make_double2(0.0, 0.0);
+#pragma unroll
+  for (int q = 0; q < kMUcPerLane; ++q) {
+    const int ch = lane + 32 * q;
+    st.uc[q] = ch < half ? __ldg(ut + (size_t)r * half + ch) : make_double2(0.0, 0.0);
+  }
+}
+
+__global__ void __launch_bounds__(kMThreads, 3) k_minreduce(SketchArgs a) {
+  extern __shared__ __align__(16) unsigned char msh[];
+  const int E = a.n_elems, m = a.m, mpad = a.mpad;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double *sW = reinterpret_cast<double *>(msh);
+  double *sHw = sW + (size_t)E * kMC;
+  double *sWb = sHw + kMHeavy * kMC;
+  double2 *sRec = reinterpret_cast<double2 *>(sWb + kMC);
+  double *sUc = reinterpret_cast<double *>(sRec + kMWarps * kMRec);
+  uint8_t *sHe = reinterpret_cast<uint8_t *>(sUc + (size_t)kMWarps * E);
+  uint8_t *sWin = sHe + kMHeavy * kMC;
+  double2 *myRec = sRec + warp * kMRec;
+  double *myUc = sUc + (size_t)warp * E;
+  const int64_t c0 = (int64_t)blockIdx.x * kMC;
+  const int nc = (int)(a.n - c0 < kMC ? a.n - c0 : kMC);
   const double inf = __longlong_as_double(0x7FF0000000000000LL);
-  for (int b = 0; b < kMBatches; ++b) {
-    const int64_t c0 = ((int64_t)blockIdx.y * kMBatches + b) * kMCon;
-    if (c0 >= a.n) break;
-    __syncthreads();
-    for (int i = threadIdx.x; i < kMCon * E; i += blockDim.x) {
-      const int cl = i / E;
-      sW[i] = (c0 + cl < a.n) ? __ldg(a.elem_winv + c0 * E + i) : inf;
+  const uint64_t kNone = ~0ull;                      // key of a slot that is no element
+  for (int i = threadIdx.x; i < kMC * E; i += kMThreads) {
+    const int c = i / E, e = i - c * E;
+    sW[e * kMC + c] = c < nc ? __ldg(a.elem_winv + c0 * E + i) : inf;
+  }
+  // Heavy sets.  A non-negative double orders as its bit pattern, so 1/w values
+  // are compared as 64-bit keys.  Each lane sorts its (up to 5) values; kMHeavy + 1
+  // rounds of a warp minimum over the lanes' heads take one element each (the
+  // lowest lane on ties), the last round giving the bound.
+  for (int c = warp; c < kMC; c += kMWarps) {
+    uint64_t v[5];
+    int id[5];
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      const int e = lane + 32 * j;
+      id[j] = e;
+      v[j] = (c < nc && e < E) ? (uint64_t)__double_as_longlong(__ldg(a.elem_winv + (c0 + c) * E + e))
+                                : kNone;
     }
-    __syncthreads();
-    double best[8];
-    int win[8];
+    cswap(v[0], id[0], v[1], id[1]); cswap(v[3], id[3], v[4], id[4]);
+    cswap(v[2], id[2], v[4], id[4]); cswap(v[2], id[2], v[3], id[3]);
+    cswap(v[0], id[0], v[3], id[3]); cswap(v[0], id[0], v[2], id[2]);
+    cswap(v[1], id[1], v[4], id[4]); cswap(v[1], id[1], v[3], id[3]);
+    cswap(v[1], id[1], v[2], id[2]);
+    for (int i = 0; i <= kMHeavy; ++i) {
+      uint64_t mn = v[0];
 #pragma unroll
-    for (int t = 0; t < 8; ++t) { best[t] = inf; win[t] = -1; }
-    const double *wrow = sW + (size_t)warp * 8 * E;     // [8 contigs][E]
-    for (int e = 0; e < E; ++e) {
-      const double u = sU[e * kMRegs + lane];
-#pragma unroll
-      for (int t = 0; t < 8; ++t) {
-        const double h = __dmul_rn(wrow[t * E + e], u);
-        if (h < best[t]) { best[t] = h; win[t] = e; }
+      for (int o = 16; o; o >>= 1) {
+        const uint64_t ov = __shfl_xor_sync(0xffffffffu, mn, o);
+        mn = ov < mn ? ov : mn;
       }
-    }
-    if (r < m) {
+      const int src = __ffs(__ballot_sync(0xffffffffu, v[0] == mn)) - 1;
+      const int ej = __shfl_sync(0xffffffffu, id[0], src);
+      if (i < kMHeavy) {
+        if (lane == src) {
 #pragma unroll
-      for (int t = 0; t < 8; ++t) {
-        const int64_t c = c0 + warp * 8 + t;
-        if (c >= a.n) break;
-        uint8_t code = 0;
-        uint32_t w32 = 0;
-        if (win[t] >= 0) {
-          code = __ldg(a.codeA + (size_t)win[t] * m + r);
-          w32 = __ldg(a.W32 + (size_t)win[t] * m + r);
+          for (int j = 0; j < 4; ++j) { v[j] = v[j + 1]; id[j] = id[j + 1]; }
+          v[4] = kNone;
         }
-        a.codesA[c * a.mpad + r] = code;
-        a.codesB[c * a.mpad + r] = code ? code : (uint8_t)0xFF;
-        if (a.winners32) a.winners32[c * m + r] = w32;
+        if (lane == 0) {
+          const bool real = mn != kNone;
+          sHe[i * kMC + c] = real ? (uint8_t)ej : (uint8_t)0;
+          sHw[i * kMC + c] = real ? __longlong_as_double((long long)mn) : inf;
+        }
+      } else if (lane == 0) {
+        sWb[c] = mn != kNone ? __longlong_as_double((long long)mn) : inf;
       }
     }
+  }
+  __syncthreads();
+  int he[kMHeavy];
+  double hw[kMHeavy];
+#pragma unroll
+  for (int i = 0; i < kMHeavy; ++i) {
+    he[i] = sHe[i * kMC + lane];
+    hw[i] = sHw[i * kMC + lane];
+  }
+  const double wb = sWb[lane];
+  const bool empty = lane >= nc || !(hw[0] < inf);
+  const double2 *ord = reinterpret_cast<const double2 *>(a.order);
+  const double2 *ut = reinterpret_cast<const double2 *>(a.UT);
+  const int half = E >> 1;
+  for (int rb = 0; rb < mpad; rb += kMChunk) {
+    const int rn = (m - rb < kMChunk) ? m - rb : kMChunk;
+    MinStage st;
+    if (warp < rn) min_fetch(st, ord, ut, rb + warp, E, lane);
+    for (int rl = warp; rl < rn; rl += kMWarps) {
+      const int r = rb + rl;
+      myRec[lane] = st.rec;
+#pragma unroll
+      for (int q = 0; q < kMUcPerLane; ++q) {
+        const int ch = lane + 32 * q;
+        if (ch < half) reinterpret_cast<double2 *>(myUc)[ch] = st.uc[q];
+      }
+      __syncwarp();
+      if (rl + kMWarps < rn) min_fetch(st, ord, ut, r + kMWarps, E, lane);
+      double best = inf;
+      int win = -1;
+      bool done = empty;
+      if (!done) {
+#pragma unroll
+        for (int i = 0; i < kMHeavy; ++i) lex_min(__dmul_rn(hw[i], myUc[he[i]]), he[i], best, win);
+      }
+      for (int k = 0; k < E; ++k) {
+        if (__all_sync(0xffffffffu, done)) break;
+        const double2 v = k < kMRec ? myRec[k] : __ldg(ord + (size_t)r * E + k);
+        if (!done) {
+          if (__dmul_rn(wb, v.x) > best) {
+            done = true;
+          } else {
+            const int e = (int)__double_as_longlong(v.y);
+            lex_min(__dmul_rn(sW[e * kMC + lane], v.x), e, best, win);
+          }
+        }
+      }
+      if (lane < nc) sWin[lane * kMWinStride + rl] = win < 0 ? (uint8_t)0xFF : (uint8_t)win;
+      __syncwarp();
+    }
+    __syncthreads();
+    // code words: columns [rb, rend) of the nc rows; padding columns A = 0, B = 0xFF
+    const int rend = (rb + kMChunk < mpad) ? rb + kMChunk : mpad;
+    const int q4 = (rend - rb) >> 2;
+    for (int i = threadIdx.x; i < nc * q4; i += kMThreads) {
+      const int cc = i / q4, rl = (i - cc * q4) * 4, r4 = rb + rl;
+      const uint32_t wins = *reinterpret_cast<const uint32_t *>(sWin + cc * kMWinStride + rl);
+      uint32_t va = 0, vb = 0;
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int rr = r4 + b;
+        uint32_t code = 0;
+        if (rr < m) {
+          const uint32_t wi = (wins >> (8 * b)) & 0xFFu;
+          uint32_t w32 = 0;
+          if (wi != 0xFFu) {
+            code = __ldg(a.codeA + (size_t)wi * m + rr);
+            w32 = __ldg(a.W32 + (size_t)wi * m + rr);
+          }
+          if (a.winners32) a.winners32[(c0 + cc) * m + rr] = w32;
+        }
+        va |= code << (8 * b);
+        vb |= (code ? code : 0xFFu) << (8 * b);
+      }
+      *reinterpret_cast<uint32_t *>(a.codesA + (c0 + cc) * mpad + r4) = va;
+      *reinterpret_cast<uint32_t *>(a.codesB + (c0 + cc) * mpad + r4) = vb;
+    }
+    __syncthreads();
   }
 }
 
@@ -288,14 +442,10 @@ void launch_count(const SketchArgs &a, cudaStream_t s) {
 
 void launch_minreduce(const SketchArgs &a, cudaStream_t s) {
   if (a.n == 0) return;
-  // padding registers [m, mpad): A = 0, B = 0xFF (never equal)
-  cudaMemsetAsync(a.codesA, 0, (size_t)a.n * a.mpad, s);
-  cudaMemsetAsync(a.codesB, 0xFF, (size_t)a.n * a.mpad, s);
-  const size_t smem = (size_t)a.n_elems * (kMRegs + kMCon) * sizeof(double);
+  const size_t smem = minreduce_smem(a.n_elems);
   cudaFuncSetAttribute(k_minreduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  const dim3 grid((unsigned)((a.m + kMRegs - 1) / kMRegs),
-                  (unsigned)((a.n + kMCon * kMBatches - 1) / (kMCon * kMBatches)));
-  k_minreduce<<<grid, 128, smem, s>>>(a);
+  const int64_t grid = (a.n + kMC - 1) / kMC;
+  k_minreduce<<<(unsigned)grid, kMThreads, smem, s>>>(a);
 }
 
 }  // namespace rbg

@@ -16,8 +16,8 @@
 // (cudaGetSymbolAddress, once per device, with that device current); make that
 // first call before any stream capture.  All calls share the array and it keeps
 // the previous call's contents; every part a call reads is written by the same
-// call first (the launchers clear the code padding), but two calls that overlap
-// on the GPU race on it.
+// call first (the register-minimum kernel writes the code padding too), but two
+// calls that overlap on the GPU race on it.
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -71,7 +71,8 @@ extern "C" int rbg_build_pmh_winners_noalloc(const rbg_params *p, const char *se
   const int E = p->k == 4 ? 136 : (p->k == 3 ? 32 : (p->k == 2 ? 10 : 2));
   const int64_t nwords = (nbases + 15) / 16 + 1;
   size_t off = 0;
-  const size_t oU = off;       off += up256((size_t)E * m * sizeof(double));
+  const size_t oOrd = off;     off += up256((size_t)E * m * sizeof(RegOrder));
+  const size_t oUT = off;      off += up256((size_t)E * m * sizeof(double));
   const size_t oCode = off;    off += up256((size_t)E * m);
   const size_t oW = off;       off += up256((size_t)E * m * sizeof(uint32_t));
   const size_t oRank = off;    off += up256(256 * sizeof(int16_t));
@@ -132,7 +133,8 @@ extern "C" int rbg_build_pmh_winners_noalloc(const rbg_params *p, const char *se
   int16_t rank[256];
   for (int v = 0; v < 256; ++v) rank[v] = v < (int)t->rank_of_code.size() ? (int16_t)t->rank_of_code[v] : -1;
   const size_t EM = (size_t)E * m;
-  if (cudaMemcpyAsync(S + oU, t->U.data(), EM * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+  if (cudaMemcpyAsync(S + oOrd, t->order.data(), EM * sizeof(RegOrder), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(S + oUT, t->UT.data(), EM * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess ||
       cudaMemcpyAsync(S + oCode, p->win_bits == 16 ? t->code16.data() : t->code32.data(), EM,
                       cudaMemcpyHostToDevice, s) != cudaSuccess ||
       cudaMemcpyAsync(S + oW, t->W32.data(), EM * sizeof(uint32_t), cudaMemcpyHostToDevice, s) != cudaSuccess ||
@@ -154,7 +156,8 @@ extern "C" int rbg_build_pmh_winners_noalloc(const rbg_params *p, const char *se
   a.rank_of_code = (const int16_t *)(S + oRank);
   a.elem_winv = (double *)(S + oWinv);
   a.elem_cnt = (int32_t *)(S + oCnt);
-  a.U = (const double *)(S + oU);
+  a.order = (const RegOrder *)(S + oOrd);
+  a.UT = (const double *)(S + oUT);
   a.codeA = (const uint8_t *)(S + oCode);
   a.W32 = (const uint32_t *)(S + oW);
   a.codesA = S + oA;

@@ -24,6 +24,7 @@
 // reference's expressions (the TED step, the exponential tail and the
 // ziggurat's rejection test); contract = 0 reproduces a -ffp-contract=off
 // build of the reference instead.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -212,6 +213,14 @@ std::shared_ptr<const PmhTables> pmh_tables(int k, int m, uint64_t seed, int con
   for (int e = 0; e < E; ++e)
     element_stream(fmix64((uint64_t)t->canon_codes[e], seed), m, ted, first_inv,
                    contract != 0, &t->U[(size_t)e * m], &t->W64[(size_t)e * m], perm);
+  t->order.resize((size_t)m * E);
+  t->UT.resize((size_t)m * E);
+  for (int r = 0; r < m; ++r) {
+    for (int e = 0; e < E; ++e) t->UT[(size_t)r * E + e] = t->U[(size_t)e * m + r];
+    RegOrder *o = &t->order[(size_t)r * E];
+    for (int e = 0; e < E; ++e) o[e] = RegOrder{t->U[(size_t)e * m + r], (uint32_t)e, 0u};
+    std::stable_sort(o, o + E, [](const RegOrder &x, const RegOrder &y) { return x.u < y.u; });
+  }
   t->W32.resize((size_t)E * m);
   t->W16.resize((size_t)E * m);
   for (size_t q = 0; q < t->W64.size(); ++q) {

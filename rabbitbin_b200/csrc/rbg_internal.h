@@ -25,12 +25,22 @@ constexpr int kRowsPerCta = 32;    // rows of one all-pairs CTA (one per lane)
 // k-mer e has a fixed ProbMinHash stream: the register it visits at each step
 // and the weight-independent part U of the value it offers there
 // (hv = (1/w) * U).  Tables are indexed [e][register].
+// One entry of a register's visiting order: the elements of register r sorted
+// by ascending U[e][r], ties by ascending e (16 bytes, one vector load).
+struct RegOrder {
+  double u;
+  uint32_t e;
+  uint32_t pad;
+};
+
 struct PmhTables {
   int k = 0, m = 0, n_elems = 0, contract = 1;
   uint64_t seed = 0;
   std::vector<int> canon_codes;        // ascending canonical codes, size n_elems
   std::vector<int> rank_of_code;       // 4^k -> element index or -1
   std::vector<double> U;               // [n_elems][m]
+  std::vector<RegOrder> order;         // [m][n_elems] visiting order per register
+  std::vector<double> UT;              // [m][n_elems] U by register, then element
   std::vector<uint64_t> W64;           // [n_elems][m] winner (RNG state)
   std::vector<uint32_t> W32;           // folded h ^ (h >> 32)
   std::vector<uint16_t> W16;           // fold_win16(W32)
@@ -61,7 +71,8 @@ struct SketchArgs {
   double *elem_winv = nullptr;         // [n][n_elems]
   int32_t *elem_cnt = nullptr;         // [n] number of present elements
   // tables
-  const double *U = nullptr;           // [E][m]
+  const RegOrder *order = nullptr;     // [m][E] elements by ascending U per register
+  const double *UT = nullptr;          // [m][E] U by register, then element
   const uint8_t *codeA = nullptr;      // [E][m]
   const uint32_t *W32 = nullptr;       // [E][m]
   // outputs
