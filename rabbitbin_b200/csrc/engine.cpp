@@ -368,27 +368,72 @@ void run_graph(rbg_ctx *c, const rbg_params *p) {
   g.maxcnt_all = c->maxc_all.as<uint32_t>();
   g.stats = c->stats.as<unsigned long long>();
   g.key_floor = admission_floor();
-  CK(cudaMemsetAsync(c->stats.p, 0, 2 * sizeof(unsigned long long), c->stream));
   CK(cudaStreamWaitEvent(c->stream, c->ev_aux, 0));   // unit rows, anynz, column norms
   c->prep_done = false;
-  {
+  std::vector<uint32_t> maxc;
+  const uint32_t *maxc_host = nullptr;
+  if (g.prefilter && n > 0) {
+    // Tensor-core regime: every unordered pair scored once, admitted pairs
+    // listed, then each row's top-K selected from its keys.  The row maxima and
+    // the pair count come back while the selection runs; a pass whose pairs did
+    // not fit the list is run again with a larger one.
+    const size_t nm4 = (size_t)((n1 + 3) & ~3);
+    c->pin.ensure(nm4 * sizeof(uint32_t) + sizeof(unsigned long long));
+    uint32_t *hmax = c->pin.as<uint32_t>();
+    unsigned long long *hnp = (unsigned long long *)(hmax + nm4);
+    if (c->sym_cap == 0) c->sym_cap = std::max<uint64_t>(1u << 20, (uint64_t)n * 128);
+    for (;;) {
+      c->sym_pairs.ensure(c->sym_cap * sizeof(uint4));
+      c->sym_keys.ensure(2 * c->sym_cap * sizeof(uint64_t));
+      c->sym_rowcnt.ensure(n1 * sizeof(int32_t));
+      c->sym_rowoff.ensure((n1 + 1) * sizeof(int64_t));
+      c->sym_np.ensure(sizeof(unsigned long long));
+      CK(cudaMemsetAsync(c->stats.p, 0, 2 * sizeof(unsigned long long), c->stream));
+      CK(cudaMemsetAsync(c->maxc_cand.p, 0, n1 * sizeof(uint32_t), c->stream));
+      CK(cudaMemsetAsync(c->sym_rowcnt.p, 0, n1 * sizeof(int32_t), c->stream));
+      CK(cudaMemsetAsync(c->sym_np.p, 0, sizeof(unsigned long long), c->stream));
+      SymOut o;
+      o.pairs = c->sym_pairs.as<uint4>();
+      o.npairs = c->sym_np.as<unsigned long long>();
+      o.cap = c->sym_cap;
+      o.rowcnt = c->sym_rowcnt.as<int32_t>();
+      launch_allpairs_sym(g, o, c->stream);
+      CK(cudaGetLastError());
+      CK(cudaEventRecord(c->ev[6], c->stream));
+      CK(cudaMemcpyAsync(hmax, c->maxc_cand.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                         c->stream));
+      CK(cudaMemcpyAsync(hnp, c->sym_np.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                         c->stream));
+      CK(cudaEventRecord(c->ev[10], c->stream));
+      launch_rows_topk(g, o, c->sym_rowoff.as<int64_t>(), c->sym_keys.as<uint64_t>(), c->stream);
+      CK(cudaGetLastError());
+      c->launches += 4;
+      CK(cudaEventSynchronize(c->ev[10]));
+      if (*hnp <= c->sym_cap) break;
+      CK(cudaStreamSynchronize(c->stream));
+      c->sym_cap = *hnp + *hnp / 4;
+    }
+    maxc_host = hmax;
+  } else {
+    CK(cudaMemsetAsync(c->stats.p, 0, 2 * sizeof(unsigned long long), c->stream));
     const size_t slots = (size_t)((n + 31) / 32) * allpairs_slices(n, K) * 32;
     c->cand_buf.ensure(slots * allpairs_cap(K) * sizeof(uint64_t));
     c->cand_cnt.ensure(slots * sizeof(int32_t));
     CK(cudaMemsetAsync(c->maxc_cand.p, 0, n1 * sizeof(uint32_t), c->stream));
     CK(cudaMemsetAsync(c->maxc_all.p, 0, n1 * sizeof(uint32_t), c->stream));
+    launch_allpairs(g, c->cand_buf.as<uint64_t>(), c->cand_cnt.as<int32_t>(), c->stream);
+    c->launches += n ? 2 : 0;
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(c->ev[6], c->stream));
+    maxc.assign(n1, 0);
+    CK(cudaMemcpyAsync(maxc.data(), fused ? c->maxc_cand.p : c->maxc_all.p, n * sizeof(uint32_t),
+                       cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    maxc_host = maxc.data();
   }
-  launch_allpairs(g, c->cand_buf.as<uint64_t>(), c->cand_cnt.as<int32_t>(), c->stream);
-  c->launches += n ? 1 : 0;
-  CK(cudaGetLastError());
-  CK(cudaEventRecord(c->ev[6], c->stream));
 
   // calibration on the host (rand() sequence of the reference)
-  std::vector<uint32_t> maxc(n1, 0);
-  CK(cudaMemcpyAsync(maxc.data(), fused ? c->maxc_cand.p : c->maxc_all.p, n * sizeof(uint32_t),
-                     cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  const double simCutoff = calibrate_cutoff(maxc.data(), n, fused, m, sv_d, sv_f, p->coverage, p->seed);
+  const double simCutoff = calibrate_cutoff(maxc_host, n, fused, m, sv_d, sv_f, p->coverage, p->seed);
   c->sim_cutoff = simCutoff;
   CK(cudaEventRecord(c->ev[7], c->stream));
 
@@ -666,7 +711,8 @@ int rbg_destroy(rbg_ctx *c) {
                   &c->anynz, &c->colnorm, &c->svbits, &c->topk, &c->topk_cnt, &c->maxc_cand,
                   &c->maxc_all, &c->stats, &c->pairs, &c->pair_out, &c->nbr, &c->nbr_sv,
                   &c->nbr_cnt, &c->row_edges, &c->e_from, &c->e_to, &c->e_scomp, &c->e_score,
-                  &c->badflag, &c->tmp, &c->cand_buf, &c->cand_cnt, &c->colacc, &c->unit16};
+                  &c->badflag, &c->tmp, &c->cand_buf, &c->cand_cnt, &c->colacc, &c->unit16,
+                  &c->sym_pairs, &c->sym_np, &c->sym_rowcnt, &c->sym_rowoff, &c->sym_keys};
   for (DBuf *b : bufs) b->release();
   if (c->tables) c->tables->release();
   release_batch_graphs(c);

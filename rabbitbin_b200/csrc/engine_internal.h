@@ -225,7 +225,10 @@ struct rbg_ctx {
   rbg::DBuf unit, unit16, anynz, colnorm, svbits, topk, topk_cnt, maxc_cand, maxc_all, stats;
   rbg::DBuf pairs, pair_out, nbr, nbr_sv, nbr_cnt, row_edges, cand_buf, cand_cnt;
   rbg::DBuf e_from, e_to, e_scomp, e_score, badflag, tmp, colacc;
-  rbg::HBuf pin;
+  // symmetric all-pairs pass: admitted pairs, per-row counts, offsets and keys
+  rbg::DBuf sym_pairs, sym_np, sym_rowcnt, sym_rowoff, sym_keys;
+  uint64_t sym_cap = 0;                  // pair-list capacity (grows when a pass overflows)
+  rbg::HBuf pin;                         // row maxima and pair count read back for calibration
   int64_t n_edges = 0;
   double b0 = 0.0, sim_cutoff = 0.0;
   int path = 0;

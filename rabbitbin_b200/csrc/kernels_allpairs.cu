@@ -219,6 +219,71 @@ __device__ __forceinline__ void count_batch_coop(const GraphArgs &g, Warp &w, co
   compact_full_rows(w, w.cap - 32);
 }
 
+// Symmetric form of count_batch_coop: the same counts, then each survivor
+// (i = row0 + r, j) raises both rows' maxima (row i through the warp's own
+// state, row j by an atomic) and, when its similarity passes the admission
+// floor, is appended once to the pair list with both rows' counts raised.
+__device__ __forceinline__ void count_batch_sym(const GraphArgs &g, const SymOut &o, uint32_t *mxc,
+                                                int64_t row0, const int *q, int nq,
+                                                const unsigned char *sA) {
+  const int lane = threadIdx.x & 31;
+  const int m16 = g.mpad >> 4;
+  uint32_t mine = 0;
+  for (int p = 0; p < nq; p += 4) {
+    const uint4 *ra[4], *cb[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const unsigned e = (unsigned)q[p + u < nq ? p + u : p];
+      ra[u] = (const uint4 *)(sA + (size_t)(e >> 27) * g.mpad);
+      cb[u] = (const uint4 *)(g.codesB + (int64_t)(e & 0x07FFFFFFu) * g.mpad);
+    }
+    uint32_t acc[4] = {0u, 0u, 0u, 0u};
+    for (int t = lane; t < m16; t += 32) {
+      uint4 b[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) b[u] = __ldg(cb[u] + t);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) acc[u] = eq16(lds128(ra[u] + t), b[u], acc[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const uint32_t c = __reduce_add_sync(FULL, acc[u]) >> 7;
+      if (lane == p + u) mine = c;
+    }
+  }
+  const unsigned act = __ballot_sync(FULL, lane < nq);
+  bool adm = false;
+  int r = 0;
+  uint32_t j = 0, svb = 0;
+  if (lane < nq) {
+    const unsigned e = (unsigned)q[lane];
+    r = (int)(e >> 27);
+    j = e & 0x07FFFFFFu;
+    const unsigned grp = __match_any_sync(act, r);
+    const uint32_t mx = __reduce_max_sync(grp, mine);
+    if (lane == __ffs(grp) - 1 && mx > mxc[r]) mxc[r] = mx;
+    if (mine) atomicMax(g.maxcnt_cand + j, mine);
+    svb = __ldg(g.sv_bits + mine);
+    adm = svb > (uint32_t)(g.key_floor >> 32);
+  }
+  const unsigned am = __ballot_sync(FULL, adm);
+  if (am) {
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(o.npairs, (unsigned long long)__popc(am));
+    base = __shfl_sync(FULL, base, 0);
+    if (adm) {
+      const unsigned long long pos = base + (unsigned)__popc(am & ((1u << lane) - 1u));
+      if (pos < o.cap) {
+        const uint32_t i = (uint32_t)(row0 + r);
+        o.pairs[pos] = make_uint4(i, j, svb, 0u);
+        atomicAdd(o.rowcnt + i, 1);
+        atomicAdd(o.rowcnt + j, 1);
+      }
+    }
+  }
+  __syncwarp();
+}
+
 // Dense regime: one work item = 32 rows (row block bx) x the column slices
 // kWarps*by .. kWarps*by+3, one warp per slice.
 __device__ __forceinline__ void dense_item(const GraphArgs &g, uint64_t *gbuf, int32_t *gcnt,
@@ -369,10 +434,10 @@ __device__ __forceinline__ void ldsm_x2(uint32_t &r0, uint32_t &r1, const void *
 
 // Exact prune decision for up to 32 queued candidates (lane = candidate),
 // survivors appended to the counting queue.
-template <int SMAX>
-__device__ __forceinline__ void check_batch(const GraphArgs &g, Warp &w, const int *cq,
-                                            unsigned head, int nq, int64_t row0, int *q,
-                                            int &qn, float lo, float hi,
+template <int SMAX, bool SYM>
+__device__ __forceinline__ void check_batch(const GraphArgs &g, Warp &w, const SymOut &o,
+                                            const int *cq, unsigned head, int nq, int64_t row0,
+                                            int *q, int &qn, float lo, float hi,
                                             unsigned long long &n_cmp, const float *sU,
                                             int SuP, const unsigned char *sA) {
   const int lane = threadIdx.x & 31;
@@ -409,7 +474,8 @@ __device__ __forceinline__ void check_batch(const GraphArgs &g, Warp &w, const i
   qn += __popc(m);
   __syncwarp();
   if (qn >= 32) {
-    count_batch_coop(g, w, q, 32, sA);
+    if constexpr (SYM) count_batch_sym(g, o, w.mxc, row0, q, 32, sA);
+    else count_batch_coop(g, w, q, 32, sA);
     n_cmp += 1;
     if (lane + 32 < qn) q[lane] = q[lane + 32];
     __syncwarp();
@@ -417,16 +483,21 @@ __device__ __forceinline__ void check_batch(const GraphArgs &g, Warp &w, const i
   }
 }
 
-template <int KS, int SMAX>
+// SYM: the warp's slice is a slice of columns [row0, n) instead of [0, n), the
+// block's own rows only pair with later rows (j > i), and survivors go to the
+// pair list (count_batch_sym) instead of the rows' candidate buffers.
+template <int KS, int SMAX, bool SYM>
 __device__ __forceinline__ void tc_item(const GraphArgs &g, uint64_t *gbuf, int32_t *gcnt,
                                         int cap, int P, float lo, float hi, float lo16,
-                                        int64_t bx, int by, unsigned char *smem) {
+                                        int64_t bx, int by, unsigned char *smem,
+                                        const SymOut &o) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gq = lane >> 2, tq = lane & 3;
   const int64_t n = g.n;
   const int64_t row0 = bx * 32;
   const int slice = by * kWarps + warp;
-  const int64_t jb = n * slice / P, je = n * (slice + 1) / P;
+  const int64_t c_lo = SYM ? row0 : 0, span = n - c_lo;
+  const int64_t jb = c_lo + span * slice / P, je = c_lo + span * (slice + 1) / P;
   const int Kp = KS * 16;
   const int cstride = Kp * 2 + 16;                 // bytes per staged column (conflict-free ldmatrix)
 
@@ -462,7 +533,7 @@ __device__ __forceinline__ void tc_item(const GraphArgs &g, uint64_t *gbuf, int3
   cnt[lane] = 0;
   mxc[lane] = 0;
   const size_t bufrow = ((size_t)bx * P + slice) * 32;
-  Warp w{gbuf + bufrow * cap, cnt, thr, mxc, cap, g.K};
+  Warp w{SYM ? gbuf : gbuf + bufrow * cap, cnt, thr, mxc, cap, g.K};
   unsigned long long n_pref = 0, n_cmp = 0;
 
   // A fragments: rows mt*16 + gq (+8), k = ks*16 + 2*tq (+8)
@@ -529,7 +600,8 @@ __device__ __forceinline__ void tc_item(const GraphArgs &g, uint64_t *gbuf, int3
         for (int i = 0; i < 4; ++i) {
           const int rr = mt * 16 + gq + 8 * (i >> 1);
           const int cc = c0 + 2 * tq + (i & 1);
-          if (acc[mt][i] >= lo16 && cc < nc && row0 + rr < n) mk |= 1u << (mt * 4 + i);
+          if (acc[mt][i] >= lo16 && cc < nc && row0 + rr < n && (!SYM || jt + cc > row0 + rr))
+            mk |= 1u << (mt * 4 + i);
         }
       n_pref += 8;
       if (__any_sync(FULL, mk != 0)) {
@@ -554,7 +626,7 @@ __device__ __forceinline__ void tc_item(const GraphArgs &g, uint64_t *gbuf, int3
         tail += (unsigned)total;
         __syncwarp();
         while (tail - head >= 32) {
-          check_batch<SMAX>(g, w, cq, head, 32, row0, q, qn, lo, hi, n_cmp, sU, SuP, sA);
+          check_batch<SMAX, SYM>(g, w, o, cq, head, 32, row0, q, qn, lo, hi, n_cmp, sU, SuP, sA);
           head += 32;
         }
       }
@@ -563,24 +635,28 @@ __device__ __forceinline__ void tc_item(const GraphArgs &g, uint64_t *gbuf, int3
   }
   while (tail != head) {
     const int nq = (int)(tail - head < 32 ? tail - head : 32);
-    check_batch<SMAX>(g, w, cq, head, nq, row0, q, qn, lo, hi, n_cmp, sU, SuP, sA);
+    check_batch<SMAX, SYM>(g, w, o, cq, head, nq, row0, q, qn, lo, hi, n_cmp, sU, SuP, sA);
     head += (unsigned)nq;
   }
   if (qn > 0) {
     n_cmp += lane < qn;
-    count_batch_coop(g, w, q, qn, sA);
+    if constexpr (SYM) count_batch_sym(g, o, mxc, row0, q, qn, sA);
+    else count_batch_coop(g, w, q, qn, sA);
   }
   if (g.stats) {
+    // ordered pairs: a symmetric evaluation stands for both orders
     const unsigned a = __reduce_add_sync(FULL, (unsigned)n_pref),
                    b = __reduce_add_sync(FULL, (unsigned)n_cmp);
     if (lane == 0) {
-      if (a) atomicAdd(g.stats, (unsigned long long)a);
-      if (b) atomicAdd(g.stats + 1, (unsigned long long)b);
+      if (a) atomicAdd(g.stats, (unsigned long long)a * (SYM ? 2u : 1u));
+      if (b) atomicAdd(g.stats + 1, (unsigned long long)b * (SYM ? 2u : 1u));
     }
   }
   __syncwarp();
-  compact_full_rows(w, g.K);
-  gcnt[bufrow + lane] = cnt[lane];
+  if constexpr (!SYM) {
+    compact_full_rows(w, g.K);
+    gcnt[bufrow + lane] = cnt[lane];
+  }
   const int64_t row = row0 + lane;
   if (row < n && mxc[lane]) atomicMax(g.maxcnt_cand + row, mxc[lane]);
 }
@@ -590,7 +666,23 @@ __global__ void __launch_bounds__(kWarps * 32)
 k_allpairs_tc(GraphArgs g, uint64_t *gbuf, int32_t *gcnt, int cap, int P, float lo, float hi,
               float lo16) {
   extern __shared__ __align__(16) unsigned char smem[];
-  tc_item<KS, SMAX>(g, gbuf, gcnt, cap, P, lo, hi, lo16, blockIdx.x, blockIdx.y, smem);
+  tc_item<KS, SMAX, false>(g, gbuf, gcnt, cap, P, lo, hi, lo16, blockIdx.x, blockIdx.y, smem,
+                           SymOut{});
+}
+
+// Symmetric pass: CTA x scores row block x and row block B-1-x (columns from
+// the block's first row on), so every CTA's column work is about n + 32.
+template <int KS, int SMAX>
+__global__ void __launch_bounds__(kWarps * 32)
+k_allpairs_tc_sym(GraphArgs g, int P, float lo, float hi, float lo16, SymOut o) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int64_t B = (g.n + 31) / 32;
+  const int64_t b1 = blockIdx.x, b2 = B - 1 - (int64_t)blockIdx.x;
+  tc_item<KS, SMAX, true>(g, nullptr, nullptr, 0, P, lo, hi, lo16, b1, blockIdx.y, smem, o);
+  if (b2 > b1) {
+    __syncthreads();
+    tc_item<KS, SMAX, true>(g, nullptr, nullptr, 0, P, lo, hi, lo16, b2, blockIdx.y, smem, o);
+  }
 }
 
 // Persistent form over a batch: CTAs pull (assembly, row block, slice group)
@@ -619,7 +711,8 @@ k_allpairs_batch(const BatchAsm *B, const int32_t *list, const int64_t *item0s, 
     const int64_t bx = local / G;
     const int by = (int)(local - bx * G);
     if constexpr (KS == 0) dense_item(g, b.gbuf, b.gcnt, b.cap, b.P, bx, by, smem);
-    else tc_item<KS, SMAX>(g, b.gbuf, b.gcnt, b.cap, b.P, b.lo, b.hi, b.lo16, bx, by, smem);
+    else tc_item<KS, SMAX, false>(g, b.gbuf, b.gcnt, b.cap, b.P, b.lo, b.hi, b.lo16, bx, by, smem,
+                                  SymOut{});
   }
 }
 
@@ -682,6 +775,82 @@ k_merge_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows) {
   }
   const BatchAsm &b = B[lo];
   merge_row(b.g, b.gbuf, b.gcnt, b.cap, b.P, r - b.row0, mk[wib]);
+}
+
+// Row offsets of the admitted keys: exclusive scan of the per-row counts, one CTA.
+__global__ void k_rows_scan(const int32_t *cnt, int64_t *off, int64_t n) {
+  __shared__ int64_t part[1024];
+  const int t = threadIdx.x;
+  const int64_t per = (n + 1023) / 1024;
+  const int64_t a = t * per, b = (a + per < n) ? a + per : n;
+  int64_t s = 0;
+  for (int64_t q = a; q < b; ++q) s += cnt[q];
+  part[t] = s;
+  __syncthreads();
+  for (int d = 1; d < 1024; d <<= 1) {
+    const int64_t add = (t >= d) ? part[t - d] : 0;
+    __syncthreads();
+    part[t] += add;
+    __syncthreads();
+  }
+  int64_t run = (t > 0) ? part[t - 1] : 0;
+  for (int64_t q = a; q < b; ++q) { off[q] = run; run += cnt[q]; }
+  if (t == 1023) off[n] = part[1023];
+}
+
+// Both keys of every admitted pair into their rows' segments (grid-stride over
+// the pairs written).  Positions count down from each row's end, so the row
+// counts return to zero.
+__global__ void k_scatter_pairs(SymOut o, const int64_t *off, uint64_t *keys) {
+  const unsigned long long np = *o.npairs < o.cap ? *o.npairs : o.cap;
+  for (unsigned long long p = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; p < np;
+       p += (unsigned long long)gridDim.x * blockDim.x) {
+    const uint4 x = o.pairs[p];
+    const uint64_t hi = (uint64_t)x.z << 32;
+    const int64_t pi = off[x.x] + atomicSub(o.rowcnt + x.x, 1) - 1;
+    keys[pi] = hi | (uint64_t)(~x.y);
+    const int64_t pj = off[x.y] + atomicSub(o.rowcnt + x.y, 1) - 1;
+    keys[pj] = hi | (uint64_t)(~x.x);
+  }
+}
+
+// Warp per row: the K best keys of the row's segment, streamed through a
+// 512-key shared buffer (the register radix select keeps the K best whenever it
+// fills).
+__global__ void __launch_bounds__(kMergeWarps * 32)
+k_select_rows(GraphArgs g, const int64_t *off, const uint64_t *keys) {
+  __shared__ uint64_t mk[kMergeWarps][kMergeBuf];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int64_t row = (int64_t)blockIdx.x * kMergeWarps + wib;
+  if (row >= g.n) return;
+  const int K = g.K;
+  const int64_t s0 = off[row];
+  const int64_t c = off[row + 1] - s0;
+  const uint64_t *src = keys + s0;
+  uint64_t *buf = mk[wib];
+  if (c <= K) {
+    for (int64_t i = lane; i < c; i += 32) g.topk[row * K + i] = src[i];
+    if (lane == 0) g.topk_cnt[row] = (int32_t)c;
+    return;
+  }
+  int fill = 0;
+  for (int64_t i0 = 0; i0 < c;) {
+    const int take = (int)(c - i0 < (int64_t)(kMergeBuf - fill) ? c - i0 : (int64_t)(kMergeBuf - fill));
+    for (int i = lane; i < take; i += 32) buf[fill + i] = src[i0 + i];
+    fill += take;
+    i0 += take;
+    __syncwarp();
+    if (fill == kMergeBuf) {
+      select_topk(buf, fill, K);
+      fill = K;
+    }
+  }
+  if (fill > K) {
+    select_topk(buf, fill, K);
+    fill = K;
+  }
+  for (int i = lane; i < fill; i += 32) g.topk[row * K + i] = buf[i];
+  if (lane == 0) g.topk_cnt[row] = fill;
 }
 
 size_t dense_smem(int mpad) {
@@ -760,6 +929,39 @@ void launch_allpairs(const GraphArgs &g, uint64_t *gbuf, int32_t *gcnt, cudaStre
 #undef RBG_TC
   k_merge_topk<<<(unsigned)((g.n + kMergeWarps - 1) / kMergeWarps), kMergeWarps * 32, 0, s>>>(
       g, gbuf, gcnt, cap, P);
+}
+
+void launch_allpairs_sym(const GraphArgs &g, const SymOut &o, cudaStream_t s) {
+  if (g.n == 0) return;
+  const int P = allpairs_slices(g.n, g.K);
+  const int64_t B = (g.n + 31) / 32;
+  const dim3 grid((unsigned)((B + 1) / 2), (unsigned)(P / kWarps));
+  float lo, hi, lo16;
+  prefilter_bands(g.S, g.prefilter_eps, &lo, &hi, &lo16);
+  const int v = allpairs_variant(g);
+  const size_t smem = tc_smem(v, g.mpad, g.Su);
+#define RBG_TS(KS, SM)                                                                        \
+  do {                                                                                        \
+    cudaFuncSetAttribute(k_allpairs_tc_sym<KS, SM>,                                           \
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);             \
+    k_allpairs_tc_sym<KS, SM><<<grid, kWarps * 32, smem, s>>>(g, P, lo, hi, lo16, o);         \
+  } while (0)
+  if (v == 1) RBG_TS(1, 16);
+  else if (v == 2) RBG_TS(2, 32);
+  else RBG_TS(4, 64);
+#undef RBG_TS
+}
+
+void launch_rows_topk(const GraphArgs &g, const SymOut &o, int64_t *rowoff, uint64_t *keys,
+                      cudaStream_t s) {
+  if (g.n == 0) return;
+  k_rows_scan<<<1, 1024, 0, s>>>(o.rowcnt, rowoff, g.n);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  k_scatter_pairs<<<(unsigned)(sms * 8), 256, 0, s>>>(o, rowoff, keys);
+  k_select_rows<<<(unsigned)((g.n + kMergeWarps - 1) / kMergeWarps), kMergeWarps * 32, 0, s>>>(
+      g, rowoff, keys);
 }
 
 void launch_allpairs_batch(const BatchAsm *B, int variant, const int32_t *list,

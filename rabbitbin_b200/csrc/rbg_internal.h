@@ -141,6 +141,22 @@ void launch_colnorm(const GraphArgs &g, double *acc, cudaStream_t s);
 void launch_pair_counts(const uint8_t *codesA, const uint8_t *codesB, int mpad, int m,
                         const int64_t *pairs, int npairs, uint32_t *out, cudaStream_t s);
 void launch_allpairs(const GraphArgs &g, uint64_t *gbuf, int32_t *gcnt, cudaStream_t s);
+
+// Output of the symmetric all-pairs pass (each unordered pair scored once): the
+// admitted pairs and, per row, how many admitted keys it holds (both ends).
+struct SymOut {
+  uint4 *pairs = nullptr;               // {i, j, similarity bits, 0}, i < j
+  unsigned long long *npairs = nullptr; // admitted pairs found (may exceed cap)
+  uint64_t cap = 0;                     // pairs written: min(npairs, cap)
+  int32_t *rowcnt = nullptr;            // [n], zero before the pass
+};
+// Symmetric pass of the abundance-pruned (tensor-core) regime: row maxima into
+// g.maxcnt_cand, admitted pairs into o.  Requires allpairs_variant(g) != 0.
+void launch_allpairs_sym(const GraphArgs &g, const SymOut &o, cudaStream_t s);
+// Per-row top-K of the admitted pairs (both keys of each pair) into g.topk /
+// g.topk_cnt.  rowoff [n+1] and keys [2 * cap] are scratch; o.rowcnt ends zero.
+void launch_rows_topk(const GraphArgs &g, const SymOut &o, int64_t *rowoff, uint64_t *keys,
+                      cudaStream_t s);
 int allpairs_slices(int64_t n, int K);
 int allpairs_cap(int K);
 
