@@ -41,10 +41,11 @@ WORKLOAD = dict(workload="binning-scale assembly: 100 genomes, 50000 contigs, S=
                 n_genomes=100, n_contigs=50000, samples=20, sketch_m=500, max_edges=200,
                 inputs_exceed_l2=True, seed=1)
 METRIC = "contig-pairs scored/s"
-# DRAM bytes (read + write) of the all-pairs kernel per ordered pair, from the
-# ncu capture of the 30,000-contig case (profiles/k_allpairs_tc_fused30k.txt),
-# scaled to a launch by its n^2 ordered pairs.
-ALLPAIRS_TRAFFIC_PER_PAIR = 0.147
+# DRAM bytes (read + write) of the symmetric all-pairs kernel per unordered
+# pair, from the ncu capture of the 30,000-contig case
+# (profiles/k_allpairs_tc_sym_fused30k.md: 61.0 MB over 4.5e8 pairs), scaled to
+# a launch by its n(n-1)/2 pairs.
+ALLPAIRS_TRAFFIC_PER_PAIR = 0.136
 UNIT = "pairs/s"
 
 
@@ -206,14 +207,15 @@ def _finish(args, ctx, asm, timings, last, ms, value, result_e2e, clk, world, ra
     n, S, m = asm.n, WORKLOAD["samples"], WORKLOAD["sketch_m"]
     mpad = (m + 15) // 16 * 16
     ap_ms = last["allpairs_ms"]
-    # dominant kernel: the all-pairs pass.  Its tensor-core prefilter multiplies
-    # the FP16 unit rank rows of every ordered pair (2 S FLOPs per pair, n^2
-    # pairs per launch); the register compares of the survivors run on the
-    # integer pipe (pairs_compared x m byte compares).
-    flops = 2.0 * S * n * n
+    # dominant kernel: the symmetric all-pairs pass.  Its tensor-core prefilter
+    # multiplies the FP16 unit rank rows of every unordered pair once (2 S FLOPs
+    # per pair, n(n-1)/2 pairs per launch); the register compares of the
+    # survivors run on the integer pipe (pairs_compared x m byte compares).
+    pairs_u = n * (n - 1) / 2.0
+    flops = 2.0 * S * pairs_u
     achieved = flops / (ap_ms / 1000.0) / 1e12 if ap_ms > 0 else 0.0
     peak = peaks.get("bf16_tflops", 1590.0)
-    traffic = (ALLPAIRS_TRAFFIC_PER_PAIR * n * n
+    traffic = (ALLPAIRS_TRAFFIC_PER_PAIR * pairs_u
                if ALLPAIRS_TRAFFIC_PER_PAIR is not None and WORKLOAD["samples"] == 20 else None)
     # sketch: ASCII read, 2-bit words + invalid mask written and read back,
     # per-contig 1/w rows written and read, two code rows written
@@ -231,12 +233,14 @@ def _finish(args, ctx, asm, timings, last, ms, value, result_e2e, clk, world, ra
         "stages_ms": {k: round(v, 4) for k, v in last.items() if k.endswith("_ms")},
         "pairs_prefiltered": last["pairs_prefiltered"],
         "pairs_compared": last["pairs_compared"],
+        "pairs_counted": "unordered (symmetric pass)" if S > 1 and n > 25000 else "ordered",
         "gpu_launches": int(last["kernel_launches"]) * args.steps,
-        "roofline": {"bound": "tensor", "kernel": "k_allpairs_tc (FP16 mma prefilter + survivor compare)",
+        "roofline": {"bound": "tensor",
+                     "kernel": "k_allpairs_tc_sym (FP16 mma prefilter + survivor compare, each pair once)",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak else None,
                      "peak_source": f"bf16_tflops of MEASURED_PEAKS.json ({peak_src})",
-                     "work": "2*S*n^2 FLOPs per launch (FP16 products of every ordered pair)",
+                     "work": "2*S*n(n-1)/2 FLOPs per launch (FP16 products of every unordered pair)",
                      "traffic": traffic},
         "int_pipe": {"register_compares_per_s": last["pairs_compared"] * m / (ap_ms / 1000.0)
                      if ap_ms > 0 else 0.0,

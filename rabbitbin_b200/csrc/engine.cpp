@@ -381,7 +381,7 @@ void run_graph(rbg_ctx *c, const rbg_params *p) {
     c->pin.ensure(nm4 * sizeof(uint32_t) + sizeof(unsigned long long));
     uint32_t *hmax = c->pin.as<uint32_t>();
     unsigned long long *hnp = (unsigned long long *)(hmax + nm4);
-    if (c->sym_cap == 0) c->sym_cap = std::max<uint64_t>(1u << 20, (uint64_t)n * 128);
+    if (c->sym_cap == 0) c->sym_cap = std::max<uint64_t>(1u << 20, (uint64_t)n * 256);
     for (;;) {
       c->sym_pairs.ensure(c->sym_cap * sizeof(uint4));
       c->sym_keys.ensure(2 * c->sym_cap * sizeof(uint64_t));

@@ -644,12 +644,12 @@ __device__ __forceinline__ void tc_item(const GraphArgs &g, uint64_t *gbuf, int3
     else count_batch_coop(g, w, q, qn, sA);
   }
   if (g.stats) {
-    // ordered pairs: a symmetric evaluation stands for both orders
+    // pairs evaluated: ordered pairs, or unordered ones in the symmetric pass
     const unsigned a = __reduce_add_sync(FULL, (unsigned)n_pref),
                    b = __reduce_add_sync(FULL, (unsigned)n_cmp);
     if (lane == 0) {
-      if (a) atomicAdd(g.stats, (unsigned long long)a * (SYM ? 2u : 1u));
-      if (b) atomicAdd(g.stats + 1, (unsigned long long)b * (SYM ? 2u : 1u));
+      if (a) atomicAdd(g.stats, (unsigned long long)a);
+      if (b) atomicAdd(g.stats + 1, (unsigned long long)b);
     }
   }
   __syncwarp();
