@@ -959,7 +959,7 @@ void launch_rows_topk(const GraphArgs &g, const SymOut &o, int64_t *rowoff, uint
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  k_scatter_pairs<<<(unsigned)(sms * 8), 256, 0, s>>>(o, rowoff, keys);
+  k_scatter_pairs<<<(unsigned)(sms * 32), 256, 0, s>>>(o, rowoff, keys);   // a few pairs per thread
   k_select_rows<<<(unsigned)((g.n + kMergeWarps - 1) / kMergeWarps), kMergeWarps * 32, 0, s>>>(
       g, rowoff, keys);
 }

@@ -347,27 +347,34 @@ __device__ __forceinline__ bool has_nbr(const uint32_t *ids, int cnt, uint32_t x
 
 // Edges of row i: (i, j) for kept neighbours j > i; with the mutual filter
 // (src/impl/rb_graph.cpp:1284-1348) i must also be a kept neighbour of j.
+// Warp per row: lane q tests neighbour q (coalesced id reads, the searches in
+// the partners' lists run side by side).
+__device__ __forceinline__ bool edge_kept(const EmitArgs &e, int64_t i, uint32_t j) {
+  if ((int64_t)j <= i) return false;
+  return !(e.mutual && !e.small_path) ||
+         has_nbr(e.nbr_sorted + (int64_t)j * e.K, e.nbr_cnt[j], (uint32_t)i);
+}
+
 __device__ __forceinline__ void count_edges_row(const EmitArgs &e, int64_t i) {
+  const int lane = threadIdx.x & 31;
   const int c = e.nbr_cnt[i];
   const uint32_t *ids = e.nbr_sorted + i * e.K;
   int cnt = 0;
-  for (int q = 0; q < c; ++q) {
-    const uint32_t j = ids[q];
-    if ((int64_t)j <= i) continue;
-    if (e.mutual && !e.small_path &&
-        !has_nbr(e.nbr_sorted + (int64_t)j * e.K, e.nbr_cnt[j], (uint32_t)i)) continue;
-    ++cnt;
+  for (int q0 = 0; q0 < c; q0 += 32) {
+    const int q = q0 + lane;
+    const bool ok = q < c && edge_kept(e, i, ids[q]);
+    cnt += __popc(__ballot_sync(FULL, ok));
   }
-  e.row_edges[i] = cnt;
+  if (lane == 0) e.row_edges[i] = cnt;
 }
 
 __global__ void k_count_edges(EmitArgs e) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t i = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (i < e.n) count_edges_row(e, i);
 }
 
 __global__ void k_count_edges_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows) {
-  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (r >= rows) return;
   const int a = find_asm(row0s, nb, r);
   count_edges_row(B[a].e, r - B[a].row0);
@@ -400,28 +407,32 @@ __global__ void k_scan(int32_t *v, int64_t n) {
 }
 
 __device__ __forceinline__ void write_edges_row(const EmitArgs &e, int64_t i) {
+  const int lane = threadIdx.x & 31;
   const int c = e.nbr_cnt[i];
   const uint32_t *ids = e.nbr_sorted + i * e.K;
   int64_t o = e.row_edges[i];
-  for (int q = 0; q < c; ++q) {
-    const uint32_t j = ids[q];
-    if ((int64_t)j <= i) continue;
-    if (e.mutual && !e.small_path &&
-        !has_nbr(e.nbr_sorted + (int64_t)j * e.K, e.nbr_cnt[j], (uint32_t)i)) continue;
-    e.from[o] = (uint32_t)i;
-    e.to[o] = j;
-    e.scomp[o] = e.nbr_sv[i * e.K + q];
-    ++o;
+  for (int q0 = 0; q0 < c; q0 += 32) {
+    const int q = q0 + lane;
+    const uint32_t j = q < c ? ids[q] : 0u;
+    const bool ok = q < c && edge_kept(e, i, j);
+    const unsigned m = __ballot_sync(FULL, ok);
+    if (ok) {
+      const int64_t at = o + __popc(m & ((1u << lane) - 1u));
+      e.from[at] = (uint32_t)i;
+      e.to[at] = j;
+      e.scomp[at] = e.nbr_sv[i * e.K + q];
+    }
+    o += __popc(m);
   }
 }
 
 __global__ void k_write_edges(EmitArgs e) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t i = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (i < e.n) write_edges_row(e, i);
 }
 
 __global__ void k_write_edges_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows) {
-  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (r >= rows) return;
   const int a = find_asm(row0s, nb, r);
   write_edges_row(B[a].e, r - B[a].row0);
@@ -564,13 +575,13 @@ void launch_sort_rows(const EmitArgs &e, cudaStream_t s) {
 
 void launch_count_edges(const EmitArgs &e, cudaStream_t s) {
   if (e.n == 0) return;
-  k_count_edges<<<(unsigned)((e.n + 127) / 128), 128, 0, s>>>(e);
+  k_count_edges<<<(unsigned)((e.n + 7) / 8), 256, 0, s>>>(e);   // warp per row
   k_scan<<<1, 1024, 0, s>>>(e.row_edges, e.n);
 }
 
 void launch_write_edges(const EmitArgs &e, cudaStream_t s) {
   if (e.n == 0) return;
-  k_write_edges<<<(unsigned)((e.n + 127) / 128), 128, 0, s>>>(e);
+  k_write_edges<<<(unsigned)((e.n + 7) / 8), 256, 0, s>>>(e);   // warp per row
 }
 
 void launch_edge_weights(const WeightArgs &w, cudaStream_t s) {
@@ -606,7 +617,7 @@ void launch_emit_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t 
     const int warps = 4;
     k_sort_rows_batch<<<(unsigned)((rows + warps - 1) / warps), warps * 32,
                         (size_t)warps * len * 8, s>>>(B, row0s, nb, rows, len);
-    k_count_edges_batch<<<(unsigned)((rows + 127) / 128), 128, 0, s>>>(B, row0s, nb, rows);
+    k_count_edges_batch<<<(unsigned)((rows + 7) / 8), 256, 0, s>>>(B, row0s, nb, rows);
   }
   k_scan<<<1, 1024, 0, s>>>(row_edges, rows);
   k_edge0s<<<1, 256, 0, s>>>(row0s, nb, row_edges, edge0s);
@@ -615,7 +626,7 @@ void launch_emit_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t 
 void launch_write_edges_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows,
                               cudaStream_t s) {
   if (rows == 0) return;
-  k_write_edges_batch<<<(unsigned)((rows + 127) / 128), 128, 0, s>>>(B, row0s, nb, rows);
+  k_write_edges_batch<<<(unsigned)((rows + 7) / 8), 256, 0, s>>>(B, row0s, nb, rows);
 }
 
 void launch_edge_weights_batch(const BatchAsm *B, const int64_t *edge0s, int nb, int64_t edges,

@@ -10,23 +10,16 @@
 namespace rbg {
 namespace {
 
-// A/a->0, C/c->1, G/g->2, T/t->3, anything else invalid
+// Base encoding: A/a->0, C/c->1, G/g->2, T/t->3, anything else invalid
 // (RB_BASE_ENC_LUT, src/rabbit_sketch.h:56-75).
-__device__ __forceinline__ uint32_t enc_base(uint32_t c, uint32_t &bad) {
-  const uint32_t l = c | 0x20u;
-  uint32_t code = 0;
-  bad = 0;
-  if (l == 'a') code = 0;
-  else if (l == 'c') code = 1;
-  else if (l == 'g') code = 2;
-  else if (l == 't') code = 3;
-  else bad = 1;
-  return code;
-}
-
 // One thread per 16 bases: a 128-bit load of ASCII, one packed word out
 // (first base in the top two bits) and 16 bits of the invalid mask; lane pairs
-// merge their halves into one 32-bit mask word.
+// merge their halves into one 32-bit mask word.  Four bases per 32-bit step:
+// with l = byte | 0x20, ((l >> 1) ^ (l >> 2)) & 3 is 0, 1, 2, 3 for a, c, g, t;
+// the letter rebuilt from that code (a byte permute of "acgt") equals l exactly
+// for the eight valid letters, which a zero-byte test of the difference marks.
+// Two multiplies gather the four codes and the four invalid bits, first base
+// highest.  Bases past nbases are invalid.
 __global__ void k_pack(const uint4 *__restrict__ ascii, int64_t nbases, int64_t nwords,
                        int64_t w_begin, int64_t w_end, uint32_t *__restrict__ packed,
                        uint32_t *__restrict__ nmask) {
@@ -37,14 +30,25 @@ __global__ void k_pack(const uint4 *__restrict__ ascii, int64_t nbases, int64_t 
     const uint4 v = ascii[w];
     const uint32_t q[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-    for (int t = 0; t < 16; ++t) {
-      const uint32_t c = (q[t >> 2] >> (8 * (t & 3))) & 0xFFu;
-      uint32_t bad;
-      uint32_t code = enc_base(c, bad);
-      if (w * 16 + t >= nbases) bad = 1;
-      if (bad) code = 0;
-      word |= code << (30 - 2 * t);
-      bad16 |= bad << (15 - t);
+    for (int k = 0; k < 4; ++k) {
+      const uint32_t l = q[k] | 0x20202020u;
+      uint32_t cw = ((l >> 1) ^ (l >> 2)) & 0x03030303u;
+      const uint32_t sel = (cw & 0x3u) | ((cw >> 4) & 0x30u) | ((cw >> 8) & 0x300u) |
+                           ((cw >> 12) & 0x3000u);
+      const uint32_t y = __byte_perm(0x74676361u, 0u, sel) ^ l;
+      const uint32_t ok = ~(((y & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | y) & 0x80808080u;
+      const uint32_t b = (ok ^ 0x80808080u) >> 7;          // 0x01 in each invalid byte
+      cw &= ~(b * 3u);
+      const uint32_t c8 = (uint32_t)(((uint64_t)cw * 0x40100401ull) >> 24) & 0xFFu;
+      const uint32_t b4 = (uint32_t)(((uint64_t)b * 0x08040201ull) >> 24) & 0xFu;
+      word |= c8 << (24 - 8 * k);
+      bad16 |= b4 << (12 - 4 * k);
+    }
+    const int64_t lim = nbases - w * 16;
+    if (lim < 16) {
+      const int keep = lim > 0 ? (int)lim : 0;
+      bad16 |= 0xFFFFu >> keep;
+      word &= ~(0xFFFFFFFFu >> (2 * keep));
     }
     packed[w] = word;
   }
