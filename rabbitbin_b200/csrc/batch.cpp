@@ -165,7 +165,10 @@ int64_t batch_request_bytes(const rbg_params *p, int64_t n, int64_t nbases, int 
   int64_t b = nbases + nbases / 4 + nbases / 8 + 64;             // ASCII, 2-bit words, mask
   b += n * (int64_t)(S * 4 + 8 + E * 8 + 4 + 2 * mpad + Su * 4 + Kp * 2 + 1);
   b += n * (int64_t)K * (8 + 4 + 4) + n * 32;                    // top-K, neighbour lists
-  b += ((n + 31) / 32) * P * 32 * (cap * 8 + 4);                 // slice candidate buffers
+  if (abd)
+    b += n * 256 * (16 + 2 * 8) + n * 12;                        // admitted pairs, keys, rows
+  else
+    b += ((n + 31) / 32) * P * 32 * (cap * 8 + 4);               // slice candidate buffers
   b += n * (int64_t)K / 2 * 16;                                   // edge arrays (bound)
   b += 30000 * 12 + (m + 1) * 4 + 4096;                          // b0 pairs, tables of sv
   return b;
@@ -189,6 +192,7 @@ struct BatchPlan {
   std::vector<int> ord;                // batch position -> caller index
   int64_t rows = 0, bases = 0, dep = 0, code = 0, unit = 0, u16 = 0, col = 0, acc = 0, sv = 0;
   int64_t topk = 0, gbuf = 0, gcnt = 0, npairs = 0, winv = 0, pairs_scored = 0;
+  int64_t sym_rows = 0;                // rows of the tensor-core (symmetric pass) assemblies
   int max_m = 2, max_k = 1, max_s = 0;
   const AsmPlan &at(int b) const { return P[ord[b]]; }
 };
@@ -240,8 +244,14 @@ void plan_batch(const rbg_params *defaults, const rbg_assembly *asms, int nb, Ba
     a.sv0 = L.sv; L.sv += a.m + 1;
     a.topk0 = L.topk; L.topk += a.n * a.K;
     const int64_t nbk = (a.n + 31) / 32;
-    a.gbuf0 = L.gbuf; L.gbuf += nbk * a.P * 32 * a.cap;
-    a.gcnt0 = L.gcnt; L.gcnt += nbk * a.P * 32;
+    a.gbuf0 = L.gbuf;
+    a.gcnt0 = L.gcnt;
+    if (a.variant == 0) {
+      L.gbuf += nbk * a.P * 32 * a.cap;
+      L.gcnt += nbk * a.P * 32;
+    } else {
+      L.sym_rows += a.n;
+    }
     a.winv0 = L.winv; L.winv += a.n * a.E;
     if (a.p->base_on) {
       a.pairs = b0_pairs(a.n);
@@ -297,6 +307,23 @@ void ensure_buffers(BatchBufs &B, const BatchPlan &L, int nb) {
   B.item0s.ensure(4 * (nb + 1) * sizeof(int64_t));
   B.queues.ensure(4 * sizeof(unsigned long long));
   B.e_from.ensure(4); B.e_to.ensure(4); B.e_scomp.ensure(4); B.e_score.ensure(4);
+  if (L.sym_rows > 0) {
+    B.sym_cap = std::max<uint64_t>(B.sym_cap, std::max<uint64_t>(1u << 16, (uint64_t)L.sym_rows * 256));
+    B.sym_pairs.ensure(B.sym_cap * sizeof(uint4));
+    B.sym_keys.ensure(2 * B.sym_cap * sizeof(uint64_t));
+    B.sym_rowcnt.ensure(rows1 * sizeof(int32_t));
+    B.sym_rowoff.ensure((rows1 + 1) * sizeof(int64_t));
+    B.sym_np.ensure(sizeof(unsigned long long));
+  }
+}
+
+SymOut sym_out(BatchBufs &B) {
+  SymOut o;
+  o.pairs = B.sym_pairs.as<uint4>();
+  o.npairs = B.sym_np.as<unsigned long long>();
+  o.cap = B.sym_cap;
+  o.rowcnt = B.sym_rowcnt.as<int32_t>();
+  return o;
 }
 
 // The device descriptor of the assembly at batch position b (edge arrays are
@@ -446,16 +473,28 @@ int launch_graph_stage(rbg_ctx *c, BatchBufs &B, const BatchPlan &L, const Lists
   CK(cudaMemsetAsync(B.maxc_all.p, 0, rows1 * sizeof(uint32_t), c->stream));
   CK(cudaMemsetAsync(B.stats.p, 0, 2 * sizeof(unsigned long long), c->stream));
   CK(cudaMemsetAsync(B.queues.p, 0, 4 * sizeof(unsigned long long), c->stream));
+  const SymOut o = L.sym_rows > 0 ? sym_out(B) : SymOut{};
+  if (L.sym_rows > 0) {
+    CK(cudaMemsetAsync(B.sym_rowcnt.p, 0, rows1 * sizeof(int32_t), c->stream));
+    CK(cudaMemsetAsync(B.sym_np.p, 0, sizeof(unsigned long long), c->stream));
+  }
   for (int v = 0; v < 4; ++v) {
     if (W.list[v].empty()) continue;
     launch_allpairs_batch(dD, kVariants[v], B.lists.as<int32_t>() + v * (nb + 1),
                           B.item0s.as<int64_t>() + v * (nb + 1), (int)W.list[v].size(),
                           W.item0[v].back(), W.smem[v], B.queues.as<unsigned long long>() + v,
-                          c->stream);
+                          o, c->stream);
     ++launches;
   }
-  launch_merge_batch(dD, B.row0s.as<int64_t>(), nb, L.rows, c->stream);
-  launches += L.rows ? 1 : 0;
+  if (!W.list[0].empty()) {
+    launch_merge_batch(dD, B.row0s.as<int64_t>(), nb, L.rows, c->stream);
+    ++launches;
+  }
+  if (L.sym_rows > 0) {
+    launch_rows_topk_batch(dD, B.row0s.as<int64_t>(), nb, L.rows, o, B.sym_rowoff.as<int64_t>(),
+                           B.sym_keys.as<uint64_t>(), c->stream);
+    launches += 3;
+  }
   return launches;
 }
 
@@ -562,24 +601,38 @@ void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
 
   // ── segment 1: sketch, depth rows, b0, all-pairs, merge ────────────────
   const size_t mx_bytes = up256(2 * rows1 * sizeof(uint32_t));
-  B.hout.ensure(mx_bytes + up256(nb * sizeof(float)) + up256((nb + 1) * sizeof(int64_t)));
+  const size_t e0_bytes = up256((nb + 1) * sizeof(int64_t));
+  B.hout.ensure(mx_bytes + up256(nb * sizeof(float)) + e0_bytes + sizeof(unsigned long long));
   uint32_t *h_maxc = B.hout.as<uint32_t>();
   float *h_b0 = (float *)(B.hout.as<char>() + mx_bytes);
   int64_t *h_edge0s = (int64_t *)(B.hout.as<char>() + mx_bytes + up256(nb * sizeof(float)));
+  unsigned long long *h_np =
+      (unsigned long long *)(B.hout.as<char>() + mx_bytes + up256(nb * sizeof(float)) + e0_bytes);
   int launches = 0;
-  captured(c, 0, use_graph, stats.graph_launches, [&] {
-    launches += launch_sketch_groups(c, B, L, tab, nb);
-    launches += launch_graph_stage(c, B, L, W, nb);
-    if (rows) {
-      CK(cudaMemcpyAsync(h_maxc, B.maxc_cand.p, rows * sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                         c->stream));
-      CK(cudaMemcpyAsync(h_maxc + rows1, B.maxc_all.p, rows * sizeof(uint32_t),
-                         cudaMemcpyDeviceToHost, c->stream));
-    }
-    CK(cudaMemcpyAsync(h_b0, B.b0.p, nb * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
-  });
-  CK(cudaEventRecord(ev2, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
+  // The symmetric pass reports how many pairs it admitted; a pass whose pairs
+  // did not fit the list runs again with a larger one.
+  for (;;) {
+    captured(c, 0, use_graph, stats.graph_launches, [&] {
+      launches += launch_sketch_groups(c, B, L, tab, nb);
+      launches += launch_graph_stage(c, B, L, W, nb);
+      if (rows) {
+        CK(cudaMemcpyAsync(h_maxc, B.maxc_cand.p, rows * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                           c->stream));
+        CK(cudaMemcpyAsync(h_maxc + rows1, B.maxc_all.p, rows * sizeof(uint32_t),
+                           cudaMemcpyDeviceToHost, c->stream));
+      }
+      CK(cudaMemcpyAsync(h_b0, B.b0.p, nb * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+      if (L.sym_rows > 0)
+        CK(cudaMemcpyAsync(h_np, B.sym_np.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                           c->stream));
+    });
+    CK(cudaEventRecord(ev2, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (L.sym_rows == 0 || *h_np <= B.sym_cap) break;
+    B.sym_cap = *h_np + *h_np / 4;
+    B.sym_pairs.ensure(B.sym_cap * sizeof(uint4));
+    B.sym_keys.ensure(2 * B.sym_cap * sizeof(uint64_t));
+  }
 
   // ── host calibration of every assembly ─────────────────────────────────
   const auto t_cal = std::chrono::steady_clock::now();

@@ -124,6 +124,9 @@ struct BatchBufs {
   DBuf nbr, nbr_sv, nbr_cnt, row_edges, edge0s;
   DBuf e_from, e_to, e_scomp, e_score;
   DBuf desc, row0s, lists, item0s, queues, pair0s;
+  // symmetric all-pairs pass of the tensor-core assemblies (row space of the batch)
+  DBuf sym_pairs, sym_np, sym_rowcnt, sym_rowoff, sym_keys;
+  uint64_t sym_cap = 0;
   HBuf hstage, hout, hedge;
   std::map<std::tuple<int, int, uint64_t, int, int>, std::unique_ptr<Tables>> tables;
   void release() {
@@ -131,11 +134,13 @@ struct BatchBufs {
                    &unit, &unit16, &anynz, &colnorm, &colacc, &svbits, &topk, &topk_cnt,
                    &maxc_cand, &maxc_all, &stats, &gbuf, &gcnt, &pairs, &pair_cnt, &b0, &nbr,
                    &nbr_sv, &nbr_cnt, &row_edges, &edge0s, &e_from, &e_to, &e_scomp, &e_score,
-                   &desc, &row0s, &lists, &item0s, &queues, &pair0s};
+                   &desc, &row0s, &lists, &item0s, &queues, &pair0s, &sym_pairs, &sym_np,
+                   &sym_rowcnt, &sym_rowoff, &sym_keys};
     for (DBuf *b : all) b->release();
     hstage.release();
     hout.release();
     hedge.release();
+    sym_cap = 0;
     for (auto &kv : tables) kv.second->release();
     tables.clear();
   }

@@ -223,8 +223,9 @@ __device__ __forceinline__ void count_batch_coop(const GraphArgs &g, Warp &w, co
 // (i = row0 + r, j) raises both rows' maxima (row i through the warp's own
 // state, row j by an atomic) and, when its similarity passes the admission
 // floor, is appended once to the pair list with both rows' counts raised.
+// grow0: the assembly's first row in the row space of the pair list.
 __device__ __forceinline__ void count_batch_sym(const GraphArgs &g, const SymOut &o, uint32_t *mxc,
-                                                int64_t row0, const int *q, int nq,
+                                                int64_t row0, int64_t grow0, const int *q, int nq,
                                                 const unsigned char *sA) {
   const int lane = threadIdx.x & 31;
   const int m16 = g.mpad >> 4;
@@ -274,10 +275,10 @@ __device__ __forceinline__ void count_batch_sym(const GraphArgs &g, const SymOut
     if (adm) {
       const unsigned long long pos = base + (unsigned)__popc(am & ((1u << lane) - 1u));
       if (pos < o.cap) {
-        const uint32_t i = (uint32_t)(row0 + r);
-        o.pairs[pos] = make_uint4(i, j, svb, 0u);
-        atomicAdd(o.rowcnt + i, 1);
-        atomicAdd(o.rowcnt + j, 1);
+        const uint32_t gi = (uint32_t)(grow0 + row0 + r), gj = (uint32_t)(grow0 + j);
+        o.pairs[pos] = make_uint4(gi, gj, svb, (uint32_t)grow0);
+        atomicAdd(o.rowcnt + gi, 1);
+        atomicAdd(o.rowcnt + gj, 1);
       }
     }
   }
@@ -436,8 +437,8 @@ __device__ __forceinline__ void ldsm_x2(uint32_t &r0, uint32_t &r1, const void *
 // survivors appended to the counting queue.
 template <int SMAX, bool SYM>
 __device__ __forceinline__ void check_batch(const GraphArgs &g, Warp &w, const SymOut &o,
-                                            const int *cq, unsigned head, int nq, int64_t row0,
-                                            int *q, int &qn, float lo, float hi,
+                                            int64_t grow0, const int *cq, unsigned head, int nq,
+                                            int64_t row0, int *q, int &qn, float lo, float hi,
                                             unsigned long long &n_cmp, const float *sU,
                                             int SuP, const unsigned char *sA) {
   const int lane = threadIdx.x & 31;
@@ -474,7 +475,7 @@ __device__ __forceinline__ void check_batch(const GraphArgs &g, Warp &w, const S
   qn += __popc(m);
   __syncwarp();
   if (qn >= 32) {
-    if constexpr (SYM) count_batch_sym(g, o, w.mxc, row0, q, 32, sA);
+    if constexpr (SYM) count_batch_sym(g, o, w.mxc, row0, grow0, q, 32, sA);
     else count_batch_coop(g, w, q, 32, sA);
     n_cmp += 1;
     if (lane + 32 < qn) q[lane] = q[lane + 32];
@@ -490,7 +491,7 @@ template <int KS, int SMAX, bool SYM>
 __device__ __forceinline__ void tc_item(const GraphArgs &g, uint64_t *gbuf, int32_t *gcnt,
                                         int cap, int P, float lo, float hi, float lo16,
                                         int64_t bx, int by, unsigned char *smem,
-                                        const SymOut &o) {
+                                        const SymOut &o, int64_t grow0) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gq = lane >> 2, tq = lane & 3;
   const int64_t n = g.n;
@@ -608,9 +609,9 @@ __device__ __forceinline__ void tc_item(const GraphArgs &g, uint64_t *gbuf, int3
         const int cntl = __popc(mk);
         int incl = cntl;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int v = __shfl_up_sync(FULL, incl, o);
-          if (lane >= o) incl += v;
+        for (int d = 1; d < 32; d <<= 1) {
+          const int v = __shfl_up_sync(FULL, incl, d);
+          if (lane >= d) incl += v;
         }
         const int total = __shfl_sync(FULL, incl, 31);
         unsigned pos = tail + (unsigned)(incl - cntl);
@@ -626,7 +627,7 @@ __device__ __forceinline__ void tc_item(const GraphArgs &g, uint64_t *gbuf, int3
         tail += (unsigned)total;
         __syncwarp();
         while (tail - head >= 32) {
-          check_batch<SMAX, SYM>(g, w, o, cq, head, 32, row0, q, qn, lo, hi, n_cmp, sU, SuP, sA);
+          check_batch<SMAX, SYM>(g, w, o, grow0, cq, head, 32, row0, q, qn, lo, hi, n_cmp, sU, SuP, sA);
           head += 32;
         }
       }
@@ -635,12 +636,12 @@ __device__ __forceinline__ void tc_item(const GraphArgs &g, uint64_t *gbuf, int3
   }
   while (tail != head) {
     const int nq = (int)(tail - head < 32 ? tail - head : 32);
-    check_batch<SMAX, SYM>(g, w, o, cq, head, nq, row0, q, qn, lo, hi, n_cmp, sU, SuP, sA);
+    check_batch<SMAX, SYM>(g, w, o, grow0, cq, head, nq, row0, q, qn, lo, hi, n_cmp, sU, SuP, sA);
     head += (unsigned)nq;
   }
   if (qn > 0) {
     n_cmp += lane < qn;
-    if constexpr (SYM) count_batch_sym(g, o, mxc, row0, q, qn, sA);
+    if constexpr (SYM) count_batch_sym(g, o, mxc, row0, grow0, q, qn, sA);
     else count_batch_coop(g, w, q, qn, sA);
   }
   if (g.stats) {
@@ -667,7 +668,7 @@ k_allpairs_tc(GraphArgs g, uint64_t *gbuf, int32_t *gcnt, int cap, int P, float 
               float lo16) {
   extern __shared__ __align__(16) unsigned char smem[];
   tc_item<KS, SMAX, false>(g, gbuf, gcnt, cap, P, lo, hi, lo16, blockIdx.x, blockIdx.y, smem,
-                           SymOut{});
+                           SymOut{}, 0);
 }
 
 // Symmetric pass: CTA x scores row block x and row block B-1-x (columns from
@@ -678,19 +679,22 @@ k_allpairs_tc_sym(GraphArgs g, int P, float lo, float hi, float lo16, SymOut o) 
   extern __shared__ __align__(16) unsigned char smem[];
   const int64_t B = (g.n + 31) / 32;
   const int64_t b1 = blockIdx.x, b2 = B - 1 - (int64_t)blockIdx.x;
-  tc_item<KS, SMAX, true>(g, nullptr, nullptr, 0, P, lo, hi, lo16, b1, blockIdx.y, smem, o);
+  tc_item<KS, SMAX, true>(g, nullptr, nullptr, 0, P, lo, hi, lo16, b1, blockIdx.y, smem, o, 0);
   if (b2 > b1) {
     __syncthreads();
-    tc_item<KS, SMAX, true>(g, nullptr, nullptr, 0, P, lo, hi, lo16, b2, blockIdx.y, smem, o);
+    tc_item<KS, SMAX, true>(g, nullptr, nullptr, 0, P, lo, hi, lo16, b2, blockIdx.y, smem, o, 0);
   }
 }
 
 // Persistent form over a batch: CTAs pull (assembly, row block, slice group)
-// items from a device counter until the variant's items are exhausted.
+// items from a device counter until the variant's items are exhausted.  The
+// tensor-core variants run the symmetric pass (a row block's slices cover the
+// columns from its first row on; items come in ascending row blocks, so the
+// largest first).
 template <int KS, int SMAX>
 __global__ void __launch_bounds__(kWarps * 32)
 k_allpairs_batch(const BatchAsm *B, const int32_t *list, const int64_t *item0s, int nv,
-                 int64_t items, unsigned long long *next) {
+                 int64_t items, unsigned long long *next, SymOut o) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ long long s_item;
   for (;;) {
@@ -711,8 +715,8 @@ k_allpairs_batch(const BatchAsm *B, const int32_t *list, const int64_t *item0s, 
     const int64_t bx = local / G;
     const int by = (int)(local - bx * G);
     if constexpr (KS == 0) dense_item(g, b.gbuf, b.gcnt, b.cap, b.P, bx, by, smem);
-    else tc_item<KS, SMAX, false>(g, b.gbuf, b.gcnt, b.cap, b.P, b.lo, b.hi, b.lo16, bx, by, smem,
-                                  SymOut{});
+    else tc_item<KS, SMAX, true>(g, nullptr, nullptr, 0, b.P, b.lo, b.hi, b.lo16, bx, by, smem, o,
+                                 b.row0);
   }
 }
 
@@ -774,6 +778,7 @@ k_merge_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows) {
     if (__ldg(row0s + mid) <= r) lo = mid; else hi = mid - 1;
   }
   const BatchAsm &b = B[lo];
+  if (b.variant != 0) return;          // top-K from the symmetric pass's pairs
   merge_row(b.g, b.gbuf, b.gcnt, b.cap, b.P, r - b.row0, mk[wib]);
 }
 
@@ -805,29 +810,26 @@ __global__ void k_scatter_pairs(SymOut o, const int64_t *off, uint64_t *keys) {
   const unsigned long long np = *o.npairs < o.cap ? *o.npairs : o.cap;
   for (unsigned long long p = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; p < np;
        p += (unsigned long long)gridDim.x * blockDim.x) {
-    const uint4 x = o.pairs[p];
+    const uint4 x = o.pairs[p];                 // ids in keys are the assembly's own
     const uint64_t hi = (uint64_t)x.z << 32;
     const int64_t pi = off[x.x] + atomicSub(o.rowcnt + x.x, 1) - 1;
-    keys[pi] = hi | (uint64_t)(~x.y);
+    keys[pi] = hi | (uint64_t)(~(x.y - x.w));
     const int64_t pj = off[x.y] + atomicSub(o.rowcnt + x.y, 1) - 1;
-    keys[pj] = hi | (uint64_t)(~x.x);
+    keys[pj] = hi | (uint64_t)(~(x.x - x.w));
   }
 }
 
-// Warp per row: the K best keys of the row's segment, streamed through a
-// 512-key shared buffer (the register radix select keeps the K best whenever it
-// fills).
-__global__ void __launch_bounds__(kMergeWarps * 32)
-k_select_rows(GraphArgs g, const int64_t *off, const uint64_t *keys) {
-  __shared__ uint64_t mk[kMergeWarps][kMergeBuf];
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int64_t row = (int64_t)blockIdx.x * kMergeWarps + wib;
-  if (row >= g.n) return;
+// Warp per row: the K best keys of the row's segment (row space index gr,
+// assembly row `row`), streamed through a 512-key shared buffer (the register
+// radix select keeps the K best whenever it fills).
+__device__ __forceinline__ void select_row(const GraphArgs &g, int64_t row, int64_t gr,
+                                           const int64_t *off, const uint64_t *keys,
+                                           uint64_t *buf) {
+  const int lane = threadIdx.x & 31;
   const int K = g.K;
-  const int64_t s0 = off[row];
-  const int64_t c = off[row + 1] - s0;
+  const int64_t s0 = off[gr];
+  const int64_t c = off[gr + 1] - s0;
   const uint64_t *src = keys + s0;
-  uint64_t *buf = mk[wib];
   if (c <= K) {
     for (int64_t i = lane; i < c; i += 32) g.topk[row * K + i] = src[i];
     if (lane == 0) g.topk_cnt[row] = (int32_t)c;
@@ -851,6 +853,31 @@ k_select_rows(GraphArgs g, const int64_t *off, const uint64_t *keys) {
   }
   for (int i = lane; i < fill; i += 32) g.topk[row * K + i] = buf[i];
   if (lane == 0) g.topk_cnt[row] = fill;
+}
+
+__global__ void __launch_bounds__(kMergeWarps * 32)
+k_select_rows(GraphArgs g, const int64_t *off, const uint64_t *keys) {
+  __shared__ uint64_t mk[kMergeWarps][kMergeBuf];
+  const int wib = threadIdx.x >> 5;
+  const int64_t row = (int64_t)blockIdx.x * kMergeWarps + wib;
+  if (row < g.n) select_row(g, row, row, off, keys, mk[wib]);
+}
+
+__global__ void __launch_bounds__(kMergeWarps * 32)
+k_select_rows_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows,
+                    const int64_t *off, const uint64_t *keys) {
+  __shared__ uint64_t mk[kMergeWarps][kMergeBuf];
+  const int wib = threadIdx.x >> 5;
+  const int64_t r = (int64_t)blockIdx.x * kMergeWarps + wib;
+  if (r >= rows) return;
+  int lo = 0, hi = nb - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(row0s + mid) <= r) lo = mid; else hi = mid - 1;
+  }
+  const BatchAsm &b = B[lo];
+  if (b.variant == 0) return;          // dense: merged from the candidate buffers
+  select_row(b.g, r - b.row0, r, off, keys, mk[wib]);
 }
 
 size_t dense_smem(int mpad) {
@@ -964,9 +991,21 @@ void launch_rows_topk(const GraphArgs &g, const SymOut &o, int64_t *rowoff, uint
       g, rowoff, keys);
 }
 
+void launch_rows_topk_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows,
+                            const SymOut &o, int64_t *rowoff, uint64_t *keys, cudaStream_t s) {
+  if (rows == 0) return;
+  k_rows_scan<<<1, 1024, 0, s>>>(o.rowcnt, rowoff, rows);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  k_scatter_pairs<<<(unsigned)(sms * 32), 256, 0, s>>>(o, rowoff, keys);
+  k_select_rows_batch<<<(unsigned)((rows + kMergeWarps - 1) / kMergeWarps), kMergeWarps * 32, 0,
+                        s>>>(B, row0s, nb, rows, rowoff, keys);
+}
+
 void launch_allpairs_batch(const BatchAsm *B, int variant, const int32_t *list,
                            const int64_t *item0s, int nv, int64_t items, size_t smem,
-                           unsigned long long *next, cudaStream_t s) {
+                           unsigned long long *next, const SymOut &o, cudaStream_t s) {
   if (items == 0 || nv == 0) return;
   int dev = 0, sms = 148, per_sm = 1;
   cudaGetDevice(&dev);
@@ -979,7 +1018,7 @@ void launch_allpairs_batch(const BatchAsm *B, int variant, const int32_t *list,
                                                   kWarps * 32, smem);                          \
     const int64_t grid = std::min<int64_t>(items, (int64_t)std::max(per_sm, 1) * sms);         \
     k_allpairs_batch<KS, SM><<<(unsigned)grid, kWarps * 32, smem, s>>>(B, list, item0s, nv,    \
-                                                                       items, next);           \
+                                                                       items, next, o);        \
   } while (0)
   if (variant == 1) RBG_PB(1, 16);
   else if (variant == 2) RBG_PB(2, 32);

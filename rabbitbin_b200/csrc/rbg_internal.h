@@ -145,7 +145,8 @@ void launch_allpairs(const GraphArgs &g, uint64_t *gbuf, int32_t *gcnt, cudaStre
 // Output of the symmetric all-pairs pass (each unordered pair scored once): the
 // admitted pairs and, per row, how many admitted keys it holds (both ends).
 struct SymOut {
-  uint4 *pairs = nullptr;               // {i, j, similarity bits, 0}, i < j
+  uint4 *pairs = nullptr;               // {i, j, similarity bits, r0}: rows i < j of the
+                                        // row space, r0 the first row of their assembly
   unsigned long long *npairs = nullptr; // admitted pairs found (may exceed cap)
   uint64_t cap = 0;                     // pairs written: min(npairs, cap)
   int32_t *rowcnt = nullptr;            // [n], zero before the pass
@@ -230,11 +231,18 @@ void launch_b0_batch(const BatchAsm *B, const int64_t *pair0s, int nb, int64_t n
 // Persistent all-pairs over the assemblies list[0..nv) of one variant: work
 // item x of assembly list[k] is x - item0s[k] (row block, slice group); CTAs
 // pull items from *next (zeroed by the caller).
+// The tensor-core variants run the symmetric pass into o (row space of the
+// batch); the dense one fills the assemblies' candidate buffers.
 void launch_allpairs_batch(const BatchAsm *B, int variant, const int32_t *list,
                            const int64_t *item0s, int nv, int64_t items, size_t smem,
-                           unsigned long long *next, cudaStream_t s);
+                           unsigned long long *next, const SymOut &o, cudaStream_t s);
+// Top-K of the dense assemblies' candidate buffers (others skipped).
 void launch_merge_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows,
                         cudaStream_t s);
+// Top-K of the tensor-core assemblies from the symmetric pass's pairs (dense
+// ones skipped); rowoff [rows+1] and keys [2 * o.cap] are scratch.
+void launch_rows_topk_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows,
+                            const SymOut &o, int64_t *rowoff, uint64_t *keys, cudaStream_t s);
 void launch_emit_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows, int max_k,
                        int32_t *row_edges, int64_t *edge0s, cudaStream_t s);
 void launch_write_edges_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows,
