@@ -56,6 +56,7 @@ void stage_meta(rbg_ctx *c, const char *seqcat, const int64_t *offsets, int64_t 
   if (n >= (1 << 27)) throw Error(RBG_ERR_UNSUPPORTED, "at most 2^27 - 1 contigs per assembly");
   for (int64_t i = 0; i < n; ++i)
     if (offsets[i + 1] < offsets[i]) throw Error(RBG_ERR_ARG, "offsets must be non-decreasing");
+  c->streamed = false;
   c->n = n;
   c->S = S;
   c->nbases = n > 0 ? offsets[n] : 0;
@@ -87,6 +88,7 @@ void stage_device(rbg_ctx *c, const char *dseq, const int64_t *doffsets, int64_t
   if (S < 0 || S > kMaxS) throw Error(RBG_ERR_UNSUPPORTED, "S must be in 0..64");
   if (S > 0 && n > 0 && !depth) throw Error(RBG_ERR_ARG, "depth is null");
   if (n >= (1 << 27)) throw Error(RBG_ERR_UNSUPPORTED, "at most 2^27 - 1 contigs per assembly");
+  c->streamed = false;
   c->n = n;
   c->S = S;
   c->nbases = nbases;
@@ -185,6 +187,15 @@ SketchArgs sketch_setup(rbg_ctx *c, const rbg_params *p, bool want_winners) {
 // copy stream; each chunk's words are packed as it lands, and the contigs
 // whose words are all packed (e <= 16 * packed words) are counted and reduced
 // while the next chunks copy.
+bool sym_regime(const rbg_params *p, int64_t n, int S);
+GraphArgs graph_args(rbg_ctx *c, const rbg_params *p);
+SymOut sym_buffers(rbg_ctx *c, int64_t n1);
+void sym_clear(rbg_ctx *c, int64_t n1);
+
+// In the tensor-core regime the all-pairs pass runs behind the copy too: once
+// chunk g's contigs [c0, c1) are sketched, the pairs whose later member lies
+// in [c0, c1) are scored (rows [0, c1)), with admission deferred until b0 is
+// known (run_graph finishes the selection).
 void stage_sketch_chunked(rbg_ctx *c, const rbg_params *p, const char *seqcat,
                           const int64_t *offsets, int64_t n, const float *depth, int S) {
   stage_meta(c, seqcat, offsets, n, depth, S);
@@ -196,6 +207,16 @@ void stage_sketch_chunked(rbg_ctx *c, const rbg_params *p, const char *seqcat,
   CK(cudaEventRecord(c->ev_cin, c->stream));             // the buffers are free to overwrite
   CK(cudaStreamWaitEvent(c->copy, c->ev_cin, 0));
   const int G = nwords >= ((int64_t)kChunks << 16) ? kChunks : 1;
+  const bool stream_pairs = G > 1 && sym_regime(p, n, S) && c->no_stream_S != S;
+  GraphArgs ga;
+  SymOut o;
+  if (stream_pairs) {
+    ga = graph_args(c, p);
+    o = sym_buffers(c, std::max<int64_t>(n, 1));
+    o.defer = 1;
+    sym_clear(c, std::max<int64_t>(n, 1));
+    CK(cudaStreamWaitEvent(c->stream, c->ev_aux, 0));   // unit rows, anynz
+  }
   int64_t c0 = 0;
   for (int g = 0; g < G; ++g) {
     const int64_t w0 = (int64_t)g * nwords / G & ~(int64_t)1;
@@ -222,9 +243,14 @@ void stage_sketch_chunked(rbg_ctx *c, const rbg_params *p, const char *seqcat,
       launch_count(a, c->stream);
       launch_minreduce(a, c->stream);
       c->launches += 2;
+      if (stream_pairs) {
+        launch_allpairs_sym_window(ga, o, c0, c1, c->stream);
+        c->launches += 1;
+      }
     }
     c0 = c1;
   }
+  c->streamed = stream_pairs;
   c->launches += G;
   CK(cudaEventRecord(c->ev[1], c->stream));
   CK(cudaEventRecord(c->ev[2], c->stream));
@@ -307,8 +333,18 @@ void count_pairs_codes(rbg_ctx *c, int mpad, int m, const int64_t *pr, int np, u
   CK(cudaStreamSynchronize(c->stream));
 }
 
-// Graph + edge weights on the codes already in c->codesA/B and the staged depth.
-void run_graph(rbg_ctx *c, const rbg_params *p) {
+// The abundance-pruned regime of the fused path, whose all-pairs pass is the
+// symmetric tensor-core pass (src/rabbitbin.cpp:5035-5054 picks the fused
+// path; the prune applies when S > 1 and the depth term can decide an edge).
+bool sym_regime(const rbg_params *p, int64_t n, int S) {
+  const double w_comp = (p->w_comp < 0.0) ? (S <= 2 ? 1.0 : 0.0) : p->w_comp;
+  const bool fused = (p->force_path == 2) || (p->force_path == 0 && n > 25000);
+  return n > 0 && fused && p->abdfirst && S > 1 && w_comp < 1.0 && w_comp < p->min_edge;
+}
+
+// Graph-stage buffers and kernel arguments of the staged assembly (the
+// similarity table's contents come once b0 is known).
+GraphArgs graph_args(rbg_ctx *c, const rbg_params *p) {
   const int64_t n = c->n;
   const int m = p->m, mpad = mpad_of(m), S = c->S, K = p->max_edges;
   const int64_t n1 = std::max<int64_t>(n, 1);
@@ -319,9 +355,8 @@ void run_graph(rbg_ctx *c, const rbg_params *p) {
   c->maxc_cand.ensure(n1 * sizeof(uint32_t));
   c->maxc_all.ensure(n1 * sizeof(uint32_t));
   c->stats.ensure(2 * sizeof(unsigned long long));
-
   const double w_comp = (p->w_comp < 0.0) ? (S <= 2 ? 1.0 : 0.0) : p->w_comp;
-  if (!c->prep_done) prep_depth(c, p);
+  const bool fused = (p->force_path == 2) || (p->force_path == 0 && n > 25000);
   GraphArgs g;
   g.n = n; g.m = m; g.mpad = mpad; g.S = S; g.K = K; g.Su = Su;
   g.codesA = c->codesA.as<uint8_t>();
@@ -334,6 +369,56 @@ void run_graph(rbg_ctx *c, const rbg_params *p) {
   g.colnorm = c->colnorm.as<double>();
   g.has_depth = S > 0;
   g.wjac_norm = p->wjac_norm;
+  g.small_path = fused ? 0 : 1;
+  const bool abdfirst = sym_regime(p, n, S);
+  const double abd_corr_min = abdfirst ? (p->min_edge - w_comp) / (1.0 - w_comp) : -2.0;
+  g.prefilter = abdfirst ? 1 : 0;
+  g.prefilter_eps = (float)(abd_corr_min - 1e-4);
+  g.sv_bits = c->svbits.as<uint32_t>();
+  g.topk = c->topk.as<uint64_t>();
+  g.topk_cnt = c->topk_cnt.as<int32_t>();
+  g.maxcnt_cand = c->maxc_cand.as<uint32_t>();
+  g.maxcnt_all = c->maxc_all.as<uint32_t>();
+  g.stats = c->stats.as<unsigned long long>();
+  g.key_floor = admission_floor();
+  return g;
+}
+
+// Pair-list buffers of the symmetric pass (capacity c->sym_cap pairs).
+SymOut sym_buffers(rbg_ctx *c, int64_t n1) {
+  if (c->sym_cap == 0) c->sym_cap = std::max<uint64_t>(1u << 20, (uint64_t)n1 * 256);
+  c->sym_pairs.ensure(c->sym_cap * sizeof(uint4));
+  c->sym_keys.ensure(2 * c->sym_cap * sizeof(uint64_t));
+  c->sym_rowcnt.ensure(n1 * sizeof(int32_t));
+  c->sym_rowoff.ensure((n1 + 1) * sizeof(int64_t));
+  c->sym_np.ensure(sizeof(unsigned long long));
+  SymOut o;
+  o.pairs = c->sym_pairs.as<uint4>();
+  o.npairs = c->sym_np.as<unsigned long long>();
+  o.cap = c->sym_cap;
+  o.rowcnt = c->sym_rowcnt.as<int32_t>();
+  return o;
+}
+
+// Zeroes what a symmetric pass accumulates into.
+void sym_clear(rbg_ctx *c, int64_t n1) {
+  CK(cudaMemsetAsync(c->stats.p, 0, 2 * sizeof(unsigned long long), c->stream));
+  CK(cudaMemsetAsync(c->maxc_cand.p, 0, n1 * sizeof(uint32_t), c->stream));
+  CK(cudaMemsetAsync(c->sym_rowcnt.p, 0, n1 * sizeof(int32_t), c->stream));
+  CK(cudaMemsetAsync(c->sym_np.p, 0, sizeof(unsigned long long), c->stream));
+}
+
+// Graph + edge weights on the codes already in c->codesA/B and the staged depth.
+void run_graph(rbg_ctx *c, const rbg_params *p) {
+  const bool streamed_in = c->streamed;     // pairs scored behind the copy (this call only)
+  c->streamed = false;
+  const int64_t n = c->n;
+  const int m = p->m, mpad = mpad_of(m), S = c->S, K = p->max_edges;
+  const int64_t n1 = std::max<int64_t>(n, 1);
+  const int Su = (std::max(S, 1) + 3) & ~3;
+  const double w_comp = (p->w_comp < 0.0) ? (S <= 2 ? 1.0 : 0.0) : p->w_comp;
+  if (!c->prep_done) prep_depth(c, p);
+  GraphArgs g = graph_args(c, p);
   const bool use_colnorm = need_colnorm(p, S);
   CK(cudaEventRecord(c->ev[4], c->stream));
 
@@ -356,18 +441,6 @@ void run_graph(rbg_ctx *c, const rbg_params *p) {
   const bool fused = (p->force_path == 2) || (p->force_path == 0 && n > 25000);
   if (fused && n <= 2500) throw Error(RBG_ERR_ARG, "the fused path samples 2500 contigs; need n > 2500");
   c->path = fused ? 2 : 1;
-  g.small_path = fused ? 0 : 1;
-  const bool abdfirst = fused && p->abdfirst && S > 1 && w_comp < 1.0 && w_comp < p->min_edge;
-  const double abd_corr_min = abdfirst ? (p->min_edge - w_comp) / (1.0 - w_comp) : -2.0;
-  g.prefilter = abdfirst ? 1 : 0;
-  g.prefilter_eps = (float)(abd_corr_min - 1e-4);
-  g.sv_bits = c->svbits.as<uint32_t>();
-  g.topk = c->topk.as<uint64_t>();
-  g.topk_cnt = c->topk_cnt.as<int32_t>();
-  g.maxcnt_cand = c->maxc_cand.as<uint32_t>();
-  g.maxcnt_all = c->maxc_all.as<uint32_t>();
-  g.stats = c->stats.as<unsigned long long>();
-  g.key_floor = admission_floor();
   CK(cudaStreamWaitEvent(c->stream, c->ev_aux, 0));   // unit rows, anynz, column norms
   c->prep_done = false;
   std::vector<uint32_t> maxc;
@@ -376,28 +449,24 @@ void run_graph(rbg_ctx *c, const rbg_params *p) {
     // Tensor-core regime: every unordered pair scored once, admitted pairs
     // listed, then each row's top-K selected from its keys.  The row maxima and
     // the pair count come back while the selection runs; a pass whose pairs did
-    // not fit the list is run again with a larger one.
+    // not fit the list is run again with a larger one.  When rbg_bin_graph
+    // already scored the pairs behind the input copy (admission deferred), the
+    // selection converts the stored counts; if those did not fit, this
+    // configuration is scored here from then on.
     const size_t nm4 = (size_t)((n1 + 3) & ~3);
     c->pin.ensure(nm4 * sizeof(uint32_t) + sizeof(unsigned long long));
     uint32_t *hmax = c->pin.as<uint32_t>();
     unsigned long long *hnp = (unsigned long long *)(hmax + nm4);
-    if (c->sym_cap == 0) c->sym_cap = std::max<uint64_t>(1u << 20, (uint64_t)n * 256);
+    bool streamed = streamed_in;
     for (;;) {
-      c->sym_pairs.ensure(c->sym_cap * sizeof(uint4));
-      c->sym_keys.ensure(2 * c->sym_cap * sizeof(uint64_t));
-      c->sym_rowcnt.ensure(n1 * sizeof(int32_t));
-      c->sym_rowoff.ensure((n1 + 1) * sizeof(int64_t));
-      c->sym_np.ensure(sizeof(unsigned long long));
-      CK(cudaMemsetAsync(c->stats.p, 0, 2 * sizeof(unsigned long long), c->stream));
-      CK(cudaMemsetAsync(c->maxc_cand.p, 0, n1 * sizeof(uint32_t), c->stream));
-      CK(cudaMemsetAsync(c->sym_rowcnt.p, 0, n1 * sizeof(int32_t), c->stream));
-      CK(cudaMemsetAsync(c->sym_np.p, 0, sizeof(unsigned long long), c->stream));
-      SymOut o;
-      o.pairs = c->sym_pairs.as<uint4>();
-      o.npairs = c->sym_np.as<unsigned long long>();
-      o.cap = c->sym_cap;
-      o.rowcnt = c->sym_rowcnt.as<int32_t>();
-      launch_allpairs_sym(g, o, c->stream);
+      SymOut o = sym_buffers(c, n1);
+      if (streamed) {
+        o.defer = 1;
+      } else {
+        sym_clear(c, n1);
+        launch_allpairs_sym(g, o, c->stream);
+        c->launches += 1;
+      }
       CK(cudaGetLastError());
       CK(cudaEventRecord(c->ev[6], c->stream));
       CK(cudaMemcpyAsync(hmax, c->maxc_cand.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost,
@@ -405,13 +474,22 @@ void run_graph(rbg_ctx *c, const rbg_params *p) {
       CK(cudaMemcpyAsync(hnp, c->sym_np.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                          c->stream));
       CK(cudaEventRecord(c->ev[10], c->stream));
-      launch_rows_topk(g, o, c->sym_rowoff.as<int64_t>(), c->sym_keys.as<uint64_t>(), c->stream);
+      if (streamed)
+        launch_rows_topk_counts(g, o, g.sv_bits, c->sym_rowoff.as<int64_t>(),
+                                c->sym_keys.as<uint64_t>(), c->stream);
+      else
+        launch_rows_topk(g, o, c->sym_rowoff.as<int64_t>(), c->sym_keys.as<uint64_t>(), c->stream);
       CK(cudaGetLastError());
-      c->launches += 4;
+      c->launches += 3;
       CK(cudaEventSynchronize(c->ev[10]));
       if (*hnp <= c->sym_cap) break;
       CK(cudaStreamSynchronize(c->stream));
-      c->sym_cap = *hnp + *hnp / 4;
+      if (streamed) {
+        c->no_stream_S = S;                  // survivors outgrow the list at this S
+        streamed = false;
+      } else {
+        c->sym_cap = *hnp + *hnp / 4;
+      }
     }
     maxc_host = hmax;
   } else {
@@ -789,6 +867,7 @@ int rbg_build_graph(rbg_ctx *c, const rbg_params *p, const uint32_t *winners32, 
     validate(p);
     if (n < 0 || (n > 0 && !winners32) || !out) throw Error(RBG_ERR_ARG, "bad arguments");
     if (S < 0 || S > kMaxS) throw Error(RBG_ERR_UNSUPPORTED, "S must be in 0..64");
+    c->streamed = false;
     c->n = n;
     c->S = S;
     c->depth.ensure(std::max<size_t>(1, (size_t)n * S) * sizeof(float));

@@ -264,8 +264,13 @@ __device__ __forceinline__ void count_batch_sym(const GraphArgs &g, const SymOut
     const uint32_t mx = __reduce_max_sync(grp, mine);
     if (lane == __ffs(grp) - 1 && mx > mxc[r]) mxc[r] = mx;
     if (mine) atomicMax(g.maxcnt_cand + j, mine);
-    svb = __ldg(g.sv_bits + mine);
-    adm = svb > (uint32_t)(g.key_floor >> 32);
+    if (o.defer) {
+      svb = mine;                        // converted once the similarity table exists
+      adm = mine > 0;
+    } else {
+      svb = __ldg(g.sv_bits + mine);
+      adm = svb > (uint32_t)(g.key_floor >> 32);
+    }
   }
   const unsigned am = __ballot_sync(FULL, adm);
   if (am) {
@@ -491,13 +496,17 @@ template <int KS, int SMAX, bool SYM>
 __device__ __forceinline__ void tc_item(const GraphArgs &g, uint64_t *gbuf, int32_t *gcnt,
                                         int cap, int P, float lo, float hi, float lo16,
                                         int64_t bx, int by, unsigned char *smem,
-                                        const SymOut &o, int64_t grow0) {
+                                        const SymOut &o, int64_t grow0, int64_t cb = 0,
+                                        int64_t ce = -1) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gq = lane >> 2, tq = lane & 3;
   const int64_t n = g.n;
   const int64_t row0 = bx * 32;
   const int slice = by * kWarps + warp;
-  const int64_t c_lo = SYM ? row0 : 0, span = n - c_lo;
+  // columns [c_lo, c_hi); rows at or past row_end are never candidates
+  const int64_t c_hi = (SYM && ce >= 0) ? ce : n, row_end = c_hi;
+  const int64_t c_lo = SYM ? (row0 > cb ? row0 : cb) : 0;
+  const int64_t span = c_hi > c_lo ? c_hi - c_lo : 0;
   const int64_t jb = c_lo + span * slice / P, je = c_lo + span * (slice + 1) / P;
   const int Kp = KS * 16;
   const int cstride = Kp * 2 + 16;                 // bytes per staged column (conflict-free ldmatrix)
@@ -601,7 +610,7 @@ __device__ __forceinline__ void tc_item(const GraphArgs &g, uint64_t *gbuf, int3
         for (int i = 0; i < 4; ++i) {
           const int rr = mt * 16 + gq + 8 * (i >> 1);
           const int cc = c0 + 2 * tq + (i & 1);
-          if (acc[mt][i] >= lo16 && cc < nc && row0 + rr < n && (!SYM || jt + cc > row0 + rr))
+          if (acc[mt][i] >= lo16 && cc < nc && row0 + rr < row_end && (!SYM || jt + cc > row0 + rr))
             mk |= 1u << (mt * 4 + i);
         }
       n_pref += 8;
@@ -684,6 +693,17 @@ k_allpairs_tc_sym(GraphArgs g, int P, float lo, float hi, float lo16, SymOut o) 
     __syncthreads();
     tc_item<KS, SMAX, true>(g, nullptr, nullptr, 0, P, lo, hi, lo16, b2, blockIdx.y, smem, o, 0);
   }
+}
+
+// Window of the symmetric pass: CTA x scores row block x against the columns
+// [max(cb, its first row), ce).
+template <int KS, int SMAX>
+__global__ void __launch_bounds__(kWarps * 32)
+k_allpairs_tc_win(GraphArgs g, int P, float lo, float hi, float lo16, SymOut o, int64_t cb,
+                  int64_t ce) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  tc_item<KS, SMAX, true>(g, nullptr, nullptr, 0, P, lo, hi, lo16, blockIdx.x, blockIdx.y, smem, o,
+                          0, cb, ce);
 }
 
 // Persistent form over a batch: CTAs pull (assembly, row block, slice group)
@@ -806,12 +826,13 @@ __global__ void k_rows_scan(const int32_t *cnt, int64_t *off, int64_t n) {
 // Both keys of every admitted pair into their rows' segments (grid-stride over
 // the pairs written).  Positions count down from each row's end, so the row
 // counts return to zero.
-__global__ void k_scatter_pairs(SymOut o, const int64_t *off, uint64_t *keys) {
+__global__ void k_scatter_pairs(SymOut o, const int64_t *off, uint64_t *keys,
+                                const uint32_t *svtab) {
   const unsigned long long np = *o.npairs < o.cap ? *o.npairs : o.cap;
   for (unsigned long long p = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; p < np;
        p += (unsigned long long)gridDim.x * blockDim.x) {
     const uint4 x = o.pairs[p];                 // ids in keys are the assembly's own
-    const uint64_t hi = (uint64_t)x.z << 32;
+    const uint64_t hi = (uint64_t)(svtab ? __ldg(svtab + x.z) : x.z) << 32;
     const int64_t pi = off[x.x] + atomicSub(o.rowcnt + x.x, 1) - 1;
     keys[pi] = hi | (uint64_t)(~(x.y - x.w));
     const int64_t pj = off[x.y] + atomicSub(o.rowcnt + x.y, 1) - 1;
@@ -979,6 +1000,43 @@ void launch_allpairs_sym(const GraphArgs &g, const SymOut &o, cudaStream_t s) {
 #undef RBG_TS
 }
 
+void launch_allpairs_sym_window(const GraphArgs &g, const SymOut &o, int64_t cb, int64_t ce,
+                                cudaStream_t s) {
+  if (g.n == 0 || ce <= cb) return;
+  // slices of about 1024 columns: a window is a fraction of the columns, and
+  // every CTA stages its row block once
+  const int Pfull = allpairs_slices(g.n, g.K);
+  const int64_t want = (ce - cb) / 1024 / kWarps * kWarps;
+  const int P = (int)std::max<int64_t>(kWarps, std::min<int64_t>(Pfull, want));
+  const dim3 grid((unsigned)((ce + 31) / 32), (unsigned)(P / kWarps));
+  float lo, hi, lo16;
+  prefilter_bands(g.S, g.prefilter_eps, &lo, &hi, &lo16);
+  const int v = allpairs_variant(g);
+  const size_t smem = tc_smem(v, g.mpad, g.Su);
+#define RBG_TW(KS, SM)                                                                        \
+  do {                                                                                        \
+    cudaFuncSetAttribute(k_allpairs_tc_win<KS, SM>,                                           \
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);             \
+    k_allpairs_tc_win<KS, SM><<<grid, kWarps * 32, smem, s>>>(g, P, lo, hi, lo16, o, cb, ce); \
+  } while (0)
+  if (v == 1) RBG_TW(1, 16);
+  else if (v == 2) RBG_TW(2, 32);
+  else RBG_TW(4, 64);
+#undef RBG_TW
+}
+
+void launch_rows_topk_counts(const GraphArgs &g, const SymOut &o, const uint32_t *svtab,
+                             int64_t *rowoff, uint64_t *keys, cudaStream_t s) {
+  if (g.n == 0) return;
+  k_rows_scan<<<1, 1024, 0, s>>>(o.rowcnt, rowoff, g.n);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  k_scatter_pairs<<<(unsigned)(sms * 32), 256, 0, s>>>(o, rowoff, keys, svtab);
+  k_select_rows<<<(unsigned)((g.n + kMergeWarps - 1) / kMergeWarps), kMergeWarps * 32, 0, s>>>(
+      g, rowoff, keys);
+}
+
 void launch_rows_topk(const GraphArgs &g, const SymOut &o, int64_t *rowoff, uint64_t *keys,
                       cudaStream_t s) {
   if (g.n == 0) return;
@@ -986,7 +1044,7 @@ void launch_rows_topk(const GraphArgs &g, const SymOut &o, int64_t *rowoff, uint
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  k_scatter_pairs<<<(unsigned)(sms * 32), 256, 0, s>>>(o, rowoff, keys);   // a few pairs per thread
+  k_scatter_pairs<<<(unsigned)(sms * 32), 256, 0, s>>>(o, rowoff, keys, nullptr);   // a few pairs per thread
   k_select_rows<<<(unsigned)((g.n + kMergeWarps - 1) / kMergeWarps), kMergeWarps * 32, 0, s>>>(
       g, rowoff, keys);
 }
@@ -998,7 +1056,7 @@ void launch_rows_topk_batch(const BatchAsm *B, const int64_t *row0s, int nb, int
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  k_scatter_pairs<<<(unsigned)(sms * 32), 256, 0, s>>>(o, rowoff, keys);
+  k_scatter_pairs<<<(unsigned)(sms * 32), 256, 0, s>>>(o, rowoff, keys, nullptr);
   k_select_rows_batch<<<(unsigned)((rows + kMergeWarps - 1) / kMergeWarps), kMergeWarps * 32, 0,
                         s>>>(B, row0s, nb, rows, rowoff, keys);
 }

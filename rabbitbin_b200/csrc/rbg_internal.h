@@ -150,14 +150,28 @@ struct SymOut {
   unsigned long long *npairs = nullptr; // admitted pairs found (may exceed cap)
   uint64_t cap = 0;                     // pairs written: min(npairs, cap)
   int32_t *rowcnt = nullptr;            // [n], zero before the pass
+  // Deferred admission (the similarity table is not known yet): every survivor
+  // with a nonzero match count is kept, with the count in place of the
+  // similarity bits; launch_rows_topk converts it.  The top-K of all keys cut
+  // at the calibrated cutoff equals the top-K of the admitted keys cut there.
+  int defer = 0;
 };
 // Symmetric pass of the abundance-pruned (tensor-core) regime: row maxima into
 // g.maxcnt_cand, admitted pairs into o.  Requires allpairs_variant(g) != 0.
 void launch_allpairs_sym(const GraphArgs &g, const SymOut &o, cudaStream_t s);
+// The same pass over the pairs (i, j), i < j, whose column j lies in [cb, ce):
+// rows [0, ce) against those columns.  Windows that tile [0, n) score every
+// pair once; rows at or past ce are not read as candidates.
+void launch_allpairs_sym_window(const GraphArgs &g, const SymOut &o, int64_t cb, int64_t ce,
+                                cudaStream_t s);
 // Per-row top-K of the admitted pairs (both keys of each pair) into g.topk /
 // g.topk_cnt.  rowoff [n+1] and keys [2 * cap] are scratch; o.rowcnt ends zero.
 void launch_rows_topk(const GraphArgs &g, const SymOut &o, int64_t *rowoff, uint64_t *keys,
                       cudaStream_t s);
+// Pass with deferred admission: o.pairs hold match counts; svtab [m+1] maps a
+// count to its similarity bits.
+void launch_rows_topk_counts(const GraphArgs &g, const SymOut &o, const uint32_t *svtab,
+                             int64_t *rowoff, uint64_t *keys, cudaStream_t s);
 int allpairs_slices(int64_t n, int K);
 int allpairs_cap(int K);
 
