@@ -3,6 +3,7 @@
 //
 // Compiled with -fmad=false: every double operation below rounds exactly like
 // the reference's (which has no contracted expression in build_pmh_winners).
+#include <algorithm>
 #include <cstdint>
 
 #include "rbg_internal.h"
@@ -93,20 +94,16 @@ __device__ __forceinline__ uint32_t spread16(uint32_t x) {
 // shared table maps each k-mer code to its canonical code.
 __global__ void k_count(SketchArgs a) {
   extern __shared__ uint32_t sh_hist[];
-  __shared__ uint8_t canon[256];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
   const int nb = 1 << (2 * a.k);
   const int k = a.k;
-  for (int v = threadIdx.x; v < nb; v += blockDim.x) {
-    uint32_t rev = 0, x = (uint32_t)v;
-    for (int q = 0; q < k; ++q) { rev = (rev << 2) | (3u - (x & 3u)); x >>= 2; }
-    canon[v] = (uint8_t)((uint32_t)v <= rev ? (uint32_t)v : rev);
-  }
   uint32_t *hist = sh_hist + wib * 256;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  // warps stride over the contigs, so a long contig does not hold a block's
+  // other warps idle
+  for (int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib; c < a.n; c += warps) {
   for (int v = lane; v < 256; v += 32) hist[v] = 0;
-  __syncthreads();
-  if (c >= a.n) return;
+  __syncwarp();
   const int64_t s = a.offsets[c], e = a.offsets[c + 1];
   const uint32_t kmask = (uint32_t)nb - 1u;
   uint32_t bc0 = 0, bc1 = 0, bc2 = 0, bc3 = 0;
@@ -133,19 +130,35 @@ __global__ void k_count(SketchArgs a) {
         bc2 += __popc(hi & ~lo & vs);
         bc1 += __popc(~hi & lo & vs);
         bc0 += __popc(~hi & ~lo & vs);
-        // k-mers ending at base t: window bases t-k+1 .. t all valid
+        // k-mers ending at base t: window bases t-k+1 .. t all valid; forward
+        // codes are counted and folded onto canonical codes per contig
         const uint32_t winbad = (prevbad << 16) | bad;
         uint32_t any = winbad;
         for (int q = 1; q < k; ++q) any |= winbad >> q;
         uint32_t kv = ~any & 0xFFFFu;                   // bit 15-t: k-mer ending at t
         const uint64_t win = ((uint64_t)prev << 32) | cur;
-        while (kv) {
-          const int bp = __ffs(kv) - 1;                 // = 15 - t
-          kv &= kv - 1;
-          const uint32_t fwd = (uint32_t)(win >> (2 * bp)) & kmask;
-          atomicAdd(&hist[canon[fwd]], 1u);
+        if (kv == 0xFFFFu) {
+#pragma unroll
+          for (int bp = 15; bp >= 0; --bp)
+            atomicAdd(&hist[(uint32_t)(win >> (2 * bp)) & kmask], 1u);
+        } else {
+          while (kv) {
+            const int bp = __ffs(kv) - 1;               // = 15 - t
+            kv &= kv - 1;
+            atomicAdd(&hist[(uint32_t)(win >> (2 * bp)) & kmask], 1u);
+          }
         }
       }
+    }
+  }
+  __syncwarp();
+  // fold each reverse-complement code onto its canonical (the smaller) code
+  for (int v = lane; v < nb; v += 32) {
+    uint32_t rev = 0, x = (uint32_t)v;
+    for (int q = 0; q < k; ++q) { rev = (rev << 2) | (3u - (x & 3u)); x >>= 2; }
+    if ((uint32_t)v < rev) {
+      hist[v] += hist[rev];
+      hist[rev] = 0;
     }
   }
   __syncwarp();
@@ -199,6 +212,8 @@ __global__ void k_count(SketchArgs a) {
     if (e >= 0) ewinv[e] = take ? 1.0 / w : inf;
   }
   if (lane == 0) a.elem_cnt[c] = pos;
+  __syncwarp();                        // the next contig clears the histogram
+  }
 }
 
 // Register minimum with an exact early exit.  The winner of register r for a
@@ -440,8 +455,13 @@ void launch_pack_range(const char *ascii, int64_t nbases, int64_t w_begin, int64
 void launch_count(const SketchArgs &a, cudaStream_t s) {
   if (a.n == 0) return;
   const int warps = 8;
-  const int64_t grid = (a.n + warps - 1) / warps;
-  k_count<<<(unsigned)grid, warps * 32, warps * 256 * sizeof(uint32_t), s>>>(a);  // + 256 B static
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // about eight contigs per warp: enough to even out the contig lengths
+  const int64_t blocks = (a.n + warps - 1) / warps;
+  const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(blocks, (int64_t)sms * 4));
+  k_count<<<(unsigned)grid, warps * 32, warps * 256 * sizeof(uint32_t), s>>>(a);
 }
 
 void launch_minreduce(const SketchArgs &a, cudaStream_t s) {

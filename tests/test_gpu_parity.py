@@ -221,3 +221,24 @@ def test_graph_nonint_depths(gpu_ctx, orc, kind):
         assert got["sim_cutoff"] == want["sim_cutoff"]
         assert np.array_equal(got["src"], s) and np.array_equal(got["dst"], dd)
         assert np.array_equal(got["scomp"], sc) and np.array_equal(got["score"], sw)
+
+
+@pytest.mark.parametrize("S", [3, 20])
+def test_streamed_pairs_equal_resident(gpu_ctx, S):
+    """rbg_bin_graph scores the pairs chunk by chunk behind the input copy with
+    admission deferred until b0 is known (falling back to the whole pass when
+    the stored survivors outgrow the list, as few samples make likely); the
+    graph equals the one of the resident path, which scores all pairs at once."""
+    asm = make_assembly(30, 4000, S, seed=410 + S, absent_frac=0.1)
+    buf, offs = asm.concat()
+    assert len(buf) >= 8 * 16 * 65536          # eight input chunks
+    p = api.default_params(force_path=2)
+    streamed = gpu_ctx.bin_graph(buf, offs, asm.depth, p)
+    again = gpu_ctx.bin_graph(buf, offs, asm.depth, p)
+    gpu_ctx.stage(buf, offs, asm.depth)
+    gpu_ctx.run_resident(p)
+    resident = gpu_ctx.fetch_graph()
+    for got in (streamed, again):
+        assert got["b0"] == resident["b0"] and got["sim_cutoff"] == resident["sim_cutoff"]
+        for k in ("src", "dst", "scomp", "score"):
+            assert np.array_equal(got[k], resident[k]), k
