@@ -260,62 +260,97 @@ __global__ void k_b0_batch(const BatchAsm *B, const uint32_t *__restrict__ count
   }
 }
 
-// Bitonic sort, descending, of `len` (power of two) keys in shared memory by
-// one warp.
-__device__ void warp_sort_desc(uint64_t *keys, int len) {
-  const int lane = threadIdx.x & 31;
-  for (int size = 2; size <= len; size <<= 1) {
-    for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      for (int i = lane; i < len; i += 32) {
-        const int j = i ^ stride;
-        if (j > i) {
-          const uint64_t a = keys[i], b = keys[j];
-          const bool desc = ((i & size) == 0);
-          if (desc ? (a < b) : (a > b)) { keys[i] = b; keys[j] = a; }
-        }
-      }
-      __syncwarp();
-    }
-  }
-}
-
 __host__ __device__ __forceinline__ int pow2_at_least(int x) {
   int p = 1;
   while (p < x) p <<= 1;
   return p;
 }
 
+// Ascending bitonic sort of 32 R keys held in registers, element r * 32 + lane
+// in v[r]: strides of 32 and more pair registers of the same lane, shorter
+// strides pair lanes through shuffles.
+template <int R>
+__device__ __forceinline__ void warp_bitonic_asc(uint64_t (&v)[R]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int size = 2; size <= 32 * R; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      if (stride >= 32) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int p = r ^ (stride >> 5);
+          if (p > r) {
+            const bool up = (((r * 32 + lane) & size) == 0);
+            const uint64_t x = v[r], y = v[p];
+            if ((x > y) == up) { v[r] = y; v[p] = x; }
+          }
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const uint64_t o = __shfl_xor_sync(FULL, v[r], stride);
+          const bool up = (((r * 32 + lane) & size) == 0);
+          const bool lower = (lane & stride) == 0;
+          v[r] = (lower == up) ? (v[r] < o ? v[r] : o) : (v[r] < o ? o : v[r]);
+        }
+      }
+    }
+  }
+}
+
+// The first `len` (= 32 R) keys of buf, ascending, written out as ids and
+// similarities; entries equal to ~0 are padding.
+template <int R>
+__device__ __forceinline__ void sort_kept(const EmitArgs &e, int64_t i, const uint64_t *buf) {
+  const int lane = threadIdx.x & 31;
+  uint64_t v[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) v[r] = buf[r * 32 + lane];
+  warp_bitonic_asc<R>(v);
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int q = r * 32 + lane;
+    if (v[r] != ~0ULL) {
+      e.nbr_sorted[i * e.K + q] = (uint32_t)(v[r] >> 32);
+      e.nbr_sv[i * e.K + q] = __uint_as_float((uint32_t)v[r]);
+    }
+  }
+}
+
 // ── neighbour lists: cut by the calibrated threshold, sorted by id ──────────
+// Keys above the cutoff are compacted into the warp's shared buffer as
+// (id, sv bits), so an ascending sort orders ids; only the next power of two
+// above their number is sorted, in registers.
 __device__ __forceinline__ void sort_row(const EmitArgs &e, int64_t i, uint64_t *keys) {
   const int lane = threadIdx.x & 31;
   const int K = e.K;
-  const int len = pow2_at_least(K > 32 ? K : 32);
   const int c = e.topk_cnt[i];
-  // keep sv > cutoff; re-key as (id, sv bits) so an ascending sort orders ids
-  for (int q = lane; q < len; q += 32) {
-    uint64_t v = ~0ULL;
+  int kept = 0;
+  for (int q0 = 0; q0 < c; q0 += 32) {
+    const int q = q0 + lane;
+    bool ok = false;
+    uint64_t v = 0;
     if (q < c) {
       const uint64_t key = e.topk[i * K + q];
       const uint32_t svb = (uint32_t)(key >> 32);
-      const float sv = __uint_as_float(svb);
-      if ((double)sv > e.cutoff) v = ((uint64_t)(~(uint32_t)key) << 32) | svb;
+      ok = (double)__uint_as_float(svb) > e.cutoff;
+      v = ((uint64_t)(~(uint32_t)key) << 32) | svb;
     }
-    keys[q] = ~v;   // descending sort of ~v = ascending sort of v
+    const unsigned m = __ballot_sync(FULL, ok);
+    if (ok) keys[kept + __popc(m & ((1u << lane) - 1u))] = v;
+    kept += __popc(m);
   }
+  const int len = pow2_at_least(kept > 32 ? kept : 32);
+  for (int q = kept + lane; q < len; q += 32) keys[q] = ~0ULL;
   __syncwarp();
-  warp_sort_desc(keys, len);
-  int kept = 0;
-  for (int q0 = 0; q0 < len; q0 += 32) {
-    const int q = q0 + lane;
-    const uint64_t v = ~keys[q];
-    const bool ok = v != ~0ULL;
-    if (ok) {
-      e.nbr_sorted[i * K + q] = (uint32_t)(v >> 32);
-      e.nbr_sv[i * K + q] = __uint_as_float((uint32_t)v);
-    }
-    kept += __popc(__ballot_sync(FULL, ok));
-  }
+  if (len <= 32) sort_kept<1>(e, i, keys);
+  else if (len <= 64) sort_kept<2>(e, i, keys);
+  else if (len <= 128) sort_kept<4>(e, i, keys);
+  else if (len <= 256) sort_kept<8>(e, i, keys);
+  else sort_kept<16>(e, i, keys);
   if (lane == 0) e.nbr_cnt[i] = kept;
+  __syncwarp();
 }
 
 __global__ void k_sort_rows(EmitArgs e) {
