@@ -581,6 +581,7 @@ __device__ __forceinline__ void tc_item(const GraphArgs &g, uint64_t *gbuf, int3
     cp_wait1();
     __syncwarp();
     const unsigned char *tile = ring + (size_t)st * kTCT * cstride;
+    const bool interior = nc == kTCT && row0 + 32 <= row_end && (!SYM || jt >= row0 + 32);
     for (int c0 = 0; c0 < nc; c0 += 8) {
       float acc[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
       // B fragments: ldmatrix rows = columns c0 + (lane & 7), k block by lane >> 3
@@ -602,17 +603,26 @@ __device__ __forceinline__ void tc_item(const GraphArgs &g, uint64_t *gbuf, int3
           }
         }
       }
-      // candidates: value i of m-tile mt -> row mt*16 + gq + 8*(i>>1), column c0 + 2*tq + (i&1)
+      // candidates: value i of m-tile mt -> row mt*16 + gq + 8*(i>>1), column c0 + 2*tq + (i&1).
+      // Away from the staged tile's end, the valid rows' end and the diagonal
+      // (a warp-uniform test), the threshold alone decides.
       unsigned mk = 0;
+      if (interior) {
 #pragma unroll
-      for (int mt = 0; mt < 2; ++mt)
+        for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const int rr = mt * 16 + gq + 8 * (i >> 1);
-          const int cc = c0 + 2 * tq + (i & 1);
-          if (acc[mt][i] >= lo16 && cc < nc && row0 + rr < row_end && (!SYM || jt + cc > row0 + rr))
-            mk |= 1u << (mt * 4 + i);
-        }
+          for (int i = 0; i < 4; ++i) mk |= (acc[mt][i] >= lo16 ? 1u : 0u) << (mt * 4 + i);
+      } else {
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const int rr = mt * 16 + gq + 8 * (i >> 1);
+            const int cc = c0 + 2 * tq + (i & 1);
+            if (acc[mt][i] >= lo16 && cc < nc && row0 + rr < row_end && (!SYM || jt + cc > row0 + rr))
+              mk |= 1u << (mt * 4 + i);
+          }
+      }
       n_pref += 8;
       if (__any_sync(FULL, mk != 0)) {
         const int cntl = __popc(mk);
