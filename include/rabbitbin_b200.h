@@ -42,7 +42,8 @@ enum {
   RBG_ERR_NOMEM = -2,      /* device or host allocation failed / over budget     */
   RBG_ERR_CUDA = -3,       /* CUDA runtime error                                 */
   RBG_ERR_UNSUPPORTED = -4,/* option value this build does not implement         */
-  RBG_ERR_TIMEOUT = -5     /* a bounded device wait gave up                      */
+  RBG_ERR_TIMEOUT = -5,    /* a bounded device wait gave up                      */
+  RBG_ERR_COMM = -6        /* the caller's collective reported a failure         */
 };
 
 /* Options of `rabbitbin bin` and the hot-path RABBIT_* variables, with the
@@ -163,6 +164,37 @@ int rbg_free_fasta(rbg_fasta *f);
  * means of the large contigs in file order. */
 int rbg_bin_fasta(rbg_ctx *ctx, const rbg_params *p, const char *fasta, int64_t nbytes,
                   int64_t min_contig, const float *depth, int32_t S, rbg_graph *out);
+
+/* ── one assembly over several GPUs ────────────────────────────────────────
+ * No counterpart in the reference (one process on one host).  The caller
+ * supplies the collective: gather `bytes` from every rank into recv, rank r's
+ * block at recv + r * bytes, complete when the function returns; return 0 on
+ * success.  With device_buffers set, send and recv are memory of the
+ * context's device (NCCL over NVLink/NVSwitch); otherwise pinned host memory
+ * (gloo, MPI, sockets). */
+typedef int (*rbg_allgather_fn)(const void *send, void *recv, size_t bytes, void *user);
+
+typedef struct rbg_shard {
+  int32_t rank, world;
+  int32_t device_buffers;
+  int32_t reserved;
+  rbg_allgather_fn allgather;
+  void *user;
+} rbg_shard;
+
+/* rbg_bin_graph for one assembly split into contiguous row ranges: rank r
+ * passes its n_local contigs (ranks in contig order) and their coverage rows.
+ * It sketches them; the ranks gather the register codes and coverage rows;
+ * each scores the full rows of its contigs (every pair with them, the
+ * per-ordered-pair kernels); the row maxima are gathered for the calibration
+ * and the neighbour lists for the mutual filter; the rank returns the edges
+ * whose `from` is one of its contigs, with global contig ids and weights.
+ * The ranks' edges concatenated in rank order are rbg_bin_graph's graph of
+ * the whole assembly.  Every rank calls with the same params and S; the
+ * collective is called five times per call, in the same order on every rank. */
+int rbg_bin_graph_sharded(rbg_ctx *ctx, const rbg_params *p, const rbg_shard *sh,
+                          const char *seqcat, const int64_t *offsets, int64_t n_local,
+                          const float *depth, int32_t S, rbg_graph *out);
 
 /* ── batching: many assemblies per launch ─────────────────────────────────
  * No counterpart in the reference, which bins one assembly per process

@@ -99,6 +99,15 @@ class RequestStats(C.Structure):
 _lib = None
 
 
+# The collective of a sharded call: (send, recv, bytes_per_rank, user) -> 0 on success.
+ALLGATHER_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p)
+
+
+class Shard(C.Structure):
+    _fields_ = [("rank", C.c_int32), ("world", C.c_int32), ("device_buffers", C.c_int32),
+                ("reserved", C.c_int32), ("allgather", ALLGATHER_FN), ("user", C.c_void_p)]
+
+
 def lib():
     """Load the in-tree library (raises if it has not been built)."""
     global _lib
@@ -124,6 +133,8 @@ def lib():
                              C.c_int32, P(Graph)], C.c_int),
         "rbg_bin_graph": ([vp, P(Params), C.c_char_p, i64p, C.c_int64, P(C.c_float),
                            C.c_int32, P(Graph)], C.c_int),
+        "rbg_bin_graph_sharded": ([vp, P(Params), P(Shard), C.c_char_p, i64p, C.c_int64,
+                                   P(C.c_float), C.c_int32, P(Graph)], C.c_int),
         "rbg_stage": ([vp, C.c_char_p, i64p, C.c_int64, P(C.c_float), C.c_int32], C.c_int),
         "rbg_run_resident": ([vp, P(Params), P(Timing)], C.c_int),
         "rbg_fetch_graph": ([vp, P(Graph)], C.c_int),
@@ -304,6 +315,30 @@ class Context:
         d = np.ascontiguousarray(depth, np.float32).reshape(n, -1)
         return self._graph_call(self._L.rbg_bin_graph, self._h, C.byref(p), seqcat,
                                 _p(offs, C.c_int64), n, _p(d, C.c_float), d.shape[1])
+
+    def bin_graph_sharded(self, seqcat, offsets, depth, rank, world, allgather,
+                          device_buffers=False, params=None):
+        """rbg_bin_graph_sharded: this rank's contigs (a contiguous part of the
+        assembly, ranks in order); `allgather(send_ptr, recv_ptr, nbytes)`
+        gathers nbytes from every rank (see rabbitbin_b200.shard).  Returns the
+        edges whose source is one of this rank's contigs, with global ids."""
+        p = params or default_params()
+        offs = np.ascontiguousarray(offsets, np.int64)
+        n = len(offs) - 1
+        dep = np.asarray(depth, np.float32)
+        S = dep.shape[1] if dep.ndim == 2 else (dep.size // n if n else 0)
+        d = np.ascontiguousarray(dep.reshape(n, S))
+
+        def call(send, recv, nbytes, user):
+            try:
+                allgather(send, recv, nbytes)
+                return 0
+            except Exception:               # a Python exception must not look like success
+                return 1
+        fn = ALLGATHER_FN(call)
+        sh = Shard(rank, world, 1 if device_buffers else 0, 0, fn, None)
+        return self._graph_call(self._L.rbg_bin_graph_sharded, self._h, C.byref(p), C.byref(sh),
+                                seqcat, _p(offs, C.c_int64), n, _p(d, C.c_float), d.shape[1])
 
     def stage(self, seqcat, offsets, depth):
         offs = np.ascontiguousarray(offsets, np.int64)

@@ -408,8 +408,47 @@ void sym_clear(rbg_ctx *c, int64_t n1) {
   CK(cudaMemsetAsync(c->sym_np.p, 0, sizeof(unsigned long long), c->stream));
 }
 
+// One assembly over several ranks (rbg_bin_graph_sharded): this rank scores
+// rows [row_lo, row_hi); row0[r] is rank r's first row (row0[world] = n) and
+// nmax the most rows a rank holds.  gather(dsend, drecv, bytes) exchanges
+// equal-size device blocks, rank r's block at drecv + r * bytes.
+struct ShardCtx {
+  int rank = 0, world = 1;
+  int64_t row_lo = 0, row_hi = 0, nmax = 0;
+  std::vector<int64_t> row0;
+  std::function<void(const void *, void *, size_t)> gather;
+};
+
+// Every rank's rows [row0[r], row0[r+1]) of `elem`-byte items: rank r's items
+// from the block exchange (blocks of nmax * elem bytes) into dst.
+void scatter_blocks(rbg_ctx *c, const ShardCtx &sc, const void *recv, void *dst, size_t elem) {
+  const size_t blk = (size_t)sc.nmax * elem;
+  for (int r = 0; r < sc.world; ++r) {
+    const size_t bytes = (size_t)(sc.row0[r + 1] - sc.row0[r]) * elem;
+    if (bytes)
+      CK(cudaMemcpyAsync((char *)dst + (size_t)sc.row0[r] * elem, (const char *)recv + r * blk,
+                         bytes, cudaMemcpyDeviceToDevice, c->stream));
+  }
+}
+
+// This rank's rows [row_lo, row_hi) of `elem`-byte items from src, gathered
+// from every rank into dst (the whole row range).
+void share_rows(rbg_ctx *c, const ShardCtx &sc, const void *src, void *dst, size_t elem) {
+  const size_t blk = (size_t)sc.nmax * elem, mine = (size_t)(sc.row_hi - sc.row_lo) * elem;
+  c->shard_send.ensure(std::max<size_t>(blk, 16));
+  c->shard_recv.ensure(std::max<size_t>(blk * sc.world, 16));
+  CK(cudaMemsetAsync(c->shard_send.p, 0, blk, c->stream));
+  if (mine)
+    CK(cudaMemcpyAsync(c->shard_send.p, (const char *)src + (size_t)sc.row_lo * elem, mine,
+                       cudaMemcpyDeviceToDevice, c->stream));
+  sc.gather(c->shard_send.p, c->shard_recv.p, blk);
+  scatter_blocks(c, sc, c->shard_recv.p, dst, elem);
+}
+
 // Graph + edge weights on the codes already in c->codesA/B and the staged depth.
-void run_graph(rbg_ctx *c, const rbg_params *p) {
+// With sc, the rows of one rank of a sharded assembly (full rows scored, row
+// maxima and neighbour lists exchanged).
+void run_graph(rbg_ctx *c, const rbg_params *p, const ShardCtx *sc = nullptr) {
   const bool streamed_in = c->streamed;     // pairs scored behind the copy (this call only)
   c->streamed = false;
   const int64_t n = c->n;
@@ -445,7 +484,7 @@ void run_graph(rbg_ctx *c, const rbg_params *p) {
   c->prep_done = false;
   std::vector<uint32_t> maxc;
   const uint32_t *maxc_host = nullptr;
-  if (g.prefilter && n > 0) {
+  if (g.prefilter && n > 0 && !sc) {
     // Tensor-core regime: every unordered pair scored once, admitted pairs
     // listed, then each row's top-K selected from its keys.  The row maxima and
     // the pair count come back while the selection runs; a pass whose pairs did
@@ -494,18 +533,24 @@ void run_graph(rbg_ctx *c, const rbg_params *p) {
     maxc_host = hmax;
   } else {
     CK(cudaMemsetAsync(c->stats.p, 0, 2 * sizeof(unsigned long long), c->stream));
-    const size_t slots = (size_t)((n + 31) / 32) * allpairs_slices(n, K) * 32;
-    c->cand_buf.ensure(slots * allpairs_cap(K) * sizeof(uint64_t));
-    c->cand_cnt.ensure(slots * sizeof(int32_t));
+    if (sc) {
+      g.row_lo = sc->row_lo;
+      g.row_hi = sc->row_hi;
+    }
+    const int64_t rows = sc ? sc->row_hi - sc->row_lo : n;
+    const size_t slots = (size_t)((rows + 31) / 32) * allpairs_slices_rows(rows, n, K) * 32;
+    c->cand_buf.ensure(std::max<size_t>(slots, 1) * allpairs_cap(K) * sizeof(uint64_t));
+    c->cand_cnt.ensure(std::max<size_t>(slots, 1) * sizeof(int32_t));
     CK(cudaMemsetAsync(c->maxc_cand.p, 0, n1 * sizeof(uint32_t), c->stream));
     CK(cudaMemsetAsync(c->maxc_all.p, 0, n1 * sizeof(uint32_t), c->stream));
     launch_allpairs(g, c->cand_buf.as<uint64_t>(), c->cand_cnt.as<int32_t>(), c->stream);
-    c->launches += n ? 2 : 0;
+    c->launches += rows ? 2 : 0;
     CK(cudaGetLastError());
     CK(cudaEventRecord(c->ev[6], c->stream));
+    uint32_t *dmax = fused ? c->maxc_cand.as<uint32_t>() : c->maxc_all.as<uint32_t>();
+    if (sc) share_rows(c, *sc, dmax, dmax, sizeof(uint32_t));     // every rank's maxima
     maxc.assign(n1, 0);
-    CK(cudaMemcpyAsync(maxc.data(), fused ? c->maxc_cand.p : c->maxc_all.p, n * sizeof(uint32_t),
-                       cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(maxc.data(), dmax, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     maxc_host = maxc.data();
   }
@@ -528,13 +573,23 @@ void run_graph(rbg_ctx *c, const rbg_params *p) {
   e.nbr_sv = c->nbr_sv.as<float>();
   e.nbr_cnt = c->nbr_cnt.as<int32_t>();
   e.row_edges = c->row_edges.as<int32_t>();
+  if (sc) {
+    e.row_lo = sc->row_lo;
+    e.row_hi = sc->row_hi;
+  }
+  const int64_t e_hi = sc ? sc->row_hi : n;
   launch_sort_rows(e, c->stream);
+  if (sc) {
+    // the mutual filter reads the partners' lists: every rank's rows
+    share_rows(c, *sc, e.nbr_sorted, e.nbr_sorted, (size_t)K * sizeof(uint32_t));
+    share_rows(c, *sc, e.nbr_cnt, e.nbr_cnt, sizeof(int32_t));
+  }
   launch_count_edges(e, c->stream);
   c->launches += n ? 3 : 0;
   int32_t ne = 0;
-  if (n > 0) {
-    CK(cudaMemcpyAsync(&ne, c->row_edges.as<int32_t>() + n, sizeof(int32_t), cudaMemcpyDeviceToHost,
-                       c->stream));
+  if (n > 0 && e_hi > e.row_lo) {
+    CK(cudaMemcpyAsync(&ne, c->row_edges.as<int32_t>() + e_hi, sizeof(int32_t),
+                       cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
   }
   c->n_edges = ne;
@@ -658,6 +713,93 @@ void fetch(rbg_ctx *c, rbg_graph *out) {
     CK(cudaMemcpyAsync(out->score, c->e_score.p, ne * 4, cudaMemcpyDeviceToHost, c->stream));
   }
   CK(cudaStreamSynchronize(c->stream));
+}
+
+// One rank of rbg_bin_graph_sharded.
+void bin_graph_sharded(rbg_ctx *c, const rbg_params *p, const rbg_shard *sh, const char *seqcat,
+                       const int64_t *offsets, int64_t n_local, const float *depth, int S,
+                       rbg_graph *out) {
+  if (!sh || !sh->allgather || sh->world < 1 || sh->rank < 0 || sh->rank >= sh->world)
+    throw Error(RBG_ERR_ARG, "bad shard description");
+  if (n_local < 0) throw Error(RBG_ERR_ARG, "n_local < 0");
+  const int W = sh->world;
+  const int m = p->m, mpad = mpad_of(m);
+  ShardCtx sc;
+  sc.rank = sh->rank;
+  sc.world = W;
+  sc.gather = [c, sh, W](const void *dsend, void *drecv, size_t bytes) {
+    CK(cudaStreamSynchronize(c->stream));
+    int rc;
+    if (sh->device_buffers) {
+      rc = sh->allgather(dsend, drecv, bytes, sh->user);
+    } else {
+      c->shard_host.ensure(bytes * (W + 1));
+      char *h = c->shard_host.as<char>();
+      CK(cudaMemcpy(h, dsend, bytes, cudaMemcpyDeviceToHost));
+      rc = sh->allgather(h, h + bytes, bytes, sh->user);
+      if (rc == 0) CK(cudaMemcpy(drecv, h + bytes, bytes * W, cudaMemcpyHostToDevice));
+    }
+    if (rc != 0) throw Error(RBG_ERR_COMM, "the caller's allgather failed");
+  };
+  // 1. how many rows each rank holds (and the same S everywhere)
+  {
+    c->shard_send.ensure(16);
+    c->shard_recv.ensure(16 * W);
+    const int64_t mine[2] = {n_local, S};
+    CK(cudaMemcpyAsync(c->shard_send.p, mine, sizeof(mine), cudaMemcpyHostToDevice, c->stream));
+    sc.gather(c->shard_send.p, c->shard_recv.p, sizeof(mine));
+    std::vector<int64_t> all(2 * W);
+    CK(cudaMemcpy(all.data(), c->shard_recv.p, all.size() * sizeof(int64_t), cudaMemcpyDeviceToHost));
+    sc.row0.assign(W + 1, 0);
+    for (int r = 0; r < W; ++r) {
+      if (all[2 * r + 1] != S) throw Error(RBG_ERR_ARG, "ranks disagree on S");
+      if (all[2 * r] < 0) throw Error(RBG_ERR_ARG, "a rank passed n_local < 0");
+      sc.row0[r + 1] = sc.row0[r] + all[2 * r];
+      sc.nmax = std::max(sc.nmax, all[2 * r]);
+    }
+  }
+  const int64_t n = sc.row0[W];
+  if (n >= (1 << 27)) throw Error(RBG_ERR_UNSUPPORTED, "at most 2^27 - 1 contigs per assembly");
+  sc.row_lo = sc.row0[sc.rank];
+  sc.row_hi = sc.row0[sc.rank + 1];
+  // 2. this rank's contigs: stage and sketch
+  stage(c, seqcat, offsets, n_local, depth, S);
+  run_sketch(c, p, false);
+  // 3. every rank's register codes and coverage rows
+  const size_t code_b = (size_t)sc.nmax * mpad, dep_b = (size_t)sc.nmax * S * sizeof(float);
+  const size_t blk = code_b + ((dep_b + 15) & ~(size_t)15);
+  c->shard_send.ensure(std::max<size_t>(blk, 16));
+  c->shard_recv.ensure(std::max<size_t>(blk * W, 16));
+  CK(cudaMemsetAsync(c->shard_send.p, 0, blk, c->stream));
+  if (n_local) {
+    CK(cudaMemcpyAsync(c->shard_send.p, c->codesA.p, (size_t)n_local * mpad, cudaMemcpyDeviceToDevice,
+                       c->stream));
+    if (S)
+      CK(cudaMemcpyAsync(c->shard_send.as<char>() + code_b, c->depth.p,
+                         (size_t)n_local * S * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
+  }
+  sc.gather(c->shard_send.p, c->shard_recv.p, blk);
+  const int64_t n1 = std::max<int64_t>(n, 1);
+  c->n = n;
+  c->codesA.ensure(n1 * mpad);
+  c->codesB.ensure(n1 * mpad);
+  c->depth.ensure(std::max<size_t>(1, (size_t)n * S) * sizeof(float));
+  const char *rb = c->shard_recv.as<char>();
+  for (int r = 0; r < W; ++r) {
+    const int64_t nr = sc.row0[r + 1] - sc.row0[r];
+    if (!nr) continue;
+    CK(cudaMemcpyAsync(c->codesA.as<char>() + sc.row0[r] * mpad, rb + r * blk, (size_t)nr * mpad,
+                       cudaMemcpyDeviceToDevice, c->stream));
+    if (S)
+      CK(cudaMemcpyAsync(c->depth.as<float>() + sc.row0[r] * S, rb + r * blk + code_b,
+                         (size_t)nr * S * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
+  }
+  launch_codes_b(c->codesA.as<uint8_t>(), c->codesB.as<uint8_t>(), n * mpad, c->stream);
+  c->launches += n ? 1 : 0;
+  c->prep_done = false;                // coverage rows of the whole assembly
+  // 4. full rows of this rank's contigs; maxima and neighbour lists exchanged
+  run_graph(c, p, &sc);
+  fetch(c, out);
 }
 
 // Map externally produced 32-bit winner rows onto register codes.
@@ -790,13 +932,15 @@ int rbg_destroy(rbg_ctx *c) {
                   &c->maxc_all, &c->stats, &c->pairs, &c->pair_out, &c->nbr, &c->nbr_sv,
                   &c->nbr_cnt, &c->row_edges, &c->e_from, &c->e_to, &c->e_scomp, &c->e_score,
                   &c->badflag, &c->tmp, &c->cand_buf, &c->cand_cnt, &c->colacc, &c->unit16,
-                  &c->sym_pairs, &c->sym_np, &c->sym_rowcnt, &c->sym_rowoff, &c->sym_keys};
+                  &c->sym_pairs, &c->sym_np, &c->sym_rowcnt, &c->sym_rowoff, &c->sym_keys,
+                  &c->shard_send, &c->shard_recv};
   for (DBuf *b : bufs) b->release();
   if (c->tables) c->tables->release();
   release_batch_graphs(c);
   if (c->batch) c->batch->release();
   if (c->fasta) c->fasta->release();
   c->pin.release();
+  c->shard_host.release();
   for (auto &e : c->ev) cudaEventDestroy(e);
   cudaStreamSynchronize(c->aux);
   cudaStreamSynchronize(c->copy);
@@ -904,6 +1048,16 @@ int rbg_bin_graph(rbg_ctx *c, const rbg_params *p, const char *seqcat, const int
     stage_sketch_chunked(c, p, seqcat, offsets, n, depth, S);
     run_graph(c, p);
     fetch(c, out);
+  });
+}
+
+int rbg_bin_graph_sharded(rbg_ctx *c, const rbg_params *p, const rbg_shard *sh,
+                          const char *seqcat, const int64_t *offsets, int64_t n_local,
+                          const float *depth, int32_t S, rbg_graph *out) {
+  return guarded(c, [&] {
+    validate(p);
+    if (!out) throw Error(RBG_ERR_ARG, "out is null");
+    bin_graph_sharded(c, p, sh, seqcat, offsets, n_local, depth, S, out);
   });
 }
 

@@ -233,6 +233,8 @@ struct rbg_ctx {
   // symmetric all-pairs pass: admitted pairs, per-row counts, offsets and keys
   rbg::DBuf sym_pairs, sym_np, sym_rowcnt, sym_rowoff, sym_keys;
   uint64_t sym_cap = 0;                  // pair-list capacity (grows when a pass overflows)
+  rbg::DBuf shard_send, shard_recv;      // exchange blocks of rbg_bin_graph_sharded
+  rbg::HBuf shard_host;                  // their host staging for host-memory collectives
   bool streamed = false;                 // rbg_bin_graph scored the pairs behind the copy
   int no_stream_S = -1;                  // S whose survivors outgrew the list when streamed
   rbg::HBuf pin;                         // row maxima and pair count read back for calibration

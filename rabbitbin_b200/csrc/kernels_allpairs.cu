@@ -297,9 +297,10 @@ __device__ __forceinline__ void dense_item(const GraphArgs &g, uint64_t *gbuf, i
                                            unsigned char *smem) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t n = g.n;
-  const int64_t row0 = bx * 32;
+  const int64_t rhi = g.row_hi < 0 ? n : g.row_hi;
+  const int64_t row0 = g.row_lo + bx * 32;
   const int64_t row = row0 + lane;
-  const bool vrow = row < n;
+  const bool vrow = row < rhi;
   const int mw = g.mpad >> 2;
   const int mwq = ((mw + 27) & ~31) + 4;           // = 4 mod 32 words: conflict-free LDS.128
   const int slice = by * kWarps + warp;              // column slice of this warp
@@ -501,10 +502,11 @@ __device__ __forceinline__ void tc_item(const GraphArgs &g, uint64_t *gbuf, int3
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gq = lane >> 2, tq = lane & 3;
   const int64_t n = g.n;
-  const int64_t row0 = bx * 32;
+  const int64_t row0 = (SYM ? 0 : g.row_lo) + bx * 32;
   const int slice = by * kWarps + warp;
   // columns [c_lo, c_hi); rows at or past row_end are never candidates
-  const int64_t c_hi = (SYM && ce >= 0) ? ce : n, row_end = c_hi;
+  const int64_t c_hi = (SYM && ce >= 0) ? ce : n;
+  const int64_t row_end = SYM ? c_hi : (g.row_hi < 0 ? n : g.row_hi);
   const int64_t c_lo = SYM ? (row0 > cb ? row0 : cb) : 0;
   const int64_t span = c_hi > c_lo ? c_hi - c_lo : 0;
   const int64_t jb = c_lo + span * slice / P, je = c_lo + span * (slice + 1) / P;
@@ -761,7 +763,7 @@ __device__ __forceinline__ void merge_row(const GraphArgs &g, const uint64_t *gb
                                           uint64_t *keys) {
   const int lane = threadIdx.x & 31;
   const int K = g.K;
-  const int64_t rb = row >> 5, rl = row & 31;
+  const int64_t rb = (row - g.row_lo) >> 5, rl = (row - g.row_lo) & 31;
   const size_t br0 = (size_t)rb * P * 32 + rl;          // slice s: br0 + 32 s
   const int cl = lane < P ? gcnt[br0 + (size_t)lane * 32] : 0;   // P <= 32
   int fill = 0;
@@ -792,8 +794,8 @@ __global__ void __launch_bounds__(kMergeWarps * 32)
 k_merge_topk(GraphArgs g, const uint64_t *gbuf, const int32_t *gcnt, int cap, int P) {
   __shared__ uint64_t mk[kMergeWarps][kMergeBuf];
   const int wib = threadIdx.x >> 5;
-  const int64_t row = (int64_t)blockIdx.x * kMergeWarps + wib;
-  if (row < g.n) merge_row(g, gbuf, gcnt, cap, P, row, mk[wib]);
+  const int64_t row = g.row_lo + (int64_t)blockIdx.x * kMergeWarps + wib;
+  if (row < (g.row_hi < 0 ? g.n : g.row_hi)) merge_row(g, gbuf, gcnt, cap, P, row, mk[wib]);
 }
 
 __global__ void __launch_bounds__(kMergeWarps * 32)
@@ -929,8 +931,10 @@ int allpairs_cap(int K) { return (K + 64 + 31) & ~31; }
 
 // Column slices per 32-row block: enough warps for several waves of the GPU,
 // each slice at least 64 columns; a multiple of the CTA's warp count.
-int allpairs_slices(int64_t n, int K) {
-  const int64_t blocks = (n + 31) / 32;
+int allpairs_slices(int64_t n, int K) { return allpairs_slices_rows(n, n, K); }
+
+int allpairs_slices_rows(int64_t rows, int64_t n, int K) {
+  const int64_t blocks = (rows + 31) / 32;
   int64_t P = (4 * 148 * 48 + blocks - 1) / std::max<int64_t>(blocks, 1);
   P = std::min<int64_t>(P, std::max<int64_t>(n / 64, 1));
   P = std::max<int64_t>(P, 1);
@@ -963,10 +967,11 @@ int allpairs_variant(const GraphArgs &g) {
 }
 
 void launch_allpairs(const GraphArgs &g, uint64_t *gbuf, int32_t *gcnt, cudaStream_t s) {
-  if (g.n == 0) return;
+  const int64_t rows = (g.row_hi < 0 ? g.n : g.row_hi) - g.row_lo;
+  if (g.n == 0 || rows <= 0) return;
   const int cap = allpairs_cap(g.K);
-  const int P = allpairs_slices(g.n, g.K);
-  const dim3 grid((unsigned)((g.n + 31) / 32), (unsigned)(P / kWarps));
+  const int P = allpairs_slices_rows(rows, g.n, g.K);
+  const dim3 grid((unsigned)((rows + 31) / 32), (unsigned)(P / kWarps));
   float lo, hi, lo16;
   prefilter_bands(g.S, g.prefilter_eps, &lo, &hi, &lo16);
   const int v = allpairs_variant(g);
@@ -985,7 +990,7 @@ void launch_allpairs(const GraphArgs &g, uint64_t *gbuf, int32_t *gcnt, cudaStre
     k_allpairs<4><<<grid, kWarps * 32, smem, s>>>(g, gbuf, gcnt, cap, P);
   }
 #undef RBG_TC
-  k_merge_topk<<<(unsigned)((g.n + kMergeWarps - 1) / kMergeWarps), kMergeWarps * 32, 0, s>>>(
+  k_merge_topk<<<(unsigned)((rows + kMergeWarps - 1) / kMergeWarps), kMergeWarps * 32, 0, s>>>(
       g, gbuf, gcnt, cap, P);
 }
 

@@ -356,8 +356,8 @@ __device__ __forceinline__ void sort_row(const EmitArgs &e, int64_t i, uint64_t 
 __global__ void k_sort_rows(EmitArgs e) {
   extern __shared__ uint64_t shk[];
   const int wib = threadIdx.x >> 5;
-  const int64_t i = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
-  if (i >= e.n) return;
+  const int64_t i = e.row_lo + (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
+  if (i >= (e.row_hi < 0 ? e.n : e.row_hi)) return;
   sort_row(e, i, shk + (size_t)wib * pow2_at_least(e.K > 32 ? e.K : 32));
 }
 
@@ -404,8 +404,8 @@ __device__ __forceinline__ void count_edges_row(const EmitArgs &e, int64_t i) {
 }
 
 __global__ void k_count_edges(EmitArgs e) {
-  const int64_t i = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (i < e.n) count_edges_row(e, i);
+  const int64_t i = e.row_lo + (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (i < (e.row_hi < 0 ? e.n : e.row_hi)) count_edges_row(e, i);
 }
 
 __global__ void k_count_edges_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows) {
@@ -462,8 +462,8 @@ __device__ __forceinline__ void write_edges_row(const EmitArgs &e, int64_t i) {
 }
 
 __global__ void k_write_edges(EmitArgs e) {
-  const int64_t i = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (i < e.n) write_edges_row(e, i);
+  const int64_t i = e.row_lo + (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (i < (e.row_hi < 0 ? e.n : e.row_hi)) write_edges_row(e, i);
 }
 
 __global__ void k_write_edges_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows) {
@@ -600,23 +600,28 @@ void launch_pair_counts(const uint8_t *A, const uint8_t *B, int mpad, int m,
 }
 
 void launch_sort_rows(const EmitArgs &e, cudaStream_t s) {
-  if (e.n == 0) return;
+  const int64_t rows = (e.row_hi < 0 ? e.n : e.row_hi) - e.row_lo;
+  if (rows <= 0) return;
   int len = 1;
   while (len < (e.K > 32 ? e.K : 32)) len <<= 1;
   const int warps = 4;
-  k_sort_rows<<<(unsigned)((e.n + warps - 1) / warps), warps * 32,
+  k_sort_rows<<<(unsigned)((rows + warps - 1) / warps), warps * 32,
                 (size_t)warps * len * 8, s>>>(e);
 }
 
+// Edge counts of the rows, then their exclusive scan in place (total at
+// row_edges[row_hi]): the edges of row i start at row_edges[i].
 void launch_count_edges(const EmitArgs &e, cudaStream_t s) {
-  if (e.n == 0) return;
-  k_count_edges<<<(unsigned)((e.n + 7) / 8), 256, 0, s>>>(e);   // warp per row
-  k_scan<<<1, 1024, 0, s>>>(e.row_edges, e.n);
+  const int64_t rows = (e.row_hi < 0 ? e.n : e.row_hi) - e.row_lo;
+  if (rows <= 0) return;
+  k_count_edges<<<(unsigned)((rows + 7) / 8), 256, 0, s>>>(e);   // warp per row
+  k_scan<<<1, 1024, 0, s>>>(e.row_edges + e.row_lo, rows);
 }
 
 void launch_write_edges(const EmitArgs &e, cudaStream_t s) {
-  if (e.n == 0) return;
-  k_write_edges<<<(unsigned)((e.n + 7) / 8), 256, 0, s>>>(e);   // warp per row
+  const int64_t rows = (e.row_hi < 0 ? e.n : e.row_hi) - e.row_lo;
+  if (rows <= 0) return;
+  k_write_edges<<<(unsigned)((rows + 7) / 8), 256, 0, s>>>(e);   // warp per row
 }
 
 void launch_edge_weights(const WeightArgs &w, cudaStream_t s) {

@@ -452,6 +452,32 @@ void launch_pack_range(const char *ascii, int64_t nbases, int64_t w_begin, int64
                                       packed, nmask);
 }
 
+namespace {
+
+// Column-side codes from row-side ones: B = A, with 0xFF where A is 0 (unset).
+__global__ void k_codes_b(const uint4 *__restrict__ A, uint4 *__restrict__ B, int64_t n16) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n16) return;
+  const uint4 a = A[i];
+  uint32_t w[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    // 0x80 in each zero byte (the add cannot carry out of a byte)
+    const uint32_t z = ~(((w[q] & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | w[q]) & 0x80808080u;
+    w[q] |= (z >> 7) * 0xFFu;
+  }
+  B[i] = make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+}  // namespace
+
+void launch_codes_b(const uint8_t *codesA, uint8_t *codesB, int64_t bytes, cudaStream_t s) {
+  const int64_t n16 = bytes / 16;
+  if (n16 == 0) return;
+  k_codes_b<<<(unsigned)((n16 + 255) / 256), 256, 0, s>>>((const uint4 *)codesA, (uint4 *)codesB,
+                                                          n16);
+}
+
 void launch_count(const SketchArgs &a, cudaStream_t s) {
   if (a.n == 0) return;
   const int warps = 8;

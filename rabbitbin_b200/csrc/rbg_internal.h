@@ -90,6 +90,8 @@ void launch_pack_range(const char *ascii, int64_t nbases, int64_t w_begin, int64
                        uint32_t *packed, uint32_t *nmask, cudaStream_t s);
 void launch_count(const SketchArgs &a, cudaStream_t s);
 void launch_minreduce(const SketchArgs &a, cudaStream_t s);
+// codesB from codesA over `bytes` (a multiple of 16): equal codes, 0xFF for unset.
+void launch_codes_b(const uint8_t *codesA, uint8_t *codesB, int64_t bytes, cudaStream_t s);
 
 struct GraphArgs {
   int64_t n = 0;
@@ -119,6 +121,10 @@ struct GraphArgs {
   // Keys at or below key_floor are never admitted to a row's candidates
   // (admission_floor()).
   uint64_t key_floor = 0;
+  // rows scored by the per-ordered-pair kernels (launch_allpairs): [row_lo,
+  // row_hi) against every column; row_hi < 0 means n (a sharded assembly
+  // scores its own rows)
+  int64_t row_lo = 0, row_hi = -1;
 };
 
 // The lowest key worth keeping: similarity 0.039 with the largest id bits.
@@ -173,6 +179,8 @@ void launch_rows_topk(const GraphArgs &g, const SymOut &o, int64_t *rowoff, uint
 void launch_rows_topk_counts(const GraphArgs &g, const SymOut &o, const uint32_t *svtab,
                              int64_t *rowoff, uint64_t *keys, cudaStream_t s);
 int allpairs_slices(int64_t n, int K);
+// Column slices for `rows` rows against n columns (launch_allpairs on a row range).
+int allpairs_slices_rows(int64_t rows, int64_t n, int K);
 int allpairs_cap(int K);
 
 struct EmitArgs {
@@ -187,6 +195,9 @@ struct EmitArgs {
   int32_t *row_edges = nullptr;        // [n+1] edges per row, then exclusive scan
   uint32_t *from = nullptr, *to = nullptr;
   float *scomp = nullptr;
+  // rows whose neighbour lists and edges the plain launchers produce:
+  // [row_lo, row_hi), row_hi < 0 means n; row_edges is scanned over that range
+  int64_t row_lo = 0, row_hi = -1;
 };
 
 void launch_sort_rows(const EmitArgs &e, cudaStream_t s);

@@ -86,3 +86,36 @@ def test_failed_rank_ends_the_job(tmp_path):
     else:
         raise AssertionError("the job did not report the failed rank")
     assert not (tmp_path / "ranks.json").exists()
+
+
+def _gather_main(rank, world, port, outdir):
+    import ctypes
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world), LOCAL_RANK=str(rank))
+    shard.init(world, "gloo", timeout_s=30)
+    fn = shard.host_allgather()
+    nbytes = 24
+    send = (np.arange(nbytes, dtype=np.uint8) + 50 * rank).astype(np.uint8)
+    recv = np.zeros(nbytes * world, np.uint8)
+    fn(send.ctypes.data, recv.ctypes.data, nbytes)
+    if rank == 0:
+        np.save(os.path.join(outdir, "recv.npy"), recv)
+    shard.finish(world)
+
+
+def test_host_allgather_adapter(tmp_path):
+    """The host-memory collective handed to rbg_bin_graph_sharded: rank r's
+    bytes land at r * nbytes of every rank's receive buffer."""
+    world = 2
+    mp.spawn(_gather_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True)
+    recv = np.load(tmp_path / "recv.npy")
+    want = np.concatenate([(np.arange(24) + 50 * r).astype(np.uint8) for r in range(world)])
+    assert np.array_equal(recv, want)
+
+
+def test_row_ranges_tile_the_assembly():
+    for n in (0, 1, 7, 4000):
+        for world in (1, 2, 3, 8):
+            rr = [shard.row_range(n, r, world) for r in range(world)]
+            assert rr[0][0] == 0 and rr[-1][1] == n
+            assert all(rr[r][1] == rr[r + 1][0] for r in range(world - 1))
