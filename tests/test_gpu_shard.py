@@ -96,3 +96,32 @@ def test_one_rank_equals_whole_graph(gpu_ctx):
         assert got["b0"] == want["b0"] and got["sim_cutoff"] == want["sim_cutoff"]
         for k in ("src", "dst", "scomp", "score"):
             assert np.array_equal(got[k], want[k]), k
+
+
+def _nccl_main(rank, world, port, outdir):
+    import datetime
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=120))
+    asm = _assembly((30, 4000, 20, 505))
+    buf, offs = asm.concat()
+    p = api.default_params(force_path=2)
+    ctx = api.Context(0)
+    want = ctx.bin_graph(buf, offs, asm.depth, p)
+    got = ctx.bin_graph_sharded(buf, offs, asm.depth, rank, world, shard.device_allgather(),
+                                device_buffers=True, params=p)
+    same = got["b0"] == want["b0"] and got["sim_cutoff"] == want["sim_cutoff"] and all(
+        np.array_equal(got[k], want[k]) for k in ("src", "dst", "scomp", "score"))
+    open(os.path.join(outdir, "same.txt"), "w").write("1" if same else "0")
+    ctx.close()
+    dist.destroy_process_group()
+
+
+def test_device_buffer_collective(tmp_path):
+    """The NCCL adapter on device buffers (world size 1: NCCL needs one GPU per
+    rank, and this run has one GPU)."""
+    mp.spawn(_nccl_main, args=(1, _free_port(), str(tmp_path)), nprocs=1, join=True)
+    assert (tmp_path / "same.txt").read_text() == "1"
