@@ -18,10 +18,12 @@ BUILD = os.path.join(HERE, "_build")
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SRCS = ["kernels_sketch.cu", "kernels_graph.cu", "kernels_allpairs.cu", "kernels_util.cu",
+CU_SRCS = ["kernels_sketch.cu", "kernels_graph.cu", "kernels_allpairs.cu", "kernels_onehot.cu",
+           "kernels_util.cu",
            "noalloc.cu", "kernels_fasta.cu"]
 CPP_SRCS = ["pmh_streams.cpp", "calib.cpp", "engine.cpp", "batch.cpp", "server.cpp", "fasta.cpp"]
-HEADERS = ["rbg_internal.h", "../../include/rabbitbin_b200.h", "gen_zig_tables.py"]
+HEADERS = ["rbg_internal.h", "select_topk.cuh", "../../include/rabbitbin_b200.h",
+           "gen_zig_tables.py"]
 
 
 def _run(cmd):
@@ -68,7 +70,9 @@ def build(verbose=False, ptxas_info=False):
         objs.append(o)
     if _newer(OUT, objs):
         tmp = OUT + ".tmp"
-        _run([NVCC] + ARCH + ["-shared", "-o", tmp] + objs + ["-cudart", "static"])
+        lib64 = os.path.join(CUDA, "lib64")
+        _run([NVCC] + ARCH + ["-shared", "-o", tmp] + objs +
+             ["-cudart", "static", "-L" + lib64, "-lcublasLt", "-Xlinker", "-rpath=" + lib64])
         shutil.move(tmp, OUT)
     return OUT
 

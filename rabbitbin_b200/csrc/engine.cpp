@@ -8,6 +8,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <string>
 #include <map>
 #include <mutex>
 #include <numeric>
@@ -16,6 +17,8 @@
 #include <unordered_map>
 #include <string>
 #include <vector>
+
+#include <cublasLt.h>
 
 #include "engine_internal.h"
 
@@ -445,6 +448,84 @@ void share_rows(rbg_ctx *c, const ShardCtx &sc, const void *src, void *dst, size
   scatter_blocks(c, sc, c->shard_recv.p, dst, elem);
 }
 
+#define LTCK(x)                                                                           \
+  do {                                                                                    \
+    const cublasStatus_t st_ = (x);                                                       \
+    if (st_ != CUBLAS_STATUS_SUCCESS)                                                     \
+      throw ::rbg::Error(RBG_ERR_CUDA, std::string(#x) + ": cuBLASLt status " +           \
+                                           std::to_string((int)st_));                     \
+  } while (0)
+
+// Dense regime (no abundance prune): the counts of rows [g.row_lo, row_hi)
+// against every contig as one-hot int8 GEMMs (cuBLASLt, int32 accumulation:
+// exact), in row chunks of at most 2 GiB of counts, each chunk scanned into
+// the rows' top-K keys, maxima and compared-pair count.
+void dense_allpairs_gemm(rbg_ctx *c, const GraphArgs &g) {
+  const int64_t n = g.n, lo = g.row_lo, hi = g.row_hi < 0 ? n : g.row_hi, rows = hi - lo;
+  if (n == 0 || rows <= 0) return;
+  const int m = g.m, mpad = g.mpad;
+  cudaStream_t s = c->stream;
+  c->oh_pres.ensure((size_t)m * 8 * sizeof(uint32_t));
+  c->oh_map.ensure((size_t)m * 256 * sizeof(int32_t));
+  c->oh_koff.ensure((size_t)(m + 1) * sizeof(int32_t));
+  launch_code_presence(g.codesA, n, m, mpad, c->oh_pres.as<uint32_t>(), s);
+  launch_onehot_map(c->oh_pres.as<uint32_t>(), m, c->oh_map.as<int32_t>(), c->oh_koff.as<int32_t>(),
+                    s);
+  int32_t K = 0;
+  CK(cudaMemcpyAsync(&K, c->oh_koff.as<int32_t>() + m, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  const int64_t ldx = std::max<int64_t>(32, ((int64_t)K + 31) / 32 * 32);   // zero-padded width
+  // the int8 GEMMs take the contig dimension in multiples of 4: zero rows pad X
+  // to ldd contigs (their counts are 0 and never read)
+  const int64_t ldd = (n + 3) / 4 * 4;
+  c->oh_X.ensure((size_t)ldd * ldx);
+  launch_onehot_fill(g.codesA, n, m, mpad, c->oh_map.as<int32_t>(), c->oh_X.as<int8_t>(), ldx, s);
+  if (ldd > n)
+    CK(cudaMemsetAsync(c->oh_X.as<int8_t>() + n * ldx, 0, (size_t)(ldd - n) * ldx, s));
+  int64_t chunk = std::max<int64_t>(32, (((int64_t)1 << 29) / ldd) / 32 * 32);
+  if (chunk > rows) chunk = rows;
+  c->oh_D.ensure((size_t)chunk * ldd * sizeof(int32_t));
+  const size_t ws = (size_t)32 << 20;
+  c->oh_ws.ensure(ws);
+  if (!c->lt) LTCK(cublasLtCreate((cublasLtHandle_t *)&c->lt));
+  cublasLtHandle_t lt = (cublasLtHandle_t)c->lt;
+  cublasLtMatmulDesc_t op = nullptr;
+  cublasLtMatmulPreference_t pref = nullptr;
+  LTCK(cublasLtMatmulDescCreate(&op, CUBLAS_COMPUTE_32I, CUDA_R_32I));
+  const cublasOperation_t tA = CUBLAS_OP_T, tB = CUBLAS_OP_N;
+  LTCK(cublasLtMatmulDescSetAttribute(op, CUBLASLT_MATMUL_DESC_TRANSA, &tA, sizeof(tA)));
+  LTCK(cublasLtMatmulDescSetAttribute(op, CUBLASLT_MATMUL_DESC_TRANSB, &tB, sizeof(tB)));
+  LTCK(cublasLtMatmulPreferenceCreate(&pref));
+  LTCK(cublasLtMatmulPreferenceSetAttribute(pref, CUBLASLT_MATMUL_PREF_MAX_WORKSPACE_BYTES, &ws,
+                                            sizeof(ws)));
+  const int8_t *X = c->oh_X.as<int8_t>();
+  int32_t *D = c->oh_D.as<int32_t>();
+  for (int64_t q0 = 0; q0 < rows; q0 += chunk) {
+    const int64_t nr = std::min(chunk, rows - q0);
+    // column-major: X is ldx x n (a contig per column); D = X^T X_rows is n x nr,
+    // so row i's counts against every contig are contiguous
+    cublasLtMatrixLayout_t La = nullptr, Lb = nullptr, Ld = nullptr;
+    LTCK(cublasLtMatrixLayoutCreate(&La, CUDA_R_8I, ldx, ldd, ldx));
+    LTCK(cublasLtMatrixLayoutCreate(&Lb, CUDA_R_8I, ldx, nr, ldx));
+    LTCK(cublasLtMatrixLayoutCreate(&Ld, CUDA_R_32I, ldd, nr, ldd));
+    cublasLtMatmulHeuristicResult_t res;
+    int found = 0;
+    LTCK(cublasLtMatmulAlgoGetHeuristic(lt, op, La, Lb, Ld, Ld, pref, 1, &res, &found));
+    if (found < 1) throw Error(RBG_ERR_CUDA, "cuBLASLt found no int8 GEMM for the one-hot counts");
+    const int32_t alpha = 1, beta = 0;
+    LTCK(cublasLtMatmul(lt, op, &alpha, X, La, X + (lo + q0) * ldx, Lb, &beta, D, Ld, D, Ld,
+                        &res.algo, c->oh_ws.p, ws, s));
+    cublasLtMatrixLayoutDestroy(La);
+    cublasLtMatrixLayoutDestroy(Lb);
+    cublasLtMatrixLayoutDestroy(Ld);
+    launch_dense_select(g, D, ldd, lo + q0, nr, s);
+    c->launches += 2;
+  }
+  cublasLtMatmulPreferenceDestroy(pref);
+  cublasLtMatmulDescDestroy(op);
+  c->launches += 3;
+}
+
 // Graph + edge weights on the codes already in c->codesA/B and the staged depth.
 // With sc, the rows of one rank of a sharded assembly (full rows scored, row
 // maxima and neighbour lists exchanged).
@@ -538,13 +619,17 @@ void run_graph(rbg_ctx *c, const rbg_params *p, const ShardCtx *sc = nullptr) {
       g.row_hi = sc->row_hi;
     }
     const int64_t rows = sc ? sc->row_hi - sc->row_lo : n;
-    const size_t slots = (size_t)((rows + 31) / 32) * allpairs_slices_rows(rows, n, K) * 32;
-    c->cand_buf.ensure(std::max<size_t>(slots, 1) * allpairs_cap(K) * sizeof(uint64_t));
-    c->cand_cnt.ensure(std::max<size_t>(slots, 1) * sizeof(int32_t));
     CK(cudaMemsetAsync(c->maxc_cand.p, 0, n1 * sizeof(uint32_t), c->stream));
     CK(cudaMemsetAsync(c->maxc_all.p, 0, n1 * sizeof(uint32_t), c->stream));
-    launch_allpairs(g, c->cand_buf.as<uint64_t>(), c->cand_cnt.as<int32_t>(), c->stream);
-    c->launches += rows ? 2 : 0;
+    if (!g.prefilter) {
+      dense_allpairs_gemm(c, g);                        // tensor cores, exact counts
+    } else {
+      const size_t slots = (size_t)((rows + 31) / 32) * allpairs_slices_rows(rows, n, K) * 32;
+      c->cand_buf.ensure(std::max<size_t>(slots, 1) * allpairs_cap(K) * sizeof(uint64_t));
+      c->cand_cnt.ensure(std::max<size_t>(slots, 1) * sizeof(int32_t));
+      launch_allpairs(g, c->cand_buf.as<uint64_t>(), c->cand_cnt.as<int32_t>(), c->stream);
+      c->launches += rows ? 2 : 0;
+    }
     CK(cudaGetLastError());
     CK(cudaEventRecord(c->ev[6], c->stream));
     uint32_t *dmax = fused ? c->maxc_cand.as<uint32_t>() : c->maxc_all.as<uint32_t>();
@@ -933,7 +1018,8 @@ int rbg_destroy(rbg_ctx *c) {
                   &c->nbr_cnt, &c->row_edges, &c->e_from, &c->e_to, &c->e_scomp, &c->e_score,
                   &c->badflag, &c->tmp, &c->cand_buf, &c->cand_cnt, &c->colacc, &c->unit16,
                   &c->sym_pairs, &c->sym_np, &c->sym_rowcnt, &c->sym_rowoff, &c->sym_keys,
-                  &c->shard_send, &c->shard_recv};
+                  &c->shard_send, &c->shard_recv, &c->oh_pres, &c->oh_map, &c->oh_koff,
+                  &c->oh_X, &c->oh_D, &c->oh_ws};
   for (DBuf *b : bufs) b->release();
   if (c->tables) c->tables->release();
   release_batch_graphs(c);
@@ -941,6 +1027,8 @@ int rbg_destroy(rbg_ctx *c) {
   if (c->fasta) c->fasta->release();
   c->pin.release();
   c->shard_host.release();
+  if (c->lt) cublasLtDestroy((cublasLtHandle_t)c->lt);
+  c->lt = nullptr;
   for (auto &e : c->ev) cudaEventDestroy(e);
   cudaStreamSynchronize(c->aux);
   cudaStreamSynchronize(c->copy);

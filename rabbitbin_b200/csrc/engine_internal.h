@@ -234,6 +234,10 @@ struct rbg_ctx {
   rbg::DBuf sym_pairs, sym_np, sym_rowcnt, sym_rowoff, sym_keys;
   uint64_t sym_cap = 0;                  // pair-list capacity (grows when a pass overflows)
   rbg::DBuf shard_send, shard_recv;      // exchange blocks of rbg_bin_graph_sharded
+  // dense regime as a one-hot int8 GEMM: code presence, one-hot map and
+  // offsets, the one-hot matrix, a chunk of counts, the GEMM workspace
+  rbg::DBuf oh_pres, oh_map, oh_koff, oh_X, oh_D, oh_ws;
+  void *lt = nullptr;                    // cuBLASLt handle, created on first use
   rbg::HBuf shard_host;                  // their host staging for host-memory collectives
   bool streamed = false;                 // rbg_bin_graph scored the pairs behind the copy
   int no_stream_S = -1;                  // S whose survivors outgrew the list when streamed

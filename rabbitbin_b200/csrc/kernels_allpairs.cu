@@ -27,13 +27,13 @@
 #include <cuda_fp16.h>
 
 #include "rbg_internal.h"
+#include "select_topk.cuh"
 
 namespace rbg {
 namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int kWarps = 4;         // warps per CTA (independent)
-constexpr int kCapW = 16;         // candidate buffer <= 32 * kCapW keys per row
 
 // One 16-byte shared-memory load (a single 128-bit access: lanes reading
 // consecutive 16-byte blocks take 4 wavefronts for the warp, where four 32-bit
@@ -101,37 +101,6 @@ __device__ __forceinline__ float dot_avx512(const float (&a)[SMAX], const float 
   v[0] = __fadd_rn(v[0], v[2]);
   v[1] = __fadd_rn(v[1], v[3]);
   return __fadd_rn(v[0], v[1]);
-}
-
-// Warp-cooperative: keep the K largest of the cnt unique keys in buf (global),
-// in place; returns the K-th largest key (the new admission threshold).
-__device__ uint64_t select_topk(uint64_t *buf, int cnt, int K) {
-  const int lane = threadIdx.x & 31;
-  uint64_t v[kCapW];
-#pragma unroll
-  for (int t = 0; t < kCapW; ++t) {
-    const int i = t * 32 + lane;
-    v[t] = i < cnt ? buf[i] : 0ull;
-  }
-  uint64_t P = 0;
-  for (int bit = 63; bit >= 0; --bit) {
-    const uint64_t c = P | (1ull << bit);
-    int k = 0;
-#pragma unroll
-    for (int t = 0; t < kCapW; ++t) k += v[t] >= c;
-    if ((int)__reduce_add_sync(FULL, (unsigned)k) >= K) P = c;
-  }
-  __syncwarp();
-  int out = 0;
-#pragma unroll
-  for (int t = 0; t < kCapW; ++t) {
-    const bool keep = v[t] >= P && v[t] != 0ull;
-    const unsigned m = __ballot_sync(FULL, keep);
-    if (keep) buf[out + __popc(m & ((1u << lane) - 1u))] = v[t];
-    out += __popc(m);
-  }
-  __syncwarp();
-  return P;
 }
 
 // 16-byte asynchronous global->shared copies (per lane), and their groups.

@@ -1,0 +1,184 @@
+// Dense regime (no abundance prune) on the tensor cores.  A register column r
+// holds at most 136 distinct codes over an assembly, and far fewer in practice
+// (a few tens: the elements of smallest U win most contigs), so a contig's
+// codes are a short binary one-hot row X_i over the (register, code) pairs
+// that occur in the assembly.  The register-match count of contigs i and j
+// (src/rabbitbin.cpp:1261-1293: equal nonzero codes) is the exact integer dot
+// product X_i . X_j, so all counts are one int8 GEMM with int32 accumulation
+// (cuBLASLt, a plain library GEMM).  A warp per row then scans its counts and
+// produces what the dense all-pairs kernel produces: the per-row top-K keys
+// above the admission floor, the row maxima and the compared-pair count.
+#include <cstdint>
+
+#include "rbg_internal.h"
+#include "select_topk.cuh"
+
+namespace rbg {
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int kPresCols = 512;          // register columns per presence block (16 KB)
+
+// Which codes occur in each register column: 256 bits per column.
+__global__ void k_code_presence(const uint8_t *__restrict__ codesA, int64_t n, int m, int mpad,
+                                int64_t rows_per_block, uint32_t *__restrict__ pres) {
+  __shared__ uint32_t sp[kPresCols * 8];
+  const int c0 = blockIdx.y * kPresCols;
+  const int nc = (m - c0 < kPresCols) ? m - c0 : kPresCols;
+  for (int i = threadIdx.x; i < kPresCols * 8; i += blockDim.x) sp[i] = 0;
+  __syncthreads();
+  const int64_t r0 = (int64_t)blockIdx.x * rows_per_block;
+  const int64_t r1 = (r0 + rows_per_block < n) ? r0 + rows_per_block : n;
+  for (int64_t e = threadIdx.x; e < (r1 - r0) * nc; e += blockDim.x) {
+    const int64_t i = r0 + e / nc;
+    const int r = (int)(e % nc);
+    const uint32_t code = codesA[i * mpad + c0 + r];
+    if (code) atomicOr(&sp[r * 8 + (code >> 5)], 1u << (code & 31));
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nc * 8; i += blockDim.x)
+    if (sp[i]) atomicOr(&pres[(int64_t)c0 * 8 + i], sp[i]);
+}
+
+// One block: koff[r] = one-hot columns before register r (koff[m] = K), and
+// map[r][code] = koff[r] + rank of code among the column's codes (-1 absent).
+__global__ void k_onehot_map(const uint32_t *__restrict__ pres, int m, int32_t *__restrict__ map,
+                             int32_t *__restrict__ koff) {
+  __shared__ int32_t part[1024];
+  const int t = threadIdx.x;
+  const int per = (m + 1023) / 1024;
+  const int a = t * per, b = (a + per < m) ? a + per : m;
+  int s = 0;
+  for (int r = a; r < b; ++r)
+    for (int w = 0; w < 8; ++w) s += __popc(pres[r * 8 + w]);
+  part[t] = s;
+  __syncthreads();
+  for (int d = 1; d < 1024; d <<= 1) {
+    const int add = (t >= d) ? part[t - d] : 0;
+    __syncthreads();
+    part[t] += add;
+    __syncthreads();
+  }
+  int run = (t > 0) ? part[t - 1] : 0;
+  for (int r = a; r < b; ++r) {
+    koff[r] = run;
+    for (int w = 0; w < 8; ++w) run += __popc(pres[r * 8 + w]);
+  }
+  if (t == 1023) koff[m] = part[1023];
+  __syncthreads();
+  for (int64_t e = t; e < (int64_t)m * 256; e += 1024) {
+    const int r = (int)(e >> 8), code = (int)(e & 255);
+    const uint32_t *p = pres + r * 8;
+    int32_t v = -1;
+    if ((p[code >> 5] >> (code & 31)) & 1u) {
+      int rank = __popc(p[code >> 5] & ((1u << (code & 31)) - 1u));
+      for (int w = 0; w < (code >> 5); ++w) rank += __popc(p[w]);
+      v = koff[r] + rank;
+    }
+    map[e] = v;
+  }
+}
+
+// X[i][map[r][code_i(r)]] = 1 (X zeroed by the caller; row stride ldx bytes).
+__global__ void k_onehot_fill(const uint8_t *__restrict__ codesA, int64_t n, int m, int mpad,
+                              const int32_t *__restrict__ map, int8_t *__restrict__ X,
+                              int64_t ldx) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n * m) return;
+  const int64_t i = e / m;
+  const int r = (int)(e - i * m);
+  const uint32_t code = codesA[i * mpad + r];
+  if (code) X[i * ldx + __ldg(map + r * 256 + code)] = 1;
+}
+
+// Warp per row i of [r0, r0 + nr): its counts against every contig j are
+// D[(i - r0) * ldd + j].  Same outputs as the dense all-pairs kernel for the
+// row: top-K keys (similarity bits << 32 | ~j) of the candidates above the
+// admission floor, kept through a 512-key shared buffer and the register radix
+// select; maxima over all other j and over the candidates (anynz); the number
+// of pairs compared.
+constexpr int kSelWarps = 8;
+constexpr int kSelBuf = 32 * kCapW;   // 512 keys per warp
+
+__global__ void __launch_bounds__(kSelWarps * 32)
+k_dense_select(GraphArgs g, const int32_t *__restrict__ D, int64_t ldd, int64_t r0, int64_t nr) {
+  __shared__ uint64_t sbuf[kSelWarps][kSelBuf];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int64_t q = (int64_t)blockIdx.x * kSelWarps + wib;
+  if (q >= nr) return;
+  const int64_t i = r0 + q, n = g.n;
+  const int K = g.K;
+  const int32_t *row = D + q * ldd;
+  uint64_t *buf = sbuf[wib];
+  const uint8_t nz_i = g.anynz[i];
+  uint64_t thr = g.key_floor;
+  uint32_t mx_a = 0, mx_c = 0;
+  unsigned n_cmp = 0;
+  int fill = 0;
+  for (int64_t j0 = 0; j0 < n; j0 += 32) {
+    const int64_t j = j0 + lane;
+    const bool other = j < n && j != i;
+    const uint32_t c = j < n ? (uint32_t)row[j] : 0u;
+    const bool cand = other && (nz_i | __ldg(g.anynz + (j < n ? j : 0)));
+    if (other && c > mx_a) mx_a = c;
+    if (cand && c > mx_c) mx_c = c;
+    n_cmp += other;
+    const uint64_t key = ((uint64_t)__ldg(g.sv_bits + c) << 32) | (uint64_t)(~(uint32_t)j);
+    const bool adm = cand && key > thr;
+    const unsigned mk = __ballot_sync(FULL, adm);
+    if (adm) buf[fill + __popc(mk & ((1u << lane) - 1u))] = key;
+    fill += __popc(mk);
+    __syncwarp();
+    if (fill > kSelBuf - 32) {
+      thr = select_topk(buf, fill, K);
+      fill = K;
+    }
+  }
+  if (fill > K) {
+    select_topk(buf, fill, K);
+    fill = K;
+  }
+  for (int t = lane; t < fill; t += 32) g.topk[i * K + t] = buf[t];
+  mx_a = __reduce_max_sync(FULL, mx_a);
+  mx_c = __reduce_max_sync(FULL, mx_c);
+  n_cmp = __reduce_add_sync(FULL, n_cmp);
+  if (lane == 0) {
+    g.topk_cnt[i] = fill;
+    g.maxcnt_all[i] = mx_a;
+    g.maxcnt_cand[i] = mx_c;
+    if (g.stats) atomicAdd(g.stats + 1, (unsigned long long)n_cmp);
+  }
+}
+
+}  // namespace
+
+void launch_code_presence(const uint8_t *codesA, int64_t n, int m, int mpad, uint32_t *pres,
+                          cudaStream_t s) {
+  cudaMemsetAsync(pres, 0, (size_t)m * 8 * sizeof(uint32_t), s);
+  if (n == 0) return;
+  const int64_t rows_per_block = 256;
+  const dim3 grid((unsigned)((n + rows_per_block - 1) / rows_per_block),
+                  (unsigned)((m + kPresCols - 1) / kPresCols));
+  k_code_presence<<<grid, 256, 0, s>>>(codesA, n, m, mpad, rows_per_block, pres);
+}
+
+void launch_onehot_map(const uint32_t *pres, int m, int32_t *map, int32_t *koff, cudaStream_t s) {
+  k_onehot_map<<<1, 1024, 0, s>>>(pres, m, map, koff);
+}
+
+void launch_onehot_fill(const uint8_t *codesA, int64_t n, int m, int mpad, const int32_t *map,
+                        int8_t *X, int64_t ldx, cudaStream_t s) {
+  cudaMemsetAsync(X, 0, (size_t)n * ldx, s);
+  const int64_t total = n * m;
+  if (total == 0) return;
+  k_onehot_fill<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(codesA, n, m, mpad, map, X, ldx);
+}
+
+void launch_dense_select(const GraphArgs &g, const int32_t *D, int64_t ldd, int64_t r0, int64_t nr,
+                         cudaStream_t s) {
+  if (nr <= 0) return;
+  k_dense_select<<<(unsigned)((nr + kSelWarps - 1) / kSelWarps), kSelWarps * 32, 0, s>>>(
+      g, D, ldd, r0, nr);
+}
+
+}  // namespace rbg

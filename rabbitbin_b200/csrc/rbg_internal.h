@@ -274,6 +274,21 @@ void launch_write_edges_batch(const BatchAsm *B, const int64_t *row0s, int nb, i
                               cudaStream_t s);
 void launch_edge_weights_batch(const BatchAsm *B, const int64_t *edge0s, int nb, int64_t edges,
                                cudaStream_t s);
+// ── dense regime on the tensor cores (kernels_onehot.cu) ───────────────────
+// Codes occurring per register column of rows [0, n): pres[m][8] (256 bits).
+void launch_code_presence(const uint8_t *codesA, int64_t n, int m, int mpad, uint32_t *pres,
+                          cudaStream_t s);
+// One-hot column of (register, code): map[r * 256 + code] (-1 absent);
+// koff[m + 1], koff[m] = K the one-hot width.
+void launch_onehot_map(const uint32_t *pres, int m, int32_t *map, int32_t *koff, cudaStream_t s);
+// X [n][ldx] int8: 1 at (i, map[r][code_i(r)]) for every set register, else 0.
+void launch_onehot_fill(const uint8_t *codesA, int64_t n, int m, int mpad, const int32_t *map,
+                        int8_t *X, int64_t ldx, cudaStream_t s);
+// Rows [r0, r0 + nr) from their counts D[(i - r0) * ldd + j]: per-row top-K
+// keys, row maxima and compared pairs, as the dense all-pairs kernel gives.
+void launch_dense_select(const GraphArgs &g, const int32_t *D, int64_t ldd, int64_t r0, int64_t nr,
+                         cudaStream_t s);
+
 // ── FASTA ingest (kernels_fasta.cu) ────────────────────────────────────────
 // One record of a FASTA file on the device: its name range in the input, its
 // body [b0, b1) with body newlines nl_pos[nl0..nl1), its length after newline

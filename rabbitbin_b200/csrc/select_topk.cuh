@@ -1,0 +1,41 @@
+// Warp-cooperative selection of the K largest of up to 512 unique 64-bit
+// keys, shared by the all-pairs kernels and the dense-regime row scan.
+#pragma once
+#include <cstdint>
+
+namespace rbg {
+
+constexpr int kCapW = 16;         // keys per lane: buffers hold up to 32 * kCapW keys
+
+// Warp-cooperative: keep the K largest of the cnt unique keys in buf (global),
+// in place; returns the K-th largest key (the new admission threshold).
+__device__ inline uint64_t select_topk(uint64_t *buf, int cnt, int K) {
+  const int lane = threadIdx.x & 31;
+  uint64_t v[kCapW];
+#pragma unroll
+  for (int t = 0; t < kCapW; ++t) {
+    const int i = t * 32 + lane;
+    v[t] = i < cnt ? buf[i] : 0ull;
+  }
+  uint64_t P = 0;
+  for (int bit = 63; bit >= 0; --bit) {
+    const uint64_t c = P | (1ull << bit);
+    int k = 0;
+#pragma unroll
+    for (int t = 0; t < kCapW; ++t) k += v[t] >= c;
+    if ((int)__reduce_add_sync(0xffffffffu, (unsigned)k) >= K) P = c;
+  }
+  __syncwarp();
+  int out = 0;
+#pragma unroll
+  for (int t = 0; t < kCapW; ++t) {
+    const bool keep = v[t] >= P && v[t] != 0ull;
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    if (keep) buf[out + __popc(m & ((1u << lane) - 1u))] = v[t];
+    out += __popc(m);
+  }
+  __syncwarp();
+  return P;
+}
+
+}  // namespace rbg
