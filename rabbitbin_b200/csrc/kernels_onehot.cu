@@ -33,7 +33,9 @@ __global__ void k_code_presence(const uint8_t *__restrict__ codesA, int64_t n, i
     const int64_t i = r0 + e / nc;
     const int r = (int)(e % nc);
     const uint32_t code = codesA[i * mpad + c0 + r];
-    if (code) atomicOr(&sp[r * 8 + (code >> 5)], 1u << (code & 31));
+    // a column holds a few distinct codes: test before the (contended) atomic
+    if (code && !(sp[r * 8 + (code >> 5)] & (1u << (code & 31))))
+      atomicOr(&sp[r * 8 + (code >> 5)], 1u << (code & 31));
   }
   __syncthreads();
   for (int i = threadIdx.x; i < nc * 8; i += blockDim.x)
@@ -115,23 +117,42 @@ k_dense_select(GraphArgs g, const int32_t *__restrict__ D, int64_t ldd, int64_t 
   uint32_t mx_a = 0, mx_c = 0;
   unsigned n_cmp = 0;
   int fill = 0;
-  for (int64_t j0 = 0; j0 < n; j0 += 32) {
-    const int64_t j = j0 + lane;
-    const bool other = j < n && j != i;
-    const uint32_t c = j < n ? (uint32_t)row[j] : 0u;
-    const bool cand = other && (nz_i | __ldg(g.anynz + (j < n ? j : 0)));
-    if (other && c > mx_a) mx_a = c;
-    if (cand && c > mx_c) mx_c = c;
-    n_cmp += other;
-    const uint64_t key = ((uint64_t)__ldg(g.sv_bits + c) << 32) | (uint64_t)(~(uint32_t)j);
-    const bool adm = cand && key > thr;
-    const unsigned mk = __ballot_sync(FULL, adm);
-    if (adm) buf[fill + __popc(mk & ((1u << lane) - 1u))] = key;
-    fill += __popc(mk);
-    __syncwarp();
-    if (fill > kSelBuf - 32) {
-      thr = select_topk(buf, fill, K);
-      fill = K;
+  // lane takes 4 consecutive contigs per step (16-byte count loads; ldd and the
+  // row starts are multiples of 4 counts)
+  for (int64_t j0 = 0; j0 < n; j0 += 128) {
+    const int64_t jb = j0 + 4 * lane;
+    int4 c4 = make_int4(0, 0, 0, 0);
+    uint32_t nz4 = 0;
+    if (jb < n) {
+      c4 = *reinterpret_cast<const int4 *>(row + jb);
+      if (jb + 4 <= n) {
+        nz4 = *reinterpret_cast<const uint32_t *>(g.anynz + jb);
+      } else {
+        for (int t = 0; t < 4 && jb + t < n; ++t) nz4 |= (uint32_t)g.anynz[jb + t] << (8 * t);
+      }
+    }
+    const uint32_t cv[4] = {(uint32_t)c4.x, (uint32_t)c4.y, (uint32_t)c4.z, (uint32_t)c4.w};
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int64_t j = jb + t;
+      const bool other = j < n && j != i;
+      const uint32_t c = cv[t];
+      const bool cand = other && (nz_i | ((nz4 >> (8 * t)) & 0xFFu));
+      if (other && c > mx_a) mx_a = c;
+      if (cand && c > mx_c) mx_c = c;
+      n_cmp += other;
+      const uint64_t key = ((uint64_t)__ldg(g.sv_bits + c) << 32) | (uint64_t)(~(uint32_t)j);
+      const bool adm = cand && key > thr;
+      const unsigned mk = __ballot_sync(FULL, adm);
+      if (mk) {
+        if (adm) buf[fill + __popc(mk & ((1u << lane) - 1u))] = key;
+        fill += __popc(mk);
+        __syncwarp();
+        if (fill > kSelBuf - 32) {
+          thr = select_topk(buf, fill, K);
+          fill = K;
+        }
+      }
     }
   }
   if (fill > K) {
