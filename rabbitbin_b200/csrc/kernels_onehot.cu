@@ -29,14 +29,13 @@ __global__ void k_code_presence(const uint8_t *__restrict__ codesA, int64_t n, i
   __syncthreads();
   const int64_t r0 = (int64_t)blockIdx.x * rows_per_block;
   const int64_t r1 = (r0 + rows_per_block < n) ? r0 + rows_per_block : n;
-  for (int64_t e = threadIdx.x; e < (r1 - r0) * nc; e += blockDim.x) {
-    const int64_t i = r0 + e / nc;
-    const int r = (int)(e % nc);
-    const uint32_t code = codesA[i * mpad + c0 + r];
-    // a column holds a few distinct codes: test before the (contended) atomic
-    if (code && !(sp[r * 8 + (code >> 5)] & (1u << (code & 31))))
-      atomicOr(&sp[r * 8 + (code >> 5)], 1u << (code & 31));
-  }
+  for (int64_t i = r0; i < r1; ++i)
+    for (int r = threadIdx.x; r < nc; r += blockDim.x) {
+      const uint32_t code = codesA[i * mpad + c0 + r];
+      // a column holds a few distinct codes: test before the (contended) atomic
+      if (code && !(sp[r * 8 + (code >> 5)] & (1u << (code & 31))))
+        atomicOr(&sp[r * 8 + (code >> 5)], 1u << (code & 31));
+    }
   __syncthreads();
   for (int i = threadIdx.x; i < nc * 8; i += blockDim.x)
     if (sp[i]) atomicOr(&pres[(int64_t)c0 * 8 + i], sp[i]);
@@ -85,12 +84,11 @@ __global__ void k_onehot_map(const uint32_t *__restrict__ pres, int m, int32_t *
 __global__ void k_onehot_fill(const uint8_t *__restrict__ codesA, int64_t n, int m, int mpad,
                               const int32_t *__restrict__ map, int8_t *__restrict__ X,
                               int64_t ldx) {
-  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= n * m) return;
-  const int64_t i = e / m;
-  const int r = (int)(e - i * m);
-  const uint32_t code = codesA[i * mpad + r];
-  if (code) X[i * ldx + __ldg(map + r * 256 + code)] = 1;
+  const int64_t i = blockIdx.x;                     // one row per block
+  for (int r = threadIdx.x; r < m; r += blockDim.x) {
+    const uint32_t code = codesA[i * mpad + r];
+    if (code) X[i * ldx + __ldg(map + r * 256 + code)] = 1;
+  }
 }
 
 // Warp per row i of [r0, r0 + nr): its counts against every contig j are
@@ -113,7 +111,21 @@ k_dense_select(GraphArgs g, const int32_t *__restrict__ D, int64_t ldd, int64_t 
   const int32_t *row = D + q * ldd;
   uint64_t *buf = sbuf[wib];
   const uint8_t nz_i = g.anynz[i];
-  uint64_t thr = g.key_floor;
+  // Keys are ranked as (count << 32 | ~j): among admitted keys the similarity
+  // strictly increases with the count, so the order is the order of the
+  // similarity keys, which replace the counts at the end.  Admission (similarity
+  // above the floor) is a count threshold c_adm >= 1 (similarity 0 never passes).
+  const uint32_t fbits = (uint32_t)(g.key_floor >> 32);
+  int c_adm = g.m + 1;
+  for (int c0 = 0; c0 <= g.m; c0 += 32) {
+    const int cc = c0 + lane;
+    const unsigned hit = __ballot_sync(FULL, cc <= g.m && __ldg(g.sv_bits + cc) > fbits);
+    if (hit) {
+      c_adm = c0 + __ffs(hit) - 1;
+      break;
+    }
+  }
+  uint64_t thr = ((uint64_t)c_adm << 32) - 1u;
   uint32_t mx_a = 0, mx_c = 0;
   unsigned n_cmp = 0;
   int fill = 0;
@@ -141,7 +153,7 @@ k_dense_select(GraphArgs g, const int32_t *__restrict__ D, int64_t ldd, int64_t 
       if (other && c > mx_a) mx_a = c;
       if (cand && c > mx_c) mx_c = c;
       n_cmp += other;
-      const uint64_t key = ((uint64_t)__ldg(g.sv_bits + c) << 32) | (uint64_t)(~(uint32_t)j);
+      const uint64_t key = ((uint64_t)c << 32) | (uint64_t)(~(uint32_t)j);
       const bool adm = cand && key > thr;
       const unsigned mk = __ballot_sync(FULL, adm);
       if (mk) {
@@ -159,7 +171,10 @@ k_dense_select(GraphArgs g, const int32_t *__restrict__ D, int64_t ldd, int64_t 
     select_topk(buf, fill, K);
     fill = K;
   }
-  for (int t = lane; t < fill; t += 32) g.topk[i * K + t] = buf[t];
+  for (int t = lane; t < fill; t += 32) {
+    const uint64_t ck = buf[t];
+    g.topk[i * K + t] = ((uint64_t)__ldg(g.sv_bits + (ck >> 32)) << 32) | (ck & 0xFFFFFFFFull);
+  }
   mx_a = __reduce_max_sync(FULL, mx_a);
   mx_c = __reduce_max_sync(FULL, mx_c);
   n_cmp = __reduce_add_sync(FULL, n_cmp);
@@ -190,9 +205,8 @@ void launch_onehot_map(const uint32_t *pres, int m, int32_t *map, int32_t *koff,
 void launch_onehot_fill(const uint8_t *codesA, int64_t n, int m, int mpad, const int32_t *map,
                         int8_t *X, int64_t ldx, cudaStream_t s) {
   cudaMemsetAsync(X, 0, (size_t)n * ldx, s);
-  const int64_t total = n * m;
-  if (total == 0) return;
-  k_onehot_fill<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(codesA, n, m, mpad, map, X, ldx);
+  if (n == 0 || m == 0) return;
+  k_onehot_fill<<<(unsigned)n, 256, 0, s>>>(codesA, n, m, mpad, map, X, ldx);
 }
 
 void launch_dense_select(const GraphArgs &g, const int32_t *D, int64_t ldd, int64_t r0, int64_t nr,
