@@ -219,7 +219,10 @@ typedef struct rbg_batch_stats {
   int32_t n_assemblies;
   int32_t kernel_launches;     /* kernels in the call's launch sequence          */
   int32_t graph_launches;      /* CUDA graph launches (0 with RBG_NO_GRAPHS set) */
-  int32_t reserved;
+  int32_t tuned_keys;          /* (variant, m, log2 n) keys whose all-pairs tile
+                                  shape the autotuner chose in this call: the
+                                  first call that meets a key times 3 shapes
+                                  (RBG_NO_AUTOTUNE set: none, the fixed rule)   */
   int64_t rows;                /* contigs over all assemblies                   */
   int64_t pairs;               /* contig pairs scored, sum of n (n - 1) / 2     */
   int64_t items;               /* all-pairs work items (32 rows x 4 slices)     */

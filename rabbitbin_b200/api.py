@@ -66,7 +66,7 @@ class BatchStats(C.Structure):
     _fields_ = [(n, C.c_float) for n in ("stage_ms", "graph_ms", "calib_ms", "emit_ms",
                                         "total_ms")] + \
                [("n_assemblies", C.c_int32), ("kernel_launches", C.c_int32),
-                ("graph_launches", C.c_int32), ("reserved", C.c_int32),
+                ("graph_launches", C.c_int32), ("tuned_keys", C.c_int32),
                 ("rows", C.c_int64), ("pairs", C.c_int64), ("items", C.c_int64),
                 ("edges", C.c_int64)]
 

@@ -22,7 +22,9 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <numeric>
+#include <tuple>
 #include <thread>
 
 #include "engine_internal.h"
@@ -53,9 +55,10 @@ struct AsmPlan {
 // Slices per row block for an assembly of the batch: the batch's row blocks
 // already give the GPU its parallelism, so slices only bound the size of one
 // work item (32 rows x n*4/P columns), which bounds the tail of the
-// persistent kernel.
-int batch_slices(int64_t n, int K, int variant) {
-  const double target = variant == 0 ? 4.0e5 : 3.0e6;       // pairs per work item
+// persistent kernel.  `mult` scales the pairs-per-item target (the autotuner's
+// choice for the assembly's (variant, m, log2 n)).
+int batch_slices(int64_t n, int K, int variant, double mult = 1.0) {
+  const double target = (variant == 0 ? 4.0e5 : 3.0e6) * mult;   // pairs per work item
   int64_t P = (int64_t)std::ceil(4.0 * 32.0 * (double)n / target);
   const int pmax = std::max(4, std::min(32, (6400 / std::max(K, 1)) / 4 * 4));
   P = std::min<int64_t>(std::max<int64_t>(P, 4), pmax);
@@ -197,7 +200,18 @@ struct BatchPlan {
   const AsmPlan &at(int b) const { return P[ord[b]]; }
 };
 
-void plan_batch(const rbg_params *defaults, const rbg_assembly *asms, int nb, BatchPlan &L) {
+using TuneKey = std::tuple<int, int, int>;
+
+TuneKey tune_key(const AsmPlan &a) {
+  int lg = 0;
+  while (lg < 62 && ((int64_t)1 << (lg + 1)) <= std::max<int64_t>(a.n, 1)) ++lg;
+  return TuneKey(a.variant, a.m, lg);
+}
+
+// tune: the autotuner's choices (null: none); untuned: the multiplier for keys
+// it has no choice for yet.
+void plan_batch(const rbg_params *defaults, const rbg_assembly *asms, int nb, BatchPlan &L,
+                const std::map<TuneKey, double> *tune = nullptr, double untuned = 1.0) {
   L.P.assign(nb, AsmPlan());
   for (int i = 0; i < nb; ++i) {
     AsmPlan &a = L.P[i];
@@ -219,7 +233,12 @@ void plan_batch(const rbg_params *defaults, const rbg_assembly *asms, int nb, Ba
     a.fused = (a.p->force_path == 2) || (a.p->force_path == 0 && a.n > 25000);
     a.abdfirst = a.fused && a.p->abdfirst && a.S > 1 && a.w_comp < 1.0 && a.w_comp < a.p->min_edge;
     a.variant = a.abdfirst ? a.Kp / 16 : 0;
-    a.P = batch_slices(a.n, a.K, a.variant);
+    double mult = untuned;
+    if (tune) {
+      const auto it = tune->find(tune_key(a));
+      if (it != tune->end()) mult = it->second;
+    }
+    a.P = batch_slices(a.n, a.K, a.variant, mult);
     a.cap = allpairs_cap(a.K);
   }
   // group order: equal count configuration, then equal sketch tables
@@ -459,7 +478,8 @@ int launch_sketch_groups(rbg_ctx *c, BatchBufs &B, const BatchPlan &L,
 }
 
 // Depth rows, b0, all-pairs and merge for the whole batch.
-int launch_graph_stage(rbg_ctx *c, BatchBufs &B, const BatchPlan &L, const Lists &W, int nb) {
+int launch_graph_stage(rbg_ctx *c, BatchBufs &B, const BatchPlan &L, const Lists &W, int nb,
+                       bool timed = false) {
   const BatchAsm *dD = B.desc.as<BatchAsm>();
   const int64_t rows1 = std::max<int64_t>(L.rows, 1);
   int launches = 0;
@@ -480,10 +500,12 @@ int launch_graph_stage(rbg_ctx *c, BatchBufs &B, const BatchPlan &L, const Lists
   }
   for (int v = 0; v < 4; ++v) {
     if (W.list[v].empty()) continue;
+    if (timed) CK(cudaEventRecord(B.tev[2 * v], c->stream));
     launch_allpairs_batch(dD, kVariants[v], B.lists.as<int32_t>() + v * (nb + 1),
                           B.item0s.as<int64_t>() + v * (nb + 1), (int)W.list[v].size(),
                           W.item0[v].back(), W.smem[v], B.queues.as<unsigned long long>() + v,
                           o, c->stream);
+    if (timed) CK(cudaEventRecord(B.tev[2 * v + 1], c->stream));
     ++launches;
   }
   if (!W.list[0].empty()) {
@@ -498,7 +520,81 @@ int launch_graph_stage(rbg_ctx *c, BatchBufs &B, const BatchPlan &L, const Lists
   return launches;
 }
 
-// BATCH_BODY2
+// Device descriptors of the batch positions and the per-variant work lists.
+void build_items(BatchBufs &B, const BatchPlan &L, int nb, std::vector<BatchAsm> &D, Lists &W) {
+  D.assign(nb, BatchAsm());
+  W = Lists();
+  for (int b = 0; b < nb; ++b) {
+    const AsmPlan &a = L.at(b);
+    D[b] = describe(B, a, b);
+    if (a.n > 0) {
+      const int vs = vslot(a.variant);
+      if (W.item0[vs].empty()) W.item0[vs].push_back(0);
+      W.list[vs].push_back(b);
+      W.item0[vs].push_back(W.item0[vs].back() + allpairs_items(a.n, a.P));
+      W.smem[vs] = std::max(W.smem[vs], allpairs_batch_smem(a.variant, a.mpad, a.Su));
+    }
+  }
+}
+
+// Autotuner.  For keys (variant, m, log2 n) of this batch it has no choice for,
+// the graph stage runs again with the pairs-per-item target at 1x, 1/4 and 4x
+// the rule's (outside the CUDA graphs), each variant's persistent launch timed
+// by events; the fastest multiplier per variant becomes the choice for
+// the batch's untuned keys of that variant.  The runs recompute the same
+// values (top-K sets and maxima do not depend on the tiling).
+int autotune_batch(rbg_ctx *c, BatchBufs &B, const rbg_params *defaults,
+                   const rbg_assembly *asms, int nb, const BatchPlan &L0) {
+  std::vector<TuneKey> fresh;
+  for (int b = 0; b < nb; ++b) {
+    const AsmPlan &a = L0.at(b);
+    if (a.n == 0) continue;
+    const TuneKey k = tune_key(a);
+    if (B.tune.count(k)) continue;
+    if (std::find(fresh.begin(), fresh.end(), k) == fresh.end()) fresh.push_back(k);
+  }
+  if (fresh.empty()) return 0;
+  const double mults[3] = {1.0, 0.25, 4.0};
+  float t[3][4];
+  for (auto &e : B.tev)
+    if (!e) CK(cudaEventCreate(&e));
+  for (int ci = 0; ci < 3; ++ci) {
+    BatchPlan L;
+    plan_batch(defaults, asms, nb, L, &B.tune, mults[ci]);
+    ensure_buffers(B, L, nb);
+    std::vector<BatchAsm> D;
+    Lists W;
+    build_items(B, L, nb, D, W);
+    std::vector<int32_t> lists(4 * (nb + 1), 0);
+    std::vector<int64_t> item0s(4 * (nb + 1), 0);
+    for (int v = 0; v < 4; ++v) {
+      std::copy(W.list[v].begin(), W.list[v].end(), lists.begin() + v * (nb + 1));
+      std::copy(W.item0[v].begin(), W.item0[v].end(), item0s.begin() + v * (nb + 1));
+    }
+    CK(cudaMemcpyAsync(B.desc.p, D.data(), (size_t)nb * sizeof(BatchAsm), cudaMemcpyHostToDevice,
+                       c->stream));
+    CK(cudaMemcpyAsync(B.lists.p, lists.data(), lists.size() * sizeof(int32_t),
+                       cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(B.item0s.p, item0s.data(), item0s.size() * sizeof(int64_t),
+                       cudaMemcpyHostToDevice, c->stream));
+    launch_graph_stage(c, B, L, W, nb, true);
+    CK(cudaStreamSynchronize(c->stream));
+    for (int v = 0; v < 4; ++v) {
+      t[ci][v] = 0.f;
+      if (!W.list[v].empty()) CK(cudaEventElapsedTime(&t[ci][v], B.tev[2 * v], B.tev[2 * v + 1]));
+    }
+  }
+  double best[4];
+  for (int v = 0; v < 4; ++v) {
+    int bi = 0;
+    for (int ci = 1; ci < 3; ++ci)
+      if (t[ci][v] < t[bi][v]) bi = ci;
+    best[v] = mults[bi];
+  }
+  for (const TuneKey &k : fresh) B.tune[k] = best[vslot(std::get<0>(k))];
+  return (int)fresh.size();
+}
+
 }  // namespace
 
 void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms, int nb,
@@ -518,7 +614,7 @@ void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
   const bool use_graph = getenv("RBG_NO_GRAPHS") == nullptr;
 
   BatchPlan L;
-  plan_batch(defaults, asms, nb, L);
+  plan_batch(defaults, asms, nb, L, &B.tune, 1.0);
   const int64_t rows = L.rows, rows1 = std::max<int64_t>(rows, 1);
   stats.rows = rows;
   stats.pairs = L.pairs_scored;
@@ -531,19 +627,10 @@ void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
     if (!slot) slot = make_tables(p, c->stream);
     tab[b] = slot.get();
   }
-  std::vector<BatchAsm> D(nb);
+  std::vector<BatchAsm> D;
   Lists W;
-  for (int b = 0; b < nb; ++b) {
-    const AsmPlan &a = L.at(b);
-    D[b] = describe(B, a, b);
-    if (a.n > 0) {
-      const int vs = vslot(a.variant);
-      if (W.item0[vs].empty()) W.item0[vs].push_back(0);
-      W.list[vs].push_back(b);
-      W.item0[vs].push_back(W.item0[vs].back() + allpairs_items(a.n, a.P));
-      W.smem[vs] = std::max(W.smem[vs], allpairs_batch_smem(a.variant, a.mpad, a.Su));
-    }
-  }
+  build_items(B, L, nb, D, W);
+  const bool autotune = getenv("RBG_NO_AUTOTUNE") == nullptr;
   for (int v = 0; v < 4; ++v) stats.items += W.item0[v].empty() ? 0 : W.item0[v].back();
 
   // pinned staging: global offsets, b0 pairs, descriptors, index arrays
@@ -632,6 +719,11 @@ void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
     B.sym_cap = *h_np + *h_np / 4;
     B.sym_pairs.ensure(B.sym_cap * sizeof(uint4));
     B.sym_keys.ensure(2 * B.sym_cap * sizeof(uint64_t));
+  }
+  if (autotune) {
+    stats.tuned_keys = autotune_batch(c, B, defaults, asms, nb, L);
+    // the later segments read this call's descriptors again
+    CK(cudaMemcpyAsync(B.desc.p, h_desc, desc_bytes, cudaMemcpyHostToDevice, c->stream));
   }
 
   // ── host calibration of every assembly ─────────────────────────────────

@@ -127,6 +127,11 @@ struct BatchBufs {
   // symmetric all-pairs pass of the tensor-core assemblies (row space of the batch)
   DBuf sym_pairs, sym_np, sym_rowcnt, sym_rowoff, sym_keys;
   uint64_t sym_cap = 0;
+  // autotuner: multiplier of the pairs-per-item target (the all-pairs tile
+  // shape) chosen per (variant, m, log2 n), and events timing each variant's
+  // persistent launch
+  std::map<std::tuple<int, int, int>, double> tune;
+  cudaEvent_t tev[8] = {};
   HBuf hstage, hout, hedge;
   std::map<std::tuple<int, int, uint64_t, int, int>, std::unique_ptr<Tables>> tables;
   void release() {
@@ -141,6 +146,10 @@ struct BatchBufs {
     hout.release();
     hedge.release();
     sym_cap = 0;
+    tune.clear();
+    for (auto &e : tev)
+      if (e) cudaEventDestroy(e);
+    for (auto &e : tev) e = nullptr;
     for (auto &kv : tables) kv.second->release();
     tables.clear();
   }

@@ -137,3 +137,31 @@ def test_batch_empty_and_errors(gpu_ctx, mix):
     # the context stays usable after a rejected call
     got, _ = gpu_ctx.bin_batch([(buf, offs, a.depth, api.default_params(m=250))])
     _same(got[0], gpu_ctx.bin_graph(buf, offs, a.depth, api.default_params(m=250)), 0)
+
+
+def test_autotuner_keeps_results(tmp_path):
+    """The autotuner times three all-pairs tile shapes on the first batch that
+    meets a (variant, m, log2 n) key and keeps the fastest; the graphs equal
+    the fixed rule's (RBG_NO_AUTOTUNE), and a second call meets no new key."""
+    import os
+    asms = []
+    for i, (n, s) in enumerate([(3000, 20), (26000, 20), (1500, 5), (27000, 5)]):
+        a = make_assembly(max(5, n // 300), n, s, seed=960 + i, absent_frac=0.1)
+        buf, offs = a.concat()
+        asms.append((buf, offs, a.depth))
+    tuned = api.Context(0)
+    first, st1 = tuned.bin_batch(asms)
+    again, st2 = tuned.bin_batch(asms)
+    assert st1["tuned_keys"] > 0 and st2["tuned_keys"] == 0
+    os.environ["RBG_NO_AUTOTUNE"] = "1"
+    try:
+        fixed = api.Context(0)
+        want, st3 = fixed.bin_batch(asms)
+        assert st3["tuned_keys"] == 0
+    finally:
+        del os.environ["RBG_NO_AUTOTUNE"]
+    for g1, g2, w in zip(first, again, want):
+        for k in ("src", "dst", "scomp", "score"):
+            assert np.array_equal(g1[k], w[k]) and np.array_equal(g2[k], w[k])
+    tuned.close()
+    fixed.close()
