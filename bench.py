@@ -43,9 +43,9 @@ WORKLOAD = dict(workload="binning-scale assembly: 100 genomes, 50000 contigs, S=
 METRIC = "contig-pairs scored/s"
 # DRAM bytes (read + write) of the symmetric all-pairs kernel per unordered
 # pair, from the ncu capture of the 30,000-contig case
-# (profiles/k_allpairs_tc_sym_fused30k.md: 61.0 MB over 4.5e8 pairs), scaled to
+# (profiles/k_allpairs_tc_sym_fused30k.md: 61.8 MB over 4.5e8 pairs), scaled to
 # a launch by its n(n-1)/2 pairs.
-ALLPAIRS_TRAFFIC_PER_PAIR = 0.136
+ALLPAIRS_TRAFFIC_PER_PAIR = 0.137
 UNIT = "pairs/s"
 
 
@@ -221,7 +221,7 @@ def _finish(args, ctx, asm, timings, last, ms, value, result_e2e, clk, world, ra
     achieved = flops / (ap_ms / 1000.0) / 1e12 if ap_ms > 0 else 0.0
     peak = peaks.get("bf16_tflops", 1590.0)
     traffic = (ALLPAIRS_TRAFFIC_PER_PAIR * pairs_u
-               if ALLPAIRS_TRAFFIC_PER_PAIR is not None and WORKLOAD["samples"] == 20 else None)
+               if WORKLOAD["samples"] == 20 and last["pairs_prefiltered"] > 0 else None)
     # sketch: ASCII read, 2-bit words + invalid mask written and read back,
     # per-contig 1/w rows written and read, two code rows written
     nbases = sum(len(q) for q in asm.seqs)
@@ -241,7 +241,10 @@ def _finish(args, ctx, asm, timings, last, ms, value, result_e2e, clk, world, ra
         "pairs_counted": "unordered (symmetric pass)" if S > 1 and n > 25000 else "ordered",
         "gpu_launches": int(last["kernel_launches"]) * args.steps,
         "roofline": {"bound": "tensor",
-                     "kernel": "k_allpairs_tc_sym (FP16 mma prefilter + survivor compare, each pair once)",
+                     "kernel": ("k_allpairs_tc_sym (FP16 mma prefilter + survivor compare, each pair once)"
+                                if last["pairs_prefiltered"] > 0 else
+                                "dense regime: one-hot int8 GEMM (cuBLASLt) + k_dense_select; "
+                                "FLOPs below are the FP16-prefilter equivalent"),
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak else None,
                      "peak_source": f"bf16_tflops of MEASURED_PEAKS.json ({peak_src})",
@@ -538,7 +541,7 @@ def run_serve_form(args):
         trace.append((t, int(rng.integers(0, len(pool)))))
     warm = [int(np.argmin(sizes)), int(np.argmax(sizes))]
     modes = {}
-    for mode in ("batched", "plain"):
+    for mode in args.serve_modes.split(","):
         srv = api.Server(workers=1 if mode == "plain" else args.workers, plain=(mode == "plain"),
                          hbm_budget=150 << 30, max_batch=64)
         with ClockSampler(0) as clk:
@@ -553,13 +556,17 @@ def run_serve_form(args):
             "span_s": span,
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "p999_ms": float(np.percentile(lat, 99.9)), "mean_ms": float(lat.mean()),
+            "mean_queue_ms": float(np.mean([st["queue_ms"] for st, _ in res])),
+            "mean_service_ms": float(np.mean([st["service_ms"] for st, _ in res])),
             "mean_batch": float(np.mean([st["batch_size"] for st, _ in res])),
             "max_batch": int(max(st["batch_size"] for st, _ in res)),
             "wall_s": wall, "clocks": clk.summary(), "digests": [d for _, d in res]}
-    identical = modes["batched"]["digests"] == modes["plain"]["digests"]
+    identical = (modes["batched"]["digests"] == modes["plain"]["digests"]
+                 if len(modes) == 2 else None)
     for m in modes.values():
         m.pop("digests")
-    b = modes["batched"]
+    b = modes.get("batched") or modes["plain"]
+    pl = modes.get("plain") or b
     res = {
         "metric": f"served graphs/s (Poisson {args.rate:g} req/s)", "value": b["graphs_per_s"],
         "unit": "graphs/s", "n_gpus": 1, "higher_is_better": True, "scaling": "weak",
@@ -573,9 +580,9 @@ def run_serve_form(args):
                    "requests": len(trace), "pool_contigs": sizes,
                    "inputs": "pinned host memory, copies inside each request"},
         "latency_ms": {"p50": b["p50_ms"], "p99": b["p99_ms"], "p999": b["p999_ms"]},
-        "batched": b, "plain": modes["plain"],
-        "graphs_per_s_vs_plain": b["graphs_per_s"] / modes["plain"]["graphs_per_s"],
-        "outputs_identical": bool(identical), "generate_s": gen_s,
+        "batched": modes.get("batched"), "plain": modes.get("plain"),
+        "graphs_per_s_vs_plain": b["graphs_per_s"] / pl["graphs_per_s"],
+        "outputs_identical": identical, "generate_s": gen_s,
     }
     print(json.dumps(res))
 
@@ -590,6 +597,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--serve-modes", default="batched,plain",
+                    help="serve form: which request loops replay the trace")
     ap.add_argument("--contigs", type=int, default=0, help="profiling: fewer contigs")
     ap.add_argument("--samples", type=int, default=0, help="profiling: other S")
     ap.add_argument("--form", default="plain", choices=["plain", "batch", "serve"],

@@ -43,6 +43,7 @@ struct AsmPlan {
   int64_t n = 0, nbases = 0;
   int S = 0, Su = 4, Kp = 16, m = 500, mpad = 512, K = 200, E = 136;
   bool fused = false, abdfirst = false;
+  bool gemm = false;                   // dense regime on the one-hot GEMM (not in the queue)
   double w_comp = 0.0;
   int variant = 0, P = 4, cap = 288;
   // offsets into the batch buffers (elements of each buffer's type)
@@ -170,6 +171,9 @@ int64_t batch_request_bytes(const rbg_params *p, int64_t n, int64_t nbases, int 
   b += n * (int64_t)K * (8 + 4 + 4) + n * 32;                    // top-K, neighbour lists
   if (abd)
     b += n * 256 * (16 + 2 * 8) + n * 12;                        // admitted pairs, keys, rows
+  else if (dense_on_gemm())
+    b += n * (int64_t)8192 + std::min<int64_t>(n * ((n + 3) / 4 * 4) * 4, (int64_t)2 << 30);
+                                                                 // one-hot rows, a count chunk
   else
     b += ((n + 31) / 32) * P * 32 * (cap * 8 + 4);               // slice candidate buffers
   b += n * (int64_t)K / 2 * 16;                                   // edge arrays (bound)
@@ -233,6 +237,7 @@ void plan_batch(const rbg_params *defaults, const rbg_assembly *asms, int nb, Ba
     a.fused = (a.p->force_path == 2) || (a.p->force_path == 0 && a.n > 25000);
     a.abdfirst = a.fused && a.p->abdfirst && a.S > 1 && a.w_comp < 1.0 && a.w_comp < a.p->min_edge;
     a.variant = a.abdfirst ? a.Kp / 16 : 0;
+    a.gemm = !a.abdfirst && dense_on_gemm();
     double mult = untuned;
     if (tune) {
       const auto it = tune->find(tune_key(a));
@@ -265,11 +270,11 @@ void plan_batch(const rbg_params *defaults, const rbg_assembly *asms, int nb, Ba
     const int64_t nbk = (a.n + 31) / 32;
     a.gbuf0 = L.gbuf;
     a.gcnt0 = L.gcnt;
-    if (a.variant == 0) {
+    if (a.variant != 0) {
+      L.sym_rows += a.n;
+    } else if (!a.gemm) {
       L.gbuf += nbk * a.P * 32 * a.cap;
       L.gcnt += nbk * a.P * 32;
-    } else {
-      L.sym_rows += a.n;
     }
     a.winv0 = L.winv; L.winv += a.n * a.E;
     if (a.p->base_on) {
@@ -379,7 +384,7 @@ BatchAsm describe(BatchBufs &B, const AsmPlan &a, int b) {
   d.gcnt = dptr<int32_t>(B.gcnt, a.gcnt0);
   d.cap = a.cap;
   d.P = a.P;
-  d.variant = a.variant;
+  d.variant = a.gemm ? -1 : a.variant;   // -1: neither the merge nor the pair-list selection
   prefilter_bands(a.S, g.prefilter_eps, &d.lo, &d.hi, &d.lo16);
   d.colnorm_on = need_colnorm(p, a.S) ? 1 : 0;
   d.colacc = dptr<double>(B.colacc, a.acc0);
@@ -527,7 +532,7 @@ void build_items(BatchBufs &B, const BatchPlan &L, int nb, std::vector<BatchAsm>
   for (int b = 0; b < nb; ++b) {
     const AsmPlan &a = L.at(b);
     D[b] = describe(B, a, b);
-    if (a.n > 0) {
+    if (a.n > 0 && !a.gemm) {
       const int vs = vslot(a.variant);
       if (W.item0[vs].empty()) W.item0[vs].push_back(0);
       W.list[vs].push_back(b);
@@ -548,7 +553,7 @@ int autotune_batch(rbg_ctx *c, BatchBufs &B, const rbg_params *defaults,
   std::vector<TuneKey> fresh;
   for (int b = 0; b < nb; ++b) {
     const AsmPlan &a = L0.at(b);
-    if (a.n == 0) continue;
+    if (a.n == 0 || a.gemm) continue;
     const TuneKey k = tune_key(a);
     if (B.tune.count(k)) continue;
     if (std::find(fresh.begin(), fresh.end(), k) == fresh.end()) fresh.push_back(k);
@@ -630,7 +635,7 @@ void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
   std::vector<BatchAsm> D;
   Lists W;
   build_items(B, L, nb, D, W);
-  const bool autotune = getenv("RBG_NO_AUTOTUNE") == nullptr;
+  const bool autotune = getenv("RBG_NO_AUTOTUNE") == nullptr && !c->no_tune;
   for (int v = 0; v < 4; ++v) stats.items += W.item0[v].empty() ? 0 : W.item0[v].back();
 
   // pinned staging: global offsets, b0 pairs, descriptors, index arrays
@@ -719,6 +724,24 @@ void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
     B.sym_cap = *h_np + *h_np / 4;
     B.sym_pairs.ensure(B.sym_cap * sizeof(uint4));
     B.sym_keys.ensure(2 * B.sym_cap * sizeof(uint64_t));
+  }
+  // dense assemblies: one-hot GEMM and row scan each (after the device b0 and
+  // similarity tables of segment 1), then their rows' maxima read again
+  {
+    bool any = false;
+    for (int b = 0; b < nb; ++b)
+      if (L.at(b).gemm && L.at(b).n > 0) {
+        dense_allpairs_gemm(c, D[b].g);
+        launches += 5;
+        any = true;
+      }
+    if (any && rows) {
+      CK(cudaMemcpyAsync(h_maxc, B.maxc_cand.p, rows * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                         c->stream));
+      CK(cudaMemcpyAsync(h_maxc + rows1, B.maxc_all.p, rows * sizeof(uint32_t),
+                         cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+    }
   }
   if (autotune) {
     stats.tuned_keys = autotune_batch(c, B, defaults, asms, nb, L);

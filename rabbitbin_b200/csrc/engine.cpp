@@ -210,7 +210,11 @@ void stage_sketch_chunked(rbg_ctx *c, const rbg_params *p, const char *seqcat,
   CK(cudaEventRecord(c->ev_cin, c->stream));             // the buffers are free to overwrite
   CK(cudaStreamWaitEvent(c->copy, c->ev_cin, 0));
   const int G = nwords >= ((int64_t)kChunks << 16) ? kChunks : 1;
-  const bool stream_pairs = G > 1 && sym_regime(p, n, S) && c->no_stream_S != S;
+  // Streaming keeps every survivor of the prune until b0 is known; with few
+  // samples the prune passes a large share of the pairs, so it streams from
+  // S >= 10, and never again at an S whose survivors outgrew the list.
+  const bool stream_pairs = G > 1 && S >= 10 && sym_regime(p, n, S) &&
+                            !((c->no_stream_S >> (S & 63)) & 1u);
   GraphArgs ga;
   SymOut o;
   if (stream_pairs) {
@@ -389,7 +393,12 @@ GraphArgs graph_args(rbg_ctx *c, const rbg_params *p) {
 
 // Pair-list buffers of the symmetric pass (capacity c->sym_cap pairs).
 SymOut sym_buffers(rbg_ctx *c, int64_t n1) {
-  if (c->sym_cap == 0) c->sym_cap = std::max<uint64_t>(1u << 20, (uint64_t)n1 * 256);
+  if (c->sym_cap == 0) {
+    // RBG_PAIR_CAP: a smaller first list, to exercise the overflow path
+    const char *e = getenv("RBG_PAIR_CAP");
+    c->sym_cap = e ? std::max<uint64_t>(1024, strtoull(e, nullptr, 10))
+                   : std::max<uint64_t>(1u << 20, (uint64_t)n1 * 256);
+  }
   c->sym_pairs.ensure(c->sym_cap * sizeof(uint4));
   c->sym_keys.ensure(2 * c->sym_cap * sizeof(uint64_t));
   c->sym_rowcnt.ensure(n1 * sizeof(int32_t));
@@ -460,6 +469,10 @@ void share_rows(rbg_ctx *c, const ShardCtx &sc, const void *src, void *dst, size
 // against every contig as one-hot int8 GEMMs (cuBLASLt, int32 accumulation:
 // exact), in row chunks of at most 2 GiB of counts, each chunk scanned into
 // the rows' top-K keys, maxima and compared-pair count.
+}  // namespace
+
+namespace rbg {
+
 void dense_allpairs_gemm(rbg_ctx *c, const GraphArgs &g) {
   const int64_t n = g.n, lo = g.row_lo, hi = g.row_hi < 0 ? n : g.row_hi, rows = hi - lo;
   if (n == 0 || rows <= 0) return;
@@ -525,6 +538,10 @@ void dense_allpairs_gemm(rbg_ctx *c, const GraphArgs &g) {
   cublasLtMatmulDescDestroy(op);
   c->launches += 3;
 }
+
+}  // namespace rbg
+
+namespace {
 
 // Graph + edge weights on the codes already in c->codesA/B and the staged depth.
 // With sc, the rows of one rank of a sharded assembly (full rows scored, row
@@ -605,7 +622,7 @@ void run_graph(rbg_ctx *c, const rbg_params *p, const ShardCtx *sc = nullptr) {
       if (*hnp <= c->sym_cap) break;
       CK(cudaStreamSynchronize(c->stream));
       if (streamed) {
-        c->no_stream_S = S;                  // survivors outgrow the list at this S
+        c->no_stream_S |= 1ull << (S & 63);  // survivors outgrow the list at this S
         streamed = false;
       } else {
         c->sym_cap = *hnp + *hnp / 4;
@@ -621,7 +638,7 @@ void run_graph(rbg_ctx *c, const rbg_params *p, const ShardCtx *sc = nullptr) {
     const int64_t rows = sc ? sc->row_hi - sc->row_lo : n;
     CK(cudaMemsetAsync(c->maxc_cand.p, 0, n1 * sizeof(uint32_t), c->stream));
     CK(cudaMemsetAsync(c->maxc_all.p, 0, n1 * sizeof(uint32_t), c->stream));
-    if (!g.prefilter) {
+    if (!g.prefilter && dense_on_gemm()) {
       dense_allpairs_gemm(c, g);                        // tensor cores, exact counts
     } else {
       const size_t slots = (size_t)((rows + 31) / 32) * allpairs_slices_rows(rows, n, K) * 32;

@@ -116,6 +116,14 @@ struct Tables {
 // (synchronised before returning).
 std::unique_ptr<Tables> make_tables(const rbg_params *p, cudaStream_t s);
 
+// Dense regime (no abundance prune) of rows [g.row_lo, row_hi): one-hot int8
+// GEMMs of the register codes (cuBLASLt) and the row scan; writes g.topk,
+// g.topk_cnt, g.maxcnt_all, g.maxcnt_cand and g.stats[1].  Synchronises c->stream.
+void dense_allpairs_gemm(rbg_ctx *c, const GraphArgs &g);
+// The dense regime runs on the one-hot GEMM unless RBG_DENSE_ALU is set (then
+// the integer-ALU register compare, kept for the measured comparison).
+inline bool dense_on_gemm() { return getenv("RBG_DENSE_ALU") == nullptr; }
+
 // Buffers of the batch engine (many assemblies per launch).
 struct BatchBufs {
   DBuf ascii, offsets, depth, packed, nmask, winv, ecnt, codesA, codesB;
@@ -249,7 +257,8 @@ struct rbg_ctx {
   void *lt = nullptr;                    // cuBLASLt handle, created on first use
   rbg::HBuf shard_host;                  // their host staging for host-memory collectives
   bool streamed = false;                 // rbg_bin_graph scored the pairs behind the copy
-  int no_stream_S = -1;                  // S whose survivors outgrew the list when streamed
+  uint64_t no_stream_S = 0;              // bit S: survivors outgrew the list when streamed
+  bool no_tune = false;                  // batch calls keep the tile shapes they have (serving)
   rbg::HBuf pin;                         // row maxima and pair count read back for calibration
   int64_t n_edges = 0;
   double b0 = 0.0, sim_cutoff = 0.0;

@@ -878,7 +878,7 @@ k_select_rows_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t row
     if (__ldg(row0s + mid) <= r) lo = mid; else hi = mid - 1;
   }
   const BatchAsm &b = B[lo];
-  if (b.variant == 0) return;          // dense: merged from the candidate buffers
+  if (b.variant <= 0) return;          // dense: candidate buffers or the one-hot GEMM
   select_row(b.g, r - b.row0, r, off, keys, mk[wib]);
 }
 

@@ -126,6 +126,8 @@ k_dense_select(GraphArgs g, const int32_t *__restrict__ D, int64_t ldd, int64_t 
     }
   }
   uint64_t thr = ((uint64_t)c_adm << 32) - 1u;
+  // anynz of a batch assembly starts at its first row: 4-byte loads only when aligned
+  const bool nz_words = (((uintptr_t)g.anynz) & 3u) == 0;
   uint32_t mx_a = 0, mx_c = 0;
   unsigned n_cmp = 0;
   int fill = 0;
@@ -137,7 +139,7 @@ k_dense_select(GraphArgs g, const int32_t *__restrict__ D, int64_t ldd, int64_t 
     uint32_t nz4 = 0;
     if (jb < n) {
       c4 = *reinterpret_cast<const int4 *>(row + jb);
-      if (jb + 4 <= n) {
+      if (jb + 4 <= n && nz_words) {
         nz4 = *reinterpret_cast<const uint32_t *>(g.anynz + jb);
       } else {
         for (int t = 0; t < 4 && jb + t < n; ++t) nz4 |= (uint32_t)g.anynz[jb + t] << (8 * t);

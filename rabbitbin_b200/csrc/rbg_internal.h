@@ -233,7 +233,8 @@ struct BatchAsm {
   // all-pairs
   uint64_t *gbuf = nullptr;            // candidate buffers [ceil(n/32)][P][32][cap]
   int32_t *gcnt = nullptr;             // [ceil(n/32)][P][32]
-  int cap = 0, P = 0, variant = 0;     // variant: 0 dense, 1/2/4 tensor-core KS
+  int cap = 0, P = 0, variant = 0;     // variant: 0 dense (ALU), -1 dense (one-hot GEMM),
+                                       // 1/2/4 tensor-core KS
   float lo = 0.f, hi = 0.f, lo16 = 0.f;
   // column norms
   int colnorm_on = 0;

@@ -223,21 +223,30 @@ def test_graph_nonint_depths(gpu_ctx, orc, kind):
         assert np.array_equal(got["scomp"], sc) and np.array_equal(got["score"], sw)
 
 
-@pytest.mark.parametrize("S", [3, 20])
-def test_streamed_pairs_equal_resident(gpu_ctx, S):
+@pytest.mark.parametrize("S,cap", [(3, None), (12, None), (20, None), (20, "4096")])
+def test_streamed_pairs_equal_resident(S, cap):
     """rbg_bin_graph scores the pairs chunk by chunk behind the input copy with
-    admission deferred until b0 is known (falling back to the whole pass when
-    the stored survivors outgrow the list, as few samples make likely); the
-    graph equals the one of the resident path, which scores all pairs at once."""
+    admission deferred until b0 is known (from S = 10 up), falling back to the
+    whole pass when the stored survivors outgrow the list (forced here with a
+    4096-pair first list, after which that S no longer streams); the graph
+    equals the one of the resident path, which scores all pairs at once."""
+    import os
     asm = make_assembly(30, 4000, S, seed=410 + S, absent_frac=0.1)
     buf, offs = asm.concat()
     assert len(buf) >= 8 * 16 * 65536          # eight input chunks
     p = api.default_params(force_path=2)
-    streamed = gpu_ctx.bin_graph(buf, offs, asm.depth, p)
-    again = gpu_ctx.bin_graph(buf, offs, asm.depth, p)
-    gpu_ctx.stage(buf, offs, asm.depth)
-    gpu_ctx.run_resident(p)
-    resident = gpu_ctx.fetch_graph()
+    if cap:
+        os.environ["RBG_PAIR_CAP"] = cap
+    try:
+        ctx = api.Context(0)
+        streamed = ctx.bin_graph(buf, offs, asm.depth, p)
+        again = ctx.bin_graph(buf, offs, asm.depth, p)
+    finally:
+        os.environ.pop("RBG_PAIR_CAP", None)
+    ctx.stage(buf, offs, asm.depth)
+    ctx.run_resident(p)
+    resident = ctx.fetch_graph()
+    ctx.close()
     for got in (streamed, again):
         assert got["b0"] == resident["b0"] and got["sim_cutoff"] == resident["sim_cutoff"]
         for k in ("src", "dst", "scomp", "score"):
