@@ -211,8 +211,8 @@ typedef struct rbg_assembly {
 } rbg_assembly;
 
 typedef struct rbg_batch_stats {
-  float stage_ms;              /* host -> device copies of the inputs (device)  */
-  float graph_ms;              /* sketch, b0, all-pairs, merge (device)         */
+  float stage_ms;              /* input copies, the sketch behind them (device) */
+  float graph_ms;              /* depth rows, b0, all-pairs, merge (device)     */
   float calib_ms;              /* cutoff calibration of every assembly (host)   */
   float emit_ms;               /* edges + weights + copies back (device)        */
   float total_ms;              /* the whole call (host clock)                   */

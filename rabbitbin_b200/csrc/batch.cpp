@@ -2,17 +2,18 @@
 //
 // The assemblies of a call share one set of device buffers (rows of all
 // assemblies laid end to end) and one pass of each stage:
-//   pack (all bases) -> count (per k / GC-norm group) -> register minimum (per
-//   sketch-table group) -> unit rows + column norms -> b0 and similarity
+//   pack -> count (per k / GC-norm group) -> register minimum (per sketch-table
+//   group), in runs of batch positions behind their input copies on a second
+//   stream -> unit rows + column norms -> b0 and similarity
 //   tables (on the device) -> persistent all-pairs kernels pulling
 //   (assembly, row block, slice group) items from a device counter, one per
 //   variant (dense / tensor-core KS) -> top-K merge
 // then one host round trip for the rand()-driven calibration of every
 // assembly (the maxima and b0 come back together), then neighbour lists, edge
 // counts and the batch-wide scan, one more round trip for the edge total, and
-// edge emission + weights.  The device part of each of the three segments is
-// captured into a CUDA graph; an instantiated graph is updated in place when
-// the next batch has the same launch topology.
+// edge emission + weights.  The device part of each of the three segments
+// after the sketch is captured into a CUDA graph; an instantiated graph is
+// updated in place when the next batch has the same launch topology.
 //
 // Each assembly's result equals rbg_bin_graph on that assembly alone: the
 // kernels are the single-assembly kernels behind a descriptor lookup, and
@@ -424,18 +425,26 @@ struct Lists {
   size_t smem[4] = {0, 0, 0, 0};
 };
 
-// Pack, count (one launch per k / GC-norm run), register minimum (one per
-// sketch-table run); returns the number of kernel launches.
+// Sketch of the batch positions [bb, be): pack of the words holding their
+// bases, count (one launch per k / GC-norm run), register minimum (one per
+// sketch-table run); returns the number of kernel launches.  A word shared
+// with the next range is packed again by that range's call (same stream,
+// complete bytes by then); this range's contigs read only their own bases.
 int launch_sketch_groups(rbg_ctx *c, BatchBufs &B, const BatchPlan &L,
-                         const std::vector<Tables *> &tab, int nb) {
+                         const std::vector<Tables *> &tab, int bb, int be) {
   int launches = 0;
-  launch_pack(B.ascii.as<char>(), L.bases, B.packed.as<uint32_t>(), B.nmask.as<uint32_t>(),
-              c->stream);
-  launches += L.bases ? 1 : 0;
-  for (int b0 = 0; b0 < nb;) {
+  if (bb >= be) return 0;
+  const int64_t base_lo = L.at(bb).base0, base_hi = L.at(be - 1).base0 + L.at(be - 1).nbases;
+  if (base_hi > base_lo) {
+    launch_pack_range(B.ascii.as<char>(), L.bases, (base_lo / 16) & ~(int64_t)1,
+                      (base_hi + 15) / 16, B.packed.as<uint32_t>(), B.nmask.as<uint32_t>(),
+                      c->stream);
+    ++launches;
+  }
+  for (int b0 = bb; b0 < be;) {
     const rbg_params *p = L.at(b0).p;
     int b1 = b0;
-    while (b1 < nb && L.at(b1).p->k == p->k && L.at(b1).p->gc_norm == p->gc_norm &&
+    while (b1 < be && L.at(b1).p->k == p->k && L.at(b1).p->gc_norm == p->gc_norm &&
            L.at(b1).p->gc_norm_cap == p->gc_norm_cap)
       ++b1;
     const AsmPlan &f = L.at(b0);
@@ -635,7 +644,7 @@ void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
   std::vector<BatchAsm> D;
   Lists W;
   build_items(B, L, nb, D, W);
-  const bool autotune = getenv("RBG_NO_AUTOTUNE") == nullptr && !c->no_tune;
+  const bool autotune = getenv("RBG_NO_AUTOTUNE") == nullptr;
   for (int v = 0; v < 4; ++v) stats.items += W.item0[v].empty() ? 0 : W.item0[v].back();
 
   // pinned staging: global offsets, b0 pairs, descriptors, index arrays
@@ -668,20 +677,9 @@ void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
     std::copy(W.item0[v].begin(), W.item0[v].end(), h_item0s + v * (nb + 1));
   }
 
-  // ── inputs to the device ────────────────────────────────────────────────
+  // ── inputs to the device, sketched behind the copies ────────────────────
   cudaEvent_t ev0 = c->ev[0], ev1 = c->ev[1], ev2 = c->ev[2], ev3 = c->ev[3], ev4 = c->ev[4];
   CK(cudaEventRecord(ev0, c->stream));
-  for (int b = 0; b < nb; ++b) {
-    const AsmPlan &a = L.at(b);
-    if (a.nbases)
-      CK(cudaMemcpyAsync(B.ascii.as<char>() + a.base0, a.in->seqcat, (size_t)a.nbases,
-                         cudaMemcpyHostToDevice, c->stream));
-    if (a.n && a.S)
-      CK(cudaMemcpyAsync(B.depth.as<float>() + a.dep0, a.in->depth,
-                         (size_t)a.n * a.S * sizeof(float), cudaMemcpyHostToDevice, c->stream));
-  }
-  const size_t abytes = (size_t)((L.bases + 15) / 16) * 16 + 16;
-  CK(cudaMemsetAsync(B.ascii.as<char>() + L.bases, 0, abytes - (size_t)L.bases, c->stream));
   CK(cudaMemcpyAsync(B.offsets.p, h_off, off_bytes, cudaMemcpyHostToDevice, c->stream));
   if (pair_bytes) CK(cudaMemcpyAsync(B.pairs.p, h_pairs, pair_bytes, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(B.desc.p, h_desc, desc_bytes, cudaMemcpyHostToDevice, c->stream));
@@ -689,6 +687,39 @@ void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
   CK(cudaMemcpyAsync(B.pair0s.p, h_pair0s, (nb + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(B.lists.p, h_lists, 4 * (nb + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(B.item0s.p, h_item0s, 4 * (nb + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
+  // Batch positions in up to kChunks runs of about equal bases: the copy
+  // stream brings in run r's sequences and depths while the main stream
+  // sketches run r - 1.
+  int launches = 0;
+  {
+    std::vector<int> cut{0};
+    const int64_t per = std::max<int64_t>(L.bases / kChunks, 1);
+    for (int b = 0; b < nb; ++b) {
+      const AsmPlan &a = L.at(b);
+      if (b + 1 < nb && (int)cut.size() < kChunks && a.base0 + a.nbases >= per * (int64_t)cut.size())
+        cut.push_back(b + 1);
+    }
+    cut.push_back(nb);
+    CK(cudaEventRecord(c->ev_cin, c->stream));             // earlier work on the buffers is done
+    CK(cudaStreamWaitEvent(c->copy, c->ev_cin, 0));
+    const size_t abytes = (size_t)((L.bases + 15) / 16) * 16 + 16;
+    for (size_t r = 0; r + 1 < cut.size(); ++r) {
+      for (int b = cut[r]; b < cut[r + 1]; ++b) {
+        const AsmPlan &a = L.at(b);
+        if (a.nbases)
+          CK(cudaMemcpyAsync(B.ascii.as<char>() + a.base0, a.in->seqcat, (size_t)a.nbases,
+                             cudaMemcpyHostToDevice, c->copy));
+        if (a.n && a.S)
+          CK(cudaMemcpyAsync(B.depth.as<float>() + a.dep0, a.in->depth,
+                             (size_t)a.n * a.S * sizeof(float), cudaMemcpyHostToDevice, c->copy));
+      }
+      if (r + 2 == cut.size())
+        CK(cudaMemsetAsync(B.ascii.as<char>() + L.bases, 0, abytes - (size_t)L.bases, c->copy));
+      CK(cudaEventRecord(c->ev_chunk[r], c->copy));
+      CK(cudaStreamWaitEvent(c->stream, c->ev_chunk[r], 0));
+      launches += launch_sketch_groups(c, B, L, tab, cut[r], cut[r + 1]);
+    }
+  }
   CK(cudaEventRecord(ev1, c->stream));
 
   // ── segment 1: sketch, depth rows, b0, all-pairs, merge ────────────────
@@ -700,12 +731,10 @@ void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
   int64_t *h_edge0s = (int64_t *)(B.hout.as<char>() + mx_bytes + up256(nb * sizeof(float)));
   unsigned long long *h_np =
       (unsigned long long *)(B.hout.as<char>() + mx_bytes + up256(nb * sizeof(float)) + e0_bytes);
-  int launches = 0;
   // The symmetric pass reports how many pairs it admitted; a pass whose pairs
   // did not fit the list runs again with a larger one.
   for (;;) {
     captured(c, 0, use_graph, stats.graph_launches, [&] {
-      launches += launch_sketch_groups(c, B, L, tab, nb);
       launches += launch_graph_stage(c, B, L, W, nb);
       if (rows) {
         CK(cudaMemcpyAsync(h_maxc, B.maxc_cand.p, rows * sizeof(uint32_t), cudaMemcpyDeviceToHost,
@@ -804,9 +833,16 @@ void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
     w.from = e.from; w.to = e.to; w.scomp = e.scomp; w.score = B.e_score.as<float>();
     w.n_edges = edge0v[b + 1] - edge0v[b];
   }
+  // the edge arrays land in one pinned block that the graphs share (no host
+  // copy per graph); the staging buffer and copies are the fallback
   const size_t eb = up256(E1 * 4);
-  B.hedge.ensure(4 * eb);
-  char *hb = B.hedge.as<char>();
+  char *shared = (char *)pinned_take(4 * eb);
+  struct Back {                         // an error before the graphs own it: back to the pool
+    void *p;
+    ~Back() { if (p) pinned_share(p, {}); }
+  } back{shared};
+  if (!shared) B.hedge.ensure(4 * eb);
+  char *hb = shared ? shared : B.hedge.as<char>();
   uint32_t *h_from = (uint32_t *)hb;
   uint32_t *h_to = (uint32_t *)(hb + eb);
   float *h_scomp = (float *)(hb + 2 * eb);
@@ -827,6 +863,8 @@ void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
   CK(cudaStreamSynchronize(c->stream));
 
   // ── results in the caller's order ──────────────────────────────────────
+  std::vector<void *> firsts;
+  bool nomem = false;
   for (int b = 0; b < nb; ++b) {
     const AsmPlan &a = L.at(b);
     rbg_graph &g = out[a.orig];
@@ -835,14 +873,22 @@ void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
     g.b0 = a.p->base_on ? (double)b0f[b] : 0.0;
     g.sim_cutoff = cut[b];
     g.path = a.fused ? 2 : 1;
+    if (shared && ne > 0) {
+      g.from = h_from + e0;
+      g.to = h_to + e0;
+      g.scomp = h_scomp + e0;
+      g.score = h_score + e0;
+      firsts.push_back(g.from);
+      continue;
+    }
     const size_t bytes = (size_t)std::max<int64_t>(ne, 1) * 4;
     g.from = (uint32_t *)malloc(bytes);
     g.to = (uint32_t *)malloc(bytes);
     g.scomp = (float *)malloc(bytes);
     g.score = (float *)malloc(bytes);
     if (!g.from || !g.to || !g.scomp || !g.score) {
-      for (int q = 0; q < nb; ++q) rbg_free_graph(&out[q]);
-      throw Error(RBG_ERR_NOMEM, "host allocation of the edge arrays failed");
+      nomem = true;
+      break;
     }
     if (ne) {
       std::memcpy(g.from, h_from + e0, ne * 4);
@@ -850,6 +896,12 @@ void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
       std::memcpy(g.scomp, h_scomp + e0, ne * 4);
       std::memcpy(g.score, h_score + e0, ne * 4);
     }
+  }
+  back.p = nullptr;
+  if (shared) pinned_share(shared, firsts);
+  if (nomem) {
+    for (int q = 0; q < nb; ++q) rbg_free_graph(&out[q]);
+    throw Error(RBG_ERR_NOMEM, "host allocation of the edge arrays failed");
   }
   float t01 = 0, t12 = 0, t34 = 0;
   cudaEventElapsedTime(&t01, ev0, ev1);

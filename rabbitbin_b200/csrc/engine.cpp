@@ -734,10 +734,17 @@ void run_graph(rbg_ctx *c, const rbg_params *p, const ShardCtx *sc = nullptr) {
 // Pinned host blocks for graph results: the four edge arrays of one graph
 // share one block, which the device writes at DMA speed (pageable destinations
 // are slow and page-fault on first touch).  rbg_free_graph returns a block to
-// the pool; a few idle blocks are kept for reuse.
+// the pool; a few idle blocks are kept for reuse.  A batch's graphs share one
+// block (each graph's arrays are ranges of the batch-wide arrays): it returns
+// to the pool when the last of them is freed.
 struct PinnedPool {
+  struct Shared {
+    void *blk;
+    int refs;
+  };
   std::mutex mu;
   std::unordered_map<void *, size_t> live;
+  std::unordered_map<void *, Shared *> part;   // a graph's first array -> its shared block
   std::multimap<size_t, void *> idle;
   size_t idle_bytes = 0;
 
@@ -760,14 +767,34 @@ struct PinnedPool {
     return p;
   }
 
+  // Hand a block taken with take() to graphs whose first arrays are `firsts`
+  // (distinct pointers inside the block); none: the block goes back at once.
+  void share(void *blk, const std::vector<void *> &firsts) {
+    if (firsts.empty()) {
+      give(blk);
+      return;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    Shared *sh = new Shared{blk, (int)firsts.size()};
+    for (void *f : firsts) part[f] = sh;
+  }
+
   bool give(void *p) {
     std::lock_guard<std::mutex> lk(mu);
+    auto sp = part.find(p);
+    if (sp != part.end()) {
+      Shared *sh = sp->second;
+      part.erase(sp);
+      if (--sh->refs > 0) return true;
+      p = sh->blk;
+      delete sh;
+    }
     auto it = live.find(p);
     if (it == live.end()) return false;
     idle.emplace(it->second, p);
     idle_bytes += it->second;
     live.erase(it);
-    while (idle.size() > 8 || idle_bytes > ((size_t)2 << 30)) {
+    while (idle.size() > 8 || idle_bytes > ((size_t)4 << 30)) {
       auto v = idle.begin();
       idle_bytes -= v->first;
       cudaFreeHost(v->second);
@@ -781,6 +808,19 @@ PinnedPool &pinned_pool() {
   static PinnedPool *pool = new PinnedPool();     // outlives every context
   return *pool;
 }
+
+}  // namespace
+
+namespace rbg {
+
+void *pinned_take(size_t bytes) { return pinned_pool().take(bytes); }
+void pinned_share(void *blk, const std::vector<void *> &firsts) {
+  pinned_pool().share(blk, firsts);
+}
+
+}  // namespace rbg
+
+namespace {
 
 void fetch(rbg_ctx *c, rbg_graph *out) {
   if (!out) throw Error(RBG_ERR_ARG, "null graph");

@@ -124,6 +124,13 @@ void dense_allpairs_gemm(rbg_ctx *c, const GraphArgs &g);
 // the integer-ALU register compare, kept for the measured comparison).
 inline bool dense_on_gemm() { return getenv("RBG_DENSE_ALU") == nullptr; }
 
+// Pinned result blocks (pooled).  pinned_take: a block of `bytes` or null;
+// pinned_share: the block now backs graphs whose first edge arrays are
+// `firsts` (distinct), and returns to the pool when rbg_free_graph has been
+// called on each of them.
+void *pinned_take(size_t bytes);
+void pinned_share(void *blk, const std::vector<void *> &firsts);
+
 // Buffers of the batch engine (many assemblies per launch).
 struct BatchBufs {
   DBuf ascii, offsets, depth, packed, nmask, winv, ecnt, codesA, codesB;
@@ -258,7 +265,6 @@ struct rbg_ctx {
   rbg::HBuf shard_host;                  // their host staging for host-memory collectives
   bool streamed = false;                 // rbg_bin_graph scored the pairs behind the copy
   uint64_t no_stream_S = 0;              // bit S: survivors outgrew the list when streamed
-  bool no_tune = false;                  // batch calls keep the tile shapes they have (serving)
   rbg::HBuf pin;                         // row maxima and pair count read back for calibration
   int64_t n_edges = 0;
   double b0 = 0.0, sim_cutoff = 0.0;

@@ -100,7 +100,7 @@ __global__ void k_onehot_fill(const uint8_t *__restrict__ codesA, int64_t n, int
 constexpr int kSelWarps = 8;
 constexpr int kSelBuf = 32 * kCapW;   // 512 keys per warp
 
-__global__ void __launch_bounds__(kSelWarps * 32)
+__global__ void __launch_bounds__(kSelWarps * 32, 4)
 k_dense_select(GraphArgs g, const int32_t *__restrict__ D, int64_t ldd, int64_t r0, int64_t nr) {
   __shared__ uint64_t sbuf[kSelWarps][kSelBuf];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -132,19 +132,28 @@ k_dense_select(GraphArgs g, const int32_t *__restrict__ D, int64_t ldd, int64_t 
   unsigned n_cmp = 0;
   int fill = 0;
   // lane takes 4 consecutive contigs per step (16-byte count loads; ldd and the
-  // row starts are multiples of 4 counts)
-  for (int64_t j0 = 0; j0 < n; j0 += 128) {
-    const int64_t jb = j0 + 4 * lane;
-    int4 c4 = make_int4(0, 0, 0, 0);
-    uint32_t nz4 = 0;
+  // row starts are multiples of 4 counts); the next step's loads are issued
+  // before this step's keys are ranked
+  auto load = [&](int64_t jb, int4 &c4, uint32_t &nz4) {
+    c4 = make_int4(0, 0, 0, 0);
+    nz4 = 0;
     if (jb < n) {
-      c4 = *reinterpret_cast<const int4 *>(row + jb);
+      c4 = __ldcs(reinterpret_cast<const int4 *>(row + jb));   // read once: stream past L1/L2
       if (jb + 4 <= n && nz_words) {
-        nz4 = *reinterpret_cast<const uint32_t *>(g.anynz + jb);
+        nz4 = __ldg(reinterpret_cast<const uint32_t *>(g.anynz + jb));
       } else {
         for (int t = 0; t < 4 && jb + t < n; ++t) nz4 |= (uint32_t)g.anynz[jb + t] << (8 * t);
       }
     }
+  };
+  int4 nxt_c;
+  uint32_t nxt_nz;
+  load(4 * lane, nxt_c, nxt_nz);
+  for (int64_t j0 = 0; j0 < n; j0 += 128) {
+    const int64_t jb = j0 + 4 * lane;
+    const int4 c4 = nxt_c;
+    const uint32_t nz4 = nxt_nz;
+    load(jb + 128, nxt_c, nxt_nz);
     const uint32_t cv[4] = {(uint32_t)c4.x, (uint32_t)c4.y, (uint32_t)c4.z, (uint32_t)c4.w};
 #pragma unroll
     for (int t = 0; t < 4; ++t) {

@@ -157,8 +157,6 @@ int rbg_server_create(const rbg_server_config *cfg, const rbg_params *defaults,
       delete s;
       return rc;
     }
-    // no tuning runs on the request path (RBG_SERVE_TUNE=1: it does)
-    c->no_tune = getenv("RBG_SERVE_TUNE") == nullptr;
     s->ctxs.push_back(c);
   }
   for (int w = 0; w < s->cfg.workers; ++w) s->workers.emplace_back([s, w] { s->worker_loop(w); });

@@ -95,6 +95,19 @@ def test_batch_equals_alone(gpu_ctx, mix):
     for i, (g, w) in enumerate(zip(again, want)):
         _same(g, w, i)
     assert st2["graph_launches"] == 3
+    # a call's graphs share one pinned block: graphs kept while the others are
+    # freed stay intact through later calls
+    keep = {i: again[i] for i in range(0, len(again), 2)}
+    del again, got
+    third, _ = gpu_ctx.bin_batch(ent)
+    fourth, _ = gpu_ctx.bin_batch(ent)
+    for i, g in keep.items():
+        _same(g, want[i], i)
+    for i, (g, w) in enumerate(zip(third, want)):
+        _same(g, w, i)
+    del third
+    for i, (g, w) in enumerate(zip(fourth, want)):
+        _same(g, w, i)
 
 
 def test_batch_order_and_subsets(gpu_ctx, mix):
