@@ -383,7 +383,7 @@ k_allpairs(GraphArgs g, uint64_t *gbuf, int32_t *gcnt, int cap, int P) {
 // pruned exactly as the reference prunes it.  The rest are checked one per
 // lane: FP32 chain with its own band, then the AVX-512 order inside the band.
 constexpr float kTcDelta = 2.5e-3f;
-constexpr int kTCT = 32;          // columns per staged tile
+constexpr int kTCT = 16;          // columns per staged tile
 constexpr int kCQ = 512;          // check-queue ring entries per warp
 
 __device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0,
