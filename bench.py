@@ -43,9 +43,9 @@ WORKLOAD = dict(workload="binning-scale assembly: 100 genomes, 50000 contigs, S=
 METRIC = "contig-pairs scored/s"
 # DRAM bytes (read + write) of the symmetric all-pairs kernel per unordered
 # pair, from the ncu capture of the 30,000-contig case
-# (profiles/k_allpairs_tc_sym_fused30k.md: 61.8 MB over 4.5e8 pairs), scaled to
+# (profiles/k_allpairs_tc_sym_fused30k.md: 65.3 MB over 4.5e8 pairs), scaled to
 # a launch by its n(n-1)/2 pairs.
-ALLPAIRS_TRAFFIC_PER_PAIR = 0.137
+ALLPAIRS_TRAFFIC_PER_PAIR = 0.145
 UNIT = "pairs/s"
 
 

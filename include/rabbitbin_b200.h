@@ -211,8 +211,11 @@ typedef struct rbg_assembly {
 } rbg_assembly;
 
 typedef struct rbg_batch_stats {
-  float stage_ms;              /* input copies, the sketch behind them (device) */
-  float graph_ms;              /* depth rows, b0, all-pairs, merge (device)     */
+  float stage_ms;              /* input copies with, behind them, each run of
+                                  assemblies' sketch, depth rows, b0, all-pairs
+                                  and dense GEMMs (device)                      */
+  float graph_ms;              /* row top-K of the symmetric pass, and the
+                                  resident rerun if its pair list overflowed    */
   float calib_ms;              /* cutoff calibration of every assembly (host)   */
   float emit_ms;               /* edges + weights + copies back (device)        */
   float total_ms;              /* the whole call (host clock)                   */

@@ -1,19 +1,20 @@
 // Batch engine: many assemblies sketched and graphed together.
 //
 // The assemblies of a call share one set of device buffers (rows of all
-// assemblies laid end to end) and one pass of each stage:
+// assemblies laid end to end).  In runs of batch positions of about equal
+// bases, each run behind its input copy on a second stream:
 //   pack -> count (per k / GC-norm group) -> register minimum (per sketch-table
-//   group), in runs of batch positions behind their input copies on a second
-//   stream -> unit rows + column norms -> b0 and similarity
-//   tables (on the device) -> persistent all-pairs kernels pulling
-//   (assembly, row block, slice group) items from a device counter, one per
-//   variant (dense / tensor-core KS) -> top-K merge
-// then one host round trip for the rand()-driven calibration of every
-// assembly (the maxima and b0 come back together), then neighbour lists, edge
-// counts and the batch-wide scan, one more round trip for the edge total, and
-// edge emission + weights.  The device part of each of the three segments
-// after the sketch is captured into a CUDA graph; an instantiated graph is
-// updated in place when the next batch has the same launch topology.
+//   group) -> unit rows + column norms -> b0 and similarity tables (on the
+//   device) -> persistent all-pairs kernels pulling (assembly, row block,
+//   slice group) items from a device counter, one per variant (dense /
+//   tensor-core KS) -> dense assemblies' one-hot GEMMs
+// then the row top-K of the symmetric pass over the whole batch, one host
+// round trip for the rand()-driven calibration of every assembly (the maxima
+// and b0 come back together), then neighbour lists, edge counts and the
+// batch-wide scan, one more round trip for the edge total, and edge emission
+// + weights.  The device part of each of the three segments after the runs
+// is captured into a CUDA graph; an instantiated graph is updated in place
+// when the next batch has the same launch topology.
 //
 // Each assembly's result equals rbg_bin_graph on that assembly alone: the
 // kernels are the single-assembly kernels behind a descriptor lookup, and
@@ -328,12 +329,18 @@ void ensure_buffers(BatchBufs &B, const BatchPlan &L, int nb) {
   B.desc.ensure(nb * sizeof(BatchAsm));
   B.row0s.ensure((nb + 1) * sizeof(int64_t));
   B.pair0s.ensure((nb + 1) * sizeof(int64_t));
-  B.lists.ensure(4 * (nb + 1) * sizeof(int32_t));
-  B.item0s.ensure(4 * (nb + 1) * sizeof(int64_t));
-  B.queues.ensure(4 * sizeof(unsigned long long));
+  // work lists and queue counters: the whole batch, then one set per run
+  B.lists.ensure((1 + kChunks) * 4 * (nb + 1) * sizeof(int32_t));
+  B.item0s.ensure((1 + kChunks) * 4 * (nb + 1) * sizeof(int64_t));
+  B.queues.ensure((1 + kChunks) * 4 * sizeof(unsigned long long));
   B.e_from.ensure(4); B.e_to.ensure(4); B.e_scomp.ensure(4); B.e_score.ensure(4);
   if (L.sym_rows > 0) {
-    B.sym_cap = std::max<uint64_t>(B.sym_cap, std::max<uint64_t>(1u << 16, (uint64_t)L.sym_rows * 256));
+    // RBG_PAIR_CAP: a small first list, to exercise the overflow path
+    const char *pc = getenv("RBG_PAIR_CAP");
+    if (pc && B.sym_cap == 0) B.sym_cap = std::max<uint64_t>(1024, strtoull(pc, nullptr, 10));
+    else
+      B.sym_cap = std::max<uint64_t>(B.sym_cap,
+                                     std::max<uint64_t>(1u << 16, (uint64_t)L.sym_rows * 256));
     B.sym_pairs.ensure(B.sym_cap * sizeof(uint4));
     B.sym_keys.ensure(2 * B.sym_cap * sizeof(uint64_t));
     B.sym_rowcnt.ensure(rows1 * sizeof(int32_t));
@@ -534,6 +541,55 @@ int launch_graph_stage(rbg_ctx *c, BatchBufs &B, const BatchPlan &L, const Lists
   return launches;
 }
 
+// Graph stage of the batch positions [bb, be) (rows [r0, r1), sampled pairs
+// [p0, p1)) on work lists Wr whose device copies start at `lists` / `item0s`,
+// with queue counters `next` (zeroed by the caller): depth rows, column norms,
+// b0, the all-pairs passes and the dense merge.  The row top-K of the
+// symmetric pass follows once every run is in.
+int launch_graph_run(rbg_ctx *c, BatchBufs &B, const BatchPlan &L, const Lists &Wr, int nb,
+                     int bb, int be, const int32_t *lists, const int64_t *item0s,
+                     unsigned long long *next) {
+  const BatchAsm *dD = B.desc.as<BatchAsm>();
+  if (bb >= be) return 0;
+  const AsmPlan &f = L.at(bb), &l = L.at(be - 1);
+  const int64_t r0 = f.row0, r1 = l.row0 + l.n, p0 = f.pair0, p1 = l.pair0 + l.np;
+  int launches = 0;
+  launch_unit_rows_batch(dD, B.row0s.as<int64_t>(), nb, r1, c->stream, r0);
+  launch_colnorm_batch(dD + bb, be - bb, L.max_s, c->stream);
+  launch_b0_batch_range(dD, B.pair0s.as<int64_t>(), nb, p0, p1, B.pairs.as<int32_t>(),
+                        B.pair_cnt.as<uint32_t>(), L.max_m, bb, be, c->stream);
+  launches += (r1 > r0 ? 1 : 0) + (L.max_s > 1 ? 2 : 0) + (p1 > p0 ? 2 : 1);
+  const SymOut o = L.sym_rows > 0 ? sym_out(B) : SymOut{};
+  for (int v = 0; v < 4; ++v) {
+    if (Wr.list[v].empty()) continue;
+    launch_allpairs_batch(dD, kVariants[v], lists + v * (nb + 1), item0s + v * (nb + 1),
+                          (int)Wr.list[v].size(), Wr.item0[v].back(), Wr.smem[v], next + v, o,
+                          c->stream);
+    ++launches;
+  }
+  if (!Wr.list[0].empty()) {
+    launch_merge_batch(dD, B.row0s.as<int64_t>(), nb, r1, c->stream, r0);
+    ++launches;
+  }
+  return launches;
+}
+
+// The work lists of batch positions [bb, be) only.
+Lists sub_lists(const Lists &W, int bb, int be) {
+  Lists R;
+  for (int v = 0; v < 4; ++v) {
+    R.smem[v] = W.smem[v];
+    for (size_t k = 0; k < W.list[v].size(); ++k) {
+      const int b = W.list[v][k];
+      if (b < bb || b >= be) continue;
+      if (R.item0[v].empty()) R.item0[v].push_back(0);
+      R.list[v].push_back(b);
+      R.item0[v].push_back(R.item0[v].back() + (W.item0[v][k + 1] - W.item0[v][k]));
+    }
+  }
+  return R;
+}
+
 // Device descriptors of the batch positions and the per-variant work lists.
 void build_items(BatchBufs &B, const BatchPlan &L, int nb, std::vector<BatchAsm> &D, Lists &W) {
   D.assign(nb, BatchAsm());
@@ -647,11 +703,30 @@ void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
   const bool autotune = getenv("RBG_NO_AUTOTUNE") == nullptr;
   for (int v = 0; v < 4; ++v) stats.items += W.item0[v].empty() ? 0 : W.item0[v].back();
 
-  // pinned staging: global offsets, b0 pairs, descriptors, index arrays
+  // Batch positions in up to kChunks runs of about equal bases: the copy
+  // stream brings in run r's sequences and depths while the main stream
+  // sketches and graphs run r - 1.
+  std::vector<int> runcut{0};
+  {
+    const int64_t per = std::max<int64_t>(L.bases / kChunks, 1);
+    for (int b = 0; b < nb; ++b) {
+      const AsmPlan &a = L.at(b);
+      if (b + 1 < nb && (int)runcut.size() < kChunks && a.base0 + a.nbases >= per * (int64_t)runcut.size())
+        runcut.push_back(b + 1);
+    }
+    runcut.push_back(nb);
+  }
+  const int nruns = (int)runcut.size() - 1;
+  std::vector<Lists> Wr(nruns);
+  for (int r = 0; r < nruns; ++r) Wr[r] = sub_lists(W, runcut[r], runcut[r + 1]);
+
+  // pinned staging: global offsets, b0 pairs, descriptors, index arrays (the
+  // work lists of the whole batch, then of each run)
   const size_t off_bytes = (rows + 1) * sizeof(int64_t);
   const size_t pair_bytes = (size_t)L.npairs * 2 * sizeof(int32_t);
   const size_t desc_bytes = (size_t)nb * sizeof(BatchAsm);
-  const size_t idx_bytes = 2 * (nb + 1) * sizeof(int64_t) + 4 * (nb + 1) * (sizeof(int32_t) + sizeof(int64_t));
+  const size_t nlist = (size_t)(1 + nruns) * 4 * (nb + 1);
+  const size_t idx_bytes = 2 * (nb + 1) * sizeof(int64_t) + nlist * (sizeof(int32_t) + sizeof(int64_t));
   B.hstage.ensure(up256(off_bytes) + up256(pair_bytes) + up256(desc_bytes) + up256(idx_bytes));
   char *hs = B.hstage.as<char>();
   int64_t *h_off = (int64_t *)hs;
@@ -660,7 +735,7 @@ void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
   int64_t *h_row0s = (int64_t *)(hs + up256(off_bytes) + up256(pair_bytes) + up256(desc_bytes));
   int64_t *h_pair0s = h_row0s + (nb + 1);
   int32_t *h_lists = (int32_t *)(h_pair0s + (nb + 1));
-  int64_t *h_item0s = (int64_t *)(h_lists + 4 * (nb + 1));
+  int64_t *h_item0s = (int64_t *)(h_lists + nlist);
   for (int b = 0; b < nb; ++b) {
     const AsmPlan &a = L.at(b);
     for (int64_t q = 0; q < a.n; ++q) h_off[a.row0 + q] = a.base0 + a.in->offsets[q];
@@ -672,9 +747,15 @@ void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
   h_row0s[nb] = rows;
   h_pair0s[nb] = L.npairs;
   std::memcpy(h_desc, D.data(), desc_bytes);
-  for (int v = 0; v < 4; ++v) {
-    std::copy(W.list[v].begin(), W.list[v].end(), h_lists + v * (nb + 1));
-    std::copy(W.item0[v].begin(), W.item0[v].end(), h_item0s + v * (nb + 1));
+  std::fill(h_lists, h_lists + nlist, 0);
+  std::fill(h_item0s, h_item0s + nlist, 0);
+  for (int r = -1; r < nruns; ++r) {
+    const Lists &X = r < 0 ? W : Wr[r];
+    const size_t base = (size_t)(r + 1) * 4 * (nb + 1);
+    for (int v = 0; v < 4; ++v) {
+      std::copy(X.list[v].begin(), X.list[v].end(), h_lists + base + v * (nb + 1));
+      std::copy(X.item0[v].begin(), X.item0[v].end(), h_item0s + base + v * (nb + 1));
+    }
   }
 
   // ── inputs to the device, sketched behind the copies ────────────────────
@@ -685,44 +766,66 @@ void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
   CK(cudaMemcpyAsync(B.desc.p, h_desc, desc_bytes, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(B.row0s.p, h_row0s, (nb + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(B.pair0s.p, h_pair0s, (nb + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
-  CK(cudaMemcpyAsync(B.lists.p, h_lists, 4 * (nb + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
-  CK(cudaMemcpyAsync(B.item0s.p, h_item0s, 4 * (nb + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
-  // Batch positions in up to kChunks runs of about equal bases: the copy
-  // stream brings in run r's sequences and depths while the main stream
-  // sketches run r - 1.
+  CK(cudaMemcpyAsync(B.lists.p, h_lists, nlist * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(B.item0s.p, h_item0s, nlist * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
+  // graph-stage accumulators, zeroed once for all runs
+  CK(cudaMemsetAsync(B.colacc.p, 0, L.acc * sizeof(double), c->stream));
+  CK(cudaMemsetAsync(B.maxc_cand.p, 0, rows1 * sizeof(uint32_t), c->stream));
+  CK(cudaMemsetAsync(B.maxc_all.p, 0, rows1 * sizeof(uint32_t), c->stream));
+  CK(cudaMemsetAsync(B.stats.p, 0, 2 * sizeof(unsigned long long), c->stream));
+  CK(cudaMemsetAsync(B.queues.p, 0, (size_t)(1 + nruns) * 4 * sizeof(unsigned long long),
+                     c->stream));
+  if (L.sym_rows > 0) {
+    CK(cudaMemsetAsync(B.sym_rowcnt.p, 0, rows1 * sizeof(int32_t), c->stream));
+    CK(cudaMemsetAsync(B.sym_np.p, 0, sizeof(unsigned long long), c->stream));
+  }
   int launches = 0;
   {
-    std::vector<int> cut{0};
-    const int64_t per = std::max<int64_t>(L.bases / kChunks, 1);
-    for (int b = 0; b < nb; ++b) {
-      const AsmPlan &a = L.at(b);
-      if (b + 1 < nb && (int)cut.size() < kChunks && a.base0 + a.nbases >= per * (int64_t)cut.size())
-        cut.push_back(b + 1);
-    }
-    cut.push_back(nb);
     CK(cudaEventRecord(c->ev_cin, c->stream));             // earlier work on the buffers is done
     CK(cudaStreamWaitEvent(c->copy, c->ev_cin, 0));
     const size_t abytes = (size_t)((L.bases + 15) / 16) * 16 + 16;
-    for (size_t r = 0; r + 1 < cut.size(); ++r) {
-      for (int b = cut[r]; b < cut[r + 1]; ++b) {
+    // Every copy is queued first: the host waits inside the dense GEMMs below,
+    // and the copies must not wait for it.  The depth rows go through pinned
+    // staging, since a copy from pageable memory would hold the host until the
+    // copies queued before it are done.
+    B.hdepth.ensure(std::max<int64_t>(L.dep, 1) * sizeof(float));
+    for (size_t r = 0; r + 1 < runcut.size(); ++r) {
+      for (int b = runcut[r]; b < runcut[r + 1]; ++b) {
         const AsmPlan &a = L.at(b);
         if (a.nbases)
           CK(cudaMemcpyAsync(B.ascii.as<char>() + a.base0, a.in->seqcat, (size_t)a.nbases,
                              cudaMemcpyHostToDevice, c->copy));
-        if (a.n && a.S)
-          CK(cudaMemcpyAsync(B.depth.as<float>() + a.dep0, a.in->depth,
-                             (size_t)a.n * a.S * sizeof(float), cudaMemcpyHostToDevice, c->copy));
+        if (a.n && a.S) {
+          float *hd = B.hdepth.as<float>() + a.dep0;
+          std::memcpy(hd, a.in->depth, (size_t)a.n * a.S * sizeof(float));
+          CK(cudaMemcpyAsync(B.depth.as<float>() + a.dep0, hd, (size_t)a.n * a.S * sizeof(float),
+                             cudaMemcpyHostToDevice, c->copy));
+        }
       }
-      if (r + 2 == cut.size())
+      if (r + 2 == runcut.size())
         CK(cudaMemsetAsync(B.ascii.as<char>() + L.bases, 0, abytes - (size_t)L.bases, c->copy));
       CK(cudaEventRecord(c->ev_chunk[r], c->copy));
+    }
+    for (size_t r = 0; r + 1 < runcut.size(); ++r) {
       CK(cudaStreamWaitEvent(c->stream, c->ev_chunk[r], 0));
-      launches += launch_sketch_groups(c, B, L, tab, cut[r], cut[r + 1]);
+      launches += launch_sketch_groups(c, B, L, tab, runcut[r], runcut[r + 1]);
+      const size_t base = (size_t)(r + 1) * 4 * (nb + 1);
+      launches += launch_graph_run(c, B, L, Wr[r], nb, runcut[r], runcut[r + 1],
+                                   B.lists.as<int32_t>() + base, B.item0s.as<int64_t>() + base,
+                                   B.queues.as<unsigned long long>() + (size_t)(r + 1) * 4);
+      // dense assemblies of the run: one-hot GEMM and row scan each, on the
+      // b0 and similarity tables just computed
+      for (int b = runcut[r]; b < runcut[r + 1]; ++b)
+        if (L.at(b).gemm && L.at(b).n > 0) {
+          dense_allpairs_gemm(c, D[b].g);
+          launches += 5;
+        }
     }
   }
+  CK(cudaGetLastError());
   CK(cudaEventRecord(ev1, c->stream));
 
-  // ── segment 1: sketch, depth rows, b0, all-pairs, merge ────────────────
+  // ── segment 1: row top-K of the symmetric pass, maxima and b0 to the host ──
   const size_t mx_bytes = up256(2 * rows1 * sizeof(uint32_t));
   const size_t e0_bytes = up256((nb + 1) * sizeof(int64_t));
   B.hout.ensure(mx_bytes + up256(nb * sizeof(float)) + e0_bytes + sizeof(unsigned long long));
@@ -732,10 +835,18 @@ void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
   unsigned long long *h_np =
       (unsigned long long *)(B.hout.as<char>() + mx_bytes + up256(nb * sizeof(float)) + e0_bytes);
   // The symmetric pass reports how many pairs it admitted; a pass whose pairs
-  // did not fit the list runs again with a larger one.
-  for (;;) {
-    captured(c, 0, use_graph, stats.graph_launches, [&] {
-      launches += launch_graph_stage(c, B, L, W, nb);
+  // did not fit the list runs again, resident, with a larger one.
+  bool reran = false;
+  for (bool first = true;; first = false) {
+    reran = !first;
+    captured(c, 0, use_graph && first, stats.graph_launches, [&] {
+      if (!first) {
+        launches += launch_graph_stage(c, B, L, W, nb);
+      } else if (L.sym_rows > 0) {
+        launch_rows_topk_batch(B.desc.as<BatchAsm>(), B.row0s.as<int64_t>(), nb, rows, sym_out(B),
+                               B.sym_rowoff.as<int64_t>(), B.sym_keys.as<uint64_t>(), c->stream);
+        launches += 3;
+      }
       if (rows) {
         CK(cudaMemcpyAsync(h_maxc, B.maxc_cand.p, rows * sizeof(uint32_t), cudaMemcpyDeviceToHost,
                            c->stream));
@@ -754,9 +865,9 @@ void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
     B.sym_pairs.ensure(B.sym_cap * sizeof(uint4));
     B.sym_keys.ensure(2 * B.sym_cap * sizeof(uint64_t));
   }
-  // dense assemblies: one-hot GEMM and row scan each (after the device b0 and
-  // similarity tables of segment 1), then their rows' maxima read again
-  {
+  // a resident rerun cleared every row's maxima: the dense assemblies run
+  // their GEMMs again, then the maxima are read again
+  if (reran) {
     bool any = false;
     for (int b = 0; b < nb; ++b)
       if (L.at(b).gemm && L.at(b).n > 0) {

@@ -147,7 +147,7 @@ struct BatchBufs {
   // persistent launch
   std::map<std::tuple<int, int, int>, double> tune;
   cudaEvent_t tev[8] = {};
-  HBuf hstage, hout, hedge;
+  HBuf hstage, hout, hedge, hdepth;     // hdepth: depth rows staged pinned for async copies
   std::map<std::tuple<int, int, uint64_t, int, int>, std::unique_ptr<Tables>> tables;
   void release() {
     DBuf *all[] = {&ascii, &offsets, &depth, &packed, &nmask, &winv, &ecnt, &codesA, &codesB,
@@ -160,6 +160,7 @@ struct BatchBufs {
     hstage.release();
     hout.release();
     hedge.release();
+    hdepth.release();
     sym_cap = 0;
     tune.clear();
     for (auto &e : tev)

@@ -768,10 +768,10 @@ k_merge_topk(GraphArgs g, const uint64_t *gbuf, const int32_t *gcnt, int cap, in
 }
 
 __global__ void __launch_bounds__(kMergeWarps * 32)
-k_merge_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows) {
+k_merge_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t r_begin, int64_t rows) {
   __shared__ uint64_t mk[kMergeWarps][kMergeBuf];
   const int wib = threadIdx.x >> 5;
-  const int64_t r = (int64_t)blockIdx.x * kMergeWarps + wib;
+  const int64_t r = r_begin + (int64_t)blockIdx.x * kMergeWarps + wib;
   if (r >= rows) return;
   int lo = 0, hi = nb - 1;
   while (lo < hi) {
@@ -947,15 +947,14 @@ void launch_allpairs(const GraphArgs &g, uint64_t *gbuf, int32_t *gcnt, cudaStre
   const size_t smem = allpairs_batch_smem(v, g.mpad, g.Su);
 #define RBG_TC(KS, SM)                                                                        \
   do {                                                                                        \
-    cudaFuncSetAttribute(k_allpairs_tc<KS, SM>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
-                         (int)smem);                                                          \
+    smem_cap_max((const void *)k_allpairs_tc<KS, SM>);                                        \
     k_allpairs_tc<KS, SM><<<grid, kWarps * 32, smem, s>>>(g, gbuf, gcnt, cap, P, lo, hi, lo16); \
   } while (0)
   if (v == 1) RBG_TC(1, 16);
   else if (v == 2) RBG_TC(2, 32);
   else if (v == 4) RBG_TC(4, 64);
   else {
-    cudaFuncSetAttribute(k_allpairs<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    smem_cap_max((const void *)k_allpairs<4>);
     k_allpairs<4><<<grid, kWarps * 32, smem, s>>>(g, gbuf, gcnt, cap, P);
   }
 #undef RBG_TC
@@ -974,8 +973,7 @@ void launch_allpairs_sym(const GraphArgs &g, const SymOut &o, cudaStream_t s) {
   const size_t smem = tc_smem(v, g.mpad, g.Su);
 #define RBG_TS(KS, SM)                                                                        \
   do {                                                                                        \
-    cudaFuncSetAttribute(k_allpairs_tc_sym<KS, SM>,                                           \
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);             \
+    smem_cap_max((const void *)k_allpairs_tc_sym<KS, SM>);                                    \
     k_allpairs_tc_sym<KS, SM><<<grid, kWarps * 32, smem, s>>>(g, P, lo, hi, lo16, o);         \
   } while (0)
   if (v == 1) RBG_TS(1, 16);
@@ -999,8 +997,7 @@ void launch_allpairs_sym_window(const GraphArgs &g, const SymOut &o, int64_t cb,
   const size_t smem = tc_smem(v, g.mpad, g.Su);
 #define RBG_TW(KS, SM)                                                                        \
   do {                                                                                        \
-    cudaFuncSetAttribute(k_allpairs_tc_win<KS, SM>,                                           \
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);             \
+    smem_cap_max((const void *)k_allpairs_tc_win<KS, SM>);                                    \
     k_allpairs_tc_win<KS, SM><<<grid, kWarps * 32, smem, s>>>(g, P, lo, hi, lo16, o, cb, ce); \
   } while (0)
   if (v == 1) RBG_TW(1, 16);
@@ -1054,8 +1051,7 @@ void launch_allpairs_batch(const BatchAsm *B, int variant, const int32_t *list,
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
 #define RBG_PB(KS, SM)                                                                         \
   do {                                                                                         \
-    cudaFuncSetAttribute(k_allpairs_batch<KS, SM>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                         (int)smem);                                                           \
+    smem_cap_max((const void *)k_allpairs_batch<KS, SM>);                                      \
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_allpairs_batch<KS, SM>,           \
                                                   kWarps * 32, smem);                          \
     const int64_t grid = std::min<int64_t>(items, (int64_t)std::max(per_sm, 1) * sms);         \
@@ -1070,10 +1066,10 @@ void launch_allpairs_batch(const BatchAsm *B, int variant, const int32_t *list,
 }
 
 void launch_merge_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows,
-                        cudaStream_t s) {
-  if (rows == 0) return;
-  k_merge_batch<<<(unsigned)((rows + kMergeWarps - 1) / kMergeWarps), kMergeWarps * 32, 0, s>>>(
-      B, row0s, nb, rows);
+                        cudaStream_t s, int64_t r_begin) {
+  if (rows <= r_begin) return;
+  k_merge_batch<<<(unsigned)((rows - r_begin + kMergeWarps - 1) / kMergeWarps), kMergeWarps * 32,
+                  0, s>>>(B, row0s, nb, r_begin, rows);
 }
 
 }  // namespace rbg

@@ -85,8 +85,9 @@ __global__ void k_unit_rows(GraphArgs g) {
   unit_row(g, r);
 }
 
-__global__ void k_unit_rows_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows) {
-  const int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+__global__ void k_unit_rows_batch(const BatchAsm *B, const int64_t *row0s, int nb,
+                                  int64_t r_begin, int64_t rows) {
+  const int64_t r = r_begin + (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   if (r >= rows) return;
   const int a = find_asm(row0s, nb, r);
   unit_row(B[a].g, r - B[a].row0);
@@ -210,9 +211,9 @@ __global__ void k_pair_counts(const uint8_t *__restrict__ A, const uint8_t *__re
 // histogram of the counts (the float match fractions sort as the counts do),
 // then the similarity table of pmh_sv_from_count (:1297-1305).
 __global__ void k_pair_counts_batch(const BatchAsm *B, const int64_t *pair0s, int nb,
-                                    int64_t npairs, const int32_t *__restrict__ pairs,
-                                    uint32_t *__restrict__ out) {
-  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+                                    int64_t p_begin, int64_t npairs,
+                                    const int32_t *__restrict__ pairs, uint32_t *__restrict__ out) {
+  const int64_t p = p_begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npairs) return;
   const int a = find_asm(pair0s, nb, p);
   const GraphArgs &g = B[a].g;
@@ -630,24 +631,32 @@ void launch_edge_weights(const WeightArgs &w, cudaStream_t s) {
 }
 
 void launch_unit_rows_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows,
-                            cudaStream_t s) {
-  if (rows == 0) return;
-  k_unit_rows_batch<<<(unsigned)((rows + 7) / 8), 256, 0, s>>>(B, row0s, nb, rows);
+                            cudaStream_t s, int64_t r_begin) {
+  if (rows <= r_begin) return;
+  k_unit_rows_batch<<<(unsigned)((rows - r_begin + 7) / 8), 256, 0, s>>>(B, row0s, nb, r_begin,
+                                                                         rows);
 }
 
 void launch_colnorm_batch(const BatchAsm *B, int nb, int max_s, cudaStream_t s) {
-  if (nb == 0 || max_s <= 1) return;
+  if (nb <= 0 || max_s <= 1) return;
   k_colsum_fast_batch<<<dim3(64, (unsigned)nb), 256, 0, s>>>(B);
   k_colnorm_batch<<<(unsigned)nb, 256, 0, s>>>(B);
 }
 
 void launch_b0_batch(const BatchAsm *B, const int64_t *pair0s, int nb, int64_t npairs,
                      const int32_t *pairs, uint32_t *counts, int max_m, cudaStream_t s) {
-  if (nb == 0) return;
-  if (npairs > 0)
-    k_pair_counts_batch<<<(unsigned)((npairs + 127) / 128), 128, 0, s>>>(B, pair0s, nb, npairs,
-                                                                          pairs, counts);
-  k_b0_batch<<<(unsigned)nb, 256, (size_t)(max_m + 1) * sizeof(int), s>>>(B, counts);
+  launch_b0_batch_range(B, pair0s, nb, 0, npairs, pairs, counts, max_m, 0, nb, s);
+}
+
+void launch_b0_batch_range(const BatchAsm *B, const int64_t *pair0s, int nb, int64_t p_begin,
+                           int64_t p_end, const int32_t *pairs, uint32_t *counts, int max_m,
+                           int b_begin, int b_end, cudaStream_t s) {
+  if (b_end <= b_begin) return;
+  if (p_end > p_begin)
+    k_pair_counts_batch<<<(unsigned)((p_end - p_begin + 127) / 128), 128, 0, s>>>(
+        B, pair0s, nb, p_begin, p_end, pairs, counts);
+  k_b0_batch<<<(unsigned)(b_end - b_begin), 256, (size_t)(max_m + 1) * sizeof(int), s>>>(
+      B + b_begin, counts);
 }
 
 void launch_emit_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows, int max_k,

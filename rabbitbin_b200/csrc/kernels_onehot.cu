@@ -96,7 +96,8 @@ __global__ void k_onehot_fill(const uint8_t *__restrict__ codesA, int64_t n, int
 // row: top-K keys (similarity bits << 32 | ~j) of the candidates above the
 // admission floor, kept through a 512-key shared buffer and the register radix
 // select; maxima over all other j and over the candidates (anynz); the number
-// of pairs compared.
+// of pairs compared.  A step whose counts are all below the current threshold
+// (the common case) takes one vote, not four.
 constexpr int kSelWarps = 8;
 constexpr int kSelBuf = 32 * kCapW;   // 512 keys per warp
 
@@ -129,7 +130,6 @@ k_dense_select(GraphArgs g, const int32_t *__restrict__ D, int64_t ldd, int64_t 
   // anynz of a batch assembly starts at its first row: 4-byte loads only when aligned
   const bool nz_words = (((uintptr_t)g.anynz) & 3u) == 0;
   uint32_t mx_a = 0, mx_c = 0;
-  unsigned n_cmp = 0;
   int fill = 0;
   // lane takes 4 consecutive contigs per step (16-byte count loads; ldd and the
   // row starts are multiples of 4 counts); the next step's loads are issued
@@ -154,18 +154,27 @@ k_dense_select(GraphArgs g, const int32_t *__restrict__ D, int64_t ldd, int64_t 
     const int4 c4 = nxt_c;
     const uint32_t nz4 = nxt_nz;
     load(jb + 128, nxt_c, nxt_nz);
-    const uint32_t cv[4] = {(uint32_t)c4.x, (uint32_t)c4.y, (uint32_t)c4.z, (uint32_t)c4.w};
+    uint32_t cv[4] = {(uint32_t)c4.x, (uint32_t)c4.y, (uint32_t)c4.z, (uint32_t)c4.w};
+    // the diagonal and the padding past n count as 0 (counts are >= 0, so the
+    // maxima are those over the other contigs) and are no candidates
+    unsigned cm = 0;
+    bool may = false;
+    const uint32_t thc = (uint32_t)(thr >> 32);   // a key passes only from this count on
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
       const int64_t j = jb + t;
-      const bool other = j < n && j != i;
-      const uint32_t c = cv[t];
-      const bool cand = other && (nz_i | ((nz4 >> (8 * t)) & 0xFFu));
-      if (other && c > mx_a) mx_a = c;
-      if (cand && c > mx_c) mx_c = c;
-      n_cmp += other;
-      const uint64_t key = ((uint64_t)c << 32) | (uint64_t)(~(uint32_t)j);
-      const bool adm = cand && key > thr;
+      if (j >= n || j == i) cv[t] = 0;
+      const bool cand = j < n && j != i && (nz_i | ((nz4 >> (8 * t)) & 0xFFu));
+      cm |= (unsigned)cand << t;
+      mx_a = cv[t] > mx_a ? cv[t] : mx_a;
+      if (cand && cv[t] > mx_c) mx_c = cv[t];
+      may |= cand && cv[t] >= thc;
+    }
+    if (!__any_sync(FULL, may)) continue;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const uint64_t key = ((uint64_t)cv[t] << 32) | (uint64_t)(~(uint32_t)(jb + t));
+      const bool adm = ((cm >> t) & 1u) && key > thr;
       const unsigned mk = __ballot_sync(FULL, adm);
       if (mk) {
         if (adm) buf[fill + __popc(mk & ((1u << lane) - 1u))] = key;
@@ -188,12 +197,11 @@ k_dense_select(GraphArgs g, const int32_t *__restrict__ D, int64_t ldd, int64_t 
   }
   mx_a = __reduce_max_sync(FULL, mx_a);
   mx_c = __reduce_max_sync(FULL, mx_c);
-  n_cmp = __reduce_add_sync(FULL, n_cmp);
   if (lane == 0) {
     g.topk_cnt[i] = fill;
     g.maxcnt_all[i] = mx_a;
     g.maxcnt_cand[i] = mx_c;
-    if (g.stats) atomicAdd(g.stats + 1, (unsigned long long)n_cmp);
+    if (g.stats) atomicAdd(g.stats + 1, (unsigned long long)(n - 1));   // every other contig
   }
 }
 

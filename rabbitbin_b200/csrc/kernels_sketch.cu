@@ -5,6 +5,9 @@
 // the reference's (which has no contracted expression in build_pmh_winners).
 #include <algorithm>
 #include <cstdint>
+#include <mutex>
+#include <set>
+#include <utility>
 
 #include "rbg_internal.h"
 
@@ -490,10 +493,25 @@ void launch_count(const SketchArgs &a, cudaStream_t s) {
   k_count<<<(unsigned)grid, warps * 32, warps * 256 * sizeof(uint32_t), s>>>(a);
 }
 
+void smem_cap_max(const void *func) {
+  static std::mutex mu;
+  static std::set<std::pair<int, const void *>> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  if (!done.insert({dev, func}).second) return;
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaFuncAttributes fa;
+  if (cudaFuncGetAttributes(&fa, func) != cudaSuccess) return;   // the launch reports it
+  cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       optin - (int)fa.sharedSizeBytes);
+}
+
 void launch_minreduce(const SketchArgs &a, cudaStream_t s) {
   if (a.n == 0) return;
   const size_t smem = minreduce_smem(a.n_elems);
-  cudaFuncSetAttribute(k_minreduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  smem_cap_max((const void *)k_minreduce);
   const int64_t grid = (a.n + kMC - 1) / kMC;
   k_minreduce<<<(unsigned)grid, kMThreads, smem, s>>>(a);
 }

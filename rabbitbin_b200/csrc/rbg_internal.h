@@ -246,14 +246,26 @@ struct BatchAsm {
   uint32_t *sv_out = nullptr;          // out: [m+1] similarity float bits (== g.sv_bits)
 };
 
+// Raise a kernel's dynamic shared-memory cap once per device to the opt-in
+// maximum; every launch then passes its own size.  Setting the cap to each
+// launch's size instead races when host threads (serving workers, contexts on
+// other threads) launch the kernel with different sizes.
+void smem_cap_max(const void *func);
+
 // Index helper arrays ("starts") are ascending int64 with starts[nb] = total;
 // a batch kernel maps a global index x to the last assembly a with
-// starts[a] <= x.
+// starts[a] <= x.  Row-range launchers cover batch rows [r_begin, rows).
 void launch_unit_rows_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows,
-                            cudaStream_t s);
+                            cudaStream_t s, int64_t r_begin = 0);
+// Column norms of the assemblies B[0..nb) (pass B + first for a range).
 void launch_colnorm_batch(const BatchAsm *B, int nb, int max_s, cudaStream_t s);
 void launch_b0_batch(const BatchAsm *B, const int64_t *pair0s, int nb, int64_t npairs,
                      const int32_t *pairs, uint32_t *counts, int max_m, cudaStream_t s);
+// b0 and similarity tables of assemblies [b_begin, b_end), whose sampled
+// pairs are [p_begin, p_end).
+void launch_b0_batch_range(const BatchAsm *B, const int64_t *pair0s, int nb, int64_t p_begin,
+                           int64_t p_end, const int32_t *pairs, uint32_t *counts, int max_m,
+                           int b_begin, int b_end, cudaStream_t s);
 // Persistent all-pairs over the assemblies list[0..nv) of one variant: work
 // item x of assembly list[k] is x - item0s[k] (row block, slice group); CTAs
 // pull items from *next (zeroed by the caller).
@@ -264,7 +276,7 @@ void launch_allpairs_batch(const BatchAsm *B, int variant, const int32_t *list,
                            unsigned long long *next, const SymOut &o, cudaStream_t s);
 // Top-K of the dense assemblies' candidate buffers (others skipped).
 void launch_merge_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows,
-                        cudaStream_t s);
+                        cudaStream_t s, int64_t r_begin = 0);
 // Top-K of the tensor-core assemblies from the symmetric pass's pairs (dense
 // ones skipped); rowoff [rows+1] and keys [2 * o.cap] are scratch.
 void launch_rows_topk_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t rows,

@@ -178,3 +178,24 @@ def test_autotuner_keeps_results(tmp_path):
             assert np.array_equal(g1[k], w[k]) and np.array_equal(g2[k], w[k])
     tuned.close()
     fixed.close()
+
+
+def test_batch_pair_list_overflow(mix):
+    """A first pair list too small for the symmetric pass: the call runs the
+    graph stage again, resident, with a larger list; graphs unchanged."""
+    ent = _entries(mix)
+    ref = api.Context(0)
+    want = _alone(ref, ent)
+    ref.close()
+    os.environ["RBG_PAIR_CAP"] = "2048"
+    try:
+        small = api.Context(0)
+        got, _ = small.bin_batch(ent)
+        again, _ = small.bin_batch(ent)
+    finally:
+        del os.environ["RBG_PAIR_CAP"]
+    for i, (g, w) in enumerate(zip(got, want)):
+        _same(g, w, i)
+    for i, (g, w) in enumerate(zip(again, want)):
+        _same(g, w, i)
+    small.close()
