@@ -46,6 +46,8 @@ METRIC = "contig-pairs scored/s"
 # (profiles/k_allpairs_tc_sym_fused30k.md: 65.3 MB over 4.5e8 pairs), scaled to
 # a launch by its n(n-1)/2 pairs.
 ALLPAIRS_TRAFFIC_PER_PAIR = 0.145
+# Integer ALU pipe utilisation of the same kernel in the same capture.
+ALLPAIRS_ALU_PIPE_FRAC = 0.476
 UNIT = "pairs/s"
 
 
@@ -253,7 +255,11 @@ def _finish(args, ctx, asm, timings, last, ms, value, result_e2e, clk, world, ra
         "int_pipe": {"register_compares_per_s": last["pairs_compared"] * m / (ap_ms / 1000.0)
                      if ap_ms > 0 else 0.0,
                      "pairs_compared": last["pairs_compared"],
-                     "note": "ALU-pipe utilisation from ncu is in profiles/"},
+                     "alu_pipe_frac_ncu": ALLPAIRS_ALU_PIPE_FRAC,
+                     "note": "integer ALU pipe busy fraction of the symmetric all-pairs kernel "
+                             "(ncu sm__pipe_alu_cycles_active, 30,000-contig capture, "
+                             "profiles/k_allpairs_tc_sym_fused30k.md): the kernel's own "
+                             "bound; the tensor-core FLOPs above are only its prefilter"},
         "sketch": {"contigs_per_s": n / (sk_ms / 1000.0) if sk_ms > 0 else 0.0,
                    "ms": sk_ms, "bytes": sk_bytes,
                    "achieved_gbs": sk_bytes / (sk_ms / 1000.0) / 1e9 if sk_ms > 0 else 0.0,
@@ -616,7 +622,7 @@ def main():
     ap.add_argument("--rate", type=float, default=20.0, help="serve form: requests per second")
     ap.add_argument("--duration", type=float, default=10.0, help="serve form: seconds of arrivals")
     ap.add_argument("--pool", type=int, default=32, help="serve form: distinct assemblies")
-    ap.add_argument("--workers", type=int, default=2, help="serve form: concurrent batches")
+    ap.add_argument("--workers", type=int, default=1, help="serve form: concurrent batches")
     ap.add_argument("--shard", default="assemblies", choices=["assemblies", "rows"],
                     help="multi-GPU: one assembly per rank (weak scaling, default) or one "
                          "assembly split by rows over the ranks (strong scaling)")

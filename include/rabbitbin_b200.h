@@ -245,13 +245,16 @@ int rbg_bin_batch(rbg_ctx *ctx, const rbg_params *defaults, const rbg_assembly *
  * threads (one device context each) take every queued request that fits
  * their share of the HBM budget and run them as one batch (rbg_bin_batch),
  * so requests that arrive while others are on the GPU are folded into the
- * next launch, and the workers' batches overlap on the device.  Each result
- * equals rbg_bin_graph on that assembly alone. */
+ * next launch.  Inside a batch the copies of later requests overlap the work
+ * of earlier ones; with two or more workers the workers' batches also overlap
+ * on the device (one worker, the default, gave the lower latencies on a
+ * Poisson trace, since two batches sharing the GPU each take about twice as
+ * long).  Each result equals rbg_bin_graph on that assembly alone. */
 typedef struct rbg_server rbg_server;
 
 typedef struct rbg_server_config {
   int32_t device;              /* CUDA device                                   */
-  int32_t workers;             /* concurrent batches (contexts); 0 -> 2         */
+  int32_t workers;             /* concurrent batches (contexts); 0 -> 1         */
   int64_t hbm_budget;          /* bytes of device memory for request state;
                                   0 -> 150 GB, capped at the free memory        */
   int32_t max_batch;           /* assemblies folded into one launch; 0 -> 64    */

@@ -430,7 +430,7 @@ class Server:
     they arrive, wait for their graphs.  Arrays passed to submit are kept
     alive here until their request has been waited for."""
 
-    def __init__(self, device=0, workers=2, hbm_budget=0, max_batch=64, plain=False,
+    def __init__(self, device=0, workers=1, hbm_budget=0, max_batch=64, plain=False,
                  params=None, max_batch_pairs=0):
         self._L = lib()
         cfg = ServerConfig(device, workers, int(hbm_budget), max_batch, 1 if plain else 0,

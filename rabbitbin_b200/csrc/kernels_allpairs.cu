@@ -596,15 +596,16 @@ __device__ __forceinline__ void tc_item(const GraphArgs &g, uint64_t *gbuf, int3
       }
       n_pref += 8;
       if (__any_sync(FULL, mk != 0)) {
-        const int cntl = __popc(mk);
-        int incl = cntl;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-          const int v = __shfl_up_sync(FULL, incl, d);
-          if (lane >= d) incl += v;
-        }
-        const int total = __shfl_sync(FULL, incl, 31);
-        unsigned pos = tail + (unsigned)(incl - cntl);
+        // each lane's slot: the candidates of the lanes below it, summed from
+        // the bit planes of the per-lane counts (0..8: four votes) rather than
+        // by a chain of dependent shuffles
+        const unsigned cntl = (unsigned)__popc(mk), below = (1u << lane) - 1u;
+        const unsigned v0 = __ballot_sync(FULL, cntl & 1u), v1 = __ballot_sync(FULL, cntl & 2u);
+        const unsigned v2 = __ballot_sync(FULL, cntl & 4u), v3 = __ballot_sync(FULL, cntl & 8u);
+        const int excl = __popc(v0 & below) + 2 * __popc(v1 & below) + 4 * __popc(v2 & below) +
+                         8 * __popc(v3 & below);
+        const int total = __popc(v0) + 2 * __popc(v1) + 4 * __popc(v2) + 8 * __popc(v3);
+        unsigned pos = tail + (unsigned)excl;
         while (mk) {
           const int b = __ffs(mk) - 1;
           mk &= mk - 1;

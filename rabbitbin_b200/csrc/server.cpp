@@ -4,9 +4,10 @@
 // device context; it takes every queued request, oldest first, whose device
 // memory estimate fits into its share of the HBM budget (budget / workers)
 // and runs them as one batch through the batch engine, so requests that
-// arrive while others are on the GPU are folded into the next launch.  With
-// two or more workers the batches of different workers overlap on the device
-// (separate streams).  A worker's device buffers grow to its largest batch
+// arrive while others are on the GPU are folded into the next launch; inside
+// a batch the copies of later requests overlap the work of earlier ones.
+// With two or more workers the batches of different workers also overlap on
+// the device (separate streams); one worker is the default.  A worker's device buffers grow to its largest batch
 // and stay allocated, so the budget share bounds its footprint.
 //
 // The plain mode runs one worker and one rbg_bin_graph call per request: the
@@ -135,7 +136,7 @@ int rbg_server_create(const rbg_server_config *cfg, const rbg_params *defaults,
   s->cfg = *cfg;
   if (defaults) s->defaults = *defaults; else rbg_default_params(&s->defaults);
   if (s->cfg.plain) s->cfg.workers = 1;
-  if (s->cfg.workers <= 0) s->cfg.workers = 2;
+  if (s->cfg.workers <= 0) s->cfg.workers = 1;
   if (s->cfg.max_batch <= 0) s->cfg.max_batch = 64;
   if (s->cfg.max_batch_pairs <= 0) s->cfg.max_batch_pairs = 2000000000LL;
   s->t_created = Clock::now();
