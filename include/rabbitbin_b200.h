@@ -73,6 +73,11 @@ typedef struct rbg_params {
                              GCC contracts a*b+c into FMA; 0: -ffp-contract=off   */
   double wjac_cut;        /* RABBIT_DEPTH_WJAC_CUT (0)                             */
   int32_t wjac_gate;      /* RABBIT_DEPTH_WJAC_GATE (0)                            */
+  int32_t oph_k;          /* 0: ProbMinHash composition similarity (RABBIT_PMH, the
+                             default); > 0: RABBIT_PMH=0, the one-permutation
+                             MinHash metric of rabbit_sketch.h with k-mers of this
+                             size (sketch_kmer_size, 8; 1..32) and m buckets     */
+  int32_t oph_bits;       /* sketch_bits: bit-planes per OPH bucket (2; 1..7)      */
   int32_t reserved;
 } rbg_params;
 
@@ -119,6 +124,15 @@ void *rbg_stream(rbg_ctx *ctx);
 int rbg_build_pmh_winners(rbg_ctx *ctx, const rbg_params *p, const char *seqcat,
                           const int64_t *offsets, int64_t n,
                           uint32_t *out_winners32);
+
+/* One-permutation MinHash signatures (the RABBIT_PMH=0 metric): replaces
+ * rabbit_sketch::KmerSketch(m, oph_k, oph_bits).update(seq, len) followed by
+ * getSignature() (src/rabbit_sketch.h:197-285) for n contigs.  out[n][m]
+ * receives each bucket's value: bit p of out[i][r] is bit r of bit-plane p of
+ * contig i's signature (a densified bucket's borrowed value; 0 for every
+ * bucket of a contig with no valid k-mer).  Requires p->oph_k in 1..32. */
+int rbg_build_oph_signature(rbg_ctx *ctx, const rbg_params *params, const char *seqcat,
+                            const int64_t *offsets, int64_t n, uint8_t *out);
 
 /* fold_win16 over `count` folded winners (src/rabbitbin.cpp:249-253). */
 int rbg_pack_win16(rbg_ctx *ctx, const uint32_t *in, int64_t count, uint16_t *out);

@@ -23,7 +23,8 @@ class RefParams(C.Structure):
                 ("min_edge", C.c_double), ("w_comp", C.c_double),
                 ("min_cv", C.c_double), ("neg_thr", C.c_double),
                 ("depth_sim", C.c_int32), ("depth_fuse", C.c_int32),
-                ("wjac_norm", C.c_int32), ("no_abdfirst", C.c_int32)]
+                ("wjac_norm", C.c_int32), ("no_abdfirst", C.c_int32),
+                ("oph_k", C.c_int32), ("oph_bits", C.c_int32)]
 
 
 class RefOut(C.Structure):
@@ -37,7 +38,8 @@ def default_params(n, m=500, S=0, **kw):
     p = RefParams(n=n, m=m, S=S, win_bits=16, max_edges=200, mutual=1,
                   base_on=1, nthreads=os.cpu_count() or 1, seed=1, force_path=0,
                   coverage=0.95, min_edge=0.70, w_comp=-1.0, min_cv=1.0,
-                  neg_thr=-0.3, depth_sim=2, depth_fuse=1, wjac_norm=1, no_abdfirst=0)
+                  neg_thr=-0.3, depth_sim=2, depth_fuse=1, wjac_norm=1, no_abdfirst=0,
+                  oph_k=0, oph_bits=2)
     if "abdfirst" in kw:
         kw["no_abdfirst"] = 0 if kw.pop("abdfirst") else 1
     for k, v in kw.items():
@@ -76,6 +78,24 @@ class _Lib:
         self._ud = getattr(L, p + "unit_dot_f")
         self._ud.restype = C.c_float
         self._ud.argtypes = [C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_uint32]
+        self._ov = getattr(L, p + "oph_values")
+        self._ov.restype = None
+        self._ov.argtypes = [C.c_char_p, C.POINTER(C.c_int64), C.c_int64, C.c_uint32, C.c_int,
+                             C.c_uint32, C.POINTER(C.c_uint8)]
+        self._rgo = getattr(L, p + "run_graph_oph", None)
+        if self._rgo is not None:
+            self._rgo.restype = C.c_int
+            self._rgo.argtypes = [C.POINTER(RefParams), C.c_char_p, C.POINTER(C.c_int64),
+                                  C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                  C.POINTER(RefOut)]
+
+    def oph_values(self, seqcat, offsets, m=500, K=8, bits=2):
+        """One-permutation MinHash bucket values [n, m] (uint8)."""
+        n = len(offsets) - 1
+        out = np.zeros((n, m), dtype=np.uint8)
+        offs = np.ascontiguousarray(offsets, dtype=np.int64)
+        self._ov(seqcat, _ptr(offs, C.c_int64), n, m, K, bits, _ptr(out, C.c_uint8))
+        return out
 
     def build_winners(self, seqcat, offsets, k=4, m=500, seed=42, gc_norm=1,
                       gc_cap=20.0, nthreads=None):
@@ -96,6 +116,22 @@ class _Lib:
                       _ptr(unit, C.c_float), C.byref(out))
         if rc != 0:
             raise RuntimeError(f"oracle run_graph failed: {rc}")
+        return self._result(out, unit, S)
+
+    def run_graph_oph(self, params, seqcat, offsets, depth):
+        """The graph with RABBIT_PMH=0 (params.oph_k, params.oph_bits set)."""
+        n, S = params.n, params.S
+        offs = np.ascontiguousarray(offsets, dtype=np.int64)
+        d = np.ascontiguousarray(depth, dtype=np.float32).reshape(n, max(S, 0))
+        unit = np.zeros((n, max(S, 1)), dtype=np.float32)
+        out = RefOut()
+        rc = self._rgo(C.byref(params), seqcat, _ptr(offs, C.c_int64), _ptr(d, C.c_float),
+                       _ptr(unit, C.c_float), C.byref(out))
+        if rc != 0:
+            raise RuntimeError(f"oracle run_graph_oph failed: {rc}")
+        return self._result(out, unit, S)
+
+    def _result(self, out, unit, S):
         ne = out.n_edges
         res = dict(b0=out.b0, sim_cutoff=out.sim_cutoff,
                    src=np.ctypeslib.as_array(out.from_, (ne,)).copy() if ne else np.zeros(0, np.uint32),

@@ -34,6 +34,7 @@ FRAGMENTS = [
     ("frag_compare_edge.inc", "rabbitbin.h", 418, 429),
     ("frag_fold16.inc", "rabbitbin.cpp", 249, 253),
     ("frag_depth_terms.inc", "rabbitbin.cpp", 685, 970),
+    ("frag_jaccard_raw.inc", "rabbitbin.cpp", 1031, 1135),
     ("frag_pmh_sim.inc", "rabbitbin.cpp", 1194, 1426),
     ("frag_build_winners.inc", "rabbitbin.cpp", 1436, 1589),
     ("frag_contig_rec.inc", "rabbitbin.cpp", 1876, 1888),

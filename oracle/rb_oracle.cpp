@@ -16,6 +16,8 @@
 //   large N     gen_fused_calib_graph        src/impl/rb_graph.cpp:501-1356
 //   calibration calib_converge               src/impl/rb_graph.cpp:390-415
 //   weights     depth_edge_term etc.         src/rabbitbin.cpp:685-970, :5482-5509
+//   OPH metric  KmerSketch update/densify/buildSig  src/rabbit_sketch.h:197-281
+//               (RABBIT_PMH=0; similarity jaccard_raw src/rabbitbin.cpp:1031-1135)
 // Floating point follows the reference's release build on an AVX-512 host:
 // compiled with -ffp-contract=off, with std::fma written where that build
 // fuses (AVX-512 FMA intrinsics and GCC-contracted expressions).  The third
@@ -698,6 +700,85 @@ int orc_parse_fasta(const char *buf, int64_t n, int64_t min_contig, int64_t min_
       out->seq_off[++k] = (int64_t)o;
     }
   return 0;
+}
+
+// One-permutation MinHash bucket values (RABBIT_PMH=0 sketch) of n contigs:
+// out[r][b] = the low `bits` bits of bucket b after densification, i.e. the
+// bit-planes of KmerSketch::getSignature read per bucket.
+//   update  src/rabbit_sketch.h:199-238 (2-bit lex codes, windows of K valid
+//           bases, canonical = min(forward, reverse complement),
+//           h = murmur3_fmix(canonical, 42), bucket (h>>32)*m>>32, keep min (uint32)h)
+//   densify src/rabbit_sketch.h:245-259 (probe base/step from murmur3_fmix of the
+//           bucket index, value ^ (uint32)murmur3_fmix(hop, 0x9E3779B97F4A7C15))
+//   buildSig src/rabbit_sketch.h:264-281 (no k-mer at all: every bucket 0)
+void orc_oph_values(const char *seqcat, const int64_t *offsets, int64_t n, uint32_t m, int K,
+                   uint32_t bits, uint8_t *out) {
+  auto fmix = [](uint64_t x, uint64_t seed) {
+    x ^= seed;
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdull;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ull;
+    x ^= x >> 33;
+    return x;
+  };
+  auto reduce = [](uint64_t h, uint32_t mm) { return (uint32_t)(((h >> 32) * (uint64_t)mm) >> 32); };
+  auto code = [](char ch) -> int {
+    switch (ch) {
+      case 'A': case 'a': return 0;
+      case 'C': case 'c': return 1;
+      case 'G': case 'g': return 2;
+      case 'T': case 't': return 3;
+      default: return -1;
+    }
+  };
+  const uint64_t seed = 42;
+  const uint32_t empty = 0xFFFFFFFFu;
+  std::vector<uint32_t> reg(m);
+  for (int64_t r = 0; r < n; ++r) {
+    std::fill(reg.begin(), reg.end(), empty);
+    const char *sq = seqcat + offsets[r];
+    const int64_t L = offsets[r + 1] - offsets[r];
+    uint32_t nonempty = 0;
+    for (int64_t i = 0; i + K <= L; ++i) {
+      uint64_t fwd = 0, rc = 0;
+      bool ok = true;
+      for (int q = 0; q < K && ok; ++q) {
+        const int c = code(sq[i + q]);
+        if (c < 0) ok = false;
+        fwd = (fwd << 2) | (uint64_t)c;
+        rc |= (uint64_t)(3 - c) << (2 * q);          // base q lands at position K-1-q
+      }
+      if (!ok) continue;
+      const uint64_t h = fmix(fwd < rc ? fwd : rc, seed);
+      const uint32_t b = reduce(h, m), v = (uint32_t)h;
+      if (v < reg[b]) {
+        if (reg[b] == empty) ++nonempty;
+        reg[b] = v;
+      }
+    }
+    const uint32_t mask = (1u << bits) - 1u;
+    for (uint32_t b = 0; b < m; ++b) {
+      uint32_t v = reg[b];
+      if (nonempty == 0) {
+        v = 0;
+      } else if (v == empty) {
+        const uint64_t base = fmix(b, seed ^ 0xA5A5A5A5DEADBEEFull);
+        const uint64_t step = fmix(b, seed ^ 0x123456789ABCDEF0ull) | 1ull;
+        uint64_t cur = base;
+        v = 0;
+        for (uint32_t t = 1; t <= m; ++t) {
+          cur += step;
+          const uint32_t x = reg[reduce(cur, m)];
+          if (x != empty) {
+            v = x ^ (uint32_t)fmix(t, 0x9E3779B97F4A7C15ull);
+            break;
+          }
+        }
+      }
+      out[(size_t)r * m + b] = (uint8_t)(v & mask);
+    }
+  }
 }
 
 }  // extern "C"

@@ -134,9 +134,7 @@ static const char *rb_getenv(const char *key) {
   const char *e = getenv(key);
   return (e && e[0]) ? e : nullptr;
 }
-// Unused branches of the fragments (OPH signatures, Welford correlation).
-static inline double jaccard_raw(const uint64_t *, const uint64_t *, uint32_t,
-                                 uint32_t, uint32_t) { abort(); }
+// Unused branch of the fragments (Welford correlation).
 double cal_depth_corr(size_t, size_t, bool = false, bool = false) { abort(); }
 
 #pragma omp declare reduction (merge_graphnode : std::vector<GraphNodeId> : omp_out.insert(omp_out.end(), omp_in.begin(), omp_in.end()) )
@@ -147,6 +145,7 @@ double cal_depth_corr(size_t, size_t, bool = false, bool = false) { abort(); }
 #include "frag_compare_edge.inc"    // src/rabbitbin.h:418-429
 #include "frag_fold16.inc"          // src/rabbitbin.cpp:249-253
 #include "frag_depth_terms.inc"     // src/rabbitbin.cpp:685-970
+#include "frag_jaccard_raw.inc"     // src/rabbitbin.cpp:1031-1135
 #include "frag_pmh_sim.inc"         // src/rabbitbin.cpp:1194-1426
 #include "frag_build_winners.inc"   // src/rabbitbin.cpp:1436-1589
 // globals and helpers the FASTA parser reads (src/rabbitbin.h:198-199 and the
@@ -213,6 +212,8 @@ struct RefParams {
   int32_t depth_fuse;   // RABBIT_DEPTH_FUSE
   int32_t wjac_norm;    // RABBIT_DEPTH_WJAC_NORM
   int32_t no_abdfirst;  // RABBIT_NO_ABDFIRST set
+  int32_t oph_k;        // 0: PMH metric; > 0: RABBIT_PMH=0 with sketch_kmer_size = oph_k
+  int32_t oph_bits;     // sketch_bits
 };
 
 struct RefOut {
@@ -280,11 +281,74 @@ int ref_parse_fasta(const char *path, int nthreads, int64_t min_contig, int64_t 
   return 0;
 }
 
+// One-permutation MinHash signatures of n contigs, the sketch loop of
+// src/rabbitbin.cpp:4819-4841 (KmerSketch(m, K, bits), update, getSignature):
+// rows of nw * bits words (plane p at [p * nw]) into sig_out.
+static void oph_signatures(const char *seqcat, const int64_t *offsets, int64_t n, uint32_t m,
+                           int K, uint32_t bits, int nthreads, uint64_t *sig_out) {
+  const uint32_t nw = (m + 63) / 64;
+  const size_t stride = (size_t)nw * bits;
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 16)
+  for (int64_t r = 0; r < n; ++r) {
+    rabbit_sketch::KmerSketch sk(m, K, bits);
+    sk.update(seqcat + offsets[r], (uint64_t)(offsets[r + 1] - offsets[r]));
+    const uint64_t *sig = sk.getSignature();
+    std::memcpy(sig_out + (size_t)r * stride, sig, stride * sizeof(uint64_t));
+  }
+}
+
+static int run_graph_body(const RefParams *p, const uint32_t *winners32,
+                          const float *depth_raw, float *unit_out, RefOut *out);
+
+// Bucket values of the one-permutation signatures: bit p of values[r][b] =
+// bit b of plane p.
+void ref_oph_values(const char *seqcat, const int64_t *offsets, int64_t n, uint32_t m, int K,
+                    uint32_t bits, uint8_t *values) {
+  const uint32_t nw = (m + 63) / 64;
+  const size_t stride = (size_t)nw * bits;
+  std::vector<uint64_t> sig((size_t)n * stride);
+  oph_signatures(seqcat, offsets, n, m, K, bits, omp_get_max_threads(), sig.data());
+  for (int64_t r = 0; r < n; ++r)
+    for (uint32_t b = 0; b < m; ++b) {
+      uint32_t v = 0;
+      for (uint32_t q = 0; q < bits; ++q)
+        v |= (uint32_t)((sig[(size_t)r * stride + (size_t)q * nw + (b >> 6)] >> (b & 63)) & 1u) << q;
+      values[(size_t)r * m + b] = (uint8_t)v;
+    }
+}
+
+// The same run with RABBIT_PMH=0: the graph similarity is jaccard_raw over
+// the one-permutation signatures (graph_sim, src/rabbitbin.cpp:1403-1426) and
+// no baseline is estimated (:4958).
+int ref_run_graph_oph(const RefParams *p, const char *seqcat, const int64_t *offsets,
+                      const float *depth_raw, float *unit_out, RefOut *out) {
+  const uint32_t m = (uint32_t)p->m, bits = (uint32_t)p->oph_bits;
+  g_sig_m = m;
+  g_sig_nw = (m + 63) / 64;
+  g_sig_np = bits;
+  g_sig_flat.assign((size_t)p->n * g_sig_nw * g_sig_np, 0ull);
+  oph_signatures(seqcat, offsets, p->n, m, p->oph_k, bits, p->nthreads > 0 ? p->nthreads : 1,
+                 g_sig_flat.data());
+  g_pmh_mode = false;
+  const int rc = run_graph_body(p, nullptr, depth_raw, unit_out, out);
+  g_pmh_mode = true;
+  std::vector<uint64_t>().swap(g_sig_flat);
+  return rc;
+}
+
 // Runs pack -> b0 -> ranks/unit rows -> graph -> edge weights exactly as
 // rb_cmd_bin does for a PMH run; winners32 holds the build_pmh_winners rows.
 // unit_out (n*S floats, may be null) receives g_depth_unit.
 int ref_run_graph(const RefParams *p, const uint32_t *winners32,
                   const float *depth_raw, float *unit_out, RefOut *out) {
+  g_pmh_mode = true;
+  return run_graph_body(p, winners32, depth_raw, unit_out, out);
+}
+
+}  // extern "C"
+
+static int run_graph_body(const RefParams *p, const uint32_t *winners32,
+                          const float *depth_raw, float *unit_out, RefOut *out) {
   nobs = (size_t)p->n;
   g_pmh_m = (uint32_t)p->m;
   sketch_size = g_pmh_m;
@@ -335,7 +399,8 @@ int ref_run_graph(const RefParams *p, const uint32_t *winners32,
   build_anynz_cache();
 
   // 16-bit pack (src/rabbitbin.cpp:4934-4952).
-  g_win_flat.assign(winners32, winners32 + nobs * g_pmh_m);
+  g_win_flat.clear();
+  if (g_pmh_mode) g_win_flat.assign(winners32, winners32 + nobs * g_pmh_m);
   g_win16.clear();
   g_win_bits = 32;
   if (p->win_bits == 16 && !g_win_flat.empty()) {
@@ -347,7 +412,7 @@ int ref_run_graph(const RefParams *p, const uint32_t *winners32,
   // b0 (src/rabbitbin.cpp:4958-4965).
   g_pmh_baseline = 0.0;
   g_inv_one_minus_b0 = 1.0;
-  if (g_pmh_base_on) {
+  if (g_pmh_mode && g_pmh_base_on) {
     g_pmh_baseline = estimate_pmh_baseline(nobs);
     g_inv_one_minus_b0 = (g_pmh_baseline < 1.0) ? (1.0 / (1.0 - g_pmh_baseline)) : 1.0;
   }
@@ -428,6 +493,8 @@ int ref_run_graph(const RefParams *p, const uint32_t *winners32,
   }
   return 0;
 }
+
+extern "C" {
 
 // Float dot of two unit rows exactly as the abundance-first prune computes it.
 float ref_unit_dot_f(const float *a, const float *b, uint32_t S) {

@@ -34,7 +34,8 @@ class Params(C.Structure):
                 ("w_comp", C.c_double), ("min_cv", C.c_double), ("neg_thr", C.c_double),
                 ("depth_sim", C.c_int32), ("depth_fuse", C.c_int32),
                 ("wjac_norm", C.c_int32), ("fp_contract", C.c_int32),
-                ("wjac_cut", C.c_double), ("wjac_gate", C.c_int32), ("reserved", C.c_int32)]
+                ("wjac_cut", C.c_double), ("wjac_gate", C.c_int32), ("oph_k", C.c_int32),
+                ("oph_bits", C.c_int32), ("reserved", C.c_int32)]
 
 
 class Graph(C.Structure):
@@ -126,6 +127,8 @@ def lib():
         "rbg_stream": ([vp], vp),
         "rbg_build_pmh_winners": ([vp, P(Params), C.c_char_p, i64p, C.c_int64,
                                    P(C.c_uint32)], C.c_int),
+        "rbg_build_oph_signature": ([vp, P(Params), C.c_char_p, i64p, C.c_int64,
+                                     P(C.c_uint8)], C.c_int),
         "rbg_pack_win16": ([vp, P(C.c_uint32), C.c_int64, P(C.c_uint16)], C.c_int),
         "rbg_estimate_pmh_baseline": ([vp, P(Params), vp, C.c_int32, C.c_int64,
                                        P(C.c_double)], C.c_int),
@@ -277,6 +280,16 @@ class Context:
         out = np.zeros((n, p.m), np.uint32)
         self._check(self._L.rbg_build_pmh_winners(self._h, C.byref(p), seqcat, _p(offs, C.c_int64),
                                                   n, _p(out, C.c_uint32)), "build_pmh_winners")
+        return out
+
+    def build_oph_signature(self, seqcat, offsets, params):
+        """One-permutation MinHash bucket values [n, m] (uint8; params.oph_k > 0)."""
+        offs = np.ascontiguousarray(offsets, np.int64)
+        n = len(offs) - 1
+        out = np.zeros((n, params.m), np.uint8)
+        self._check(self._L.rbg_build_oph_signature(self._h, C.byref(params), seqcat,
+                                                    _p(offs, C.c_int64), n, _p(out, C.c_uint8)),
+                    "build_oph_signature")
         return out
 
     def pack_win16(self, w32):

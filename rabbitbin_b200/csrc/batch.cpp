@@ -226,6 +226,9 @@ void plan_batch(const rbg_params *defaults, const rbg_assembly *asms, int nb, Ba
     a.in = &x;
     a.p = x.params ? x.params : defaults;
     validate_assembly(x, a.p, "assembly " + std::to_string(i) + ": ");
+    if (a.p->oph_k > 0)
+      throw Error(RBG_ERR_UNSUPPORTED, "assembly " + std::to_string(i) +
+                                           ": the batch form uses the ProbMinHash metric (oph_k = 0)");
     a.n = x.n;
     a.nbases = x.n > 0 ? x.offsets[x.n] : 0;
     a.S = x.S;

@@ -152,6 +152,9 @@ void validate_params(const rbg_params *p) {
   if (p->gc_norm != 0 && p->gc_norm != 1) throw Error(RBG_ERR_UNSUPPORTED, "gc_norm must be 0 or 1");
   if (p->max_edges < 1 || p->max_edges > 448) throw Error(RBG_ERR_UNSUPPORTED, "max_edges must be in 1..448");
   if (!(p->coverage > 0.0 && p->coverage < 1.0)) throw Error(RBG_ERR_ARG, "coverage must be in (0,1)");
+  if (p->oph_k < 0 || p->oph_k > 32) throw Error(RBG_ERR_ARG, "oph_k must be in 0..32");
+  if (p->oph_k > 0 && (p->oph_bits < 1 || p->oph_bits > 7))
+    throw Error(RBG_ERR_UNSUPPORTED, "oph_bits must be in 1..7");
 }
 
 std::unique_ptr<Tables> make_tables(const rbg_params *p, cudaStream_t s) {

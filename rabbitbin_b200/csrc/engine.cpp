@@ -151,17 +151,17 @@ void prep_depth(rbg_ctx *c, const rbg_params *p) {
 // Sketch stage: pack, count + weights, register minimum.
 // Sketch buffers and the kernel arguments over all contigs.
 SketchArgs sketch_setup(rbg_ctx *c, const rbg_params *p, bool want_winners) {
-  Tables &T = tables_for(c, p);
+  const bool oph = p->oph_k > 0;          // one-permutation MinHash: no PMH tables
+  if (want_winners && oph)
+    throw Error(RBG_ERR_ARG, "winner rows exist only for the ProbMinHash metric (oph_k = 0)");
+  Tables *T = oph ? nullptr : &tables_for(c, p);
   const int64_t n = c->n;
   const int m = p->m, mpad = mpad_of(p->m);
   const int64_t nwords = (c->nbases + 15) / 16 + 1;
   c->packed.ensure(nwords * 4);
   c->nmask.ensure((nwords / 2 + 2) * 4);
-  c->elem_winv.ensure(std::max<int64_t>(n, 1) * T.t->n_elems * sizeof(double));
-  c->elem_cnt.ensure(std::max<int64_t>(n, 1) * sizeof(int32_t));
   c->codesA.ensure(std::max<int64_t>(n, 1) * mpad);
   c->codesB.ensure(std::max<int64_t>(n, 1) * mpad);
-  if (want_winners) c->winners32.ensure(std::max<int64_t>(n, 1) * m * sizeof(uint32_t));
   SketchArgs a;
   a.packed = c->packed.as<uint32_t>();
   a.nmask = c->nmask.as<uint32_t>();
@@ -169,21 +169,42 @@ SketchArgs sketch_setup(rbg_ctx *c, const rbg_params *p, bool want_winners) {
   a.n = n;
   a.k = p->k;
   a.m = m;
+  a.mpad = mpad;
   a.gc_norm = p->gc_norm;
   a.gc_cap = p->gc_norm_cap;
-  a.n_elems = T.t->n_elems;
-  a.rank_of_code = T.rank.as<int16_t>();
-  a.elem_winv = c->elem_winv.as<double>();
-  a.elem_cnt = c->elem_cnt.as<int32_t>();
-  a.order = T.order.as<RegOrder>();
-  a.UT = T.UT.as<double>();
-  a.codeA = T.codeA.as<uint8_t>();
-  a.W32 = T.W32.as<uint32_t>();
   a.codesA = c->codesA.as<uint8_t>();
   a.codesB = c->codesB.as<uint8_t>();
-  a.winners32 = want_winners ? c->winners32.as<uint32_t>() : nullptr;
-  a.mpad = mpad;
+  if (!oph) {
+    c->elem_winv.ensure(std::max<int64_t>(n, 1) * T->t->n_elems * sizeof(double));
+    c->elem_cnt.ensure(std::max<int64_t>(n, 1) * sizeof(int32_t));
+    if (want_winners) c->winners32.ensure(std::max<int64_t>(n, 1) * m * sizeof(uint32_t));
+    a.n_elems = T->t->n_elems;
+    a.rank_of_code = T->rank.as<int16_t>();
+    a.elem_winv = c->elem_winv.as<double>();
+    a.elem_cnt = c->elem_cnt.as<int32_t>();
+    a.order = T->order.as<RegOrder>();
+    a.UT = T->UT.as<double>();
+    a.codeA = T->codeA.as<uint8_t>();
+    a.W32 = T->W32.as<uint32_t>();
+    a.winners32 = want_winners ? c->winners32.as<uint32_t>() : nullptr;
+  }
   return a;
+}
+
+// Sketch of contigs [a.offsets - first, + a.n): k-mer counts and the register
+// minimum (ProbMinHash), or the one-permutation MinHash buckets; `mid` is
+// recorded between the two ProbMinHash kernels (null: none).
+void sketch_contigs(rbg_ctx *c, const rbg_params *p, const SketchArgs &a, cudaEvent_t mid) {
+  if (p->oph_k > 0) {
+    if (mid) CK(cudaEventRecord(mid, c->stream));
+    launch_oph(a, p->oph_k, p->oph_bits, kOphSeed, c->stream);
+    c->launches += a.n ? 1 : 0;
+    return;
+  }
+  launch_count(a, c->stream);
+  if (mid) CK(cudaEventRecord(mid, c->stream));
+  launch_minreduce(a, c->stream);
+  c->launches += a.n ? 2 : 0;
 }
 
 // The host-input path of rbg_bin_graph: the ASCII copy runs in chunks on the
@@ -243,13 +264,11 @@ void stage_sketch_chunked(rbg_ctx *c, const rbg_params *p, const char *seqcat,
       SketchArgs a = all;
       a.offsets += c0;
       a.n = c1 - c0;
-      a.elem_winv += c0 * E;
-      a.elem_cnt += c0;
+      if (a.elem_winv) a.elem_winv += c0 * E;
+      if (a.elem_cnt) a.elem_cnt += c0;
       a.codesA += c0 * mpad;
       a.codesB += c0 * mpad;
-      launch_count(a, c->stream);
-      launch_minreduce(a, c->stream);
-      c->launches += 2;
+      sketch_contigs(c, p, a, nullptr);
       if (stream_pairs) {
         launch_allpairs_sym_window(ga, o, c0, c1, c->stream);
         c->launches += 1;
@@ -266,49 +285,15 @@ void stage_sketch_chunked(rbg_ctx *c, const rbg_params *p, const char *seqcat,
 }
 
 void run_sketch(rbg_ctx *c, const rbg_params *p, bool want_winners) {
-  Tables &T = tables_for(c, p);
-  const int64_t n = c->n;
-  const int m = p->m, mpad = mpad_of(p->m);
-  const int64_t nwords = (c->nbases + 15) / 16 + 1;
-  c->packed.ensure(nwords * 4);
-  c->nmask.ensure((nwords / 2 + 2) * 4);
-  c->elem_winv.ensure(std::max<int64_t>(n, 1) * T.t->n_elems * sizeof(double));
-  c->elem_cnt.ensure(std::max<int64_t>(n, 1) * sizeof(int32_t));
-  c->codesA.ensure(std::max<int64_t>(n, 1) * mpad);
-  c->codesB.ensure(std::max<int64_t>(n, 1) * mpad);
-  if (want_winners) c->winners32.ensure(std::max<int64_t>(n, 1) * m * sizeof(uint32_t));
+  const SketchArgs a = sketch_setup(c, p, want_winners);
   CK(cudaEventRecord(c->ev[0], c->stream));
   prep_depth(c, p);
   launch_pack(c->ascii.as<char>(), c->nbases, c->packed.as<uint32_t>(), c->nmask.as<uint32_t>(),
               c->stream);
   c->launches += c->nbases ? 1 : 0;
   CK(cudaEventRecord(c->ev[1], c->stream));
-  SketchArgs a;
-  a.packed = c->packed.as<uint32_t>();
-  a.nmask = c->nmask.as<uint32_t>();
-  a.offsets = c->offsets.as<int64_t>();
-  a.n = n;
-  a.k = p->k;
-  a.m = m;
-  a.gc_norm = p->gc_norm;
-  a.gc_cap = p->gc_norm_cap;
-  a.n_elems = T.t->n_elems;
-  a.rank_of_code = T.rank.as<int16_t>();
-  a.elem_winv = c->elem_winv.as<double>();
-  a.elem_cnt = c->elem_cnt.as<int32_t>();
-  a.order = T.order.as<RegOrder>();
-  a.UT = T.UT.as<double>();
-  a.codeA = T.codeA.as<uint8_t>();
-  a.W32 = T.W32.as<uint32_t>();
-  a.codesA = c->codesA.as<uint8_t>();
-  a.codesB = c->codesB.as<uint8_t>();
-  a.winners32 = want_winners ? c->winners32.as<uint32_t>() : nullptr;
-  a.mpad = mpad;
-  launch_count(a, c->stream);
-  CK(cudaEventRecord(c->ev[2], c->stream));
-  launch_minreduce(a, c->stream);
+  sketch_contigs(c, p, a, c->ev[2]);
   CK(cudaEventRecord(c->ev[3], c->stream));
-  c->launches += n ? 2 : 0;
   CK(cudaGetLastError());
 }
 
@@ -346,7 +331,8 @@ void count_pairs_codes(rbg_ctx *c, int mpad, int m, const int64_t *pr, int np, u
 bool sym_regime(const rbg_params *p, int64_t n, int S) {
   const double w_comp = (p->w_comp < 0.0) ? (S <= 2 ? 1.0 : 0.0) : p->w_comp;
   const bool fused = (p->force_path == 2) || (p->force_path == 0 && n > 25000);
-  return n > 0 && fused && p->abdfirst && S > 1 && w_comp < 1.0 && w_comp < p->min_edge;
+  return n > 0 && fused && p->oph_k == 0 && p->abdfirst && S > 1 && w_comp < 1.0 &&
+         w_comp < p->min_edge;
 }
 
 // Graph-stage buffers and kernel arguments of the staged assembly (the
@@ -559,16 +545,19 @@ void run_graph(rbg_ctx *c, const rbg_params *p, const ShardCtx *sc = nullptr) {
   const bool use_colnorm = need_colnorm(p, S);
   CK(cudaEventRecord(c->ev[4], c->stream));
 
-  // b0 on the codes (equal codes <=> equal winners of the chosen width)
+  // b0 on the codes (equal codes <=> equal winners of the chosen width); the
+  // one-permutation metric has no baseline (src/rabbitbin.cpp:4958)
+  const bool oph = p->oph_k > 0;
   c->b0 = 0.0;
-  if (p->base_on) {
+  if (p->base_on && !oph) {
     c->b0 = estimate_b0(c, n, m, [&](const int64_t *pr, int np, uint32_t *out) {
       count_pairs_codes(c, mpad, m, pr, np, out);
     });
   }
   std::vector<double> sv_d;
   std::vector<float> sv_f;
-  sv_table(m, p->base_on != 0, c->b0, sv_d, sv_f);
+  if (oph) oph_sv_table(m, sv_d, sv_f);
+  else sv_table(m, p->base_on != 0, c->b0, sv_d, sv_f);
   std::vector<uint32_t> sv_bits(m + 1);
   std::memcpy(sv_bits.data(), sv_f.data(), (m + 1) * sizeof(uint32_t));
   CK(cudaMemcpyAsync(c->svbits.p, sv_bits.data(), (m + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice,
@@ -577,6 +566,9 @@ void run_graph(rbg_ctx *c, const rbg_params *p, const ShardCtx *sc = nullptr) {
 
   const bool fused = (p->force_path == 2) || (p->force_path == 0 && n > 25000);
   if (fused && n <= 2500) throw Error(RBG_ERR_ARG, "the fused path samples 2500 contigs; need n > 2500");
+  if (fused && oph)
+    throw Error(RBG_ERR_UNSUPPORTED, "the one-permutation metric runs the small path only "
+                                     "(n <= 25000 or force_path = 1)");
   c->path = fused ? 2 : 1;
   CK(cudaStreamWaitEvent(c->stream, c->ev_aux, 0));   // unit rows, anynz, column norms
   c->prep_done = false;
@@ -864,6 +856,8 @@ void bin_graph_sharded(rbg_ctx *c, const rbg_params *p, const rbg_shard *sh, con
   if (!sh || !sh->allgather || sh->world < 1 || sh->rank < 0 || sh->rank >= sh->world)
     throw Error(RBG_ERR_ARG, "bad shard description");
   if (n_local < 0) throw Error(RBG_ERR_ARG, "n_local < 0");
+  if (p->oph_k > 0)
+    throw Error(RBG_ERR_UNSUPPORTED, "sharded assemblies use the ProbMinHash metric (oph_k = 0)");
   const int W = sh->world;
   const int m = p->m, mpad = mpad_of(m);
   ShardCtx sc;
@@ -1025,6 +1019,8 @@ int rbg_default_params(rbg_params *p) {
   p->fp_contract = 1;
   p->wjac_cut = 0.0;
   p->wjac_gate = 0;
+  p->oph_k = 0;
+  p->oph_bits = 2;
   return RBG_OK;
 }
 
@@ -1115,6 +1111,25 @@ int rbg_build_pmh_winners(rbg_ctx *c, const rbg_params *p, const char *seqcat,
   });
 }
 
+int rbg_build_oph_signature(rbg_ctx *c, const rbg_params *p, const char *seqcat,
+                            const int64_t *offsets, int64_t n, uint8_t *out) {
+  return guarded(c, [&] {
+    validate(p);
+    if (p->oph_k < 1) throw Error(RBG_ERR_ARG, "oph_k must be set (1..32)");
+    if (!out && n > 0) throw Error(RBG_ERR_ARG, "null output");
+    stage(c, seqcat, offsets, n, nullptr, 0);
+    run_sketch(c, p, false);
+    c->prep_done = false;
+    const int m = p->m, mpad = mpad_of(m);
+    if (n) {
+      c->tmp.ensure((size_t)n * m);
+      launch_oph_values(c->codesA.as<uint8_t>(), n, m, mpad, c->tmp.as<uint8_t>(), c->stream);
+      CK(cudaMemcpyAsync(out, c->tmp.p, (size_t)n * m, cudaMemcpyDeviceToHost, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
 int rbg_pack_win16(rbg_ctx *c, const uint32_t *in, int64_t count, uint16_t *out) {
   return guarded(c, [&] {
     if (count < 0 || (count > 0 && (!in || !out))) throw Error(RBG_ERR_ARG, "bad arguments");
@@ -1155,6 +1170,9 @@ int rbg_build_graph(rbg_ctx *c, const rbg_params *p, const uint32_t *winners32, 
   return guarded(c, [&] {
     validate(p);
     if (n < 0 || (n > 0 && !winners32) || !out) throw Error(RBG_ERR_ARG, "bad arguments");
+    if (p->oph_k > 0)
+      throw Error(RBG_ERR_ARG, "winner rows are ProbMinHash sketches; the one-permutation "
+                               "metric starts from sequences (rbg_bin_graph)");
     if (S < 0 || S > kMaxS) throw Error(RBG_ERR_UNSUPPORTED, "S must be in 0..64");
     c->streamed = false;
     c->n = n;

@@ -516,4 +516,163 @@ void launch_minreduce(const SketchArgs &a, cudaStream_t s) {
   k_minreduce<<<(unsigned)grid, kMThreads, smem, s>>>(a);
 }
 
+namespace {
+
+// ── One-permutation MinHash (the RABBIT_PMH=0 metric, src/rabbit_sketch.h) ──
+// KmerSketch::update (src/rabbit_sketch.h:199-238): every window of K bases
+// that are all A/C/G/T offers h = murmur3_fmix(min(forward, reverse
+// complement), seed) to bucket ((h >> 32) * m) >> 32 with value (uint32_t)h,
+// kept if smaller.  buildSig (:264-281) gives an empty bucket the value that
+// densify (:245-259) borrows along its probe sequence, and keeps `bits` low
+// bits of every bucket (bit-planes); a sketch with no k-mer at all has an
+// all-zero signature.  Here a bucket's kept bits + 1 are its 8-bit code (A
+// side; the B side is the same), so equal codes are exactly the buckets whose
+// bit-planes all agree (jaccard_raw, src/rabbitbin.cpp:1035-1130).
+
+__device__ __forceinline__ uint64_t oph_fmix(uint64_t x, uint64_t seed) {
+  x ^= seed;
+  x ^= x >> 33;
+  x *= 0xff51afd7ed558ccdull;
+  x ^= x >> 33;
+  x *= 0xc4ceb9fe1a85ec53ull;
+  x ^= x >> 33;
+  return x;
+}
+
+__device__ __forceinline__ uint32_t oph_bucket(uint64_t h, uint32_t m) {
+  return (uint32_t)(((h >> 32) * (uint64_t)m) >> 32);
+}
+
+// Reverse complement of a K-base word (2 bits a base, first base highest).
+__device__ __forceinline__ uint64_t oph_revcomp(uint64_t x, int K) {
+  x = __brevll(~x);                        // complement, then every bit reversed
+  x = ((x >> 1) & 0x5555555555555555ull) | ((x & 0x5555555555555555ull) << 1);
+  return x >> (64 - 2 * K);                // the base pairs back in order
+}
+
+constexpr int kOphWarps = 4;
+
+// Warp per contig (warps stride over the contigs); the warp's m registers in
+// shared memory; a lane takes one 16-base word per step and the windows that
+// end in it.
+__global__ void __launch_bounds__(kOphWarps * 32)
+k_oph(SketchArgs a, int K, int bits, uint64_t seed) {
+  extern __shared__ uint32_t sh_oph[];
+  constexpr uint32_t kEmpty = 0xFFFFFFFFu;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint32_t m = (uint32_t)a.m;
+  uint32_t *reg = sh_oph + (size_t)wib * m;
+  const uint64_t kmask = K >= 32 ? ~0ull : ((1ull << (2 * K)) - 1ull);
+  const uint32_t vmask = (1u << bits) - 1u;
+  const int64_t warps = (int64_t)gridDim.x * kOphWarps;
+  for (int64_t c = (int64_t)blockIdx.x * kOphWarps + wib; c < a.n; c += warps) {
+    for (uint32_t r = lane; r < m; r += 32) reg[r] = kEmpty;
+    __syncwarp();
+    const int64_t s = a.offsets[c], e = a.offsets[c + 1];
+    if (e - s >= K) {
+      const int64_t w0 = s >> 4, w1 = (e + 15) >> 4;
+      uint32_t c1 = 0, c2 = 0, b1 = 0xFFFFu, b2 = 0xFFFFu;   // the two words before w0
+      for (int64_t base = w0; base < w1; base += 32) {
+        const int64_t wi = base + lane;
+        uint32_t cur = 0, bad = 0xFFFFu;
+        if (wi < w1) {
+          cur = __ldg(a.packed + wi);
+          bad = invalid16(a.nmask, wi, s, e);
+        }
+        uint32_t p1 = __shfl_up_sync(0xffffffffu, cur, 1), q1 = __shfl_up_sync(0xffffffffu, bad, 1);
+        uint32_t p2 = __shfl_up_sync(0xffffffffu, cur, 2), q2 = __shfl_up_sync(0xffffffffu, bad, 2);
+        if (lane == 0) { p1 = c1; q1 = b1; p2 = c2; q2 = b2; }
+        if (lane == 1) { p2 = c1; q2 = b1; }
+        c2 = __shfl_sync(0xffffffffu, cur, 30);
+        b2 = __shfl_sync(0xffffffffu, bad, 30);
+        c1 = __shfl_sync(0xffffffffu, cur, 31);
+        b1 = __shfl_sync(0xffffffffu, bad, 31);
+        if (wi >= w1) continue;
+        // bit 15 - p: base p of the word (p < 0: the words before); a window
+        // ending at base t is valid when bits 15-t .. 15-t+K-1 are all clear
+        const uint64_t wbad = ((uint64_t)q2 << 32) | ((uint64_t)q1 << 16) | bad;
+        uint64_t any = wbad;
+        for (int q = 1; q < K; ++q) any |= wbad >> q;
+        uint32_t kv = ~(uint32_t)any & 0xFFFFu;
+        const uint64_t lo = ((uint64_t)p1 << 32) | cur;
+        while (kv) {
+          const int bp = __ffs(kv) - 1;                // = 15 - t
+          kv &= kv - 1;
+          const int sh = 2 * bp;
+          const uint64_t fwd = (sh ? (lo >> sh) | ((uint64_t)p2 << (64 - sh)) : lo) & kmask;
+          const uint64_t rc = oph_revcomp(fwd, K);
+          const uint64_t h = oph_fmix(fwd < rc ? fwd : rc, seed);
+          atomicMin(&reg[oph_bucket(h, m)], (uint32_t)h);
+        }
+      }
+    }
+    __syncwarp();
+    uint32_t ne = 0;
+    for (uint32_t r = lane; r < m; r += 32) ne += reg[r] != kEmpty;
+    ne = __reduce_add_sync(0xffffffffu, ne);
+    uint8_t *ca = a.codesA + c * a.mpad, *cb = a.codesB + c * a.mpad;
+    for (uint32_t r = lane; r < (uint32_t)a.mpad; r += 32) {
+      if (r >= m) {                                    // padding never matches
+        ca[r] = 0;
+        cb[r] = 0xFF;
+        continue;
+      }
+      uint32_t v = reg[r];
+      if (ne == 0) {
+        v = 0;
+      } else if (v == kEmpty) {
+        // densify: the shared probe sequence of bucket r
+        const uint64_t pb = oph_fmix((uint64_t)r, seed ^ 0xA5A5A5A5DEADBEEFull);
+        const uint64_t step = oph_fmix((uint64_t)r, seed ^ 0x123456789ABCDEF0ull) | 1ull;
+        uint64_t cur = pb;
+        v = 0;
+        for (uint32_t t = 1; t <= m; ++t) {
+          cur += step;
+          const uint32_t x = reg[oph_bucket(cur, m)];
+          if (x != kEmpty) {
+            v = x ^ (uint32_t)oph_fmix((uint64_t)t, 0x9E3779B97F4A7C15ull);
+            break;
+          }
+        }
+      }
+      const uint8_t code = (uint8_t)((v & vmask) + 1u);
+      ca[r] = code;
+      cb[r] = code;
+    }
+    __syncwarp();
+  }
+}
+
+}  // namespace
+
+namespace {
+// Bucket values (code - 1) of n code rows, m per row, packed.
+__global__ void k_oph_values(const uint8_t *__restrict__ codes, int64_t n, int m, int mpad,
+                             uint8_t *__restrict__ out) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * m) return;
+  const int64_t i = t / m, r = t - i * m;
+  out[t] = (uint8_t)(codes[i * mpad + r] - 1u);
+}
+}  // namespace
+
+void launch_oph_values(const uint8_t *codes, int64_t n, int m, int mpad, uint8_t *out,
+                       cudaStream_t s) {
+  if (n <= 0) return;
+  const int64_t tot = n * m;
+  k_oph_values<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(codes, n, m, mpad, out);
+}
+
+void launch_oph(const SketchArgs &a, int K, int bits, uint64_t seed, cudaStream_t s) {
+  if (a.n == 0) return;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const size_t smem = (size_t)kOphWarps * a.m * sizeof(uint32_t);
+  smem_cap_max((const void *)k_oph);
+  const int64_t blocks = (a.n + kOphWarps - 1) / kOphWarps;
+  const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(blocks, (int64_t)sms * 8));
+  k_oph<<<(unsigned)grid, kOphWarps * 32, smem, s>>>(a, K, bits, seed);
+}
+
 }  // namespace rbg

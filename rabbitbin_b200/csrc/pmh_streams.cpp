@@ -250,6 +250,18 @@ std::shared_ptr<const PmhTables> pmh_tables(int k, int m, uint64_t seed, int con
   return it->second;
 }
 
+// Similarity of c equal buckets of m under the one-permutation metric:
+// jaccard_raw's matches / m (src/rabbitbin.cpp:1035-1130), as graph_sim returns
+// it (:1423-1425; no baseline, no clamp).
+void oph_sv_table(int m, std::vector<double> &sv_d, std::vector<float> &sv_f) {
+  sv_d.resize(m + 1);
+  sv_f.resize(m + 1);
+  for (int c = 0; c <= m; ++c) {
+    sv_d[c] = (double)(uint64_t)c / (double)(uint32_t)m;
+    sv_f[c] = (float)sv_d[c];
+  }
+}
+
 void sv_table(int m, bool base_on, double b0, std::vector<double> &sv_d,
               std::vector<float> &sv_f) {
   const double inv_m = 1.0 / (double)m;

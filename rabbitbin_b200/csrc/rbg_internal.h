@@ -53,6 +53,8 @@ std::shared_ptr<const PmhTables> pmh_tables(int k, int m, uint64_t seed, int con
 
 // The reference's similarity of a winner-match count, as a float and its
 // double (pmh_sv_from_count, src/rabbitbin.cpp:1297-1305).
+// Similarity by equal-bucket count of the one-permutation metric: c / m.
+void oph_sv_table(int m, std::vector<double> &sv_d, std::vector<float> &sv_f);
 void sv_table(int m, bool base_on, double b0, std::vector<double> &sv_d,
               std::vector<float> &sv_f);
 
@@ -92,6 +94,15 @@ void launch_count(const SketchArgs &a, cudaStream_t s);
 void launch_minreduce(const SketchArgs &a, cudaStream_t s);
 // codesB from codesA over `bytes` (a multiple of 16): equal codes, 0xFF for unset.
 void launch_codes_b(const uint8_t *codesA, uint8_t *codesB, int64_t bytes, cudaStream_t s);
+// One-permutation MinHash codes of contigs [0, a.n) (a.packed, a.nmask,
+// a.offsets, a.m buckets, a.mpad) into a.codesA / a.codesB: each bucket's low
+// `bits` bits + 1, padding 0 / 0xFF.  K: k-mer size (1..32).
+void launch_oph(const SketchArgs &a, int K, int bits, uint64_t seed, cudaStream_t s);
+// Bucket values (code - 1) of n OPH code rows into out[n][m].
+void launch_oph_values(const uint8_t *codes, int64_t n, int m, int mpad, uint8_t *out,
+                       cudaStream_t s);
+// Seed of rabbit_sketch::KmerSketch as rb_cmd_bin constructs it (default, 42).
+constexpr uint64_t kOphSeed = 42;
 
 struct GraphArgs {
   int64_t n = 0;

@@ -1,0 +1,68 @@
+"""The one-permutation MinHash metric (RABBIT_PMH=0) on the device: bucket
+values against the reference's own KmerSketch (src/rabbit_sketch.h) bit for
+bit, and the small-path graph with that metric against the reference's
+rb_cmd_bin sequence (graph_sim -> jaccard_raw, no baseline) compiled in the
+harness: edges, sComp, edge scores and the calibrated cutoff identical."""
+import numpy as np
+import pytest
+
+import oracle
+from rabbitbin_b200 import api
+from rabbitbin_b200.synth import make_assembly
+
+from test_oph_cpu import _fuzz
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("m,K,bits", [(500, 8, 2), (2, 1, 1), (64, 4, 1), (130, 15, 3),
+                                      (1000, 21, 2), (4096, 12, 2), (250, 32, 7)])
+def test_oph_signature_bit_exact(gpu_ctx, ref_lib, m, K, bits):
+    cat, offs = _fuzz(m + K)
+    p = api.default_params(m=m, oph_k=K, oph_bits=bits)
+    got = gpu_ctx.build_oph_signature(cat, offs, p)
+    want = ref_lib.oph_values(cat, offs, m, K, bits)
+    assert np.array_equal(got, want)
+
+
+def test_oph_signature_assembly(gpu_ctx, ref_lib):
+    asm = make_assembly(10, 1500, 0, seed=77)
+    buf, offs = asm.concat()
+    p = api.default_params(m=500, oph_k=8, oph_bits=2)
+    assert np.array_equal(gpu_ctx.build_oph_signature(buf, offs, p),
+                          ref_lib.oph_values(buf, offs, 500, 8, 2))
+
+
+@pytest.mark.parametrize("S,m,bits", [(0, 500, 2), (1, 500, 2), (5, 500, 2), (10, 1000, 1),
+                                      (5, 250, 3)])
+def test_oph_graph_small_path(gpu_ctx, ref_lib, S, m, bits):
+    asm = make_assembly(20, 2000, S, seed=90 + S, absent_frac=0.1 if S > 2 else 0.0)
+    buf, offs = asm.concat()
+    op = oracle.default_params(asm.n, m, S, oph_k=8, oph_bits=bits)
+    want = ref_lib.run_graph_oph(op, buf, offs, asm.depth)
+    got = gpu_ctx.bin_graph(buf, offs, asm.depth, api.default_params(m=m, oph_k=8, oph_bits=bits))
+    assert got["path"] == 1 and got["b0"] == 0.0 == want["b0"]
+    assert got["sim_cutoff"] == want["sim_cutoff"]
+    ws, wd, wsc, wsw = oracle.sorted_edges(want)
+    assert np.array_equal(got["src"], ws) and np.array_equal(got["dst"], wd), \
+        f"edge sets differ: {len(got['src'])} vs {len(ws)}"
+    assert np.array_equal(got["scomp"], wsc)
+    assert np.array_equal(got["score"], wsw)
+    assert len(ws) > 0
+
+
+def test_oph_unsupported_forms(gpu_ctx):
+    asm = make_assembly(10, 3000, 5, seed=5)
+    buf, offs = asm.concat()
+    p = api.default_params(oph_k=8, force_path=2)
+    with pytest.raises(api.RbgError) as e:                 # large-N path of the metric
+        gpu_ctx.bin_graph(buf, offs, asm.depth, p)
+    assert e.value.code == -4
+    with pytest.raises(api.RbgError) as e:                 # batch form: ProbMinHash only
+        gpu_ctx.bin_batch([(buf, offs, asm.depth, api.default_params(oph_k=8))])
+    assert e.value.code == -4
+    with pytest.raises(api.RbgError):                      # winner rows are ProbMinHash
+        gpu_ctx.build_pmh_winners(buf, offs, api.default_params(oph_k=8))
+    # the context stays usable
+    g = gpu_ctx.bin_graph(buf, offs, asm.depth, api.default_params(oph_k=8))
+    assert g["path"] == 1
