@@ -44,6 +44,7 @@ FRAGMENTS = [
     ("frag_calib_converge.inc", "impl/rb_graph.cpp", 390, 415),
     ("frag_fused_graph.inc", "impl/rb_graph.cpp", 489, 1356),
     ("frag_calibrate.inc", "impl/rb_graph.cpp", 1362, 1384),
+    ("frag_calibrate_fused.inc", "impl/rb_graph.cpp", 1386, 1438),
 ]
 
 

@@ -163,6 +163,7 @@ static inline void rb_fill_tnf(const char *, size_t, float *) { abort(); }
 #include "frag_calib_converge.inc"  // src/impl/rb_graph.cpp:390-415
 #include "frag_fused_graph.inc"     // src/impl/rb_graph.cpp:480-1356
 #include "frag_calibrate.inc"       // src/impl/rb_graph.cpp:1362-1384
+#include "frag_calibrate_fused.inc" // src/impl/rb_graph.cpp:1386-1438
 
 // ═════════════════════════════════════════════════════════════════════════════
 // C entry points used by the tests and the CPU baseline.
@@ -443,10 +444,13 @@ static int run_graph_body(const RefParams *p, const uint32_t *winners32,
   Graph g(nobs);
   double simCutoff = 0.0;
   const bool fused = (p->force_path == 2) || (p->force_path == 0 && nobs > 25000);
-  if (fused) {
+  if (fused && g_pmh_mode) {
     simCutoff = gen_fused_calib_graph(g, p->coverage);
   } else {
-    simCutoff = (double)calibrate_sim_cutoff(p->coverage, true);
+    // small N, or the one-permutation metric at large N (calibration on ten
+    // 2500-contig samples, then the same all-pairs build), :5035-5054
+    simCutoff = fused ? (double)calibrate_sim_cutoff_fused(p->coverage)
+                      : (double)calibrate_sim_cutoff(p->coverage, true);
     build_graph_allpairs(g, simCutoff / 1000.);
   }
 

@@ -902,7 +902,8 @@ void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
     std::vector<float> sv_f;
     sv_table(a.m, a.p->base_on != 0, a.p->base_on ? (double)b0f[b] : 0.0, sv_d, sv_f);
     const uint32_t *mc = (a.fused ? h_maxc : h_maxc + rows1) + a.row0;
-    cut[b] = calibrate_cutoff(mc, a.n, a.fused, a.m, sv_d, sv_f, a.p->coverage, a.p->seed);
+    cut[b] = calibrate_cutoff(mc, a.n, a.fused ? CalibMode::fused : CalibMode::all, a.m, sv_d,
+                              sv_f, a.p->coverage, a.p->seed);
   };
   {
     const int nt = std::max(1, std::min<int>(nb, (int)std::thread::hardware_concurrency()));

@@ -65,11 +65,11 @@ void rand_prefix_of_iota(size_t n, size_t count, std::vector<size_t> &val,
 
 }  // namespace
 
-double calibrate_cutoff(const uint32_t *maxc, int64_t n, bool fused, int m,
+double calibrate_cutoff(const uint32_t *maxc, int64_t n, CalibMode mode, int m,
                         const std::vector<double> &sv_d, const std::vector<float> &sv_f,
                         double coverage, unsigned seed) {
   CRand rnd(seed);
-  if (!fused) {
+  if (mode == CalibMode::all) {
     // random_unique over all n contigs: only its rand() calls matter here,
     // the maxima are counted, not ordered
     for (int64_t left = n; left > 0; --left) (void)(rnd() % left);
@@ -83,6 +83,21 @@ double calibrate_cutoff(const uint32_t *maxc, int64_t n, bool fused, int m,
   std::vector<uint32_t> stamp((size_t)n, 0);
   for (size_t r = 0; r < NR; ++r)
     rand_prefix_of_iota((size_t)n, SAMP, val, stamp, (uint32_t)(r + 1), rnd, idxs[r]);
+  if (mode == CalibMode::samples_all) {
+    // every (round, slot) holds its contig's maximum over all others, as a
+    // double similarity (Similarity); each round converges on its own
+    std::vector<int64_t> hist(m + 1);
+    double sum_p = 0;
+    for (size_t r = 0; r < NR; ++r) {
+      std::fill(hist.begin(), hist.end(), 0);
+      for (size_t li = 0; li < SAMP; ++li) ++hist[maxc[idxs[r][li]]];
+      double mp = (double)converge_hist(hist, sv_d, (int64_t)SAMP, coverage, rnd);
+      if (mp < 51.0) mp = 50.0;
+      sum_p += mp;
+      if (r == 1 && sum_p / 2 < 51.0) return 50.0;
+    }
+    return sum_p / (double)NR;
+  }
   // each sampled contig feeds the slot of the first round that drew it; a
   // slot holds sv_f of its maximum count (sv_f is non-decreasing, sv_f[0] = 0)
   std::vector<int8_t> sround((size_t)n, -1);

@@ -349,7 +349,9 @@ GraphArgs graph_args(rbg_ctx *c, const rbg_params *p) {
   c->maxc_all.ensure(n1 * sizeof(uint32_t));
   c->stats.ensure(2 * sizeof(unsigned long long));
   const double w_comp = (p->w_comp < 0.0) ? (S <= 2 ? 1.0 : 0.0) : p->w_comp;
-  const bool fused = (p->force_path == 2) || (p->force_path == 0 && n > 25000);
+  // the one-permutation metric has no fused path: its large-N route builds the
+  // small path's graph (only its calibration differs)
+  const bool fused = p->oph_k == 0 && ((p->force_path == 2) || (p->force_path == 0 && n > 25000));
   GraphArgs g;
   g.n = n; g.m = m; g.mpad = mpad; g.S = S; g.K = K; g.Su = Su;
   g.codesA = c->codesA.as<uint8_t>();
@@ -564,11 +566,13 @@ void run_graph(rbg_ctx *c, const rbg_params *p, const ShardCtx *sc = nullptr) {
                      c->stream));
   CK(cudaEventRecord(c->ev[5], c->stream));
 
-  const bool fused = (p->force_path == 2) || (p->force_path == 0 && n > 25000);
-  if (fused && n <= 2500) throw Error(RBG_ERR_ARG, "the fused path samples 2500 contigs; need n > 2500");
-  if (fused && oph)
-    throw Error(RBG_ERR_UNSUPPORTED, "the one-permutation metric runs the small path only "
-                                     "(n <= 25000 or force_path = 1)");
+  // N > 25000 (or force_path 2): the fused path of the ProbMinHash metric; the
+  // one-permutation metric keeps the small path's graph and calibrates on ten
+  // 2500-contig samples (calibrate_sim_cutoff_fused, src/impl/rb_graph.cpp:1386-1431)
+  const bool large = (p->force_path == 2) || (p->force_path == 0 && n > 25000);
+  const bool fused = large && !oph;
+  if (large && n <= 2500) throw Error(RBG_ERR_ARG, "the large-N path samples 2500 contigs; need n > 2500");
+  const CalibMode cmode = !large ? CalibMode::all : (oph ? CalibMode::samples_all : CalibMode::fused);
   c->path = fused ? 2 : 1;
   CK(cudaStreamWaitEvent(c->stream, c->ev_aux, 0));   // unit rows, anynz, column norms
   c->prep_done = false;
@@ -650,7 +654,7 @@ void run_graph(rbg_ctx *c, const rbg_params *p, const ShardCtx *sc = nullptr) {
   }
 
   // calibration on the host (rand() sequence of the reference)
-  const double simCutoff = calibrate_cutoff(maxc_host, n, fused, m, sv_d, sv_f, p->coverage, p->seed);
+  const double simCutoff = calibrate_cutoff(maxc_host, n, cmode, m, sv_d, sv_f, p->coverage, p->seed);
   c->sim_cutoff = simCutoff;
   CK(cudaEventRecord(c->ev[7], c->stream));
 

@@ -207,13 +207,19 @@ struct CRand {
   }
 };
 
+// Calibration of the similarity cutoff:
+//   all          calibrate_sim_cutoff over every contig (src/impl/rb_graph.cpp:1362-1384),
+//                the small path; maxc over all j != i
+//   fused        the sampling rounds of gen_fused_calib_graph (:505-522, per-round
+//                converge and mean); maxc over the candidates
+//   samples_all  calibrate_sim_cutoff_fused (:1386-1431), the large-N route of the
+//                one-permutation metric: ten 2500-contig samples, each sampled
+//                contig's maximum over all j != i
+enum class CalibMode { all, fused, samples_all };
+
 // The calibrated similarity cutoff (x1000) of one assembly from its per-row
-// maximum register-match counts (maxc over candidates for the fused path,
-// over all j != i for the small path) and its similarity tables:
-// calibrate_sim_cutoff (src/impl/rb_graph.cpp:1362-1384) for the small path,
-// the sampling rounds of gen_fused_calib_graph (:505-522, per-round converge
-// and mean) for the fused path.
-double calibrate_cutoff(const uint32_t *maxc, int64_t n, bool fused, int m,
+// maximum register-match counts and its similarity tables.
+double calibrate_cutoff(const uint32_t *maxc, int64_t n, CalibMode mode, int m,
                         const std::vector<double> &sv_d, const std::vector<float> &sv_f,
                         double coverage, unsigned seed);
 

@@ -1,8 +1,9 @@
 """The one-permutation MinHash metric (RABBIT_PMH=0) on the device: bucket
 values against the reference's own KmerSketch (src/rabbit_sketch.h) bit for
-bit, and the small-path graph with that metric against the reference's
-rb_cmd_bin sequence (graph_sim -> jaccard_raw, no baseline) compiled in the
-harness: edges, sComp, edge scores and the calibrated cutoff identical."""
+bit, and the graph with that metric (small path, and the large-N route with
+its sampled calibration) against the reference's rb_cmd_bin sequence
+(graph_sim -> jaccard_raw, no baseline) compiled in the harness: edges, sComp,
+edge scores and the calibrated cutoff identical."""
 import numpy as np
 import pytest
 
@@ -33,14 +34,13 @@ def test_oph_signature_assembly(gpu_ctx, ref_lib):
                           ref_lib.oph_values(buf, offs, 500, 8, 2))
 
 
-@pytest.mark.parametrize("S,m,bits", [(0, 500, 2), (1, 500, 2), (5, 500, 2), (10, 1000, 1),
-                                      (5, 250, 3)])
-def test_oph_graph_small_path(gpu_ctx, ref_lib, S, m, bits):
-    asm = make_assembly(20, 2000, S, seed=90 + S, absent_frac=0.1 if S > 2 else 0.0)
+def _oph_case(gpu_ctx, ref_lib, G, N, S, m, bits, seed, **kw):
+    asm = make_assembly(G, N, S, seed=seed, absent_frac=0.1 if S > 2 else 0.0)
     buf, offs = asm.concat()
-    op = oracle.default_params(asm.n, m, S, oph_k=8, oph_bits=bits)
+    op = oracle.default_params(asm.n, m, S, oph_k=8, oph_bits=bits, **kw)
     want = ref_lib.run_graph_oph(op, buf, offs, asm.depth)
-    got = gpu_ctx.bin_graph(buf, offs, asm.depth, api.default_params(m=m, oph_k=8, oph_bits=bits))
+    got = gpu_ctx.bin_graph(buf, offs, asm.depth,
+                            api.default_params(m=m, oph_k=8, oph_bits=bits, **kw))
     assert got["path"] == 1 and got["b0"] == 0.0 == want["b0"]
     assert got["sim_cutoff"] == want["sim_cutoff"]
     ws, wd, wsc, wsw = oracle.sorted_edges(want)
@@ -49,15 +49,26 @@ def test_oph_graph_small_path(gpu_ctx, ref_lib, S, m, bits):
     assert np.array_equal(got["scomp"], wsc)
     assert np.array_equal(got["score"], wsw)
     assert len(ws) > 0
+    return got
+
+
+@pytest.mark.parametrize("S,m,bits", [(0, 500, 2), (1, 500, 2), (5, 500, 2), (10, 1000, 1),
+                                      (5, 250, 3)])
+def test_oph_graph_small_path(gpu_ctx, ref_lib, S, m, bits):
+    _oph_case(gpu_ctx, ref_lib, 20, 2000, S, m, bits, seed=90 + S)
+
+
+@pytest.mark.parametrize("S", [0, 5, 20])
+def test_oph_graph_large_route(gpu_ctx, ref_lib, S):
+    """N > 25000 route of the metric (forced at 4000 contigs): the cutoff from
+    ten 2500-contig samples, then the small path's all-pairs graph."""
+    g = _oph_case(gpu_ctx, ref_lib, 30, 4000, S, 500, 2, seed=120 + S, force_path=2)
+    assert g["path"] == 1
 
 
 def test_oph_unsupported_forms(gpu_ctx):
     asm = make_assembly(10, 3000, 5, seed=5)
     buf, offs = asm.concat()
-    p = api.default_params(oph_k=8, force_path=2)
-    with pytest.raises(api.RbgError) as e:                 # large-N path of the metric
-        gpu_ctx.bin_graph(buf, offs, asm.depth, p)
-    assert e.value.code == -4
     with pytest.raises(api.RbgError) as e:                 # batch form: ProbMinHash only
         gpu_ctx.bin_batch([(buf, offs, asm.depth, api.default_params(oph_k=8))])
     assert e.value.code == -4
