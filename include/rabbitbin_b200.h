@@ -52,7 +52,7 @@ typedef struct rbg_params {
   int32_t k;              /* RABBIT_PMHK (4); 1..4 supported                       */
   int32_t m;              /* --sketch-m (500); 2..4096                             */
   uint64_t pmh_seed;      /* g_pmh_seed (42)                                       */
-  int32_t gc_norm;        /* RABBIT_GC_NORM (1); 0 and 1 supported                 */
+  int32_t gc_norm;        /* RABBIT_GC_NORM (1); 0, 1 and 2                        */
   int32_t win_bits;       /* RABBIT_WIN_BITS (16) or 32                            */
   double gc_norm_cap;     /* RABBIT_GC_NORM_CAP (20)                               */
   int32_t max_edges;      /* --max-edges (200)                                     */

@@ -202,7 +202,8 @@ void contig_winners(const char *seq, size_t len, int k, int m, uint64_t seed, in
     hist.assign(nb, 0);
     const uint64_t mask = nb - 1;
     uint64_t f = 0, r = 0, bc[4] = {0, 0, 0, 0};
-    int run = 0;
+    uint64_t dn[4][4] = {};           // consecutive valid bases (prev, next), mode 2
+    int run = 0, prevb = -1;
     size_t total = 0;
     for (size_t i = 0; i < len; ++i) {
       int b;
@@ -213,8 +214,10 @@ void contig_winners(const char *seq, size_t len, int k, int m, uint64_t seed, in
         case 't': b = 3; break;
         default: b = -1;
       }
-      if (b < 0) { run = 0; f = r = 0; continue; }
+      if (b < 0) { run = 0; f = r = 0; prevb = -1; continue; }
       bc[b]++;
+      if (prevb >= 0) dn[prevb][b]++;
+      prevb = b;
       f = ((f << 2) | (uint64_t)b) & mask;
       r = (r >> 2) | ((uint64_t)(3 - b) << (2 * (k - 1)));
       if (++run >= k) { hist[f <= r ? f : r]++; total++; }
@@ -229,6 +232,27 @@ void contig_winners(const char *seq, size_t len, int k, int m, uint64_t seed, in
         double w;
         if (gc_norm == 0) {
           w = (double)hist[v] * inv;
+        } else if (gc_norm == 2) {
+          // first-order Markov model (src/rabbitbin.cpp:1517-1554): base
+          // frequencies with pseudocount 1, P(next | prev) with Laplace
+          // pseudocount 1; bases[i] = (v >> 2i) & 3
+          double pm[4], pc[4][4];
+          for (int b = 0; b < 4; ++b)
+            pm[b] = vb > 0 ? ((double)bc[b] + 1.0) / ((double)vb + 4.0) : 0.25;
+          for (int x = 0; x < 4; ++x) {
+            double rs = 4.0;
+            for (int y = 0; y < 4; ++y) rs += (double)dn[x][y];
+            for (int y = 0; y < 4; ++y) pc[x][y] = ((double)dn[x][y] + 1.0) / rs;
+          }
+          int bs[8];
+          for (int q = 0; q < k; ++q) bs[q] = (int)((v >> (2 * q)) & 3);
+          double pf = pm[bs[0]];
+          for (int q = 1; q < k; ++q) pf *= pc[bs[q - 1]][bs[q]];
+          double pr = pm[3 - bs[k - 1]];
+          for (int q = 1; q < k; ++q) pr *= pc[3 - bs[k - q]][3 - bs[k - 1 - q]];
+          const double ex = pf + pr;
+          const double obs = (double)hist[v] * inv;
+          w = (ex > 1e-16) ? std::min(obs / ex, cap) : 0.0;
         } else {
           double pf = 1.0, pr = 1.0;
           uint64_t code = v;

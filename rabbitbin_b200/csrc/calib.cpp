@@ -164,7 +164,7 @@ void validate_params(const rbg_params *p) {
   if (p->k < 1 || p->k > 4) throw Error(RBG_ERR_UNSUPPORTED, "k must be in 1..4");
   if (p->m < 2 || p->m > kMaxM) throw Error(RBG_ERR_ARG, "m must be in 2..4096");
   if (p->win_bits != 16 && p->win_bits != 32) throw Error(RBG_ERR_ARG, "win_bits must be 16 or 32");
-  if (p->gc_norm != 0 && p->gc_norm != 1) throw Error(RBG_ERR_UNSUPPORTED, "gc_norm must be 0 or 1");
+  if (p->gc_norm < 0 || p->gc_norm > 2) throw Error(RBG_ERR_UNSUPPORTED, "gc_norm must be 0, 1 or 2");
   if (p->max_edges < 1 || p->max_edges > 448) throw Error(RBG_ERR_UNSUPPORTED, "max_edges must be in 1..448");
   if (!(p->coverage > 0.0 && p->coverage < 1.0)) throw Error(RBG_ERR_ARG, "coverage must be in (0,1)");
   if (p->oph_k < 0 || p->oph_k > 32) throw Error(RBG_ERR_ARG, "oph_k must be in 0..32");

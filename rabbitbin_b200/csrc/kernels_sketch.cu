@@ -95,6 +95,7 @@ __device__ __forceinline__ uint32_t spread16(uint32_t x) {
 // A lane takes one packed word (16 bases) per step, the 3 bases before it come
 // from the previous lane; base counts use popcounts over the 2-bit fields and a
 // shared table maps each k-mer code to its canonical code.
+template <bool GC2>                    // GC-norm mode 2 (dinucleotide model)
 __global__ void k_count(SketchArgs a) {
   extern __shared__ uint32_t sh_hist[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -110,6 +111,7 @@ __global__ void k_count(SketchArgs a) {
   const int64_t s = a.offsets[c], e = a.offsets[c + 1];
   const uint32_t kmask = (uint32_t)nb - 1u;
   uint32_t bc0 = 0, bc1 = 0, bc2 = 0, bc3 = 0;
+  uint32_t dn[GC2 ? 16 : 1] = {};      // mode 2: dinucleotides (prev, next) = dn[4 prev + next]
   if (e - s >= k) {
     const int64_t w0 = s >> 4, w1 = (e + 15) >> 4;
     uint32_t carry_word = 0, carry_bad = 0xFFFFu;     // word before w0: all invalid
@@ -133,6 +135,19 @@ __global__ void k_count(SketchArgs a) {
         bc2 += __popc(hi & ~lo & vs);
         bc1 += __popc(~hi & lo & vs);
         bc0 += __popc(~hi & ~lo & vs);
+        if constexpr (GC2) {
+          // consecutive valid bases (t-1, t); base -1 is the previous word's last
+          const uint32_t vprev = ((((~prevbad & 0xFFFFu) << 16) | (~bad & 0xFFFFu)) >> 1) & 0xFFFFu;
+          const uint32_t vp = spread16(~bad & vprev & 0xFFFFu);
+          const uint32_t q = (uint32_t)((((uint64_t)prev << 32) | cur) >> 2);
+          const uint32_t qh = (q >> 1) & 0x55555555u, ql = q & 0x55555555u;
+          const uint32_t mb[4] = {~hi & ~lo & vp, ~hi & lo & vp, hi & ~lo & vp, hi & lo & vp};
+          const uint32_t ma[4] = {~qh & ~ql, ~qh & ql, qh & ~ql, qh & ql};
+#pragma unroll
+          for (int x = 0; x < 4; ++x)
+#pragma unroll
+            for (int y = 0; y < 4; ++y) dn[4 * x + y] += __popc(ma[x] & mb[y]);
+        }
         // k-mers ending at base t: window bases t-k+1 .. t all valid; forward
         // codes are counted and folded onto canonical codes per contig
         const uint32_t winbad = (prevbad << 16) | bad;
@@ -183,6 +198,25 @@ __global__ void k_count(SketchArgs a) {
   p[2] = vb > 0 ? (double)bc2 / (double)vb : 0.25;
   p[3] = vb > 0 ? (double)bc3 / (double)vb : 0.25;
   const double inv = tot > 0 ? 1.0 / (double)tot : 0.0;
+  // mode 2 (src/rabbitbin.cpp:1517-1554): base frequencies with pseudocount 1,
+  // P(next | prev) with Laplace pseudocount 1
+  double pm[4], pc[GC2 ? 16 : 1];
+  if constexpr (GC2) {
+#pragma unroll
+    for (int x = 0; x < 16; ++x) dn[x] = __reduce_add_sync(0xffffffffu, dn[x]);
+    const uint32_t bcs[4] = {bc0, bc1, bc2, bc3};
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+      pm[b] = vb > 0 ? ((double)bcs[b] + 1.0) / ((double)vb + 4.0) : 0.25;
+#pragma unroll
+    for (int x = 0; x < 4; ++x) {
+      double rs = 4.0;
+#pragma unroll
+      for (int y = 0; y < 4; ++y) rs += (double)dn[4 * x + y];
+#pragma unroll
+      for (int y = 0; y < 4; ++y) pc[4 * x + y] = ((double)dn[4 * x + y] + 1.0) / rs;
+    }
+  }
   for (int v0 = 0; v0 < nb; v0 += 32) {
     const int v = v0 + lane;
     double w = 0.0;
@@ -191,6 +225,20 @@ __global__ void k_count(SketchArgs a) {
       if (cnt) {
         if (a.gc_norm == 0) {
           w = (double)cnt * inv;
+        } else if constexpr (GC2) {
+          // bases[i] = (v >> 2i) & 3; forward and reverse-complement chains
+          uint32_t bs[4];
+          for (int q = 0; q < k; ++q) bs[q] = ((uint32_t)v >> (2 * q)) & 3u;
+          double pf = pm[bs[0]];
+          for (int q = 1; q < k; ++q) pf = __dmul_rn(pf, pc[4 * bs[q - 1] + bs[q]]);
+          double pr = pm[3u - bs[k - 1]];
+          for (int q = 1; q < k; ++q) pr = __dmul_rn(pr, pc[4 * (3u - bs[k - q]) + (3u - bs[k - 1 - q])]);
+          const double obs = (double)cnt * inv;
+          const double ex = __dadd_rn(pf, pr);
+          if (ex > 1e-16) {
+            const double r = obs / ex;
+            w = (a.gc_cap < r) ? a.gc_cap : r;
+          }
         } else {
           double pf = 1.0, pr = 1.0;
           uint32_t code = (uint32_t)v;
@@ -490,7 +538,10 @@ void launch_count(const SketchArgs &a, cudaStream_t s) {
   // about eight contigs per warp: enough to even out the contig lengths
   const int64_t blocks = (a.n + warps - 1) / warps;
   const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(blocks, (int64_t)sms * 4));
-  k_count<<<(unsigned)grid, warps * 32, warps * 256 * sizeof(uint32_t), s>>>(a);
+  if (a.gc_norm == 2)
+    k_count<true><<<(unsigned)grid, warps * 32, warps * 256 * sizeof(uint32_t), s>>>(a);
+  else
+    k_count<false><<<(unsigned)grid, warps * 32, warps * 256 * sizeof(uint32_t), s>>>(a);
 }
 
 void smem_cap_max(const void *func) {

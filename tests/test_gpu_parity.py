@@ -53,7 +53,8 @@ def test_winners_bit_exact(gpu_ctx, orc, m):
     assert bad.size == 0, f"{len(bad)} registers differ, first {bad[:5]}"
 
 
-@pytest.mark.parametrize("k,gc", [(1, 1), (2, 1), (3, 1), (4, 0), (4, 1)])
+@pytest.mark.parametrize("k,gc", [(1, 1), (2, 1), (3, 1), (4, 0), (4, 1),
+                                  (1, 2), (2, 2), (3, 2), (4, 2)])
 def test_winners_k_and_gcnorm(gpu_ctx, orc, k, gc):
     asm = make_assembly(5, 80, 0, seed=7 * k + gc)
     buf, offs = _concat(_edge_cases() + asm.seqs)

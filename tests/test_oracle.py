@@ -37,7 +37,8 @@ def test_restated_winners_match_reference(ref_lib, orc, m):
     assert np.array_equal(orc.build_winners(buf, offs, m=m), ref_lib.build_winners(buf, offs, m=m))
 
 
-@pytest.mark.parametrize("k,gc", [(1, 1), (2, 1), (3, 0), (4, 0), (5, 1), (6, 1)])
+@pytest.mark.parametrize("k,gc", [(1, 1), (2, 1), (3, 0), (4, 0), (5, 1), (6, 1),
+                                  (2, 2), (3, 2), (4, 2), (6, 2)])
 def test_restated_winners_k_gc(ref_lib, orc, k, gc):
     asm = make_assembly(4, 40, 0, seed=10 + k)
     buf, offs = _concat(_edge_case_seqs() + asm.seqs)
