@@ -671,6 +671,8 @@ void run_graph(rbg_ctx *c, const rbg_params *p, const ShardCtx *sc = nullptr) {
   e.nbr_sv = c->nbr_sv.as<float>();
   e.nbr_cnt = c->nbr_cnt.as<int32_t>();
   e.row_edges = c->row_edges.as<int32_t>();
+  c->kept.ensure(n1 * ((K + 31) / 32) * sizeof(uint32_t));
+  e.kept = c->kept.as<uint32_t>();
   if (sc) {
     e.row_lo = sc->row_lo;
     e.row_hi = sc->row_hi;
@@ -845,11 +847,15 @@ void fetch(rbg_ctx *c, rbg_graph *out) {
     throw Error(RBG_ERR_NOMEM, "host allocation of the edge arrays failed");
   }
   if (ne) {
-    CK(cudaMemcpyAsync(out->from, c->e_from.p, ne * 4, cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaMemcpyAsync(out->to, c->e_to.p, ne * 4, cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaMemcpyAsync(out->scomp, c->e_scomp.p, ne * 4, cudaMemcpyDeviceToHost, c->stream));
+    // from, to and sComp are final once the edges are written (event 8): they
+    // come back on the copy stream while the edge weights are computed
+    CK(cudaStreamWaitEvent(c->copy, c->ev[8], 0));
+    CK(cudaMemcpyAsync(out->from, c->e_from.p, ne * 4, cudaMemcpyDeviceToHost, c->copy));
+    CK(cudaMemcpyAsync(out->to, c->e_to.p, ne * 4, cudaMemcpyDeviceToHost, c->copy));
+    CK(cudaMemcpyAsync(out->scomp, c->e_scomp.p, ne * 4, cudaMemcpyDeviceToHost, c->copy));
     CK(cudaMemcpyAsync(out->score, c->e_score.p, ne * 4, cudaMemcpyDeviceToHost, c->stream));
   }
+  CK(cudaStreamSynchronize(c->copy));
   CK(cudaStreamSynchronize(c->stream));
 }
 
@@ -1076,7 +1082,7 @@ int rbg_destroy(rbg_ctx *c) {
                   &c->badflag, &c->tmp, &c->cand_buf, &c->cand_cnt, &c->colacc, &c->unit16,
                   &c->sym_pairs, &c->sym_np, &c->sym_rowcnt, &c->sym_rowoff, &c->sym_keys,
                   &c->shard_send, &c->shard_recv, &c->oh_pres, &c->oh_map, &c->oh_koff,
-                  &c->oh_X, &c->oh_D, &c->oh_ws};
+                  &c->oh_X, &c->oh_D, &c->oh_ws, &c->kept};
   for (DBuf *b : bufs) b->release();
   if (c->tables) c->tables->release();
   release_batch_graphs(c);

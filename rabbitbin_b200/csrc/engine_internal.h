@@ -261,6 +261,7 @@ struct rbg_ctx {
   rbg::DBuf unit, unit16, anynz, colnorm, svbits, topk, topk_cnt, maxc_cand, maxc_all, stats;
   rbg::DBuf pairs, pair_out, nbr, nbr_sv, nbr_cnt, row_edges, cand_buf, cand_cnt;
   rbg::DBuf e_from, e_to, e_scomp, e_score, badflag, tmp, colacc;
+  rbg::DBuf kept;                        // kept-neighbour masks of the edge count
   // symmetric all-pairs pass: admitted pairs, per-row counts, offsets and keys
   rbg::DBuf sym_pairs, sym_np, sym_rowcnt, sym_rowoff, sym_keys;
   uint64_t sym_cap = 0;                  // pair-list capacity (grows when a pass overflows)

@@ -396,10 +396,13 @@ __device__ __forceinline__ void count_edges_row(const EmitArgs &e, int64_t i) {
   const int c = e.nbr_cnt[i];
   const uint32_t *ids = e.nbr_sorted + i * e.K;
   int cnt = 0;
+  const int kw = (e.K + 31) >> 5;
   for (int q0 = 0; q0 < c; q0 += 32) {
     const int q = q0 + lane;
     const bool ok = q < c && edge_kept(e, i, ids[q]);
-    cnt += __popc(__ballot_sync(FULL, ok));
+    const unsigned m = __ballot_sync(FULL, ok);
+    if (e.kept && lane == 0) e.kept[i * kw + (q0 >> 5)] = m;
+    cnt += __popc(m);
   }
   if (lane == 0) e.row_edges[i] = cnt;
 }
@@ -447,11 +450,17 @@ __device__ __forceinline__ void write_edges_row(const EmitArgs &e, int64_t i) {
   const int c = e.nbr_cnt[i];
   const uint32_t *ids = e.nbr_sorted + i * e.K;
   int64_t o = e.row_edges[i];
+  const int kw = (e.K + 31) >> 5;
   for (int q0 = 0; q0 < c; q0 += 32) {
     const int q = q0 + lane;
     const uint32_t j = q < c ? ids[q] : 0u;
-    const bool ok = q < c && edge_kept(e, i, j);
-    const unsigned m = __ballot_sync(FULL, ok);
+    unsigned m;
+    if (e.kept) {
+      m = e.kept[i * kw + (q0 >> 5)];              // recorded by the edge count
+    } else {
+      m = __ballot_sync(FULL, q < c && edge_kept(e, i, j));
+    }
+    const bool ok = (m >> lane) & 1u;
     if (ok) {
       const int64_t at = o + __popc(m & ((1u << lane) - 1u));
       e.from[at] = (uint32_t)i;

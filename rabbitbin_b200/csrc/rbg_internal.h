@@ -206,6 +206,10 @@ struct EmitArgs {
   int32_t *row_edges = nullptr;        // [n+1] edges per row, then exclusive scan
   uint32_t *from = nullptr, *to = nullptr;
   float *scomp = nullptr;
+  // optional [n][ceil(K/32)] bit masks: the edge count records which of a
+  // row's neighbours it kept, and the edge write reads them (null: the write
+  // tests each neighbour again)
+  uint32_t *kept = nullptr;
   // rows whose neighbour lists and edges the plain launchers produce:
   // [row_lo, row_hi), row_hi < 0 means n; row_edges is scanned over that range
   int64_t row_lo = 0, row_hi = -1;
