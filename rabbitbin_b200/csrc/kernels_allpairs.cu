@@ -126,7 +126,7 @@ __device__ __forceinline__ void compact_full_rows(Warp &w, int limit) {
   while (full) {
     const int r = __ffs(full) - 1;
     full &= full - 1;
-    const uint64_t P = select_topk(w.gbuf + (size_t)r * w.cap, w.cnt[r], w.K);
+    const uint64_t P = select_topk<false>(w.gbuf + (size_t)r * w.cap, w.cnt[r], w.K);
     if (lane == 0) { w.cnt[r] = w.K; w.thr[r] = P; }
     __syncwarp();
   }
