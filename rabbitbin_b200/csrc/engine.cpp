@@ -549,21 +549,42 @@ void run_graph(rbg_ctx *c, const rbg_params *p, const ShardCtx *sc = nullptr) {
 
   // b0 on the codes (equal codes <=> equal winners of the chosen width); the
   // one-permutation metric has no baseline (src/rabbitbin.cpp:4958)
+  // With the baseline on, b0 and the similarity table are made on the device
+  // (sample counts, median by histogram) and b0 comes back with the row maxima.
   const bool oph = p->oph_k > 0;
+  const bool dev_b0 = p->base_on && !oph;
   c->b0 = 0.0;
-  if (p->base_on && !oph) {
-    c->b0 = estimate_b0(c, n, m, [&](const int64_t *pr, int np, uint32_t *out) {
-      count_pairs_codes(c, mpad, m, pr, np, out);
-    });
-  }
   std::vector<double> sv_d;
   std::vector<float> sv_f;
-  if (oph) oph_sv_table(m, sv_d, sv_f);
-  else sv_table(m, p->base_on != 0, c->b0, sv_d, sv_f);
-  std::vector<uint32_t> sv_bits(m + 1);
-  std::memcpy(sv_bits.data(), sv_f.data(), (m + 1) * sizeof(uint32_t));
-  CK(cudaMemcpyAsync(c->svbits.p, sv_bits.data(), (m + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice,
-                     c->stream));
+  if (dev_b0) {
+    const auto prs = b0_pairs(n);
+    const int np = (int)(prs->size() / 2);
+    c->pairs.ensure(std::max<size_t>((size_t)np, 1) * 2 * sizeof(int64_t));
+    c->pair_out.ensure(std::max<size_t>((size_t)np, 1) * sizeof(uint32_t) + 16);
+    if (np) {
+      std::vector<int64_t> pr(prs->begin(), prs->end());
+      CK(cudaMemcpyAsync(c->pairs.p, pr.data(), pr.size() * sizeof(int64_t), cudaMemcpyHostToDevice,
+                         c->stream));
+      launch_pair_counts(c->codesA.as<uint8_t>(), c->codesB.as<uint8_t>(), mpad, m,
+                         c->pairs.as<int64_t>(), np, c->pair_out.as<uint32_t>(), c->stream);
+      c->launches++;
+    }
+    c->b0dev.ensure(sizeof(float));
+    launch_b0(c->pair_out.as<uint32_t>(), np, m, c->b0dev.as<float>(), c->svbits.as<uint32_t>(),
+              c->stream);
+    c->launches++;
+    // comes back with the row maxima (their read synchronises the stream)
+    c->b0pin.ensure(sizeof(float));
+    CK(cudaMemcpyAsync(c->b0pin.p, c->b0dev.p, sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  } else {
+    if (oph) oph_sv_table(m, sv_d, sv_f);
+    else sv_table(m, false, 0.0, sv_d, sv_f);
+    std::vector<uint32_t> sv_bits(m + 1);
+    std::memcpy(sv_bits.data(), sv_f.data(), (m + 1) * sizeof(uint32_t));
+    CK(cudaMemcpyAsync(c->svbits.p, sv_bits.data(), (m + 1) * sizeof(uint32_t),
+                       cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));               // sv_bits is a stack vector
+  }
   CK(cudaEventRecord(c->ev[5], c->stream));
 
   // N > 25000 (or force_path 2): the fused path of the ProbMinHash metric; the
@@ -653,6 +674,12 @@ void run_graph(rbg_ctx *c, const rbg_params *p, const ShardCtx *sc = nullptr) {
     maxc_host = maxc.data();
   }
 
+  if (dev_b0) {
+    // b0 as the device stored it (float; its copy completed with the maxima
+    // read), and the same tables on the host
+    c->b0 = (double)*c->b0pin.as<float>();
+    sv_table(m, true, c->b0, sv_d, sv_f);
+  }
   // calibration on the host (rand() sequence of the reference)
   const double simCutoff = calibrate_cutoff(maxc_host, n, cmode, m, sv_d, sv_f, p->coverage, p->seed);
   c->sim_cutoff = simCutoff;
@@ -1082,13 +1109,14 @@ int rbg_destroy(rbg_ctx *c) {
                   &c->badflag, &c->tmp, &c->cand_buf, &c->cand_cnt, &c->colacc, &c->unit16,
                   &c->sym_pairs, &c->sym_np, &c->sym_rowcnt, &c->sym_rowoff, &c->sym_keys,
                   &c->shard_send, &c->shard_recv, &c->oh_pres, &c->oh_map, &c->oh_koff,
-                  &c->oh_X, &c->oh_D, &c->oh_ws, &c->kept};
+                  &c->oh_X, &c->oh_D, &c->oh_ws, &c->kept, &c->b0dev};
   for (DBuf *b : bufs) b->release();
   if (c->tables) c->tables->release();
   release_batch_graphs(c);
   if (c->batch) c->batch->release();
   if (c->fasta) c->fasta->release();
   c->pin.release();
+  c->b0pin.release();
   c->shard_host.release();
   if (c->lt) cublasLtDestroy((cublasLtHandle_t)c->lt);
   c->lt = nullptr;

@@ -262,6 +262,8 @@ struct rbg_ctx {
   rbg::DBuf pairs, pair_out, nbr, nbr_sv, nbr_cnt, row_edges, cand_buf, cand_cnt;
   rbg::DBuf e_from, e_to, e_scomp, e_score, badflag, tmp, colacc;
   rbg::DBuf kept;                        // kept-neighbour masks of the edge count
+  rbg::DBuf b0dev;                       // b0 as made on the device (float)
+  rbg::HBuf b0pin;                       // and its pinned host copy
   // symmetric all-pairs pass: admitted pairs, per-row counts, offsets and keys
   rbg::DBuf sym_pairs, sym_np, sym_rowcnt, sym_rowoff, sym_keys;
   uint64_t sym_cap = 0;                  // pair-list capacity (grows when a pass overflows)

@@ -224,16 +224,18 @@ __global__ void k_pair_counts_batch(const BatchAsm *B, const int64_t *pair0s, in
   out[p] = c;
 }
 
-__global__ void k_b0_batch(const BatchAsm *B, const uint32_t *__restrict__ counts) {
+// b0 = the count at index np/2 of the sorted sample counts (a histogram of
+// the counts: the float match fractions sort as the counts do), then the
+// similarity table of pmh_sv_from_count.  One CTA.
+__device__ __forceinline__ void b0_body(const uint32_t *__restrict__ counts, int np, int m,
+                                        bool base_on_in, float *b0_out, uint32_t *sv_out) {
   extern __shared__ int hist[];
   __shared__ int med;
-  const BatchAsm &b = B[blockIdx.x];
-  const int m = b.g.m, np = b.np;
-  const bool on = b.base_on && np > 0;
+  const bool on = base_on_in && np > 0;
   if (on) {
     for (int c = threadIdx.x; c <= m; c += blockDim.x) hist[c] = 0;
     __syncthreads();
-    for (int q = threadIdx.x; q < np; q += blockDim.x) atomicAdd(&hist[counts[b.pair0 + q]], 1);
+    for (int q = threadIdx.x; q < np; q += blockDim.x) atomicAdd(&hist[counts[q]], 1);
     __syncthreads();
     if (threadIdx.x == 0) {
       int cum = 0, c = 0;
@@ -248,17 +250,27 @@ __global__ void k_b0_batch(const BatchAsm *B, const uint32_t *__restrict__ count
   const double inv_m = 1.0 / (double)m;
   const float b0f = on ? (float)__dmul_rn((double)(uint32_t)med, inv_m) : 0.0f;
   const double b0 = (double)b0f;
-  if (threadIdx.x == 0) *b.b0 = b0f;
+  if (threadIdx.x == 0) *b0_out = b0f;
   const double inv1mb0 = (b0 < 1.0) ? 1.0 / __dsub_rn(1.0, b0) : 1.0;
   for (int c = threadIdx.x; c <= m; c += blockDim.x) {
     double j = __dmul_rn((double)(uint32_t)c, inv_m);
-    if (b.base_on && b0 > 0.0 && b0 < 1.0) {
+    if (base_on_in && b0 > 0.0 && b0 < 1.0) {
       j = __dmul_rn(__dsub_rn(j, b0), inv1mb0);
       if (j < 0.0) j = 0.0;
     }
     if (j > 1.0 - 1e-6) j = 1.0 - 1e-6;
-    b.sv_out[c] = __float_as_uint((float)j);
+    sv_out[c] = __float_as_uint((float)j);
   }
+}
+
+__global__ void k_b0_batch(const BatchAsm *B, const uint32_t *__restrict__ counts) {
+  const BatchAsm &b = B[blockIdx.x];
+  b0_body(counts + b.pair0, b.np, b.g.m, b.base_on != 0, b.b0, b.sv_out);
+}
+
+__global__ void k_b0(const uint32_t *__restrict__ counts, int np, int m, float *b0_out,
+                     uint32_t *sv_out) {
+  b0_body(counts, np, m, true, b0_out, sv_out);
 }
 
 __host__ __device__ __forceinline__ int pow2_at_least(int x) {
@@ -600,6 +612,11 @@ void launch_colnorm(const GraphArgs &g, double *acc, cudaStream_t s) {
   cudaMemsetAsync(acc, 0, 3 * sizeof(double) * g.S, s);
   k_colsum_fast<<<296, 256, 0, s>>>(g, acc);
   k_colnorm<<<1, 256, 0, s>>>(g, acc);
+}
+
+void launch_b0(const uint32_t *counts, int np, int m, float *b0_out, uint32_t *sv_out,
+               cudaStream_t s) {
+  k_b0<<<1, 256, (size_t)(m + 1) * sizeof(int), s>>>(counts, np, m, b0_out, sv_out);
 }
 
 void launch_pair_counts(const uint8_t *A, const uint8_t *B, int mpad, int m,

@@ -155,6 +155,10 @@ inline uint64_t admission_floor() {
 
 void launch_unit_rows(const GraphArgs &g, cudaStream_t s);
 void launch_colnorm(const GraphArgs &g, double *acc, cudaStream_t s);
+// b0 from the np sample counts on the device (median by histogram) into
+// *b0_out (float, as stored) and the similarity table sv_out[m+1]; one CTA.
+void launch_b0(const uint32_t *counts, int np, int m, float *b0_out, uint32_t *sv_out,
+               cudaStream_t s);
 void launch_pair_counts(const uint8_t *codesA, const uint8_t *codesB, int mpad, int m,
                         const int64_t *pairs, int npairs, uint32_t *out, cudaStream_t s);
 void launch_allpairs(const GraphArgs &g, uint64_t *gbuf, int32_t *gcnt, cudaStream_t s);
