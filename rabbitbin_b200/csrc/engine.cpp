@@ -317,6 +317,7 @@ double estimate_b0(rbg_ctx *c, int64_t n, int m, const std::function<void(const 
 void count_pairs_codes(rbg_ctx *c, int mpad, int m, const int64_t *pr, int np, uint32_t *out) {
   c->pairs.ensure((size_t)np * 2 * sizeof(int64_t));
   c->pair_out.ensure((size_t)np * sizeof(uint32_t));
+  c->pairs_n = -1;                       // no longer the run_graph sample
   CK(cudaMemcpyAsync(c->pairs.p, pr, (size_t)np * 2 * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
   launch_pair_counts(c->codesA.as<uint8_t>(), c->codesB.as<uint8_t>(), mpad, m,
                      c->pairs.as<int64_t>(), np, c->pair_out.as<uint32_t>(), c->stream);
@@ -562,9 +563,12 @@ void run_graph(rbg_ctx *c, const rbg_params *p, const ShardCtx *sc = nullptr) {
     c->pairs.ensure(std::max<size_t>((size_t)np, 1) * 2 * sizeof(int64_t));
     c->pair_out.ensure(std::max<size_t>((size_t)np, 1) * sizeof(uint32_t) + 16);
     if (np) {
-      std::vector<int64_t> pr(prs->begin(), prs->end());
-      CK(cudaMemcpyAsync(c->pairs.p, pr.data(), pr.size() * sizeof(int64_t), cudaMemcpyHostToDevice,
-                         c->stream));
+      if (c->pairs_n != n) {              // the sample depends on n only: uploaded once per n
+        std::vector<int64_t> pr(prs->begin(), prs->end());
+        CK(cudaMemcpyAsync(c->pairs.p, pr.data(), pr.size() * sizeof(int64_t),
+                           cudaMemcpyHostToDevice, c->stream));
+        c->pairs_n = n;
+      }
       launch_pair_counts(c->codesA.as<uint8_t>(), c->codesB.as<uint8_t>(), mpad, m,
                          c->pairs.as<int64_t>(), np, c->pair_out.as<uint32_t>(), c->stream);
       c->launches++;
@@ -1193,6 +1197,7 @@ int rbg_estimate_pmh_baseline(rbg_ctx *c, const rbg_params *p, const void *winne
     if (bytes) CK(cudaMemcpyAsync(c->tmp.p, winners, bytes, cudaMemcpyHostToDevice, c->stream));
     *b0 = estimate_b0(c, n, m, [&](const int64_t *pr, int np, uint32_t *o) {
       c->pairs.ensure((size_t)np * 16);
+      c->pairs_n = -1;                   // no longer the run_graph sample
       c->pair_out.ensure((size_t)np * 4);
       CK(cudaMemcpyAsync(c->pairs.p, pr, (size_t)np * 16, cudaMemcpyHostToDevice, c->stream));
       launch_raw_pair_counts(c->tmp.p, win_bits, m, c->pairs.as<int64_t>(), np,

@@ -264,6 +264,7 @@ struct rbg_ctx {
   rbg::DBuf kept;                        // kept-neighbour masks of the edge count
   rbg::DBuf b0dev;                       // b0 as made on the device (float)
   rbg::HBuf b0pin;                       // and its pinned host copy
+  int64_t pairs_n = -1;                  // contig count whose b0 sample `pairs` holds
   // symmetric all-pairs pass: admitted pairs, per-row counts, offsets and keys
   rbg::DBuf sym_pairs, sym_np, sym_rowcnt, sym_rowoff, sym_keys;
   uint64_t sym_cap = 0;                  // pair-list capacity (grows when a pass overflows)
