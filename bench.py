@@ -47,7 +47,7 @@ METRIC = "contig-pairs scored/s"
 # a launch by its n(n-1)/2 pairs.
 ALLPAIRS_TRAFFIC_PER_PAIR = 0.145
 # Integer ALU pipe utilisation of the same kernel in the same capture.
-ALLPAIRS_ALU_PIPE_FRAC = 0.476
+ALLPAIRS_ALU_PIPE_FRAC = 0.504
 UNIT = "pairs/s"
 
 

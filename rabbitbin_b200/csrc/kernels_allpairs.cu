@@ -384,7 +384,10 @@ k_allpairs(GraphArgs g, uint64_t *gbuf, int32_t *gcnt, int cap, int P) {
 // lane: FP32 chain with its own band, then the AVX-512 order inside the band.
 constexpr float kTcDelta = 2.5e-3f;
 constexpr int kTCT = 16;          // columns per staged tile
-constexpr int kCQ = 512;          // check-queue ring entries per warp
+// check-queue ring entries per warp: at least 31 left over + 256 new ones
+// (32 rows x 8 columns) of one step; not a power of two, indexed modulo
+constexpr int kCQ = 320;
+constexpr int kTcWs = 768;        // per-warp workspace: thresholds, counts, maxima, survivors
 
 __device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0,
                                          uint32_t b1) {
@@ -418,7 +421,7 @@ __device__ __forceinline__ void check_batch(const GraphArgs &g, Warp &w, const S
                                             int SuP, const unsigned char *sA) {
   const int lane = threadIdx.x & 31;
   const bool act = lane < nq;
-  const unsigned e = act ? (unsigned)cq[(head + lane) & (kCQ - 1)] : 0u;
+  const unsigned e = act ? (unsigned)cq[(head + lane) % kCQ] : 0u;
   const int r = (int)(e >> 27);
   const int64_t j = e & 0x07FFFFFFu;
   const int64_t row = row0 + r;
@@ -482,13 +485,13 @@ __device__ __forceinline__ void tc_item(const GraphArgs &g, uint64_t *gbuf, int3
   const int Kp = KS * 16;
   const int cstride = Kp * 2 + 16;                 // bytes per staged column (conflict-free ldmatrix)
 
-  unsigned char *ws = smem + (size_t)warp * 1024;
+  unsigned char *ws = smem + (size_t)warp * kTcWs;
   uint64_t *thr = (uint64_t *)ws;
   int *cnt = (int *)(thr + 32);
   uint32_t *mxc = (uint32_t *)(cnt + 32);
   int *q = (int *)(mxc + 32);                      // [64] survivors to count
-  int *cq = (int *)(smem + (size_t)kWarps * 1024) + (size_t)warp * kCQ;      // check ring
-  unsigned char *rings = smem + (size_t)kWarps * 1024 + (size_t)kWarps * kCQ * 4;
+  int *cq = (int *)(smem + (size_t)kWarps * kTcWs) + (size_t)warp * kCQ;     // check ring
+  unsigned char *rings = smem + (size_t)kWarps * kTcWs + (size_t)kWarps * kCQ * 4;
   unsigned char *ring = rings + (size_t)warp * 2 * kTCT * cstride;
   // the block's 32 rows: register codes [32][mpad] and unit rows [32][Su]
   unsigned char *sA = rings + (size_t)kWarps * 2 * kTCT * cstride;
@@ -612,7 +615,7 @@ __device__ __forceinline__ void tc_item(const GraphArgs &g, uint64_t *gbuf, int3
           const int mt = b >> 2, i = b & 3;
           const int rr = mt * 16 + gq + 8 * (i >> 1);
           const int64_t jj = jt + c0 + 2 * tq + (i & 1);
-          cq[pos & (kCQ - 1)] = (int)(((unsigned)rr << 27) | (unsigned)jj);
+          cq[pos % kCQ] = (int)(((unsigned)rr << 27) | (unsigned)jj);
           ++pos;
         }
         tail += (unsigned)total;
@@ -665,7 +668,7 @@ k_allpairs_tc(GraphArgs g, uint64_t *gbuf, int32_t *gcnt, int cap, int P, float 
 // Symmetric pass: CTA x scores row block x and row block B-1-x (columns from
 // the block's first row on), so every CTA's column work is about n + 32.
 template <int KS, int SMAX>
-__global__ void __launch_bounds__(kWarps * 32)
+__global__ void __launch_bounds__(kWarps * 32, KS <= 2 ? 6 : 1)
 k_allpairs_tc_sym(GraphArgs g, int P, float lo, float hi, float lo16, SymOut o) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int64_t B = (g.n + 31) / 32;
@@ -890,7 +893,7 @@ size_t dense_smem(int mpad) {
 }
 
 size_t tc_smem(int KS, int mpad, int Su) {
-  return (size_t)kWarps * 1024 + (size_t)kWarps * kCQ * 4 +
+  return (size_t)kWarps * kTcWs + (size_t)kWarps * kCQ * 4 +
          (size_t)kWarps * 2 * kTCT * (KS * 16 * 2 + 16) + (size_t)32 * mpad +
          (size_t)32 * su_stride(Su) * 4;
 }
