@@ -668,7 +668,7 @@ k_allpairs_tc(GraphArgs g, uint64_t *gbuf, int32_t *gcnt, int cap, int P, float 
 // Symmetric pass: CTA x scores row block x and row block B-1-x (columns from
 // the block's first row on), so every CTA's column work is about n + 32.
 template <int KS, int SMAX>
-__global__ void __launch_bounds__(kWarps * 32, KS <= 2 ? 6 : 1)
+__global__ void __launch_bounds__(kWarps * 32, KS == 2 ? 6 : 1)
 k_allpairs_tc_sym(GraphArgs g, int P, float lo, float hi, float lo16, SymOut o) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int64_t B = (g.n + 31) / 32;
