@@ -41,30 +41,50 @@ WORKLOAD = dict(workload="binning-scale assembly: 100 genomes, 50000 contigs, S=
                 n_genomes=100, n_contigs=50000, samples=20, sketch_m=500, max_edges=200,
                 inputs_exceed_l2=True, seed=1)
 METRIC = "contig-pairs scored/s"
-# DRAM bytes (read + write) of the symmetric all-pairs kernel per unordered
-# pair, from the ncu capture of the 30,000-contig case
-# (profiles/k_allpairs_tc_sym_fused30k.md: 65.3 MB over 4.5e8 pairs), scaled to
-# a launch by its n(n-1)/2 pairs.
-ALLPAIRS_TRAFFIC_PER_PAIR = 0.145
-# Integer ALU pipe utilisation of the same kernel in the same capture.
-ALLPAIRS_ALU_PIPE_FRAC = 0.504
 UNIT = "pairs/s"
+# INT32 lanes per SM assumed for the integer peak of the all-pairs roofline
+# (SMs x lanes x sampled SM clock); the measured peaks carry no INT32 figure.
+INT32_LANES_PER_SM = 128
+# DRAM bytes (read + write) and integer ALU pipe share of one launch of the
+# symmetric all-pairs kernel on the default workload (50,000 contigs, S = 20),
+# from one ncu capture of that launch:
+#   ncu --clock-control none -k regex:k_allpairs_tc_sym -s 3 -c 1 --metrics
+#     dram__bytes_read.sum,dram__bytes_write.sum,sm__pipe_alu_cycles_active.avg.pct_of_peak_sustained_active
+#     python bench.py --steps 1 --warmup 3 --no-e2e --no-cpu-baseline
+# Reported only when the timed workload is that one.
+ALLPAIRS_NCU = {"contigs": 50000, "samples": 20, "dram_bytes": None, "alu_pipe_frac": None}
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled every 5 ms during a timed region
+    (NVML reads only; nvidia-smi at 50 ms when NVML is unavailable)."""
 
-    def __init__(self, index):
-        self.index, self.rows, self.proc = index, [], None
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "sw_power_cap": 0x4}
+
+    def __init__(self, index, period_s=0.005):
+        self.index, self.period, self.rows, self.proc, self.nvml = index, period_s, [], None, None
+        self.mx = None
 
     def __enter__(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.mx = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            self.nvml, self.h, self.stop = pynvml, h, threading.Event()
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return self
+        except Exception:
+            self.nvml = None
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -72,13 +92,37 @@ class ClockSampler:
             self.proc = None
         return self
 
+    def _poll(self):
+        nv = self.nvml
+        while not self.stop.is_set():
+            try:
+                sm = float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                rs = int(nv.nvmlDeviceGetCurrentClocksEventReasons(self.h))
+                self.rows.append((sm, rs))
+            except Exception:
+                pass
+            self.stop.wait(self.period)
+
     def _read(self):
         for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+            r = [x.strip() for x in line.split(",")]
+            try:
+                rs = sum(bit for (name, bit), v in zip(
+                    [("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40),
+                     ("sw_thermal_slowdown", 0x20), ("sw_power_cap", 0x4)], r[5:9])
+                    if v.lower() == "active")
+                self.mx = float(r[2])
+                self.rows.append((float(r[1]), rs))
+            except (ValueError, IndexError):
+                pass
 
     def __exit__(self, *a):
+        if self.nvml is not None:
+            self.stop.set()
+            self.t.join(timeout=2)
+            return
         if self.proc:
-            time.sleep(0.3)
+            time.sleep(0.1)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -86,19 +130,11 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in self.rows:
-            try:
-                sm.append(float(r[1]))
-                mx = float(r[2])
-                for n, v in zip(names, r[5:9]):
-                    if v.lower() == "active":
-                        reasons.add(n)
-            except (ValueError, IndexError):
-                pass
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        sm = [r[0] for r in self.rows]
+        reasons = sorted({n for _, rs in self.rows for n, b in self.REASONS.items() if rs & b})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.mx,
+                "reasons": reasons, "samples": len(sm),
+                "sampler": "nvml 5 ms" if self.nvml is not None else "nvidia-smi 50 ms"}
 
 
 def _peaks():
@@ -170,15 +206,16 @@ def run_b200(args):
     value = shard.whole_job_rate(pairs, world, ms / 1000.0)
 
     # ── end to end through rbg_bin_graph with pinned host inputs ────────────
-    e2e_ms, e2e_edges = float("nan"), 0
-    if args.no_e2e:
-        pin_seq = None
-    else:
-        e2e_ms, e2e_edges = _e2e(args, ctx, buf, offs, asm, params, barrier, world, dev)
+    e2e_ms, e2e_edges, e2e_clk = float("nan"), 0, None
+    if not args.no_e2e:
+        e2e_ms, e2e_edges, e2e_clk = _e2e(args, ctx, buf, offs, asm, params, barrier, world, dev)
     result_e2e = None if args.no_e2e else {
         "value": world * pairs / (e2e_ms / 1000.0), "unit": UNIT, "ms_per_step": e2e_ms,
         "h2d_bytes_per_step": int(len(buf) + offs.nbytes + asm.depth.nbytes),
-        "d2h_bytes_per_step": int(e2e_edges * 16)}
+        "d2h_bytes_per_step": int(e2e_edges * 16),
+        "time": "host clock around the rbg_bin_graph calls (each returns with its edges on "
+                "the host), barrier before and after, max over ranks",
+        "clocks": e2e_clk}
     last = timings[-1]
     return _finish(args, ctx, asm, timings, last, ms, value, result_e2e, clk, world, rank, dev)
 
@@ -197,33 +234,44 @@ def _e2e(args, ctx, buf, offs, asm, params, barrier, world, dev):
         g = ctx.bin_graph(seq_ptr, offs, pin_depth.numpy(), params)
     del g
     barrier()
-    t0 = time.perf_counter()
     e2e_edges = 0
-    for _ in range(args.steps):
-        g = ctx.bin_graph(seq_ptr, offs, pin_depth.numpy(), params)
-        e2e_edges = len(g["src"])
-    barrier()
+    with ClockSampler(int(dev.index or 0)) as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            g = ctx.bin_graph(seq_ptr, offs, pin_depth.numpy(), params)
+            e2e_edges = len(g["src"])
+        barrier()
+        wall = time.perf_counter() - t0
     from rabbitbin_b200 import shard
-    e2e_ms = shard.max_over_ranks((time.perf_counter() - t0) * 1000.0 / args.steps, world, dev)
-    return e2e_ms, e2e_edges
+    e2e_ms = shard.max_over_ranks(wall * 1000.0 / args.steps, world, dev)
+    return e2e_ms, e2e_edges, clk.summary()
 
 
 def _finish(args, ctx, asm, timings, last, ms, value, result_e2e, clk, world, rank, dev):
+    import torch
     peaks, peak_src = _peaks()
     clocks = clk.summary()
     n, S, m = asm.n, WORKLOAD["samples"], WORKLOAD["sketch_m"]
     mpad = (m + 15) // 16 * 16
     ap_ms = last["allpairs_ms"]
-    # dominant kernel: the symmetric all-pairs pass.  Its tensor-core prefilter
-    # multiplies the FP16 unit rank rows of every unordered pair once (2 S FLOPs
-    # per pair, n(n-1)/2 pairs per launch); the register compares of the
-    # survivors run on the integer pipe (pairs_compared x m byte compares).
+    sym = last["pairs_prefiltered"] > 0
+    # dominant kernel: the all-pairs pass.  Its algorithmic work is the register
+    # compare of every pair that reaches it: ceil(m/4) packed 32-bit word
+    # compares of 8-bit register codes per pair, against the INT32 issue rate
+    # of the SMs at the clock sampled during the timed region.
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    sm_mhz = clocks["sm_mhz"] or peaks.get("sm_max_mhz", 1965.0)
+    int_peak = sms * INT32_LANES_PER_SM * sm_mhz * 1e6 / 1e9          # Gop/s
     pairs_u = n * (n - 1) / 2.0
-    flops = 2.0 * S * pairs_u
-    achieved = flops / (ap_ms / 1000.0) / 1e12 if ap_ms > 0 else 0.0
-    peak = peaks.get("bf16_tflops", 1590.0)
-    traffic = (ALLPAIRS_TRAFFIC_PER_PAIR * pairs_u
-               if WORKLOAD["samples"] == 20 and last["pairs_prefiltered"] > 0 else None)
+    p_pmh = last["pairs_compared"] if sym else 2.0 * pairs_u
+    words = -(-m // 4)
+    int_ach = p_pmh * words / (ap_ms / 1000.0) / 1e9 if ap_ms > 0 else 0.0
+    # secondary: the FP16 tensor-core prefilter of the symmetric pass (2 S FLOPs
+    # per unordered pair)
+    tc_ach = 2.0 * S * pairs_u / (ap_ms / 1000.0) / 1e12 if ap_ms > 0 and sym else 0.0
+    tc_peak = peaks.get("bf16_tflops", 1590.0)
+    ncu_match = (n == ALLPAIRS_NCU["contigs"] and S == ALLPAIRS_NCU["samples"] and sym)
+    traffic = ALLPAIRS_NCU["dram_bytes"] if ncu_match else None
     # sketch: ASCII read, 2-bit words + invalid mask written and read back,
     # per-contig 1/w rows written and read, two code rows written
     nbases = sum(len(q) for q in asm.seqs)
@@ -240,36 +288,43 @@ def _finish(args, ctx, asm, timings, last, ms, value, result_e2e, clk, world, ra
         "stages_ms": {k: round(v, 4) for k, v in last.items() if k.endswith("_ms")},
         "pairs_prefiltered": last["pairs_prefiltered"],
         "pairs_compared": last["pairs_compared"],
-        "pairs_counted": "unordered (symmetric pass)" if S > 1 and n > 25000 else "ordered",
+        "pairs_counted": "unordered (symmetric pass)" if sym else "ordered",
         "gpu_launches": int(last["kernel_launches"]) * args.steps,
-        "roofline": {"bound": "tensor",
-                     "kernel": ("k_allpairs_tc_sym (FP16 mma prefilter + survivor compare, each pair once)"
-                                if last["pairs_prefiltered"] > 0 else
-                                "dense regime: one-hot int8 GEMM (cuBLASLt) + k_dense_select; "
-                                "FLOPs below are the FP16-prefilter equivalent"),
-                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak if peak else None,
-                     "peak_source": f"bf16_tflops of MEASURED_PEAKS.json ({peak_src})",
-                     "work": "2*S*n(n-1)/2 FLOPs per launch (FP16 products of every unordered pair)",
-                     "traffic": traffic},
-        "int_pipe": {"register_compares_per_s": last["pairs_compared"] * m / (ap_ms / 1000.0)
-                     if ap_ms > 0 else 0.0,
-                     "pairs_compared": last["pairs_compared"],
-                     "alu_pipe_frac_ncu": ALLPAIRS_ALU_PIPE_FRAC,
-                     "note": "integer ALU pipe busy fraction of the symmetric all-pairs kernel "
-                             "(ncu sm__pipe_alu_cycles_active, 30,000-contig capture, "
-                             "profiles/k_allpairs_tc_sym_fused30k.md): the kernel's own "
-                             "bound; the tensor-core FLOPs above are only its prefilter"},
+        "roofline": {
+            "bound": "int32",
+            "kernel": ("k_allpairs_tc_sym (FP16 prefilter, register compare of the survivors, "
+                       "each unordered pair once)" if sym else
+                       "dense regime: one-hot int8 contraction + row top-K"),
+            "achieved": int_ach, "peak": int_peak, "unit": "Gop/s",
+            "frac": int_ach / int_peak if int_peak else None,
+            "work": f"P_pmh x ceil(m/4) packed 32-bit register compares per launch "
+                    f"(P_pmh = {int(p_pmh)} pairs reaching the compare)",
+            "peak_source": f"{sms} SMs x {INT32_LANES_PER_SM} INT32 lanes x {sm_mhz:.0f} MHz "
+                           "(median SM clock sampled in the timed region; the measured peaks "
+                           "carry no INT32 figure)",
+            "time": "CUDA events around the all-pairs launch on its stream, last timed step",
+            "traffic": traffic,
+            "alu_pipe_frac_ncu": ALLPAIRS_NCU["alu_pipe_frac"] if ncu_match else None,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch "
+                              "on this workload" if ncu_match else None,
+            "secondary": {"bound": "tensor", "what": "FP16 prefilter, 2 S FLOPs per unordered pair",
+                          "achieved": tc_ach, "peak": tc_peak, "unit": "TFLOP/s",
+                          "frac": tc_ach / tc_peak if tc_peak else None,
+                          "peak_source": f"bf16_tflops of MEASURED_PEAKS.json ({peak_src})"}},
         "sketch": {"contigs_per_s": n / (sk_ms / 1000.0) if sk_ms > 0 else 0.0,
                    "ms": sk_ms, "bytes": sk_bytes,
                    "achieved_gbs": sk_bytes / (sk_ms / 1000.0) / 1e9 if sk_ms > 0 else 0.0,
                    "hbm_peak_gbs": peaks.get("hbm_gbs", 6650.0),
                    "frac_hbm": (sk_bytes / (sk_ms / 1000.0) / 1e9) / peaks.get("hbm_gbs", 6650.0)
-                   if sk_ms > 0 else 0.0},
+                   if sk_ms > 0 else 0.0,
+                   "peak_source": f"hbm_gbs of MEASURED_PEAKS.json ({peak_src})"},
         "clocks": clocks,
     }
+    ref_graph = None
     if rank == 0 and not args.no_cpu_baseline:
-        result["cpu_baseline"] = cpu_baseline(asm, seconds=args.cpu_seconds)
+        result["cpu_baseline"], ref_graph = cpu_baseline(asm, seconds=args.cpu_seconds)
+    if rank == 0 and (ref_graph is not None or args.check):
+        result["parity"] = parity(ctx.fetch_graph(), asm, ref_graph)
     ctx.close()
     from rabbitbin_b200 import shard
     shard.finish(world)
@@ -277,13 +332,20 @@ def _finish(args, ctx, asm, timings, last, ms, value, result_e2e, clk, world, ra
         print(json.dumps(result))
 
 
-def cpu_baseline(asm, seconds=20.0):
-    """RabbitBin's own CPU code on a bounded sample of the workload."""
+def _ref_lib():
     import oracle
     lib = oracle.ref()
-    kind = "reference"
     if lib is None:
-        lib, kind = oracle.restated(), "port"
+        return oracle.restated(), "port"
+    return lib, "reference"
+
+
+def cpu_baseline(asm, seconds=20.0):
+    """RabbitBin's own CPU code on a bounded sample of the workload (the first
+    50,000 contigs: the whole default workload).  Returns the baseline record
+    and, when the sample is the whole workload, the reference's graph."""
+    import oracle
+    lib, kind = _ref_lib()
     cores = os.cpu_count() or 1
     n = min(asm.n, 50000)
     buf, offs = asm.concat()
@@ -291,12 +353,41 @@ def cpu_baseline(asm, seconds=20.0):
     t0 = time.perf_counter()
     w = lib.build_winners(buf[:int(sub_offs[-1])], sub_offs, nthreads=cores)
     p = oracle.default_params(n, 500, asm.n_samples, force_path=2, nthreads=cores)
-    lib.run_graph(p, w, asm.depth[:n])
+    g = lib.run_graph(p, w, asm.depth[:n])
     dt = time.perf_counter() - t0
     pairs = n * (n - 1) // 2
-    return {"value": pairs / dt, "unit": UNIT, "cores": cores, "kind": kind,
-            "sample": f"{n} contigs of the workload (sketch + fused graph + weights), "
-                      f"one pass, {dt:.1f} s"}
+    return ({"value": pairs / dt, "unit": UNIT, "cores": cores, "kind": kind,
+             "sample": f"{n} contigs of the workload (sketch + fused graph + weights), "
+                       f"one pass, {dt:.1f} s"},
+            g if n == asm.n else None)
+
+
+def parity(got, asm, ref_graph=None):
+    """The timed workload's device graph against RabbitBin's own code on the
+    same inputs (run here when not given): edge set, sComp, weights, b0 and
+    cutoff identical; the weights' largest distance to the FP64 recomputation."""
+    import oracle
+    lib, kind = _ref_lib()
+    t0 = time.perf_counter()
+    if ref_graph is None:
+        buf, offs = asm.concat()
+        w = lib.build_winners(buf, offs)
+        ref_graph = lib.run_graph(oracle.default_params(asm.n, WORKLOAD["sketch_m"],
+                                                        asm.n_samples), w, asm.depth)
+    ref_s = time.perf_counter() - t0
+    s, d, sc, sw = oracle.sorted_edges(ref_graph)
+    order = np.lexsort((got["dst"], got["src"]))
+    same = (got["b0"] == ref_graph["b0"] and got["sim_cutoff"] == ref_graph["sim_cutoff"] and
+            len(order) == len(s) and
+            all(np.array_equal(np.asarray(got[k])[order], v)
+                for k, v in (("src", s), ("dst", d), ("scomp", sc), ("score", sw))))
+    rep = oracle.fp64_report(asm.depth, got)
+    return {"config": WORKLOAD["workload"], "against": f"{kind} ({'oracle/_ref' if kind == 'reference' else 'oracle port'})",
+            "identical": bool(same), "edges": int(len(order)), "b0": got["b0"],
+            "sim_cutoff": got["sim_cutoff"], "max_abs_err_fp64": rep["max_abs_err_fp64"],
+            "fp64_cut_disagreements": rep["cut_disagreements"],
+            "fp64_max_margin_disagreeing": rep["max_margin_disagreeing"],
+            "reference_s": round(ref_s, 2)}
 
 
 def run_shard_form(args):
@@ -609,6 +700,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--check", action="store_true",
+                    help="compare the device graph with the reference's on the whole workload "
+                         "(always done when the CPU baseline covers the whole workload)")
     ap.add_argument("--serve-modes", default="batched,plain",
                     help="serve form: which request loops replay the trace")
     ap.add_argument("--contigs", type=int, default=0, help="profiling: fewer contigs")

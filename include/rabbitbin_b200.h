@@ -125,6 +125,42 @@ int rbg_build_pmh_winners(rbg_ctx *ctx, const rbg_params *p, const char *seqcat,
                           const int64_t *offsets, int64_t n,
                           uint32_t *out_winners32);
 
+/* ── ProbMinHash4 sketches and queries (src/probmh.h:103-283) ────────────
+ * rbg_build_pmh_sketches: the ProbMinHash4(m, k, pmh_seed) sketch that
+ * build_pmh_winners builds per contig (src/rabbitbin.cpp:1436-1589), as
+ * ProbMinHash4::getWinners() (out_winners64 [n][m]: RNG state of the element
+ * that won each register, 0 unset; the out64 argument of build_pmh_winners)
+ * and ProbMinHash4::getRegisters() (out_registers [n][m]: register values,
+ * +inf unset).  Either output may be NULL.  The ProbMinHash metric only. */
+int rbg_build_pmh_sketches(rbg_ctx *ctx, const rbg_params *p, const char *seqcat,
+                           const int64_t *offsets, int64_t n, uint64_t *out_winners64,
+                           double *out_registers);
+
+/* Many-vs-many sketch comparison: out[i * nb + j] = metric(A_i, B_j) for row
+ * sets A [na][m] and B [nb][m], exactly as the ProbMinHash4 method of sketch
+ * A_i called on B_j:
+ *   RBG_PMH_JACCARD_WEIGHTED  jaccard_weighted (src/probmh.cpp:1364-1376):
+ *                             rows are winners (uint64_t), equal and nonzero
+ *   RBG_PMH_JACCARD           jaccard (:1325-1362): rows are register values
+ *                             (double), equal and finite
+ *   RBG_PMH_DISTANCE          distance (:1378-1385) = -ln(2J/(1+J)) / kmer_size
+ *   RBG_PMH_ANI               ani (:1404-1410) = (2J/(1+J))^(1/kmer_size)
+ * (J = jaccard for the last two; kmer_size is the sketch's k, 4 for the
+ * winners build_pmh_winners makes). */
+enum {
+  RBG_PMH_JACCARD_WEIGHTED = 0,
+  RBG_PMH_JACCARD = 1,
+  RBG_PMH_DISTANCE = 2,
+  RBG_PMH_ANI = 3
+};
+int rbg_pmh_compare(rbg_ctx *ctx, int32_t metric, int32_t m, int32_t kmer_size, const void *A,
+                    int64_t na, const void *B, int64_t nb, double *out);
+
+/* ProbMinHash4::merge (src/probmh.cpp:1416-1440) of n pairs of register rows:
+ * out[i][r] = min(A[i][r], B[i][r]) (the merged sketch's getRegisters()). */
+int rbg_pmh_merge_registers(rbg_ctx *ctx, const double *A, const double *B, int64_t n,
+                            int32_t m, double *out);
+
 /* One-permutation MinHash signatures (the RABBIT_PMH=0 metric): replaces
  * rabbit_sketch::KmerSketch(m, oph_k, oph_bits).update(seq, len) followed by
  * getSignature() (src/rabbit_sketch.h:197-285) for n contigs.  out[n][m]
@@ -325,13 +361,18 @@ int rbg_free_graph(rbg_graph *g);
  * intermediate lives in one static 24 MiB device array that the library
  * reserves on each GPU that loads it (held until exit).  seq_device is the
  * concatenated ASCII (16-byte aligned, readable up to a multiple of 16 bytes),
- * offsets_device the n+1 base offsets (offsets[0] == 0, offsets[n] == nbases),
- * winners_device n*m folded 32-bit winner rows.  Requests needing more scratch
- * than the array holds return RBG_ERR_ARG (message in errbuf) before any device
- * work.  The first call on a device looks up the array's address: make it
- * before any stream capture.  Calls share the array; calls that overlap on the
- * GPU race.  `stream` is a cudaStream_t (null: the default stream); the call
- * returns after the work has finished on it. */
+ * offsets_device the n+1 base offsets, which must start at 0, end at nbases
+ * and never decrease (checked on the device: RBG_ERR_ARG otherwise, before any
+ * sketch work), winners_device n*m folded 32-bit winner rows.  Parameters as
+ * rbg_build_pmh_winners: k 1..4, m 2..4096, gc_norm 0..2, the ProbMinHash
+ * metric only (oph_k = 0).  Requests needing more scratch than the array
+ * holds (roughly > 4,000 contigs or > 40 Mbp per call at m = 500) return
+ * RBG_ERR_ARG (message in errbuf) before any device work.  The first call on
+ * a device looks up the array's address.  Every call reads a check flag back
+ * and synchronises `stream`, so it must never be called while that stream is
+ * being captured.  Calls share the array; calls that overlap on the GPU race.
+ * `stream` is a cudaStream_t (null: the default stream); the call returns
+ * after the work has finished on it. */
 int rbg_build_pmh_winners_noalloc(const rbg_params *p, const char *seq_device,
                                   const int64_t *offsets_device, int64_t n, int64_t nbases,
                                   uint32_t *winners_device, void *stream, char *errbuf,

@@ -152,6 +152,24 @@ class _Lib:
                  _ptr(regs, C.c_double), _ptr(win, C.c_uint64))
         return regs, win
 
+    def pmh_metrics(self, ka, wa, kb, wb, m=500, seed=42, kmer=4):
+        """(jaccard_weighted, jaccard, distance, ani) of two ProbMinHash4
+        sketches built from element sets, by the reference's own methods
+        (harness only)."""
+        f = self.lib.ref_pmh_metrics
+        f.restype = None
+        f.argtypes = [C.POINTER(C.c_uint64), C.POINTER(C.c_double), C.c_int64,
+                      C.POINTER(C.c_uint64), C.POINTER(C.c_double), C.c_int64, C.c_uint32,
+                      C.c_uint64, C.c_int, C.POINTER(C.c_double)]
+        ka = np.ascontiguousarray(ka, np.uint64)
+        kb = np.ascontiguousarray(kb, np.uint64)
+        wa = np.ascontiguousarray(wa, np.float64)
+        wb = np.ascontiguousarray(wb, np.float64)
+        out = np.zeros(4, np.float64)
+        f(_ptr(ka, C.c_uint64), _ptr(wa, C.c_double), len(ka), _ptr(kb, C.c_uint64),
+          _ptr(wb, C.c_double), len(kb), m, seed, kmer, _ptr(out, C.c_double))
+        return tuple(out)
+
     def unit_dot_f(self, a, b):
         a = np.ascontiguousarray(a, dtype=np.float32)
         b = np.ascontiguousarray(b, dtype=np.float32)
@@ -237,3 +255,77 @@ def parse_fasta_restated(data, min_contig=2500, min_small=1000):
         lib._free(p)
     pairs = list(zip(names, seqs))
     return {"num_seqs": out.num_seqs, "large": pairs[:out.n_large], "small": pairs[out.n_large:]}
+
+
+def fp64_edge_weights(depth, src, dst, scomp, w_comp=-1.0, min_edge=0.70, neg_thr=-0.3,
+                      wjac_norm=True, chunk=1 << 20, margins=False):
+    """Edge weights in FP64 from the raw coverage (the tolerance oracle).
+
+    The edge-weight loop of src/rabbitbin.cpp:5482-5509 with depth_edge_term
+    (:930-970) in its default mode (RABBIT_DEPTH_SIM=2, fuse = min): average
+    ranks of each contig's S coverage values (src/ranker.h:55-66), centred and
+    L2-normalised (:4972-4988), their dot product as the rank correlation, the
+    weighted Jaccard of the column-normalised raw depths (:685-698, column norm
+    1/mean :4792-4809), dterm = min(max(rho, 0), clip(wJ)), w = a*sComp +
+    (1-a)*dterm with a = 1 for S <= 2 else 0 (auto_w_comp :470-473), cut to 0
+    when rho < neg_thr or w < min_edge.  Everything is evaluated in double,
+    nothing stored as float, so the device weights' distance to these values is
+    their FP32 error.  Returns float64[E] (sComp itself when S <= 1); with
+    margins=True also each edge's FP64 distance to the nearer cut threshold
+    (|w - min_edge|, |rho - neg_thr|)."""
+    from scipy.stats import rankdata
+    d = np.ascontiguousarray(depth, dtype=np.float32).astype(np.float64)
+    n = d.shape[0]
+    S = d.shape[1] if d.ndim == 2 else 0
+    scomp = np.asarray(scomp, dtype=np.float64)
+    if S <= 1:
+        return (scomp.copy(), np.full(len(scomp), np.inf)) if margins else scomp.copy()
+    r = rankdata(d, axis=1, method="average")
+    r -= r.mean(axis=1, keepdims=True)
+    ss = np.sqrt((r * r).sum(axis=1, keepdims=True))
+    u = np.divide(r, ss, out=np.zeros_like(r), where=ss > 0)
+    if wjac_norm:
+        mean = d.sum(axis=0) / max(n, 1)
+        cn = np.where(mean > 1e-12, 1.0 / np.where(mean > 1e-12, mean, 1.0), 0.0)
+    else:
+        cn = np.ones(S)
+    a = (1.0 if S <= 2 else 0.0) if w_comp < 0 else float(w_comp)
+    src = np.asarray(src, dtype=np.int64)
+    dst = np.asarray(dst, dtype=np.int64)
+    out = np.zeros(len(src), dtype=np.float64)
+    marg = np.full(len(src), np.inf)
+    for b in range(0, len(src), chunk):
+        i, j = src[b:b + chunk], dst[b:b + chunk]
+        rho = np.einsum("ij,ij->i", u[i], u[j])
+        x, y = d[i] * cn, d[j] * cn
+        mx = np.maximum(x, y).sum(axis=1)
+        wj = np.divide(np.minimum(x, y).sum(axis=1), mx, out=np.zeros_like(mx), where=mx > 0)
+        wj = np.clip(wj, 0.0, 1.0)
+        dterm = np.minimum(np.maximum(rho, 0.0), wj)
+        w = a * scomp[b:b + chunk] + (1.0 - a) * dterm
+        cut = (w < min_edge) | ((rho < neg_thr) if neg_thr > -0.99 else False)
+        out[b:b + chunk] = np.where(cut, 0.0, w)
+        mg = np.abs(w - min_edge)
+        if neg_thr > -0.99:
+            mg = np.minimum(mg, np.abs(rho - neg_thr))
+        marg[b:b + chunk] = mg
+    return (out, marg) if margins else out
+
+
+def fp64_report(depth, g, **kw):
+    """{max_abs_err_fp64, edges, cut_disagreements, max_margin_disagreeing} of
+    a graph's edge weights against fp64_edge_weights.  The error is taken over
+    the edges on whose cut the two agree.  cut_disagreements counts the edges
+    that one side keeps and the other cuts: values that sit on a threshold in
+    exact arithmetic (with S = 5 the rank correlation is a multiple of 1/20, so
+    0.70 is reached exactly), where the FP32 rounding decides, as it does in
+    the reference; max_margin_disagreeing is the largest FP64 distance of such
+    an edge to its threshold (at most the FP32 error when the cut is a tie)."""
+    fp, marg = fp64_edge_weights(depth, g["src"], g["dst"], g["scomp"], margins=True, **kw)
+    got = np.asarray(g["score"], dtype=np.float64)
+    agree = (fp > 0) == (got > 0)
+    err = np.abs(fp[agree] - got[agree])
+    dis = marg[~agree]
+    return {"max_abs_err_fp64": float(err.max()) if err.size else 0.0,
+            "edges": int(len(got)), "cut_disagreements": int((~agree).sum()),
+            "max_margin_disagreeing": float(dis.max()) if dis.size else 0.0}

@@ -507,6 +507,20 @@ float ref_unit_dot_f(const float *a, const float *b, uint32_t S) {
 
 // Full ProbMinHash4 state for one weighted element list (addHash order), for
 // kernel-level parity of registers and winners.
+// jaccard_weighted, jaccard, distance, ani of sketch A against sketch B (each
+// built by addHash over its elements), through ProbMinHash4's own methods.
+void ref_pmh_metrics(const uint64_t *ka, const double *wa, int64_t na, const uint64_t *kb,
+                     const double *wb, int64_t nb, uint32_t m, uint64_t seed, int kmer,
+                     double *out4) {
+  Sketch::ProbMinHash4 a(m, kmer, seed), b(m, kmer, seed);
+  for (int64_t t = 0; t < na; ++t) a.addHash(ka[t], wa[t]);
+  for (int64_t t = 0; t < nb; ++t) b.addHash(kb[t], wb[t]);
+  out4[0] = a.jaccard_weighted(b);
+  out4[1] = a.jaccard(b);
+  out4[2] = a.distance(b);
+  out4[3] = a.ani(b);
+}
+
 void ref_pmh_elements(const uint64_t *keys, const double *weights, int64_t ne,
                       uint32_t m, uint64_t seed, double *regs_out,
                       uint64_t *winners_out) {

@@ -129,6 +129,12 @@ def lib():
                                    P(C.c_uint32)], C.c_int),
         "rbg_build_oph_signature": ([vp, P(Params), C.c_char_p, i64p, C.c_int64,
                                      P(C.c_uint8)], C.c_int),
+        "rbg_build_pmh_sketches": ([vp, P(Params), C.c_char_p, i64p, C.c_int64,
+                                    P(C.c_uint64), P(C.c_double)], C.c_int),
+        "rbg_pmh_compare": ([vp, C.c_int32, C.c_int32, C.c_int32, vp, C.c_int64, vp,
+                             C.c_int64, P(C.c_double)], C.c_int),
+        "rbg_pmh_merge_registers": ([vp, P(C.c_double), P(C.c_double), C.c_int64, C.c_int32,
+                                     P(C.c_double)], C.c_int),
         "rbg_pack_win16": ([vp, P(C.c_uint32), C.c_int64, P(C.c_uint16)], C.c_int),
         "rbg_estimate_pmh_baseline": ([vp, P(Params), vp, C.c_int32, C.c_int64,
                                        P(C.c_double)], C.c_int),
@@ -280,6 +286,43 @@ class Context:
         out = np.zeros((n, p.m), np.uint32)
         self._check(self._L.rbg_build_pmh_winners(self._h, C.byref(p), seqcat, _p(offs, C.c_int64),
                                                   n, _p(out, C.c_uint32)), "build_pmh_winners")
+        return out
+
+    def build_pmh_sketches(self, seqcat, offsets, params=None):
+        """(winners64 [n, m] uint64, registers [n, m] float64) of every contig's
+        ProbMinHash4 sketch (rbg_build_pmh_sketches)."""
+        p = params or default_params()
+        offs = np.ascontiguousarray(offsets, np.int64)
+        n = len(offs) - 1
+        w = np.zeros((n, p.m), np.uint64)
+        r = np.zeros((n, p.m), np.float64)
+        self._check(self._L.rbg_build_pmh_sketches(self._h, C.byref(p), seqcat,
+                                                   _p(offs, C.c_int64), n, _p(w, C.c_uint64),
+                                                   _p(r, C.c_double)), "build_pmh_sketches")
+        return w, r
+
+    PMH_METRICS = {"jaccard_weighted": 0, "jaccard": 1, "distance": 2, "ani": 3}
+
+    def pmh_compare(self, metric, A, B, kmer_size=4):
+        """out[i, j] = metric(A_i, B_j) (rbg_pmh_compare); A, B: winner rows
+        (uint64) for jaccard_weighted, register rows (float64) otherwise."""
+        code = self.PMH_METRICS[metric]
+        dt = np.uint64 if code == 0 else np.float64
+        A = np.ascontiguousarray(A, dt)
+        B = np.ascontiguousarray(B, dt)
+        out = np.zeros((A.shape[0], B.shape[0]), np.float64)
+        self._check(self._L.rbg_pmh_compare(self._h, code, A.shape[1], kmer_size,
+                                            A.ctypes.data, A.shape[0], B.ctypes.data,
+                                            B.shape[0], _p(out, C.c_double)), "pmh_compare")
+        return out
+
+    def pmh_merge_registers(self, A, B):
+        A = np.ascontiguousarray(A, np.float64)
+        B = np.ascontiguousarray(B, np.float64)
+        out = np.zeros_like(A)
+        self._check(self._L.rbg_pmh_merge_registers(self._h, _p(A, C.c_double), _p(B, C.c_double),
+                                                    A.shape[0], A.shape[1], _p(out, C.c_double)),
+                    "pmh_merge_registers")
         return out
 
     def build_oph_signature(self, seqcat, offsets, params):

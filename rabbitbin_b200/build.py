@@ -19,7 +19,7 @@ CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SRCS = ["kernels_sketch.cu", "kernels_graph.cu", "kernels_allpairs.cu", "kernels_onehot.cu",
-           "kernels_util.cu",
+           "kernels_onehot_mma.cu", "kernels_pmh_query.cu", "kernels_util.cu",
            "noalloc.cu", "kernels_fasta.cu"]
 CPP_SRCS = ["pmh_streams.cpp", "calib.cpp", "engine.cpp", "batch.cpp", "server.cpp", "fasta.cpp"]
 HEADERS = ["rbg_internal.h", "engine_internal.h", "select_topk.cuh",
@@ -72,7 +72,7 @@ def build(verbose=False, ptxas_info=False):
         tmp = OUT + ".tmp"
         lib64 = os.path.join(CUDA, "lib64")
         _run([NVCC] + ARCH + ["-shared", "-o", tmp] + objs +
-             ["-cudart", "static", "-L" + lib64, "-lcublasLt", "-Xlinker", "-rpath=" + lib64])
+             ["-cudart", "static", "-L" + lib64, "-Xlinker", "-rpath=" + lib64])
         shutil.move(tmp, OUT)
     return OUT
 

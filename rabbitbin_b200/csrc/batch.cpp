@@ -173,9 +173,12 @@ int64_t batch_request_bytes(const rbg_params *p, int64_t n, int64_t nbases, int 
   b += n * (int64_t)K * (8 + 4 + 4) + n * 32;                    // top-K, neighbour lists
   if (abd)
     b += n * 256 * (16 + 2 * 8) + n * 12;                        // admitted pairs, keys, rows
-  else if (dense_on_gemm())
-    b += n * (int64_t)8192 + std::min<int64_t>(n * ((n + 3) / 4 * 4) * 4, (int64_t)2 << 30);
-                                                                 // one-hot rows, a count chunk
+  else if (dense_on_gemm()) {                                    // one-hot rows, candidate lists
+    int GR = 1, GC = 1;
+    onehot_mma_grid((int)((n + 255) / 256), (int)((n + 255) / 256), 148, &GR, &GC);
+    b += n * (int64_t)std::max(128, 136 * m / 8) +
+         ((n + 31) / 32) * 32 * GC * ((int64_t)onehot_mma_cap(K) * 8 + 4);
+  }
   else
     b += ((n + 31) / 32) * P * 32 * (cap * 8 + 4);               // slice candidate buffers
   b += n * (int64_t)K / 2 * 16;                                   // edge arrays (bound)
@@ -820,8 +823,8 @@ void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
       // b0 and similarity tables just computed
       for (int b = runcut[r]; b < runcut[r + 1]; ++b)
         if (L.at(b).gemm && L.at(b).n > 0) {
-          dense_allpairs_gemm(c, D[b].g);
-          launches += 5;
+          dense_allpairs_onehot(c, D[b].g);
+          launches += 6;
         }
     }
   }
@@ -863,6 +866,7 @@ void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
     });
     CK(cudaEventRecord(ev2, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    check_onehot_status(c);
     if (L.sym_rows == 0 || *h_np <= B.sym_cap) break;
     B.sym_cap = *h_np + *h_np / 4;
     B.sym_pairs.ensure(B.sym_cap * sizeof(uint4));
@@ -874,8 +878,8 @@ void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
     bool any = false;
     for (int b = 0; b < nb; ++b)
       if (L.at(b).gemm && L.at(b).n > 0) {
-        dense_allpairs_gemm(c, D[b].g);
-        launches += 5;
+        dense_allpairs_onehot(c, D[b].g);
+        launches += 6;
         any = true;
       }
     if (any && rows) {
@@ -884,6 +888,7 @@ void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
       CK(cudaMemcpyAsync(h_maxc + rows1, B.maxc_all.p, rows * sizeof(uint32_t),
                          cudaMemcpyDeviceToHost, c->stream));
       CK(cudaStreamSynchronize(c->stream));
+      check_onehot_status(c);
     }
   }
   if (autotune) {

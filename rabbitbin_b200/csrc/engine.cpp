@@ -2,6 +2,7 @@
 // steps that stay sequential by definition (b0 sampling with mt19937_64, the
 // rand()-driven cutoff calibration), and the C ABI of include/rabbitbin_b200.h.
 #include <algorithm>
+#include <limits>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -18,7 +19,6 @@
 #include <string>
 #include <vector>
 
-#include <cublasLt.h>
 
 #include "engine_internal.h"
 
@@ -284,8 +284,9 @@ void stage_sketch_chunked(rbg_ctx *c, const rbg_params *p, const char *seqcat,
   CK(cudaGetLastError());
 }
 
-void run_sketch(rbg_ctx *c, const rbg_params *p, bool want_winners) {
-  const SketchArgs a = sketch_setup(c, p, want_winners);
+void run_sketch(rbg_ctx *c, const rbg_params *p, bool want_winners, uint8_t *win_elem = nullptr) {
+  SketchArgs a = sketch_setup(c, p, want_winners);
+  a.win_elem = win_elem;
   CK(cudaEventRecord(c->ev[0], c->stream));
   prep_depth(c, p);
   launch_pack(c->ascii.as<char>(), c->nbases, c->packed.as<uint32_t>(), c->nmask.as<uint32_t>(),
@@ -446,23 +447,16 @@ void share_rows(rbg_ctx *c, const ShardCtx &sc, const void *src, void *dst, size
   scatter_blocks(c, sc, c->shard_recv.p, dst, elem);
 }
 
-#define LTCK(x)                                                                           \
-  do {                                                                                    \
-    const cublasStatus_t st_ = (x);                                                       \
-    if (st_ != CUBLAS_STATUS_SUCCESS)                                                     \
-      throw ::rbg::Error(RBG_ERR_CUDA, std::string(#x) + ": cuBLASLt status " +           \
-                                           std::to_string((int)st_));                     \
-  } while (0)
-
 // Dense regime (no abundance prune): the counts of rows [g.row_lo, row_hi)
-// against every contig as one-hot int8 GEMMs (cuBLASLt, int32 accumulation:
-// exact), in row chunks of at most 2 GiB of counts, each chunk scanned into
-// the rows' top-K keys, maxima and compared-pair count.
+// against every contig as the product of one-hot int8 rows on the tensor
+// cores (k_onehot_mma, int32 accumulation in TMEM: exact), consumed in the
+// kernel into per-(row, column group) candidate lists, the row maxima and the
+// compared-pair count; k_merge_topk then gives each row its top-K keys.
 }  // namespace
 
 namespace rbg {
 
-void dense_allpairs_gemm(rbg_ctx *c, const GraphArgs &g) {
+void dense_allpairs_onehot(rbg_ctx *c, const GraphArgs &g) {
   const int64_t n = g.n, lo = g.row_lo, hi = g.row_hi < 0 ? n : g.row_hi, rows = hi - lo;
   if (n == 0 || rows <= 0) return;
   const int m = g.m, mpad = g.mpad;
@@ -473,59 +467,44 @@ void dense_allpairs_gemm(rbg_ctx *c, const GraphArgs &g) {
   launch_code_presence(g.codesA, n, m, mpad, c->oh_pres.as<uint32_t>(), s);
   launch_onehot_map(c->oh_pres.as<uint32_t>(), m, c->oh_map.as<int32_t>(), c->oh_koff.as<int32_t>(),
                     s);
-  int32_t K = 0;
-  CK(cudaMemcpyAsync(&K, c->oh_koff.as<int32_t>() + m, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  int32_t K1 = 0;
+  CK(cudaMemcpyAsync(&K1, c->oh_koff.as<int32_t>() + m, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
-  const int64_t ldx = std::max<int64_t>(32, ((int64_t)K + 31) / 32 * 32);   // zero-padded width
-  // the int8 GEMMs take the contig dimension in multiples of 4: zero rows pad X
-  // to ldd contigs (their counts are 0 and never read)
-  const int64_t ldd = (n + 3) / 4 * 4;
-  c->oh_X.ensure((size_t)ldd * ldx);
+  // one-hot rows zero-padded to whole 128-byte chunks of the contraction
+  const int64_t ldx = std::max<int64_t>(128, ((int64_t)K1 + 127) / 128 * 128);
+  c->oh_X.ensure((size_t)n * ldx);
   launch_onehot_fill(g.codesA, n, m, mpad, c->oh_map.as<int32_t>(), c->oh_X.as<int8_t>(), ldx, s);
-  if (ldd > n)
-    CK(cudaMemsetAsync(c->oh_X.as<int8_t>() + n * ldx, 0, (size_t)(ldd - n) * ldx, s));
-  int64_t chunk = std::max<int64_t>(32, (((int64_t)1 << 29) / ldd) / 32 * 32);
-  if (chunk > rows) chunk = rows;
-  c->oh_D.ensure((size_t)chunk * ldd * sizeof(int32_t));
-  const size_t ws = (size_t)32 << 20;
-  c->oh_ws.ensure(ws);
-  if (!c->lt) LTCK(cublasLtCreate((cublasLtHandle_t *)&c->lt));
-  cublasLtHandle_t lt = (cublasLtHandle_t)c->lt;
-  cublasLtMatmulDesc_t op = nullptr;
-  cublasLtMatmulPreference_t pref = nullptr;
-  LTCK(cublasLtMatmulDescCreate(&op, CUBLAS_COMPUTE_32I, CUDA_R_32I));
-  const cublasOperation_t tA = CUBLAS_OP_T, tB = CUBLAS_OP_N;
-  LTCK(cublasLtMatmulDescSetAttribute(op, CUBLASLT_MATMUL_DESC_TRANSA, &tA, sizeof(tA)));
-  LTCK(cublasLtMatmulDescSetAttribute(op, CUBLASLT_MATMUL_DESC_TRANSB, &tB, sizeof(tB)));
-  LTCK(cublasLtMatmulPreferenceCreate(&pref));
-  LTCK(cublasLtMatmulPreferenceSetAttribute(pref, CUBLASLT_MATMUL_PREF_MAX_WORKSPACE_BYTES, &ws,
-                                            sizeof(ws)));
-  const int8_t *X = c->oh_X.as<int8_t>();
-  int32_t *D = c->oh_D.as<int32_t>();
-  for (int64_t q0 = 0; q0 < rows; q0 += chunk) {
-    const int64_t nr = std::min(chunk, rows - q0);
-    // column-major: X is ldx x n (a contig per column); D = X^T X_rows is n x nr,
-    // so row i's counts against every contig are contiguous
-    cublasLtMatrixLayout_t La = nullptr, Lb = nullptr, Ld = nullptr;
-    LTCK(cublasLtMatrixLayoutCreate(&La, CUDA_R_8I, ldx, ldd, ldx));
-    LTCK(cublasLtMatrixLayoutCreate(&Lb, CUDA_R_8I, ldx, nr, ldx));
-    LTCK(cublasLtMatrixLayoutCreate(&Ld, CUDA_R_32I, ldd, nr, ldd));
-    cublasLtMatmulHeuristicResult_t res;
-    int found = 0;
-    LTCK(cublasLtMatmulAlgoGetHeuristic(lt, op, La, Lb, Ld, Ld, pref, 1, &res, &found));
-    if (found < 1) throw Error(RBG_ERR_CUDA, "cuBLASLt found no int8 GEMM for the one-hot counts");
-    const int32_t alpha = 1, beta = 0;
-    LTCK(cublasLtMatmul(lt, op, &alpha, X, La, X + (lo + q0) * ldx, Lb, &beta, D, Ld, D, Ld,
-                        &res.algo, c->oh_ws.p, ws, s));
-    cublasLtMatrixLayoutDestroy(La);
-    cublasLtMatrixLayoutDestroy(Lb);
-    cublasLtMatrixLayoutDestroy(Ld);
-    launch_dense_select(g, D, ldd, lo + q0, nr, s);
-    c->launches += 2;
-  }
-  cublasLtMatmulPreferenceDestroy(pref);
-  cublasLtMatmulDescDestroy(op);
-  c->launches += 3;
+  int dev = 0, sms = 148;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  int GR = 1, GC = 1;
+  onehot_mma_grid((int)((rows + 255) / 256), (int)((n + 255) / 256), sms, &GR, &GC);
+  const int cap = onehot_mma_cap(g.K);
+  const size_t lists = (size_t)((rows + 31) / 32) * 32 * GC;
+  c->oh_cand.ensure(lists * cap * sizeof(uint64_t));
+  c->oh_cnt.ensure(lists * sizeof(int32_t));
+  c->oh_err.ensure(sizeof(int));
+  c->oh_errpin.ensure(sizeof(int));
+  // the status accumulates over the calls before the caller's next check
+  if (!c->oh_pending) CK(cudaMemsetAsync(c->oh_err.p, 0, sizeof(int), s));
+  const char *why = "";
+  const int rc = launch_onehot_mma(g, c->oh_X.as<int8_t>(), ldx, rows, c->oh_cand.as<uint64_t>(),
+                                   c->oh_cnt.as<int32_t>(), c->oh_err.as<int>(), GR, GC, s, &why);
+  if (rc != RBG_OK) throw Error(rc, std::string("one-hot tensor-core pass: ") + why);
+  launch_merge_topk(g, c->oh_cand.as<uint64_t>(), c->oh_cnt.as<int32_t>(), cap, GC, s);
+  // the kernel's wait status comes back with the caller's next synchronisation
+  CK(cudaMemcpyAsync(c->oh_errpin.p, c->oh_err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  c->oh_pending = true;
+  c->launches += 6;
+}
+
+void check_onehot_status(rbg_ctx *c) {
+  if (!c->oh_pending) return;
+  c->oh_pending = false;
+  const int e = *c->oh_errpin.as<int>();
+  if (e != 0)
+    throw Error(RBG_ERR_TIMEOUT, "one-hot tensor-core pass: a bounded device wait gave up (stage " +
+                                     std::to_string(e) + ")");
 }
 
 }  // namespace rbg
@@ -660,7 +639,7 @@ void run_graph(rbg_ctx *c, const rbg_params *p, const ShardCtx *sc = nullptr) {
     CK(cudaMemsetAsync(c->maxc_cand.p, 0, n1 * sizeof(uint32_t), c->stream));
     CK(cudaMemsetAsync(c->maxc_all.p, 0, n1 * sizeof(uint32_t), c->stream));
     if (!g.prefilter && dense_on_gemm()) {
-      dense_allpairs_gemm(c, g);                        // tensor cores, exact counts
+      dense_allpairs_onehot(c, g);                      // tensor cores, exact counts
     } else {
       const size_t slots = (size_t)((rows + 31) / 32) * allpairs_slices_rows(rows, n, K) * 32;
       c->cand_buf.ensure(std::max<size_t>(slots, 1) * allpairs_cap(K) * sizeof(uint64_t));
@@ -675,6 +654,7 @@ void run_graph(rbg_ctx *c, const rbg_params *p, const ShardCtx *sc = nullptr) {
     maxc.assign(n1, 0);
     CK(cudaMemcpyAsync(maxc.data(), dmax, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    check_onehot_status(c);
     maxc_host = maxc.data();
   }
 
@@ -1113,7 +1093,8 @@ int rbg_destroy(rbg_ctx *c) {
                   &c->badflag, &c->tmp, &c->cand_buf, &c->cand_cnt, &c->colacc, &c->unit16,
                   &c->sym_pairs, &c->sym_np, &c->sym_rowcnt, &c->sym_rowoff, &c->sym_keys,
                   &c->shard_send, &c->shard_recv, &c->oh_pres, &c->oh_map, &c->oh_koff,
-                  &c->oh_X, &c->oh_D, &c->oh_ws, &c->kept, &c->b0dev};
+                  &c->oh_X, &c->oh_cand, &c->oh_cnt, &c->oh_err, &c->kept, &c->b0dev,
+                  &c->qa, &c->qb, &c->qo, &c->qt};
   for (DBuf *b : bufs) b->release();
   if (c->tables) c->tables->release();
   release_batch_graphs(c);
@@ -1122,8 +1103,6 @@ int rbg_destroy(rbg_ctx *c) {
   c->pin.release();
   c->b0pin.release();
   c->shard_host.release();
-  if (c->lt) cublasLtDestroy((cublasLtHandle_t)c->lt);
-  c->lt = nullptr;
   for (auto &e : c->ev) cudaEventDestroy(e);
   cudaStreamSynchronize(c->aux);
   cudaStreamSynchronize(c->copy);
@@ -1329,6 +1308,126 @@ int rbg_pmh_stream_tables(int32_t k, int32_t m, uint64_t seed, int32_t contract,
   } catch (...) {
     return RBG_ERR_NOMEM;
   }
+}
+
+// ── ProbMinHash4 rows and queries ──────────────────────────────────────────
+// getWinners() / getRegisters() of the sketch build_pmh_winners makes per
+// contig (src/rabbitbin.cpp:1436-1589: ProbMinHash4(m, k, seed) with one
+// addHash per canonical k-mer), for n contigs.
+int rbg_build_pmh_sketches(rbg_ctx *c, const rbg_params *p, const char *seqcat,
+                           const int64_t *offsets, int64_t n, uint64_t *out_winners64,
+                           double *out_registers) {
+  return guarded(c, [&] {
+    validate(p);
+    if (p->oph_k > 0) throw Error(RBG_ERR_ARG, "ProbMinHash sketches need oph_k = 0");
+    if (n > 0 && !out_winners64 && !out_registers) throw Error(RBG_ERR_ARG, "null outputs");
+    stage(c, seqcat, offsets, n, nullptr, 0);
+    const int m = p->m;
+    c->tmp.ensure(std::max<size_t>((size_t)n * m, 16));
+    run_sketch(c, p, false, c->tmp.as<uint8_t>());
+    c->prep_done = false;
+    Tables &T = tables_for(c, p);
+    if (!T.rows_ready) {                 // winner states and U by element, once per table
+      const PmhTables &t = *T.t;
+      const size_t EM = (size_t)t.n_elems * t.m;
+      T.W64.ensure(EM * sizeof(uint64_t));
+      T.U.ensure(EM * sizeof(double));
+      CK(cudaMemcpyAsync(T.W64.p, t.W64.data(), EM * sizeof(uint64_t), cudaMemcpyHostToDevice,
+                         c->stream));
+      CK(cudaMemcpyAsync(T.U.p, t.U.data(), EM * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      T.rows_ready = true;
+    }
+    if (n) {
+      const size_t cells = (size_t)n * m;
+      c->qa.ensure(cells * sizeof(uint64_t) * (out_winners64 && out_registers ? 2 : 1));
+      uint64_t *dw = out_winners64 ? c->qa.as<uint64_t>() : nullptr;
+      double *dr = out_registers ? (double *)(c->qa.as<uint64_t>() + (dw ? cells : 0)) : nullptr;
+      launch_pmh_rows(c->tmp.as<uint8_t>(), c->elem_winv.as<double>(), n, m, T.t->n_elems,
+                      T.W64.as<uint64_t>(), T.U.as<double>(), dw, dr, c->stream);
+      CK(cudaGetLastError());
+      if (dw) CK(cudaMemcpyAsync(out_winners64, dw, cells * 8, cudaMemcpyDeviceToHost, c->stream));
+      if (dr) CK(cudaMemcpyAsync(out_registers, dr, cells * 8, cudaMemcpyDeviceToHost, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
+// Value of a comparison for every register-match count 0..m, with the
+// reference's formulas (src/probmh.cpp:1325-1414) on the host's libm.
+static std::vector<double> pmh_metric_table(int metric, int m, int kmer_size) {
+  std::vector<double> t((size_t)m + 1);
+  for (int c = 0; c <= m; ++c) {
+    const double j = static_cast<double>(c) / static_cast<double>(m);
+    double v = j;
+    if (metric == RBG_PMH_DISTANCE) {
+      if (j <= 0.0) v = std::numeric_limits<double>::infinity();
+      else if (j >= 1.0) v = 0.0;
+      else v = -std::log(2.0 * j / (1.0 + j)) / static_cast<double>(kmer_size);
+    } else if (metric == RBG_PMH_ANI) {
+      if (j <= 0.0) v = 0.0;
+      else if (j >= 1.0) v = 1.0;
+      else v = std::pow(2.0 * j / (1.0 + j), 1.0 / static_cast<double>(kmer_size));
+    }
+    t[c] = v;
+  }
+  return t;
+}
+
+int rbg_pmh_compare(rbg_ctx *c, int32_t metric, int32_t m, int32_t kmer_size, const void *A,
+                    int64_t na, const void *B, int64_t nb, double *out) {
+  return guarded(c, [&] {
+    if (metric < RBG_PMH_JACCARD_WEIGHTED || metric > RBG_PMH_ANI)
+      throw Error(RBG_ERR_ARG, "unknown ProbMinHash metric");
+    if (m < 2 || m > kMaxM || na < 0 || nb < 0 || kmer_size < 1)
+      throw Error(RBG_ERR_ARG, "m, row counts or k-mer size out of range");
+    if (na == 0 || nb == 0) return;
+    if (!A || !B || !out) throw Error(RBG_ERR_ARG, "null argument");
+    const std::vector<double> tab = pmh_metric_table(metric, m, kmer_size);
+    c->qt.ensure(tab.size() * sizeof(double));
+    CK(cudaMemcpyAsync(c->qt.p, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice,
+                       c->stream));
+    const size_t rowb = (size_t)m * 8;
+    c->qb.ensure((size_t)nb * rowb);
+    CK(cudaMemcpyAsync(c->qb.p, B, (size_t)nb * rowb, cudaMemcpyHostToDevice, c->stream));
+    // A in blocks of rows whose outputs stay within 1 GiB (and the grid's y limit)
+    int64_t blk = std::max<int64_t>(32, std::min<int64_t>(((int64_t)1 << 27) / nb, 65535 * 32));
+    blk = std::min(blk, na);
+    c->qa.ensure((size_t)blk * rowb);
+    c->qo.ensure((size_t)blk * nb * sizeof(double));
+    const bool regs = metric != RBG_PMH_JACCARD_WEIGHTED;
+    for (int64_t a0 = 0; a0 < na; a0 += blk) {
+      const int64_t ra = std::min(blk, na - a0);
+      CK(cudaMemcpyAsync(c->qa.p, (const char *)A + (size_t)a0 * rowb, (size_t)ra * rowb,
+                         cudaMemcpyHostToDevice, c->stream));
+      launch_pmh_compare(c->qa.as<uint64_t>(), ra, c->qb.as<uint64_t>(), nb, m, regs,
+                         c->qt.as<double>(), c->qo.as<double>(), c->stream);
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(out + (size_t)a0 * nb, c->qo.p, (size_t)ra * nb * sizeof(double),
+                         cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+    }
+  });
+}
+
+int rbg_pmh_merge_registers(rbg_ctx *c, const double *A, const double *B, int64_t n, int32_t m,
+                            double *out) {
+  return guarded(c, [&] {
+    if (n < 0 || m < 2 || m > kMaxM) throw Error(RBG_ERR_ARG, "row count or m out of range");
+    if (n == 0) return;
+    if (!A || !B || !out) throw Error(RBG_ERR_ARG, "null argument");
+    const size_t bytes = (size_t)n * m * sizeof(double);
+    c->qa.ensure(bytes);
+    c->qb.ensure(bytes);
+    c->qo.ensure(bytes);
+    CK(cudaMemcpyAsync(c->qa.p, A, bytes, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->qb.p, B, bytes, cudaMemcpyHostToDevice, c->stream));
+    launch_pmh_merge(c->qa.as<double>(), c->qb.as<double>(), (int64_t)n * m, c->qo.as<double>(),
+                     c->stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, c->qo.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  });
 }
 
 int rbg_free_graph(rbg_graph *g) {

@@ -106,9 +106,12 @@ struct Tables {
   DBuf order, UT, codeA, W32, rank;
   DBuf dict_vals, dict_codes, dict_n;   // per-column sorted dictionaries
   bool dict_ready = false;
+  DBuf W64, U;                          // winner states and U by element (sketch rows)
+  bool rows_ready = false;
   void release() {
     order.release(); UT.release(); codeA.release(); W32.release(); rank.release();
     dict_vals.release(); dict_codes.release(); dict_n.release();
+    W64.release(); U.release();
   }
 };
 
@@ -116,12 +119,17 @@ struct Tables {
 // (synchronised before returning).
 std::unique_ptr<Tables> make_tables(const rbg_params *p, cudaStream_t s);
 
-// Dense regime (no abundance prune) of rows [g.row_lo, row_hi): one-hot int8
-// GEMMs of the register codes (cuBLASLt) and the row scan; writes g.topk,
-// g.topk_cnt, g.maxcnt_all, g.maxcnt_cand and g.stats[1].  Synchronises c->stream.
-void dense_allpairs_gemm(rbg_ctx *c, const GraphArgs &g);
-// The dense regime runs on the one-hot GEMM unless RBG_DENSE_ALU is set (then
-// the integer-ALU register compare, kept for the measured comparison).
+// Dense regime (no abundance prune) of rows [g.row_lo, row_hi): the one-hot
+// int8 product of the register codes on the tensor cores (k_onehot_mma) and
+// the merge of its candidate lists; writes g.topk, g.topk_cnt, g.maxcnt_all,
+// g.maxcnt_cand (which the caller zeroed) and g.stats[1].  Synchronises
+// c->stream once (the one-hot width); call check_onehot_status after the
+// caller's next synchronisation of c->stream.
+void dense_allpairs_onehot(rbg_ctx *c, const GraphArgs &g);
+void check_onehot_status(rbg_ctx *c);
+// The dense regime runs on the one-hot tensor-core kernel unless RBG_DENSE_ALU
+// is set (then the integer-ALU register compare, kept for the measured
+// comparison).
 inline bool dense_on_gemm() { return getenv("RBG_DENSE_ALU") == nullptr; }
 
 // Pinned result blocks (pooled).  pinned_take: a block of `bytes` or null;
@@ -269,10 +277,14 @@ struct rbg_ctx {
   rbg::DBuf sym_pairs, sym_np, sym_rowcnt, sym_rowoff, sym_keys;
   uint64_t sym_cap = 0;                  // pair-list capacity (grows when a pass overflows)
   rbg::DBuf shard_send, shard_recv;      // exchange blocks of rbg_bin_graph_sharded
-  // dense regime as a one-hot int8 GEMM: code presence, one-hot map and
-  // offsets, the one-hot matrix, a chunk of counts, the GEMM workspace
-  rbg::DBuf oh_pres, oh_map, oh_koff, oh_X, oh_D, oh_ws;
-  void *lt = nullptr;                    // cuBLASLt handle, created on first use
+  // dense regime on the tensor cores: code presence, one-hot map and offsets,
+  // the one-hot matrix, the candidate lists and their counts, the kernel's
+  // wait status (and its pinned copy, valid after the next synchronisation)
+  rbg::DBuf oh_pres, oh_map, oh_koff, oh_X, oh_cand, oh_cnt, oh_err;
+  rbg::HBuf oh_errpin;
+  bool oh_pending = false;
+  // ProbMinHash4 queries: operand blocks, output block, metric table
+  rbg::DBuf qa, qb, qo, qt;
   rbg::HBuf shard_host;                  // their host staging for host-memory collectives
   bool streamed = false;                 // rbg_bin_graph scored the pairs behind the copy
   uint64_t no_stream_S = 0;              // bit S: survivors outgrew the list when streamed

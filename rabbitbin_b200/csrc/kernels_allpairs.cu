@@ -966,6 +966,14 @@ void launch_allpairs(const GraphArgs &g, uint64_t *gbuf, int32_t *gcnt, cudaStre
       g, gbuf, gcnt, cap, P);
 }
 
+void launch_merge_topk(const GraphArgs &g, const uint64_t *gbuf, const int32_t *gcnt, int cap,
+                       int P, cudaStream_t s) {
+  const int64_t rows = (g.row_hi < 0 ? g.n : g.row_hi) - g.row_lo;
+  if (rows <= 0) return;
+  k_merge_topk<<<(unsigned)((rows + kMergeWarps - 1) / kMergeWarps), kMergeWarps * 32, 0, s>>>(
+      g, gbuf, gcnt, cap, P);
+}
+
 void launch_allpairs_sym(const GraphArgs &g, const SymOut &o, cudaStream_t s) {
   if (g.n == 0) return;
   const int P = allpairs_slices(g.n, g.K);

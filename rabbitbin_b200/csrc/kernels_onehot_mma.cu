@@ -1,0 +1,581 @@
+// Dense regime on the 5th-generation tensor cores, hand-written for sm_100a.
+//
+// The register-match count of contigs i and j (pmh_match_count16,
+// src/rabbitbin.cpp:1261-1293: registers with equal nonzero codes) is the dot
+// product X_i . X_j of their binary one-hot rows over the (register, code)
+// pairs that occur in the assembly (kernels_onehot.cu builds X).  The small
+// path (build_graph_allpairs, src/impl/rb_graph.cpp:7-72) needs every pair's
+// count, so the counts are one int8 contraction X X^T, computed here with
+// tcgen05.mma kind::i8 into TMEM and consumed in the same kernel: no count
+// matrix is written to memory.
+//
+// CTA tile: 256 rows x 256 columns = two UMMA 128x256 accumulators (A rows
+// 0-127 and 128-255 against the same B columns), which fill the 512 TMEM
+// columns of the SM.  The one-hot width is walked in chunks of 128 bytes (one
+// 128-byte swizzle atom): TMA brings the chunk of the 256 A rows and the 256
+// B rows (64 KB) into a 3-stage shared-memory ring.  Warp 0 issues the TMA
+// loads, warp 1 allocates TMEM and issues the MMAs (4 K-steps of 32 per
+// chunk per accumulator), warps 2-9 are the epilogue: each thread owns one row
+// of the tile, reads its 256 counts from TMEM (tcgen05.ld 32x32b, 64 columns
+// at a time), keeps the row maxima and appends the keys (similarity bits << 32
+// | ~j) above its running threshold to its own candidate list in global
+// memory; a list that reaches its capacity is cut to the K best by the warp
+// together (select_topk), which raises the threshold.
+//
+// Work split: the CTAs form a GR x GC grid; CTA (a, b) takes the row blocks
+// a, a + GR, ... and, in each, the column tiles of column group b, so at any
+// moment GR row blocks and GC column tiles are in use (their operands stay in
+// L2).  Each (row, column group) pair has its own list: k_merge_topk then
+// merges a row's GC lists into its top-K, exactly what the other dense
+// kernels produce (top-K keys over the candidates above the admission floor,
+// maxima over all other contigs and over the candidates).
+//
+// Every wait on an mbarrier is bounded (2 s of %globaltimer); a wait that
+// runs out records an error code for the host and the CTA stops issuing work,
+// waits (bounded) for its own copies and MMAs in flight, frees its TMEM and
+// returns.  No TMA load uses cluster multicast.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+
+#include "rbg_internal.h"
+#include "select_topk.cuh"
+
+namespace rbg {
+namespace {
+
+constexpr int kTM = 256;                      // rows per CTA tile
+constexpr int kTN = 256;                      // columns per CTA tile
+constexpr int kKC = 128;                      // one-hot bytes per stage (one swizzle atom)
+constexpr int kStages = 3;
+constexpr int kHalfBytes = 128 * kKC;         // one 128-row operand block: 16 KB
+constexpr int kStageBytes = (kTM + kTN) * kKC;   // 64 KB
+constexpr int kEpiWarps = 8;
+constexpr int kThreads = (2 + kEpiWarps) * 32;
+constexpr unsigned FULL = 0xffffffffu;
+constexpr uint64_t kWaitNs = 2000000000ull;   // bound of every mbarrier wait
+
+// instruction descriptor: D s32 (bits 4-5 = 2), A and B unsigned 8-bit (bits
+// 7-9, 10-12 = 0), both K-major (bits 15, 16 = 0), N >> 3 at bits 17-22,
+// M >> 4 at bits 24-28
+constexpr uint32_t kIdesc = (2u << 4) | ((uint32_t)(kTN >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+
+struct OhArgs {
+  GraphArgs g;
+  int64_t rows;          // rows scored: [g.row_lo, g.row_lo + rows)
+  int nkc;               // one-hot chunks of 128 bytes
+  int RB, NT;            // 256-row blocks, 256-column tiles
+  int GR, GC;            // CTA grid: row groups x column groups
+  uint64_t *cand;        // [rows32 x GC x 32] lists of cap keys
+  int cap;               // keys per list (<= 512, >= K + 64)
+  int32_t *cand_cnt;     // [rows32 x GC x 32]
+  int *err;              // set when a bounded wait runs out
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ uint64_t now_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t a, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count));
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(a), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait for the phase of parity `parity` to complete; false (and the
+// error code recorded) when it does not within kWaitNs.
+__device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity, int *err, int code) {
+  if (mbar_try(a, parity)) return true;
+  const uint64_t t0 = now_ns();
+  for (;;) {
+    if (mbar_try(a, parity)) return true;
+    if (now_ns() - t0 > kWaitNs) {
+      atomicCAS(err, 0, code);
+      return false;
+    }
+  }
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t a) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(a) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t a, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes)
+               : "memory");
+}
+
+// 2-D TMA tile load (no multicast): box at (x bytes, y rows) into dst.
+__device__ __forceinline__ void tma_load(uint32_t dst, const CUtensorMap *map, int x, int y,
+                                         uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+      ::"r"(dst), "l"((uint64_t)map), "r"(x), "r"(y), "r"(mbar)
+      : "memory");
+}
+
+// UMMA shared-memory descriptor of a K-major operand block in the 128-byte
+// swizzle layout TMA writes: rows of 128 bytes, 8-row atoms 1024 bytes apart
+// (SBO), version 1 (bits 46-47), layout SWIZZLE_128B (2 at bits 61-63).
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
+  return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)1 << 16) |
+         ((uint64_t)(1024 >> 4) << 32) | ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t dt, uint64_t ad, uint64_t bd, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
+      ::"r"(dt), "l"(ad), "l"(bd), "r"(kIdesc), "r"(acc));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+               ::"r"(mbar) : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// 64 consecutive 32-bit TMEM columns of this warp's 32 lanes.
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, uint32_t (&v)[64]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x64.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, "
+      "%32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, "
+      "%48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%64];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+        "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]),
+        "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]),
+        "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31]),
+        "=r"(v[32]), "=r"(v[33]), "=r"(v[34]), "=r"(v[35]), "=r"(v[36]), "=r"(v[37]),
+        "=r"(v[38]), "=r"(v[39]), "=r"(v[40]), "=r"(v[41]), "=r"(v[42]), "=r"(v[43]),
+        "=r"(v[44]), "=r"(v[45]), "=r"(v[46]), "=r"(v[47]), "=r"(v[48]), "=r"(v[49]),
+        "=r"(v[50]), "=r"(v[51]), "=r"(v[52]), "=r"(v[53]), "=r"(v[54]), "=r"(v[55]),
+        "=r"(v[56]), "=r"(v[57]), "=r"(v[58]), "=r"(v[59]), "=r"(v[60]), "=r"(v[61]),
+        "=r"(v[62]), "=r"(v[63])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Named barrier 1 of the epilogue warps; returns the OR of every thread's flag.
+__device__ __forceinline__ uint32_t epi_barrier_or(uint32_t flag) {
+  uint32_t out;
+  asm volatile(
+      "{\n\t.reg .pred pi, po;\n\t"
+      "setp.ne.u32 pi, %1, 0;\n\t"
+      "barrier.cta.red.or.pred po, 1, %2, pi;\n\t"
+      "selp.u32 %0, 1, 0, po;\n\t}"
+      : "=r"(out)
+      : "r"(flag), "n"(kEpiWarps * 32)
+      : "memory");
+  return out;
+}
+
+// Smallest count whose similarity key can exceed thr (sv is non-decreasing).
+__device__ __forceinline__ uint32_t count_floor(const uint32_t *sv, int m, uint64_t thr) {
+  const uint32_t hi = (uint32_t)(thr >> 32);
+  int lo = 0, up = m + 1;
+  while (lo < up) {
+    const int mid = (lo + up) >> 1;
+    if (sv[mid] >= hi) up = mid; else lo = mid + 1;
+  }
+  return (uint32_t)max(lo, 1);
+}
+
+// The tiles of CTA (a, b): row blocks a, a + GR, ...; columns tiles
+// [c0, c1) of column group b.
+__device__ __forceinline__ void col_range(const OhArgs &A, int b, int &c0, int &c1) {
+  c0 = (int)((int64_t)b * A.NT / A.GC);
+  c1 = (int)((int64_t)(b + 1) * A.NT / A.GC);
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+k_onehot_mma(const __grid_constant__ CUtensorMap tmap, const OhArgs A) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  // 1024-byte aligned stage ring (the swizzle pattern follows address bits)
+  uint8_t *ring = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t *bars = (uint64_t *)(ring + kStages * kStageBytes);
+  // bars: full[kStages], empty[kStages], tmem_full, tmem_empty, mma_done
+  uint32_t *tmem_slot = (uint32_t *)(bars + 2 * kStages + 3);
+  uint32_t *nzw = tmem_slot + 4;               // [2][8] candidate-flag words of a tile
+  int *abort_flag = (int *)(nzw + 16);
+  uint32_t *sv = (uint32_t *)(abort_flag + 4); // [m + 1] similarity bits
+
+  const GraphArgs &g = A.g;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int a = blockIdx.x / A.GC, b = blockIdx.x % A.GC;
+  int c0, c1;
+  col_range(A, b, c0, c1);
+  const uint32_t bar0 = smem_u32(bars);
+  auto full_bar = [&](int s) { return bar0 + 8u * s; };
+  auto empty_bar = [&](int s) { return bar0 + 8u * (kStages + s); };
+  const uint32_t tfull = bar0 + 8u * (2 * kStages), tempty = tfull + 8u, mdone = tfull + 16u;
+
+  for (int i = threadIdx.x; i <= g.m; i += kThreads) sv[i] = g.sv_bits[i];
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(full_bar(s), 1);
+      mbar_init(empty_bar(s), 1);
+    }
+    mbar_init(tfull, 1);
+    mbar_init(tempty, kEpiWarps * 32);
+    mbar_init(mdone, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {                               // TMEM: all 512 columns
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;"
+                 ::"r"(smem_u32(tmem_slot)) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = *tmem_slot;
+  const int nrb = (A.RB - a + A.GR - 1) / A.GR;  // row blocks of this CTA
+
+  if (warp == 0) {
+    // ── TMA producer ──
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0;
+      uint32_t issued = 0;                       // bit s: stage s holds an issued load
+      uint32_t last_ph = 0;                      // bit s: phase of its last load
+      bool ok = true;
+      for (int r = 0; r < nrb && ok; ++r) {
+        const int y_a = (int)(g.row_lo + (int64_t)(a + r * A.GR) * kTM);
+        for (int ct = c0; ct < c1 && ok; ++ct) {
+          for (int kc = 0; kc < A.nkc; ++kc) {
+            if (!mbar_wait(empty_bar(s), ph ^ 1u, A.err, 1) || *(volatile int *)abort_flag) {
+              ok = false;
+              *(volatile int *)abort_flag = 1;
+              break;
+            }
+            const uint32_t dst = smem_u32(ring + (size_t)s * kStageBytes);
+            mbar_expect_tx(full_bar(s), kStageBytes);
+            tma_load(dst, &tmap, kc * kKC, y_a, full_bar(s));
+            tma_load(dst + 2 * kHalfBytes, &tmap, kc * kKC, ct * kTN, full_bar(s));
+            issued |= 1u << s;
+            last_ph = (last_ph & ~(1u << s)) | (ph << s);
+            if (++s == kStages) { s = 0; ph ^= 1u; }
+          }
+        }
+      }
+      // copies in flight land before the CTA leaves (already true when the
+      // MMAs consumed them)
+      for (int t = 0; t < kStages; ++t)
+        if ((issued >> t) & 1u) mbar_wait(full_bar(t), (last_ph >> t) & 1u, A.err, 2);
+    }
+  } else if (warp == 1) {
+    // ── MMA issuer ──
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0, tph = 0;
+      bool ok = true;
+      for (int r = 0; r < nrb && ok; ++r) {
+        for (int ct = c0; ct < c1 && ok; ++ct) {
+          if (!mbar_wait(tempty, tph ^ 1u, A.err, 3) || *(volatile int *)abort_flag) {
+            ok = false;
+            *(volatile int *)abort_flag = 1;
+            break;
+          }
+          tc_fence_after();
+          for (int kc = 0; kc < A.nkc; ++kc) {
+            if (!mbar_wait(full_bar(s), ph, A.err, 4) || *(volatile int *)abort_flag) {
+              ok = false;
+              *(volatile int *)abort_flag = 1;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t st = smem_u32(ring + (size_t)s * kStageBytes);
+            const uint64_t da0 = sdesc(st), da1 = sdesc(st + kHalfBytes),
+                           db = sdesc(st + 2 * kHalfBytes);
+#pragma unroll
+            for (int k = 0; k < kKC / 32; ++k) {
+              const uint32_t acc = (kc | k) ? 1u : 0u;
+              // +32 bytes of K per step: +2 in the descriptor's 16-byte units
+              mma_i8(tbase, da0 + 2 * k, db + 2 * k, acc);
+              mma_i8(tbase + kTN, da1 + 2 * k, db + 2 * k, acc);
+            }
+            mma_commit(empty_bar(s));            // the stage is free once these finish
+            if (++s == kStages) { s = 0; ph ^= 1u; }
+          }
+          if (!ok) break;
+          mma_commit(tfull);                     // the tile's counts are in TMEM
+          tph ^= 1u;
+        }
+      }
+      mma_commit(mdone);                         // every MMA issued has finished
+      mbar_wait(mdone, 0, A.err, 5);
+    }
+  } else {
+    // ── epilogue: thread = row ──
+    const int e = warp - 2;                      // 0..7
+    const int q = warp & 3;                      // TMEM lane quarter of this warp
+    const int half = e >> 2;                     // accumulator 0 or 1
+    const int K = g.K, m = g.m;
+    const int64_t n = g.n;
+    const int P = A.GC;
+    uint32_t tph = 0;
+    int tcount = 0;
+    bool ok = true;
+    for (int r = 0; r < nrb && ok; ++r) {
+      const int rb = a + r * A.GR;
+      const int64_t li = (int64_t)rb * kTM + half * 128 + q * 32 + lane;   // local row
+      const int64_t i = g.row_lo + li;
+      const bool valid_row = li < A.rows;
+      const uint32_t nz_i = valid_row ? g.anynz[i] : 0u;
+      uint64_t *buf = nullptr;
+      size_t slot = 0;
+      if (valid_row) {
+        slot = ((size_t)(li >> 5) * P + b) * 32 + (size_t)(li & 31);
+        buf = A.cand + slot * (size_t)A.cap;
+      }
+      int fill = 0;
+      uint64_t thr = g.key_floor;
+      uint32_t cthr = count_floor(sv, m, thr);
+      uint32_t mx_a = 0, mx_c = 0;
+      for (int ct = c0; ct < c1; ++ct, ++tcount) {
+        // candidate flags of the tile's columns (anynz), one word per warp
+        {
+          const int64_t j = (int64_t)ct * kTN + e * 32 + lane;
+          const unsigned w = __ballot_sync(FULL, j < n && g.anynz[j]);
+          if (lane == 0) nzw[(tcount & 1) * 8 + e] = w;
+        }
+        uint32_t bad = mbar_wait(tfull, tph, A.err, 6) ? 0u : 1u;
+        if (*(volatile int *)abort_flag) bad = 1u;
+        // one decision for all epilogue threads (they meet at this barrier every tile)
+        bad = epi_barrier_or(bad);
+        if (bad) {
+          ok = false;
+          *(volatile int *)abort_flag = 1;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t *nzt = nzw + (tcount & 1) * 8;
+        for (int c = 0; c < kTN / 64; ++c) {
+          uint32_t v[64];
+          tmem_ld64(tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(half * kTN + c * 64), v);
+          if (c == kTN / 64 - 1) {               // every count of the tile is in registers
+            tc_fence_before();
+            mbar_arrive(tempty);
+          }
+          const int64_t j0 = (int64_t)ct * kTN + c * 64;
+          // valid columns: j < n and j != i; candidates: valid and (nz_i or nz_j)
+          uint64_t vm = ~0ull;
+          if (j0 + 64 > n) vm = (n <= j0) ? 0ull : (~0ull >> (64 - (n - j0)));
+          if (i >= j0 && i < j0 + 64) vm &= ~(1ull << (i - j0));
+          if (!valid_row) vm = 0ull;
+          const uint64_t nz64 = ((uint64_t)nzt[c * 2 + 1] << 32) | nzt[c * 2];
+          const uint64_t cm = vm & (nz_i ? ~0ull : nz64);
+          bool hit = false;
+          if (vm == ~0ull && cm == ~0ull) {
+            uint32_t cmx = 0;
+#pragma unroll
+            for (int t = 0; t < 64; ++t) {
+              cmx = max(cmx, v[t]);
+              hit |= v[t] >= cthr;
+            }
+            mx_a = max(mx_a, cmx);
+            mx_c = max(mx_c, cmx);
+          } else {
+#pragma unroll
+            for (int t = 0; t < 64; ++t) {
+              const uint32_t va = ((vm >> t) & 1ull) ? v[t] : 0u;
+              const uint32_t vc = ((cm >> t) & 1ull) ? v[t] : 0u;
+              mx_a = max(mx_a, va);
+              mx_c = max(mx_c, vc);
+              hit |= vc >= cthr;
+            }
+          }
+          if (hit) {
+#pragma unroll
+            for (int t = 0; t < 64; ++t) {
+              if (((cm >> t) & 1ull) && v[t] >= cthr) {
+                const uint64_t key = ((uint64_t)sv[v[t]] << 32) |
+                                     (uint64_t)(~(uint32_t)(j0 + t));
+                if (key > thr) buf[fill++] = key;
+              }
+            }
+          }
+          // lists that could not take another chunk are cut to the K best
+          unsigned need = __ballot_sync(FULL, fill > A.cap - 64);
+          while (need) {
+            const int L = __ffs(need) - 1;
+            need &= need - 1;
+            uint64_t *lb = (uint64_t *)__shfl_sync(FULL, (unsigned long long)buf, L);
+            const int lc = __shfl_sync(FULL, fill, L);
+            __syncwarp();
+            const uint64_t t = select_topk(lb, lc, K);
+            if (lane == L) {
+              thr = t;
+              fill = K;
+              cthr = count_floor(sv, m, thr);
+            }
+          }
+        }
+        tph ^= 1u;
+      }
+      if (!ok) break;
+      // the column group's list of this row: its K best, the maxima, the count
+      unsigned need = __ballot_sync(FULL, fill > K);
+      while (need) {
+        const int L = __ffs(need) - 1;
+        need &= need - 1;
+        uint64_t *lb = (uint64_t *)__shfl_sync(FULL, (unsigned long long)buf, L);
+        const int lc = __shfl_sync(FULL, fill, L);
+        __syncwarp();
+        select_topk(lb, lc, K);
+        if (lane == L) fill = K;
+      }
+      if (valid_row) {
+        A.cand_cnt[slot] = fill;
+        if (mx_a) atomicMax(g.maxcnt_all + i, mx_a);
+        if (mx_c) atomicMax(g.maxcnt_cand + i, mx_c);
+      }
+      if (b == 0 && g.stats) {                   // every other contig, once per row
+        const unsigned vr = __ballot_sync(FULL, valid_row);
+        if (lane == 0 && vr)
+          atomicAdd(g.stats + 1, (unsigned long long)__popc(vr) * (unsigned long long)(n - 1));
+      }
+    }
+  }
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 1)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tbase) : "memory");
+}
+
+// cuTensorMapEncodeTiled from the driver the runtime already loaded.
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static std::once_flag once;
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess && q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  });
+  return fn;
+}
+
+size_t oh_smem(int m) {
+  return 1024 + (size_t)kStages * kStageBytes + (2 * kStages + 3) * 8 + 16 + 64 + 16 +
+         (size_t)(m + 1) * 4;
+}
+
+}  // namespace
+
+// Keys per (row, column group) list: room for K plus at least 64 more, so a
+// chunk of 64 columns always fits after a cut to K.
+int onehot_mma_cap(int K) { return std::min(512, (K + 160 + 31) & ~31); }
+
+// GR x GC CTA grid for RB row blocks and NT column tiles on `sms` SMs: the
+// split with the smallest largest share of tiles (then the fewest CTAs).
+void onehot_mma_grid(int RB, int NT, int sms, int *GR, int *GC) {
+  int bestR = 1, bestC = 1;
+  int64_t best = INT64_MAX;
+  for (int gr = 1; gr <= std::min(RB, sms); ++gr)
+    for (int gc = 1; gc <= std::min(NT, std::min(32, sms / gr)); ++gc) {
+      const int64_t load = (int64_t)((RB + gr - 1) / gr) * ((NT + gc - 1) / gc);
+      if (load < best || (load == best && gr * gc < bestR * bestC)) {
+        best = load;
+        bestR = gr;
+        bestC = gc;
+      }
+    }
+  *GR = bestR;
+  *GC = bestC;
+}
+
+// X: [n][ldx] one-hot rows (ldx a multiple of 128, zero padded); the rows
+// [g.row_lo, g.row_lo + rows) against every column, on a GR x GC CTA grid.
+// cand/cand_cnt hold ceil(rows / 32) * 32 * GC lists of onehot_mma_cap(K) keys
+// (cand_cnt is zeroed here).  Returns RBG_OK or a status with *why set.
+int launch_onehot_mma(const GraphArgs &g, const int8_t *X, int64_t ldx, int64_t rows,
+                      uint64_t *cand, int32_t *cand_cnt, int *err, int GR, int GC,
+                      cudaStream_t s, const char **why) {
+  auto enc = encode_fn();
+  if (!enc) {
+    *why = "cuTensorMapEncodeTiled is not available";
+    return RBG_ERR_CUDA;
+  }
+  if (ldx % kKC != 0 || ((uintptr_t)X & 15u) != 0 || g.n >= ((int64_t)1 << 31) || GC > 32 ||
+      g.K > onehot_mma_cap(g.K) - 64) {
+    *why = "one-hot operand layout";
+    return RBG_ERR_ARG;
+  }
+  CUtensorMap map;
+  std::memset(&map, 0, sizeof(map));
+  const cuuint64_t dims[2] = {(cuuint64_t)ldx, (cuuint64_t)g.n};
+  const cuuint64_t strides[1] = {(cuuint64_t)ldx};
+  const cuuint32_t box[2] = {(cuuint32_t)kKC, (cuuint32_t)kTM};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void *)X, dims, strides, box,
+                         estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    *why = "cuTensorMapEncodeTiled failed";
+    return RBG_ERR_CUDA;
+  }
+  OhArgs A;
+  A.g = g;
+  A.rows = rows;
+  A.nkc = (int)(ldx / kKC);
+  A.RB = (int)((rows + kTM - 1) / kTM);
+  A.NT = (int)((g.n + kTN - 1) / kTN);
+  A.GR = GR;
+  A.GC = GC;
+  A.cand = cand;
+  A.cap = onehot_mma_cap(g.K);
+  A.cand_cnt = cand_cnt;
+  A.err = err;
+  const size_t nslots = (size_t)((rows + 31) / 32) * 32 * GC;
+  cudaError_t e = cudaMemsetAsync(cand_cnt, 0, nslots * sizeof(int32_t), s);
+  if (e == cudaSuccess) {
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lk(mu);
+    e = cudaFuncSetAttribute(k_onehot_mma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)oh_smem(4096));
+  }
+  if (e == cudaSuccess) {
+    k_onehot_mma<<<GR * GC, kThreads, oh_smem(g.m), s>>>(map, A);
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) {
+    *why = cudaGetErrorString(e);
+    return RBG_ERR_CUDA;
+  }
+  return RBG_OK;
+}
+
+}  // namespace rbg

@@ -474,6 +474,7 @@ __global__ void __launch_bounds__(kMThreads, 3) k_minreduce(SketchArgs a) {
             w32 = __ldg(a.W32 + (size_t)wi * m + rr);
           }
           if (a.winners32) a.winners32[(c0 + cc) * m + rr] = w32;
+          if (a.win_elem) a.win_elem[(c0 + cc) * m + rr] = (uint8_t)wi;
         }
         va |= code << (8 * b);
         vb |= (code ? code : 0xFFu) << (8 * b);

@@ -7,17 +7,20 @@
 // serves them: the caller passes the ASCII sequences, the offsets and the
 // output winner rows as device buffers, and every intermediate buffer (2-bit
 // packed bases, invalid-base mask, 1/w table, register codes, the ProbMinHash
-// stream tables) lives in one file-scope array reserved when the library is
-// loaded.  The array is kRbgNoAllocScratchBytes (24 MiB) on every GPU that
-// loads the library, kept until the process exits; requests that need more
-// are rejected with RBG_ERR_ARG before anything runs on the device.
+// stream tables, the offsets check flag) lives in one file-scope array
+// reserved when the library is loaded.  The array is kRbgNoAllocScratchBytes
+// (24 MiB) on every GPU that loads the library, kept until the process exits;
+// requests that need more are rejected with RBG_ERR_ARG before anything runs
+// on the device.
 //
 // Set-up: the first call on a device looks up the array's device address
-// (cudaGetSymbolAddress, once per device, with that device current); make that
-// first call before any stream capture.  All calls share the array and it keeps
-// the previous call's contents; every part a call reads is written by the same
-// call first (the register-minimum kernel writes the code padding too), but two
-// calls that overlap on the GPU race on it.
+// (cudaGetSymbolAddress, once per device, with that device current).  Every
+// call reads a check flag back and synchronises the caller's stream, so no
+// call may be made while that stream is being captured into a CUDA graph.
+// All calls share the array and it keeps the previous call's contents; every
+// part a call reads is written by the same call first (the check kernel writes
+// its flag unconditionally, the register-minimum kernel writes the code
+// padding too), but two calls that overlap on the GPU race on it.
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -44,6 +47,21 @@ void put_err(char *buf, size_t len, const char *msg) {
   }
 }
 
+// Offsets check, one block: flag = 1 unless offsets[0] == 0, offsets[n] ==
+// nbases and 0 <= offsets[i] <= offsets[i+1] <= nbases for every i.  The
+// flag is written whatever the outcome, so nothing needs clearing first.
+__global__ void k_check_offsets(const int64_t *__restrict__ off, int64_t n, int64_t nbases,
+                                int32_t *__restrict__ flag) {
+  int bad = 0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const int64_t a = off[i], b = off[i + 1];
+    bad |= (a < 0) | (a > b) | (b > nbases);
+  }
+  if (threadIdx.x == 0) bad |= (off[0] != 0) | (off[n] != nbases);
+  bad = __syncthreads_or(bad);
+  if (threadIdx.x == 0) *flag = bad;
+}
+
 }  // namespace
 }  // namespace rbg
 
@@ -56,9 +74,13 @@ extern "C" int rbg_build_pmh_winners_noalloc(const rbg_params *p, const char *se
     put_err(errbuf, errlen, "null or negative argument");
     return RBG_ERR_ARG;
   }
-  if (p->k < 1 || p->k > 4 || p->m < 2 || p->m > 1024 || (p->gc_norm != 0 && p->gc_norm != 1) ||
+  if (p->oph_k > 0) {
+    put_err(errbuf, errlen, "winner rows exist only for the ProbMinHash metric (oph_k = 0)");
+    return RBG_ERR_ARG;
+  }
+  if (p->k < 1 || p->k > 4 || p->m < 2 || p->m > 4096 || p->gc_norm < 0 || p->gc_norm > 2 ||
       (p->win_bits != 16 && p->win_bits != 32)) {
-    put_err(errbuf, errlen, "unsupported parameters (k 1..4, m 2..1024, gc_norm 0/1)");
+    put_err(errbuf, errlen, "unsupported parameters (k 1..4, m 2..4096, gc_norm 0..2)");
     return RBG_ERR_UNSUPPORTED;
   }
   if (((uintptr_t)seq_device & 15u) != 0) {
@@ -82,6 +104,7 @@ extern "C" int rbg_build_pmh_winners_noalloc(const rbg_params *p, const char *se
   const size_t oCnt = off;     off += up256((size_t)n * sizeof(int32_t));
   const size_t oA = off;       off += up256((size_t)n * mpad);
   const size_t oB = off;       off += up256((size_t)n * mpad);
+  const size_t oFlag = off;    off += 256;
   if (off > kRbgNoAllocScratchBytes) {
     char msg[200];
     std::snprintf(msg, sizeof(msg),
@@ -111,16 +134,21 @@ extern "C" int rbg_build_pmh_winners_noalloc(const rbg_params *p, const char *se
   }
   unsigned char *S = (unsigned char *)base;
   cudaStream_t s = (cudaStream_t)stream;
-  // offsets sanity (two 8-byte reads into host variables)
-  int64_t first = -1, last = -1;
-  if (cudaMemcpyAsync(&first, offsets_device, 8, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-      cudaMemcpyAsync(&last, offsets_device + n, 8, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-      cudaStreamSynchronize(s) != cudaSuccess) {
-    put_err(errbuf, errlen, "cannot read offsets_device");
+  // offsets check on the device; its flag comes back before any sketch work
+  int32_t bad = 1;
+  k_check_offsets<<<1, 1024, 0, s>>>(offsets_device, n, nbases, (int32_t *)(S + oFlag));
+  cudaError_t e = cudaPeekAtLastError();
+  if (e != cudaSuccess) {
+    put_err(errbuf, errlen, cudaGetErrorString(e));
     return RBG_ERR_CUDA;
   }
-  if (first != 0 || last != nbases) {
-    put_err(errbuf, errlen, "offsets_device must start at 0 and end at nbases");
+  if ((e = cudaMemcpyAsync(&bad, S + oFlag, sizeof(bad), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(s)) != cudaSuccess) {
+    put_err(errbuf, errlen, cudaGetErrorString(e));
+    return RBG_ERR_CUDA;
+  }
+  if (bad) {
+    put_err(errbuf, errlen, "offsets_device must start at 0, end at nbases and never decrease");
     return RBG_ERR_ARG;
   }
   std::shared_ptr<const PmhTables> t;
@@ -166,9 +194,14 @@ extern "C" int rbg_build_pmh_winners_noalloc(const rbg_params *p, const char *se
   a.mpad = mpad;
   launch_count(a, s);
   launch_minreduce(a, s);
+  // a failed launch is reported by its own code; the sync's code separately
+  if ((e = cudaPeekAtLastError()) != cudaSuccess) {
+    cudaStreamSynchronize(s);              // the host tables must outlive the copies
+    put_err(errbuf, errlen, cudaGetErrorString(e));
+    return RBG_ERR_CUDA;
+  }
   // the host tables must outlive the asynchronous copies
-  const cudaError_t e = cudaStreamSynchronize(s);
-  if (e != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) {
     put_err(errbuf, errlen, cudaGetErrorString(e));
     return RBG_ERR_CUDA;
   }

@@ -81,6 +81,7 @@ struct SketchArgs {
   uint8_t *codesA = nullptr;           // [n][mpad]  (0 = unset)
   uint8_t *codesB = nullptr;           // [n][mpad]  (0xFF = unset)
   uint32_t *winners32 = nullptr;       // [n][m], optional
+  uint8_t *win_elem = nullptr;         // [n][m], optional: winning element (0xFF unset)
   int mpad = 512;                      // row stride of the code arrays (bytes)
 };
 
@@ -162,6 +163,33 @@ void launch_b0(const uint32_t *counts, int np, int m, float *b0_out, uint32_t *s
 void launch_pair_counts(const uint8_t *codesA, const uint8_t *codesB, int mpad, int m,
                         const int64_t *pairs, int npairs, uint32_t *out, cudaStream_t s);
 void launch_allpairs(const GraphArgs &g, uint64_t *gbuf, int32_t *gcnt, cudaStream_t s);
+// Warp per row of [g.row_lo, row_hi): its top-K from P partial lists of up to
+// cap keys (list of row r, part s at ((r/32 * P + s) * 32 + r%32) * cap).
+// ProbMinHash4 rows of n contigs from their winning elements (win_elem [n][m])
+// and 1/w rows (elem_winv [n][E]): winners_ (W64 [E][m]; 0 unset) and the
+// register values (1/w_e) * U_e(r) (U [E][m]; +inf unset).  Either output may be null.
+void launch_pmh_rows(const uint8_t *win_elem, const double *elem_winv, int64_t n, int m, int E,
+                     const uint64_t *W64, const double *U, uint64_t *w64_out, double *reg_out,
+                     cudaStream_t s);
+// out[i * nb + j] = table[count(A_i, B_j)], count = registers with equal values
+// that are set (winners != 0 with regs == false; register values != +inf with
+// regs == true); A [na][m], B [nb][m] 64-bit words.
+void launch_pmh_compare(const uint64_t *A, int64_t na, const uint64_t *B, int64_t nb, int m,
+                        bool regs, const double *table, double *out, cudaStream_t s);
+// out[i][r] = std::min(a[i][r], b[i][r]) over n x m register values.
+void launch_pmh_merge(const double *a, const double *b, int64_t count, double *out, cudaStream_t s);
+void launch_merge_topk(const GraphArgs &g, const uint64_t *gbuf, const int32_t *gcnt, int cap,
+                       int P, cudaStream_t s);
+// Dense regime on tcgen05 (kernels_onehot_mma.cu): counts of the rows
+// [g.row_lo, g.row_lo + rows) against every contig as the int8 product of
+// one-hot rows X [n][ldx] (ldx a multiple of 128), consumed in the kernel into
+// per-(row, column group) candidate lists for launch_merge_topk (P = GC) and
+// the row maxima; *err != 0 after it ran when a bounded wait gave up.
+int onehot_mma_cap(int K);
+void onehot_mma_grid(int RB, int NT, int sms, int *GR, int *GC);
+int launch_onehot_mma(const GraphArgs &g, const int8_t *X, int64_t ldx, int64_t rows,
+                      uint64_t *cand, int32_t *cand_cnt, int *err, int GR, int GC,
+                      cudaStream_t s, const char **why);
 
 // Output of the symmetric all-pairs pass (each unordered pair scored once): the
 // admitted pairs and, per row, how many admitted keys it holds (both ends).

@@ -252,3 +252,24 @@ def test_streamed_pairs_equal_resident(S, cap):
         assert got["b0"] == resident["b0"] and got["sim_cutoff"] == resident["sim_cutoff"]
         for k in ("src", "dst", "scomp", "score"):
             assert np.array_equal(got[k], resident[k]), k
+
+
+@pytest.mark.parametrize("S", [1, 5])
+def test_graph_small_path_alu_compare(gpu_ctx, orc, S):
+    """The dense regime on the integer-ALU register compare (RBG_DENSE_ALU=1)
+    instead of the one-hot tensor-core kernel: the same graph."""
+    import os
+    os.environ["RBG_DENSE_ALU"] = "1"
+    try:
+        g = _graph_case(gpu_ctx, orc, 20, 1500, S, seed=70 + S)
+    finally:
+        os.environ.pop("RBG_DENSE_ALU", None)
+    assert g["path"] == 1
+
+
+@pytest.mark.parametrize("N,S", [(300, 5), (1000, 0), (5000, 3), (9000, 2)])
+def test_graph_small_path_onehot_sizes(gpu_ctx, orc, N, S):
+    """The one-hot tensor-core kernel at row/column counts that leave partial
+    256-row and 256-column tiles, a single tile, and several column groups."""
+    g = _graph_case(gpu_ctx, orc, max(4, N // 250), N, S, seed=900 + N)
+    assert g["path"] == 1

@@ -112,3 +112,30 @@ def test_golden_fixtures(orc):
             assert res["b0"] == float(z["b0"]) and res["sim_cutoff"] == float(z["sim_cutoff"]), f
             assert np.array_equal(s, z["src"]) and np.array_equal(d, z["dst"]), f
             assert np.array_equal(sc, z["scomp"]) and np.array_equal(sw, z["score"]), f
+
+
+def test_fp64_weights_against_reference(ref_lib):
+    """The FP64 edge-weight oracle against the reference's own FP32 weights:
+    within 1e-6 wherever both make the same cut, and any cut they disagree on
+    sits on the threshold in exact arithmetic."""
+    asm = make_assembly(20, 3000, 10, seed=88, absent_frac=0.1)
+    buf, offs = asm.concat()
+    w = ref_lib.build_winners(buf, offs)
+    for fp, S in ((2, 10), (1, 5)):
+        d = asm.depth[:, :S]
+        res = ref_lib.run_graph(oracle.default_params(asm.n, 500, S, force_path=fp), w, d)
+        rep = oracle.fp64_report(d, res)
+        assert rep["edges"] > 1000
+        assert rep["max_abs_err_fp64"] <= 1e-6, rep
+        assert rep["max_margin_disagreeing"] <= 1e-6, rep
+
+
+def test_scale_digests_cover_every_case():
+    import json
+    import os
+    import scale_cases
+    with open(os.path.join(os.path.dirname(__file__), "golden", "scale_digests.json")) as f:
+        table = json.load(f)
+    assert set(table) == set(scale_cases.CASES)
+    for name, rec in table.items():
+        assert rec["edges"] > 0 and len(rec["digest"]) == 32, name
