@@ -716,7 +716,9 @@ def main():
     ap.add_argument("--rate", type=float, default=20.0, help="serve form: requests per second")
     ap.add_argument("--duration", type=float, default=10.0, help="serve form: seconds of arrivals")
     ap.add_argument("--pool", type=int, default=32, help="serve form: distinct assemblies")
-    ap.add_argument("--workers", type=int, default=1, help="serve form: concurrent batches")
+    ap.add_argument("--workers", type=int, default=0,
+                    help="serve form: lanes (0: the server's default of two, one taking "
+                         "large requests first, one small requests only)")
     ap.add_argument("--shard", default="assemblies", choices=["assemblies", "rows"],
                     help="multi-GPU: one assembly per rank (weak scaling, default) or one "
                          "assembly split by rows over the ranks (strong scaling)")

@@ -78,6 +78,13 @@ typedef struct rbg_params {
                              MinHash metric of rabbit_sketch.h with k-mers of this
                              size (sketch_kmer_size, 8; 1..32) and m buckets     */
   int32_t oph_bits;       /* sketch_bits: bit-planes per OPH bucket (2; 1..7)      */
+  int32_t graph_index;    /* RABBIT_GRAPH_INDEX (0): 1 restricts the small path's
+                             neighbours to contigs sharing >= min_common
+                             one-permutation sketch keys (build_similarity_graph,
+                             src/impl/rb_graph.cpp:199-383); rbg_bin_graph only */
+  int32_t index_k;        /* sketch_kmer_size of the index's sketches (8; 1..32;
+                             oph_k when the one-permutation metric is on)      */
+  int32_t min_common;     /* RABBIT_MINCOMMON (0: floor(cutoff * m * 0.7), >= 1)  */
   int32_t reserved;
 } rbg_params;
 
@@ -291,20 +298,22 @@ int rbg_bin_batch(rbg_ctx *ctx, const rbg_params *defaults, const rbg_assembly *
                   int32_t n_asm, rbg_graph *out, rbg_batch_stats *stats);
 
 /* ── serving: a request loop over a stream of assemblies ──────────────────
- * No counterpart in the reference.  Requests are queued on submit; worker
- * threads (one device context each) take every queued request that fits
- * their share of the HBM budget and run them as one batch (rbg_bin_batch),
- * so requests that arrive while others are on the GPU are folded into the
- * next launch.  Inside a batch the copies of later requests overlap the work
- * of earlier ones; with two or more workers the workers' batches also overlap
- * on the device (one worker, the default, gave the lower latencies on a
- * Poisson trace, since two batches sharing the GPU each take about twice as
- * long).  Each result equals rbg_bin_graph on that assembly alone. */
+ * No counterpart in the reference.  Requests are queued on submit in two size
+ * classes (small: at most small_pairs contig pairs).  Each lane is a worker
+ * thread with its own device context: lane 0 serves large requests first and
+ * small ones when no large one waits, the other lanes serve small requests
+ * only.  A lane that becomes free folds every queued request of its class
+ * that fits into the HBM budget the running batches leave (a batch's share is
+ * released when it finishes) into one rbg_bin_batch call.  Requests that
+ * arrive while others are on the GPU are therefore admitted as soon as a lane
+ * of their class and the memory are free, small requests never wait behind a
+ * large batch, and the lanes' batches overlap on the device.  Each result
+ * equals rbg_bin_graph on that assembly alone. */
 typedef struct rbg_server rbg_server;
 
 typedef struct rbg_server_config {
   int32_t device;              /* CUDA device                                   */
-  int32_t workers;             /* concurrent batches (contexts); 0 -> 1         */
+  int32_t workers;             /* lanes (contexts, concurrent batches); 0 -> 2  */
   int64_t hbm_budget;          /* bytes of device memory for request state;
                                   0 -> 150 GB, capped at the free memory        */
   int32_t max_batch;           /* assemblies folded into one launch; 0 -> 64    */
@@ -313,6 +322,8 @@ typedef struct rbg_server_config {
   int64_t max_batch_pairs;     /* fold requests while the batch's contig pairs
                                   stay below this (a larger request runs alone);
                                   0 -> 2e9                                      */
+  int64_t small_pairs;         /* requests with at most this many contig pairs
+                                  are small; 0 -> 2e8 (about 20,000 contigs)    */
 } rbg_server_config;
 
 typedef struct rbg_request_stats {
@@ -342,6 +353,44 @@ int rbg_server_wait(rbg_server *srv, int64_t request_id, double timeout_s, rbg_g
 const char *rbg_server_last_error(rbg_server *srv);
 /* Stops accepting work, finishes queued requests, frees the contexts. */
 int rbg_server_destroy(rbg_server *srv);
+
+/* ── RBCACHE1 v3: the on-disk state of a built graph ──────────────────────
+ * rb_write_cache / rb_load_cache (src/impl/rb_cache.cpp:103-319): the state
+ * RabbitBin keeps after the expensive stages so that a later run (or a
+ * restarted server) goes straight to the cheap tail.  The file is byte for
+ * byte the one the reference writes for the same state and is readable by
+ * either program; reading also accepts versions 1 and 2.  Names are bytes
+ * back to back with n + 1 offsets; matrices are row-major floats (the ranked
+ * depth matrix of the large contigs, the raw one of the small contigs).
+ * rbg_read_cache allocates every array (free with rbg_free_cache). */
+typedef struct rbg_cache {
+  int64_t n_large, n_small, samples;            /* nobs, nobs1, num_depth_samples */
+  uint64_t seed, total_size, total_size_small;  /* --seed, totalSize, totalSize1  */
+  double sim_cutoff, b0;                        /* simCutoff, g_pmh_baseline      */
+  uint64_t min_contig, min_small_contig;
+  int32_t has_depth, has_snv;
+  char *large_names;   int64_t *large_name_off;   int64_t n_large_names;
+  char *small_names;   int64_t *small_name_off;   int64_t n_small_names;
+  uint64_t *large_len; int64_t n_large_len;      /* seq_lens                       */
+  uint64_t *small_len; int64_t n_small_len;      /* small_seq_lens                 */
+  float *depth_ranked; int64_t depth_rows, depth_cols;              /* depth_matrix */
+  float *small_depth;  int64_t small_depth_rows, small_depth_cols;  /* small_depth_matrix */
+  float *large_means;  int64_t n_large_means;    /* g_large_means                  */
+  float *depth_raw;    int64_t n_depth_raw;      /* g_depth_raw                    */
+  double *colnorm;     int64_t n_colnorm;        /* g_depth_colnorm                */
+  uint32_t *from, *to; float *scomp; int64_t n_edges;   /* the graph              */
+  float *snv_pi; uint32_t *snv_nsnv, *snv_cov; int64_t n_snv;   /* --strain block */
+  int32_t version;                               /* read: the file's version       */
+  int32_t reserved;
+} rbg_cache;
+
+/* Write the state (names, lengths and vectors with a null pointer are written
+ * as empty; the SNV block only with has_snv and n_snv > 0). */
+int rbg_write_cache(const char *path, const rbg_cache *state);
+/* Read a cache written by either program (RBG_ERR_ARG: missing, truncated or
+ * corrupt file; RBG_ERR_UNSUPPORTED: other version or ABI). */
+int rbg_read_cache(const char *path, rbg_cache *out);
+int rbg_free_cache(rbg_cache *c);
 
 /* Device-resident form used by batching, serving and the benchmark: stage the
  * inputs once (host -> device), run the hot path on them any number of times,

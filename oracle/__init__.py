@@ -24,7 +24,8 @@ class RefParams(C.Structure):
                 ("min_cv", C.c_double), ("neg_thr", C.c_double),
                 ("depth_sim", C.c_int32), ("depth_fuse", C.c_int32),
                 ("wjac_norm", C.c_int32), ("no_abdfirst", C.c_int32),
-                ("oph_k", C.c_int32), ("oph_bits", C.c_int32)]
+                ("oph_k", C.c_int32), ("oph_bits", C.c_int32),
+                ("graph_index", C.c_int32), ("min_common", C.c_int32), ("index_k", C.c_int32)]
 
 
 class RefOut(C.Structure):
@@ -39,7 +40,7 @@ def default_params(n, m=500, S=0, **kw):
                   base_on=1, nthreads=os.cpu_count() or 1, seed=1, force_path=0,
                   coverage=0.95, min_edge=0.70, w_comp=-1.0, min_cv=1.0,
                   neg_thr=-0.3, depth_sim=2, depth_fuse=1, wjac_norm=1, no_abdfirst=0,
-                  oph_k=0, oph_bits=2)
+                  oph_k=0, oph_bits=2, graph_index=0, min_common=0, index_k=8)
     if "abdfirst" in kw:
         kw["no_abdfirst"] = 0 if kw.pop("abdfirst") else 1
     for k, v in kw.items():
@@ -116,6 +117,26 @@ class _Lib:
                       _ptr(unit, C.c_float), C.byref(out))
         if rc != 0:
             raise RuntimeError(f"oracle run_graph failed: {rc}")
+        return self._result(out, unit, S)
+
+    def run_graph_index(self, params, seqcat, offsets, winners32, depth):
+        """The small path with RABBIT_GRAPH_INDEX=1 (harness only): candidates
+        from the inverted index of one-permutation sketch keys."""
+        f = self.lib.ref_run_graph_index
+        f.restype = C.c_int
+        f.argtypes = [C.POINTER(RefParams), C.c_char_p, C.POINTER(C.c_int64),
+                      C.POINTER(C.c_uint32), C.POINTER(C.c_float), C.POINTER(C.c_float),
+                      C.POINTER(RefOut)]
+        n, S = params.n, params.S
+        offs = np.ascontiguousarray(offsets, dtype=np.int64)
+        w = np.ascontiguousarray(winners32, dtype=np.uint32)
+        d = np.ascontiguousarray(depth, dtype=np.float32).reshape(n, max(S, 0))
+        unit = np.zeros((n, max(S, 1)), dtype=np.float32)
+        out = RefOut()
+        rc = f(C.byref(params), seqcat, _ptr(offs, C.c_int64), _ptr(w, C.c_uint32),
+               _ptr(d, C.c_float), _ptr(unit, C.c_float), C.byref(out))
+        if rc != 0:
+            raise RuntimeError(f"oracle run_graph_index failed: {rc}")
         return self._result(out, unit, S)
 
     def run_graph_oph(self, params, seqcat, offsets, depth):
@@ -329,3 +350,59 @@ def fp64_report(depth, g, **kw):
     return {"max_abs_err_fp64": float(err.max()) if err.size else 0.0,
             "edges": int(len(got)), "cut_disagreements": int((~agree).sum()),
             "max_margin_disagreeing": float(dis.max()) if dis.size else 0.0}
+
+
+def ref_cache_write(path, state):
+    """RabbitBin's own rb_write_cache of a state dict (harness only; the dict
+    layout of rabbitbin_b200.api.cache_struct)."""
+    from rabbitbin_b200 import api
+    lib = ref()
+
+    class RefCacheState(C.Structure):
+        _fields_ = api._CACHE_FIELDS
+    st, keep = api.cache_struct(RefCacheState, state)
+    f = lib.lib.ref_cache_write
+    f.restype = C.c_int
+    f.argtypes = [C.c_char_p, C.POINTER(RefCacheState)]
+    if f(str(path).encode(), C.byref(st)) != 0:
+        raise RuntimeError("reference rb_write_cache failed")
+
+
+def ref_cache_read(path):
+    """RabbitBin's own rb_load_cache of a file, as a state dict (harness
+    only), or None when the reference rejects the file."""
+    from rabbitbin_b200 import api
+    lib = ref()
+
+    class RefCacheState(C.Structure):
+        _fields_ = api._CACHE_FIELDS
+    f = lib.lib.ref_cache_read
+    f.restype = C.c_int
+    f.argtypes = [C.c_char_p, C.POINTER(RefCacheState)] + [C.c_void_p] * 17
+    st = RefCacheState()
+    if f(str(path).encode(), C.byref(st), *([None] * 17)) != 0:
+        return None
+    nl, ns = st.n_large_names, st.n_small_names
+    bufs = {}
+    # name bytes: the file size bounds them
+    size = os.path.getsize(path)
+    lnames, snames = np.zeros(size + 1, np.uint8), np.zeros(size + 1, np.uint8)
+    lnoff, snoff = np.zeros(nl + 1, np.int64), np.zeros(ns + 1, np.int64)
+    arrays = []
+    for name, dt, cnt in api.CACHE_ARRAYS:
+        n = getattr(st, cnt[0]) * getattr(st, cnt[1]) if isinstance(cnt, tuple) else getattr(st, cnt)
+        bufs[name] = np.zeros(max(int(n), 1), dt)
+        arrays.append(bufs[name].ctypes.data)
+    args = [lnames.ctypes.data, lnoff.ctypes.data, snames.ctypes.data, snoff.ctypes.data] + arrays
+    if f(str(path).encode(), C.byref(st), *args) != 0:
+        return None
+    out = {k: getattr(st, k) for k in api.CACHE_SCALARS}
+    out["large_names"] = [lnames[lnoff[i]:lnoff[i + 1]].tobytes() for i in range(nl)]
+    out["small_names"] = [snames[snoff[i]:snoff[i + 1]].tobytes() for i in range(ns)]
+    for name, dt, cnt in api.CACHE_ARRAYS:
+        if isinstance(cnt, tuple):
+            r, c = getattr(st, cnt[0]), getattr(st, cnt[1])
+            out[name] = bufs[name][:r * c].reshape(r, c)
+        else:
+            out[name] = bufs[name][:getattr(st, cnt)]
+    return out

@@ -41,10 +41,12 @@ FRAGMENTS = [
     ("frag_parse_fasta.inc", "rabbitbin.cpp", 1890, 2248),
     ("frag_anynz.inc", "impl/rb_abundance.cpp", 94, 114),
     ("frag_graph_allpairs.inc", "impl/rb_graph.cpp", 7, 72),
+    ("frag_graph_index.inc", "impl/rb_graph.cpp", 199, 383),
     ("frag_calib_converge.inc", "impl/rb_graph.cpp", 390, 415),
     ("frag_fused_graph.inc", "impl/rb_graph.cpp", 489, 1356),
     ("frag_calibrate.inc", "impl/rb_graph.cpp", 1362, 1384),
     ("frag_calibrate_fused.inc", "impl/rb_graph.cpp", 1386, 1438),
+    ("frag_cache.inc", "impl/rb_cache.cpp", 26, 319),
 ]
 
 
@@ -93,9 +95,10 @@ def build_ref():
             with open(path, "w", encoding="utf-8") as f:
                 f.write(text)
     shim = os.path.join(HERE, "ref_shim.cpp")
-    deps = [shim, __file__, os.path.join(REF_SRC, "probmh.cpp")]
+    cache_shim = os.path.join(HERE, "ref_cache_shim.cpp")
+    deps = [shim, cache_shim, __file__, os.path.join(REF_SRC, "probmh.cpp")]
     if _stale(out, deps):
-        _run(["g++"] + FLAGS + ["-I", frag_dir, "-I", REF_SRC, shim,
+        _run(["g++"] + FLAGS + ["-I", frag_dir, "-I", REF_SRC, shim, cache_shim,
                                 os.path.join(REF_SRC, "probmh.cpp"), "-o", out])
     return out
 

@@ -45,6 +45,7 @@
 #include <unistd.h>
 
 #include "probmh.h"
+#include "rabbit_invidx.h"
 #include "rabbit_sketch.h"
 #include "ranker.h"
 #include "tile.h"
@@ -160,6 +161,10 @@ static inline void rb_fill_tnf(const char *, size_t, float *) { abort(); }
 #include "frag_parse_fasta.inc"     // src/rabbitbin.cpp:1890-2248
 #include "frag_anynz.inc"           // src/impl/rb_abundance.cpp:94-114
 #include "frag_graph_allpairs.inc"  // src/impl/rb_graph.cpp:7-72
+// state of the inverted-index graph build (src/rabbitbin.cpp:209, :1593)
+static std::vector<rabbit_sketch::KmerSketch *> g_sketches;
+static std::unique_ptr<rabbit_invidx::InvertedIndex> g_inv_idx;
+#include "frag_graph_index.inc"     // src/impl/rb_graph.cpp:199-383
 #include "frag_calib_converge.inc"  // src/impl/rb_graph.cpp:390-415
 #include "frag_fused_graph.inc"     // src/impl/rb_graph.cpp:480-1356
 #include "frag_calibrate.inc"       // src/impl/rb_graph.cpp:1362-1384
@@ -215,6 +220,9 @@ struct RefParams {
   int32_t no_abdfirst;  // RABBIT_NO_ABDFIRST set
   int32_t oph_k;        // 0: PMH metric; > 0: RABBIT_PMH=0 with sketch_kmer_size = oph_k
   int32_t oph_bits;     // sketch_bits
+  int32_t graph_index;  // RABBIT_GRAPH_INDEX=1 (small path: inverted-index candidates)
+  int32_t min_common;   // RABBIT_MINCOMMON (0: unset)
+  int32_t index_k;      // sketch_kmer_size of the index's one-permutation sketches
 };
 
 struct RefOut {
@@ -337,6 +345,45 @@ int ref_run_graph_oph(const RefParams *p, const char *seqcat, const int64_t *off
   return rc;
 }
 
+static bool g_use_index = false;
+
+// The same run with RABBIT_GRAPH_INDEX=1: the one-permutation sketches of
+// every contig (KmerSketch(sketch_size, index_k, sketch_bits), update) and
+// the inverted index of their keys, built as the sketch loop of rb_cmd_bin
+// builds them (src/rabbitbin.cpp:4737-4741, :4819-4830, :4885-4891) but with
+// one insertion thread, so every posting list holds its contigs in ascending
+// order; the small path's graph then comes from build_similarity_graph
+// (src/impl/rb_graph.cpp:199-383).
+int ref_run_graph_index(const RefParams *p, const char *seqcat, const int64_t *offsets,
+                        const uint32_t *winners32, const float *depth_raw, float *unit_out,
+                        RefOut *out) {
+  const int64_t n = p->n;
+  const uint32_t bits = (uint32_t)(p->oph_bits > 0 ? p->oph_bits : 2);
+  g_sketches.assign((size_t)n, nullptr);
+  rabbit_invidx::InvertedIndexBuilder builder(1);
+  std::vector<uint64_t> ks;
+  for (int64_t r = 0; r < n; ++r) {
+    g_sketches[r] = new rabbit_sketch::KmerSketch((uint32_t)p->m, p->index_k > 0 ? p->index_k : 8,
+                                                  bits);
+    g_sketches[r]->update(seqcat + offsets[r], (uint64_t)(offsets[r + 1] - offsets[r]));
+    g_sketches[r]->getKeys(ks);
+    for (uint64_t k : ks) builder.insert(0, k, (uint32_t)r);
+  }
+  g_inv_idx = std::make_unique<rabbit_invidx::InvertedIndex>(builder.build(1));
+  setenv("RABBIT_GRAPH_INDEX", "1", 1);
+  if (p->min_common > 0) setenv("RABBIT_MINCOMMON", std::to_string(p->min_common).c_str(), 1);
+  g_pmh_mode = true;
+  g_use_index = true;
+  const int rc = run_graph_body(p, winners32, depth_raw, unit_out, out);
+  g_use_index = false;
+  unsetenv("RABBIT_GRAPH_INDEX");
+  unsetenv("RABBIT_MINCOMMON");
+  for (auto *sk : g_sketches) delete sk;
+  g_sketches.clear();
+  g_inv_idx.reset();
+  return rc;
+}
+
 // Runs pack -> b0 -> ranks/unit rows -> graph -> edge weights exactly as
 // rb_cmd_bin does for a PMH run; winners32 holds the build_pmh_winners rows.
 // unit_out (n*S floats, may be null) receives g_depth_unit.
@@ -451,7 +498,8 @@ static int run_graph_body(const RefParams *p, const uint32_t *winners32,
     // 2500-contig samples, then the same all-pairs build), :5035-5054
     simCutoff = fused ? (double)calibrate_sim_cutoff_fused(p->coverage)
                       : (double)calibrate_sim_cutoff(p->coverage, true);
-    build_graph_allpairs(g, simCutoff / 1000.);
+    if (g_use_index) build_similarity_graph(g, simCutoff / 1000.);
+    else build_graph_allpairs(g, simCutoff / 1000.);
   }
 
   // Edge weights, default fixed-cutoff branch (src/rabbitbin.cpp:5482-5509

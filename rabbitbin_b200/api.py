@@ -35,7 +35,8 @@ class Params(C.Structure):
                 ("depth_sim", C.c_int32), ("depth_fuse", C.c_int32),
                 ("wjac_norm", C.c_int32), ("fp_contract", C.c_int32),
                 ("wjac_cut", C.c_double), ("wjac_gate", C.c_int32), ("oph_k", C.c_int32),
-                ("oph_bits", C.c_int32), ("reserved", C.c_int32)]
+                ("oph_bits", C.c_int32), ("graph_index", C.c_int32), ("index_k", C.c_int32),
+                ("min_common", C.c_int32), ("reserved", C.c_int32)]
 
 
 class Graph(C.Structure):
@@ -85,7 +86,8 @@ class Fasta(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("workers", C.c_int32), ("hbm_budget", C.c_int64),
-                ("max_batch", C.c_int32), ("plain", C.c_int32), ("max_batch_pairs", C.c_int64)]
+                ("max_batch", C.c_int32), ("plain", C.c_int32), ("max_batch_pairs", C.c_int64),
+                ("small_pairs", C.c_int64)]
 
 
 class RequestStats(C.Structure):
@@ -95,6 +97,123 @@ class RequestStats(C.Structure):
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+_CACHE_FIELDS = [
+    ("n_large", C.c_int64), ("n_small", C.c_int64), ("samples", C.c_int64),
+    ("seed", C.c_uint64), ("total_size", C.c_uint64), ("total_size_small", C.c_uint64),
+    ("sim_cutoff", C.c_double), ("b0", C.c_double),
+    ("min_contig", C.c_uint64), ("min_small_contig", C.c_uint64),
+    ("has_depth", C.c_int32), ("has_snv", C.c_int32),
+    ("large_names", C.c_void_p), ("large_name_off", C.c_void_p), ("n_large_names", C.c_int64),
+    ("small_names", C.c_void_p), ("small_name_off", C.c_void_p), ("n_small_names", C.c_int64),
+    ("large_len", C.c_void_p), ("n_large_len", C.c_int64),
+    ("small_len", C.c_void_p), ("n_small_len", C.c_int64),
+    ("depth_ranked", C.c_void_p), ("depth_rows", C.c_int64), ("depth_cols", C.c_int64),
+    ("small_depth", C.c_void_p), ("small_depth_rows", C.c_int64), ("small_depth_cols", C.c_int64),
+    ("large_means", C.c_void_p), ("n_large_means", C.c_int64),
+    ("depth_raw", C.c_void_p), ("n_depth_raw", C.c_int64),
+    ("colnorm", C.c_void_p), ("n_colnorm", C.c_int64),
+    ("from_", C.c_void_p), ("to", C.c_void_p), ("scomp", C.c_void_p), ("n_edges", C.c_int64),
+    ("snv_pi", C.c_void_p), ("snv_nsnv", C.c_void_p), ("snv_cov", C.c_void_p),
+    ("n_snv", C.c_int64)]
+
+
+class CacheState(C.Structure):
+    """rbg_cache: the state stored in an RBCACHE1 file."""
+    _fields_ = _CACHE_FIELDS + [("version", C.c_int32), ("reserved", C.c_int32)]
+
+
+# (field, numpy dtype, count field or (rows, cols)) of every array of the state
+CACHE_ARRAYS = [("large_len", np.uint64, "n_large_len"), ("small_len", np.uint64, "n_small_len"),
+                ("depth_ranked", np.float32, ("depth_rows", "depth_cols")),
+                ("small_depth", np.float32, ("small_depth_rows", "small_depth_cols")),
+                ("large_means", np.float32, "n_large_means"),
+                ("depth_raw", np.float32, "n_depth_raw"), ("colnorm", np.float64, "n_colnorm"),
+                ("from_", np.uint32, "n_edges"), ("to", np.uint32, "n_edges"),
+                ("scomp", np.float32, "n_edges"), ("snv_pi", np.float32, "n_snv"),
+                ("snv_nsnv", np.uint32, "n_snv"), ("snv_cov", np.uint32, "n_snv")]
+CACHE_SCALARS = ["n_large", "n_small", "samples", "seed", "total_size", "total_size_small",
+                 "sim_cutoff", "b0", "min_contig", "min_small_contig", "has_depth", "has_snv"]
+
+
+def cache_struct(cls, state):
+    """A ctypes state of class `cls` pointing into numpy copies of `state`
+    (dict: the scalars, 'large_names' / 'small_names' lists of bytes, the
+    arrays); returns (struct, keep-alive list)."""
+    st, keep = cls(), []
+    for k in CACHE_SCALARS:
+        setattr(st, k, state.get(k, 0))
+    for key in ("large_names", "small_names"):
+        names = state.get(key) or []
+        off = np.zeros(len(names) + 1, np.int64)
+        off[1:] = np.cumsum([len(x) for x in names])
+        buf = np.frombuffer(b"".join(names) + b"\0", np.uint8).copy()
+        keep += [buf, off]
+        setattr(st, key, buf.ctypes.data if names else None)
+        setattr(st, key.replace("names", "name_off"), off.ctypes.data if names else None)
+        setattr(st, "n_" + key, len(names))
+    for name, dt, cnt in CACHE_ARRAYS:
+        a = state.get(name)
+        if a is None:
+            a = np.zeros(0, dt)
+        a = np.ascontiguousarray(a, dt)
+        keep.append(a)
+        setattr(st, name, a.ctypes.data if a.size else None)
+        if isinstance(cnt, tuple):
+            r, c = (a.shape if a.ndim == 2 else (0, 0))
+            setattr(st, cnt[0], r)
+            setattr(st, cnt[1], c)
+        else:
+            setattr(st, cnt, a.size)
+    return st, keep
+
+
+def cache_dict(st):
+    """The state of a filled ctypes struct as a dict of copies."""
+    out = {k: getattr(st, k) for k in CACHE_SCALARS}
+    for key in ("large_names", "small_names"):
+        n = getattr(st, "n_" + key)
+        base, off = getattr(st, key), getattr(st, key.replace("names", "name_off"))
+        if n and base:
+            o = np.ctypeslib.as_array(C.cast(off, C.POINTER(C.c_int64)), (n + 1,))
+            out[key] = [C.string_at(base + int(o[i]), int(o[i + 1] - o[i])) for i in range(n)]
+        else:
+            out[key] = []
+    for name, dt, cnt in CACHE_ARRAYS:
+        p = getattr(st, name)
+        shape = (getattr(st, cnt[0]), getattr(st, cnt[1])) if isinstance(cnt, tuple) \
+            else (getattr(st, cnt),)
+        size = int(np.prod(shape))
+        if p and size:
+            ct = np.ctypeslib.as_ctypes_type(dt)
+            out[name] = np.ctypeslib.as_array(C.cast(p, C.POINTER(ct)), shape).copy()
+        else:
+            out[name] = np.zeros(shape if isinstance(cnt, tuple) else (0,), dt)
+    return out
+
+
+def write_cache(path, state):
+    """rbg_write_cache of a state dict (see cache_struct)."""
+    st, keep = cache_struct(CacheState, state)
+    rc = lib().rbg_write_cache(str(path).encode(), C.byref(st))
+    if rc != RBG_OK:
+        raise RbgError(rc, f"cannot write the cache {path}")
+
+
+def read_cache(path):
+    """rbg_read_cache as a state dict (plus 'version')."""
+    st = CacheState()
+    L = lib()
+    rc = L.rbg_read_cache(str(path).encode(), C.byref(st))
+    if rc != RBG_OK:
+        raise RbgError(rc, f"cannot read the cache {path}")
+    try:
+        d = cache_dict(st)
+        d["version"] = st.version
+        return d
+    finally:
+        L.rbg_free_cache(C.byref(st))
 
 
 _lib = None
@@ -162,6 +281,9 @@ def lib():
         "rbg_server_wait": ([vp, C.c_int64, C.c_double, P(Graph), P(RequestStats)], C.c_int),
         "rbg_server_last_error": ([vp], C.c_char_p),
         "rbg_server_destroy": ([vp], C.c_int),
+        "rbg_write_cache": ([C.c_char_p, P(CacheState)], C.c_int),
+        "rbg_read_cache": ([C.c_char_p, P(CacheState)], C.c_int),
+        "rbg_free_cache": ([P(CacheState)], C.c_int),
         "rbg_build_pmh_winners_noalloc": ([P(Params), vp, vp, C.c_int64, C.c_int64, vp, vp,
                                            C.c_char_p, C.c_size_t], C.c_int),
     }
@@ -486,11 +608,11 @@ class Server:
     they arrive, wait for their graphs.  Arrays passed to submit are kept
     alive here until their request has been waited for."""
 
-    def __init__(self, device=0, workers=1, hbm_budget=0, max_batch=64, plain=False,
-                 params=None, max_batch_pairs=0):
+    def __init__(self, device=0, workers=0, hbm_budget=0, max_batch=64, plain=False,
+                 params=None, max_batch_pairs=0, small_pairs=0):
         self._L = lib()
         cfg = ServerConfig(device, workers, int(hbm_budget), max_batch, 1 if plain else 0,
-                           int(max_batch_pairs))
+                           int(max_batch_pairs), int(small_pairs))
         h = C.c_void_p()
         p = params or default_params()
         rc = self._L.rbg_server_create(C.byref(cfg), C.byref(p), C.byref(h))

@@ -232,6 +232,9 @@ void plan_batch(const rbg_params *defaults, const rbg_assembly *asms, int nb, Ba
     if (a.p->oph_k > 0)
       throw Error(RBG_ERR_UNSUPPORTED, "assembly " + std::to_string(i) +
                                            ": the batch form uses the ProbMinHash metric (oph_k = 0)");
+    if (a.p->graph_index)
+      throw Error(RBG_ERR_UNSUPPORTED, "assembly " + std::to_string(i) +
+                                           ": graph_index is available through rbg_bin_graph only");
     a.n = x.n;
     a.nbases = x.n > 0 ? x.offsets[x.n] : 0;
     a.S = x.S;

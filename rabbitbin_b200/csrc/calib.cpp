@@ -170,6 +170,10 @@ void validate_params(const rbg_params *p) {
   if (p->oph_k < 0 || p->oph_k > 32) throw Error(RBG_ERR_ARG, "oph_k must be in 0..32");
   if (p->oph_k > 0 && (p->oph_bits < 1 || p->oph_bits > 7))
     throw Error(RBG_ERR_UNSUPPORTED, "oph_bits must be in 1..7");
+  if (p->graph_index < 0 || p->graph_index > 1) throw Error(RBG_ERR_ARG, "graph_index must be 0 or 1");
+  if (p->graph_index && (p->index_k < 1 || p->index_k > 32))
+    throw Error(RBG_ERR_ARG, "index_k must be in 1..32");
+  if (p->min_common < 0) throw Error(RBG_ERR_ARG, "min_common must be >= 0");
 }
 
 std::unique_ptr<Tables> make_tables(const rbg_params *p, cudaStream_t s) {

@@ -447,6 +447,59 @@ void share_rows(rbg_ctx *c, const ShardCtx &sc, const void *src, void *dst, size
   scatter_blocks(c, sc, c->shard_recv.p, dst, elem);
 }
 
+// The inverted-index candidate graph of the small path: one-permutation
+// sketch keys of every contig (KmerSketch(m, index_k, bits), getKeys), the
+// index of those keys, and each row's neighbours from its candidates, written
+// over the row's top-K keys.  minCommon and the posting-list cap as
+// build_similarity_graph computes them (src/impl/rb_graph.cpp:228-246, :287).
+void index_graph(rbg_ctx *c, const rbg_params *p, const GraphArgs &g, double cutoff) {
+  const int64_t n = c->n;
+  if (n == 0) return;
+  const int m = p->m, K = p->max_edges;
+  if (index_rows_smem(n, K) > (size_t)227 * 1024)
+    throw Error(RBG_ERR_UNSUPPORTED, "graph_index: at most about 37,000 contigs");
+  const double Md = (double)m;
+  size_t min_common = (size_t)std::floor(cutoff * Md * 0.7);
+  if (min_common < 1) min_common = 1;
+  if (p->min_common >= 1) min_common = (size_t)p->min_common;
+  const int64_t pl_cap = (int64_t)(uint32_t)std::max((size_t)256, (size_t)n / 8);
+  const int64_t total = n * (int64_t)m;
+  c->ix_keys.ensure((size_t)total * 8);
+  c->ix_sorted.ensure((size_t)total * 8);
+  c->ix_contig.ensure((size_t)total * 4);
+  c->ix_post.ensure((size_t)total * 4);
+  c->ix_ukeys.ensure((size_t)total * 8);
+  c->ix_count.ensure((size_t)total * 4);
+  c->ix_off.ensure((size_t)total * 8);
+  c->ix_nk.ensure(16);
+  const size_t sb = index_build_bytes(total);
+  c->ix_scratch.ensure(sb);
+  // keys of the one-permutation sketches (the packed bases are still staged)
+  SketchArgs a;
+  a.packed = c->packed.as<uint32_t>();
+  a.nmask = c->nmask.as<uint32_t>();
+  a.offsets = c->offsets.as<int64_t>();
+  a.n = n;
+  a.m = m;
+  a.mpad = mpad_of(m);
+  a.oph_keys = c->ix_keys.as<uint64_t>();
+  launch_oph(a, p->oph_k > 0 ? p->oph_k : p->index_k, 1, kOphSeed, c->stream);
+  if (launch_index_build(c->ix_keys.as<uint64_t>(), n, m, c->ix_sorted.as<uint64_t>(),
+                         c->ix_contig.as<uint32_t>(), c->ix_post.as<uint32_t>(),
+                         c->ix_ukeys.as<uint64_t>(), c->ix_count.as<int32_t>(),
+                         c->ix_off.as<int64_t>(), c->ix_nk.as<int32_t>(), c->ix_scratch.p, sb,
+                         c->stream) != 0)
+    throw Error(RBG_ERR_CUDA, "graph_index: index build failed");
+  int dev = 0, sms = 148;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  launch_index_rows(g, c->ix_keys.as<uint64_t>(), c->ix_ukeys.as<uint64_t>(),
+                    c->ix_count.as<int32_t>(), c->ix_off.as<int64_t>(), c->ix_post.as<uint32_t>(),
+                    c->ix_nk.as<int32_t>(), pl_cap, (int)min_common, cutoff, sms, c->stream);
+  CK(cudaGetLastError());
+  c->launches += 6;
+}
+
 // Dense regime (no abundance prune): the counts of rows [g.row_lo, row_hi)
 // against every contig as the product of one-hot int8 rows on the tensor
 // cores (k_onehot_mma, int32 accumulation in TMEM: exact), consumed in the
@@ -668,6 +721,13 @@ void run_graph(rbg_ctx *c, const rbg_params *p, const ShardCtx *sc = nullptr) {
   const double simCutoff = calibrate_cutoff(maxc_host, n, cmode, m, sv_d, sv_f, p->coverage, p->seed);
   c->sim_cutoff = simCutoff;
   CK(cudaEventRecord(c->ev[7], c->stream));
+
+  // RABBIT_GRAPH_INDEX=1 on the small path: each row's neighbours again, from
+  // the candidates of the inverted index (src/impl/rb_graph.cpp:199-383)
+  if (!fused && p->graph_index) {
+    if (sc) throw Error(RBG_ERR_UNSUPPORTED, "graph_index is not available for sharded assemblies");
+    index_graph(c, p, g, simCutoff / 1000.);
+  }
 
   // neighbour lists, edges
   c->nbr.ensure(n1 * K * sizeof(uint32_t));
@@ -1042,6 +1102,9 @@ int rbg_default_params(rbg_params *p) {
   p->wjac_gate = 0;
   p->oph_k = 0;
   p->oph_bits = 2;
+  p->graph_index = 0;
+  p->index_k = 8;
+  p->min_common = 0;
   return RBG_OK;
 }
 
@@ -1094,7 +1157,9 @@ int rbg_destroy(rbg_ctx *c) {
                   &c->sym_pairs, &c->sym_np, &c->sym_rowcnt, &c->sym_rowoff, &c->sym_keys,
                   &c->shard_send, &c->shard_recv, &c->oh_pres, &c->oh_map, &c->oh_koff,
                   &c->oh_X, &c->oh_cand, &c->oh_cnt, &c->oh_err, &c->kept, &c->b0dev,
-                  &c->qa, &c->qb, &c->qo, &c->qt};
+                  &c->qa, &c->qb, &c->qo, &c->qt, &c->ix_keys, &c->ix_sorted,
+                  &c->ix_contig, &c->ix_post, &c->ix_ukeys, &c->ix_count, &c->ix_off,
+                  &c->ix_nk, &c->ix_scratch};
   for (DBuf *b : bufs) b->release();
   if (c->tables) c->tables->release();
   release_batch_graphs(c);

@@ -285,6 +285,9 @@ struct rbg_ctx {
   bool oh_pending = false;
   // ProbMinHash4 queries: operand blocks, output block, metric table
   rbg::DBuf qa, qb, qo, qt;
+  // inverted-index graph: sketch keys, sorted pairs, unique keys, list
+  // lengths and offsets, their count, sort scratch
+  rbg::DBuf ix_keys, ix_sorted, ix_contig, ix_post, ix_ukeys, ix_count, ix_off, ix_nk, ix_scratch;
   rbg::HBuf shard_host;                  // their host staging for host-memory collectives
   bool streamed = false;                 // rbg_bin_graph scored the pairs behind the copy
   uint64_t no_stream_S = 0;              // bit S: survivors outgrew the list when streamed

@@ -659,6 +659,18 @@ k_oph(SketchArgs a, int K, int bits, uint64_t seed) {
       }
     }
     __syncwarp();
+    if (a.oph_keys) {
+      // KmerSketch::getKeys (src/rabbit_sketch.h:166-175): one key per
+      // non-empty bucket, murmur3_fmix((bucket << 32) | register, seed ^
+      // 0x51A3C2B7); 0 marks an empty bucket here (no key)
+      for (uint32_t r = lane; r < m; r += 32) {
+        const uint32_t v = reg[r];
+        a.oph_keys[c * m + r] =
+            v == kEmpty ? 0ull : oph_fmix(((uint64_t)r << 32) | v, seed ^ 0x51A3C2B7ull);
+      }
+      __syncwarp();
+      continue;
+    }
     uint32_t ne = 0;
     for (uint32_t r = lane; r < m; r += 32) ne += reg[r] != kEmpty;
     ne = __reduce_add_sync(0xffffffffu, ne);

@@ -82,6 +82,8 @@ struct SketchArgs {
   uint8_t *codesB = nullptr;           // [n][mpad]  (0xFF = unset)
   uint32_t *winners32 = nullptr;       // [n][m], optional
   uint8_t *win_elem = nullptr;         // [n][m], optional: winning element (0xFF unset)
+  // one-permutation sketch keys instead of codes (launch_oph): [n][m], 0 = empty bucket
+  uint64_t *oph_keys = nullptr;
   int mpad = 512;                      // row stride of the code arrays (bytes)
 };
 
@@ -178,6 +180,17 @@ void launch_pmh_compare(const uint64_t *A, int64_t na, const uint64_t *B, int64_
                         bool regs, const double *table, double *out, cudaStream_t s);
 // out[i][r] = std::min(a[i][r], b[i][r]) over n x m register values.
 void launch_pmh_merge(const double *a, const double *b, int64_t count, double *out, cudaStream_t s);
+// Inverted-index candidate graph (kernels_index.cu).
+size_t index_rows_smem(int64_t n, int K);
+size_t index_build_bytes(int64_t total);
+int launch_index_build(const uint64_t *row_keys, int64_t n, int m, uint64_t *keys_sorted,
+                       uint32_t *contig_in, uint32_t *post, uint64_t *ukeys, int32_t *ucount,
+                       int64_t *uoff, int32_t *nruns_dev, void *scratch, size_t scratch_bytes,
+                       cudaStream_t s);
+void launch_index_rows(const GraphArgs &g, const uint64_t *row_keys, const uint64_t *ukeys,
+                       const int32_t *ucount, const int64_t *uoff, const uint32_t *post,
+                       const int32_t *nk, int64_t pl_cap, int min_common, double cutoff, int sms,
+                       cudaStream_t s);
 void launch_merge_topk(const GraphArgs &g, const uint64_t *gbuf, const int32_t *gcnt, int cap,
                        int P, cudaStream_t s);
 // Dense regime on tcgen05 (kernels_onehot_mma.cu): counts of the rows

@@ -1,17 +1,23 @@
 // Serving form: a request loop over a stream of assemblies (rbg_server_*).
 //
-// Requests are validated and queued on submit.  Each worker thread owns a
-// device context; it takes every queued request, oldest first, whose device
-// memory estimate fits into its share of the HBM budget (budget / workers)
-// and runs them as one batch through the batch engine, so requests that
-// arrive while others are on the GPU are folded into the next launch; inside
-// a batch the copies of later requests overlap the work of earlier ones.
-// With two or more workers the batches of different workers also overlap on
-// the device (separate streams); one worker is the default.  A worker's device buffers grow to its largest batch
-// and stay allocated, so the budget share bounds its footprint.
+// Requests are validated and queued on submit, in one of two size classes:
+// small (at most small_pairs contig pairs) and large.  Each lane is a worker
+// thread with its own device context and stream.  Lane 0 takes large requests
+// first and small ones when no large one waits; the other lanes take small
+// requests only.  A lane that becomes free folds every queued request of its
+// class, oldest first, that fits into the HBM budget left by the batches
+// already running (admission against a global budget; a batch's reservation
+// is released the moment it finishes, and the lanes waiting for memory are
+// woken), up to max_batch requests and max_batch_pairs pairs, and runs them as
+// one rbg_bin_batch call.  So a request that arrives while others are on the
+// GPU is admitted as soon as a lane of its class and the memory are free; a
+// small request never waits behind a large batch, and the lanes' batches
+// overlap on the device (their streams run concurrently).  Inside a batch the
+// copies of later requests overlap the work of earlier ones.  A lane's device
+// buffers grow to its largest batch and are kept for the next one.
 //
-// The plain mode runs one worker and one rbg_bin_graph call per request: the
-// unbatched path, for comparisons on the same arrival stream.
+// The plain mode runs one lane and one rbg_bin_graph call per request, in
+// arrival order: the unbatched path, for comparisons on the same stream.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -47,13 +53,13 @@ double ms_between(Clock::time_point a, Clock::time_point b) {
 struct rbg_server {
   rbg_server_config cfg{};
   rbg_params defaults{};
-  int64_t share = 0;                    // bytes per worker batch
+  int64_t reserved = 0;                 // device bytes of the batches running now
   Clock::time_point t_created;
   std::vector<rbg_ctx *> ctxs;
   std::vector<std::thread> workers;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
-  std::deque<std::shared_ptr<Request>> queue;
+  std::deque<std::shared_ptr<Request>> queue[2];   // 0: large, 1: small
   std::unordered_map<int64_t, std::shared_ptr<Request>> reqs;
   int64_t next_id = 1;
   bool stop = false;
@@ -67,21 +73,36 @@ void rbg_server::worker_loop(int w) {
   const size_t max_batch = cfg.plain ? 1 : (size_t)cfg.max_batch;
   for (;;) {
     std::vector<std::shared_ptr<Request>> take;
+    int64_t bytes = 0;
     {
       std::unique_lock<std::mutex> lk(mu);
-      cv_work.wait(lk, [&] { return stop || !queue.empty(); });
-      if (queue.empty()) return;         // stop requested and nothing left
-      int64_t bytes = 0, pairs = 0;
-      while (!queue.empty() && take.size() < max_batch) {
-        const std::shared_ptr<Request> &r = queue.front();
-        if (!take.empty() &&
-            (bytes + r->est_bytes > share || pairs + r->pairs > cfg.max_batch_pairs))
-          break;
-        bytes += r->est_bytes;
-        pairs += r->pairs;
-        take.push_back(r);
-        queue.pop_front();
+      for (;;) {
+        // the queue this lane serves now: lane 0 large first, the others small only
+        std::deque<std::shared_ptr<Request>> *q = nullptr;
+        if (w == 0 && !queue[0].empty()) q = &queue[0];
+        else if (!queue[1].empty() && (w > 0 || cfg.plain || queue[0].empty())) q = &queue[1];
+        if (!q) {
+          if (stop) return;                // stop requested and nothing left for this lane
+          cv_work.wait(lk);
+          continue;
+        }
+        int64_t pairs = 0;
+        while (!q->empty() && take.size() < max_batch) {
+          const std::shared_ptr<Request> &r = q->front();
+          // admission against the budget the running batches leave; alone on an
+          // idle device a request is always admitted (submit checked its size)
+          const bool fits = reserved + bytes + r->est_bytes <= cfg.hbm_budget ||
+                            (reserved == 0 && take.empty());
+          if (!fits || (!take.empty() && pairs + r->pairs > cfg.max_batch_pairs)) break;
+          bytes += r->est_bytes;
+          pairs += r->pairs;
+          take.push_back(r);
+          q->pop_front();
+        }
+        if (!take.empty()) break;
+        cv_work.wait(lk);                  // memory frees when a running batch finishes
       }
+      reserved += bytes;
     }
     const Clock::time_point t0 = Clock::now();
     for (auto &r : take) {
@@ -94,8 +115,10 @@ void rbg_server::worker_loop(int w) {
       std::lock_guard<std::mutex> lk(mu);
       const Clock::time_point t1 = Clock::now();
       for (auto &r : take) r->t_done = t1;
+      reserved -= bytes;
     }
     cv_done.notify_all();
+    cv_work.notify_all();
   }
 }
 
@@ -136,7 +159,8 @@ int rbg_server_create(const rbg_server_config *cfg, const rbg_params *defaults,
   s->cfg = *cfg;
   if (defaults) s->defaults = *defaults; else rbg_default_params(&s->defaults);
   if (s->cfg.plain) s->cfg.workers = 1;
-  if (s->cfg.workers <= 0) s->cfg.workers = 1;
+  if (s->cfg.workers <= 0) s->cfg.workers = 2;
+  if (s->cfg.small_pairs <= 0) s->cfg.small_pairs = 200000000LL;
   if (s->cfg.max_batch <= 0) s->cfg.max_batch = 64;
   if (s->cfg.max_batch_pairs <= 0) s->cfg.max_batch_pairs = 2000000000LL;
   s->t_created = Clock::now();
@@ -149,7 +173,6 @@ int rbg_server_create(const rbg_server_config *cfg, const rbg_params *defaults,
   // leave room for the library's own allocations (tables, pinned staging)
   const int64_t usable = (int64_t)freeb - ((int64_t)2 << 30);
   s->cfg.hbm_budget = std::min<int64_t>(s->cfg.hbm_budget, std::max<int64_t>(usable, 1));
-  s->share = s->cfg.hbm_budget / s->cfg.workers;
   for (int w = 0; w < s->cfg.workers; ++w) {
     rbg_ctx *c = nullptr;
     const int rc = rbg_create(cfg->device, &c);
@@ -186,18 +209,19 @@ int rbg_server_submit(rbg_server *s, const rbg_assembly *a, int64_t *request_id)
     s->err = "the server is shutting down";
     return RBG_ERR_ARG;
   }
-  if (r->est_bytes > s->share) {
+  if (r->est_bytes > s->cfg.hbm_budget) {
     s->err = "the request needs " + std::to_string(r->est_bytes) +
-             " bytes of device memory, more than a worker's share of the HBM budget (" +
-             std::to_string(s->share) + ")";
+             " bytes of device memory, more than the HBM budget (" +
+             std::to_string(s->cfg.hbm_budget) + ")";
     return RBG_ERR_NOMEM;
   }
   r->id = s->next_id++;
   r->t_submit = Clock::now();
   s->reqs[r->id] = r;
-  s->queue.push_back(r);
+  // the plain mode keeps one arrival-order queue
+  s->queue[!s->cfg.plain && r->pairs <= s->cfg.small_pairs ? 1 : 0].push_back(r);
   *request_id = r->id;
-  s->cv_work.notify_one();
+  s->cv_work.notify_all();
   return RBG_OK;
 }
 

@@ -112,3 +112,29 @@ def test_server_rejections(requests_mix):
         assert len(g["src"]) > 0 and st["batch_size"] == 1
     finally:
         srv.close()
+
+
+def test_small_requests_overlap_a_large_batch(gpu_ctx):
+    """Continuous admission: small requests submitted while a large one runs
+    start on the small-request lane before the large one finishes, and every
+    result equals rbg_bin_graph on that assembly alone."""
+    from rabbitbin_b200.synth import make_assembly
+    big = make_assembly(60, 30000, 5, seed=611)
+    smalls = [make_assembly(8, 400 + 50 * k, 5, seed=620 + k) for k in range(4)]
+    reqs = [(a,) + a.concat() for a in [big] + smalls]
+    want = [gpu_ctx.bin_graph(b, o, a.depth) for a, b, o in reqs]
+    srv = api.Server(workers=2, small_pairs=1_000_000)
+    try:
+        ids = [srv.submit(b, o, a.depth) for a, b, o in reqs]
+        got = [srv.wait(i, timeout=600.0) for i in ids]
+    finally:
+        srv.close()
+    for k, ((g, st), w) in enumerate(zip(got, want)):
+        for key in ("src", "dst", "scomp", "score"):
+            assert np.array_equal(g[key], w[key]), (k, key)
+    big_st = got[0][1]
+    assert big_st["worker"] == 0
+    for g, st in got[1:]:
+        assert st["worker"] == 1
+        assert st["submit_s"] + st["queue_ms"] / 1000.0 < big_st["done_s"], \
+            "a small request waited for the large batch"
