@@ -241,14 +241,18 @@ typedef struct rbg_shard {
 
 /* rbg_bin_graph for one assembly split into contiguous row ranges: rank r
  * passes its n_local contigs (ranks in contig order) and their coverage rows.
- * It sketches them; the ranks gather the register codes and coverage rows;
- * each scores the full rows of its contigs (every pair with them, the
- * per-ordered-pair kernels); the row maxima are gathered for the calibration
- * and the neighbour lists for the mutual filter; the rank returns the edges
- * whose `from` is one of its contigs, with global contig ids and weights.
- * The ranks' edges concatenated in rank order are rbg_bin_graph's graph of
- * the whole assembly.  Every rank calls with the same params and S; the
- * collective is called five times per call, in the same order on every rank. */
+ * It sketches them; the ranks gather the register codes and coverage rows.
+ * In the abundance-pruned regime (the fused path with S > 1) each rank runs
+ * its share of the symmetric pass (every unordered pair scored by one rank),
+ * the ranks gather their admitted pairs and partial row maxima, and every
+ * rank selects every row's top-K from the whole list; otherwise each rank
+ * scores the full rows of its contigs and the ranks gather the row maxima and
+ * the neighbour lists.  The rank returns the edges whose `from` is one of its
+ * contigs, with global contig ids and weights; the ranks' edges concatenated
+ * in rank order are rbg_bin_graph's graph of the whole assembly.  Every rank
+ * calls with the same params and S; the collective is called five times per
+ * call (two more for each rerun after a pair list overflowed on some rank),
+ * in the same order on every rank. */
 int rbg_bin_graph_sharded(rbg_ctx *ctx, const rbg_params *p, const rbg_shard *sh,
                           const char *seqcat, const int64_t *offsets, int64_t n_local,
                           const float *depth, int32_t S, rbg_graph *out);

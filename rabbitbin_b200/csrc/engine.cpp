@@ -635,7 +635,81 @@ void run_graph(rbg_ctx *c, const rbg_params *p, const ShardCtx *sc = nullptr) {
   c->prep_done = false;
   std::vector<uint32_t> maxc;
   const uint32_t *maxc_host = nullptr;
-  if (g.prefilter && n > 0 && !sc) {
+  const bool sym_shard = sc && g.prefilter && n > 0;
+  if (sym_shard) {
+    // Sharded assembly, tensor-core regime: this rank runs its share of the
+    // symmetric pass (every unordered pair is scored by exactly one rank), then
+    // the ranks exchange their admitted pairs and partial row maxima, and every
+    // rank selects every row's top-K from the whole pair list (so no neighbour
+    // lists need exchanging for the mutual filter).  A list that overflowed on
+    // any rank is rerun everywhere with a larger one: every rank sees the same
+    // gathered counts, so all take the same collective steps.
+    const int W = sc->world;
+    const size_t nm4 = (size_t)((n1 + 3) & ~3);
+    c->pin.ensure(nm4 * sizeof(uint32_t) + sizeof(unsigned long long));
+    uint32_t *hmax = c->pin.as<uint32_t>();
+    for (;;) {
+      SymOut o = sym_buffers(c, n1);
+      sym_clear(c, n1);
+      launch_allpairs_sym(g, o, c->stream, sc->rank, W);
+      c->launches += 1;
+      CK(cudaGetLastError());
+      CK(cudaEventRecord(c->ev[6], c->stream));
+      c->shard_send.ensure(16);
+      c->shard_recv.ensure(16 * (size_t)W);
+      CK(cudaMemcpyAsync(c->shard_send.p, c->sym_np.p, sizeof(unsigned long long),
+                         cudaMemcpyDeviceToDevice, c->stream));
+      sc->gather(c->shard_send.p, c->shard_recv.p, sizeof(unsigned long long));
+      std::vector<unsigned long long> np(W);
+      CK(cudaMemcpy(np.data(), c->shard_recv.p, W * sizeof(unsigned long long),
+                    cudaMemcpyDeviceToHost));
+      unsigned long long npmax = 0, total = 0;
+      for (int r = 0; r < W; ++r) {
+        npmax = std::max(npmax, np[r]);
+        total += np[r];
+      }
+      if (npmax > c->sym_cap) {
+        c->sym_cap = npmax + npmax / 4;
+        continue;
+      }
+      const size_t blk = (size_t)std::max<unsigned long long>(npmax, 1) * sizeof(uint4);
+      c->shard_send.ensure(blk);
+      c->shard_recv.ensure(blk * W);
+      if (np[sc->rank])
+        CK(cudaMemcpyAsync(c->shard_send.p, c->sym_pairs.p, np[sc->rank] * sizeof(uint4),
+                           cudaMemcpyDeviceToDevice, c->stream));
+      sc->gather(c->shard_send.p, c->shard_recv.p, blk);
+      if (total > c->sym_cap) c->sym_cap = total;
+      o = sym_buffers(c, n1);
+      unsigned long long at = 0;
+      for (int r = 0; r < W; ++r) {
+        if (np[r])
+          CK(cudaMemcpyAsync(o.pairs + at, c->shard_recv.as<char>() + r * blk,
+                             np[r] * sizeof(uint4), cudaMemcpyDeviceToDevice, c->stream));
+        at += np[r];
+      }
+      CK(cudaMemcpyAsync(o.npairs, &total, sizeof(total), cudaMemcpyHostToDevice, c->stream));
+      CK(cudaMemsetAsync(o.rowcnt, 0, n1 * sizeof(int32_t), c->stream));
+      launch_pair_rowcounts(o.pairs, total, o.rowcnt, c->stream);
+      // row maxima: the largest of every rank's partial maxima
+      const size_t mb = ((size_t)n1 * sizeof(uint32_t) + 15) & ~(size_t)15;
+      c->shard_send.ensure(mb);
+      c->shard_recv.ensure(mb * W);
+      CK(cudaMemcpyAsync(c->shard_send.p, c->maxc_cand.p, n * sizeof(uint32_t),
+                         cudaMemcpyDeviceToDevice, c->stream));
+      sc->gather(c->shard_send.p, c->shard_recv.p, mb);
+      launch_max_blocks(c->shard_recv.as<uint32_t>(), W, (int64_t)(mb / sizeof(uint32_t)), n,
+                        c->maxc_cand.as<uint32_t>(), c->stream);
+      CK(cudaMemcpyAsync(hmax, c->maxc_cand.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                         c->stream));
+      launch_rows_topk(g, o, c->sym_rowoff.as<int64_t>(), c->sym_keys.as<uint64_t>(), c->stream);
+      CK(cudaGetLastError());
+      c->launches += 5;
+      CK(cudaStreamSynchronize(c->stream));          // `total` and the maxima on the host
+      break;
+    }
+    maxc_host = hmax;
+  } else if (g.prefilter && n > 0 && !sc) {
     // Tensor-core regime: every unordered pair scored once, admitted pairs
     // listed, then each row's top-K selected from its keys.  The row maxima and
     // the pair count come back while the selection runs; a pass whose pairs did
@@ -744,16 +818,20 @@ void run_graph(rbg_ctx *c, const rbg_params *p, const ShardCtx *sc = nullptr) {
   e.row_edges = c->row_edges.as<int32_t>();
   c->kept.ensure(n1 * ((K + 31) / 32) * sizeof(uint32_t));
   e.kept = c->kept.as<uint32_t>();
-  if (sc) {
+  if (sc && !sym_shard) {
     e.row_lo = sc->row_lo;
     e.row_hi = sc->row_hi;
   }
   const int64_t e_hi = sc ? sc->row_hi : n;
   launch_sort_rows(e, c->stream);
-  if (sc) {
+  if (sc && !sym_shard) {
     // the mutual filter reads the partners' lists: every rank's rows
     share_rows(c, *sc, e.nbr_sorted, e.nbr_sorted, (size_t)K * sizeof(uint32_t));
     share_rows(c, *sc, e.nbr_cnt, e.nbr_cnt, sizeof(int32_t));
+  }
+  if (sym_shard) {                      // every row's list is here; the edges of this rank's rows
+    e.row_lo = sc->row_lo;
+    e.row_hi = sc->row_hi;
   }
   launch_count_edges(e, c->stream);
   c->launches += n ? 3 : 0;

@@ -667,12 +667,15 @@ k_allpairs_tc(GraphArgs g, uint64_t *gbuf, int32_t *gcnt, int cap, int P, float 
 
 // Symmetric pass: CTA x scores row block x and row block B-1-x (columns from
 // the block's first row on), so every CTA's column work is about n + 32.
+// With x0, xs: CTA x0 + blockIdx.x * xs of that layout (the share of one rank
+// of a sharded assembly).
 template <int KS, int SMAX>
 __global__ void __launch_bounds__(kWarps * 32, KS == 2 ? 6 : 1)
-k_allpairs_tc_sym(GraphArgs g, int P, float lo, float hi, float lo16, SymOut o) {
+k_allpairs_tc_sym(GraphArgs g, int P, float lo, float hi, float lo16, SymOut o, int x0, int xs) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int64_t B = (g.n + 31) / 32;
-  const int64_t b1 = blockIdx.x, b2 = B - 1 - (int64_t)blockIdx.x;
+  const int64_t x = x0 + (int64_t)blockIdx.x * xs;
+  const int64_t b1 = x, b2 = B - 1 - x;
   tc_item<KS, SMAX, true>(g, nullptr, nullptr, 0, P, lo, hi, lo16, b1, blockIdx.y, smem, o, 0);
   if (b2 > b1) {
     __syncthreads();
@@ -785,6 +788,28 @@ k_merge_batch(const BatchAsm *B, const int64_t *row0s, int nb, int64_t r_begin, 
   const BatchAsm &b = B[lo];
   if (b.variant != 0) return;          // top-K from the symmetric pass's pairs
   merge_row(b.g, b.gbuf, b.gcnt, b.cap, b.P, r - b.row0, mk[wib]);
+}
+
+// Admitted keys per row of a pair list gathered from several ranks (both ends).
+__global__ void k_pair_rowcounts(const uint4 *__restrict__ pairs, unsigned long long np,
+                                 int32_t *__restrict__ rowcnt) {
+  for (unsigned long long p = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; p < np;
+       p += (unsigned long long)gridDim.x * blockDim.x) {
+    const uint4 x = pairs[p];
+    atomicAdd(rowcnt + x.x, 1);
+    atomicAdd(rowcnt + x.y, 1);
+  }
+}
+
+// out[i] = the largest of the W ranks' partial maxima (blocks of `stride`).
+__global__ void k_max_blocks(const uint32_t *__restrict__ blocks, int W, int64_t stride,
+                             int64_t n, uint32_t *__restrict__ out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t v = 0;
+    for (int r = 0; r < W; ++r) v = max(v, blocks[(int64_t)r * stride + i]);
+    out[i] = v;
+  }
 }
 
 // Row offsets of the admitted keys: exclusive scan of the per-row counts, one CTA.
@@ -966,6 +991,20 @@ void launch_allpairs(const GraphArgs &g, uint64_t *gbuf, int32_t *gcnt, cudaStre
       g, gbuf, gcnt, cap, P);
 }
 
+void launch_pair_rowcounts(const uint4 *pairs, unsigned long long np, int32_t *rowcnt,
+                           cudaStream_t s) {
+  if (np == 0) return;
+  k_pair_rowcounts<<<(unsigned)std::min<unsigned long long>((np + 255) / 256, 148 * 8), 256, 0,
+                     s>>>(pairs, np, rowcnt);
+}
+
+void launch_max_blocks(const uint32_t *blocks, int W, int64_t stride, int64_t n, uint32_t *out,
+                       cudaStream_t s) {
+  if (n == 0) return;
+  k_max_blocks<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 8), 256, 0, s>>>(
+      blocks, W, stride, n, out);
+}
+
 void launch_merge_topk(const GraphArgs &g, const uint64_t *gbuf, const int32_t *gcnt, int cap,
                        int P, cudaStream_t s) {
   const int64_t rows = (g.row_hi < 0 ? g.n : g.row_hi) - g.row_lo;
@@ -974,11 +1013,13 @@ void launch_merge_topk(const GraphArgs &g, const uint64_t *gbuf, const int32_t *
       g, gbuf, gcnt, cap, P);
 }
 
-void launch_allpairs_sym(const GraphArgs &g, const SymOut &o, cudaStream_t s) {
+void launch_allpairs_sym(const GraphArgs &g, const SymOut &o, cudaStream_t s, int x0, int xs) {
   if (g.n == 0) return;
   const int P = allpairs_slices(g.n, g.K);
   const int64_t B = (g.n + 31) / 32;
-  const dim3 grid((unsigned)((B + 1) / 2), (unsigned)(P / kWarps));
+  const int64_t nx = (B + 1) / 2;                 // CTAs of the whole pass
+  if (x0 >= nx) return;
+  const dim3 grid((unsigned)((nx - x0 + xs - 1) / xs), (unsigned)(P / kWarps));
   float lo, hi, lo16;
   prefilter_bands(g.S, g.prefilter_eps, &lo, &hi, &lo16);
   const int v = allpairs_variant(g);
@@ -986,7 +1027,7 @@ void launch_allpairs_sym(const GraphArgs &g, const SymOut &o, cudaStream_t s) {
 #define RBG_TS(KS, SM)                                                                        \
   do {                                                                                        \
     smem_cap_max((const void *)k_allpairs_tc_sym<KS, SM>);                                    \
-    k_allpairs_tc_sym<KS, SM><<<grid, kWarps * 32, smem, s>>>(g, P, lo, hi, lo16, o);         \
+    k_allpairs_tc_sym<KS, SM><<<grid, kWarps * 32, smem, s>>>(g, P, lo, hi, lo16, o, x0, xs); \
   } while (0)
   if (v == 1) RBG_TS(1, 16);
   else if (v == 2) RBG_TS(2, 32);

@@ -220,7 +220,15 @@ struct SymOut {
 };
 // Symmetric pass of the abundance-pruned (tensor-core) regime: row maxima into
 // g.maxcnt_cand, admitted pairs into o.  Requires allpairs_variant(g) != 0.
-void launch_allpairs_sym(const GraphArgs &g, const SymOut &o, cudaStream_t s);
+void launch_allpairs_sym(const GraphArgs &g, const SymOut &o, cudaStream_t s, int x0 = 0,
+                         int xs = 1);
+// A pair list gathered from several ranks: its per-row key counts (rowcnt
+// zeroed by the caller), and the elementwise maximum of W blocks of partial
+// row maxima.
+void launch_pair_rowcounts(const uint4 *pairs, unsigned long long np, int32_t *rowcnt,
+                           cudaStream_t s);
+void launch_max_blocks(const uint32_t *blocks, int W, int64_t stride, int64_t n, uint32_t *out,
+                       cudaStream_t s);
 // The same pass over the pairs (i, j), i < j, whose column j lies in [cb, ce):
 // rows [0, ce) against those columns.  Windows that tile [0, n) score every
 // pair once; rows at or past ce are not read as candidates.
