@@ -23,7 +23,7 @@ CU_SRCS = ["kernels_sketch.cu", "kernels_graph.cu", "kernels_allpairs.cu", "kern
            "kernels_util.cu",
            "noalloc.cu", "kernels_fasta.cu"]
 CPP_SRCS = ["pmh_streams.cpp", "calib.cpp", "engine.cpp", "batch.cpp", "server.cpp", "fasta.cpp",
-            "cache.cpp"]
+            "cache.cpp", "host_pack.cpp"]
 HEADERS = ["rbg_internal.h", "engine_internal.h", "select_topk.cuh",
            "../../include/rabbitbin_b200.h", "gen_zig_tables.py"]
 

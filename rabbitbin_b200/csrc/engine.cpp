@@ -245,18 +245,41 @@ void stage_sketch_chunked(rbg_ctx *c, const rbg_params *p, const char *seqcat,
     sym_clear(c, std::max<int64_t>(n, 1));
     CK(cudaStreamWaitEvent(c->stream, c->ev_aux, 0));   // unit rows, anynz
   }
+  // Packing on the host sends 3/8 of a byte per base instead of the ASCII
+  // byte: while chunk g's words copy, the host packs chunk g + 1 into the
+  // other pinned slot.
+  const bool hpack = pack_on_host();
   int64_t c0 = 0;
   for (int g = 0; g < G; ++g) {
     const int64_t w0 = (int64_t)g * nwords / G & ~(int64_t)1;
     const int64_t w1 = g + 1 == G ? nwords : ((int64_t)(g + 1) * nwords / G & ~(int64_t)1);
     const int64_t b0 = 16 * w0, b1 = std::min<int64_t>(16 * w1, nb);
-    if (b1 > b0)
-      CK(cudaMemcpyAsync(c->ascii.as<char>() + b0, seqcat + b0, (size_t)(b1 - b0),
-                         cudaMemcpyHostToDevice, c->copy));
-    CK(cudaEventRecord(c->ev_chunk[g], c->copy));
-    CK(cudaStreamWaitEvent(c->stream, c->ev_chunk[g], 0));
-    launch_pack_range(c->ascii.as<char>(), nb, w0, w1, c->packed.as<uint32_t>(),
-                      c->nmask.as<uint32_t>(), c->stream);
+    if (hpack) {
+      const int sl = g & 1;
+      const int64_t pairs = (w1 - w0 + 1) / 2;
+      if (pairs > 0) {
+        if (g >= 2) CK(cudaEventSynchronize(c->ev_slot[sl]));   // its previous copy is done
+        const size_t wbytes = (size_t)pairs * 8, mbytes = (size_t)pairs * 4;
+        c->pack_pin[sl].ensure(wbytes + mbytes);
+        uint32_t *hw = c->pack_pin[sl].as<uint32_t>(), *hm = hw + 2 * pairs;
+        host_pack_words(seqcat, nb, w0, w1, hw, hm);
+        CK(cudaMemcpyAsync(c->packed.as<uint32_t>() + w0, hw, wbytes, cudaMemcpyHostToDevice,
+                           c->copy));
+        CK(cudaMemcpyAsync(c->nmask.as<uint32_t>() + w0 / 2, hm, mbytes, cudaMemcpyHostToDevice,
+                           c->copy));
+        CK(cudaEventRecord(c->ev_slot[sl], c->copy));
+      }
+      CK(cudaEventRecord(c->ev_chunk[g], c->copy));
+      CK(cudaStreamWaitEvent(c->stream, c->ev_chunk[g], 0));
+    } else {
+      if (b1 > b0)
+        CK(cudaMemcpyAsync(c->ascii.as<char>() + b0, seqcat + b0, (size_t)(b1 - b0),
+                           cudaMemcpyHostToDevice, c->copy));
+      CK(cudaEventRecord(c->ev_chunk[g], c->copy));
+      CK(cudaStreamWaitEvent(c->stream, c->ev_chunk[g], 0));
+      launch_pack_range(c->ascii.as<char>(), nb, w0, w1, c->packed.as<uint32_t>(),
+                        c->nmask.as<uint32_t>(), c->stream);
+    }
     const int64_t c1 = g + 1 == G ? n
                      : (int64_t)(std::upper_bound(offsets + 1, offsets + n + 1, 16 * w1) -
                                  (offsets + 1));
@@ -277,7 +300,7 @@ void stage_sketch_chunked(rbg_ctx *c, const rbg_params *p, const char *seqcat,
     c0 = c1;
   }
   c->streamed = stream_pairs;
-  c->launches += G;
+  c->launches += hpack ? 0 : G;
   CK(cudaEventRecord(c->ev[1], c->stream));
   CK(cudaEventRecord(c->ev[2], c->stream));
   CK(cudaEventRecord(c->ev[3], c->stream));
@@ -1218,6 +1241,7 @@ int rbg_create(int device, rbg_ctx **out) {
   }
   cudaEventCreateWithFlags(&c->ev_cin, cudaEventDisableTiming);
   for (auto &e : c->ev_chunk) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+  for (auto &e : c->ev_slot) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   *out = c;
   return RBG_OK;
 }
@@ -1251,6 +1275,9 @@ int rbg_destroy(rbg_ctx *c) {
   cudaStreamSynchronize(c->copy);
   for (cudaEvent_t e : {c->ev_in, c->ev_aux, c->ev_a0, c->ev_a1, c->ev_cin}) cudaEventDestroy(e);
   for (auto &e : c->ev_chunk) cudaEventDestroy(e);
+  for (auto &e : c->ev_slot) cudaEventDestroy(e);
+  c->pack_pin[0].release();
+  c->pack_pin[1].release();
   cudaStreamDestroy(c->copy);
   cudaStreamDestroy(c->aux);
   cudaStreamDestroy(c->stream);

@@ -132,6 +132,20 @@ void check_onehot_status(rbg_ctx *c);
 // comparison).
 inline bool dense_on_gemm() { return getenv("RBG_DENSE_ALU") == nullptr; }
 
+// 2-bit packing on the host (host_pack.cpp): words [w0, w1) of the packed
+// bases (w0 even; rounded up to whole word pairs: 2 * ceil((w1 - w0) / 2)
+// words) and their ceil((w1 - w0) / 2) mask words, in k_pack's layout.
+void host_pack_words(const char *ascii, int64_t nbases, int64_t w0, int64_t w1,
+                     uint32_t *packed, uint32_t *mask);
+int host_pack_threads();
+// The end-to-end call copies the ASCII and packs on the device unless
+// RBG_HOST_PACK is set (then the host packs and the copies carry 3/8 of a byte
+// per base; it pays only where the host packs faster than the link copies
+// ASCII) and the host has at least four threads.
+inline bool pack_on_host() {
+  return getenv("RBG_HOST_PACK") != nullptr && host_pack_threads() >= 4;
+}
+
 // Pinned result blocks (pooled).  pinned_take: a block of `bytes` or null;
 // pinned_share: the block now backs graphs whose first edge arrays are
 // `firsts` (distinct), and returns to the pool when rbg_free_graph has been
@@ -308,6 +322,10 @@ struct rbg_ctx {
   // chunked input copy behind the sketch (rbg_bin_graph)
   cudaStream_t copy = nullptr;
   cudaEvent_t ev_cin = nullptr, ev_chunk[rbg::kChunks] = {};
+  // chunks packed on the host (2-bit words, then mask words), two slots, and
+  // the events of their copies
+  rbg::HBuf pack_pin[2];
+  cudaEvent_t ev_slot[2] = {};
   // batch engine
   std::unique_ptr<rbg::BatchBufs> batch;
   // FASTA ingest
