@@ -52,7 +52,8 @@ INT32_LANES_PER_SM = 128
 #     dram__bytes_read.sum,dram__bytes_write.sum,sm__pipe_alu_cycles_active.avg.pct_of_peak_sustained_active
 #     python bench.py --steps 1 --warmup 3 --no-e2e --no-cpu-baseline
 # Reported only when the timed workload is that one.
-ALLPAIRS_NCU = {"contigs": 50000, "samples": 20, "dram_bytes": None, "alu_pipe_frac": None}
+ALLPAIRS_NCU = {"contigs": 50000, "samples": 20, "dram_bytes": 124995328 + 143117312,
+                "alu_pipe_frac": 0.5661}
 
 
 class ClockSampler:
