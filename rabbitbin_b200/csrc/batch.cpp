@@ -173,11 +173,11 @@ int64_t batch_request_bytes(const rbg_params *p, int64_t n, int64_t nbases, int 
   b += n * (int64_t)K * (8 + 4 + 4) + n * 32;                    // top-K, neighbour lists
   if (abd)
     b += n * 256 * (16 + 2 * 8) + n * 12;                        // admitted pairs, keys, rows
-  else if (dense_on_gemm()) {                                    // one-hot rows, candidate lists
+  else if (dense_on_gemm() && onehot_mma_fits(n, m)) {           // one-hot rows, candidate lists
     int GR = 1, GC = 1;
     onehot_mma_grid((int)((n + 255) / 256), (int)((n + 255) / 256), 148, &GR, &GC);
     b += n * (int64_t)std::max(128, 136 * m / 8) +
-         ((n + 31) / 32) * 32 * GC * ((int64_t)onehot_mma_cap(K) * 8 + 4);
+         ((n + 31) / 32) * 32 * 2 * GC * ((int64_t)onehot_mma_cap(n, GC, K, 0) * 4 + 4);
   }
   else
     b += ((n + 31) / 32) * P * 32 * (cap * 8 + 4);               // slice candidate buffers
@@ -248,7 +248,7 @@ void plan_batch(const rbg_params *defaults, const rbg_assembly *asms, int nb, Ba
     a.fused = (a.p->force_path == 2) || (a.p->force_path == 0 && a.n > 25000);
     a.abdfirst = a.fused && a.p->abdfirst && a.S > 1 && a.w_comp < 1.0 && a.w_comp < a.p->min_edge;
     a.variant = a.abdfirst ? a.Kp / 16 : 0;
-    a.gemm = !a.abdfirst && dense_on_gemm();
+    a.gemm = !a.abdfirst && dense_on_gemm() && onehot_mma_fits(a.n, a.m);
     double mult = untuned;
     if (tune) {
       const auto it = tune->find(tune_key(a));

@@ -2,6 +2,7 @@
 // steps that stay sequential by definition (b0 sampling with mt19937_64, the
 // rand()-driven cutoff calibration), and the C ABI of include/rabbitbin_b200.h.
 #include <algorithm>
+#include <deque>
 #include <limits>
 #include <chrono>
 #include <cmath>
@@ -37,15 +38,26 @@ using namespace rbg;
 
 void validate(const rbg_params *p) { validate_params(p); }
 
+// The device tables of the last few (k, m, seed, contract, win_bits)
+// configurations stay resident (about 10 MB each at m = 1000): a stream of
+// assemblies with different sketch sizes reuses them instead of freeing and
+// re-uploading a set per call (cudaFree waits for the device).
 Tables &tables_for(rbg_ctx *c, const rbg_params *p) {
-  if (c->tables && c->tab_k == p->k && c->tab_m == p->m && c->tab_seed == p->pmh_seed &&
-      c->tab_contract == (p->fp_contract != 0) && c->tab_bits == p->win_bits)
-    return *c->tables;
-  if (c->tables) c->tables->release();
-  c->tables = make_tables(p, c->stream);
-  c->tab_k = p->k; c->tab_m = p->m; c->tab_seed = p->pmh_seed;
-  c->tab_contract = p->fp_contract != 0; c->tab_bits = p->win_bits;
-  return *c->tables;
+  const auto key = std::make_tuple(p->k, p->m, p->pmh_seed, p->fp_contract != 0 ? 1 : 0,
+                                   p->win_bits);
+  for (auto it = c->tab_cache.begin(); it != c->tab_cache.end(); ++it)
+    if (it->first == key) {
+      if (it != c->tab_cache.begin())            // most recently used first
+        c->tab_cache.splice(c->tab_cache.begin(), c->tab_cache, it);
+      return *c->tab_cache.front().second;
+    }
+  constexpr size_t kKeep = 6;
+  if (c->tab_cache.size() >= kKeep) {
+    c->tab_cache.back().second->release();
+    c->tab_cache.pop_back();
+  }
+  c->tab_cache.emplace_front(key, make_tables(p, c->stream));
+  return *c->tab_cache.front().second;
 }
 
 // Checks, sizes, offsets and coverage to the device; the ASCII bases are
@@ -201,7 +213,11 @@ void sketch_contigs(rbg_ctx *c, const rbg_params *p, const SketchArgs &a, cudaEv
     c->launches += a.n ? 1 : 0;
     return;
   }
-  launch_count(a, c->stream);
+  c->count_work.ensure(sizeof(unsigned));
+  CK(cudaMemsetAsync(c->count_work.p, 0, sizeof(unsigned), c->stream));
+  SketchArgs ac = a;
+  ac.work = c->count_work.as<unsigned>();
+  launch_count(ac, c->stream);
   if (mid) CK(cudaEventRecord(mid, c->stream));
   launch_minreduce(a, c->stream);
   c->launches += a.n ? 2 : 0;
@@ -555,19 +571,22 @@ void dense_allpairs_onehot(rbg_ctx *c, const GraphArgs &g) {
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   int GR = 1, GC = 1;
   onehot_mma_grid((int)((rows + 255) / 256), (int)((n + 255) / 256), sms, &GR, &GC);
-  const int cap = onehot_mma_cap(g.K);
-  const size_t lists = (size_t)((rows + 31) / 32) * 32 * GC;
-  c->oh_cand.ensure(lists * cap * sizeof(uint64_t));
+  // RBG_ONEHOT_CAP: shorter lists, to exercise the cut inside the kernel
+  const char *cap_env = getenv("RBG_ONEHOT_CAP");
+  const int cap = onehot_mma_cap(n, GC, g.K, cap_env ? atoi(cap_env) : 0);
+  const size_t lists = (size_t)((rows + 31) / 32) * 32 * 2 * GC;
+  c->oh_cand.ensure(lists * cap * sizeof(uint32_t));
   c->oh_cnt.ensure(lists * sizeof(int32_t));
+  c->oh_tab.ensure((size_t)(2 * m + 4) * sizeof(uint32_t));
   c->oh_err.ensure(sizeof(int));
   c->oh_errpin.ensure(sizeof(int));
   // the status accumulates over the calls before the caller's next check
   if (!c->oh_pending) CK(cudaMemsetAsync(c->oh_err.p, 0, sizeof(int), s));
   const char *why = "";
-  const int rc = launch_onehot_mma(g, c->oh_X.as<int8_t>(), ldx, rows, c->oh_cand.as<uint64_t>(),
-                                   c->oh_cnt.as<int32_t>(), c->oh_err.as<int>(), GR, GC, s, &why);
+  const int rc = launch_onehot_mma(g, c->oh_X.as<int8_t>(), ldx, rows, c->oh_cand.as<uint32_t>(),
+                                   cap, c->oh_cnt.as<int32_t>(), c->oh_tab.as<uint32_t>(),
+                                   c->oh_err.as<int>(), GR, GC, s, &why);
   if (rc != RBG_OK) throw Error(rc, std::string("one-hot tensor-core pass: ") + why);
-  launch_merge_topk(g, c->oh_cand.as<uint64_t>(), c->oh_cnt.as<int32_t>(), cap, GC, s);
   // the kernel's wait status comes back with the caller's next synchronisation
   CK(cudaMemcpyAsync(c->oh_errpin.p, c->oh_err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
   c->oh_pending = true;
@@ -788,7 +807,7 @@ void run_graph(rbg_ctx *c, const rbg_params *p, const ShardCtx *sc = nullptr) {
     const int64_t rows = sc ? sc->row_hi - sc->row_lo : n;
     CK(cudaMemsetAsync(c->maxc_cand.p, 0, n1 * sizeof(uint32_t), c->stream));
     CK(cudaMemsetAsync(c->maxc_all.p, 0, n1 * sizeof(uint32_t), c->stream));
-    if (!g.prefilter && dense_on_gemm()) {
+    if (!g.prefilter && dense_on_gemm() && onehot_mma_fits(n, m)) {
       dense_allpairs_onehot(c, g);                      // tensor cores, exact counts
     } else {
       const size_t slots = (size_t)((rows + 31) / 32) * allpairs_slices_rows(rows, n, K) * 32;
@@ -904,9 +923,12 @@ void run_graph(rbg_ctx *c, const rbg_params *p, const ShardCtx *sc = nullptr) {
 // Pinned host blocks for graph results: the four edge arrays of one graph
 // share one block, which the device writes at DMA speed (pageable destinations
 // are slow and page-fault on first touch).  rbg_free_graph returns a block to
-// the pool; a few idle blocks are kept for reuse.  A batch's graphs share one
-// block (each graph's arrays are ranges of the batch-wide arrays): it returns
-// to the pool when the last of them is freed.
+// the pool.  Blocks come in sizes 2^k and 1.5 x 2^k from 1 MB, so a stream of
+// graphs of varying sizes reuses a few blocks instead of pinning and unpinning
+// memory per call (each costs milliseconds); up to 16 idle blocks and 4 GB are
+// kept, the longest idle freed first.  A batch's graphs share one block (each
+// graph's arrays are ranges of the batch-wide arrays): it returns to the pool
+// when the last of them is freed.
 struct PinnedPool {
   struct Shared {
     void *blk;
@@ -915,25 +937,33 @@ struct PinnedPool {
   std::mutex mu;
   std::unordered_map<void *, size_t> live;
   std::unordered_map<void *, Shared *> part;   // a graph's first array -> its shared block
-  std::multimap<size_t, void *> idle;
+  std::deque<std::pair<size_t, void *>> idle;  // oldest first
   size_t idle_bytes = 0;
 
+  // 1, 1.5, 2, 3, 4, 6, ... MB: at most a third of a block unused
+  static size_t size_class(size_t bytes) {
+    size_t c = (size_t)1 << 20;
+    while (c < bytes) c = (c & (c - 1)) == 0 ? c / 2 * 3 : c / 3 * 4;
+    return c;
+  }
+
   void *take(size_t bytes) {
+    const size_t cls = size_class(bytes);
     std::lock_guard<std::mutex> lk(mu);
-    auto it = idle.lower_bound(bytes);
-    if (it != idle.end() && it->first <= 2 * bytes + ((size_t)1 << 20)) {
-      void *p = it->second;
-      live[p] = it->first;
-      idle_bytes -= it->first;
-      idle.erase(it);
-      return p;
-    }
+    for (auto it = idle.rbegin(); it != idle.rend(); ++it)
+      if (it->first == cls) {
+        void *p = it->second;
+        idle_bytes -= cls;
+        idle.erase(std::next(it).base());
+        live[p] = cls;
+        return p;
+      }
     void *p = nullptr;
-    if (cudaHostAlloc(&p, bytes, cudaHostAllocPortable) != cudaSuccess) {
+    if (cudaHostAlloc(&p, cls, cudaHostAllocPortable) != cudaSuccess) {
       cudaGetLastError();
       return nullptr;
     }
-    live[p] = bytes;
+    live[p] = cls;
     return p;
   }
 
@@ -961,14 +991,13 @@ struct PinnedPool {
     }
     auto it = live.find(p);
     if (it == live.end()) return false;
-    idle.emplace(it->second, p);
+    idle.emplace_back(it->second, p);
     idle_bytes += it->second;
     live.erase(it);
-    while (idle.size() > 8 || idle_bytes > ((size_t)4 << 30)) {
-      auto v = idle.begin();
-      idle_bytes -= v->first;
-      cudaFreeHost(v->second);
-      idle.erase(v);
+    while (idle.size() > 16 || idle_bytes > ((size_t)4 << 30)) {
+      idle_bytes -= idle.front().first;
+      cudaFreeHost(idle.front().second);
+      idle.pop_front();
     }
     return true;
   }
@@ -1258,12 +1287,13 @@ int rbg_destroy(rbg_ctx *c) {
                   &c->badflag, &c->tmp, &c->cand_buf, &c->cand_cnt, &c->colacc, &c->unit16,
                   &c->sym_pairs, &c->sym_np, &c->sym_rowcnt, &c->sym_rowoff, &c->sym_keys,
                   &c->shard_send, &c->shard_recv, &c->oh_pres, &c->oh_map, &c->oh_koff,
-                  &c->oh_X, &c->oh_cand, &c->oh_cnt, &c->oh_err, &c->kept, &c->b0dev,
+                  &c->oh_X, &c->oh_cand, &c->oh_cnt, &c->oh_tab, &c->oh_err, &c->kept, &c->b0dev,
+                  &c->count_work,
                   &c->qa, &c->qb, &c->qo, &c->qt, &c->ix_keys, &c->ix_sorted,
                   &c->ix_contig, &c->ix_post, &c->ix_ukeys, &c->ix_count, &c->ix_off,
                   &c->ix_nk, &c->ix_scratch};
   for (DBuf *b : bufs) b->release();
-  if (c->tables) c->tables->release();
+  for (auto &t : c->tab_cache) t.second->release();
   release_batch_graphs(c);
   if (c->batch) c->batch->release();
   if (c->fasta) c->fasta->release();

@@ -5,6 +5,7 @@
 #pragma once
 #include <cstdlib>
 #include <cstring>
+#include <list>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -294,7 +295,8 @@ struct rbg_ctx {
   // dense regime on the tensor cores: code presence, one-hot map and offsets,
   // the one-hot matrix, the candidate lists and their counts, the kernel's
   // wait status (and its pinned copy, valid after the next synchronisation)
-  rbg::DBuf oh_pres, oh_map, oh_koff, oh_X, oh_cand, oh_cnt, oh_err;
+  rbg::DBuf oh_pres, oh_map, oh_koff, oh_X, oh_cand, oh_cnt, oh_tab, oh_err;
+  rbg::DBuf count_work;                 // contig counter of the k-mer count kernel
   rbg::HBuf oh_errpin;
   bool oh_pending = false;
   // ProbMinHash4 queries: operand blocks, output block, metric table
@@ -311,9 +313,9 @@ struct rbg_ctx {
   int path = 0;
   bool graph_ready = false;
   // tables (one configuration cached)
-  std::unique_ptr<rbg::Tables> tables;
-  int tab_k = -1, tab_m = -1, tab_contract = -1, tab_bits = -1;
-  uint64_t tab_seed = 0;
+  // sketch tables by (k, m, seed, contract, win_bits), most recently used first
+  std::list<std::pair<std::tuple<int, int, uint64_t, int, int>, std::unique_ptr<rbg::Tables>>>
+      tab_cache;
   cudaEvent_t ev[12];
   cudaStream_t aux = nullptr;            // depth preparation, overlapped with the sketch
   cudaEvent_t ev_in = nullptr, ev_aux = nullptr, ev_a0 = nullptr, ev_a1 = nullptr;

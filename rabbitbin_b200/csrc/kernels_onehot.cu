@@ -19,7 +19,10 @@ namespace {
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int kPresCols = 512;          // register columns per presence block (16 KB)
 
-// Which codes occur in each register column: 256 bits per column.
+// Which codes occur in each register column: 256 bits per column.  A block
+// takes rows_per_block rows and 512 register columns; a thread reads 4
+// columns of a row at a time (mpad is a multiple of 16, so the 4-byte loads
+// are aligned) and the block's two row streams run side by side.
 __global__ void k_code_presence(const uint8_t *__restrict__ codesA, int64_t n, int m, int mpad,
                                 int64_t rows_per_block, uint32_t *__restrict__ pres) {
   __shared__ uint32_t sp[kPresCols * 8];
@@ -29,13 +32,20 @@ __global__ void k_code_presence(const uint8_t *__restrict__ codesA, int64_t n, i
   __syncthreads();
   const int64_t r0 = (int64_t)blockIdx.x * rows_per_block;
   const int64_t r1 = (r0 + rows_per_block < n) ? r0 + rows_per_block : n;
-  for (int64_t i = r0; i < r1; ++i)
-    for (int r = threadIdx.x; r < nc; r += blockDim.x) {
-      const uint32_t code = codesA[i * mpad + c0 + r];
-      // a column holds a few distinct codes: test before the (contended) atomic
-      if (code && !(sp[r * 8 + (code >> 5)] & (1u << (code & 31))))
-        atomicOr(&sp[r * 8 + (code >> 5)], 1u << (code & 31));
+  const int cq = (threadIdx.x & 127) * 4;               // blockDim.x == 256
+  if (cq < nc) {
+    for (int64_t i = r0 + (threadIdx.x >> 7); i < r1; i += 2) {
+      const uint32_t w4 = __ldg(reinterpret_cast<const uint32_t *>(codesA + i * mpad + c0 + cq));
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const uint32_t code = (w4 >> (8 * u)) & 0xFFu;
+        const int r = cq + u;
+        // a column holds a few distinct codes: test before the (contended) atomic
+        if (code && r < nc && !(sp[r * 8 + (code >> 5)] & (1u << (code & 31))))
+          atomicOr(&sp[r * 8 + (code >> 5)], 1u << (code & 31));
+      }
     }
+  }
   __syncthreads();
   for (int i = threadIdx.x; i < nc * 8; i += blockDim.x)
     if (sp[i]) atomicOr(&pres[(int64_t)c0 * 8 + i], sp[i]);
@@ -211,7 +221,7 @@ void launch_code_presence(const uint8_t *codesA, int64_t n, int m, int mpad, uin
                           cudaStream_t s) {
   cudaMemsetAsync(pres, 0, (size_t)m * 8 * sizeof(uint32_t), s);
   if (n == 0) return;
-  const int64_t rows_per_block = 256;
+  const int64_t rows_per_block = 64;
   const dim3 grid((unsigned)((n + rows_per_block - 1) / rows_per_block),
                   (unsigned)((m + kPresCols - 1) / kPresCols));
   k_code_presence<<<grid, 256, 0, s>>>(codesA, n, m, mpad, rows_per_block, pres);

@@ -16,67 +16,73 @@ namespace {
 
 // Base encoding: A/a->0, C/c->1, G/g->2, T/t->3, anything else invalid
 // (RB_BASE_ENC_LUT, src/rabbit_sketch.h:56-75).
-// One thread per 16 bases: a 128-bit load of ASCII, one packed word out
-// (first base in the top two bits) and 16 bits of the invalid mask; lane pairs
-// merge their halves into one 32-bit mask word.  Four bases per 32-bit step:
-// with l = byte | 0x20, ((l >> 1) ^ (l >> 2)) & 3 is 0, 1, 2, 3 for a, c, g, t;
-// the letter rebuilt from that code (a byte permute of "acgt") equals l exactly
-// for the eight valid letters, which a zero-byte test of the difference marks.
-// Two multiplies gather the four codes and the four invalid bits, first base
-// highest.  Bases past nbases are invalid.
-__global__ void k_pack(const uint4 *__restrict__ ascii, int64_t nbases, int64_t nwords,
-                       int64_t w_begin, int64_t w_end, uint32_t *__restrict__ packed,
-                       uint32_t *__restrict__ nmask) {
-  // w_begin is even, so lane pairs (2i, 2i+1) hold the word pairs of one mask word
-  const int64_t w = w_begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  uint32_t word = 0, bad16 = 0;
-  if (w < w_end) {
-    const uint4 v = ascii[w];
-    const uint32_t q[4] = {v.x, v.y, v.z, v.w};
+// One thread per 32 bases: two 128-bit loads of ASCII, two packed words out
+// (first base in the top two bits) and the mask word of the pair (16 invalid
+// bits per word, the first word in the high half).  Four bases per 32-bit
+// step: with l = byte | 0x20, ((l >> 1) ^ (l >> 2)) & 3 is 0, 1, 2, 3 for a,
+// c, g, t; the letter rebuilt from that code (a byte permute of "acgt") equals
+// l exactly for the eight valid letters, which a zero-byte test of the
+// difference marks.  Two multiplies gather the four codes and the four invalid
+// bits, first base highest.  Bases past nbases are invalid.
+__device__ __forceinline__ void pack16(const uint4 v, int64_t w, int64_t nbases, uint32_t &word,
+                                       uint32_t &bad16) {
+  word = 0;
+  bad16 = 0;
+  const uint32_t q[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const uint32_t l = q[k] | 0x20202020u;
-      uint32_t cw = ((l >> 1) ^ (l >> 2)) & 0x03030303u;
-      const uint32_t sel = (cw & 0x3u) | ((cw >> 4) & 0x30u) | ((cw >> 8) & 0x300u) |
-                           ((cw >> 12) & 0x3000u);
-      const uint32_t y = __byte_perm(0x74676361u, 0u, sel) ^ l;
-      const uint32_t ok = ~(((y & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | y) & 0x80808080u;
-      const uint32_t b = (ok ^ 0x80808080u) >> 7;          // 0x01 in each invalid byte
-      cw &= ~(b * 3u);
-      const uint32_t c8 = (uint32_t)(((uint64_t)cw * 0x40100401ull) >> 24) & 0xFFu;
-      const uint32_t b4 = (uint32_t)(((uint64_t)b * 0x08040201ull) >> 24) & 0xFu;
-      word |= c8 << (24 - 8 * k);
-      bad16 |= b4 << (12 - 4 * k);
-    }
-    const int64_t lim = nbases - w * 16;
-    if (lim < 16) {
-      const int keep = lim > 0 ? (int)lim : 0;
-      bad16 |= 0xFFFFu >> keep;
-      word &= ~(0xFFFFFFFFu >> (2 * keep));
-    }
-    packed[w] = word;
+  for (int k = 0; k < 4; ++k) {
+    const uint32_t l = q[k] | 0x20202020u;
+    uint32_t cw = ((l >> 1) ^ (l >> 2)) & 0x03030303u;
+    const uint32_t sel = (cw & 0x3u) | ((cw >> 4) & 0x30u) | ((cw >> 8) & 0x300u) |
+                         ((cw >> 12) & 0x3000u);
+    const uint32_t y = __byte_perm(0x74676361u, 0u, sel) ^ l;
+    const uint32_t ok = ~(((y & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | y) & 0x80808080u;
+    const uint32_t b = (ok ^ 0x80808080u) >> 7;          // 0x01 in each invalid byte
+    cw &= ~(b * 3u);
+    const uint32_t c8 = (uint32_t)(((uint64_t)cw * 0x40100401ull) >> 24) & 0xFFu;
+    const uint32_t b4 = (uint32_t)(((uint64_t)b * 0x08040201ull) >> 24) & 0xFu;
+    word |= c8 << (24 - 8 * k);
+    bad16 |= b4 << (12 - 4 * k);
   }
-  const uint32_t other = __shfl_xor_sync(0xffffffffu, bad16, 1);
-  if (w < w_end && (threadIdx.x & 1) == 0) {
-    const uint32_t m = (bad16 << 16) | ((w + 1 < nwords) ? other : 0xFFFFu);
-    nmask[w >> 1] = m;
+  const int64_t lim = nbases - w * 16;
+  if (lim < 16) {
+    const int keep = lim > 0 ? (int)lim : 0;
+    bad16 |= 0xFFFFu >> keep;
+    word &= ~(0xFFFFFFFFu >> (2 * keep));
   }
 }
 
-// Invalid bits of the 16 bases of packed word wi, restricted to [s, e).
+// Words [w_begin, w_end) (w_begin even): thread t packs words w_begin + 2t, + 1.
+__global__ void k_pack(const uint4 *__restrict__ ascii, int64_t nbases, int64_t nwords,
+                       int64_t w_begin, int64_t w_end, uint32_t *__restrict__ packed,
+                       uint32_t *__restrict__ nmask) {
+  const int64_t w = w_begin + 2 * ((int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+  if (w >= w_end) return;
+  const bool two = w + 1 < w_end;
+  const uint4 v0 = ascii[w];
+  const uint4 v1 = two ? ascii[w + 1] : make_uint4(0u, 0u, 0u, 0u);
+  uint32_t p0, b0, p1, b1;
+  pack16(v0, w, nbases, p0, b0);
+  pack16(v1, w + 1, nbases, p1, b1);
+  if (two) {
+    *reinterpret_cast<uint2 *>(packed + w) = make_uint2(p0, p1);   // w even: 8-byte aligned
+  } else {
+    packed[w] = p0;
+  }
+  nmask[w >> 1] = (b0 << 16) | ((w + 1 < nwords) ? b1 : 0xFFFFu);
+}
+
+// Invalid bits of the 16 bases of packed word wi, restricted to [s, e)
+// (base t of the word at bit 15 - t; bases before s or from e on are invalid).
 __device__ __forceinline__ uint32_t invalid16(const uint32_t *__restrict__ nmask, int64_t wi,
                                               int64_t s, int64_t e) {
   if (wi < 0) return 0xFFFFu;
   const uint32_t mw = __ldg(nmask + (wi >> 1));
   uint32_t b = (wi & 1) ? (mw & 0xFFFFu) : (mw >> 16);
   const int64_t g0 = wi * 16;
-  if (g0 < s || g0 + 16 > e) {
-#pragma unroll
-    for (int t = 0; t < 16; ++t) {
-      const int64_t g = g0 + t;
-      if (g < s || g >= e) b |= 1u << (15 - t);
-    }
-  }
+  const int64_t dl = s - g0, dh = e - g0;             // first valid, first invalid offset
+  if (dl > 0) b |= dl >= 16 ? 0xFFFFu : (0xFFFFu << (16 - (int)dl)) & 0xFFFFu;
+  if (dh < 16) b |= dh <= 0 ? 0xFFFFu : 0xFFFFu >> (int)dh;
   return b;
 }
 
@@ -103,9 +109,19 @@ __global__ void k_count(SketchArgs a) {
   const int k = a.k;
   uint32_t *hist = sh_hist + wib * 256;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  // warps stride over the contigs, so a long contig does not hold a block's
-  // other warps idle
-  for (int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib; c < a.n; c += warps) {
+  // Each warp takes its next contig from a.work (a counter zeroed before the
+  // launch) when the caller gives one, else every warps-th contig: contig
+  // lengths vary by an order of magnitude, and the counter keeps every warp
+  // busy until the last contigs.
+  auto next_contig = [&](int64_t cur) -> int64_t {
+    if (a.work == nullptr) return cur + warps;
+    unsigned t = 0;
+    if (lane == 0) t = atomicAdd(a.work, 1u);
+    return (int64_t)__shfl_sync(0xffffffffu, t, 0);
+  };
+  const int64_t c_first = a.work ? next_contig(0)
+                                 : (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
+  for (int64_t c = c_first; c < a.n; c = next_contig(c)) {
   for (int v = lane; v < 256; v += 32) hist[v] = 0;
   __syncwarp();
   const int64_t s = a.offsets[c], e = a.offsets[c + 1];
@@ -155,7 +171,15 @@ __global__ void k_count(SketchArgs a) {
         for (int q = 1; q < k; ++q) any |= winbad >> q;
         uint32_t kv = ~any & 0xFFFFu;                   // bit 15-t: k-mer ending at t
         const uint64_t win = ((uint64_t)prev << 32) | cur;
-        if (kv == 0xFFFFu) {
+        if (kv == 0xFFFFu && k == 4) {
+          // the 16 codes are the bytes of the window shifted by 0, 2, 4 and 6 bits
+          const uint32_t sw[4] = {cur, __funnelshift_r(cur, prev, 2),
+                                  __funnelshift_r(cur, prev, 4), __funnelshift_r(cur, prev, 6)};
+#pragma unroll
+          for (int x = 0; x < 4; ++x)
+#pragma unroll
+            for (int y = 0; y < 4; ++y) atomicAdd(&hist[__byte_perm(sw[x], 0u, 0x4440u + y)], 1u);
+        } else if (kv == 0xFFFFu) {
 #pragma unroll
           for (int bp = 15; bp >= 0; --bp)
             atomicAdd(&hist[(uint32_t)(win >> (2 * bp)) & kmask], 1u);
@@ -499,7 +523,8 @@ void launch_pack_range(const char *ascii, int64_t nbases, int64_t w_begin, int64
   if (w_end > nwords) w_end = nwords;
   if (w_end <= w_begin) return;
   const int tb = 256;
-  const int64_t grid = (w_end - w_begin + tb - 1) / tb;
+  const int64_t pairs = (w_end - w_begin + 1) / 2;
+  const int64_t grid = (pairs + tb - 1) / tb;
   k_pack<<<(unsigned)grid, tb, 0, s>>>((const uint4 *)ascii, nbases, nwords, w_begin, w_end,
                                       packed, nmask);
 }
@@ -536,9 +561,12 @@ void launch_count(const SketchArgs &a, cudaStream_t s) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  // about eight contigs per warp: enough to even out the contig lengths
+  // with the contig counter, as many warps as fit (five blocks of 48-register
+  // threads per SM); without it, about eight contigs per warp to even out the
+  // contig lengths
   const int64_t blocks = (a.n + warps - 1) / warps;
-  const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(blocks, (int64_t)sms * 4));
+  const int64_t grid =
+      std::max<int64_t>(1, std::min<int64_t>(blocks, (int64_t)sms * (a.work ? 5 : 4)));
   if (a.gc_norm == 2)
     k_count<true><<<(unsigned)grid, warps * 32, warps * 256 * sizeof(uint32_t), s>>>(a);
   else

@@ -85,6 +85,9 @@ struct SketchArgs {
   // one-permutation sketch keys instead of codes (launch_oph): [n][m], 0 = empty bucket
   uint64_t *oph_keys = nullptr;
   int mpad = 512;                      // row stride of the code arrays (bytes)
+  // optional: a counter, zero at the launch, from which the count kernel's
+  // warps take their contigs (null: a fixed stride)
+  unsigned *work = nullptr;
 };
 
 void launch_pack(const char *ascii, int64_t nbases, uint32_t *packed, uint32_t *nmask,
@@ -196,13 +199,16 @@ void launch_merge_topk(const GraphArgs &g, const uint64_t *gbuf, const int32_t *
 // Dense regime on tcgen05 (kernels_onehot_mma.cu): counts of the rows
 // [g.row_lo, g.row_lo + rows) against every contig as the int8 product of
 // one-hot rows X [n][ldx] (ldx a multiple of 128), consumed in the kernel into
-// per-(row, column group) candidate lists for launch_merge_topk (P = GC) and
-// the row maxima; *err != 0 after it ran when a bounded wait gave up.
-int onehot_mma_cap(int K);
+// per-(row, column group, tile half) lists of 32-bit keys (2 GC lists of cap
+// keys per row) and the row maxima, then merged into g.topk / g.topk_cnt; tab [2m + 4]
+// is scratch for the similarity-rank tables; *err != 0 after it ran when a
+// bounded wait gave up.  Needs onehot_mma_fits(n, m) and 1 <= K <= 448.
+bool onehot_mma_fits(int64_t n, int m);
+int onehot_mma_cap(int64_t n, int GC, int K, int cap_max);
 void onehot_mma_grid(int RB, int NT, int sms, int *GR, int *GC);
 int launch_onehot_mma(const GraphArgs &g, const int8_t *X, int64_t ldx, int64_t rows,
-                      uint64_t *cand, int32_t *cand_cnt, int *err, int GR, int GC,
-                      cudaStream_t s, const char **why);
+                      uint32_t *cand, int cap, int32_t *cand_cnt, uint32_t *tab, int *err, int GR,
+                      int GC, cudaStream_t s, const char **why);
 
 // Output of the symmetric all-pairs pass (each unordered pair scored once): the
 // admitted pairs and, per row, how many admitted keys it holds (both ends).

@@ -65,3 +65,52 @@ __device__ inline uint64_t select_topk(uint64_t *buf, int cnt, int K) {
 }
 
 }  // namespace rbg
+
+namespace rbg {
+
+// The same selection over up to 32 * CAPW unique nonzero 32-bit keys (global
+// or shared buffer), with the early stop; returns the K-th largest key.
+template <int CAPW>
+__device__ inline uint32_t select_topk32(uint32_t *buf, int cnt, int K) {
+  const int lane = threadIdx.x & 31;
+  uint32_t v[CAPW];
+#pragma unroll
+  for (int t = 0; t < CAPW; ++t) {
+    const int i = t * 32 + lane;
+    v[t] = i < cnt ? buf[i] : 0u;
+  }
+  uint32_t P = 0;
+  bool exact = true;
+  for (int bit = 31; bit >= 0; --bit) {
+    const uint32_t c = P | (1u << bit);
+    int k = 0;
+#pragma unroll
+    for (int t = 0; t < CAPW; ++t) k += v[t] >= c;
+    const int tot = (int)__reduce_add_sync(0xffffffffu, (unsigned)k);
+    if (tot >= K) {
+      P = c;
+      if (tot == K) {
+        exact = bit == 0;
+        break;
+      }
+    }
+  }
+  __syncwarp();
+  int out = 0;
+  uint32_t kmin = ~0u;
+#pragma unroll
+  for (int t = 0; t < CAPW; ++t) {
+    const bool keep = v[t] >= P && v[t] != 0u;
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    if (keep) {
+      buf[out + __popc(m & ((1u << lane) - 1u))] = v[t];
+      kmin = v[t] < kmin ? v[t] : kmin;
+    }
+    out += __popc(m);
+  }
+  __syncwarp();
+  if (!exact) P = __reduce_min_sync(0xffffffffu, kmin);
+  return P;
+}
+
+}  // namespace rbg

@@ -273,3 +273,17 @@ def test_graph_small_path_onehot_sizes(gpu_ctx, orc, N, S):
     256-row and 256-column tiles, a single tile, and several column groups."""
     g = _graph_case(gpu_ctx, orc, max(4, N // 250), N, S, seed=900 + N)
     assert g["path"] == 1
+
+
+@pytest.mark.parametrize("N,S", [(3000, 2), (6000, 5)])
+def test_graph_small_path_onehot_cut(gpu_ctx, orc, N, S):
+    """Candidate lists shorter than their column group (RBG_ONEHOT_CAP): the
+    lists are cut to the K best inside the tensor-core kernel, several times
+    per row, and the graph stays the same."""
+    import os
+    os.environ["RBG_ONEHOT_CAP"] = "1"          # the floor: K + 136 keys, rounded
+    try:
+        g = _graph_case(gpu_ctx, orc, 6, N, S, seed=950 + N)
+    finally:
+        os.environ.pop("RBG_ONEHOT_CAP", None)
+    assert g["path"] == 1
