@@ -19,12 +19,12 @@ CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SRCS = ["kernels_sketch.cu", "kernels_graph.cu", "kernels_allpairs.cu", "kernels_onehot.cu",
-           "kernels_onehot_mma.cu", "kernels_pmh_query.cu", "kernels_index.cu",
+           "kernels_onehot_mma.cu", "kernels_sym_tc5.cu", "kernels_pmh_query.cu", "kernels_index.cu",
            "kernels_util.cu",
            "noalloc.cu", "kernels_fasta.cu"]
 CPP_SRCS = ["pmh_streams.cpp", "calib.cpp", "engine.cpp", "batch.cpp", "server.cpp", "fasta.cpp",
             "cache.cpp", "host_pack.cpp"]
-HEADERS = ["rbg_internal.h", "engine_internal.h", "select_topk.cuh",
+HEADERS = ["rbg_internal.h", "engine_internal.h", "select_topk.cuh", "tc05.cuh",
            "../../include/rabbitbin_b200.h", "gen_zig_tables.py"]
 
 

@@ -593,6 +593,97 @@ void dense_allpairs_onehot(rbg_ctx *c, const GraphArgs &g) {
   c->launches += 6;
 }
 
+// Symmetric pass as the tcgen05 prefilter and the per-block check
+// (kernels_sym_tc5.cu): candidate lists per 32-row block, with capacities
+// from the fraction of pairs the last passes kept (or exact ones after a pass
+// whose lists overflowed).  RBG_SYM_SINGLE=1: the single-kernel pass
+// (mma.sync prefilter) instead.
+bool sym_tc5_on() { return getenv("RBG_SYM_SINGLE") == nullptr; }
+
+void sym_tc5_launch(rbg_ctx *c, const GraphArgs &g, const SymOut &o) {
+  const int64_t n = g.n, B32 = (n + 31) / 32;
+  std::vector<int32_t> item0;
+  int RB = 0, NT = 0;
+  const int items = sym_tc5_items(n, item0, &RB, &NT);
+  if (c->tc5_cap.size() != (size_t)B32 || c->tc5_n != n) {   // capacities from the fraction
+    c->tc5_cap.assign((size_t)B32, 0);
+    for (int64_t b = 0; b < B32; ++b) {
+      const double pairs = 32.0 * (double)std::max<int64_t>(n - 32 * b, 0);
+      c->tc5_cap[b] = ((int64_t)(pairs * c->tc5_frac) + 256 + 31) & ~(int64_t)31;
+    }
+    c->tc5_n = n;
+  }
+  // host staging: item0 [RB + 1] int32, coff [B32 + 1] int64
+  const size_t ib = (size_t)(RB + 1) * sizeof(int32_t), ob = (size_t)(B32 + 1) * sizeof(int64_t);
+  c->tc5_pin.ensure(((ib + 15) & ~(size_t)15) + ob);
+  int32_t *hi0 = c->tc5_pin.as<int32_t>();
+  int64_t *hoff = (int64_t *)((char *)c->tc5_pin.p + ((ib + 15) & ~(size_t)15));
+  std::memcpy(hi0, item0.data(), ib);
+  hoff[0] = 0;
+  for (int64_t b = 0; b < B32; ++b) hoff[b + 1] = hoff[b] + c->tc5_cap[b];
+  c->tc5_items.ensure(ib);
+  c->tc5_coff.ensure(ob);
+  c->tc5_cand.ensure((size_t)std::max<int64_t>(hoff[B32], 1) * sizeof(uint32_t));
+  c->tc5_cnt.ensure((size_t)B32 * sizeof(int32_t));
+  c->tc5_u16p.ensure((size_t)n * 128);
+  c->tc5_flags.ensure(2 * sizeof(int));
+  cudaStream_t s = c->stream;
+  CK(cudaMemcpyAsync(c->tc5_items.p, hi0, ib, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(c->tc5_coff.p, hoff, ob, cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(c->tc5_cnt.p, 0, (size_t)B32 * sizeof(int32_t), s));
+  CK(cudaMemsetAsync(c->tc5_flags.p, 0, 2 * sizeof(int), s));
+  int dev = 0, sms = 148;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const char *why = "";
+  const int rc = launch_sym_prefilter(
+      g, c->tc5_u16p.as<uint16_t>(), prefilter_lo16(g.S, g.prefilter_eps),
+      c->tc5_items.as<int32_t>(), RB, NT, items, c->tc5_cand.as<uint32_t>(),
+      c->tc5_coff.as<int64_t>(), c->tc5_cnt.as<int32_t>(), c->tc5_flags.as<int>(),
+      c->tc5_flags.as<int>() + 1, sms, s, &why);
+  if (rc != RBG_OK) throw Error(rc, std::string("tensor-core prefilter: ") + why);
+  launch_sym_check(g, o, c->tc5_cand.as<uint32_t>(), c->tc5_coff.as<int64_t>(),
+                   c->tc5_cnt.as<int32_t>(), s);
+  c->launches += 3;
+}
+
+// After the pass's synchronisation (the flags and counts read back into
+// c->tc5_host): false when a list overflowed (capacities now exact: rerun).
+bool sym_tc5_settle(rbg_ctx *c, int64_t n) {
+  const int64_t B32 = (n + 31) / 32;
+  const int *fl = c->tc5_host.as<int>();
+  const int32_t *cnt = fl + 4;
+  if (fl[1] != 0)
+    throw Error(RBG_ERR_TIMEOUT, "tensor-core prefilter: a bounded device wait gave up (stage " +
+                                     std::to_string(fl[1]) + ")");
+  double frac = 0.0;
+  for (int64_t b = 0; b < B32; ++b) {
+    const double pairs = 32.0 * (double)std::max<int64_t>(n - 32 * b, 0);
+    if (pairs > 0) frac = std::max(frac, cnt[b] / pairs);
+  }
+  if (fl[0] != 0) {
+    for (int64_t b = 0; b < B32; ++b)
+      c->tc5_cap[b] = std::max<int64_t>(c->tc5_cap[b], ((int64_t)cnt[b] + 256 + 31) & ~(int64_t)31);
+    c->tc5_frac = std::max(c->tc5_frac, frac * 1.25);
+    return false;
+  }
+  if (frac * 1.25 > c->tc5_frac) {           // the next assemblies get room to spare
+    c->tc5_frac = frac * 1.25;
+    c->tc5_n = -1;
+  }
+  return true;
+}
+
+// The flags and per-block counts to the host on the stream (read after its sync).
+void sym_tc5_readback(rbg_ctx *c, int64_t n) {
+  const int64_t B32 = (n + 31) / 32;
+  c->tc5_host.ensure((size_t)(4 + B32) * sizeof(int32_t));
+  CK(cudaMemcpyAsync(c->tc5_host.p, c->tc5_flags.p, 2 * sizeof(int), cudaMemcpyDeviceToHost,
+                     c->stream));
+  CK(cudaMemcpyAsync(c->tc5_host.as<int32_t>() + 4, c->tc5_cnt.p, (size_t)B32 * sizeof(int32_t),
+                     cudaMemcpyDeviceToHost, c->stream));
+}
+
 void check_onehot_status(rbg_ctx *c) {
   if (!c->oh_pending) return;
   c->oh_pending = false;
@@ -766,12 +857,18 @@ void run_graph(rbg_ctx *c, const rbg_params *p, const ShardCtx *sc = nullptr) {
     bool streamed = streamed_in;
     for (;;) {
       SymOut o = sym_buffers(c, n1);
+      const bool tc5 = !streamed && sym_tc5_on() && g.Kp <= 64 && n < ((int64_t)1 << 27);
       if (streamed) {
         o.defer = 1;
       } else {
         sym_clear(c, n1);
-        launch_allpairs_sym(g, o, c->stream);
-        c->launches += 1;
+        if (tc5) {
+          sym_tc5_launch(c, g, o);
+          sym_tc5_readback(c, n);
+        } else {
+          launch_allpairs_sym(g, o, c->stream);
+          c->launches += 1;
+        }
       }
       CK(cudaGetLastError());
       CK(cudaEventRecord(c->ev[6], c->stream));
@@ -788,6 +885,10 @@ void run_graph(rbg_ctx *c, const rbg_params *p, const ShardCtx *sc = nullptr) {
       CK(cudaGetLastError());
       c->launches += 3;
       CK(cudaEventSynchronize(c->ev[10]));
+      if (tc5 && !sym_tc5_settle(c, n)) {           // a candidate list overflowed: rerun
+        CK(cudaStreamSynchronize(c->stream));
+        continue;
+      }
       if (*hnp <= c->sym_cap) break;
       CK(cudaStreamSynchronize(c->stream));
       if (streamed) {
@@ -1288,7 +1389,8 @@ int rbg_destroy(rbg_ctx *c) {
                   &c->sym_pairs, &c->sym_np, &c->sym_rowcnt, &c->sym_rowoff, &c->sym_keys,
                   &c->shard_send, &c->shard_recv, &c->oh_pres, &c->oh_map, &c->oh_koff,
                   &c->oh_X, &c->oh_cand, &c->oh_cnt, &c->oh_tab, &c->oh_err, &c->kept, &c->b0dev,
-                  &c->count_work,
+                  &c->count_work, &c->tc5_u16p, &c->tc5_cand, &c->tc5_cnt, &c->tc5_items,
+                  &c->tc5_coff, &c->tc5_flags,
                   &c->qa, &c->qb, &c->qo, &c->qt, &c->ix_keys, &c->ix_sorted,
                   &c->ix_contig, &c->ix_post, &c->ix_ukeys, &c->ix_count, &c->ix_off,
                   &c->ix_nk, &c->ix_scratch};
@@ -1308,6 +1410,8 @@ int rbg_destroy(rbg_ctx *c) {
   for (auto &e : c->ev_slot) cudaEventDestroy(e);
   c->pack_pin[0].release();
   c->pack_pin[1].release();
+  c->tc5_pin.release();
+  c->tc5_host.release();
   cudaStreamDestroy(c->copy);
   cudaStreamDestroy(c->aux);
   cudaStreamDestroy(c->stream);

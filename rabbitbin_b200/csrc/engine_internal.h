@@ -297,6 +297,13 @@ struct rbg_ctx {
   // wait status (and its pinned copy, valid after the next synchronisation)
   rbg::DBuf oh_pres, oh_map, oh_koff, oh_X, oh_cand, oh_cnt, oh_tab, oh_err;
   rbg::DBuf count_work;                 // contig counter of the k-mer count kernel
+  // symmetric pass on the tensor-core prefilter: candidate lists per 32-row
+  // block (capacities tc5_cap, sized from the kept fraction tc5_frac)
+  rbg::DBuf tc5_u16p, tc5_cand, tc5_cnt, tc5_items, tc5_coff, tc5_flags;
+  rbg::HBuf tc5_pin, tc5_host;
+  std::vector<int64_t> tc5_cap;
+  int64_t tc5_n = -1;
+  double tc5_frac = 0.03;
   rbg::HBuf oh_errpin;
   bool oh_pending = false;
   // ProbMinHash4 queries: operand blocks, output block, metric table

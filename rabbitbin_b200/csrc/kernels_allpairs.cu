@@ -193,30 +193,33 @@ __device__ __forceinline__ void count_batch_coop(const GraphArgs &g, Warp &w, co
 // state, row j by an atomic) and, when its similarity passes the admission
 // floor, is appended once to the pair list with both rows' counts raised.
 // grow0: the assembly's first row in the row space of the pair list.
+template <int NF = 4>
 __device__ __forceinline__ void count_batch_sym(const GraphArgs &g, const SymOut &o, uint32_t *mxc,
                                                 int64_t row0, int64_t grow0, const int *q, int nq,
                                                 const unsigned char *sA) {
   const int lane = threadIdx.x & 31;
   const int m16 = g.mpad >> 4;
   uint32_t mine = 0;
-  for (int p = 0; p < nq; p += 4) {
-    const uint4 *ra[4], *cb[4];
+  for (int p = 0; p < nq; p += NF) {               // NF survivors' column codes in flight
+    const uint4 *ra[NF], *cb[NF];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
+    for (int u = 0; u < NF; ++u) {
       const unsigned e = (unsigned)q[p + u < nq ? p + u : p];
       ra[u] = (const uint4 *)(sA + (size_t)(e >> 27) * g.mpad);
       cb[u] = (const uint4 *)(g.codesB + (int64_t)(e & 0x07FFFFFFu) * g.mpad);
     }
-    uint32_t acc[4] = {0u, 0u, 0u, 0u};
+    uint32_t acc[NF];
+#pragma unroll
+    for (int u = 0; u < NF; ++u) acc[u] = 0u;
     for (int t = lane; t < m16; t += 32) {
-      uint4 b[4];
+      uint4 b[NF];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) b[u] = __ldg(cb[u] + t);
+      for (int u = 0; u < NF; ++u) b[u] = __ldg(cb[u] + t);
 #pragma unroll
-      for (int u = 0; u < 4; ++u) acc[u] = eq16(lds128(ra[u] + t), b[u], acc[u]);
+      for (int u = 0; u < NF; ++u) acc[u] = eq16(lds128(ra[u] + t), b[u], acc[u]);
     }
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
+    for (int u = 0; u < NF; ++u) {
       const uint32_t c = __reduce_add_sync(FULL, acc[u]) >> 7;
       if (lane == p + u) mine = c;
     }
@@ -412,8 +415,9 @@ __device__ __forceinline__ void ldsm_x2(uint32_t &r0, uint32_t &r1, const void *
 }
 
 // Exact prune decision for up to 32 queued candidates (lane = candidate),
-// survivors appended to the counting queue.
-template <int SMAX, bool SYM>
+// survivors appended to the counting queue.  RING: candidates in the check
+// ring at head (modulo kCQ); otherwise a plain list from cq + head.
+template <int SMAX, bool SYM, bool RING = true>
 __device__ __forceinline__ void check_batch(const GraphArgs &g, Warp &w, const SymOut &o,
                                             int64_t grow0, const int *cq, unsigned head, int nq,
                                             int64_t row0, int *q, int &qn, float lo, float hi,
@@ -421,7 +425,7 @@ __device__ __forceinline__ void check_batch(const GraphArgs &g, Warp &w, const S
                                             int SuP, const unsigned char *sA) {
   const int lane = threadIdx.x & 31;
   const bool act = lane < nq;
-  const unsigned e = act ? (unsigned)cq[(head + lane) % kCQ] : 0u;
+  const unsigned e = act ? (unsigned)cq[RING ? (head + lane) % kCQ : head + lane] : 0u;
   const int r = (int)(e >> 27);
   const int64_t j = e & 0x07FFFFFFu;
   const int64_t row = row0 + r;
@@ -453,7 +457,7 @@ __device__ __forceinline__ void check_batch(const GraphArgs &g, Warp &w, const S
   qn += __popc(m);
   __syncwarp();
   if (qn >= 32) {
-    if constexpr (SYM) count_batch_sym(g, o, w.mxc, row0, grow0, q, 32, sA);
+    if constexpr (SYM) count_batch_sym<RING ? 4 : 8>(g, o, w.mxc, row0, grow0, q, 32, sA);
     else count_batch_coop(g, w, q, 32, sA);
     n_cmp += 1;
     if (lane + 32 < qn) q[lane] = q[lane + 32];
@@ -692,6 +696,80 @@ k_allpairs_tc_win(GraphArgs g, int P, float lo, float hi, float lo16, SymOut o, 
   extern __shared__ __align__(16) unsigned char smem[];
   tc_item<KS, SMAX, true>(g, nullptr, nullptr, 0, P, lo, hi, lo16, blockIdx.x, blockIdx.y, smem, o,
                           0, cb, ce);
+}
+
+// Symmetric pass, part 2 (after k_sym_prefilter, kernels_sym_tc5.cu): a CTA
+// takes 32-row block x and block B-1-x (as k_allpairs_tc_sym pairs them), with
+// the block's register codes and unit rows in shared memory, and its warps work
+// through the block's candidate list 32 entries at a time: the exact prune
+// decision (check_batch), then the survivors' register compares and pair
+// records (count_batch_sym), exactly as in the single-kernel pass.
+template <int SMAX>
+__device__ __forceinline__ void sym_check_block(const GraphArgs &g, const SymOut &o, float lo,
+                                                float hi, const uint32_t *cand,
+                                                const int64_t *coff, const int32_t *ccnt,
+                                                int64_t bx, unsigned char *smem) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t n = g.n, row0 = bx * 32;
+  unsigned char *ws = smem + (size_t)warp * kTcWs;
+  uint64_t *thr = (uint64_t *)ws;
+  int *cntw = (int *)(thr + 32);
+  uint32_t *mxc = (uint32_t *)(cntw + 32);
+  int *q = (int *)(mxc + 32);                      // [64] survivors to count
+  unsigned char *sA = smem + (size_t)kWarps * kTcWs;
+  float *sU = (float *)(sA + (size_t)32 * g.mpad);
+  const int SuP = su_stride(g.Su);
+  {
+    const int m16 = g.mpad >> 4, s4 = g.Su >> 2;
+    for (int i = threadIdx.x; i < 32 * m16; i += blockDim.x) {
+      const int r = i / m16, t = i - r * m16;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (row0 + r < n) v = __ldg((const uint4 *)(g.codesA + (row0 + r) * g.mpad) + t);
+      *((uint4 *)(sA + (size_t)r * g.mpad) + t) = v;
+    }
+    for (int i = threadIdx.x; i < 32 * s4; i += blockDim.x) {
+      const int r = i / s4, t = i - r * s4;
+      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (row0 + r < n) v = __ldg((const float4 *)(g.unit + (row0 + r) * g.Su) + t);
+      *((float4 *)(sU + (size_t)r * SuP) + t) = v;
+    }
+  }
+  mxc[lane] = 0;
+  __syncthreads();
+  Warp w{nullptr, cntw, thr, mxc, 0, g.K};
+  unsigned long long n_cmp = 0;
+  int qn = 0;
+  const int64_t off = coff[bx];
+  const int cnt = (int)min((int64_t)ccnt[bx], coff[bx + 1] - off);
+  const int *list = (const int *)(cand + off);
+  for (int i0 = warp * 32; i0 < cnt; i0 += kWarps * 32)
+    check_batch<SMAX, true, false>(g, w, o, 0, list, (unsigned)i0, min(32, cnt - i0), row0, q,
+                                   qn, lo, hi, n_cmp, sU, SuP, sA);
+  if (qn > 0) {
+    n_cmp += lane < qn;
+    count_batch_sym<8>(g, o, mxc, row0, 0, q, qn, sA);
+  }
+  if (g.stats) {
+    const unsigned b = __reduce_add_sync(FULL, (unsigned)n_cmp);
+    if (lane == 0 && b) atomicAdd(g.stats + 1, (unsigned long long)b);
+  }
+  __syncwarp();
+  const int64_t row = row0 + lane;
+  if (row < n && mxc[lane]) atomicMax(g.maxcnt_cand + row, mxc[lane]);
+}
+
+template <int SMAX>
+__global__ void __launch_bounds__(kWarps * 32, SMAX == 32 ? 6 : 1)
+k_sym_check(GraphArgs g, float lo, float hi, SymOut o, const uint32_t *cand,
+            const int64_t *coff, const int32_t *ccnt) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int64_t B = (g.n + 31) / 32;
+  const int64_t b1 = blockIdx.x, b2 = B - 1 - b1;
+  sym_check_block<SMAX>(g, o, lo, hi, cand, coff, ccnt, b1, smem);
+  if (b2 > b1) {
+    __syncthreads();
+    sym_check_block<SMAX>(g, o, lo, hi, cand, coff, ccnt, b2, smem);
+  }
 }
 
 // Persistent form over a batch: CTAs pull (assembly, row block, slice group)
@@ -1011,6 +1089,33 @@ void launch_merge_topk(const GraphArgs &g, const uint64_t *gbuf, const int32_t *
   if (rows <= 0) return;
   k_merge_topk<<<(unsigned)((rows + kMergeWarps - 1) / kMergeWarps), kMergeWarps * 32, 0, s>>>(
       g, gbuf, gcnt, cap, P);
+}
+
+void launch_sym_check(const GraphArgs &g, const SymOut &o, const uint32_t *cand,
+                      const int64_t *coff, const int32_t *ccnt, cudaStream_t s) {
+  if (g.n == 0) return;
+  const int64_t B = (g.n + 31) / 32;
+  float lo, hi, lo16;
+  prefilter_bands(g.S, g.prefilter_eps, &lo, &hi, &lo16);
+  const int v = allpairs_variant(g);
+  const size_t smem = (size_t)kWarps * kTcWs + (size_t)32 * g.mpad +
+                      (size_t)32 * su_stride(g.Su) * 4;
+  const unsigned grid = (unsigned)((B + 1) / 2);
+#define RBG_SC(SM)                                                                        \
+  do {                                                                                    \
+    smem_cap_max((const void *)k_sym_check<SM>);                                          \
+    k_sym_check<SM><<<grid, kWarps * 32, smem, s>>>(g, lo, hi, o, cand, coff, ccnt);      \
+  } while (0)
+  if (v == 1) RBG_SC(16);
+  else if (v == 2) RBG_SC(32);
+  else RBG_SC(64);
+#undef RBG_SC
+}
+
+float prefilter_lo16(int S, float eps) {
+  float lo, hi, lo16;
+  prefilter_bands(S, eps, &lo, &hi, &lo16);
+  return lo16;
 }
 
 void launch_allpairs_sym(const GraphArgs &g, const SymOut &o, cudaStream_t s, int x0, int xs) {

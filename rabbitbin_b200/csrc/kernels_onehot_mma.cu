@@ -55,9 +55,12 @@
 
 #include "rbg_internal.h"
 #include "select_topk.cuh"
+#include "tc05.cuh"
 
 namespace rbg {
 namespace {
+
+using namespace tc05;
 
 constexpr int kTM = 256;                      // rows per CTA tile
 constexpr int kTN = 256;                      // columns per CTA tile
@@ -69,7 +72,6 @@ constexpr int kEpiWarps = 16;
 constexpr int kCapW32 = 32;                   // list capacity: 32 * kCapW32 keys
 constexpr int kThreads = (2 + kEpiWarps) * 32;
 constexpr unsigned FULL = 0xffffffffu;
-constexpr uint64_t kWaitNs = 2000000000ull;   // bound of every mbarrier wait
 
 // instruction descriptor: D s32 (bits 4-5 = 2), A and B unsigned 8-bit (bits
 // 7-9, 10-12 = 0), both K-major (bits 15, 16 = 0), N >> 3 at bits 17-22,
@@ -89,90 +91,12 @@ struct OhArgs {
   int *err;              // set when a bounded wait runs out
 };
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ uint64_t now_ns() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t a, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count));
-}
-
-__device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(a), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// Bounded wait for the phase of parity `parity` to complete; false (and the
-// error code recorded) when it does not within kWaitNs.
-__device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity, int *err, int code) {
-  if (mbar_try(a, parity)) return true;
-  const uint64_t t0 = now_ns();
-  for (;;) {
-    if (mbar_try(a, parity)) return true;
-    if (now_ns() - t0 > kWaitNs) {
-      atomicCAS(err, 0, code);
-      return false;
-    }
-  }
-}
-
-__device__ __forceinline__ void mbar_arrive(uint32_t a) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(a) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint32_t a, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes)
-               : "memory");
-}
-
-// 2-D TMA tile load (no multicast): box at (x bytes, y rows) into dst.
-__device__ __forceinline__ void tma_load(uint32_t dst, const CUtensorMap *map, int x, int y,
-                                         uint32_t mbar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
-      ::"r"(dst), "l"((uint64_t)map), "r"(x), "r"(y), "r"(mbar)
-      : "memory");
-}
-
-// UMMA shared-memory descriptor of a K-major operand block in the 128-byte
-// swizzle layout TMA writes: rows of 128 bytes, 8-row atoms 1024 bytes apart
-// (SBO), version 1 (bits 46-47), layout SWIZZLE_128B (2 at bits 61-63).
-__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
-  return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)1 << 16) |
-         ((uint64_t)(1024 >> 4) << 32) | ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
-}
-
 __device__ __forceinline__ void mma_i8(uint32_t dt, uint64_t ad, uint64_t bd, uint32_t acc) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
       ::"r"(dt), "l"(ad), "l"(bd), "r"(kIdesc), "r"(acc));
-}
-
-__device__ __forceinline__ void mma_commit(uint32_t mbar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-               ::"r"(mbar) : "memory");
-}
-
-__device__ __forceinline__ void tc_fence_before() {
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() {
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
 
 // 128 consecutive TMEM columns of this warp's 32 lanes as 16-bit values, two
@@ -258,9 +182,9 @@ k_onehot_mma(const __grid_constant__ CUtensorMap tmap, const OhArgs A) {
                  ::"r"(smem_u32(tmem_slot)) : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  tc_fence_before();
+  fence_before();
   __syncthreads();
-  tc_fence_after();
+  fence_after();
   const uint32_t tbase = *tmem_slot;
   const int nrb = (A.RB - a + A.GR - 1) / A.GR;  // row blocks of this CTA
 
@@ -309,17 +233,17 @@ k_onehot_mma(const __grid_constant__ CUtensorMap tmap, const OhArgs A) {
             *(volatile int *)abort_flag = 1;
             break;
           }
-          tc_fence_after();
+          fence_after();
           for (int kc = 0; kc < A.nkc; ++kc) {
             if (!mbar_wait(full_bar(s), ph, A.err, 4) || *(volatile int *)abort_flag) {
               ok = false;
               *(volatile int *)abort_flag = 1;
               break;
             }
-            tc_fence_after();
+            fence_after();
             const uint32_t st = smem_u32(ring + (size_t)s * kStageBytes);
-            const uint64_t da0 = sdesc(st), da1 = sdesc(st + kHalfBytes),
-                           db = sdesc(st + 2 * kHalfBytes);
+            const uint64_t da0 = sdesc128(st), da1 = sdesc128(st + kHalfBytes),
+                           db = sdesc128(st + 2 * kHalfBytes);
 #pragma unroll
             for (int k = 0; k < kKC / 32; ++k) {
               const uint32_t acc = (kc | k) ? 1u : 0u;
@@ -409,12 +333,12 @@ k_onehot_mma(const __grid_constant__ CUtensorMap tmap, const OhArgs A) {
           *(volatile int *)abort_flag = 1;
           break;
         }
-        tc_fence_after();
+        fence_after();
         const uint32_t *nzt = nzw + (tcount & 1) * 8 + ch * 4;
         uint32_t pk[64];                         // the 128 counts, two per register
         tmem_ld128_pack16(tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(half * kTN + ch * 128),
                           pk);
-        tc_fence_before();
+        fence_before();
         mbar_arrive(tempty);                     // TMEM is free for the next tile's MMAs
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
@@ -509,23 +433,9 @@ k_onehot_mma(const __grid_constant__ CUtensorMap tmap, const OhArgs A) {
     }
   }
   __syncthreads();
-  tc_fence_after();
+  fence_after();
   if (warp == 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tbase) : "memory");
-}
-
-// cuTensorMapEncodeTiled from the driver the runtime already loaded.
-PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-  static std::once_flag once;
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  std::call_once(once, [] {
-    void *p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
-            cudaSuccess && q == cudaDriverEntryPointSuccess)
-      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
-  });
-  return fn;
 }
 
 size_t oh_smem(int m) {

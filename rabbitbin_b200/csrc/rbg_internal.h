@@ -228,6 +228,23 @@ struct SymOut {
 // g.maxcnt_cand, admitted pairs into o.  Requires allpairs_variant(g) != 0.
 void launch_allpairs_sym(const GraphArgs &g, const SymOut &o, cudaStream_t s, int x0 = 0,
                          int xs = 1);
+
+// Symmetric pass in two kernels (kernels_sym_tc5.cu, kernels_allpairs.cu): the
+// tcgen05 abundance prefilter writes each 32-row block's candidates (entries
+// r << 27 | j at cand + coff[b], capacity coff[b + 1] - coff[b], the count in
+// ccnt[b] even past it; *overflow set then), k_sym_check decides and counts
+// them into o.  item0 [RB + 1] from sym_tc5_items; u16p: n x 128 bytes of
+// scratch (16-byte aligned).  Needs g.Kp <= 64 and n < 2^27.
+int sym_tc5_items(int64_t n, std::vector<int32_t> &item0, int *RB, int *NT);
+int launch_sym_prefilter(const GraphArgs &g, uint16_t *u16p, float lo16, const int32_t *item0,
+                         int RB, int NT, int items, uint32_t *cand, const int64_t *coff,
+                         int32_t *ccnt, int *overflow, int *err, int sms, cudaStream_t s,
+                         const char **why);
+void launch_sym_check(const GraphArgs &g, const SymOut &o, const uint32_t *cand,
+                      const int64_t *coff, const int32_t *ccnt, cudaStream_t s);
+// The prefilter's FP16 threshold: a candidate from lo16 on.
+float prefilter_lo16(int S, float eps);
+
 // A pair list gathered from several ranks: its per-row key counts (rowcnt
 // zeroed by the caller), and the elementwise maximum of W blocks of partial
 // row maxima.
