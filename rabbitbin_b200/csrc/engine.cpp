@@ -254,12 +254,15 @@ void stage_sketch_chunked(rbg_ctx *c, const rbg_params *p, const char *seqcat,
                             !((c->no_stream_S >> (S & 63)) & 1u);
   GraphArgs ga;
   SymOut o;
+  bool tc5 = false;
   if (stream_pairs) {
     ga = graph_args(c, p);
     o = sym_buffers(c, std::max<int64_t>(n, 1));
     o.defer = 1;
     sym_clear(c, std::max<int64_t>(n, 1));
     CK(cudaStreamWaitEvent(c->stream, c->ev_aux, 0));   // unit rows, anynz
+    tc5 = sym_tc5_fits(ga);
+    if (tc5) sym_tc5_setup(c, ga, G);
   }
   // Packing on the host sends 3/8 of a byte per base instead of the ASCII
   // byte: while chunk g's words copy, the host packs chunk g + 1 into the
@@ -309,13 +312,18 @@ void stage_sketch_chunked(rbg_ctx *c, const rbg_params *p, const char *seqcat,
       a.codesB += c0 * mpad;
       sketch_contigs(c, p, a, nullptr);
       if (stream_pairs) {
-        launch_allpairs_sym_window(ga, o, c0, c1, c->stream);
-        c->launches += 1;
+        if (tc5) {
+          sym_tc5_pass(c, ga, o, c0, c1, g);
+        } else {
+          launch_allpairs_sym_window(ga, o, c0, c1, c->stream);
+          c->launches += 1;
+        }
       }
     }
     c0 = c1;
   }
   c->streamed = stream_pairs;
+  c->streamed_tc5 = stream_pairs && tc5;
   c->launches += hpack ? 0 : G;
   CK(cudaEventRecord(c->ev[1], c->stream));
   CK(cudaEventRecord(c->ev[2], c->stream));
@@ -600,50 +608,68 @@ void dense_allpairs_onehot(rbg_ctx *c, const GraphArgs &g) {
 // (mma.sync prefilter) instead.
 bool sym_tc5_on() { return getenv("RBG_SYM_SINGLE") == nullptr; }
 
-void sym_tc5_launch(rbg_ctx *c, const GraphArgs &g, const SymOut &o) {
-  const int64_t n = g.n, B32 = (n + 31) / 32;
-  std::vector<int32_t> item0;
-  int RB = 0, NT = 0;
-  const int items = sym_tc5_items(n, item0, &RB, &NT);
-  if (c->tc5_cap.size() != (size_t)B32 || c->tc5_n != n) {   // capacities from the fraction
-    c->tc5_cap.assign((size_t)B32, 0);
-    for (int64_t b = 0; b < B32; ++b) {
-      const double pairs = 32.0 * (double)std::max<int64_t>(n - 32 * b, 0);
-      c->tc5_cap[b] = ((int64_t)(pairs * c->tc5_frac) + 256 + 31) & ~(int64_t)31;
-    }
-    c->tc5_n = n;
+bool sym_tc5_fits(const GraphArgs &g) {
+  return sym_tc5_on() && g.Kp <= 64 && g.n > 0 && g.n < ((int64_t)1 << 27);
+}
+
+// Buffers, list capacities (for the whole assembly), the padded FP16 rows and
+// cleared flags for the passes over one assembly; `slots` item tables (one per
+// pass in flight).  The capacities come from the kept fraction, or exact ones
+// right after a pass whose lists overflowed (the one host copy here, on a
+// rerun only); offsets and item tables are made on the device, so nothing is
+// copied in while input chunks stream in.
+void sym_tc5_setup(rbg_ctx *c, const GraphArgs &g, int slots) {
+  const int64_t n = g.n, B32 = (n + 31) / 32, RBmax = (n + 127) / 128;
+  cudaStream_t s = c->stream;
+  int64_t total = 0;
+  c->tc5_coff.ensure((size_t)(B32 + 1) * sizeof(int64_t));
+  if (c->tc5_exact && c->tc5_n == n && c->tc5_cap.size() == (size_t)B32) {
+    for (int64_t b = 0; b < B32; ++b) total += c->tc5_cap[b];
+    c->tc5_pin.ensure((size_t)B32 * sizeof(int64_t));
+    std::memcpy(c->tc5_pin.p, c->tc5_cap.data(), (size_t)B32 * sizeof(int64_t));
+    c->tc5_caps.ensure((size_t)B32 * sizeof(int64_t));
+    CK(cudaMemcpyAsync(c->tc5_caps.p, c->tc5_pin.p, (size_t)B32 * sizeof(int64_t),
+                       cudaMemcpyHostToDevice, s));
+    launch_tc5_coff(n, 0.0, c->tc5_caps.as<int64_t>(), c->tc5_coff.as<int64_t>(), s);
+  } else {
+    total = tc5_capacity(n, c->tc5_frac);
+    launch_tc5_coff(n, c->tc5_frac, nullptr, c->tc5_coff.as<int64_t>(), s);
   }
-  // host staging: item0 [RB + 1] int32, coff [B32 + 1] int64
-  const size_t ib = (size_t)(RB + 1) * sizeof(int32_t), ob = (size_t)(B32 + 1) * sizeof(int64_t);
-  c->tc5_pin.ensure(((ib + 15) & ~(size_t)15) + ob);
-  int32_t *hi0 = c->tc5_pin.as<int32_t>();
-  int64_t *hoff = (int64_t *)((char *)c->tc5_pin.p + ((ib + 15) & ~(size_t)15));
-  std::memcpy(hi0, item0.data(), ib);
-  hoff[0] = 0;
-  for (int64_t b = 0; b < B32; ++b) hoff[b + 1] = hoff[b] + c->tc5_cap[b];
-  c->tc5_items.ensure(ib);
-  c->tc5_coff.ensure(ob);
-  c->tc5_cand.ensure((size_t)std::max<int64_t>(hoff[B32], 1) * sizeof(uint32_t));
+  c->tc5_exact = false;
+  c->tc5_n = n;
+  c->tc5_rbmax = RBmax;
+  c->tc5_items.ensure((size_t)slots * (RBmax + 1) * sizeof(int32_t));
+  c->tc5_cand.ensure((size_t)std::max<int64_t>(total, 1) * sizeof(uint32_t));
   c->tc5_cnt.ensure((size_t)B32 * sizeof(int32_t));
   c->tc5_u16p.ensure((size_t)n * 128);
   c->tc5_flags.ensure(2 * sizeof(int));
-  cudaStream_t s = c->stream;
-  CK(cudaMemcpyAsync(c->tc5_items.p, hi0, ib, cudaMemcpyHostToDevice, s));
-  CK(cudaMemcpyAsync(c->tc5_coff.p, hoff, ob, cudaMemcpyHostToDevice, s));
-  CK(cudaMemsetAsync(c->tc5_cnt.p, 0, (size_t)B32 * sizeof(int32_t), s));
   CK(cudaMemsetAsync(c->tc5_flags.p, 0, 2 * sizeof(int), s));
+  launch_pad_unit16(g, c->tc5_u16p.as<uint16_t>(), s);
+  c->launches += 2;
+}
+
+// The pass over the pairs i < j with j in [cb, ce) (item table in `slot`).
+void sym_tc5_pass(rbg_ctx *c, const GraphArgs &g, const SymOut &o, int64_t cb, int64_t ce,
+                  int slot) {
+  int RB = 0, NT = 0;
+  const int items = sym_tc5_items(cb, ce, &RB, &NT);
+  if (items == 0) return;
+  const int64_t blocks = (ce + 31) / 32;
+  int32_t *di0 = c->tc5_items.as<int32_t>() + (size_t)slot * (c->tc5_rbmax + 1);
+  cudaStream_t s = c->stream;
+  launch_tc5_items(cb, ce, di0, s);
+  CK(cudaMemsetAsync(c->tc5_cnt.p, 0, (size_t)blocks * sizeof(int32_t), s));
   int dev = 0, sms = 148;
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const char *why = "";
   const int rc = launch_sym_prefilter(
-      g, c->tc5_u16p.as<uint16_t>(), prefilter_lo16(g.S, g.prefilter_eps),
-      c->tc5_items.as<int32_t>(), RB, NT, items, c->tc5_cand.as<uint32_t>(),
-      c->tc5_coff.as<int64_t>(), c->tc5_cnt.as<int32_t>(), c->tc5_flags.as<int>(),
-      c->tc5_flags.as<int>() + 1, sms, s, &why);
+      g, c->tc5_u16p.as<uint16_t>(), prefilter_lo16(g.S, g.prefilter_eps), cb, ce, di0, RB, NT,
+      items, c->tc5_cand.as<uint32_t>(), c->tc5_coff.as<int64_t>(), c->tc5_cnt.as<int32_t>(),
+      c->tc5_flags.as<int>(), c->tc5_flags.as<int>() + 1, sms, s, &why);
   if (rc != RBG_OK) throw Error(rc, std::string("tensor-core prefilter: ") + why);
   launch_sym_check(g, o, c->tc5_cand.as<uint32_t>(), c->tc5_coff.as<int64_t>(),
-                   c->tc5_cnt.as<int32_t>(), s);
+                   c->tc5_cnt.as<int32_t>(), blocks, s);
   c->launches += 3;
 }
 
@@ -661,16 +687,18 @@ bool sym_tc5_settle(rbg_ctx *c, int64_t n) {
     const double pairs = 32.0 * (double)std::max<int64_t>(n - 32 * b, 0);
     if (pairs > 0) frac = std::max(frac, cnt[b] / pairs);
   }
-  if (fl[0] != 0) {
-    for (int64_t b = 0; b < B32; ++b)
-      c->tc5_cap[b] = std::max<int64_t>(c->tc5_cap[b], ((int64_t)cnt[b] + 256 + 31) & ~(int64_t)31);
+  if (fl[0] != 0) {                          // rerun with room for every block's count
+    c->tc5_cap.assign((size_t)B32, 0);
+    for (int64_t b = 0; b < B32; ++b) {
+      const double pairs = 32.0 * (double)std::max<int64_t>(n - 32 * b, 0);
+      const int64_t fc = ((int64_t)(pairs * c->tc5_frac) + 256 + 31) & ~(int64_t)31;
+      c->tc5_cap[b] = std::max<int64_t>(fc, ((int64_t)cnt[b] + 256 + 31) & ~(int64_t)31);
+    }
+    c->tc5_exact = true;
     c->tc5_frac = std::max(c->tc5_frac, frac * 1.25);
     return false;
   }
-  if (frac * 1.25 > c->tc5_frac) {           // the next assemblies get room to spare
-    c->tc5_frac = frac * 1.25;
-    c->tc5_n = -1;
-  }
+  if (frac * 1.25 > c->tc5_frac) c->tc5_frac = frac * 1.25;   // room to spare next time
   return true;
 }
 
@@ -857,13 +885,15 @@ void run_graph(rbg_ctx *c, const rbg_params *p, const ShardCtx *sc = nullptr) {
     bool streamed = streamed_in;
     for (;;) {
       SymOut o = sym_buffers(c, n1);
-      const bool tc5 = !streamed && sym_tc5_on() && g.Kp <= 64 && n < ((int64_t)1 << 27);
+      const bool tc5 = !streamed && sym_tc5_fits(g);
       if (streamed) {
         o.defer = 1;
+        if (c->streamed_tc5) sym_tc5_readback(c, n);
       } else {
         sym_clear(c, n1);
         if (tc5) {
-          sym_tc5_launch(c, g, o);
+          sym_tc5_setup(c, g, 1);
+          sym_tc5_pass(c, g, o, 0, n, 0);
           sym_tc5_readback(c, n);
         } else {
           launch_allpairs_sym(g, o, c->stream);
@@ -885,6 +915,18 @@ void run_graph(rbg_ctx *c, const rbg_params *p, const ShardCtx *sc = nullptr) {
       CK(cudaGetLastError());
       c->launches += 3;
       CK(cudaEventSynchronize(c->ev[10]));
+      if (streamed && c->streamed_tc5) {
+        const int *fl = c->tc5_host.as<int>();
+        if (fl[1] != 0)
+          throw Error(RBG_ERR_TIMEOUT, "tensor-core prefilter: a bounded device wait gave up "
+                                       "(stage " + std::to_string(fl[1]) + ")");
+        if (fl[0] != 0) {                            // a window's list overflowed: rescore
+          CK(cudaStreamSynchronize(c->stream));
+          c->tc5_frac *= 2.0;
+          streamed = false;
+          continue;
+        }
+      }
       if (tc5 && !sym_tc5_settle(c, n)) {           // a candidate list overflowed: rerun
         CK(cudaStreamSynchronize(c->stream));
         continue;
@@ -1390,7 +1432,7 @@ int rbg_destroy(rbg_ctx *c) {
                   &c->shard_send, &c->shard_recv, &c->oh_pres, &c->oh_map, &c->oh_koff,
                   &c->oh_X, &c->oh_cand, &c->oh_cnt, &c->oh_tab, &c->oh_err, &c->kept, &c->b0dev,
                   &c->count_work, &c->tc5_u16p, &c->tc5_cand, &c->tc5_cnt, &c->tc5_items,
-                  &c->tc5_coff, &c->tc5_flags,
+                  &c->tc5_coff, &c->tc5_caps, &c->tc5_flags,
                   &c->qa, &c->qb, &c->qo, &c->qt, &c->ix_keys, &c->ix_sorted,
                   &c->ix_contig, &c->ix_post, &c->ix_ukeys, &c->ix_count, &c->ix_off,
                   &c->ix_nk, &c->ix_scratch};

@@ -128,6 +128,18 @@ std::unique_ptr<Tables> make_tables(const rbg_params *p, cudaStream_t s);
 // caller's next synchronisation of c->stream.
 void dense_allpairs_onehot(rbg_ctx *c, const GraphArgs &g);
 void check_onehot_status(rbg_ctx *c);
+
+// Symmetric pass on the tcgen05 prefilter (engine.cpp): whether it takes the
+// assembly; per-assembly setup (list capacities, padded FP16 rows, cleared
+// flags; `slots` item tables for passes in flight); one pass over the pairs
+// i < j with j in [cb, ce); the flags and block counts read back on the stream;
+// after the sync, false when a list overflowed (the caller reruns).
+bool sym_tc5_fits(const GraphArgs &g);
+void sym_tc5_setup(rbg_ctx *c, const GraphArgs &g, int slots);
+void sym_tc5_pass(rbg_ctx *c, const GraphArgs &g, const SymOut &o, int64_t cb, int64_t ce,
+                  int slot);
+void sym_tc5_readback(rbg_ctx *c, int64_t n);
+bool sym_tc5_settle(rbg_ctx *c, int64_t n);
 // The dense regime runs on the one-hot tensor-core kernel unless RBG_DENSE_ALU
 // is set (then the integer-ALU register compare, kept for the measured
 // comparison).
@@ -299,11 +311,14 @@ struct rbg_ctx {
   rbg::DBuf count_work;                 // contig counter of the k-mer count kernel
   // symmetric pass on the tensor-core prefilter: candidate lists per 32-row
   // block (capacities tc5_cap, sized from the kept fraction tc5_frac)
-  rbg::DBuf tc5_u16p, tc5_cand, tc5_cnt, tc5_items, tc5_coff, tc5_flags;
+  rbg::DBuf tc5_u16p, tc5_cand, tc5_cnt, tc5_items, tc5_coff, tc5_caps, tc5_flags;
   rbg::HBuf tc5_pin, tc5_host;
   std::vector<int64_t> tc5_cap;
   int64_t tc5_n = -1;
   double tc5_frac = 0.03;
+  bool tc5_exact = false;               // tc5_cap holds exact capacities for the next setup
+  int64_t tc5_rbmax = 0;                // item-table slot length - 1
+  bool streamed_tc5 = false;            // the pairs behind the copy went through that pass
   rbg::HBuf oh_errpin;
   bool oh_pending = false;
   // ProbMinHash4 queries: operand blocks, output block, metric table

@@ -699,7 +699,8 @@ k_allpairs_tc_win(GraphArgs g, int P, float lo, float hi, float lo16, SymOut o, 
 }
 
 // Symmetric pass, part 2 (after k_sym_prefilter, kernels_sym_tc5.cu): a CTA
-// takes 32-row block x and block B-1-x (as k_allpairs_tc_sym pairs them), with
+// takes 32-row block x and block B-1-x of the B blocks in play (as
+// k_allpairs_tc_sym pairs them; gridDim.y CTAs share a pair's lists), with
 // the block's register codes and unit rows in shared memory, and its warps work
 // through the block's candidate list 32 entries at a time: the exact prune
 // decision (check_batch), then the survivors' register compares and pair
@@ -742,7 +743,9 @@ __device__ __forceinline__ void sym_check_block(const GraphArgs &g, const SymOut
   const int64_t off = coff[bx];
   const int cnt = (int)min((int64_t)ccnt[bx], coff[bx + 1] - off);
   const int *list = (const int *)(cand + off);
-  for (int i0 = warp * 32; i0 < cnt; i0 += kWarps * 32)
+  // the gridDim.y CTAs of a block pair share its list
+  for (int i0 = ((int)blockIdx.y * kWarps + warp) * 32; i0 < cnt;
+       i0 += (int)gridDim.y * kWarps * 32)
     check_batch<SMAX, true, false>(g, w, o, 0, list, (unsigned)i0, min(32, cnt - i0), row0, q,
                                    qn, lo, hi, n_cmp, sU, SuP, sA);
   if (qn > 0) {
@@ -761,9 +764,8 @@ __device__ __forceinline__ void sym_check_block(const GraphArgs &g, const SymOut
 template <int SMAX>
 __global__ void __launch_bounds__(kWarps * 32, SMAX == 32 ? 6 : 1)
 k_sym_check(GraphArgs g, float lo, float hi, SymOut o, const uint32_t *cand,
-            const int64_t *coff, const int32_t *ccnt) {
+            const int64_t *coff, const int32_t *ccnt, int64_t B) {
   extern __shared__ __align__(16) unsigned char smem[];
-  const int64_t B = (g.n + 31) / 32;
   const int64_t b1 = blockIdx.x, b2 = B - 1 - b1;
   sym_check_block<SMAX>(g, o, lo, hi, cand, coff, ccnt, b1, smem);
   if (b2 > b1) {
@@ -1092,19 +1094,22 @@ void launch_merge_topk(const GraphArgs &g, const uint64_t *gbuf, const int32_t *
 }
 
 void launch_sym_check(const GraphArgs &g, const SymOut &o, const uint32_t *cand,
-                      const int64_t *coff, const int32_t *ccnt, cudaStream_t s) {
-  if (g.n == 0) return;
-  const int64_t B = (g.n + 31) / 32;
+                      const int64_t *coff, const int32_t *ccnt, int64_t B, cudaStream_t s) {
+  if (g.n == 0 || B <= 0) return;
   float lo, hi, lo16;
   prefilter_bands(g.S, g.prefilter_eps, &lo, &hi, &lo16);
   const int v = allpairs_variant(g);
   const size_t smem = (size_t)kWarps * kTcWs + (size_t)32 * g.mpad +
                       (size_t)32 * su_stride(g.Su) * 4;
-  const unsigned grid = (unsigned)((B + 1) / 2);
+  // enough CTAs for six per SM: a block pair's list is split over gridDim.y CTAs
+  const int64_t pairs = (B + 1) / 2;
+  const unsigned gy =
+      (unsigned)std::min<int64_t>(4, std::max<int64_t>(1, (6 * 148 + pairs - 1) / pairs));
+  const dim3 grid((unsigned)pairs, gy);
 #define RBG_SC(SM)                                                                        \
   do {                                                                                    \
     smem_cap_max((const void *)k_sym_check<SM>);                                          \
-    k_sym_check<SM><<<grid, kWarps * 32, smem, s>>>(g, lo, hi, o, cand, coff, ccnt);      \
+    k_sym_check<SM><<<grid, kWarps * 32, smem, s>>>(g, lo, hi, o, cand, coff, ccnt, B);   \
   } while (0)
   if (v == 1) RBG_SC(16);
   else if (v == 2) RBG_SC(32);

@@ -10,15 +10,17 @@
 // prefilter_bands) is a candidate, and only candidates reach the exact check
 // and the register compare of part 2 (k_sym_check, kernels_allpairs.cu).
 //
-// Work: items (128-row block rb, 256-column tile ct) of the upper triangle
-// (ct from the tile holding the block's first row on), each CTA (one per SM)
-// a contiguous range of them in row-block order.  Warp 0 issues the TMA loads
+// Work: items (128-row block rb, 256-column tile ct) of the pairs i < j with j
+// in a column window [jlo, jhi) (the whole upper triangle, or the columns of
+// one input chunk while later chunks are still being copied in; ct from the
+// tile holding the block's first row, or the window's first tile, on), each
+// CTA (one per SM) a contiguous range of them in row-block order.  Warp 0 issues the TMA loads
 // (the row block's 128 rows once per block into a 2-deep ring, each column
 // tile's 256 rows into a 4-deep ring), warp 1 allocates TMEM (two 256-column
 // accumulators, so an item's MMAs run while the epilogue reads the previous
 // item) and issues 4 MMAs of K = 16 per item, warps 2-17 are the epilogue: a
 // thread takes one row and 64 of the tile's columns, keeps the pairs j > i
-// with j < n, either contig carrying abundance (anynz) and a product of at
+// with j in the window, either contig carrying abundance (anynz) and a product of at
 // least lo16, and appends them to its 32-row block's candidate list (entry
 // r << 27 | j, r the row within the block) with one atomic per warp and item.
 // The abundance flags of an item's columns are loaded before its wait.
@@ -60,15 +62,16 @@ constexpr uint32_t kIdescF16 =
 
 struct PfArgs {
   const uint8_t *anynz;   // [n]
-  int n;
+  int jlo, jhi;           // pairs i < j with j in [jlo, jhi) (rows [0, jhi))
+  int ct_lo;              // first column tile: jlo / 256
   float lo16;             // candidate from lo16 on
   const int32_t *item0;   // [RB + 1] first item of each 128-row block
-  int RB, NT, items;
+  int RB, NT, items;      // row blocks below jhi, column tiles below jhi, items
   uint32_t *cand;         // block b's entries at cand + coff[b], coff[b + 1] - coff[b] of them
   const int64_t *coff;    // [B32 + 1]
   int32_t *ccnt;          // [B32] entries found (counted on past the capacity)
   int *overflow;          // set when a block's entries outgrow its capacity
-  unsigned long long *stats;   // [0] += pairs evaluated (i < j < n)
+  unsigned long long *stats;   // [0] += pairs evaluated
   int *err;               // set when a bounded wait runs out
 };
 
@@ -104,12 +107,12 @@ struct ItemWalk {
       if (A.item0[mid] <= it) lo = mid; else hi = mid - 1;
     }
     rb = lo;
-    ct = (kPM * rb) / kPN + (it - A.item0[rb]);
+    ct = max((kPM * rb) / kPN, A.ct_lo) + (it - A.item0[rb]);
   }
   __device__ void next(const PfArgs &A) {
     if (++ct == A.NT) {
       ++rb;
-      ct = (kPM * rb) / kPN;
+      ct = max((kPM * rb) / kPN, A.ct_lo);
     }
   }
 };
@@ -254,7 +257,7 @@ k_sym_prefilter(const __grid_constant__ CUtensorMap tmap, const PfArgs A) {
     const int e = warp - 2;                             // 0..15
     const int q = warp & 3;                             // TMEM lane quarter of this warp
     const int p = e >> 2;                               // columns [64 p, 64 p + 64)
-    const int n = A.n;
+    const int jlo = A.jlo, jhi = A.jhi;
     const float lo16 = A.lo16;
     ItemWalk w;
     w.start(A, it0);
@@ -269,7 +272,7 @@ k_sym_prefilter(const __grid_constant__ CUtensorMap tmap, const PfArgs A) {
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int j = kPN * w.ct + 64 * p + 32 * h + lane;
-        nzw[h] = __ballot_sync(FULL, j < n && A.anynz[j]);
+        nzw[h] = __ballot_sync(FULL, j < jhi && A.anynz[j]);
       }
       uint32_t bad = mbar_wait(tfull(tb), (uint32_t)(k >> 1) & 1u, A.err, 19) ? 0u : 1u;
       if (*(volatile int *)abort_flag) bad = 1u;
@@ -288,7 +291,7 @@ k_sym_prefilter(const __grid_constant__ CUtensorMap tmap, const PfArgs A) {
       const int row0w = kPM * w.rb + 32 * q;            // the warp's 32 rows
       const int row = row0w + lane;
       if (w.rb != nzrb) {
-        nz_row = row < n ? A.anynz[row] : 0u;
+        nz_row = row < jhi ? A.anynz[row] : 0u;
         nzrb = w.rb;
       }
       uint32_t cm[2];
@@ -297,16 +300,16 @@ k_sym_prefilter(const __grid_constant__ CUtensorMap tmap, const PfArgs A) {
       for (int h = 0; h < 2; ++h) {
         const uint32_t(&v)[32] = h ? v1 : v0;
         const int j0 = kPN * w.ct + 64 * p + 32 * h;
-        // valid columns: i < j < n (the warp-uniform interior case first)
+        // valid columns: i < j, jlo <= j < jhi (the warp-uniform interior case first)
         uint32_t valid;
-        if (j0 > row0w + 31 && j0 + 32 <= n && row0w + 31 < n) {
+        if (j0 > row0w + 31 && j0 >= jlo && j0 + 32 <= jhi && row0w + 31 < jhi) {
           valid = ~0u;
         } else {
-          const int dl = row - j0;                        // j > row: t > dl
-          const int dh = n - j0;                          // j < n:   t < dh
-          valid = dl < 0 ? ~0u : (dl >= 31 ? 0u : (~0u << (dl + 1)));
+          const int tl = max(row - j0 + 1, jlo - j0);     // first valid t
+          const int dh = jhi - j0;                        // t < dh
+          valid = tl <= 0 ? ~0u : (tl >= 32 ? 0u : (~0u << tl));
           valid &= dh >= 32 ? ~0u : (dh <= 0 ? 0u : ((1u << dh) - 1u));
-          if (row >= n) valid = 0u;
+          if (row >= jhi) valid = 0u;
         }
         uint32_t mk = 0;
 #pragma unroll
@@ -369,35 +372,104 @@ __global__ void k_pad_unit16(const uint16_t *__restrict__ u, int Kp, int64_t n,
   out[i] = k < Kp ? u[r * Kp + k] : (uint16_t)0;
 }
 
-}  // namespace
-
-// Items (128-row block, 256-column tile) of the upper triangle of n contigs:
-// item0[rb] = the first item of row block rb, item0[RB] = the total.
-int sym_tc5_items(int64_t n, std::vector<int32_t> &item0, int *RB, int *NT) {
-  *RB = (int)((n + kPM - 1) / kPM);
-  *NT = (int)((n + kPN - 1) / kPN);
-  item0.assign((size_t)*RB + 1, 0);
-  for (int rb = 0; rb < *RB; ++rb)
-    item0[rb + 1] = item0[rb] + std::max(0, *NT - (kPM * rb) / kPN);
-  return item0[*RB];
+// Exclusive prefix sums of one CTA (1024 threads) over v(0 .. count-1) into
+// out[0 .. count]; v(k) a value the caller's functor gives.
+template <class F, class T>
+__device__ void block_scan_into(int64_t count, F v, T *out) {
+  __shared__ int64_t part[1024];
+  const int t = threadIdx.x;
+  const int64_t per = (count + 1023) / 1024;
+  const int64_t a = min(count, t * per), b = min(count, a + per);
+  int64_t sum = 0;
+  for (int64_t k = a; k < b; ++k) sum += v(k);
+  part[t] = sum;
+  __syncthreads();
+  for (int d = 1; d < 1024; d <<= 1) {
+    const int64_t add = t >= d ? part[t - d] : 0;
+    __syncthreads();
+    part[t] += add;
+    __syncthreads();
+  }
+  int64_t run = t ? part[t - 1] : 0;
+  for (int64_t k = a; k < b; ++k) {
+    out[k] = (T)run;
+    run += v(k);
+  }
+  if (t == 1023) out[count] = (T)part[1023];
 }
 
-int launch_sym_prefilter(const GraphArgs &g, uint16_t *u16p, float lo16, const int32_t *item0,
-                         int RB, int NT, int items, uint32_t *cand, const int64_t *coff,
-                         int32_t *ccnt, int *overflow, int *err, int sms, cudaStream_t s,
-                         const char **why) {
+// List offsets of the 32-row blocks: capacities from the kept fraction
+// (32 (n - 32 b) pairs x frac + 256, rounded up to 32) or given ones.
+__global__ void k_tc5_coff(int64_t n, double frac, const int64_t *caps, int64_t *coff) {
+  const int64_t B32 = (n + 31) / 32;
+  block_scan_into(B32, [&](int64_t b) -> int64_t {
+    if (caps) return caps[b];
+    const double pairs = 32.0 * (double)max((int64_t)0, n - 32 * b);
+    return (((int64_t)(pairs * frac) + 256 + 31) & ~(int64_t)31);
+  }, coff);
+}
+
+// Item table of a pass (see sym_tc5_items).
+__global__ void k_tc5_items(int RB, int NT, int ct_lo, int32_t *item0) {
+  block_scan_into((int64_t)RB, [&](int64_t rb) -> int64_t {
+    return (int64_t)max(0, NT - max((kPM * (int)rb) / kPN, ct_lo));
+  }, item0);
+}
+
+}  // namespace
+
+// Items (128-row block, 256-column tile) of the pairs i < j with j in
+// [cb, ce): row blocks below ce, column tiles from cb / 256 (and from the
+// tile of the block's first row) below ce; item0[rb] = the first item of row
+// block rb, item0[RB] = the total.
+int sym_tc5_items(int64_t cb, int64_t ce, int *RB, int *NT) {
+  *RB = (int)((ce + kPM - 1) / kPM);
+  *NT = (int)((ce + kPN - 1) / kPN);
+  const int ct_lo = (int)(cb / kPN);
+  int tot = 0;
+  for (int rb = 0; rb < *RB; ++rb) tot += std::max(0, *NT - std::max((kPM * rb) / kPN, ct_lo));
+  return tot;
+}
+
+// Total list capacity of the frac-based capacities (the arithmetic of k_tc5_coff).
+int64_t tc5_capacity(int64_t n, double frac) {
+  int64_t tot = 0;
+  for (int64_t b = 0; b < (n + 31) / 32; ++b) {
+    const double pairs = 32.0 * (double)std::max<int64_t>(0, n - 32 * b);
+    tot += ((int64_t)(pairs * frac) + 256 + 31) & ~(int64_t)31;
+  }
+  return tot;
+}
+
+void launch_tc5_coff(int64_t n, double frac, const int64_t *caps, int64_t *coff, cudaStream_t s) {
+  k_tc5_coff<<<1, 1024, 0, s>>>(n, frac, caps, coff);
+}
+
+void launch_tc5_items(int64_t cb, int64_t ce, int32_t *item0, cudaStream_t s) {
+  const int RB = (int)((ce + kPM - 1) / kPM), NT = (int)((ce + kPN - 1) / kPN);
+  k_tc5_items<<<1, 1024, 0, s>>>(RB, NT, (int)(cb / kPN), item0);
+}
+
+void launch_pad_unit16(const GraphArgs &g, uint16_t *u16p, cudaStream_t s) {
+  const int64_t nh = g.n * kPK;
+  if (nh > 0) k_pad_unit16<<<(unsigned)((nh + 255) / 256), 256, 0, s>>>(g.unit16, g.Kp, g.n, u16p);
+}
+
+int launch_sym_prefilter(const GraphArgs &g, const uint16_t *u16p, float lo16, int64_t cb,
+                         int64_t ce, const int32_t *item0, int RB, int NT, int items,
+                         uint32_t *cand, const int64_t *coff, int32_t *ccnt, int *overflow,
+                         int *err, int sms, cudaStream_t s, const char **why) {
   if (g.n == 0 || items == 0) return RBG_OK;
   auto enc = encode_fn();
   if (!enc) {
     *why = "cuTensorMapEncodeTiled is not available";
     return RBG_ERR_CUDA;
   }
-  if (g.Kp > kPK || g.n >= ((int64_t)1 << 27) || ((uintptr_t)u16p & 15u) != 0) {
+  if (g.Kp > kPK || g.n >= ((int64_t)1 << 27) || ((uintptr_t)u16p & 15u) != 0 || cb < 0 ||
+      ce > g.n || cb >= ce) {
     *why = "prefilter operand layout";
     return RBG_ERR_ARG;
   }
-  const int64_t nh = g.n * kPK;
-  k_pad_unit16<<<(unsigned)((nh + 255) / 256), 256, 0, s>>>(g.unit16, g.Kp, g.n, u16p);
   CUtensorMap map;
   std::memset(&map, 0, sizeof(map));
   const cuuint64_t dims[2] = {(cuuint64_t)kPK, (cuuint64_t)g.n};
@@ -413,7 +485,9 @@ int launch_sym_prefilter(const GraphArgs &g, uint16_t *u16p, float lo16, const i
   }
   PfArgs A;
   A.anynz = g.anynz;
-  A.n = (int)g.n;
+  A.jlo = (int)cb;
+  A.jhi = (int)ce;
+  A.ct_lo = (int)(cb / kPN);
   A.lo16 = lo16;
   A.item0 = item0;
   A.RB = RB;

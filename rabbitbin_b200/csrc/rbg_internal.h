@@ -229,20 +229,28 @@ struct SymOut {
 void launch_allpairs_sym(const GraphArgs &g, const SymOut &o, cudaStream_t s, int x0 = 0,
                          int xs = 1);
 
-// Symmetric pass in two kernels (kernels_sym_tc5.cu, kernels_allpairs.cu): the
-// tcgen05 abundance prefilter writes each 32-row block's candidates (entries
-// r << 27 | j at cand + coff[b], capacity coff[b + 1] - coff[b], the count in
-// ccnt[b] even past it; *overflow set then), k_sym_check decides and counts
-// them into o.  item0 [RB + 1] from sym_tc5_items; u16p: n x 128 bytes of
-// scratch (16-byte aligned).  Needs g.Kp <= 64 and n < 2^27.
-int sym_tc5_items(int64_t n, std::vector<int32_t> &item0, int *RB, int *NT);
-int launch_sym_prefilter(const GraphArgs &g, uint16_t *u16p, float lo16, const int32_t *item0,
-                         int RB, int NT, int items, uint32_t *cand, const int64_t *coff,
-                         int32_t *ccnt, int *overflow, int *err, int sms, cudaStream_t s,
-                         const char **why);
+// Symmetric pass in two kernels (kernels_sym_tc5.cu, kernels_allpairs.cu) over
+// the pairs i < j with j in [cb, ce): the tcgen05 abundance prefilter writes
+// each 32-row block's candidates (entries r << 27 | j at cand + coff[b],
+// capacity coff[b + 1] - coff[b], the count in ccnt[b] even past it; *overflow
+// set then), k_sym_check decides and counts them into o (blocks below
+// ceil(ce / 32)).  The item table [RB + 1] comes from launch_tc5_items (its
+// total from sym_tc5_items); u16p: the unit16 rows padded to 64 halves by
+// launch_pad_unit16 (n x 128 bytes, 16-byte aligned).  Needs g.Kp <= 64 and
+// n < 2^27.  The offsets and item tables are made on the device, so nothing
+// crosses PCIe while input chunks stream in; tc5_capacity is the total of the
+// frac-based capacities of launch_tc5_coff (caps null).
+int sym_tc5_items(int64_t cb, int64_t ce, int *RB, int *NT);
+int64_t tc5_capacity(int64_t n, double frac);
+void launch_tc5_coff(int64_t n, double frac, const int64_t *caps, int64_t *coff, cudaStream_t s);
+void launch_tc5_items(int64_t cb, int64_t ce, int32_t *item0, cudaStream_t s);
+void launch_pad_unit16(const GraphArgs &g, uint16_t *u16p, cudaStream_t s);
+int launch_sym_prefilter(const GraphArgs &g, const uint16_t *u16p, float lo16, int64_t cb,
+                         int64_t ce, const int32_t *item0, int RB, int NT, int items,
+                         uint32_t *cand, const int64_t *coff, int32_t *ccnt, int *overflow,
+                         int *err, int sms, cudaStream_t s, const char **why);
 void launch_sym_check(const GraphArgs &g, const SymOut &o, const uint32_t *cand,
-                      const int64_t *coff, const int32_t *ccnt, cudaStream_t s);
-// The prefilter's FP16 threshold: a candidate from lo16 on.
+                      const int64_t *coff, const int32_t *ccnt, int64_t blocks, cudaStream_t s);
 float prefilter_lo16(int S, float eps);
 
 // A pair list gathered from several ranks: its per-row key counts (rowcnt
