@@ -57,8 +57,8 @@ INT32_LANES_PER_SM = 128
 # ALU 50.7%; the ALU share below is their time-weighted mean).  Reported only
 # when the timed workload is that one.
 ALLPAIRS_NCU = {"contigs": 50000, "samples": 20,
-                "dram_bytes": 6504192 + 4735488 + 132049664 + 155734272,
-                "alu_pipe_frac": (0.627456 * 0.5376 + 1.051328 * 0.5072) / (0.627456 + 1.051328)}
+                "dram_bytes": 12854016 + 4613632 + 131647232 + 155896576,
+                "alu_pipe_frac": (0.460032 * 0.4908 + 1.020576 * 0.5053) / (0.460032 + 1.020576)}
 
 
 class ClockSampler:

@@ -609,7 +609,8 @@ void dense_allpairs_onehot(rbg_ctx *c, const GraphArgs &g) {
 bool sym_tc5_on() { return getenv("RBG_SYM_SINGLE") == nullptr; }
 
 bool sym_tc5_fits(const GraphArgs &g) {
-  return sym_tc5_on() && g.Kp <= 64 && g.n > 0 && g.n < ((int64_t)1 << 27);
+  // S < 64 leaves the last of the 64 padded halves for the threshold column
+  return sym_tc5_on() && g.S < 64 && g.Kp <= 64 && g.n > 0 && g.n < ((int64_t)1 << 27);
 }
 
 // Buffers, list capacities (for the whole assembly), the padded FP16 rows and
@@ -641,10 +642,10 @@ void sym_tc5_setup(rbg_ctx *c, const GraphArgs &g, int slots) {
   c->tc5_items.ensure((size_t)slots * (RBmax + 1) * sizeof(int32_t));
   c->tc5_cand.ensure((size_t)std::max<int64_t>(total, 1) * sizeof(uint32_t));
   c->tc5_cnt.ensure((size_t)B32 * sizeof(int32_t));
-  c->tc5_u16p.ensure((size_t)n * 128);
+  c->tc5_u16p.ensure((size_t)n * 256);         // row and column copies
   c->tc5_flags.ensure(2 * sizeof(int));
   CK(cudaMemsetAsync(c->tc5_flags.p, 0, 2 * sizeof(int), s));
-  launch_pad_unit16(g, c->tc5_u16p.as<uint16_t>(), s);
+  launch_pad_unit16(g, prefilter_lo16(g.S, g.prefilter_eps), c->tc5_u16p.as<uint16_t>(), s);
   c->launches += 2;
 }
 
@@ -664,8 +665,7 @@ void sym_tc5_pass(rbg_ctx *c, const GraphArgs &g, const SymOut &o, int64_t cb, i
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const char *why = "";
   const int rc = launch_sym_prefilter(
-      g, c->tc5_u16p.as<uint16_t>(), prefilter_lo16(g.S, g.prefilter_eps), cb, ce, di0, RB, NT,
-      items, c->tc5_cand.as<uint32_t>(), c->tc5_coff.as<int64_t>(), c->tc5_cnt.as<int32_t>(),
+      g, c->tc5_u16p.as<uint16_t>(), cb, ce, di0, RB, NT, items, c->tc5_cand.as<uint32_t>(), c->tc5_coff.as<int64_t>(), c->tc5_cnt.as<int32_t>(),
       c->tc5_flags.as<int>(), c->tc5_flags.as<int>() + 1, sms, s, &why);
   if (rc != RBG_OK) throw Error(rc, std::string("tensor-core prefilter: ") + why);
   launch_sym_check(g, o, c->tc5_cand.as<uint32_t>(), c->tc5_coff.as<int64_t>(),

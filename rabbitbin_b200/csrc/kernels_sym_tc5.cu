@@ -7,8 +7,12 @@
 // to 64 halves (one 128-byte swizzle atom), are multiplied here with
 // tcgen05.mma kind::f16 (FP32 accumulation in TMEM); every pair whose product
 // reaches lo16 = eps - 2.5e-3 (the bound that makes the FP16 prune exact, see
-// prefilter_bands) is a candidate, and only candidates reach the exact check
-// and the register compare of part 2 (k_sym_check, kernels_allpairs.cu).
+// prefilter_bands; here lo16 rounded down to FP16) is a candidate, and only
+// candidates reach the exact check and the register compare of part 2
+// (k_sym_check, kernels_allpairs.cu).  The threshold rides in the MMA as a
+// bias column (row side 1.0, column side -lo16 in the last half, free for
+// S < 64), so a candidate is a product whose sign bit is clear; byte permutes
+// gather the sign bits of 32 products into one mask.
 //
 // Work: items (128-row block rb, 256-column tile ct) of the pairs i < j with j
 // in a column window [jlo, jhi) (the whole upper triangle, or the columns of
@@ -20,10 +24,10 @@
 // accumulators, so an item's MMAs run while the epilogue reads the previous
 // item) and issues 4 MMAs of K = 16 per item, warps 2-17 are the epilogue: a
 // thread takes one row and 64 of the tile's columns, keeps the pairs j > i
-// with j in the window, either contig carrying abundance (anynz) and a product of at
-// least lo16, and appends them to its 32-row block's candidate list (entry
+// with j in the window and a product of at least lo16 (a contig without
+// abundance has a zero unit row, so it never gets there; part 2 checks the
+// flags), and appends them to its 32-row block's candidate list (entry
 // r << 27 | j, r the row within the block) with one atomic per warp and item.
-// The abundance flags of an item's columns are loaded before its wait.
 // A block's list has the capacity the host gave it; the count goes on past it,
 // so a pass that overflows is rerun with exact capacities.
 //
@@ -61,10 +65,8 @@ constexpr uint32_t kIdescF16 =
     (1u << 4) | ((uint32_t)(kPN >> 3) << 17) | ((uint32_t)(kPM >> 4) << 24);
 
 struct PfArgs {
-  const uint8_t *anynz;   // [n]
   int jlo, jhi;           // pairs i < j with j in [jlo, jhi) (rows [0, jhi))
   int ct_lo;              // first column tile: jlo / 256
-  float lo16;             // candidate from lo16 on
   const int32_t *item0;   // [RB + 1] first item of each 128-row block
   int RB, NT, items;      // row blocks below jhi, column tiles below jhi, items
   uint32_t *cand;         // block b's entries at cand + coff[b], coff[b + 1] - coff[b] of them
@@ -118,7 +120,8 @@ struct ItemWalk {
 };
 
 __global__ void __launch_bounds__(kPThreads, 1)
-k_sym_prefilter(const __grid_constant__ CUtensorMap tmap, const PfArgs A) {
+k_sym_prefilter(const __grid_constant__ CUtensorMap tmapA, const __grid_constant__ CUtensorMap tmapB,
+                const PfArgs A) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t *base = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t *sa = base;                                  // [2][kABytes]
@@ -184,7 +187,7 @@ k_sym_prefilter(const __grid_constant__ CUtensorMap tmap, const PfArgs A) {
             break;
           }
           mbar_expect_tx(fullA(ai), kABytes);
-          tma_load(smem_u32(sa + ai * kABytes), &tmap, 0, kPM * w.rb, fullA(ai));
+          tma_load(smem_u32(sa + ai * kABytes), &tmapA, 0, kPM * w.rb, fullA(ai));
           a_issued |= 1u << ai;
           a_last = (a_last & ~(1u << ai)) | (aph << ai);
           arb = w.rb;
@@ -196,8 +199,8 @@ k_sym_prefilter(const __grid_constant__ CUtensorMap tmap, const PfArgs A) {
         }
         const uint32_t dst = smem_u32(sb + (size_t)s * kBBytes);
         mbar_expect_tx(full(s), kBBytes);
-        tma_load(dst, &tmap, 0, kPN * w.ct, full(s));
-        tma_load(dst + kBBytes / 2, &tmap, 0, kPN * w.ct + kPN / 2, full(s));
+        tma_load(dst, &tmapB, 0, kPN * w.ct, full(s));
+        tma_load(dst + kBBytes / 2, &tmapB, 0, kPN * w.ct + kPN / 2, full(s));
         issued |= 1u << s;
         last_ph = (last_ph & ~(1u << s)) | (ph << s);
         if (++s == kPStages) { s = 0; ph ^= 1u; }
@@ -258,22 +261,12 @@ k_sym_prefilter(const __grid_constant__ CUtensorMap tmap, const PfArgs A) {
     const int q = warp & 3;                             // TMEM lane quarter of this warp
     const int p = e >> 2;                               // columns [64 p, 64 p + 64)
     const int jlo = A.jlo, jhi = A.jhi;
-    const float lo16 = A.lo16;
     ItemWalk w;
     w.start(A, it0);
-    int nzrb = -1;
-    uint32_t nz_row = 0;
     unsigned long long npref = 0;
     int k = 0;
     for (int it = it0; it < it1; ++it, ++k, w.next(A)) {
       const int tb = k & 1;
-      // the abundance flags of the warp's 64 columns, loaded before the wait
-      uint32_t nzw[2];
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int j = kPN * w.ct + 64 * p + 32 * h + lane;
-        nzw[h] = __ballot_sync(FULL, j < jhi && A.anynz[j]);
-      }
       uint32_t bad = mbar_wait(tfull(tb), (uint32_t)(k >> 1) & 1u, A.err, 19) ? 0u : 1u;
       if (*(volatile int *)abort_flag) bad = 1u;
       if (pf_barrier_or(bad)) {                         // one decision for all epilogue threads
@@ -290,10 +283,8 @@ k_sym_prefilter(const __grid_constant__ CUtensorMap tmap, const PfArgs A) {
       mbar_arrive(tempty(tb));                          // the accumulator is free again
       const int row0w = kPM * w.rb + 32 * q;            // the warp's 32 rows
       const int row = row0w + lane;
-      if (w.rb != nzrb) {
-        nz_row = row < jhi ? A.anynz[row] : 0u;
-        nzrb = w.rb;
-      }
+      // Masks in "gather order": bit 8 q + k stands for column t = 4 k + q of
+      // the 32-column chunk (the order the byte permutes below produce).
       uint32_t cm[2];
       int cnt = 0;
 #pragma unroll
@@ -304,18 +295,30 @@ k_sym_prefilter(const __grid_constant__ CUtensorMap tmap, const PfArgs A) {
         uint32_t valid;
         if (j0 > row0w + 31 && j0 >= jlo && j0 + 32 <= jhi && row0w + 31 < jhi) {
           valid = ~0u;
+          npref += 32;
         } else {
           const int tl = max(row - j0 + 1, jlo - j0);     // first valid t
           const int dh = jhi - j0;                        // t < dh
-          valid = tl <= 0 ? ~0u : (tl >= 32 ? 0u : (~0u << tl));
-          valid &= dh >= 32 ? ~0u : (dh <= 0 ? 0u : ((1u << dh) - 1u));
-          if (row >= jhi) valid = 0u;
-        }
-        uint32_t mk = 0;
+          uint32_t vt = tl <= 0 ? ~0u : (tl >= 32 ? 0u : (~0u << tl));
+          vt &= dh >= 32 ? ~0u : (dh <= 0 ? 0u : ((1u << dh) - 1u));
+          if (row >= jhi) vt = 0u;
+          npref += (unsigned)__popc(vt);
+          valid = 0;
 #pragma unroll
-        for (int t = 0; t < 32; ++t) mk |= (__uint_as_float(v[t]) >= lo16 ? 1u : 0u) << t;
-        npref += (unsigned)__popc(valid);
-        cm[h] = mk & valid & (nz_row ? ~0u : nzw[h]);
+          for (int kk = 0; kk < 8; ++kk)                  // t = 4 kk + q -> bit 8 q + kk
+            valid |= ((((vt >> (4 * kk)) & 0xFu) * 0x00204081u) & 0x01010101u) << kk;
+        }
+        // The MMA carried the threshold as a bias column (product - lo16): a
+        // candidate's sign bit is clear.  Top bytes of four products per word.
+        uint32_t sg = 0;
+#pragma unroll
+        for (int kk = 0; kk < 8; ++kk) {
+          const uint32_t lo2 = __byte_perm(v[4 * kk], v[4 * kk + 1], 0x0073u);
+          const uint32_t hi2 = __byte_perm(v[4 * kk + 2], v[4 * kk + 3], 0x0073u);
+          const uint32_t g = __byte_perm(lo2, hi2, 0x5410u);
+          sg |= ((g >> 7) & 0x01010101u) << kk;
+        }
+        cm[h] = ~sg & valid;
         cnt += __popc(cm[h]);
       }
       // one slot range per warp and item in the 32-row block's list
@@ -339,8 +342,9 @@ k_sym_prefilter(const __grid_constant__ CUtensorMap tmap, const PfArgs A) {
           const uint32_t j0 = (uint32_t)(kPN * w.ct + 64 * p + 32 * h);
           uint32_t m = cm[h];
           while (m) {
-            const int t = __ffs(m) - 1;
+            const int bit = __ffs(m) - 1;
             m &= m - 1;
+            const int t = 4 * (bit & 7) + (bit >> 3);
             if (pos < cap) A.cand[off + pos] = ((uint32_t)lane << 27) | (j0 + (uint32_t)t);
             ++pos;
           }
@@ -362,14 +366,24 @@ size_t pf_smem() {
          16 + 16;
 }
 
-// unit16 rows (Kp halves) -> [n][64] halves, zero padded.
-__global__ void k_pad_unit16(const uint16_t *__restrict__ u, int Kp, int64_t n,
-                             uint16_t *__restrict__ out) {
+// unit16 rows (Kp halves) -> two [n][64] copies, zero padded, with the
+// threshold as a bias column in the last half (S < 64 leaves it free): the row
+// side (A) holds 1.0 there and the column side (B) -lo16', lo16' the largest
+// FP16 value not above lo16, so each product comes out of the MMA as
+// U_i . U_j - lo16'.
+__global__ void k_pad_unit16(const uint16_t *__restrict__ u, int Kp, int64_t n, float lo16,
+                             uint16_t *__restrict__ outA, uint16_t *__restrict__ outB) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;   // one half each
   if (i >= n * kPK) return;
   const int64_t r = i / kPK;
   const int k = (int)(i - r * kPK);
-  out[i] = k < Kp ? u[r * Kp + k] : (uint16_t)0;
+  uint16_t a = k < Kp ? u[r * Kp + k] : (uint16_t)0, b = a;
+  if (k == kPK - 1) {
+    a = __half_as_ushort(__float2half_rn(1.0f));
+    b = __half_as_ushort(__hneg(__float2half_rd(lo16)));
+  }
+  outA[i] = a;
+  outB[i] = b;
 }
 
 // Exclusive prefix sums of one CTA (1024 threads) over v(0 .. count-1) into
@@ -450,45 +464,48 @@ void launch_tc5_items(int64_t cb, int64_t ce, int32_t *item0, cudaStream_t s) {
   k_tc5_items<<<1, 1024, 0, s>>>(RB, NT, (int)(cb / kPN), item0);
 }
 
-void launch_pad_unit16(const GraphArgs &g, uint16_t *u16p, cudaStream_t s) {
+void launch_pad_unit16(const GraphArgs &g, float lo16, uint16_t *u16p, cudaStream_t s) {
   const int64_t nh = g.n * kPK;
-  if (nh > 0) k_pad_unit16<<<(unsigned)((nh + 255) / 256), 256, 0, s>>>(g.unit16, g.Kp, g.n, u16p);
+  if (nh > 0)
+    k_pad_unit16<<<(unsigned)((nh + 255) / 256), 256, 0, s>>>(g.unit16, g.Kp, g.n, lo16, u16p,
+                                                              u16p + nh);
 }
 
-int launch_sym_prefilter(const GraphArgs &g, const uint16_t *u16p, float lo16, int64_t cb,
-                         int64_t ce, const int32_t *item0, int RB, int NT, int items,
-                         uint32_t *cand, const int64_t *coff, int32_t *ccnt, int *overflow,
-                         int *err, int sms, cudaStream_t s, const char **why) {
+int launch_sym_prefilter(const GraphArgs &g, const uint16_t *u16p, int64_t cb, int64_t ce,
+                         const int32_t *item0, int RB, int NT, int items, uint32_t *cand,
+                         const int64_t *coff, int32_t *ccnt, int *overflow, int *err, int sms,
+                         cudaStream_t s, const char **why) {
   if (g.n == 0 || items == 0) return RBG_OK;
   auto enc = encode_fn();
   if (!enc) {
     *why = "cuTensorMapEncodeTiled is not available";
     return RBG_ERR_CUDA;
   }
-  if (g.Kp > kPK || g.n >= ((int64_t)1 << 27) || ((uintptr_t)u16p & 15u) != 0 || cb < 0 ||
-      ce > g.n || cb >= ce) {
+  if (g.Kp > kPK || g.S >= kPK || g.n >= ((int64_t)1 << 27) || ((uintptr_t)u16p & 15u) != 0 ||
+      cb < 0 || ce > g.n || cb >= ce) {
     *why = "prefilter operand layout";
     return RBG_ERR_ARG;
   }
-  CUtensorMap map;
-  std::memset(&map, 0, sizeof(map));
+  CUtensorMap map[2];
+  std::memset(map, 0, sizeof(map));
   const cuuint64_t dims[2] = {(cuuint64_t)kPK, (cuuint64_t)g.n};
   const cuuint64_t strides[1] = {(cuuint64_t)kPK * 2};
   const cuuint32_t box[2] = {(cuuint32_t)kPK, (cuuint32_t)kPM};
   const cuuint32_t estr[2] = {1, 1};
-  const CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, (void *)u16p, dims, strides, box,
-                         estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) {
-    *why = "cuTensorMapEncodeTiled failed";
-    return RBG_ERR_CUDA;
+  for (int side = 0; side < 2; ++side) {       // rows (A), then columns (B)
+    const CUresult r = enc(&map[side], CU_TENSOR_MAP_DATA_TYPE_UINT16, 2,
+                           (void *)(u16p + (size_t)side * g.n * kPK), dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+      *why = "cuTensorMapEncodeTiled failed";
+      return RBG_ERR_CUDA;
+    }
   }
   PfArgs A;
-  A.anynz = g.anynz;
   A.jlo = (int)cb;
   A.jhi = (int)ce;
   A.ct_lo = (int)(cb / kPN);
-  A.lo16 = lo16;
   A.item0 = item0;
   A.RB = RB;
   A.NT = NT;
@@ -508,7 +525,7 @@ int launch_sym_prefilter(const GraphArgs &g, const uint16_t *u16p, float lo16, i
   }
   if (e == cudaSuccess) {
     const int grid = std::max(1, std::min(sms, items));
-    k_sym_prefilter<<<grid, kPThreads, pf_smem(), s>>>(map, A);
+    k_sym_prefilter<<<grid, kPThreads, pf_smem(), s>>>(map[0], map[1], A);
     e = cudaGetLastError();
   }
   if (e != cudaSuccess) {

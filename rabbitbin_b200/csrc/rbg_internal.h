@@ -236,7 +236,8 @@ void launch_allpairs_sym(const GraphArgs &g, const SymOut &o, cudaStream_t s, in
 // set then), k_sym_check decides and counts them into o (blocks below
 // ceil(ce / 32)).  The item table [RB + 1] comes from launch_tc5_items (its
 // total from sym_tc5_items); u16p: the unit16 rows padded to 64 halves by
-// launch_pad_unit16 (n x 128 bytes, 16-byte aligned).  Needs g.Kp <= 64 and
+// launch_pad_unit16, a row copy and a column copy carrying the threshold lo16
+// in the last half (2 x n x 128 bytes, 16-byte aligned).  Needs g.S < 64 and
 // n < 2^27.  The offsets and item tables are made on the device, so nothing
 // crosses PCIe while input chunks stream in; tc5_capacity is the total of the
 // frac-based capacities of launch_tc5_coff (caps null).
@@ -244,11 +245,11 @@ int sym_tc5_items(int64_t cb, int64_t ce, int *RB, int *NT);
 int64_t tc5_capacity(int64_t n, double frac);
 void launch_tc5_coff(int64_t n, double frac, const int64_t *caps, int64_t *coff, cudaStream_t s);
 void launch_tc5_items(int64_t cb, int64_t ce, int32_t *item0, cudaStream_t s);
-void launch_pad_unit16(const GraphArgs &g, uint16_t *u16p, cudaStream_t s);
-int launch_sym_prefilter(const GraphArgs &g, const uint16_t *u16p, float lo16, int64_t cb,
-                         int64_t ce, const int32_t *item0, int RB, int NT, int items,
-                         uint32_t *cand, const int64_t *coff, int32_t *ccnt, int *overflow,
-                         int *err, int sms, cudaStream_t s, const char **why);
+void launch_pad_unit16(const GraphArgs &g, float lo16, uint16_t *u16p, cudaStream_t s);
+int launch_sym_prefilter(const GraphArgs &g, const uint16_t *u16p, int64_t cb, int64_t ce,
+                         const int32_t *item0, int RB, int NT, int items, uint32_t *cand,
+                         const int64_t *coff, int32_t *ccnt, int *overflow, int *err, int sms,
+                         cudaStream_t s, const char **why);
 void launch_sym_check(const GraphArgs &g, const SymOut &o, const uint32_t *cand,
                       const int64_t *coff, const int32_t *ccnt, int64_t blocks, cudaStream_t s);
 float prefilter_lo16(int S, float eps);
