@@ -698,6 +698,79 @@ def run_serve_form(args):
     print(json.dumps(res))
 
 
+def run_lpa_form(args):
+    """Label propagation (the step after the graph): the Fisher sweep on the
+    binning-scale graph, device-resident and through the host-buffer C-ABI call,
+    against the reference's own cluster_by_propagation on the host cores
+    (identical labels checked)."""
+    import torch
+    from rabbitbin_b200 import api
+    torch.cuda.set_device(0)
+    asm = _assembly(WORKLOAD["seed"])
+    buf, offs = asm.concat()
+    n = asm.n
+    params = api.default_params(m=WORKLOAD["sketch_m"], max_edges=WORKLOAD["max_edges"])
+    ctx = api.Context(0)
+    g = ctx.bin_graph(buf, offs, asm.depth, params)
+    src, dst, score = (np.array(g[k]) for k in ("src", "dst", "score"))
+    out = {}
+    for sync in (False, True):
+        for _ in range(max(args.warmup, 1)):
+            ctx.label_propagation_resident(n, seed=1, rule="fisher", synchronous=sync)
+        with ClockSampler(0) as clk:
+            t0 = time.perf_counter()
+            dev = []
+            for _ in range(args.steps):
+                lab, st = ctx.label_propagation_resident(n, seed=1, rule="fisher",
+                                                         synchronous=sync)
+                dev.append(st["incidence_ms"] + st["sweep_ms"])
+            wall = (time.perf_counter() - t0) * 1000.0 / args.steps
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            lab_h, _ = ctx.label_propagation(n, src, dst, score, seed=1, rule="fisher",
+                                             synchronous=sync)
+        e2e = (time.perf_counter() - t0) * 1000.0 / args.steps
+        out["sync" if sync else "gs"] = dict(
+            device_ms=float(np.median(dev)), resident_call_ms=wall, e2e_ms=e2e,
+            rounds=st["rounds"], changes=st["changes"], frozen=st["frozen"], arcs=st["arcs"],
+            incidence_ms=st["incidence_ms"], sweep_ms=st["sweep_ms"], labels=int(len(np.unique(lab))),
+            clocks=clk.summary(), _lab=lab, _lab_h=lab_h)
+    ref = None
+    if not args.no_cpu_baseline:
+        import oracle
+        R = oracle.ref()
+        if R is not None:
+            ref = {}
+            for key in ("gs", "sync"):
+                if key == "sync":
+                    os.environ["RABBIT_PAR_LPA"] = "1"
+                t0 = time.perf_counter()
+                want = R.label_propagation(n, src, dst, score, seed=1, nthreads=os.cpu_count())
+                ref[key] = dict(ms=(time.perf_counter() - t0) * 1000.0,
+                                identical=bool((want == out[key]["_lab"]).all() and
+                                               (want == out[key]["_lab_h"]).all()))
+                os.environ.pop("RABBIT_PAR_LPA", None)
+    for v in out.values():
+        v.pop("_lab")
+        v.pop("_lab_h")
+    gs = out["gs"]
+    res = {
+        "metric": "label propagation time per graph (Fisher, sequential sweep)",
+        "value": gs["device_ms"], "unit": "ms", "n_gpus": 1, "higher_is_better": False,
+        "form": "lpa", "steps": args.steps, "warmup": args.warmup,
+        "config": {"workload": WORKLOAD["workload"] + "; its graph, then label propagation",
+                   "nodes": n, "edges": int(len(src)), "seed": 1},
+        "e2e": {"value": gs["e2e_ms"], "unit": "ms",
+                "h2d_bytes_per_step": int(len(src) * 12), "d2h_bytes_per_step": int(n * 4)},
+        "sweeps": out,
+        "cpu_baseline": None if ref is None else {
+            "kind": "reference", "cores": os.cpu_count(), "value": ref["gs"]["ms"], "unit": "ms",
+            "sample": "the whole graph (the sequential sweep uses one thread; the synchronous "
+                      "one all cores)", "sweeps": ref},
+    }
+    print(json.dumps(res))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -715,9 +788,10 @@ def main():
                     help="serve form: which request loops replay the trace")
     ap.add_argument("--contigs", type=int, default=0, help="profiling: fewer contigs")
     ap.add_argument("--samples", type=int, default=0, help="profiling: other S")
-    ap.add_argument("--form", default="plain", choices=["plain", "batch", "serve"],
+    ap.add_argument("--form", default="plain", choices=["plain", "batch", "serve", "lpa"],
                     help="plain: the binning-scale assembly; batch: a mixed stream per call; "
-                         "serve: a Poisson request stream through the request loop")
+                         "serve: a Poisson request stream through the request loop; lpa: label "
+                         "propagation on the binning-scale graph")
     ap.add_argument("--batch-size", type=int, default=64, help="batch form: assemblies")
     ap.add_argument("--config", default="binning", choices=["binning", "large"],
                     help="binning: 50,000 contigs, S=20 (default); large: 300,000 contigs, S=30")
@@ -741,6 +815,8 @@ def main():
         run_batch_form(args)
     elif args.form == "serve":
         run_serve_form(args)
+    elif args.form == "lpa":
+        run_lpa_form(args)
     elif args.shard == "rows":
         run_shard_form(args)
     else:

@@ -441,6 +441,62 @@ int rbg_build_pmh_winners_noalloc(const rbg_params *p, const char *seq_device,
 int rbg_pmh_stream_tables(int32_t k, int32_t m, uint64_t pmh_seed, int32_t fp_contract,
                           int32_t *n_elems, int32_t *canon_codes, double *U, uint32_t *W32);
 
+/* ── Fisher label propagation: the step after the graph ───────────────────
+ *   rbg_label_propagation ← the incidence build src/rabbitbin.cpp:5597-5622
+ *                           (edges with edgeScore > 0, clamped to 1 - 1e-6f,
+ *                           lists ordered by neighbour id), the node order
+ *                           :5643-5645 (std::shuffle of 0..n-1 with
+ *                           std::default_random_engine(seed)) and
+ *                           cluster_by_propagation src/impl/rb_cluster.cpp:376-740
+ * Score rules of RABBIT_LPA_SCORE (rb_cluster.cpp:40-70); RABBIT_PAR_LPA
+ * selects the synchronous sweep (:490-594), otherwise the sequential
+ * (Gauss-Seidel) sweep in node order (:596-714), both until a round changes no
+ * label.  membership[v] is v's label (a node id), identity for nodes without
+ * edges; with no edges at all every node keeps its own label (the reference
+ * returns early there, :381-385).  Status: RBG_ERR_ARG for a negative score
+ * ("edgeScore must be non-negative", :441-444) or an endpoint >= n_nodes.
+ * The Louvain, fused and multilevel variants of RABBIT_CLUSTER and the seed
+ * ensemble are not built. */
+enum {
+  RBG_LPA_FISHER = 0,   /* chi2 CDF of -2 sum log(1 - w) (default)               */
+  RBG_LPA_TAIL = 1,     /* minus the chi2 upper tail                              */
+  RBG_LPA_LOGSUM = 2,   /* sum of -log(1 - w)                                     */
+  RBG_LPA_SUM = 3,      /* sum of w                                               */
+  RBG_LPA_MEAN = 4,     /* sum of w / count                                       */
+  RBG_LPA_MAX = 5       /* max w                                                  */
+};
+
+typedef struct rbg_lpa_params {
+  uint64_t seed;                /* --seed: the node order                            */
+  const uint32_t *node_order;   /* or an explicit order (a permutation of 0..n-1)    */
+  int32_t score_rule;           /* RBG_LPA_* (RABBIT_LPA_SCORE)                      */
+  int32_t synchronous;          /* RABBIT_PAR_LPA                                    */
+  int32_t max_rounds;           /* 0: until converged (the reference has no limit)   */
+  int32_t reserved;
+} rbg_lpa_params;
+
+typedef struct rbg_lpa_stats {
+  int32_t rounds;               /* sweeps run, the last one without a change         */
+  int32_t reserved;
+  int64_t changes;              /* label changes over all rounds                     */
+  int64_t frozen;               /* nodes frozen by the cycle guard                   */
+  int64_t arcs;                 /* incidence entries (2 x edges with a score > 0)    */
+  float incidence_ms;           /* device time: incidence lists                      */
+  float sweep_ms;               /* device time: all rounds                           */
+} rbg_lpa_stats;
+
+/* Reference defaults: seed 1 (the bin command's default), the rule and the
+ * sweep from RABBIT_LPA_SCORE / RABBIT_PAR_LPA as the reference reads them. */
+int rbg_default_lpa_params(rbg_lpa_params *lp);
+/* On a host edge list (n_edges entries each of from, to, edge_score). */
+int rbg_label_propagation(rbg_ctx *ctx, const rbg_lpa_params *lp, int64_t n_nodes,
+                          int64_t n_edges, const uint32_t *from, const uint32_t *to,
+                          const float *edge_score, uint32_t *membership, rbg_lpa_stats *stats);
+/* On the graph of the context's last rbg_bin_graph / rbg_run_resident call,
+ * still on the device (no edge copy); n_nodes is that call's contig count. */
+int rbg_label_propagation_resident(rbg_ctx *ctx, const rbg_lpa_params *lp, uint32_t *membership,
+                                   rbg_lpa_stats *stats);
+
 #ifdef __cplusplus
 }
 #endif

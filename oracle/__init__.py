@@ -90,6 +90,36 @@ class _Lib:
                                   C.POINTER(C.c_float), C.POINTER(C.c_float),
                                   C.POINTER(RefOut)]
 
+    def label_propagation(self, n, src, dst, score, seed=1, node_order=None, nthreads=0):
+        """cluster_by_propagation of the reference on an edge list (harness
+        only): membership uint32[n].  The score rule follows RABBIT_LPA_SCORE
+        as it was when the library loaded; RABBIT_PAR_LPA is read per call."""
+        f = getattr(self.lib, "ref_label_propagation")
+        f.restype = C.c_int
+        f.argtypes = [C.c_int64, C.c_int64, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                      C.POINTER(C.c_float), C.c_ulonglong, C.POINTER(C.c_uint32),
+                      C.POINTER(C.c_uint32), C.c_int]
+        a = np.ascontiguousarray(src, np.uint32)
+        b = np.ascontiguousarray(dst, np.uint32)
+        w = np.ascontiguousarray(score, np.float32)
+        order = None if node_order is None else np.ascontiguousarray(node_order, np.uint32)
+        out = np.zeros(int(n), np.uint32)
+        rc = f(int(n), len(a), _ptr(a, C.c_uint32), _ptr(b, C.c_uint32), _ptr(w, C.c_float),
+               int(seed), None if order is None else _ptr(order, C.c_uint32),
+               _ptr(out, C.c_uint32), int(nthreads))
+        if rc != 0:
+            raise ValueError("edgeScore must be non-negative")
+        return out
+
+    def lpa_node_order(self, n, seed=1):
+        """The seeded node order of the reference (src/rabbitbin.cpp:5643-5645)."""
+        f = getattr(self.lib, "ref_lpa_node_order")
+        f.restype = None
+        f.argtypes = [C.c_int64, C.c_ulonglong, C.POINTER(C.c_uint32)]
+        out = np.zeros(int(n), np.uint32)
+        f(int(n), int(seed), _ptr(out, C.c_uint32))
+        return out
+
     def oph_values(self, seqcat, offsets, m=500, K=8, bits=2):
         """One-permutation MinHash bucket values [n, m] (uint8)."""
         n = len(offsets) - 1

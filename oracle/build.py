@@ -47,6 +47,10 @@ FRAGMENTS = [
     ("frag_calibrate.inc", "impl/rb_graph.cpp", 1362, 1384),
     ("frag_calibrate_fused.inc", "impl/rb_graph.cpp", 1386, 1438),
     ("frag_cache.inc", "impl/rb_cache.cpp", 26, 319),
+    ("frag_lpa_rules.inc", "impl/rb_cluster.cpp", 3, 93),
+    ("frag_lpa.inc", "impl/rb_cluster.cpp", 336, 740),
+    ("frag_incidence.inc", "rabbitbin.cpp", 5600, 5622),
+    ("frag_node_order.inc", "rabbitbin.cpp", 5643, 5645),
 ]
 
 
@@ -96,9 +100,10 @@ def build_ref():
                 f.write(text)
     shim = os.path.join(HERE, "ref_shim.cpp")
     cache_shim = os.path.join(HERE, "ref_cache_shim.cpp")
-    deps = [shim, cache_shim, __file__, os.path.join(REF_SRC, "probmh.cpp")]
+    lpa_shim = os.path.join(HERE, "ref_lpa_shim.cpp")
+    deps = [shim, cache_shim, lpa_shim, __file__, os.path.join(REF_SRC, "probmh.cpp")]
     if _stale(out, deps):
-        _run(["g++"] + FLAGS + ["-I", frag_dir, "-I", REF_SRC, shim, cache_shim,
+        _run(["g++"] + FLAGS + ["-I", frag_dir, "-I", REF_SRC, shim, cache_shim, lpa_shim,
                                 os.path.join(REF_SRC, "probmh.cpp"), "-o", out])
     return out
 

@@ -223,6 +223,24 @@ _lib = None
 ALLGATHER_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p)
 
 
+class LpaParams(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("node_order", C.c_void_p), ("score_rule", C.c_int32),
+                ("synchronous", C.c_int32), ("max_rounds", C.c_int32), ("reserved", C.c_int32)]
+
+
+class LpaStats(C.Structure):
+    _fields_ = [("rounds", C.c_int32), ("reserved", C.c_int32), ("changes", C.c_int64),
+                ("frozen", C.c_int64), ("arcs", C.c_int64), ("incidence_ms", C.c_float),
+                ("sweep_ms", C.c_float)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+# RABBIT_LPA_SCORE names (src/impl/rb_cluster.cpp:41-50) -> RBG_LPA_*
+LPA_RULES = {"fisher": 0, "tail": 1, "logsum": 2, "sum": 3, "mean": 4, "max": 5}
+
+
 class Shard(C.Structure):
     _fields_ = [("rank", C.c_int32), ("world", C.c_int32), ("device_buffers", C.c_int32),
                 ("reserved", C.c_int32), ("allgather", ALLGATHER_FN), ("user", C.c_void_p)]
@@ -286,6 +304,12 @@ def lib():
         "rbg_free_cache": ([P(CacheState)], C.c_int),
         "rbg_build_pmh_winners_noalloc": ([P(Params), vp, vp, C.c_int64, C.c_int64, vp, vp,
                                            C.c_char_p, C.c_size_t], C.c_int),
+        "rbg_default_lpa_params": ([P(LpaParams)], C.c_int),
+        "rbg_label_propagation": ([vp, P(LpaParams), C.c_int64, C.c_int64, P(C.c_uint32),
+                                   P(C.c_uint32), P(C.c_float), P(C.c_uint32), P(LpaStats)],
+                                  C.c_int),
+        "rbg_label_propagation_resident": ([vp, P(LpaParams), P(C.c_uint32), P(LpaStats)],
+                                           C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -533,6 +557,53 @@ class Context:
 
     def fetch_graph(self):
         return self._graph_call(self._L.rbg_fetch_graph, self._h)
+
+    @staticmethod
+    def _lpa_params(seed, rule, synchronous, node_order, max_rounds):
+        lp = LpaParams()
+        lib().rbg_default_lpa_params(C.byref(lp))
+        if seed is not None:
+            lp.seed = int(seed)
+        if rule is not None:
+            lp.score_rule = LPA_RULES[rule] if isinstance(rule, str) else int(rule)
+        if synchronous is not None:
+            lp.synchronous = int(bool(synchronous))
+        lp.max_rounds = int(max_rounds)
+        order = None
+        if node_order is not None:
+            order = np.ascontiguousarray(node_order, np.uint32)
+            lp.node_order = order.ctypes.data
+        return lp, order
+
+    def label_propagation(self, n_nodes, src, dst, score, seed=None, rule=None,
+                          synchronous=None, node_order=None, max_rounds=0):
+        """cluster_by_propagation on an edge list (rbg_label_propagation):
+        (membership uint32[n_nodes], stats dict).  rule: a RABBIT_LPA_SCORE
+        name or RBG_LPA_* value; None takes the environment, as the reference."""
+        lp, order = self._lpa_params(seed, rule, synchronous, node_order, max_rounds)
+        f = np.ascontiguousarray(src, np.uint32)
+        t = np.ascontiguousarray(dst, np.uint32)
+        w = np.ascontiguousarray(score, np.float32)
+        out = np.zeros(int(n_nodes), np.uint32)
+        st = LpaStats()
+        self._check(self._L.rbg_label_propagation(
+            self._h, C.byref(lp), int(n_nodes), len(f), _p(f, C.c_uint32), _p(t, C.c_uint32),
+            _p(w, C.c_float), _p(out, C.c_uint32), C.byref(st)), "label_propagation")
+        del order
+        return out, st.as_dict()
+
+    def label_propagation_resident(self, n_nodes, seed=None, rule=None, synchronous=None,
+                                   node_order=None, max_rounds=0):
+        """Label propagation on the graph of the last bin_graph / run_resident
+        call, still on the device (rbg_label_propagation_resident)."""
+        lp, order = self._lpa_params(seed, rule, synchronous, node_order, max_rounds)
+        out = np.zeros(int(n_nodes), np.uint32)
+        st = LpaStats()
+        self._check(self._L.rbg_label_propagation_resident(
+            self._h, C.byref(lp), _p(out, C.c_uint32), C.byref(st)),
+            "label_propagation_resident")
+        del order
+        return out, st.as_dict()
 
     def parse_fasta(self, data, min_contig=2500, min_small_contig=1000):
         """Device FASTA parse (rbg_parse_fasta) of the bytes `data`:

@@ -21,10 +21,10 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SRCS = ["kernels_sketch.cu", "kernels_graph.cu", "kernels_allpairs.cu", "kernels_onehot.cu",
            "kernels_onehot_mma.cu", "kernels_sym_tc5.cu", "kernels_pmh_query.cu", "kernels_index.cu",
            "kernels_util.cu",
-           "noalloc.cu", "kernels_fasta.cu"]
+           "noalloc.cu", "kernels_fasta.cu", "kernels_lpa.cu"]
 CPP_SRCS = ["pmh_streams.cpp", "calib.cpp", "engine.cpp", "batch.cpp", "server.cpp", "fasta.cpp",
-            "cache.cpp", "host_pack.cpp"]
-HEADERS = ["rbg_internal.h", "engine_internal.h", "select_topk.cuh", "tc05.cuh",
+            "cache.cpp", "host_pack.cpp", "lpa.cpp"]
+HEADERS = ["rbg_internal.h", "engine_internal.h", "select_topk.cuh", "tc05.cuh", "ddmath.cuh",
            "../../include/rabbitbin_b200.h", "gen_zig_tables.py"]
 
 

@@ -1441,6 +1441,7 @@ int rbg_destroy(rbg_ctx *c) {
   release_batch_graphs(c);
   if (c->batch) c->batch->release();
   if (c->fasta) c->fasta->release();
+  if (c->lpa) c->lpa->release();
   c->pin.release();
   c->b0pin.release();
   c->shard_host.release();

@@ -218,6 +218,22 @@ struct FastaBufs {
   }
 };
 
+// Buffers of label propagation (lpa.cpp): the edge list as copied in, the
+// incidence lists and the sweep state.
+struct LpaBufs {
+  DBuf from, to, score, q, deg, off, fill, key, nbr, w, order, pos, label, act0, act1, frozen,
+      done, prop, vlab, vcnt, vnext, misc, gtab;
+  HBuf pin, order_pin;
+  void release() {
+    DBuf *all[] = {&from, &to, &score, &q, &deg, &off, &fill, &key, &nbr, &w, &order, &pos,
+                   &label, &act0, &act1, &frozen, &done, &prop, &vlab, &vcnt, &vnext, &misc,
+                   &gtab};
+    for (DBuf *b : all) b->release();
+    pin.release();
+    order_pin.release();
+  }
+};
+
 // Counts of one parse; the outputs are in FastaBufs: slot 0 large, 1 small
 // (seq: sequences back to back, seq_off: n+1 offsets, name_start / name_len:
 // name ranges in the input).
@@ -354,6 +370,8 @@ struct rbg_ctx {
   std::unique_ptr<rbg::BatchBufs> batch;
   // FASTA ingest
   std::unique_ptr<rbg::FastaBufs> fasta;
+  // label propagation
+  std::unique_ptr<rbg::LpaBufs> lpa;
 };
 
 namespace rbg {

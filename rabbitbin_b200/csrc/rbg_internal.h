@@ -440,4 +440,50 @@ int allpairs_variant(const GraphArgs &g);
 // lo/hi: band of the exact-safe FP32 chain; lo16: the tensor-core prune bound.
 void prefilter_bands(int S, float eps, float *lo, float *hi, float *lo16);
 
+// Label propagation (kernels_lpa.cu).  Incidence: per-edge quantities q and
+// endpoint degrees (err: 1 negative score, 2 endpoint out of range), offsets
+// (n + 1) and the largest degree, arc keys scattered per node, keys sorted per
+// node into neighbour and quantity arrays.
+int lpa_raw_rule(int rule);
+void launch_lpa_edges(const uint32_t *from, const uint32_t *to, const float *score, int64_t E,
+                      int64_t n, int rule, float *q, uint32_t *deg, int *err, cudaStream_t s);
+void launch_lpa_offsets(const uint32_t *deg, int64_t n, int64_t *off, int64_t *maxdeg,
+                        cudaStream_t s);
+void launch_lpa_scatter(const uint32_t *from, const uint32_t *to, const float *score, int64_t E,
+                        int64_t n, const int64_t *off, uint32_t *fill, uint64_t *key,
+                        cudaStream_t s);
+void launch_lpa_sort(const int64_t *off, int64_t n, uint64_t *key, const float *q, uint32_t *nbr,
+                     float *w, cudaStream_t s);
+void launch_lpa_init(const uint32_t *order, int64_t n, uint32_t *pos, uint32_t *label,
+                     uint8_t *active, uint8_t *next_active, uint8_t *frozen, uint32_t *done,
+                     uint32_t *vcnt, uint32_t *vnext, cudaStream_t s);
+// State of the sweeps (see kernels_lpa.cu); vlab holds lpa_visit_block()
+// labels per visited-set block, blocks 0..n-1 owned by the nodes, vpool_cap
+// spill blocks after them; gtab: gtab_slots x 20 bytes per sweep warp when the
+// largest degree exceeds lpa_table_max_deg() (slots >= 4/3 of it, a power of 2).
+struct LpaSweepArgs {
+  int64_t n = 0;
+  const int64_t *off = nullptr;
+  const uint32_t *nbr = nullptr;
+  const float *w = nullptr;
+  const uint32_t *order = nullptr, *pos = nullptr;
+  uint32_t *label = nullptr;
+  uint8_t *active = nullptr, *next_active = nullptr, *frozen = nullptr;
+  uint32_t *done = nullptr, *prop = nullptr;
+  uint32_t *vlab = nullptr, *vcnt = nullptr, *vnext = nullptr, *vpool_used = nullptr;
+  uint32_t vpool_cap = 0;
+  uint32_t *claim = nullptr;
+  unsigned long long *counts = nullptr;   // [0] changes, [1] freezes of the round
+  uint32_t *gtab = nullptr;
+  int gtab_slots = 0;
+  int rule = 0;
+  uint32_t round = 0;
+  int *err = nullptr;
+};
+// Warps of one sweep launch (a multiple of the CTA's 8).
+int lpa_sweep_warps(int sms);
+int lpa_table_max_deg();
+int lpa_visit_block();
+void launch_lpa_round(const LpaSweepArgs &a, int sync, int warps, cudaStream_t s);
+
 }  // namespace rbg

@@ -1,6 +1,7 @@
 """Regenerate the golden fixtures from RabbitBin's own code (oracle/_ref).
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          # all fixtures
+    python tests/golden/make_golden.py --lpa    # label-propagation labels only
 
 Runs in the build container, where the reference tree is present: the
 reference harness (src/probmh.cpp + the hot-path functions of
@@ -57,5 +58,35 @@ def main():
         print(name, len(seqs), "contigs", len(out.get("src", [])), "edges")
 
 
+LPA_GRAPHS = ["small_path_s5", "fused_s20_m64", "fused_s3_m96"]
+
+
+def make_lpa():
+    """Labels of the reference's label propagation (cluster_by_propagation,
+    src/impl/rb_cluster.cpp:376-740) on the edge lists of the graph fixtures,
+    sequential and synchronous sweeps, seeds 1 and 7 -> lpa.npz."""
+    ref = oracle.ref()
+    if ref is None:
+        raise SystemExit("reference tree not available")
+    out = {}
+    for name in LPA_GRAPHS:
+        g = np.load(os.path.join(HERE, name + ".npz"))
+        n = len(g["offsets"]) - 1
+        for seed in (1, 7):
+            out[f"{name}_gs_{seed}"] = ref.label_propagation(n, g["src"], g["dst"], g["score"],
+                                                             seed=seed)
+            os.environ["RABBIT_PAR_LPA"] = "1"
+            out[f"{name}_sync_{seed}"] = ref.label_propagation(n, g["src"], g["dst"],
+                                                               g["score"], seed=seed)
+            del os.environ["RABBIT_PAR_LPA"]
+        out[f"{name}_order_1"] = ref.lpa_node_order(n, 1)
+        print(name, n, "nodes", len(np.unique(out[f"{name}_gs_1"])), "labels")
+    np.savez_compressed(os.path.join(HERE, "lpa.npz"), **out)
+
+
 if __name__ == "__main__":
-    main()
+    if "--lpa" in sys.argv:
+        make_lpa()
+    else:
+        main()
+        make_lpa()
