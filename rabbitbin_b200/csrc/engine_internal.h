@@ -221,11 +221,11 @@ struct FastaBufs {
 // Buffers of label propagation (lpa.cpp): the edge list as copied in, the
 // incidence lists and the sweep state.
 struct LpaBufs {
-  DBuf from, to, score, q, deg, off, fill, key, nbr, w, order, pos, label, act0, act1, frozen,
-      done, prop, vlab, vcnt, vnext, misc, gtab;
+  DBuf from, to, score, q, deg, off, fill, key, nbr, w, early, rec, order, pos, label, act0,
+      act1, frozen, done, prop, vlab, vcnt, vnext, misc, gtab;
   HBuf pin, order_pin;
   void release() {
-    DBuf *all[] = {&from, &to, &score, &q, &deg, &off, &fill, &key, &nbr, &w, &order, &pos,
+    DBuf *all[] = {&from, &to, &score, &q, &deg, &off, &fill, &key, &nbr, &w, &early, &rec, &order, &pos,
                    &label, &act0, &act1, &frozen, &done, &prop, &vlab, &vcnt, &vnext, &misc,
                    &gtab};
     for (DBuf *b : all) b->release();

@@ -29,7 +29,7 @@
 // the group's lowest lane adds the group's quantities to that label's running
 // score one by one in arc order, so every label's score is the reference's
 // left-to-right double sum.  Labels live in a per-warp hash table (shared
-// memory up to 384 arcs, a per-warp global table above), and the labels in
+// memory up to 256 arcs, a per-warp global table above), and the labels in
 // order of first appearance in a list, which gives the reference's first-max
 // tie-break.  The decision (keep the current label when it is within 1e-12 of
 // the best), the cycle guard (a node that returns to a label it had is frozen)
@@ -56,7 +56,11 @@ constexpr unsigned FULL = 0xFFFFFFFFu;
 constexpr uint32_t kEmpty = 0xFFFFFFFFu;
 constexpr int kLpaWarps = 8;                  // warps per CTA of the sweep kernels
 constexpr int kTabSlots = 512;                // shared hash slots per warp
-constexpr int kTabMaxDeg = 384;               // arcs above which a node uses the global table
+constexpr int kTabMaxDeg = 256;               // arcs above which a node takes the general path
+// per-warp shared region: scores, keys, counts, first-appearance list, then the
+// arc stage (neighbour / label and quantity per arc, later the label score
+// intervals), then a 32-float exchange buffer of the general path
+constexpr int kWarpSmem = kTabSlots * 16 + kTabMaxDeg * 4 + kTabMaxDeg * 16 + 32 * 4;
 constexpr int kVisitPer = 14;                 // labels per visited-set block
 constexpr uint64_t kWaitNs = 5000000000ull;   // bound of one wait
 
@@ -75,19 +79,21 @@ __device__ __forceinline__ uint32_t ld_relaxed(const uint32_t *p) {
   asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
-__device__ __forceinline__ uint32_t ld_relaxed_u8(const uint8_t *p) {
-  uint16_t v;
-  asm volatile("ld.relaxed.gpu.global.u8 %0, [%1];" : "=h"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_relaxed_u8(uint8_t *p, uint32_t v) {
-  asm volatile("st.relaxed.gpu.global.u8 [%0], %1;" ::"l"(p), "h"((uint16_t)v) : "memory");
-}
 __device__ __forceinline__ void st_relaxed(uint32_t *p, uint32_t v) {
   asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 __device__ __forceinline__ void st_release(uint32_t *p, uint32_t v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+// State that other launches wrote (labels, flags, visited sets, proposals) is
+// read at the L2, never from a line an SM's L1 may still hold from an earlier
+// round: ld.global.cg.
+__device__ __forceinline__ uint32_t ld_cg(const uint32_t *p) { return __ldcg(p); }
+__device__ __forceinline__ uint32_t ld_cg8(const uint8_t *p) {
+  uint16_t v;
+  asm volatile("ld.global.cg.u8 %0, [%1];" : "=h"(v) : "l"(p));
+  return v;
 }
 
 // ── the score rules (rb_cluster.cpp:3-22, :40-76) ──────────────────────────
@@ -120,6 +126,58 @@ __device__ __forceinline__ void lpa_accumulate(int rule, double &dst, float x) {
   } else {
     dst = dd::add(dst, (double)x);
   }
+}
+
+// An interval [lo, hi] that holds lpa_combine(rule, m, acc) without its cost
+// (lo == hi: the value itself).  The fisher and tail rules repeat the tail sum
+// with the library exp (within 1 ulp) and u * (1/i) (inv[i] = RN(1/i)) in place
+// of the correctly rounded exp and u / i.  Against the exact evaluation the
+// start differs by at most 1.5 ulp and every step of the product chain adds at
+// most 5 units of 2^-53 of relative drift (two operand roundings, two product
+// roundings, the quotient), the m roundings of each sum another 2^-53 Q each,
+// so |Q' - Q| <= (7m + 3) 2^-53 Q' (+ m 2^-1074 for subnormal terms); the bound
+// used, (8m + 16) 2^-52 Q' + m 2^-1070, holds it twice over.  The value then
+// lies in RN(1 - [Q' - E, Q' + E]) (fisher, monotone) or -[Q' - E, Q' + E]
+// (tail).  Below acc = -700 the start is near the subnormal range: there the
+// fisher value is exactly 1 when the whole tail sum is below 2^-60 (then the
+// computed one is below 2^-54 and 1 - Q rounds to 1), which the largest term
+// bounds (u > m - 1, so the terms rise: Q <= m e^-u u^(m-1) / (m-1)!, tested
+// with one unit of slack in the log); anything else is evaluated exactly.
+__device__ void lpa_interval(int rule, int m, double acc, const double *inv, double *lo,
+                             double *hi) {
+  if (rule != RBG_LPA_FISHER && rule != RBG_LPA_TAIL) {
+    *lo = *hi = lpa_combine(rule, m, acc);              // no exp: exact and cheap
+    return;
+  }
+  const double u = dd::mul(0.5, dd::mul(-2.0, acc));
+  if (-u >= -700.0) {
+    double p = ::exp(-u);
+    double Q = p;
+    for (int i = 1; i < m; ++i) {
+      p = dd::mul(p, dd::mul(u, inv[i]));
+      Q = dd::add(Q, p);
+    }
+    const double E = __dadd_ru(__dmul_ru(__dmul_ru(8.0 * m + 16.0, 0x1p-52), Q),
+                               __dmul_ru((double)m, 0x1p-1070));
+    const double tlo = fmax(0.0, __dsub_rd(Q, E)), thi = __dadd_ru(Q, E);
+    if (rule == RBG_LPA_FISHER) {
+      const double a = dd::sub(1.0, thi), b = dd::sub(1.0, tlo);
+      *lo = a < 0.0 ? 0.0 : a;
+      *hi = b < 0.0 ? 0.0 : b;
+    } else {
+      *lo = -thi;
+      *hi = -tlo;
+    }
+    return;
+  }
+  if (rule == RBG_LPA_FISHER && u > (double)(m - 1)) {
+    const double lq = ::log((double)m) - u + (double)(m - 1) * ::log(u) - ::lgamma((double)m);
+    if (lq < -60.0 * 0.6931471805599453 - 1.0) {
+      *lo = *hi = 1.0;
+      return;
+    }
+  }
+  *lo = *hi = lpa_combine(rule, m, acc);
 }
 
 // ── incidence ──────────────────────────────────────────────────────────────
@@ -278,6 +336,22 @@ __global__ void k_lpa_init(const uint32_t *__restrict__ order, int64_t n, uint32
   }
 }
 
+// Per arc: does the neighbour come earlier in the node order than the node?
+// Per position: the node there, its degree and first arc.
+__global__ void k_lpa_early(const int64_t *__restrict__ off, const uint32_t *__restrict__ nbr,
+                            const uint32_t *__restrict__ pos, int64_t n,
+                            uint8_t *__restrict__ early, uint4 *__restrict__ rec) {
+  const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const int lane = threadIdx.x & 31;
+  for (int64_t v = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); v < n; v += nw) {
+    const uint32_t pv = pos[v];
+    const int64_t a0 = off[v], a1 = off[v + 1];
+    for (int64_t a = a0 + lane; a < a1; a += 32) early[a] = pos[nbr[a]] < pv;
+    if (lane == 0)
+      rec[pv] = make_uint4((uint32_t)v, (uint32_t)(a1 - a0), (uint32_t)a0, (uint32_t)(a0 >> 32));
+  }
+}
+
 // ── the sweeps ──────────────────────────────────────────────────────────────
 struct Sweep {
   int64_t n;
@@ -285,6 +359,8 @@ struct Sweep {
   const uint32_t *nbr;
   const float *w;
   const uint32_t *order, *pos;
+  const uint8_t *early;           // per arc: the neighbour comes earlier in the order
+  const uint4 *rec;               // per position: node, degree, first arc (low, high)
   uint32_t *label;
   uint8_t *active, *next_active, *frozen;
   uint32_t *done;                 // round of a node's last visit (Gauss-Seidel)
@@ -415,26 +491,34 @@ __device__ uint32_t decide(const Sweep &S, Table &T, float *wb, uint32_t v, int6
 // Applies a change of v from kprev to best (rb_cluster.cpp:565-582 and
 // :685-708): label, counters, neighbours' activation marks, visited set and
 // freeze.  Called by the whole warp.
+// Marks go to next_active, which no one reads before the next round: in the
+// synchronous sweep every neighbour, in the sequential one only the neighbours
+// already visited in this round (and the node itself on a self-loop) -- the
+// later ones learn of the change from the stamp within this round.
 __device__ void commit(const Sweep &S, uint32_t v, uint32_t kprev, uint32_t best, int64_t a0,
-                       int64_t a1, uint8_t *mark) {
+                       int64_t a1, bool sequential) {
   const int lane = threadIdx.x & 31;
-  for (int64_t a = a0 + lane; a < a1; a += 32) st_relaxed_u8(mark + __ldg(S.nbr + a), 1u);
+  for (int64_t a = a0 + lane; a < a1; a += 32) {
+    const uint32_t u = __ldg(S.nbr + a);
+    if (!sequential || __ldg(S.early + a) || u == v) S.next_active[u] = 1;
+  }
   if (lane == 0) {
     st_relaxed(S.label + v, best);
     atomicAdd(S.counts, 1ull);
     // visited set: {kprev} on the first change, then best; a label seen before freezes v
     uint32_t *blk = S.vlab + (size_t)v * kVisitPer;
     uint32_t *cntp = S.vcnt + v, *nextp = S.vnext + v;
-    if (S.vcnt[v] == 0) {
+    if (ld_cg(S.vcnt + v) == 0) {
       blk[0] = kprev;
       S.vcnt[v] = 1;
     }
     bool seen = false;
+    uint32_t c = 0;
     for (;;) {
-      const uint32_t c = *cntp;
-      for (uint32_t i = 0; i < c && !seen; ++i) seen = blk[i] == best;
-      if (seen || *nextp == kEmpty) break;
-      const uint32_t b = *nextp;
+      c = ld_cg(cntp);
+      for (uint32_t i = 0; i < c && !seen; ++i) seen = ld_cg(blk + i) == best;
+      const uint32_t b = ld_cg(nextp);
+      if (seen || b == kEmpty) break;
       blk = S.vlab + (size_t)b * kVisitPer;
       cntp = S.vcnt + b;
       nextp = S.vnext + b;
@@ -442,9 +526,9 @@ __device__ void commit(const Sweep &S, uint32_t v, uint32_t kprev, uint32_t best
     if (seen) {
       S.frozen[v] = 1;
       atomicAdd(S.counts + 1, 1ull);
-    } else if (*cntp < (uint32_t)kVisitPer) {
-      blk[*cntp] = best;
-      *cntp += 1;
+    } else if (c < (uint32_t)kVisitPer) {
+      blk[c] = best;
+      *cntp = c + 1;
     } else {
       const uint32_t b = atomicAdd(S.vpool_used, 1u);
       if (b >= S.vpool_cap) {
@@ -460,12 +544,32 @@ __device__ void commit(const Sweep &S, uint32_t v, uint32_t kprev, uint32_t best
   }
 }
 
+// Per-warp shared region (kWarpSmem bytes): table, then the arc stage.
+__device__ __forceinline__ unsigned char *warp_region(unsigned char *smem) {
+  return smem + (size_t)(threadIdx.x >> 5) * kWarpSmem;
+}
+__device__ __forceinline__ uint32_t *warp_stage_u(unsigned char *smem) {
+  return (uint32_t *)(warp_region(smem) + kTabSlots * 16 + kTabMaxDeg * 4);
+}
+__device__ __forceinline__ float *warp_stage_w(unsigned char *smem) {
+  return (float *)(warp_stage_u(smem) + kTabMaxDeg);
+}
+__device__ __forceinline__ double *warp_stage_d(unsigned char *smem) {   // lo, hi intervals
+  return (double *)warp_stage_u(smem);
+}
+__device__ __forceinline__ float *warp_wbuf(unsigned char *smem) {
+  return (float *)(warp_region(smem) + kTabSlots * 16 + kTabMaxDeg * 20);
+}
+// 1/i rounded, i < kTabMaxDeg, after the warps' regions
+__device__ __forceinline__ double *cta_inv(unsigned char *smem) {
+  return (double *)(smem + (size_t)kLpaWarps * kWarpSmem);
+}
+
 __device__ __forceinline__ Table warp_table(const Sweep &S, unsigned char *smem, int64_t deg,
                                             int gwarp) {
-  const int wi = threadIdx.x >> 5;
   Table T;
   if (deg <= kTabMaxDeg) {
-    unsigned char *b = smem + (size_t)wi * (kTabSlots * 16 + kTabMaxDeg * 4);
+    unsigned char *b = warp_region(smem);
     T.score = (double *)b;
     T.key = (uint32_t *)(b + kTabSlots * 8);
     T.cnt = (int32_t *)(b + kTabSlots * 12);
@@ -483,37 +587,196 @@ __device__ __forceinline__ Table warp_table(const Sweep &S, unsigned char *smem,
   return T;
 }
 
-size_t sweep_smem() {
-  return (size_t)kLpaWarps * (kTabSlots * 16 + kTabMaxDeg * 4 + 32 * 4);
-}
+size_t sweep_smem() { return (size_t)kLpaWarps * kWarpSmem + kTabMaxDeg * 8; }
 
-__device__ __forceinline__ float *warp_wbuf(unsigned char *smem) {
-  return (float *)(smem + (size_t)kLpaWarps * (kTabSlots * 16 + kTabMaxDeg * 4)) +
-         (threadIdx.x >> 5) * 32;
-}
-
-// Tables start empty: keys of every shared and global table set to kEmpty.
+// Tables start empty: keys of every shared and global table set to kEmpty;
+// the reciprocal table of the CTA filled.  Called by all threads of the CTA.
 __device__ void clear_tables(const Sweep &S, unsigned char *smem, int gwarp) {
   const int lane = threadIdx.x & 31;
-  const int wi = threadIdx.x >> 5;
-  uint32_t *k = (uint32_t *)(smem + (size_t)wi * (kTabSlots * 16 + kTabMaxDeg * 4) + kTabSlots * 8);
+  uint32_t *k = (uint32_t *)(warp_region(smem) + kTabSlots * 8);
   for (int i = lane; i < kTabSlots; i += 32) k[i] = kEmpty;
   if (S.gtab) {
     const size_t G = (size_t)S.gtab_slots;
     uint32_t *gk = S.gtab + (size_t)gwarp * G * 5 + 2 * G;
     for (size_t i = lane; i < G; i += 32) gk[i] = kEmpty;
   }
-  __syncwarp();
+  double *inv = cta_inv(smem);
+  for (int i = threadIdx.x; i < kTabMaxDeg; i += blockDim.x)
+    inv[i] = i ? __drcp_rn((double)i) : 0.0;
+  __syncthreads();
 }
 
-// Bounded wait until node u was visited in this round.
-__device__ __forceinline__ bool wait_visited(const Sweep &S, uint32_t u) {
-  if (ld_acquire(S.done + u) >= S.round) return true;
+// Visit stamps: a node visited in round r holds 2r + 1 when its label
+// changed, 2r otherwise, published after its writes.  Bounded wait (relaxed
+// polls; the caller fences before it reads what the node wrote) until u was
+// visited in this round; returns its stamp, or 0 after giving up.
+__device__ __forceinline__ uint32_t wait_visited(const Sweep &S, uint32_t u) {
+  const uint32_t want = 2u * S.round;
+  uint32_t st = ld_relaxed(S.done + u);
+  if (st >= want) return st;
   const uint64_t t0 = now_ns();
   for (int it = 1;; ++it) {
-    __nanosleep(it < 8 ? 32 : 256);
-    if (ld_acquire(S.done + u) >= S.round) return true;
+    __nanosleep(it < 16 ? 20 : 200);
+    st = ld_relaxed(S.done + u);
+    if (st >= want) return st;
     if ((it & 15) == 0) {
+      if (*(volatile int *)S.err != 0) return 0;
+      if (now_ns() - t0 > kWaitNs) {
+        atomicCAS(S.err, 0, RBG_ERR_TIMEOUT);
+        return 0;
+      }
+    }
+  }
+}
+
+// Fast path of a node with d <= kTabMaxDeg arcs whose labels are staged in su
+// (and quantities in sw): the table accumulation of decide(), then label
+// scores as intervals (lpa_interval), exact evaluation only where intervals
+// leave the choice open (rb_cluster.cpp:532-553): the labels that can still be
+// the best (upper end at or above the largest lower end) when more than one
+// can, and the current label against the best when the 1e-12 rule is not
+// settled by the intervals.  Same result as decide().
+__device__ uint32_t decide_staged(const Sweep &S, Table &T, const uint32_t *su, const float *sw,
+                                  double *dlo, const double *inv, int d, uint32_t cur,
+                                  bool *touched) {
+  const int lane = threadIdx.x & 31;
+  int nlist = 0;
+  for (int c = 0; c < d; c += 32) {
+    const int i = c + lane;
+    const bool valid = i < d;
+    const uint32_t L = valid ? su[i] : kEmpty;
+    const uint32_t grp = __match_any_sync(FULL, L);
+    const bool lead = valid && lane == __ffs(grp) - 1;
+    bool fresh = false;
+    int slot = 0;
+    if (lead) {
+      slot = table_find(T, L, &fresh);
+      double s = T.score[slot];
+      for (uint32_t g = grp; g; g &= g - 1) lpa_accumulate(S.rule, s, sw[c + __ffs(g) - 1]);
+      T.score[slot] = s;
+      T.cnt[slot] += __popc(grp);
+    }
+    const uint32_t nb = __ballot_sync(FULL, fresh);
+    if (fresh) T.list[nlist + __popc(nb & ((1u << lane) - 1u))] = (uint32_t)slot;
+    nlist += __popc(nb);
+    __syncwarp();
+  }
+  *touched = nlist > 0;
+  if (nlist == 0) return cur;
+  double *dhi = dlo + kTabMaxDeg;                         // the stage, now free
+  double M = -INFINITY;
+  int ci = -1;
+  for (int i = lane; i < nlist; i += 32) {
+    const int s = (int)T.list[i];
+    double l, h;
+    lpa_interval(S.rule, T.cnt[s], T.score[s], inv, &l, &h);
+    dlo[i] = l;
+    dhi[i] = h;
+    M = fmax(M, l);
+    if (T.key[s] == cur) ci = i;
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) M = fmax(M, __shfl_xor_sync(FULL, M, o));
+  ci = __reduce_max_sync(FULL, (unsigned)(ci + 1)) - 1;   // list index of the current label
+  __syncwarp();
+  int nc = 0, first = 0x7FFFFFFF;
+  for (int i = lane; i < nlist; i += 32)
+    if (dhi[i] >= M) {
+      ++nc;
+      first = min(first, i);
+    }
+  nc = (int)__reduce_add_sync(FULL, (unsigned)nc);
+  int bi;
+  if (nc == 1) {
+    bi = (int)__reduce_min_sync(FULL, (unsigned)first);
+  } else {
+    double bv = -INFINITY;
+    int b = 0x7FFFFFFF;
+    for (int i = lane; i < nlist; i += 32) {
+      if (!(dhi[i] >= M)) continue;
+      double v = dlo[i];
+      if (v != dhi[i]) {
+        const int s = (int)T.list[i];
+        v = lpa_combine(S.rule, T.cnt[s], T.score[s]);
+        dlo[i] = dhi[i] = v;
+      }
+      if (v > bv || (v == bv && i < b)) {
+        bv = v;
+        b = i;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+      const double ov = __shfl_xor_sync(FULL, bv, o);
+      const int ob = __shfl_xor_sync(FULL, b, o);
+      if (ov > bv || (ov == bv && ob < b)) {
+        bv = ov;
+        b = ob;
+      }
+    }
+    bi = b;
+  }
+  __syncwarp();
+  uint32_t bk = T.key[T.list[bi]];
+  if (ci >= 0 && bk != cur) {
+    // keep cur when cv >= RN(bv - 1e-12); decided by the intervals when they allow
+    double blo = dlo[bi], bhi = dhi[bi], clo = dlo[ci], chi = dhi[ci];
+    bool keep;
+    if (clo >= dd::sub(bhi, 1e-12)) {
+      keep = true;
+    } else if (chi < dd::sub(blo, 1e-12)) {
+      keep = false;
+    } else {
+      if (blo != bhi) blo = lpa_combine(S.rule, T.cnt[T.list[bi]], T.score[T.list[bi]]);
+      if (clo != chi) clo = lpa_combine(S.rule, T.cnt[T.list[ci]], T.score[T.list[ci]]);
+      keep = clo >= dd::sub(blo, 1e-12);
+    }
+    if (keep) bk = cur;
+  }
+  __syncwarp();
+  for (int i = lane; i < nlist; i += 32) T.key[T.list[i]] = kEmpty;   // reset for the next node
+  __syncwarp();
+  return bk;
+}
+
+// Stages v's arcs (neighbour ids into su, quantities into sw) and, in the
+// Gauss-Seidel sweep, waits (bounded) until every earlier neighbour has been
+// visited in this round, polling all their stamps at once.  *chg: some earlier
+// neighbour of this lane's arcs changed its label in this round.  Returns
+// false after a wait gave up.  The caller fences before reading labels.
+__device__ bool stage_and_wait(const Sweep &S, uint32_t *su, float *sw, int64_t a0, int d,
+                               bool wait, bool *chg) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t want = 2u * S.round;
+  uint32_t pend = 0;
+  *chg = false;
+#pragma unroll
+  for (int j = 0; j < kTabMaxDeg / 32; ++j) {
+    const int i = lane + 32 * j;
+    if (i < d) {
+      const uint32_t u = __ldg(S.nbr + a0 + i);
+      su[i] = u;
+      sw[i] = __ldg(S.w + a0 + i);
+      if (wait && __ldg(S.early + a0 + i)) pend |= 1u << j;
+    }
+  }
+  if (!wait || __reduce_or_sync(FULL, pend) == 0) return true;
+  uint64_t t0 = 0;
+  bool changed = false;
+  for (int it = 0; pend; ++it) {
+#pragma unroll
+    for (int j = 0; j < kTabMaxDeg / 32; ++j)
+      if ((pend >> j) & 1u) {
+        const uint32_t st = ld_relaxed(S.done + su[lane + 32 * j]);
+        if (st >= want) {
+          pend &= ~(1u << j);
+          changed |= st == want + 1u;
+        }
+      }
+    if (!pend) break;
+    if (it == 0) t0 = now_ns();
+    __nanosleep(it < 16 ? 20 : 200);
+    if ((it & 15) == 15) {
       if (*(volatile int *)S.err != 0) return false;
       if (now_ns() - t0 > kWaitNs) {
         atomicCAS(S.err, 0, RBG_ERR_TIMEOUT);
@@ -521,47 +784,146 @@ __device__ __forceinline__ bool wait_visited(const Sweep &S, uint32_t u) {
       }
     }
   }
+  *chg = changed;
+  return true;
 }
 
 // One Gauss-Seidel round (rb_cluster.cpp:611-714).
+//
+// Activity.  In the reference a node is active when a neighbour changed since
+// its last visit.  Here that is split by when the change happened: changes of
+// later neighbours in the previous round (after this node's visit there) are
+// marks in `active`, written during the previous round into what is now read,
+// and changes of earlier neighbours in this round are the change bits of their
+// stamps.  No flag is written while it can be read, so nothing races.
+// An inactive node writes nothing; it only publishes its stamp.
 __global__ void __launch_bounds__(kLpaWarps * 32) k_lpa_gs_round(const Sweep S) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31;
   const int gwarp = blockIdx.x * kLpaWarps + (threadIdx.x >> 5);
   clear_tables(S, smem, gwarp);
   float *wb = warp_wbuf(smem);
+  uint32_t *su = warp_stage_u(smem);
+  float *sw = warp_stage_w(smem);
+  double *sd = warp_stage_d(smem);
+  const double *inv = cta_inv(smem);
+  const uint32_t want = 2u * S.round;
+  constexpr int J = kTabMaxDeg / 32;
   for (;;) {
     uint32_t p = 0;
     if (lane == 0) p = atomicAdd(S.claim, 1u);
     p = __shfl_sync(FULL, p, 0);
     if ((int64_t)p >= S.n) break;
-    const uint32_t v = __ldg(S.order + p);
-    const int64_t a0 = __ldg(S.off + v), a1 = __ldg(S.off + v + 1);
-    bool ok = true;
-    for (int64_t a = a0 + lane; a < a1; a += 32) {
-      const uint32_t u = __ldg(S.nbr + a);
-      if (__ldg(S.pos + u) < p) ok = ok && wait_visited(S, u);
+    const uint4 r = __ldg(S.rec + p);
+    const uint32_t v = r.x;
+    const int64_t d = r.y, a0 = (int64_t)r.z | ((int64_t)r.w << 32), a1 = a0 + d;
+    const bool marked = ld_cg8(S.active + v) != 0;          // written in the previous round
+    bool ok = true, chg = false, changed = false;
+    const uint32_t cur = ld_cg(S.label + v);
+    if (d <= kTabMaxDeg) {
+      // stage the arcs and poll the earlier neighbours once
+      uint32_t uid[J];
+      uint32_t pend = 0;
+#pragma unroll
+      for (int j = 0; j < J; ++j) {
+        const int i = lane + 32 * j;
+        uid[j] = 0;
+        if (i < d) {
+          uid[j] = __ldg(S.nbr + a0 + i);
+          sw[i] = __ldg(S.w + a0 + i);
+          if (__ldg(S.early + a0 + i)) pend |= 1u << j;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < J; ++j) {
+        const int i = lane + 32 * j;
+        if ((pend >> j) & 1u) {
+          const uint32_t st = ld_relaxed(S.done + uid[j]);
+          if (st >= want) {
+            pend &= ~(1u << j);
+            chg |= st == want + 1u;
+          }
+        }
+      }
+      bool touched = false;
+      uint32_t best = cur;
+      Table T = warp_table(S, smem, d, gwarp);
+      // the remaining waits (bounded)
+      uint64_t t0 = 0;
+      for (int it = 0; pend && ok; ++it) {
+        if (it == 0) t0 = now_ns();
+        __nanosleep(it < 16 ? 20 : 200);
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+          if ((pend >> j) & 1u) {
+            const uint32_t st = ld_relaxed(S.done + uid[j]);
+            if (st >= want) {
+              pend &= ~(1u << j);
+              chg |= st == want + 1u;
+            }
+          }
+        if (pend && (it & 15) == 15) {
+          if (*(volatile int *)S.err != 0) ok = false;
+          else if (now_ns() - t0 > kWaitNs) {
+            atomicCAS(S.err, 0, RBG_ERR_TIMEOUT);
+            ok = false;
+          }
+        }
+      }
+      if (!__all_sync(FULL, ok)) {
+        if (lane == 0) st_release(S.done + v, want);
+        break;
+      }
+      const bool anychg = __any_sync(FULL, chg);
+      if ((marked || anychg) && d > 0) {
+        // the labels after the waits: an earlier neighbour that changed wrote its
+        // label before its stamp (acquired by the fence); the others did not move
+        if (anychg) fence_acq_rel();
+#pragma unroll
+        for (int j = 0; j < J; ++j) {
+          const int i = lane + 32 * j;
+          if (i < d) su[i] = ld_relaxed(S.label + uid[j]);
+        }
+        __syncwarp();
+        best = decide_staged(S, T, su, sw, sd, inv, (int)d, cur, &touched);
+        if (touched && best != cur && !ld_cg8(S.frozen + v)) {
+          commit(S, v, cur, best, a0, a1, true);
+          changed = true;
+        }
+      }
+      __syncwarp();
+      if (lane == 0) {
+        if (marked || anychg) st_release(S.done + v, want + (changed ? 1u : 0u));
+        else st_relaxed(S.done + v, want);
+      }
+      continue;
     }
-    // each lane reads the flag after its own acquires; any lane that saw a mark counts
-    const bool act = __any_sync(FULL, ld_relaxed_u8(S.active + v) != 0);
+    // general path (more arcs than the stage holds): wait, then decide
+    for (int64_t a = a0 + lane; a < a1 && ok; a += 32)
+      if (__ldg(S.early + a)) {
+        const uint32_t st = wait_visited(S, __ldg(S.nbr + a));
+        ok = st != 0;
+        chg |= st == want + 1u;
+      }
     if (!__all_sync(FULL, ok)) {
-      if (lane == 0) st_release(S.done + v, S.round);
+      if (lane == 0) st_release(S.done + v, want);
       break;
     }
+    const bool act = __any_sync(FULL, marked || chg);
     if (act) {
-      if (lane == 0) st_relaxed_u8(S.active + v, 0u);    // consumed
-      const uint32_t cur = S.label[v];
-      if (a1 > a0) {
-        Table T = warp_table(S, smem, a1 - a0, gwarp);
-        bool touched = false;
-        const uint32_t best = decide(S, T, wb, v, a0, a1, cur, &touched);
-        if (touched && best != cur && !S.frozen[v]) commit(S, v, cur, best, a0, a1, S.active);
+      fence_acq_rel();
+      Table T = warp_table(S, smem, d, gwarp);
+      bool touched = false;
+      const uint32_t best = decide(S, T, wb, v, a0, a1, cur, &touched);
+      if (touched && best != cur && !ld_cg8(S.frozen + v)) {
+        commit(S, v, cur, best, a0, a1, true);
+        changed = true;
       }
     }
     __syncwarp();
     if (lane == 0) {
-      __threadfence();
-      st_release(S.done + v, S.round);
+      if (act) st_release(S.done + v, want + (changed ? 1u : 0u));
+      else st_relaxed(S.done + v, want);
     }
   }
 }
@@ -573,15 +935,32 @@ __global__ void __launch_bounds__(kLpaWarps * 32) k_lpa_sync_propose(const Sweep
   const int gwarp = blockIdx.x * kLpaWarps + (threadIdx.x >> 5);
   clear_tables(S, smem, gwarp);
   float *wb = warp_wbuf(smem);
+  uint32_t *su = warp_stage_u(smem);
+  float *sw = warp_stage_w(smem);
+  const double *inv = cta_inv(smem);
   const int64_t nw = (int64_t)gridDim.x * kLpaWarps;
   for (int64_t v = gwarp; v < S.n; v += nw) {
     uint32_t prop = kEmpty;
     const int64_t a0 = __ldg(S.off + v), a1 = __ldg(S.off + v + 1);
-    if (S.active[v] && a1 > a0) {
+    if (ld_cg8(S.active + v) && a1 > a0) {
       Table T = warp_table(S, smem, a1 - a0, gwarp);
       bool touched = false;
-      const uint32_t cur = S.label[v];
-      const uint32_t best = decide(S, T, wb, (uint32_t)v, a0, a1, cur, &touched);
+      const uint32_t cur = ld_cg(S.label + v);
+      uint32_t best;
+      if (a1 - a0 <= kTabMaxDeg) {
+        const int d = (int)(a1 - a0);
+        bool chg = false;
+        stage_and_wait(S, su, sw, a0, d, false, &chg);
+#pragma unroll
+        for (int j = 0; j < kTabMaxDeg / 32; ++j) {
+          const int i = lane + 32 * j;
+          if (i < d) su[i] = ld_cg(S.label + su[i]);
+        }
+        __syncwarp();
+        best = decide_staged(S, T, su, sw, warp_stage_d(smem), inv, d, cur, &touched);
+      } else {
+        best = decide(S, T, wb, (uint32_t)v, a0, a1, cur, &touched);
+      }
       if (touched) prop = best;
     }
     if (lane == 0) S.prop[v] = prop;
@@ -593,11 +972,11 @@ __global__ void __launch_bounds__(kLpaWarps * 32) k_lpa_sync_commit(const Sweep 
   const int gwarp = blockIdx.x * kLpaWarps + (threadIdx.x >> 5);
   const int64_t nw = (int64_t)gridDim.x * kLpaWarps;
   for (int64_t v = gwarp; v < S.n; v += nw) {
-    const uint32_t best = S.prop[v];
+    const uint32_t best = ld_cg(S.prop + v);
     if (best == kEmpty) continue;
-    const uint32_t kprev = S.label[v];
-    if (kprev != best && !S.frozen[v])
-      commit(S, (uint32_t)v, kprev, best, __ldg(S.off + v), __ldg(S.off + v + 1), S.next_active);
+    const uint32_t kprev = ld_cg(S.label + v);
+    if (kprev != best && !ld_cg8(S.frozen + v))
+      commit(S, (uint32_t)v, kprev, best, __ldg(S.off + v), __ldg(S.off + v + 1), false);
   }
 }
 
@@ -643,6 +1022,13 @@ void launch_lpa_init(const uint32_t *order, int64_t n, uint32_t *pos, uint32_t *
                                               done, vcnt, vnext);
 }
 
+void launch_lpa_early(const int64_t *off, const uint32_t *nbr, const uint32_t *pos, int64_t n,
+                      uint8_t *early, uint4 *rec, cudaStream_t s) {
+  if (n == 0) return;
+  const int64_t blocks = std::min<int64_t>((n + 7) / 8, 148 * 16);
+  k_lpa_early<<<(unsigned)blocks, 256, 0, s>>>(off, nbr, pos, n, early, rec);
+}
+
 int lpa_sweep_warps(int sms) {
   static const int occ = [] {                         // once per process (thread-safe init)
     cudaFuncSetAttribute((const void *)k_lpa_gs_round, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -668,6 +1054,8 @@ void launch_lpa_round(const LpaSweepArgs &a, int sync, int warps, cudaStream_t s
   S.w = a.w;
   S.order = a.order;
   S.pos = a.pos;
+  S.early = a.early;
+  S.rec = a.rec;
   S.label = a.label;
   S.active = a.active;
   S.next_active = a.next_active;

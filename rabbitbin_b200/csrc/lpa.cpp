@@ -10,6 +10,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <numeric>
@@ -180,10 +182,19 @@ void propagate(rbg_ctx *c, const rbg_lpa_params *lp, int64_t n, const EdgeView &
     CK(cudaMemsetAsync(misc + 5, 0, 4, s));
     launch_lpa_init(a.order, n, B.pos.as<uint32_t>(), a.label, act, nxt, a.frozen, a.done, a.vcnt,
                     a.vnext, s);
+    if (attempt == 0) {
+      B.early.ensure(a1);
+      B.rec.ensure(n1 * 16);
+      launch_lpa_early(a.off, a.nbr, a.pos, n, B.early.as<uint8_t>(), B.rec.as<uint4>(), s);
+      a.early = B.early.as<uint8_t>();
+      a.rec = B.rec.as<uint4>();
+    }
     st.rounds = 0;
     st.changes = 0;
     st.frozen = 0;
     bool pool_out = false;
+    const bool trace = getenv("RB_LPA_TRACE") != nullptr;
+    auto tr0 = std::chrono::steady_clock::now();
     for (uint32_t round = 1;; ++round) {
       if (lp->max_rounds > 0 && (int)round > lp->max_rounds)
         throw Error(RBG_ERR_TIMEOUT, "label propagation did not converge within max_rounds");
@@ -192,7 +203,7 @@ void propagate(rbg_ctx *c, const rbg_lpa_params *lp, int64_t n, const EdgeView &
       a.next_active = nxt;
       CK(cudaMemsetAsync(misc + 4, 0, 4, s));
       CK(cudaMemsetAsync(misc + 8, 0, 16, s));
-      if (lp->synchronous) CK(cudaMemsetAsync(nxt, 0, (size_t)n, s));
+      CK(cudaMemsetAsync(nxt, 0, (size_t)n, s));            // marks for the next round
       launch_lpa_round(a, lp->synchronous, warps, s);
       CK(cudaGetLastError());
       CK(cudaMemcpyAsync((void *)pin, misc, 64, cudaMemcpyDeviceToHost, s));
@@ -200,6 +211,12 @@ void propagate(rbg_ctx *c, const rbg_lpa_params *lp, int64_t n, const EdgeView &
       st.rounds = (int)round;
       unsigned long long cnt[2];
       std::memcpy(cnt, (const char *)pin + 32, 16);
+      if (trace) {                                   // RB_LPA_TRACE, rb_cluster.cpp:711-713
+        const auto t1 = std::chrono::steady_clock::now();
+        fprintf(stderr, "[LPA] round=%u changed=%llu frozen=%llu ms=%.3f\n", round, cnt[0], cnt[1],
+                std::chrono::duration<double, std::milli>(t1 - tr0).count());
+        tr0 = t1;
+      }
       st.changes += (int64_t)cnt[0];
       st.frozen += (int64_t)cnt[1];
       const int err = pin[1];
@@ -211,7 +228,7 @@ void propagate(rbg_ctx *c, const rbg_lpa_params *lp, int64_t n, const EdgeView &
         throw Error(RBG_ERR_TIMEOUT, "label propagation: a bounded wait for an earlier node ran out");
       if (err != 0) throw Error(RBG_ERR_CUDA, "label propagation: device error");
       if (cnt[0] == 0) break;
-      if (lp->synchronous) std::swap(act, nxt);
+      std::swap(act, nxt);
     }
     if (!pool_out) break;
     if (attempt >= 4) throw Error(RBG_ERR_NOMEM, "label propagation: visited sets outgrew their pool");

@@ -467,6 +467,8 @@ struct LpaSweepArgs {
   const uint32_t *nbr = nullptr;
   const float *w = nullptr;
   const uint32_t *order = nullptr, *pos = nullptr;
+  const uint8_t *early = nullptr;         // per arc: neighbour earlier in the order
+  const uint4 *rec = nullptr;             // per position: node, degree, first arc
   uint32_t *label = nullptr;
   uint8_t *active = nullptr, *next_active = nullptr, *frozen = nullptr;
   uint32_t *done = nullptr, *prop = nullptr;
@@ -480,6 +482,10 @@ struct LpaSweepArgs {
   uint32_t round = 0;
   int *err = nullptr;
 };
+// Per arc: the neighbour precedes the node in the order; per position: node,
+// degree, first arc (low, high word).
+void launch_lpa_early(const int64_t *off, const uint32_t *nbr, const uint32_t *pos, int64_t n,
+                      uint8_t *early, uint4 *rec, cudaStream_t s);
 // Warps of one sweep launch (a multiple of the CTA's 8).
 int lpa_sweep_warps(int sms);
 int lpa_table_max_deg();
