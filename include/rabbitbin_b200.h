@@ -308,7 +308,8 @@ int rbg_bin_batch(rbg_ctx *ctx, const rbg_params *defaults, const rbg_assembly *
  * small ones when no large one waits, the other lanes serve small requests
  * only.  A lane that becomes free folds every queued request of its class
  * that fits into the HBM budget the running batches leave (a batch's share is
- * released when it finishes) into one rbg_bin_batch call.  Requests that
+ * released when it finishes) into one batch: small requests through one
+ * rbg_bin_batch call, large ones through rbg_bin_graph each.  Requests that
  * arrive while others are on the GPU are therefore admitted as soon as a lane
  * of their class and the memory are free, small requests never wait behind a
  * large batch, and the lanes' batches overlap on the device.  Each result

@@ -9,7 +9,8 @@
 // already running (admission against a global budget; a batch's reservation
 // is released the moment it finishes, and the lanes waiting for memory are
 // woken), up to max_batch requests and max_batch_pairs pairs, and runs them as
-// one rbg_bin_batch call.  So a request that arrives while others are on the
+// one call: rbg_bin_graph for each large request, one rbg_bin_batch for the
+// small ones.  So a request that arrives while others are on the
 // GPU is admitted as soon as a lane of its class and the memory are free; a
 // small request never waits behind a large batch, and the lanes' batches
 // overlap on the device (their streams run concurrently).  Inside a batch the
@@ -122,30 +123,49 @@ void rbg_server::worker_loop(int w) {
   }
 }
 
+// Large requests go through rbg_bin_graph one by one (its all-pairs pass over
+// one assembly, behind that assembly's own input copy, is faster than the
+// batch engine's shared kernel for one large assembly), the small ones of the
+// batch through one rbg_bin_batch call.
 void rbg_server::run_batch_of(int w, std::vector<std::shared_ptr<Request>> &take) {
   rbg_ctx *c = ctxs[w];
   const int nb = (int)take.size();
   std::vector<rbg_graph> outs(nb);
-  int rc;
-  if (cfg.plain) {
-    Request &r = *take[0];
-    rc = rbg_bin_graph(c, &r.p, r.a.seqcat, r.a.offsets, r.a.n, r.a.depth, r.a.S, &outs[0]);
-  } else {
-    std::vector<rbg_assembly> asms(nb);
-    for (int i = 0; i < nb; ++i) {
-      asms[i] = take[i]->a;
-      asms[i].params = &take[i]->p;
+  std::vector<int> rcs(nb, RBG_OK);
+  std::vector<std::string> errs(nb);
+  std::vector<int> small;
+  for (int i = 0; i < nb; ++i) {
+    Request &r = *take[i];
+    if (cfg.plain || r.pairs > cfg.small_pairs) {
+      rcs[i] = rbg_bin_graph(c, &r.p, r.a.seqcat, r.a.offsets, r.a.n, r.a.depth, r.a.S, &outs[i]);
+      if (rcs[i] != RBG_OK) errs[i] = rbg_last_error(c);
+    } else {
+      small.push_back(i);
     }
-    rc = rbg_bin_batch(c, &defaults, asms.data(), nb, outs.data(), nullptr);
+  }
+  if (!small.empty()) {
+    const int ns = (int)small.size();
+    std::vector<rbg_assembly> asms(ns);
+    std::vector<rbg_graph> so(ns);
+    for (int t = 0; t < ns; ++t) {
+      asms[t] = take[small[t]]->a;
+      asms[t].params = &take[small[t]]->p;
+    }
+    const int rc = rbg_bin_batch(c, &defaults, asms.data(), ns, so.data(), nullptr);
+    const std::string e = rc == RBG_OK ? std::string() : std::string(rbg_last_error(c));
+    for (int t = 0; t < ns; ++t) {
+      rcs[small[t]] = rc;
+      errs[small[t]] = e;
+      outs[small[t]] = so[t];
+    }
   }
   std::lock_guard<std::mutex> lk(mu);
-  const std::string e = rc == RBG_OK ? std::string() : std::string(rbg_last_error(c));
   for (int i = 0; i < nb; ++i) {
-    take[i]->status = rc;
-    take[i]->err = e;
-    if (rc == RBG_OK) take[i]->g = outs[i];
+    take[i]->status = rcs[i];
+    take[i]->err = errs[i];
+    if (rcs[i] == RBG_OK) take[i]->g = outs[i];
+    else err = errs[i];
   }
-  if (rc != RBG_OK) err = e;
 }
 
 extern "C" {
