@@ -771,10 +771,97 @@ def run_lpa_form(args):
     print(json.dumps(res))
 
 
+def run_depth_form(args):
+    """BAM -> depth (the step before the path when the bin command gets BAMs):
+    one coordinate-sorted BAM of 150 bp reads over the binning-scale assembly
+    (seeded synthetic reads, mean depth 2x, htslib-style BGZF at deflate level
+    6) through rbg_bam_depth_mem: BGZF bytes in host memory in, the depth
+    matrix back in host memory.  Checked against the reference's own
+    depth_accumulate_sample on the same records; its per-read pass on the host
+    cores (records already decoded, so without its BGZF decoding) is the CPU
+    baseline."""
+    import torch
+    from rabbitbin_b200 import api
+    from rabbitbin_b200.synth import BAM_CLEAN, bam_records, make_bam
+    torch.cuda.set_device(0)
+    asm = _assembly(WORKLOAD["seed"])
+    buf, offs = asm.concat()
+    lens = np.diff(offs).astype(np.uint32)
+    cov = np.asarray(asm.depth[:, 0], np.float64)
+    cov = cov * (2.0 / max(cov.mean(), 1e-9))
+    t0 = time.perf_counter()
+    bam = make_bam(lens, cov, names=[f"contig_{i}" for i in range(asm.n)], seq=buf, seq_off=offs,
+                   seed=7, read_len=150, level=6, **BAM_CLEAN)
+    gen_s = time.perf_counter() - t0
+    ctx = api.Context(0)
+    for _ in range(max(args.warmup, 1)):
+        out = ctx.bam_depth([bam])
+    walls, kern, infl = [], [], []
+    with ClockSampler(0) as clk:
+        for _ in range(args.steps):
+            t1 = time.perf_counter()
+            out = ctx.bam_depth([bam])
+            walls.append((time.perf_counter() - t1) * 1000.0)
+            kern.append(out["kernel_ms"])
+            infl.append(out["inflate_ms"])
+    ms = float(np.median(walls))
+    recs = out["records"]
+    ub = out["decompressed_bytes"]
+    kms = float(np.median(kern))
+    # per-record algorithmic bytes of k_depth_reads: the fixed fields (36), the
+    # CIGAR (4 per op) and the aux fields it walks, plus its 4-byte offset; the
+    # records' sequence, quality and name bytes are never read
+    raw, tl, _ = bam_records(bam)
+    pk = _peaks()[0]
+    res = {
+        "metric": "BAM records summarised/s (reads into per-contig depth)",
+        "value": recs / (ms / 1000.0), "unit": "records/s", "n_gpus": 1, "higher_is_better": True,
+        "form": "depth", "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "dtype": "u8 records, u64 sums, f32 means", "data": "synthetic (seeded reads over the "
+        "binning-scale assembly's contigs)",
+        "config": {"workload": "BAM -> depth: 50,000-contig binning-scale assembly, one BAM of "
+                   f"{recs} 150 bp reads (mean depth 2x), BGZF level 6",
+                   "records": recs, "bam_bytes": len(bam), "decompressed_bytes": ub,
+                   "generation_s": round(gen_s, 2), "inputs_exceed_l2": True},
+        "e2e": {"value": recs / (ms / 1000.0), "unit": "records/s",
+                "h2d_bytes_per_step": int(ub), "d2h_bytes_per_step": int(out["means"].nbytes +
+                                                                         out["sums"].nbytes),
+                "time": "host clock around rbg_bam_depth_mem (BGZF bytes in host memory in, the "
+                        "depth matrix in host memory out)"},
+        "stages_ms": {"inflate_and_walk_ms": float(np.median(infl)), "kernel_ms": kms,
+                      "total_ms": ms},
+        "decompressed_gbs": ub / (ms / 1000.0) / 1e9,
+        "kernel": {"name": "k_depth_reads", "records_per_s": recs / (kms / 1000.0),
+                   "stream_gbs": ub / (kms / 1000.0) / 1e9,
+                   "hbm_peak_gbs": pk.get("hbm_gbs") if pk else None},
+        "gpu_launches": None,
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu_baseline:
+        import oracle
+        if oracle.ref_depth() is not None:
+            t0 = time.perf_counter()
+            want, avg = oracle.depth_accumulate_ref(raw, tl, 0.97, 75, False, 0,
+                                                    threads=os.cpu_count() or 1)
+            ref_s = time.perf_counter() - t0
+            res["cpu_baseline"] = {
+                "kind": "reference", "cores": os.cpu_count(), "value": recs / ref_s,
+                "unit": "records/s", "sample": "the whole BAM's records, already decoded "
+                "(depth_accumulate_sample: its BGZF decoding is not timed)",
+                "ms": ref_s * 1000.0}
+            edge = min(75, avg // 3)
+            means = oracle.depth_means(want, tl, edge)
+            res["parity"] = {"against": "reference (oracle/_ref)", "avg_read": avg,
+                             "sums_identical": bool(np.array_equal(out["sums"][0], want)),
+                             "means_identical": bool(np.array_equal(out["means"][:, 0],
+                                                                    means[out["tid"]]))}
+    print(json.dumps(res))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--ref-contigs", type=int, default=50000)
@@ -788,10 +875,11 @@ def main():
                     help="serve form: which request loops replay the trace")
     ap.add_argument("--contigs", type=int, default=0, help="profiling: fewer contigs")
     ap.add_argument("--samples", type=int, default=0, help="profiling: other S")
-    ap.add_argument("--form", default="plain", choices=["plain", "batch", "serve", "lpa"],
+    ap.add_argument("--form", default="plain", choices=["plain", "batch", "serve", "lpa", "depth"],
                     help="plain: the binning-scale assembly; batch: a mixed stream per call; "
                          "serve: a Poisson request stream through the request loop; lpa: label "
-                         "propagation on the binning-scale graph")
+                         "propagation on the binning-scale graph; depth: BAM -> depth over "
+                         "the binning-scale assembly")
     ap.add_argument("--batch-size", type=int, default=64, help="batch form: assemblies")
     ap.add_argument("--config", default="binning", choices=["binning", "large"],
                     help="binning: 50,000 contigs, S=20 (default); large: 300,000 contigs, S=30")
@@ -817,6 +905,8 @@ def main():
         run_serve_form(args)
     elif args.form == "lpa":
         run_lpa_form(args)
+    elif args.form == "depth":
+        run_depth_form(args)
     elif args.shard == "rows":
         run_shard_form(args)
     else:

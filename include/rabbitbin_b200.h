@@ -498,6 +498,79 @@ int rbg_label_propagation(rbg_ctx *ctx, const rbg_lpa_params *lp, int64_t n_node
 int rbg_label_propagation_resident(rbg_ctx *ctx, const rbg_lpa_params *lp, uint32_t *membership,
                                    rbg_lpa_stats *stats);
 
+/* ── BAM -> depth: the step before the path when the bin command gets BAMs ──
+ *   rbg_bam_depth ← compute_depth_tsv_inmem with a DepthMatrixOut
+ *                   (src/rabbit_depth_fuse.h:114-123, src/rabbit_depth.cpp:1096-1535),
+ *                   as the bin command calls it (src/rabbitbin.cpp:3806-3811):
+ *                   means only (intraDepthVariance = false), edges excluded
+ *   rbg_depth_accumulate ← depth_accumulate_sample (src/rabbit_depth_fuse.h:72-75,
+ *                   src/rabbit_depth.cpp:1615-1685) on records already in memory
+ * Per read: the filters of src/rabbit_depth.cpp:1656-1667 (mapped, mate on a
+ * known contig when paired, not secondary / QC-fail / duplicate, MAPQ >=
+ * min_map_qual), the end check and clip of src/CheckRead.hpp:82-265, the
+ * covered bases of caldepth (src/rabbit_depth.h:618-887: aligned M/=/X bases
+ * minus the edge bases and the NM-derived substitutions) and the percent
+ * identity of ReadStatistics (:193-346), kept when >= percent_identity.
+ * edge = include_edge_bases ? 0 : min(max_edge_bases, avg_read / 3), avg_read
+ * being the integer mean query length of the first 4,000 mapped records of
+ * that BAM (:787-834).  Mean of (contig, BAM) = sum / (len - 2 edge) for
+ * contigs longer than 2 edge + 1 (else sum / len), 0 for len <= 2, values above
+ * 1e6 set to 0 (:1515-1534).  Rows: the contigs of the first BAM's header with
+ * length >= min_contig_length, in header order; columns: one per BAM, then
+ * with dual_map_qual > 0 a second block of the reads with MAPQ >= dual_map_qual.
+ * Every BAM must carry the same contigs.  Records must be complete and
+ * consistent (block_size, name, CIGAR, sequence and qualities inside the
+ * record): a malformed record or BGZF block returns RBG_ERR_ARG (the reference
+ * stops reading that file there).  CIGARs of more than 65,535 ops (the CG tag)
+ * are taken as stored. */
+typedef struct rbg_depth_params {
+  float percent_identity;       /* --percent-identity / 100 (0.97)                   */
+  int32_t min_contig_length;    /* rows: contigs at least this long (1)              */
+  int32_t max_edge_bases;       /* 75                                                */
+  int32_t include_edge_bases;   /* 0                                                 */
+  int32_t min_map_qual;         /* 0                                                 */
+  int32_t dual_map_qual;        /* 0: off                                            */
+  int32_t threads;              /* host threads inflating BGZF blocks (0: all)       */
+  int32_t chunk_mb;             /* decompressed bytes per device hand-over (64)      */
+} rbg_depth_params;
+
+typedef struct rbg_depth_matrix {
+  int64_t n_rows;               /* kept contigs                                      */
+  int32_t n_cols;               /* BAMs (x 2 with dual_map_qual)                     */
+  int32_t n_targets;            /* contigs in the header                             */
+  int32_t *tid;                 /* [n_rows] header index of each row                 */
+  int32_t *lens;                /* [n_rows]                                          */
+  float *means;                 /* [n_rows][n_cols] row-major                        */
+  char *names;                  /* the rows' names, each NUL-terminated              */
+  int64_t *name_off;            /* [n_rows] offset of each name in `names`           */
+  int32_t *avg_read;            /* [n_bams]                                          */
+  uint64_t *sums;               /* [n_cols][n_targets] depth sums (CountType)        */
+  int64_t records;              /* records read over all BAMs                        */
+  int64_t compressed_bytes;     /* BGZF bytes read                                   */
+  int64_t decompressed_bytes;   /* bytes after inflation                             */
+  float inflate_ms;             /* host time inflating and walking records           */
+  float total_ms;               /* host time of the whole call                       */
+  float kernel_ms;              /* device time of the per-record launches            */
+  int32_t reserved;
+} rbg_depth_matrix;
+
+int rbg_default_depth_params(rbg_depth_params *p);
+/* BAM files by path. */
+int rbg_bam_depth(rbg_ctx *ctx, const char *const *bam_paths, int32_t n_bams,
+                  const rbg_depth_params *p, rbg_depth_matrix *out);
+/* BAM files already in host memory (whole files, BGZF as on disk). */
+int rbg_bam_depth_mem(rbg_ctx *ctx, const uint8_t *const *bam_bytes, const int64_t *bam_sizes,
+                      int32_t n_bams, const rbg_depth_params *p, rbg_depth_matrix *out);
+int rbg_free_depth_matrix(rbg_depth_matrix *m);
+/* One sample's sums from decompressed records (each: block_size, then the
+ * record, back to back) on host memory; depth_out[n_targets] receives the
+ * sums of the reads with MAPQ >= min_map_qual, depth_u_out (may be null) those
+ * with MAPQ >= dual_map_qual; *avg_read the sampled read length. */
+int rbg_depth_accumulate(rbg_ctx *ctx, const uint8_t *records, int64_t n_bytes,
+                         const uint32_t *target_len, int32_t n_targets,
+                         const rbg_depth_params *p, uint64_t *depth_out, uint64_t *depth_u_out,
+                         int32_t *avg_read);
+
 #ifdef __cplusplus
 }
 #endif

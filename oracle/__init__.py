@@ -436,3 +436,55 @@ def ref_cache_read(path):
         else:
             out[name] = bufs[name][:getattr(st, cnt)]
     return out
+
+
+# ── BAM -> depth: the reference's per-read code (librbref_depth.so) ─────────
+def ref_depth():
+    """depth_accumulate_sample and the code under it, compiled from the
+    reference tree (ref_depth_shim.cpp); None when neither built nor buildable."""
+    if "depth" not in _cache:
+        _build.build_ref()
+        path = os.path.join(_HERE, "_ref", "librbref_depth.so")
+        lib = None
+        if os.path.exists(path):
+            lib = C.CDLL(path)
+            f = lib.ref_depth_accumulate
+            f.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_uint32), C.c_int32, C.c_float,
+                          C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint64),
+                          C.POINTER(C.c_int32)]
+            f.restype = C.c_int
+        _cache["depth"] = lib
+    return _cache["depth"]
+
+
+def depth_accumulate_ref(records, target_len, pctid=0.97, max_edge=75, include_edge=False,
+                         min_mapq=0, threads=0):
+    """(sums uint64[n_targets], avg_read) of depth_accumulate_sample
+    (src/rabbit_depth.cpp:1615-1685) over decompressed records."""
+    lib = ref_depth()
+    if lib is None:
+        return None
+    rec = np.frombuffer(bytes(records), np.uint8) if len(records) else np.zeros(1, np.uint8)
+    tl = np.ascontiguousarray(target_len, np.uint32)
+    out = np.zeros(max(len(tl), 1), np.uint64)
+    avg = C.c_int32(0)
+    rc = lib.ref_depth_accumulate(rec.ctypes.data, len(records), _ptr(tl, C.c_uint32), len(tl),
+                                  C.c_float(pctid), int(max_edge), int(bool(include_edge)),
+                                  int(min_mapq), int(threads), _ptr(out, C.c_uint64),
+                                  C.byref(avg))
+    if rc != 0:
+        raise ValueError("malformed records")
+    return out[:len(tl)], int(avg.value)
+
+
+def depth_means(sums, target_len, edge):
+    """Means of src/rabbit_depth.cpp:1515-1534: (float)((double)sum / adj) with
+    adj = len - 2 edge for len > 2 edge + 1 (else len), 0 for adj <= 2, values
+    above 1e6 set to 0."""
+    cl = np.asarray(target_len, np.uint32).astype(np.int32).astype(np.int64)
+    adj = np.where(cl > 2 * edge + 1, cl - 2 * edge, cl)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        m = (np.asarray(sums, np.uint64).astype(np.float64) / np.where(adj > 2, adj, 1)).astype(np.float32)
+    m = np.where(adj > 2, m, np.float32(0))
+    m[m > np.float32(1000000.0)] = 0
+    return m.astype(np.float32)

@@ -51,6 +51,14 @@ FRAGMENTS = [
     ("frag_lpa.inc", "impl/rb_cluster.cpp", 336, 740),
     ("frag_incidence.inc", "rabbitbin.cpp", 5600, 5622),
     ("frag_node_order.inc", "rabbitbin.cpp", 5643, 5645),
+    ("frag_bam_chooser.inc", "BamUtils.h", 275, 318),
+    ("frag_checkread.inc", "CheckRead.hpp", 20, 276),
+    ("frag_thread_blocker.inc", "rabbit_depth.h", 48, 66),
+    ("frag_depth_counts.inc", "rabbit_depth.h", 70, 162),
+    ("frag_read_stats.inc", "rabbit_depth.h", 181, 376),
+    ("frag_caldepth.inc", "rabbit_depth.h", 601, 887),
+    ("frag_depth_column.inc", "rabbit_depth_fuse.h", 65, 68),
+    ("frag_depth_accumulate.inc", "rabbit_depth.cpp", 1615, 1685),
 ]
 
 
@@ -101,10 +109,18 @@ def build_ref():
     shim = os.path.join(HERE, "ref_shim.cpp")
     cache_shim = os.path.join(HERE, "ref_cache_shim.cpp")
     lpa_shim = os.path.join(HERE, "ref_lpa_shim.cpp")
-    deps = [shim, cache_shim, lpa_shim, __file__, os.path.join(REF_SRC, "probmh.cpp")]
+    depth_shim = os.path.join(HERE, "ref_depth_shim.cpp")
+    deps = [shim, cache_shim, lpa_shim, depth_shim, os.path.join(HERE, "htslib_shim.h"), __file__,
+            os.path.join(REF_SRC, "probmh.cpp")]
     if _stale(out, deps):
         _run(["g++"] + FLAGS + ["-I", frag_dir, "-I", REF_SRC, shim, cache_shim, lpa_shim,
                                 os.path.join(REF_SRC, "probmh.cpp"), "-o", out])
+    # the depth harness includes the reference's BamUtils.h fragments against the
+    # htslib stand-in; it is a separate library so that those headers' names do
+    # not meet the graph harness's
+    dout = os.path.join(out_dir, "librbref_depth.so")
+    if _stale(dout, deps):
+        _run(["g++"] + FLAGS + ["-I", frag_dir, "-I", HERE, depth_shim, "-o", dout])
     return out
 
 

@@ -241,6 +241,24 @@ class LpaStats(C.Structure):
 LPA_RULES = {"fisher": 0, "tail": 1, "logsum": 2, "sum": 3, "mean": 4, "max": 5}
 
 
+class DepthParams(C.Structure):
+    _fields_ = [("percent_identity", C.c_float), ("min_contig_length", C.c_int32),
+                ("max_edge_bases", C.c_int32), ("include_edge_bases", C.c_int32),
+                ("min_map_qual", C.c_int32), ("dual_map_qual", C.c_int32),
+                ("threads", C.c_int32), ("chunk_mb", C.c_int32)]
+
+
+class DepthMatrix(C.Structure):
+    _fields_ = [("n_rows", C.c_int64), ("n_cols", C.c_int32), ("n_targets", C.c_int32),
+                ("tid", C.POINTER(C.c_int32)), ("lens", C.POINTER(C.c_int32)),
+                ("means", C.POINTER(C.c_float)), ("names", C.c_void_p),
+                ("name_off", C.POINTER(C.c_int64)), ("avg_read", C.POINTER(C.c_int32)),
+                ("sums", C.POINTER(C.c_uint64)), ("records", C.c_int64),
+                ("compressed_bytes", C.c_int64), ("decompressed_bytes", C.c_int64),
+                ("inflate_ms", C.c_float), ("total_ms", C.c_float), ("kernel_ms", C.c_float),
+                ("reserved", C.c_int32)]
+
+
 class Shard(C.Structure):
     _fields_ = [("rank", C.c_int32), ("world", C.c_int32), ("device_buffers", C.c_int32),
                 ("reserved", C.c_int32), ("allgather", ALLGATHER_FN), ("user", C.c_void_p)]
@@ -310,6 +328,14 @@ def lib():
                                   C.c_int),
         "rbg_label_propagation_resident": ([vp, P(LpaParams), P(C.c_uint32), P(LpaStats)],
                                            C.c_int),
+        "rbg_default_depth_params": ([P(DepthParams)], C.c_int),
+        "rbg_bam_depth": ([vp, P(C.c_char_p), C.c_int32, P(DepthParams), P(DepthMatrix)], C.c_int),
+        "rbg_bam_depth_mem": ([vp, P(C.c_void_p), i64p, C.c_int32, P(DepthParams),
+                               P(DepthMatrix)], C.c_int),
+        "rbg_free_depth_matrix": ([P(DepthMatrix)], C.c_int),
+        "rbg_depth_accumulate": ([vp, C.c_void_p, C.c_int64, P(C.c_uint32), C.c_int32,
+                                  P(DepthParams), P(C.c_uint64), P(C.c_uint64), P(C.c_int32)],
+                                 C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -323,6 +349,15 @@ def exported_symbols():
     hdr = os.path.join(os.path.dirname(_HERE), "include", "rabbitbin_b200.h")
     import re
     return sorted(set(re.findall(r"\b(rbg_[a-z0-9_]+)\s*\(", open(hdr).read())))
+
+
+def default_depth_params(**kw):
+    """rbg_default_depth_params with fields overridden by keyword."""
+    p = DepthParams()
+    lib().rbg_default_depth_params(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
 
 
 def default_params(**kw):
@@ -604,6 +639,65 @@ class Context:
             "label_propagation_resident")
         del order
         return out, st.as_dict()
+
+    def bam_depth(self, bams, **kw):
+        """Depth matrix of BAM files (rbg_bam_depth_mem for bytes, rbg_bam_depth
+        for paths): dict with names, lens, tid, means [rows, cols], sums
+        [cols, n_targets], avg_read, records and timings.  Keywords set
+        rbg_depth_params fields."""
+        p = default_depth_params(**kw)
+        m = DepthMatrix()
+        n = len(bams)
+        if all(isinstance(b, (bytes, bytearray)) for b in bams):
+            keep = [C.create_string_buffer(bytes(b), len(b)) for b in bams]
+            ptrs = (C.c_void_p * n)(*[C.cast(k, C.c_void_p) for k in keep])
+            sizes = np.asarray([len(b) for b in bams], np.int64)
+            rc = self._L.rbg_bam_depth_mem(self._h, ptrs, _p(sizes, C.c_int64), n, C.byref(p),
+                                           C.byref(m))
+        else:
+            keep = [os.fsencode(b) for b in bams]
+            ptrs = (C.c_char_p * n)(*keep)
+            rc = self._L.rbg_bam_depth(self._h, ptrs, n, C.byref(p), C.byref(m))
+        self._check(rc, "bam_depth")
+        try:
+            nr, nc, nt = int(m.n_rows), int(m.n_cols), int(m.n_targets)
+            names = []
+            if nr:
+                off = np.ctypeslib.as_array(m.name_off, (nr,)).copy()
+                for o in off:
+                    names.append(C.string_at(m.names + int(o)).decode())
+            out = {
+                "names": names,
+                "tid": np.ctypeslib.as_array(m.tid, (nr,)).copy() if nr else np.zeros(0, np.int32),
+                "lens": np.ctypeslib.as_array(m.lens, (nr,)).copy() if nr else np.zeros(0, np.int32),
+                "means": (np.ctypeslib.as_array(m.means, (nr * nc,)).reshape(nr, nc).copy()
+                          if nr * nc else np.zeros((nr, nc), np.float32)),
+                "sums": (np.ctypeslib.as_array(m.sums, (nc * nt,)).reshape(nc, nt).copy()
+                         if nc * nt else np.zeros((nc, nt), np.uint64)),
+                "avg_read": np.ctypeslib.as_array(m.avg_read, (n,)).copy(),
+                "records": int(m.records), "compressed_bytes": int(m.compressed_bytes),
+                "decompressed_bytes": int(m.decompressed_bytes),
+                "inflate_ms": float(m.inflate_ms), "total_ms": float(m.total_ms),
+                "kernel_ms": float(m.kernel_ms),
+            }
+        finally:
+            self._L.rbg_free_depth_matrix(C.byref(m))
+        return out
+
+    def depth_accumulate(self, records, target_len, **kw):
+        """One sample's depth sums from decompressed records
+        (rbg_depth_accumulate): (sums, sums with MAPQ >= dual_map_qual, avg_read)."""
+        p = default_depth_params(**kw)
+        rec = np.frombuffer(bytes(records), np.uint8) if len(records) else np.zeros(1, np.uint8)
+        tl = np.ascontiguousarray(target_len, np.uint32)
+        nt = len(tl)
+        d = np.zeros(max(nt, 1), np.uint64)
+        du = np.zeros(max(nt, 1), np.uint64)
+        avg = C.c_int32(0)
+        self._check(self._L.rbg_depth_accumulate(
+            self._h, rec.ctypes.data, len(records), _p(tl, C.c_uint32), nt, C.byref(p),
+            _p(d, C.c_uint64), _p(du, C.c_uint64), C.byref(avg)), "depth_accumulate")
+        return d[:nt], du[:nt], int(avg.value)
 
     def parse_fasta(self, data, min_contig=2500, min_small_contig=1000):
         """Device FASTA parse (rbg_parse_fasta) of the bytes `data`:

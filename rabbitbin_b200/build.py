@@ -21,10 +21,11 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SRCS = ["kernels_sketch.cu", "kernels_graph.cu", "kernels_allpairs.cu", "kernels_onehot.cu",
            "kernels_onehot_mma.cu", "kernels_sym_tc5.cu", "kernels_pmh_query.cu", "kernels_index.cu",
            "kernels_util.cu",
-           "noalloc.cu", "kernels_fasta.cu", "kernels_lpa.cu"]
+           "noalloc.cu", "kernels_fasta.cu", "kernels_lpa.cu", "kernels_depth.cu"]
 CPP_SRCS = ["pmh_streams.cpp", "calib.cpp", "engine.cpp", "batch.cpp", "server.cpp", "fasta.cpp",
-            "cache.cpp", "host_pack.cpp", "lpa.cpp"]
+            "cache.cpp", "host_pack.cpp", "lpa.cpp", "bam.cpp"]
 HEADERS = ["rbg_internal.h", "engine_internal.h", "select_topk.cuh", "tc05.cuh", "ddmath.cuh",
+           "depth_record.cuh",
            "../../include/rabbitbin_b200.h", "gen_zig_tables.py"]
 
 
@@ -74,17 +75,17 @@ def build(verbose=False, ptxas_info=False):
         tmp = OUT + ".tmp"
         lib64 = os.path.join(CUDA, "lib64")
         _run([NVCC] + ARCH + ["-shared", "-o", tmp] + objs +
-             ["-cudart", "static", "-L" + lib64, "-Xlinker", "-rpath=" + lib64])
+             ["-cudart", "static", "-L" + lib64, "-Xlinker", "-rpath=" + lib64, "-lz"])
         shutil.move(tmp, OUT)
     return OUT
 
 
 def build_synth():
-    """The synthetic-assembly chain generator (host C, OpenMP)."""
-    src = os.path.join(CSRC, "synth_chain.c")
+    """The synthetic-assembly chain and BAM generators (host C, OpenMP)."""
+    srcs = [os.path.join(CSRC, "synth_chain.c"), os.path.join(CSRC, "synth_bam.c")]
     out = os.path.join(HERE, "libsynth_chain.so")
-    if _newer(out, [src]):
-        _run(["gcc", "-O3", "-fopenmp", "-fPIC", "-shared", src, "-o", out])
+    if _newer(out, srcs):
+        _run(["gcc", "-O3", "-fopenmp", "-fPIC", "-shared"] + srcs + ["-o", out, "-lz", "-lm"])
     return out
 
 

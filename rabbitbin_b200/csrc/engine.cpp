@@ -1442,6 +1442,7 @@ int rbg_destroy(rbg_ctx *c) {
   if (c->batch) c->batch->release();
   if (c->fasta) c->fasta->release();
   if (c->lpa) c->lpa->release();
+  if (c->depthb) c->depthb->release();
   c->pin.release();
   c->b0pin.release();
   c->shard_host.release();

@@ -234,6 +234,28 @@ struct LpaBufs {
   }
 };
 
+// BAM -> depth: two hand-over slots (decompressed records and one offset per
+// record, pinned on the host and on the device), the sums, the header's
+// lengths, the kept rows, each column's edge and the means.
+struct DepthBufs {
+  DBuf buf[2], off[2], sums, tlen, kept, edge, means;
+  HBuf slot[2], offp[2];
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  cudaEvent_t k0[2] = {nullptr, nullptr}, k1[2] = {nullptr, nullptr};   // per-record launch times
+  void release() {
+    DBuf *all[] = {&buf[0], &buf[1], &off[0], &off[1], &sums, &tlen, &kept, &edge, &means};
+    for (DBuf *b : all) b->release();
+    for (int i = 0; i < 2; ++i) {
+      slot[i].release();
+      offp[i].release();
+      if (ev[i]) cudaEventDestroy(ev[i]);
+      if (k0[i]) cudaEventDestroy(k0[i]);
+      if (k1[i]) cudaEventDestroy(k1[i]);
+      ev[i] = k0[i] = k1[i] = nullptr;
+    }
+  }
+};
+
 // Counts of one parse; the outputs are in FastaBufs: slot 0 large, 1 small
 // (seq: sequences back to back, seq_off: n+1 offsets, name_start / name_len:
 // name ranges in the input).
@@ -372,6 +394,8 @@ struct rbg_ctx {
   std::unique_ptr<rbg::FastaBufs> fasta;
   // label propagation
   std::unique_ptr<rbg::LpaBufs> lpa;
+  // BAM -> depth
+  std::unique_ptr<rbg::DepthBufs> depthb;
 };
 
 namespace rbg {

@@ -201,3 +201,86 @@ def write_depth(asm: Assembly, path: str):
                 v = float(asm.depth[i, k])
                 row += [f"{v:.6g}", f"{v:.6g}"]
             f.write("\t".join(row) + "\n")
+
+
+# ── synthetic BAM files (depth summariser) ─────────────────────────────────
+_BAM_OPT_FIELDS = [("seed", "u64"), ("read_len", "i32"), ("level", "i32"), ("straddle", "i32"),
+                   ("n_unmapped_tail", "i32"),
+                   ("p_indel", "f64"), ("p_soft", "f64"), ("p_overhang", "f64"),
+                   ("p_secondary", "f64"), ("p_dup", "f64"), ("p_qcfail", "f64"),
+                   ("p_unmapped", "f64"), ("p_badmate", "f64"), ("p_nonm", "f64"),
+                   ("p_lowq", "f64"), ("p_eqx", "f64"), ("p_mixed", "f64"), ("p_nm_off", "f64"),
+                   ("err_mean", "f64")]
+
+# the variety of reads the tests use; the benchmark keeps mostly clean reads
+BAM_EDGE_CASES = dict(p_indel=0.15, p_soft=0.1, p_overhang=0.05, p_secondary=0.03, p_dup=0.03,
+                      p_qcfail=0.02, p_unmapped=0.02, p_badmate=0.03, p_nonm=0.03, p_lowq=0.1,
+                      p_eqx=0.15, p_mixed=0.1, p_nm_off=0.05, err_mean=0.02)
+BAM_CLEAN = dict(p_indel=0.05, p_soft=0.05, p_overhang=0.0, p_secondary=0.01, p_dup=0.01,
+                 p_qcfail=0.0, p_unmapped=0.005, p_badmate=0.0, p_nonm=0.0, p_lowq=0.05,
+                 p_eqx=0.0, p_mixed=0.0, p_nm_off=0.0, err_mean=0.01)
+
+
+def make_bam(lengths, depth, names=None, seq=None, seq_off=None, seed=1, read_len=150,
+             level=6, straddle=False, n_unmapped_tail=50, **probs) -> bytes:
+    """A coordinate-sorted BAM (BGZF bytes) of reads over contigs of the given
+    lengths at the given mean depths (one value per contig).  `probs` override
+    the read-variety probabilities of BAM_EDGE_CASES; `seq` / `seq_off` (ASCII
+    bases and n+1 offsets) make the reads' bases those of the contigs."""
+    import ctypes
+    lengths = np.ascontiguousarray(lengths, dtype=np.uint32)
+    n = len(lengths)
+    depth = np.ascontiguousarray(depth, dtype=np.float32)
+    assert depth.shape == (n,)
+    if names is None:
+        names = [f"contig_{i}" for i in range(n)]
+    nb = b"".join(s.encode() + b"\0" for s in names) or b"\0"
+    vals = dict(BAM_EDGE_CASES)
+    vals.update(probs)
+    vals.update(seed=seed, read_len=read_len, level=level, straddle=int(bool(straddle)),
+                n_unmapped_tail=n_unmapped_tail)
+
+    class Opts(ctypes.Structure):
+        _fields_ = [(k, {"u64": ctypes.c_uint64, "i32": ctypes.c_int32, "f64": ctypes.c_double}[t])
+                    for k, t in _BAM_OPT_FIELDS]
+
+    o = Opts(**{k: vals[k] for k, _ in _BAM_OPT_FIELDS})
+    lib = _chain_so()
+    lib.synth_bam.restype = ctypes.c_int64
+    out = ctypes.POINTER(ctypes.c_uint8)()
+    P = ctypes.c_void_p
+    if seq is not None:
+        seq = (np.frombuffer(seq, dtype=np.uint8) if isinstance(seq, (bytes, bytearray))
+               else np.ascontiguousarray(seq, dtype=np.uint8))
+        seq_off = np.ascontiguousarray(seq_off, dtype=np.int64)
+    size = lib.synth_bam(ctypes.byref(o), ctypes.c_int32(n), P(lengths.ctypes.data), nb,
+                         P(depth.ctypes.data), P(seq.ctypes.data) if seq is not None else None,
+                         P(seq_off.ctypes.data) if seq is not None else None, ctypes.byref(out))
+    data = ctypes.string_at(out, size)
+    lib.synth_bam_free(out)
+    return data
+
+
+def bam_records(bam: bytes):
+    """(records, target lengths, names) of a BAM: the decompressed bytes after
+    the header (each record: block_size, then the record), for the oracle."""
+    import zlib
+    mv = memoryview(bam)
+    parts, o = [], 0
+    while o < len(bam):                     # BGZF members, by their BC size field
+        bsize = int.from_bytes(bam[o + 16:o + 18], "little") + 1
+        parts.append(zlib.decompress(mv[o + 18:o + bsize - 8], -15))
+        o += bsize
+    raw = b"".join(parts)
+    assert raw[:4] == b"BAM\1"
+    l_text = int.from_bytes(raw[4:8], "little")
+    o = 8 + l_text
+    n_ref = int.from_bytes(raw[o:o + 4], "little")
+    o += 4
+    tl, nm = [], []
+    for _ in range(n_ref):
+        ln = int.from_bytes(raw[o:o + 4], "little")
+        nm.append(raw[o + 4:o + 4 + ln].rstrip(b"\0").decode())
+        tl.append(int.from_bytes(raw[o + 4 + ln:o + 8 + ln], "little"))
+        o += 8 + ln
+    return raw[o:], np.asarray(tl, dtype=np.uint32), nm
