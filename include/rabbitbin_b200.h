@@ -530,8 +530,11 @@ typedef struct rbg_depth_params {
   int32_t include_edge_bases;   /* 0                                                 */
   int32_t min_map_qual;         /* 0                                                 */
   int32_t dual_map_qual;        /* 0: off                                            */
-  int32_t threads;              /* host threads inflating BGZF blocks (0: all)       */
-  int32_t chunk_mb;             /* decompressed bytes per device hand-over (64)      */
+  int32_t threads;              /* host threads (0: all)                             */
+  int32_t chunk_mb;             /* host route: decompressed MiB per hand-over (64)   */
+  int32_t device_inflate;       /* 1: BGZF blocks inflated on the device (default);
+                                   0: on the host threads                          */
+  int32_t device_chunk_mb;      /* device route: decompressed MiB per chunk (1024)   */
 } rbg_depth_params;
 
 typedef struct rbg_depth_matrix {
@@ -550,8 +553,8 @@ typedef struct rbg_depth_matrix {
   int64_t decompressed_bytes;   /* bytes after inflation                             */
   float inflate_ms;             /* host time inflating and walking records           */
   float total_ms;               /* host time of the whole call                       */
-  float kernel_ms;              /* device time of the per-record launches            */
-  int32_t reserved;
+  float kernel_ms;              /* device time of the launches (inflate, walk, sums) */
+  int32_t device_bams;          /* BAMs that took the device route                   */
 } rbg_depth_matrix;
 
 int rbg_default_depth_params(rbg_depth_params *p);

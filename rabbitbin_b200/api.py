@@ -245,7 +245,8 @@ class DepthParams(C.Structure):
     _fields_ = [("percent_identity", C.c_float), ("min_contig_length", C.c_int32),
                 ("max_edge_bases", C.c_int32), ("include_edge_bases", C.c_int32),
                 ("min_map_qual", C.c_int32), ("dual_map_qual", C.c_int32),
-                ("threads", C.c_int32), ("chunk_mb", C.c_int32)]
+                ("threads", C.c_int32), ("chunk_mb", C.c_int32), ("device_inflate", C.c_int32),
+                ("device_chunk_mb", C.c_int32)]
 
 
 class DepthMatrix(C.Structure):
@@ -256,7 +257,7 @@ class DepthMatrix(C.Structure):
                 ("sums", C.POINTER(C.c_uint64)), ("records", C.c_int64),
                 ("compressed_bytes", C.c_int64), ("decompressed_bytes", C.c_int64),
                 ("inflate_ms", C.c_float), ("total_ms", C.c_float), ("kernel_ms", C.c_float),
-                ("reserved", C.c_int32)]
+                ("device_bams", C.c_int32)]
 
 
 class Shard(C.Structure):
@@ -648,9 +649,10 @@ class Context:
         p = default_depth_params(**kw)
         m = DepthMatrix()
         n = len(bams)
-        if all(isinstance(b, (bytes, bytearray)) for b in bams):
-            keep = [C.create_string_buffer(bytes(b), len(b)) for b in bams]
-            ptrs = (C.c_void_p * n)(*[C.cast(k, C.c_void_p) for k in keep])
+        if all(isinstance(b, (bytes, bytearray, memoryview, np.ndarray)) for b in bams):
+            # the callers' buffers themselves, without a copy
+            keep = [np.frombuffer(b, np.uint8) for b in bams]
+            ptrs = (C.c_void_p * n)(*[k.ctypes.data if len(k) else None for k in keep])
             sizes = np.asarray([len(b) for b in bams], np.int64)
             rc = self._L.rbg_bam_depth_mem(self._h, ptrs, _p(sizes, C.c_int64), n, C.byref(p),
                                            C.byref(m))
@@ -678,7 +680,7 @@ class Context:
                 "records": int(m.records), "compressed_bytes": int(m.compressed_bytes),
                 "decompressed_bytes": int(m.decompressed_bytes),
                 "inflate_ms": float(m.inflate_ms), "total_ms": float(m.total_ms),
-                "kernel_ms": float(m.kernel_ms),
+                "kernel_ms": float(m.kernel_ms), "device_bams": int(m.device_bams),
             }
         finally:
             self._L.rbg_free_depth_matrix(C.byref(m))

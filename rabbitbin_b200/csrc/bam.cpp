@@ -47,6 +47,12 @@ void launch_depth_reads(const uint8_t *buf, const uint32_t *rec_off, int64_t nre
 void launch_depth_means(const unsigned long long *sums, int64_t n_targets, const int32_t *kept_tid,
                         int64_t n_kept, const uint32_t *target_len, const int32_t *edge_of_col,
                         int ncols, float *out, cudaStream_t s);
+void launch_depth_device(const uint8_t *comp, const DevBlk *blk, int nb, const uint64_t *ubound,
+                         uint64_t hdr_end, uint8_t *out, uint32_t *counts, uint32_t *scan,
+                         uint32_t *offs, uint32_t *flags, unsigned long long *rec_total,
+                         const uint32_t *target_len, const depth::Params &P,
+                         unsigned long long *sum, unsigned long long *sum_u, int sms,
+                         cudaStream_t s);
 
 namespace {
 
@@ -60,7 +66,7 @@ uint32_t le32(const uint8_t *p) { return depth::ld_u32(p); }
 
 // One BGZF member: its deflate data, inflated size and CRC32.
 struct Blk {
-  uint64_t cdata;
+  uint64_t start, cdata;     // the member's first byte, its deflate data
   uint32_t clen, isize, crc;
 };
 
@@ -84,6 +90,7 @@ void index_blocks(const uint8_t *f, uint64_t n, std::vector<Blk> &out) {
     if (!bsize) throw Error(RBG_ERR_ARG, "BGZF block without its BC size field");
     if (bsize < 12 + xlen + 8 || bsize > n - o) throw Error(RBG_ERR_ARG, "BGZF block size out of range");
     Blk b;
+    b.start = o;
     b.cdata = o + 12 + xlen;
     b.clen = bsize - 12 - xlen - 8;
     b.crc = le32(f + o + bsize - 8);
@@ -343,6 +350,165 @@ struct FileView {
   uint64_t n = 0;
 };
 
+// memcpy on `threads` host threads (the copy into a pinned slot)
+void par_copy(uint8_t *dst, const uint8_t *src, size_t n, int threads) {
+  const size_t per = std::max<size_t>(n / (size_t)std::max(1, threads) + 1, 1 << 20);
+  if (n <= per) {
+    std::memcpy(dst, src, n);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (size_t a = 0; a < n; a += per)
+    pool.emplace_back([=] { std::memcpy(dst + a, src + a, std::min(per, n - a)); });
+  for (auto &t : pool) t.join();
+}
+
+// The header and the read-length sample of one BAM, from its first blocks
+// inflated on the host (groups of `threads` blocks until 4,000 mapped records
+// have been seen or the file ends).
+struct Prefix {
+  Header h;
+  int64_t hdr_end = 0;
+  int32_t avg = 0;
+};
+
+Prefix host_prefix(const FileView &f, const std::vector<Blk> &B, const std::vector<uint64_t> &uoff,
+                   int threads) {
+  Prefix r;
+  std::vector<uint8_t> buf;
+  size_t done_blocks = 0;
+  uint64_t q = 0;
+  int64_t srs = 0, src = 0;
+  bool have_hdr = false, full = false;
+  while (!full && done_blocks < B.size()) {
+    const size_t take = std::min(B.size() - done_blocks, (size_t)std::max(1, threads));
+    buf.resize(uoff[done_blocks + take]);
+    inflate_blocks(f.p, B, uoff, done_blocks, done_blocks + take, buf.data() + uoff[done_blocks],
+                   threads);
+    done_blocks += take;
+    if (!have_hdr) {
+      r.hdr_end = parse_header(buf.data(), (int64_t)buf.size(), r.h);
+      if (!r.hdr_end) continue;
+      have_hdr = true;
+      q = (uint64_t)r.hdr_end;
+    }
+    while (buf.size() - q >= 36) {
+      const uint32_t rb = depth::record_bytes(buf.data() + q, buf.size() - q);
+      if (!rb) break;                 // cut by the inflated prefix, or malformed
+      if (!(depth::ld_u16(buf.data() + q + 18) & depth::kUnmap)) {
+        srs += depth::ld_i32(buf.data() + q + 20);
+        if (++src >= 4000) {
+          full = true;
+          break;
+        }
+      }
+      q += rb;
+    }
+  }
+  if (!have_hdr) throw Error(RBG_ERR_ARG, "truncated BAM header");
+  r.avg = src ? (int32_t)(srs / src) : 0;
+  return r;
+}
+
+// One BAM through the device route: chunks of compressed blocks are copied in
+// and inflated, walked and summed on the device.  Returns false when a block
+// did not start on a record (a writer that lets records cross blocks): the
+// caller then clears the sums and takes the host route.
+bool run_sample_device(rbg_ctx *c, const FileView &f, const std::vector<Blk> &B,
+                       const std::vector<uint64_t> &uoff, int64_t hdr_end, const depth::Params &P,
+                       const rbg_depth_params *p, const uint32_t *d_tlen, unsigned long long *sum,
+                       unsigned long long *sum_u, int threads, SampleOut &so) {
+  DepthBufs &D = *c->depthb;
+  cudaStream_t s = c->stream;
+  for (int i = 0; i < 2; ++i) {
+    if (!D.ev[i]) CK(cudaEventCreateWithFlags(&D.ev[i], cudaEventDisableTiming));
+    if (!D.k0[i]) CK(cudaEventCreate(&D.k0[i]));
+    if (!D.k1[i]) CK(cudaEventCreate(&D.k1[i]));
+  }
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+  const uint64_t budget = (uint64_t)std::max(1, std::min(p->device_chunk_mb, 3072)) << 20;
+  D.flags.ensure(16);
+  CK(cudaMemsetAsync(D.flags.p, 0, 16, s));
+  uint32_t *flags = D.flags.as<uint32_t>();
+  unsigned long long *rec_total = (unsigned long long *)(D.flags.as<uint8_t>() + 8);
+  bool timed[2] = {false, false};
+  size_t b0 = 0;
+  int slot = 0;
+  while (b0 < B.size()) {
+    size_t b1 = b0;
+    uint64_t bytes = 0;
+    while (b1 < B.size() && (b1 == b0 || bytes + B[b1].isize <= budget)) bytes += B[b1++].isize;
+    const int nb = (int)(b1 - b0);
+    const uint64_t cstart = B[b0].start;
+    const uint64_t cend = B[b1 - 1].cdata + B[b1 - 1].clen + 8;
+    const size_t cbytes = (size_t)(cend - cstart);
+    if (cbytes > 0xFFFFFFFFull) throw Error(RBG_ERR_ARG, "device chunk too large");
+    CK(cudaEventSynchronize(D.ev[slot]));
+    if (timed[slot]) {
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, D.k0[slot], D.k1[slot]));
+      so.kernel_ms += ms;
+      timed[slot] = false;
+    }
+    D.cpin[slot].ensure(cbytes + 16);
+    const size_t tab_bytes = (size_t)nb * sizeof(DevBlk) + (size_t)(nb + 1) * 8;
+    D.tpin[slot].ensure(tab_bytes);
+    par_copy(D.cpin[slot].as<uint8_t>(), f.p + cstart, cbytes, threads);
+    DevBlk *tb = D.tpin[slot].as<DevBlk>();
+    uint64_t *ub = (uint64_t *)(D.tpin[slot].as<uint8_t>() + (size_t)nb * sizeof(DevBlk));
+    for (int i = 0; i < nb; ++i) {
+      const Blk &x = B[b0 + i];
+      tb[i].cofs = (uint32_t)(x.cdata - cstart);
+      tb[i].clen = x.clen;
+      tb[i].isize = x.isize;
+      tb[i].crc = x.crc;
+      tb[i].uofs = uoff[b0 + i] - uoff[b0];
+      ub[i] = tb[i].uofs;
+    }
+    ub[nb] = bytes;
+    D.cdev[slot].ensure(cbytes + 16);
+    D.tdev[slot].ensure(tab_bytes);
+    D.outd[slot].ensure(bytes + 64);
+    D.cntd[slot].ensure((size_t)(2 * nb + 2) * 4);
+    D.offd[slot].ensure((size_t)(bytes / 36 + nb + 16) * 4);
+    CK(cudaMemcpyAsync(D.cdev[slot].p, D.cpin[slot].p, cbytes, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(D.tdev[slot].p, D.tpin[slot].p, tab_bytes, cudaMemcpyHostToDevice, s));
+    const int64_t he = hdr_end - (int64_t)uoff[b0];
+    const uint64_t hdr_chunk = he <= 0 ? 0 : std::min<uint64_t>((uint64_t)he, bytes);
+    uint32_t *cnt = D.cntd[slot].as<uint32_t>();
+    CK(cudaEventRecord(D.k0[slot], s));
+    launch_depth_device(D.cdev[slot].as<uint8_t>(), D.tdev[slot].as<DevBlk>(), nb,
+                        (const uint64_t *)(D.tdev[slot].as<uint8_t>() + (size_t)nb * sizeof(DevBlk)),
+                        hdr_chunk, D.outd[slot].as<uint8_t>(), cnt, cnt + nb + 1,
+                        D.offd[slot].as<uint32_t>(), flags, rec_total, d_tlen, P, sum,
+                        p->dual_map_qual > 0 ? sum_u : nullptr, sms, s);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(D.k1[slot], s));
+    CK(cudaEventRecord(D.ev[slot], s));
+    timed[slot] = true;
+    c->launches += 5;
+    b0 = b1;
+    slot ^= 1;
+  }
+  uint32_t fl[4] = {0, 0, 0, 0};
+  D.hflag.ensure(16);
+  CK(cudaMemcpyAsync(D.hflag.p, D.flags.p, 16, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  std::memcpy(fl, D.hflag.p, 16);
+  for (int i = 0; i < 2; ++i)
+    if (timed[i]) {
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, D.k0[i], D.k1[i]));
+      so.kernel_ms += ms;
+    }
+  if (fl[0] & 1u) throw Error(RBG_ERR_ARG, "BGZF block does not inflate to its stated size or fails its CRC32");
+  uint64_t recs = 0;
+  std::memcpy(&recs, (uint8_t *)fl + 8, 8);
+  so.records = (int64_t)recs;
+  return (fl[0] & 2u) == 0;
+}
+
 void bam_depth(rbg_ctx *c, const std::vector<FileView> &files, const rbg_depth_params *p,
                rbg_depth_matrix *out) {
   const auto t_all = Clock::now();
@@ -360,6 +526,7 @@ void bam_depth(rbg_ctx *c, const std::vector<FileView> &files, const rbg_depth_p
   std::vector<int32_t> avg(nb, 0), edge_col(ncols, 0);
   double walk_ms = 0, kernel_ms = 0;
   int64_t records = 0, cbytes = 0, ubytes = 0;
+  int32_t device_bams = 0;
   for (int b = 0; b < nb; ++b) {
     std::vector<Blk> B;
     index_blocks(files[b].p, files[b].n, B);
@@ -367,6 +534,43 @@ void bam_depth(rbg_ctx *c, const std::vector<FileView> &files, const rbg_depth_p
     for (size_t i = 0; i < B.size(); ++i) uoff[i + 1] = uoff[i] + B[i].isize;
     cbytes += (int64_t)files[b].n;
     ubytes += (int64_t)uoff.back();
+    unsigned long long *sums_all = nullptr;
+    if (p->device_inflate) {
+      const auto t0 = Clock::now();
+      Prefix pre = host_prefix(files[b], B, uoff, threads);
+      walk_ms += ms_since(t0);
+      if (b == 0) {
+        h0 = pre.h;
+        const int32_t nt = (int32_t)h0.tlen.size();
+        D.tlen.ensure(std::max<size_t>(1, (size_t)nt) * 4);
+        if (nt) CK(cudaMemcpyAsync(D.tlen.p, h0.tlen.data(), (size_t)nt * 4, cudaMemcpyHostToDevice, s));
+        D.sums.ensure(std::max<size_t>(1, (size_t)ncols * nt) * 8);
+        CK(cudaMemsetAsync(D.sums.p, 0, std::max<size_t>(1, (size_t)ncols * nt) * 8, s));
+      } else if (pre.h.tlen != h0.tlen) {
+        throw Error(RBG_ERR_ARG, "BAM files carry different contigs");
+      }
+      const int32_t nt = (int32_t)h0.tlen.size();
+      sums_all = D.sums.as<unsigned long long>();
+      depth::Params P{p->percent_identity,
+                      p->include_edge_bases ? 0 : std::min(p->max_edge_bases, pre.avg / 3),
+                      p->min_map_qual, p->dual_map_qual, nt};
+      SampleOut so;
+      if (run_sample_device(c, files[b], B, uoff, pre.hdr_end, P, p, D.tlen.as<uint32_t>(),
+                            sums_all + (size_t)b * nt, sums_all + (size_t)(nb + b) * nt, threads,
+                            so)) {
+        avg[b] = pre.avg;
+        records += so.records;
+        kernel_ms += so.kernel_ms;
+        edge_col[b] = P.edge;
+        if (dual) edge_col[nb + b] = edge_col[b];
+        ++device_bams;
+        continue;
+      }
+      // a block did not start on a record: this BAM takes the host route
+      kernel_ms += so.kernel_ms;
+      CK(cudaMemsetAsync(sums_all + (size_t)b * nt, 0, (size_t)nt * 8, s));
+      if (dual) CK(cudaMemsetAsync(sums_all + (size_t)(nb + b) * nt, 0, (size_t)nt * 8, s));
+    }
     // header: inflate blocks one by one until it is complete
     std::vector<uint8_t> hb;
     Header h;
@@ -453,6 +657,7 @@ void bam_depth(rbg_ctx *c, const std::vector<FileView> &files, const rbg_depth_p
   out->inflate_ms = (float)walk_ms;
   out->total_ms = (float)ms_since(t_all);
   out->kernel_ms = (float)kernel_ms;
+  out->device_bams = device_bams;
 }
 
 }  // namespace
@@ -473,6 +678,8 @@ int rbg_default_depth_params(rbg_depth_params *p) {
   p->dual_map_qual = 0;
   p->threads = 0;
   p->chunk_mb = 64;
+  p->device_inflate = 1;
+  p->device_chunk_mb = 1024;
   return RBG_OK;
 }
 

@@ -240,14 +240,23 @@ struct LpaBufs {
 struct DepthBufs {
   DBuf buf[2], off[2], sums, tlen, kept, edge, means;
   HBuf slot[2], offp[2];
+  // device route: compressed chunk, block table, inflated chunk, counts and
+  // scan, record offsets; the route's flags and record count
+  DBuf cdev[2], tdev[2], outd[2], cntd[2], offd[2], flags;
+  HBuf cpin[2], tpin[2], hflag;
   cudaEvent_t ev[2] = {nullptr, nullptr};
   cudaEvent_t k0[2] = {nullptr, nullptr}, k1[2] = {nullptr, nullptr};   // per-record launch times
   void release() {
-    DBuf *all[] = {&buf[0], &buf[1], &off[0], &off[1], &sums, &tlen, &kept, &edge, &means};
+    DBuf *all[] = {&buf[0], &buf[1], &off[0], &off[1], &sums, &tlen, &kept, &edge, &means,
+                   &cdev[0], &cdev[1], &tdev[0], &tdev[1], &outd[0], &outd[1], &cntd[0],
+                   &cntd[1], &offd[0], &offd[1], &flags};
     for (DBuf *b : all) b->release();
+    hflag.release();
     for (int i = 0; i < 2; ++i) {
       slot[i].release();
       offp[i].release();
+      cpin[i].release();
+      tpin[i].release();
       if (ev[i]) cudaEventDestroy(ev[i]);
       if (k0[i]) cudaEventDestroy(k0[i]);
       if (k1[i]) cudaEventDestroy(k1[i]);

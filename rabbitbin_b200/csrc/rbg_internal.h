@@ -58,6 +58,14 @@ void oph_sv_table(int m, std::vector<double> &sv_d, std::vector<float> &sv_f);
 void sv_table(int m, bool base_on, double b0, std::vector<double> &sv_d,
               std::vector<float> &sv_f);
 
+// One BGZF block of a device chunk: its deflate data (offset in the chunk's
+// compressed bytes), inflated size, CRC32 and place in the chunk's output.
+struct DevBlk {
+  uint32_t cofs, clen, isize, crc;
+  uint64_t uofs;
+};
+constexpr int kInflateWarps = 8;        // BGZF blocks in flight per CTA of the inflate kernel
+
 // ── kernel launchers (kernels_*.cu) ─────────────────────────────────────────
 struct SketchArgs {
   // input: 2-bit packed bases (16 per word, first base in the top bits) and

@@ -42,11 +42,17 @@ def _check_means(out, tl, edges, min_len=1):
         np.testing.assert_array_equal(out["means"][:, c], want, err_msg=f"column {c}")
 
 
+@pytest.mark.parametrize("route", ["device", "host"])
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_bam_depth_matches_reference(gpu_ctx, golden, name):
+def test_bam_depth_matches_reference(gpu_ctx, golden, name, route):
+    """Both routes: BGZF inflated on the device (files whose records cross
+    block ends fall back to the host walk) or on the host threads."""
     lens, _, bam = case(name)
     for i, (pid, edge, inc, mq, dq) in enumerate(PARAMS):
-        out = gpu_ctx.bam_depth([bam], **_kw(pid, edge, inc, mq, dq))
+        out = gpu_ctx.bam_depth([bam], device_inflate=int(route == "device"),
+                                **_kw(pid, edge, inc, mq, dq))
+        straddle = CASES[name][2].get("straddle", False)
+        assert out["device_bams"] == (1 if route == "device" and not straddle else 0)
         avg = int(golden[f"{name}/{i}/avg"])
         assert out["avg_read"][0] == avg
         np.testing.assert_array_equal(out["sums"][0], golden[f"{name}/{i}/sums"],
@@ -60,12 +66,15 @@ def test_bam_depth_matches_reference(gpu_ctx, golden, name):
 
 def test_small_chunks_carry_records_and_sample_read_length(gpu_ctx, golden):
     """1 MiB hand-overs: records cut by every chunk end, and fewer than 4,000
-    mapped records in the first chunk (the read-length sample spans chunks)."""
+    mapped records in the first chunk (the read-length sample spans chunks);
+    on the device route, chunks of 1 MiB of blocks (many launches per file)."""
     for name in ("edge_mix", "edge_mix_straddle", "long_reads"):
         lens, _, bam = case(name)
-        out = gpu_ctx.bam_depth([bam], chunk_mb=1, threads=3, **_kw(*PARAMS[0]))
-        np.testing.assert_array_equal(out["sums"][0], golden[f"{name}/0/sums"])
-        assert out["avg_read"][0] == int(golden[f"{name}/0/avg"])
+        for dev in (0, 1):
+            out = gpu_ctx.bam_depth([bam], chunk_mb=1, device_chunk_mb=1, threads=3,
+                                    device_inflate=dev, **_kw(*PARAMS[0]))
+            np.testing.assert_array_equal(out["sums"][0], golden[f"{name}/0/sums"])
+            assert out["avg_read"][0] == int(golden[f"{name}/0/avg"])
 
 
 def test_several_bams_and_dual_columns(gpu_ctx, golden):
@@ -147,9 +156,10 @@ def test_malformed_input_is_rejected(gpu_ctx):
            + cdata + struct.pack("<II", zlib.crc32(bytes(body)), len(body)))
     bad.append(blk)
     for b in bad:
-        with pytest.raises(api.RbgError) as e:
-            gpu_ctx.bam_depth([b])
-        assert e.value.code == -1
+        for dev in (0, 1):
+            with pytest.raises(api.RbgError) as e:
+                gpu_ctx.bam_depth([b], device_inflate=dev)
+            assert e.value.code == -1
     other = make_bam(np.array([300, 401], np.uint32), np.ones(2))
     with pytest.raises(api.RbgError) as e:
         gpu_ctx.bam_depth([bam, other])
