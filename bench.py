@@ -828,8 +828,8 @@ def run_depth_form(args):
                                                                          out["sums"].nbytes),
                 "time": "host clock around rbg_bam_depth_mem (BGZF bytes in host memory in, the "
                         "depth matrix in host memory out)"},
-        "stages_ms": {"inflate_and_walk_ms": float(np.median(infl)), "kernel_ms": kms,
-                      "total_ms": ms},
+        "stages_ms": {"host_prefix_ms": float(np.median(infl)), "kernel_ms": kms,
+                      "call_ms": float(out["total_ms"]), "total_ms": ms},
         "decompressed_gbs": ub / (ms / 1000.0) / 1e9,
         "device_route": bool(out["device_bams"] == 1),
         "kernels": {"names": "k_inflate + k_walk (2 passes) + k_scan_counts + k_depth_reads_dev "

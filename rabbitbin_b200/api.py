@@ -665,9 +665,12 @@ class Context:
             nr, nc, nt = int(m.n_rows), int(m.n_cols), int(m.n_targets)
             names = []
             if nr:
-                off = np.ctypeslib.as_array(m.name_off, (nr,)).copy()
-                for o in off:
-                    names.append(C.string_at(m.names + int(o)).decode())
+                # one read of the NUL-terminated names block
+                off = np.ctypeslib.as_array(m.name_off, (nr,))
+                last = int(off[-1])
+                tail = C.string_at(m.names + last)
+                blob = C.string_at(m.names, last + len(tail) + 1)
+                names = blob[:-1].decode().split("\0")
             out = {
                 "names": names,
                 "tid": np.ctypeslib.as_array(m.tid, (nr,)).copy() if nr else np.zeros(0, np.int32),

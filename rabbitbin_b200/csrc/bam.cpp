@@ -422,6 +422,7 @@ bool run_sample_device(rbg_ctx *c, const FileView &f, const std::vector<Blk> &B,
   cudaStream_t s = c->stream;
   for (int i = 0; i < 2; ++i) {
     if (!D.ev[i]) CK(cudaEventCreateWithFlags(&D.ev[i], cudaEventDisableTiming));
+    if (!D.evc[i]) CK(cudaEventCreateWithFlags(&D.evc[i], cudaEventDisableTiming));
     if (!D.k0[i]) CK(cudaEventCreate(&D.k0[i]));
     if (!D.k1[i]) CK(cudaEventCreate(&D.k1[i]));
   }
@@ -472,8 +473,13 @@ bool run_sample_device(rbg_ctx *c, const FileView &f, const std::vector<Blk> &B,
     D.outd[slot].ensure(bytes + 64);
     D.cntd[slot].ensure((size_t)(2 * nb + 2) * 4);
     D.offd[slot].ensure((size_t)(bytes / 36 + nb + 16) * 4);
-    CK(cudaMemcpyAsync(D.cdev[slot].p, D.cpin[slot].p, cbytes, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(D.tdev[slot].p, D.tpin[slot].p, tab_bytes, cudaMemcpyHostToDevice, s));
+    // copies on the context's copy stream, so that chunk c + 1 arrives while
+    // chunk c is inflated
+    CK(cudaStreamWaitEvent(c->copy, D.ev[slot], 0));
+    CK(cudaMemcpyAsync(D.cdev[slot].p, D.cpin[slot].p, cbytes, cudaMemcpyHostToDevice, c->copy));
+    CK(cudaMemcpyAsync(D.tdev[slot].p, D.tpin[slot].p, tab_bytes, cudaMemcpyHostToDevice, c->copy));
+    CK(cudaEventRecord(D.evc[slot], c->copy));
+    CK(cudaStreamWaitEvent(s, D.evc[slot], 0));
     const int64_t he = hdr_end - (int64_t)uoff[b0];
     const uint64_t hdr_chunk = he <= 0 ? 0 : std::min<uint64_t>((uint64_t)he, bytes);
     uint32_t *cnt = D.cntd[slot].as<uint32_t>();

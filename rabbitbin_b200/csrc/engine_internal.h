@@ -246,6 +246,7 @@ struct DepthBufs {
   HBuf cpin[2], tpin[2], hflag;
   cudaEvent_t ev[2] = {nullptr, nullptr};
   cudaEvent_t k0[2] = {nullptr, nullptr}, k1[2] = {nullptr, nullptr};   // per-record launch times
+  cudaEvent_t evc[2] = {nullptr, nullptr};                             // device route: chunk copied
   void release() {
     DBuf *all[] = {&buf[0], &buf[1], &off[0], &off[1], &sums, &tlen, &kept, &edge, &means,
                    &cdev[0], &cdev[1], &tdev[0], &tdev[1], &outd[0], &outd[1], &cntd[0],
@@ -260,7 +261,8 @@ struct DepthBufs {
       if (ev[i]) cudaEventDestroy(ev[i]);
       if (k0[i]) cudaEventDestroy(k0[i]);
       if (k1[i]) cudaEventDestroy(k1[i]);
-      ev[i] = k0[i] = k1[i] = nullptr;
+      if (evc[i]) cudaEventDestroy(evc[i]);
+      ev[i] = k0[i] = k1[i] = evc[i] = nullptr;
     }
   }
 };

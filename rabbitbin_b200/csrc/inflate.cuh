@@ -77,10 +77,28 @@ struct Bits {
   uint64_t buf;
   int cnt;
   RBG_IHD void refill() {
+#ifdef __CUDA_ARCH__
+    // two aligned 8-byte loads and a funnel shift; the device buffers hold the
+    // input from a 256-byte aligned start with 16 bytes of slack after its end,
+    // and bytes past the stream's end are masked off
+    if (pos >= n || cnt > 56) return;
+    const uintptr_t a = (uintptr_t)(p + pos);
+    const uint64_t *q = (const uint64_t *)(a & ~(uintptr_t)7);
+    const uint32_t sh = (uint32_t)(a & 7) * 8;
+    uint64_t w = __ldg(q) >> sh;
+    if (sh) w |= __ldg(q + 1) << (64 - sh);
+    uint32_t take = (uint32_t)(63 - cnt) >> 3;
+    if (take > n - pos) take = n - pos;
+    w &= take >= 8 ? ~0ull : ((1ull << (8 * take)) - 1);
+    buf |= w << cnt;
+    pos += take;
+    cnt += 8 * (int)take;
+#else
     while (cnt <= 56 && pos < n) {
       buf |= (uint64_t)p[pos++] << cnt;
       cnt += 8;
     }
+#endif
   }
   RBG_IHD bool need(int k) {
     if (cnt < k) refill();

@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "depth_record.cuh"
 #include "inflate.cuh"
@@ -81,7 +82,8 @@ __global__ void k_depth_means(const unsigned long long *__restrict__ sums, int64
 // (inflate.cuh: the lanes decode in lockstep and copy together; the warp's
 // Huffman tables in shared memory) and checks its CRC32 (lane segments joined
 // over GF(2)).  Failures set bit 0 of *flags.
-__global__ void __launch_bounds__(kInflateWarps * 32) k_inflate(const uint8_t *__restrict__ comp,
+template <int kMinCtas>
+__global__ void __launch_bounds__(kInflateWarps * 32, kMinCtas) k_inflate(const uint8_t *__restrict__ comp,
                                                                const DevBlk *__restrict__ blk,
                                                                int nb, uint8_t *__restrict__ out,
                                                                uint32_t *__restrict__ flags) {
@@ -234,8 +236,18 @@ void launch_depth_device(const uint8_t *comp, const DevBlk *blk, int nb, const u
                          unsigned long long *sum, unsigned long long *sum_u, int sms,
                          cudaStream_t s) {
   if (nb <= 0) return;
-  const int ctas = std::min((nb + kInflateWarps - 1) / kInflateWarps, sms * 4);
-  k_inflate<<<ctas, kInflateWarps * 32, 0, s>>>(comp, blk, nb, out, flags);
+  // four CTAs per SM (64 registers, a few spilled: 40 ms against 46 ms for the
+  // 80-register build on the 5.6 M-read benchmark BAM); RBG_INFLATE_CTAS=3
+  // takes the 80-register build
+  static const int per_sm = [] {
+    const char *e = getenv("RBG_INFLATE_CTAS");
+    return (e && atoi(e) == 3) ? 3 : 4;
+  }();
+  const int ctas = std::min((nb + kInflateWarps - 1) / kInflateWarps, sms * per_sm);
+  if (per_sm == 4)
+    k_inflate<4><<<ctas, kInflateWarps * 32, 0, s>>>(comp, blk, nb, out, flags);
+  else
+    k_inflate<3><<<ctas, kInflateWarps * 32, 0, s>>>(comp, blk, nb, out, flags);
   const unsigned g = (unsigned)((nb + 127) / 128);
   k_walk<<<g, 128, 0, s>>>(out, ubound, nb, hdr_end, counts, scan, offs, flags, 0);
   k_scan_counts<<<1, 1024, 0, s>>>(counts, nb, scan, rec_total);
