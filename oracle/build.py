@@ -23,7 +23,10 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("RABBITBIN_REFERENCE", "/root/reference")
+# the reference tree: RABBITBIN_REFERENCE, else a checkout named "reference"
+# beside this repository (absent on machines that only run the prebuilt files)
+REF = os.environ.get("RABBITBIN_REFERENCE") or os.path.join(
+    os.path.dirname(os.path.dirname(HERE)), "reference")
 REF_SRC = os.path.join(REF, "src")
 FLAGS = ["-std=c++17", "-O3", "-march=x86-64-v4", "-funroll-loops", "-fopenmp",
          "-fPIC", "-shared", "-w"]

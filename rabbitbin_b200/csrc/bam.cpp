@@ -24,6 +24,10 @@
 // Two slots alternate: while the device copies and scores chunk c, the host
 // inflates chunk c + 1 into the other slot.  Nothing but the sums stays on the
 // device between chunks; the means matrix is made on the device at the end.
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
 #include <zlib.h>
 
 #include <algorithm>
@@ -720,25 +724,39 @@ int rbg_bam_depth(rbg_ctx *c, const char *const *paths, int32_t n_bams, const rb
                   rbg_depth_matrix *out) {
   return guarded(c, [&] {
     if (!paths || n_bams < 1) throw Error(RBG_ERR_ARG, "null argument or no BAM");
-    std::vector<std::vector<uint8_t>> data((size_t)n_bams);
+    // the files are mapped read-only, not read into memory: BAMs can be far
+    // larger than the host's memory, and every byte is touched once
+    struct Mapped {
+      void *p = MAP_FAILED;
+      size_t n = 0;
+      ~Mapped() {
+        if (p != MAP_FAILED && n) munmap(p, n);
+      }
+    };
+    std::vector<Mapped> maps((size_t)n_bams);
     std::vector<FileView> files((size_t)n_bams);
     for (int32_t b = 0; b < n_bams; ++b) {
       if (!paths[b]) throw Error(RBG_ERR_ARG, "null BAM path");
-      FILE *fp = std::fopen(paths[b], "rb");
-      if (!fp) throw Error(RBG_ERR_ARG, std::string("cannot open ") + paths[b]);
-      std::fseek(fp, 0, SEEK_END);
-      const long sz = std::ftell(fp);
-      std::fseek(fp, 0, SEEK_SET);
-      if (sz < 0) {
-        std::fclose(fp);
+      const int fd = open(paths[b], O_RDONLY);
+      if (fd < 0) throw Error(RBG_ERR_ARG, std::string("cannot open ") + paths[b]);
+      struct stat st;
+      if (fstat(fd, &st) != 0) {
+        close(fd);
         throw Error(RBG_ERR_ARG, std::string("cannot size ") + paths[b]);
       }
-      data[b].resize((size_t)sz);
-      const size_t got = sz ? std::fread(data[b].data(), 1, (size_t)sz, fp) : 0;
-      std::fclose(fp);
-      if (got != (size_t)sz) throw Error(RBG_ERR_ARG, std::string("short read of ") + paths[b]);
-      files[b].p = data[b].data();
-      files[b].n = (uint64_t)sz;
+      maps[b].n = (size_t)st.st_size;
+      if (maps[b].n) {
+        maps[b].p = mmap(nullptr, maps[b].n, PROT_READ, MAP_PRIVATE, fd, 0);
+        if (maps[b].p == MAP_FAILED) {
+          close(fd);
+          throw Error(RBG_ERR_ARG, std::string("cannot map ") + paths[b]);
+        }
+        madvise(maps[b].p, maps[b].n, MADV_SEQUENTIAL);
+      }
+      close(fd);
+      static const uint8_t none = 0;
+      files[b].p = maps[b].n ? (const uint8_t *)maps[b].p : &none;
+      files[b].n = (uint64_t)maps[b].n;
     }
     bam_depth(c, files, p, out);
   });
