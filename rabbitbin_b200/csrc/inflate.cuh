@@ -8,8 +8,9 @@
 // blocks together, in rounds no longer than the match distance so that every
 // byte read was written in an earlier round.  The same code runs on the host
 // with one lane (the CPU tests).  Symbols are decoded with a 9-bit (literal /
-// length) and 8-bit (distance) lookup table, with the canonical code walk for
-// longer codes.  Every read stays inside [in, in + inlen),
+// length) and 8-bit (distance) lookup table of 32-bit entries that carry each
+// symbol's meaning (literal byte, length or distance base, extra bits), with
+// the canonical code walk for longer codes.  Every read stays inside [in, in + inlen),
 // every write inside [out, out + outlen), and every match must point into
 // bytes already written: a stream that breaks a rule ends with a status, never
 // with an access out of bounds.
@@ -56,14 +57,22 @@ struct WarpLanes {
 };
 #endif
 
-// One Huffman code: lookup table for codes up to kBits bits (entry = symbol << 4
-// | length, 0 = longer code or unused) and the canonical tables for the rest.
+// One Huffman code: lookup table for codes up to kBits bits and the canonical
+// tables for the rest.  A table entry carries what the symbol means, so the
+// decode loop needs no per-symbol arithmetic:
+//   bits 0-3   code length (0: longer code, or no code)
+//   bits 4-5   kind: 0 literal / distance / code-length symbol, 1 length,
+//              2 end of block, 3 invalid symbol
+//   bits 6-9   extra bits that follow the code
+//   bits 16-31 value: the literal byte, the length or distance base, or the
+//              code-length symbol
 template <int kBits, int kSyms>
 struct Code {
-  uint16_t lut[1 << kBits];
+  uint32_t lut[1 << kBits];
   uint16_t count[16];
   uint16_t sym[kSyms];
 };
+constexpr uint32_t kEndOfInput = 0xFFFFFFFFu, kNoCode = 0xFFFFFFFEu;
 
 struct Tables {
   Code<kLitBits, 288> lit;
@@ -126,9 +135,41 @@ RBG_IHD uint32_t reverse_bits(uint32_t v, int n) {
   return r;
 }
 
+// Length symbols 257 + i: i < 8 give 3 + i with no extra bits; then groups of
+// four with e = (i - 4) / 4 extra bits starting at ((4 + (i & 3)) << e) + 3;
+// i = 28 (symbol 285) is 258.  Distance symbols d < 4 give d + 1; then pairs
+// with e = (d - 2) / 2 extra bits starting at ((2 + (d & 1)) << e) + 1.
+RBG_IHD int len_extra(int i) { return (i < 8 || i == 28) ? 0 : (i - 4) / 4; }
+RBG_IHD uint32_t len_base(int i) {
+  return i < 8 ? 3u + i : (i == 28 ? 258u : ((4u + (i & 3)) << len_extra(i)) + 3u);
+}
+RBG_IHD int dist_extra(int d) { return d < 4 ? 0 : (d - 2) / 2; }
+RBG_IHD uint32_t dist_base(int d) { return d < 4 ? 1u + d : ((2u + (d & 1)) << dist_extra(d)) + 1u; }
+
+
+// Table entries of the three codes.
+struct LitEntry {
+  RBG_IHD static uint32_t make(int s, int l) {
+    if (s < 256) return (uint32_t)s << 16 | (uint32_t)l;
+    if (s == 256) return 2u << 4 | (uint32_t)l;
+    const int i = s - 257;
+    if (i >= 29) return 3u << 4 | (uint32_t)l;
+    return len_base(i) << 16 | (uint32_t)len_extra(i) << 6 | 1u << 4 | (uint32_t)l;
+  }
+};
+struct DistEntry {
+  RBG_IHD static uint32_t make(int s, int l) {
+    if (s >= 30) return 3u << 4 | (uint32_t)l;
+    return dist_base(s) << 16 | (uint32_t)dist_extra(s) << 6 | (uint32_t)l;
+  }
+};
+struct PlainEntry {
+  RBG_IHD static uint32_t make(int s, int l) { return (uint32_t)s << 16 | (uint32_t)l; }
+};
+
 // Builds a code from `n` code lengths.  Incomplete codes are accepted (a code
 // of one distance symbol is legal); over-subscribed ones are not.
-template <int kBits, int kSyms>
+template <class Entry, int kBits, int kSyms>
 RBG_IHD int build(Code<kBits, kSyms> &c, const uint8_t *len, int n) {
   for (int i = 0; i < 16; ++i) c.count[i] = 0;
   for (int s = 0; s < n; ++s) c.count[len[s]]++;
@@ -157,48 +198,39 @@ RBG_IHD int build(Code<kBits, kSyms> &c, const uint8_t *len, int n) {
     const uint32_t cd = next[l]++;
     if (l > kBits) continue;
     const uint32_t r = reverse_bits(cd, l);
-    for (uint32_t f = r; f < (1u << kBits); f += (1u << l)) c.lut[f] = (uint16_t)(s << 4 | l);
+    const uint32_t e = Entry::make(s, l);
+    for (uint32_t f = r; f < (1u << kBits); f += (1u << l)) c.lut[f] = e;
   }
   return kOk;
 }
 
-// Decodes one symbol; -1 when the stream ends, -2 for an unused code.
-template <int kBits, int kSyms>
-RBG_IHD int decode(const Code<kBits, kSyms> &c, Bits &b) {
+// Decodes one symbol and returns its table entry; kEndOfInput when the stream
+// ends, kNoCode for a code that is not in the table.
+template <class Entry, int kBits, int kSyms>
+RBG_IHD uint32_t decode(const Code<kBits, kSyms> &c, Bits &b) {
   if (b.cnt < 15) b.refill();
   // bits above cnt are zero, so the table index is defined near the end too;
   // an entry counts only when its whole code is in the buffer
-  const uint16_t e = c.lut[b.peek(kBits)];
+  const uint32_t e = c.lut[b.peek(kBits)];
   if (e && (int)(e & 15) <= b.cnt) {
     b.drop(e & 15);
-    return e >> 4;
+    return e;
   }
   // canonical walk, one bit at a time (codes longer than the table)
   int code = 0, first = 0, index = 0;
   for (int l = 1; l < 16; ++l) {
-    if (!b.need(1)) return -1;
+    if (!b.need(1)) return kEndOfInput;
     code |= (int)b.peek(1);
     b.drop(1);
     const int cnt = c.count[l];
-    if (code - cnt < first) return c.sym[index + (code - first)];
+    if (code - cnt < first) return Entry::make(c.sym[index + (code - first)], l);
     index += cnt;
     first += cnt;
     first <<= 1;
     code <<= 1;
   }
-  return -2;
+  return kNoCode;
 }
-
-// Length symbols 257 + i: i < 8 give 3 + i with no extra bits; then groups of
-// four with e = (i - 4) / 4 extra bits starting at ((4 + (i & 3)) << e) + 3;
-// i = 28 (symbol 285) is 258.  Distance symbols d < 4 give d + 1; then pairs
-// with e = (d - 2) / 2 extra bits starting at ((2 + (d & 1)) << e) + 1.
-RBG_IHD int len_extra(int i) { return (i < 8 || i == 28) ? 0 : (i - 4) / 4; }
-RBG_IHD uint32_t len_base(int i) {
-  return i < 8 ? 3u + i : (i == 28 ? 258u : ((4u + (i & 3)) << len_extra(i)) + 3u);
-}
-RBG_IHD int dist_extra(int d) { return d < 4 ? 0 : (d - 2) / 2; }
-RBG_IHD uint32_t dist_base(int d) { return d < 4 ? 1u + d : ((2u + (d & 1)) << dist_extra(d)) + 1u; }
 
 // Inflates one raw deflate stream into out[0, outlen).  Returns kOk when the
 // final block ends with exactly outlen bytes written.
@@ -259,12 +291,13 @@ RBG_IHD int inflate_block(const uint8_t *in, uint32_t inlen, uint8_t *out, uint3
         // the code-length code decodes through the distance table's storage
         // (it has 19 symbols and codes of at most 7 bits)
         Code<kDistBits, 32> &cc = T.dist;
-        if (build(cc, cl, 19) != kOk) return kErrCodes;
+        if (build<PlainEntry>(cc, cl, 19) != kOk) return kErrCodes;
         L.sync();
         int i = 0;
         while (i < nlen + ndist) {
-          const int sym = decode(cc, b);
-          if (sym < 0) return sym == -1 ? kErrInput : kErrSymbol;
+          const uint32_t ce = decode<PlainEntry>(cc, b);
+          if (ce >= kNoCode) return ce == kEndOfInput ? kErrInput : kErrSymbol;
+          const int sym = (int)(ce >> 16);
           if (sym < 16) {
             T.lens[i < nlen ? i : 288 + (i - nlen)] = (uint8_t)sym;
             ++i;
@@ -291,32 +324,32 @@ RBG_IHD int inflate_block(const uint8_t *in, uint32_t inlen, uint8_t *out, uint3
         if (T.lens[256] == 0) return kErrCodes;       // no end-of-block code
       }
       L.sync();
-      if (build(T.lit, T.lens, nlen) != kOk) return kErrCodes;
-      if (build(T.dist, T.lens + 288, ndist) != kOk) return kErrCodes;
+      if (build<LitEntry>(T.lit, T.lens, nlen) != kOk) return kErrCodes;
+      if (build<DistEntry>(T.dist, T.lens + 288, ndist) != kOk) return kErrCodes;
       L.sync();
       for (;;) {
-        const int sym = decode(T.lit, b);
-        if (sym < 0) return sym == -1 ? kErrInput : kErrSymbol;
-        if (sym < 256) {
+        const uint32_t e = decode<LitEntry>(T.lit, b);
+        if (e >= kNoCode) return e == kEndOfInput ? kErrInput : kErrSymbol;
+        const uint32_t kind = (e >> 4) & 3;
+        if (kind == 0) {
           if (o >= outlen) return kErrOutput;
-          if (L.leader()) out[o] = (uint8_t)sym;
+          if (L.leader()) out[o] = (uint8_t)(e >> 16);
           ++o;
           continue;
         }
-        if (sym == 256) break;
-        const int li = sym - 257;
-        if (li >= 29) return kErrSymbol;
-        uint32_t len = len_base(li), ex;
-        const int le = len_extra(li);
+        if (kind == 2) break;
+        if (kind == 3) return kErrSymbol;
+        uint32_t len = e >> 16, ex;
+        const int le = (int)((e >> 6) & 15);
         if (le) {
           if (!b.get(le, ex)) return kErrInput;
           len += ex;
         }
-        const int ds = decode(T.dist, b);
-        if (ds < 0) return ds == -1 ? kErrInput : kErrSymbol;
-        if (ds >= 30) return kErrSymbol;
-        uint32_t dist = dist_base(ds);
-        const int de = dist_extra(ds);
+        const uint32_t d = decode<DistEntry>(T.dist, b);
+        if (d >= kNoCode) return d == kEndOfInput ? kErrInput : kErrSymbol;
+        if (((d >> 4) & 3) == 3) return kErrSymbol;
+        uint32_t dist = d >> 16;
+        const int de = (int)((d >> 6) & 15);
         if (de) {
           if (!b.get(de, ex)) return kErrInput;
           dist += ex;
