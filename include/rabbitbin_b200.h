@@ -565,6 +565,24 @@ int rbg_bam_depth(rbg_ctx *ctx, const char *const *bam_paths, int32_t n_bams,
 int rbg_bam_depth_mem(rbg_ctx *ctx, const uint8_t *const *bam_bytes, const int64_t *bam_sizes,
                       int32_t n_bams, const rbg_depth_params *p, rbg_depth_matrix *out);
 int rbg_free_depth_matrix(rbg_depth_matrix *m);
+/* The MetaBAT / JGI depth table of a matrix from rbg_bam_depth*: the TSV that
+ * compute_depth_tsv_inmem returns without a DepthMatrixOut (printDepthTable,
+ * src/rabbit_depth.cpp:125-313, called at :1589-1593), byte for byte.  Header
+ * "contigName contigLen totalAvgDepth" and each BAM's base name (with a "-var"
+ * column when intra_depth_variance); one row per matrix row: the name up to
+ * its first blank, the length, the corrected-length-weighted total depth and
+ * each BAM's mean, printed as "%g" of the float value.  Without the variance
+ * columns each mean is the integer quotient sum / corrected length, corrected
+ * length = len - 2 min(min(max_edge_bases, min avg_read / 3), avg_read / 3)
+ * (len when edges are included or that reaches the whole contig); with them,
+ * the matrix's mean and a variance of 0, as the reference computes them.
+ * Means above 1e6 print as 0.  bam_names: the n_bams file names for the
+ * header; the unique-read block of a dual matrix is not part of the table.
+ * Host only; free *tsv with rbg_free_tsv. */
+int rbg_depth_tsv(const rbg_depth_matrix *m, const char *const *bam_names, int32_t n_bams,
+                  const rbg_depth_params *p, int32_t intra_depth_variance, char **tsv,
+                  int64_t *tsv_len);
+int rbg_free_tsv(char *tsv);
 /* One sample's sums from decompressed records (each: block_size, then the
  * record, back to back) on host memory; depth_out[n_targets] receives the
  * sums of the reads with MAPQ >= min_map_qual, depth_u_out (may be null) those

@@ -488,3 +488,30 @@ def depth_means(sums, target_len, edge):
     m = np.where(adj > 2, m, np.float32(0))
     m[m > np.float32(1000000.0)] = 0
     return m.astype(np.float32)
+
+
+def depth_tsv_ref(sums, avg, target_len, names, bam_names, variance=False, include_edge=False,
+                  max_edge=75, min_contig_len=1, min_contig_depth=0.0):
+    """printDepthTable's bytes (src/rabbit_depth.cpp:125-313) for per-BAM sums
+    [n_bams, n_targets] and read lengths, as compute_depth_tsv_inmem calls it."""
+    lib = ref_depth()
+    if lib is None:
+        return None
+    f = lib.ref_depth_tsv
+    f.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_char_p, C.c_int32,
+                  C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
+                  C.POINTER(C.c_void_p), C.POINTER(C.c_int64)]
+    f.restype = C.c_int
+    lib.ref_free.argtypes = [C.c_void_p]
+    s = np.ascontiguousarray(sums, np.uint64)
+    a = np.ascontiguousarray(avg, np.int32)
+    tl = np.ascontiguousarray(target_len, np.uint32)
+    nb = b"".join(x.encode() + b"\0" for x in names) or b"\0"
+    bb = b"".join(x.encode() + b"\0" for x in bam_names)
+    out, ln = C.c_void_p(), C.c_int64()
+    f(s.ctypes.data, a.ctypes.data, len(a), tl.ctypes.data, nb, len(tl), bb, int(variance),
+      int(include_edge), int(max_edge), int(min_contig_len), C.c_float(min_contig_depth),
+      C.byref(out), C.byref(ln))
+    r = C.string_at(out, ln.value)
+    lib.ref_free(out)
+    return r

@@ -62,6 +62,9 @@ FRAGMENTS = [
     ("frag_caldepth.inc", "rabbit_depth.h", 601, 887),
     ("frag_depth_column.inc", "rabbit_depth_fuse.h", 65, 68),
     ("frag_depth_accumulate.inc", "rabbit_depth.cpp", 1615, 1685),
+    ("frag_variance_type.inc", "rabbit_depth.h", 164, 176),
+    ("frag_depth_basename.inc", "rabbit_depth.cpp", 114, 123),
+    ("frag_depth_table.inc", "rabbit_depth.cpp", 125, 313),
 ]
 
 

@@ -334,6 +334,9 @@ def lib():
         "rbg_bam_depth_mem": ([vp, P(C.c_void_p), i64p, C.c_int32, P(DepthParams),
                                P(DepthMatrix)], C.c_int),
         "rbg_free_depth_matrix": ([P(DepthMatrix)], C.c_int),
+        "rbg_depth_tsv": ([P(DepthMatrix), P(C.c_char_p), C.c_int32, P(DepthParams), C.c_int32,
+                           P(C.c_void_p), i64p], C.c_int),
+        "rbg_free_tsv": ([C.c_void_p], C.c_int),
         "rbg_depth_accumulate": ([vp, C.c_void_p, C.c_int64, P(C.c_uint32), C.c_int32,
                                   P(DepthParams), P(C.c_uint64), P(C.c_uint64), P(C.c_int32)],
                                  C.c_int),
@@ -641,11 +644,12 @@ class Context:
         del order
         return out, st.as_dict()
 
-    def bam_depth(self, bams, **kw):
+    def bam_depth(self, bams, tsv_names=None, tsv_variance=False, **kw):
         """Depth matrix of BAM files (rbg_bam_depth_mem for bytes, rbg_bam_depth
         for paths): dict with names, lens, tid, means [rows, cols], sums
-        [cols, n_targets], avg_read, records and timings.  Keywords set
-        rbg_depth_params fields."""
+        [cols, n_targets], avg_read, records and timings; with tsv_names (the
+        BAMs' file names) also "tsv", the depth table (rbg_depth_tsv).
+        Keywords set rbg_depth_params fields."""
         p = default_depth_params(**kw)
         m = DepthMatrix()
         n = len(bams)
@@ -662,6 +666,16 @@ class Context:
             rc = self._L.rbg_bam_depth(self._h, ptrs, n, C.byref(p), C.byref(m))
         self._check(rc, "bam_depth")
         try:
+            tsv = None
+            if tsv_names is not None:
+                nm = (C.c_char_p * n)(*[os.fsencode(x) for x in tsv_names])
+                buf, ln = C.c_void_p(), C.c_int64()
+                st = self._L.rbg_depth_tsv(C.byref(m), nm, n, C.byref(p), int(bool(tsv_variance)),
+                                           C.byref(buf), C.byref(ln))
+                if st != RBG_OK:
+                    raise RbgError(st, "depth_tsv")
+                tsv = C.string_at(buf, ln.value)
+                self._L.rbg_free_tsv(buf)
             nr, nc, nt = int(m.n_rows), int(m.n_cols), int(m.n_targets)
             names = []
             if nr:
@@ -684,6 +698,7 @@ class Context:
                 "decompressed_bytes": int(m.decompressed_bytes),
                 "inflate_ms": float(m.inflate_ms), "total_ms": float(m.total_ms),
                 "kernel_ms": float(m.kernel_ms), "device_bams": int(m.device_bams),
+                "tsv": tsv,
             }
         finally:
             self._L.rbg_free_depth_matrix(C.byref(m))

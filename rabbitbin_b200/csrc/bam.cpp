@@ -762,6 +762,100 @@ int rbg_bam_depth(rbg_ctx *c, const char *const *paths, int32_t n_bams, const rb
   });
 }
 
+int rbg_depth_tsv(const rbg_depth_matrix *m, const char *const *bam_names, int32_t n_bams,
+                  const rbg_depth_params *p, int32_t intra_depth_variance, char **tsv,
+                  int64_t *tsv_len) {
+  if (!m || !bam_names || n_bams < 1 || !p || !tsv || !tsv_len) return RBG_ERR_ARG;
+  if ((m->n_cols != n_bams && m->n_cols != 2 * n_bams) || !m->avg_read ||
+      (m->n_rows > 0 && (!m->tid || !m->lens || !m->names || !m->name_off || !m->sums)))
+    return RBG_ERR_ARG;
+  for (int32_t b = 0; b < n_bams; ++b)
+    if (!bam_names[b]) return RBG_ERR_ARG;
+  try {
+    const int nb = n_bams;
+    const int64_t nt = m->n_targets;
+    int min_avg = INT32_MAX;
+    for (int b = 0; b < nb; ++b) min_avg = std::min(min_avg, (int)m->avg_read[b]);
+    const int edge_all = std::min(p->max_edge_bases, min_avg / 3);
+    std::string out;
+    out.reserve((size_t)(m->n_rows + 1) * (24 + 12 * (size_t)nb));
+    out += "contigName\tcontigLen\ttotalAvgDepth";
+    for (int b = 0; b < nb; ++b) {
+      // the file's base name: no directories, no extension
+      std::string n(bam_names[b]);
+      const size_t sl = n.find_last_of('/');
+      if (sl != std::string::npos) n = n.substr(sl + 1);
+      const size_t dot = n.find_last_of('.');
+      if (dot != std::string::npos) n = n.substr(0, dot);
+      out += "\t" + n;
+      if (intra_depth_variance) out += "\t" + n + "-var";
+    }
+    out += "\n";
+    auto put_float = [&](double v) {
+      char b[64];
+      const int k = std::snprintf(b, sizeof b, "%g", (double)(float)v);
+      out.append(b, (size_t)k);
+    };
+    for (int64_t r = 0; r < m->n_rows; ++r) {
+      const int32_t t = m->tid[r], cl = m->lens[r];
+      double weighted = 0.0;
+      uint64_t total_len = 0;
+      double means[512];
+      std::vector<double> many;
+      double *mv = nb <= 512 ? means : (many.resize((size_t)nb), many.data());
+      for (int b = 0; b < nb; ++b) {
+        // corrected length: 2 min(edge, avg_read / 3) bases fewer, unless that
+        // is the whole contig or edges are included
+        const int x = 2 * std::min(edge_all, (int)m->avg_read[b] / 3);
+        const int corr = (p->include_edge_bases || x >= cl) ? cl : cl - x;
+        const uint64_t sum = m->sums[(size_t)b * (size_t)nt + (size_t)t];
+        double mean;
+        if (intra_depth_variance) {
+          const int e = p->include_edge_bases ? 0 : std::min(p->max_edge_bases, (int)m->avg_read[b] / 3);
+          const int32_t adj = (cl > 2 * e + 1) ? (cl - 2 * e) : cl;
+          mean = (double)(adj > 2 ? (float)((double)sum / (double)adj) : 0.0f);
+        } else {
+          mean = corr > 0 ? (double)(sum / (uint64_t)corr) : 0.0;   // integer quotient
+        }
+        if (mean > 1000000) mean = 0;
+        total_len += (uint64_t)(int64_t)corr;
+        weighted += mean * corr;
+        mv[b] = mean;
+      }
+      double total = total_len > 0 ? weighted / (double)total_len : 0.0;
+      total *= nb;
+      const char *name = m->names + m->name_off[r];
+      out.append(name, std::strcspn(name, " \t"));
+      out += '\t';
+      out += std::to_string(cl);
+      out += '\t';
+      put_float(total);
+      for (int b = 0; b < nb; ++b) {
+        out += '\t';
+        put_float(mv[b]);
+        if (intra_depth_variance) {
+          out += '\t';
+          put_float(0.0);
+        }
+      }
+      out += '\n';
+    }
+    char *buf = (char *)malloc(out.size() + 1);
+    if (!buf) return RBG_ERR_NOMEM;
+    std::memcpy(buf, out.c_str(), out.size() + 1);
+    *tsv = buf;
+    *tsv_len = (int64_t)out.size();
+    return RBG_OK;
+  } catch (const std::bad_alloc &) {
+    return RBG_ERR_NOMEM;
+  }
+}
+
+int rbg_free_tsv(char *tsv) {
+  free(tsv);
+  return RBG_OK;
+}
+
 int rbg_depth_accumulate(rbg_ctx *c, const uint8_t *records, int64_t n_bytes,
                          const uint32_t *target_len, int32_t n_targets, const rbg_depth_params *p,
                          uint64_t *depth_out, uint64_t *depth_u_out, int32_t *avg_read) {

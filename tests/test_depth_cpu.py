@@ -89,3 +89,72 @@ def test_means_formula():
     assert m[4] == 0                                   # adj <= 2
     assert m[5] == np.float32(7 / 10)
     assert m[6] == 0                                   # 152 - 150 = 2: adj <= 2
+
+
+def _matrix(api_mod, sums, avg, tl, names, min_len, nb):
+    """An rbg_depth_matrix as rbg_bam_depth returns it, built on the host."""
+    import ctypes as C
+    kept = np.nonzero(tl.astype(np.int64) >= min_len)[0].astype(np.int32)
+    blob = b"".join(names[t].encode() + b"\0" for t in kept) or b"\0"
+    off = np.zeros(max(len(kept), 1), np.int64)
+    o = 0
+    for i, t in enumerate(kept):
+        off[i] = o
+        o += len(names[t].encode()) + 1
+    lens = tl[kept].astype(np.int32)
+    sums = np.ascontiguousarray(sums, np.uint64)
+    avg = np.ascontiguousarray(avg, np.int32)
+    keep = [kept, blob, off, lens, sums, avg]
+    m = api_mod.DepthMatrix()
+    m.n_rows, m.n_cols, m.n_targets = len(kept), nb, len(tl)
+    m.tid = kept.ctypes.data_as(C.POINTER(C.c_int32))
+    m.lens = lens.ctypes.data_as(C.POINTER(C.c_int32))
+    bbuf = C.create_string_buffer(blob, len(blob))
+    keep.append(bbuf)
+    m.names = C.cast(bbuf, C.c_void_p)
+    m.name_off = off.ctypes.data_as(C.POINTER(C.c_int64))
+    m.avg_read = avg.ctypes.data_as(C.POINTER(C.c_int32))
+    m.sums = sums.ctypes.data_as(C.POINTER(C.c_uint64))
+    return m, keep
+
+
+def test_depth_table_matches_reference_printer():
+    """rbg_depth_tsv (host formatting of the device sums) against the
+    reference's own printDepthTable, byte for byte."""
+    import ctypes as C
+    from rabbitbin_b200 import api
+    from rabbitbin_b200.synth import make_bam
+    if oracle.ref_depth() is None:
+        pytest.skip("reference harness not built")
+    L = api.lib()
+    rng = np.random.default_rng(8)
+    lens, _, _ = case("edge_mix")
+    names = [f"ctg_{i}" + (" some description" if i % 5 == 0 else "") +
+             ("\tx" if i % 7 == 0 else "") for i in range(len(lens))]
+    for nb, read_lens in ((1, [150]), (3, [150, 60, 250])):
+        sums, avg = [], []
+        for b in range(nb):
+            bam = make_bam(lens, rng.uniform(0.1, 40, len(lens)), seed=200 + b,
+                           read_len=read_lens[b])
+            recs, tl, _ = bam_records(bam)
+            s, a = oracle.depth_accumulate_ref(recs, tl, 0.97, 75, False, 0)
+            sums.append(s)
+            avg.append(a)
+        sums = np.stack(sums)
+        for variance in (False, True):
+            for inc, edge, min_len in ((False, 75, 1), (True, 75, 1), (False, 20, 1000),
+                                       (False, 300, 1)):
+                want = oracle.depth_tsv_ref(sums, avg, lens, names,
+                                            [f"/data/run{b}/sample{b}.sorted.bam" for b in range(nb)],
+                                            variance, inc, edge, min_len)
+                m, keep = _matrix(api, sums, avg, lens, names, min_len, nb)
+                p = api.default_depth_params(include_edge_bases=int(inc), max_edge_bases=edge,
+                                             min_contig_length=min_len)
+                bn = (C.c_char_p * nb)(*[f"/data/run{b}/sample{b}.sorted.bam".encode()
+                                        for b in range(nb)])
+                buf, ln = C.c_void_p(), C.c_int64()
+                assert L.rbg_depth_tsv(C.byref(m), bn, nb, C.byref(p), int(variance),
+                                       C.byref(buf), C.byref(ln)) == 0
+                got = C.string_at(buf, ln.value)
+                L.rbg_free_tsv(buf)
+                assert got == want, (nb, variance, inc, edge, min_len)

@@ -167,3 +167,27 @@ def test_malformed_input_is_rejected(gpu_ctx):
     # the context still works afterwards
     out = gpu_ctx.bam_depth([bam])
     assert out["records"] > 0
+
+
+def test_depth_table_from_device_sums(gpu_ctx):
+    """The TSV of compute_depth_tsv_inmem from the device route's sums
+    (rbg_depth_tsv), byte for byte against the reference's printDepthTable fed
+    the reference's own sums."""
+    lens, _, b0 = case("edge_mix")
+    b1 = make_bam(lens, np.random.default_rng(4).uniform(0.2, 25.0, len(lens)), seed=77,
+                  read_len=100)
+    names = ["x/s1.bam", "y/s2.bam"]
+    sums, avg = [], []
+    for bam in (b0, b1):
+        recs, tl, _ = bam_records(bam)
+        want = oracle.depth_accumulate_ref(recs, tl)
+        if want is None:
+            pytest.skip("reference harness not built")
+        sums.append(want[0])
+        avg.append(want[1])
+    for variance in (False, True):
+        out = gpu_ctx.bam_depth([b0, b1], tsv_names=names, tsv_variance=variance)
+        assert out["device_bams"] == 2
+        ref = oracle.depth_tsv_ref(np.stack(sums), avg, lens,
+                                   [f"contig_{i}" for i in range(len(lens))], names, variance)
+        assert out["tsv"] == ref
