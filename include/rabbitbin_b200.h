@@ -81,7 +81,8 @@ typedef struct rbg_params {
   int32_t graph_index;    /* RABBIT_GRAPH_INDEX (0): 1 restricts the small path's
                              neighbours to contigs sharing >= min_common
                              one-permutation sketch keys (build_similarity_graph,
-                             src/impl/rb_graph.cpp:199-383); rbg_bin_graph only */
+                             src/impl/rb_graph.cpp:199-383); rbg_bin_graph, or
+                             rbg_bin_batch through the single-assembly path */
   int32_t index_k;        /* sketch_kmer_size of the index's sketches (8; 1..32;
                              oph_k when the one-permutation metric is on)      */
   int32_t min_common;     /* RABBIT_MINCOMMON (0: floor(cutoff * m * 0.7), >= 1)  */
@@ -297,7 +298,10 @@ typedef struct rbg_batch_stats {
  * all of them (persistent all-pairs kernels pull (assembly, row block)
  * items from a device queue; each stage's launches form one CUDA graph) and
  * one host round trip for all calibrations.  out[i] (n_asm entries) receives
- * assembly i's graph; free each with rbg_free_graph.  `stats` may be NULL. */
+ * assembly i's graph; free each with rbg_free_graph.  `stats` may be NULL and
+ * covers the batched assemblies.  Assemblies on the one-permutation metric
+ * (oph_k > 0) or the inverted-index graph (graph_index) have no batch kernels:
+ * they run one after the other through rbg_bin_graph's path in the same call. */
 int rbg_bin_batch(rbg_ctx *ctx, const rbg_params *defaults, const rbg_assembly *asms,
                   int32_t n_asm, rbg_graph *out, rbg_batch_stats *stats);
 

@@ -229,12 +229,10 @@ void plan_batch(const rbg_params *defaults, const rbg_assembly *asms, int nb, Ba
     a.in = &x;
     a.p = x.params ? x.params : defaults;
     validate_assembly(x, a.p, "assembly " + std::to_string(i) + ": ");
-    if (a.p->oph_k > 0)
-      throw Error(RBG_ERR_UNSUPPORTED, "assembly " + std::to_string(i) +
-                                           ": the batch form uses the ProbMinHash metric (oph_k = 0)");
-    if (a.p->graph_index)
-      throw Error(RBG_ERR_UNSUPPORTED, "assembly " + std::to_string(i) +
-                                           ": graph_index is available through rbg_bin_graph only");
+    // (assemblies on the one-permutation metric or the inverted index are
+    // routed to the single-assembly path by rbg_bin_batch)
+    if (a.p->oph_k > 0 || a.p->graph_index)
+      throw Error(RBG_ERR_ARG, "assembly " + std::to_string(i) + ": not a batch-kernel assembly");
     a.n = x.n;
     a.nbases = x.n > 0 ? x.offsets[x.n] : 0;
     a.S = x.S;
@@ -1042,5 +1040,35 @@ void run_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
 
 extern "C" int rbg_bin_batch(rbg_ctx *c, const rbg_params *defaults, const rbg_assembly *asms,
                              int32_t n_asm, rbg_graph *out, rbg_batch_stats *stats) {
-  return rbg::guarded(c, [&] { rbg::run_batch(c, defaults, asms, n_asm, out, stats); });
+  return rbg::guarded(c, [&] {
+    if (n_asm > 0 && (!asms || !out || !defaults)) throw rbg::Error(RBG_ERR_ARG, "null argument");
+    // Assemblies on the one-permutation metric or the inverted-index graph
+    // have no batch kernels: they run one after the other through the
+    // single-assembly path on this context, after the batch of the others.
+    std::vector<int> one, many;
+    for (int i = 0; i < n_asm; ++i) {
+      const rbg_params *p = asms[i].params ? asms[i].params : defaults;
+      (p->oph_k > 0 || p->graph_index ? one : many).push_back(i);
+    }
+    if (one.empty()) {
+      rbg::run_batch(c, defaults, asms, n_asm, out, stats);
+      return;
+    }
+    std::vector<rbg_assembly> sub;
+    for (int i : many) sub.push_back(asms[i]);
+    std::vector<rbg_graph> got(sub.size());
+    if (!sub.empty()) rbg::run_batch(c, defaults, sub.data(), (int)sub.size(), got.data(), stats);
+    else if (stats) std::memset(stats, 0, sizeof(*stats));
+    for (size_t k = 0; k < many.size(); ++k) out[many[k]] = got[k];
+    for (int i : one) {
+      const rbg_params *p = asms[i].params ? asms[i].params : defaults;
+      try {
+        rbg::validate_assembly(asms[i], p, "assembly " + std::to_string(i) + ": ");
+        rbg::bin_graph_one(c, p, asms[i], &out[i]);
+      } catch (...) {
+        for (int j : many) rbg_free_graph(&out[j]);
+        throw;
+      }
+    }
+  });
 }

@@ -1345,6 +1345,17 @@ void codes_from_winners(rbg_ctx *c, const rbg_params *p, const uint32_t *w32, in
 
 }  // namespace
 
+namespace rbg {
+// One assembly through the single-assembly path (sketch behind the chunked
+// copy, graph, fetch) under a lock the caller already holds.
+void bin_graph_one(rbg_ctx *c, const rbg_params *p, const rbg_assembly &x, rbg_graph *out) {
+  validate(p);
+  stage_sketch_chunked(c, p, x.seqcat, x.offsets, x.n, x.depth, x.S);
+  run_graph(c, p);
+  fetch(c, out);
+}
+}  // namespace rbg
+
 extern "C" {
 
 int rbg_default_params(rbg_params *p) {

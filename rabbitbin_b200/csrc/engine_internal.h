@@ -326,6 +326,7 @@ int64_t batch_request_bytes(const rbg_params *p, int64_t n, int64_t nbases, int 
 
 // Validation of one assembly's arguments (the checks rbg_bin_batch makes).
 void validate_assembly(const rbg_assembly &x, const rbg_params *p, const std::string &who);
+void bin_graph_one(rbg_ctx *c, const rbg_params *p, const rbg_assembly &x, rbg_graph *out);
 
 }  // namespace rbg
 

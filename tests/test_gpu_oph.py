@@ -66,14 +66,23 @@ def test_oph_graph_large_route(gpu_ctx, ref_lib, S):
     assert g["path"] == 1
 
 
-def test_oph_unsupported_forms(gpu_ctx):
-    asm = make_assembly(10, 3000, 5, seed=5)
-    buf, offs = asm.concat()
-    with pytest.raises(api.RbgError) as e:                 # batch form: ProbMinHash only
-        gpu_ctx.bin_batch([(buf, offs, asm.depth, api.default_params(oph_k=8))])
-    assert e.value.code == -4
+def test_oph_and_index_assemblies_in_a_batch(gpu_ctx):
+    """The batch form takes assemblies on the one-permutation metric and the
+    inverted-index graph beside ProbMinHash ones: they run through the
+    single-assembly path inside the same call, each graph identical to
+    rbg_bin_graph's on that assembly alone."""
+    ent = []
+    for seed, (G, N, S), kw in ((5, (10, 3000, 5), dict(oph_k=8)), (6, (8, 2000, 3), {}),
+                                (7, (6, 1500, 2), dict(graph_index=1)),
+                                (8, (9, 2600, 4), dict(oph_k=6))):
+        asm = make_assembly(G, N, S, seed=seed)
+        buf, offs = asm.concat()
+        ent.append((buf, offs, asm.depth, api.default_params(**kw)))
+    got, st = gpu_ctx.bin_batch(ent)
+    assert st["n_assemblies"] == 1                         # the ProbMinHash one
+    for g, e in zip(got, ent):
+        want = gpu_ctx.bin_graph(*e)
+        for k in ("src", "dst", "scomp", "score"):
+            assert np.array_equal(np.asarray(g[k]), np.asarray(want[k])), k
     with pytest.raises(api.RbgError):                      # winner rows are ProbMinHash
-        gpu_ctx.build_pmh_winners(buf, offs, api.default_params(oph_k=8))
-    # the context stays usable
-    g = gpu_ctx.bin_graph(buf, offs, asm.depth, api.default_params(oph_k=8))
-    assert g["path"] == 1
+        gpu_ctx.build_pmh_winners(ent[0][0], ent[0][1], api.default_params(oph_k=8))
