@@ -819,7 +819,9 @@ int rbg_depth_tsv(const rbg_depth_matrix *m, const char *const *bam_names, int32
         }
         if (mean > 1000000) mean = 0;
         total_len += (uint64_t)(int64_t)corr;
-        weighted += mean * corr;
+        // with the variance columns the mean is a float and its product with
+        // the corrected length is a float product, as the reference forms it
+        weighted += intra_depth_variance ? (double)((float)mean * (float)corr) : mean * corr;
         mv[b] = mean;
       }
       double total = total_len > 0 ? weighted / (double)total_len : 0.0;

@@ -131,10 +131,11 @@ def test_depth_table_matches_reference_printer():
     lens, _, _ = case("edge_mix")
     names = [f"ctg_{i}" + (" some description" if i % 5 == 0 else "") +
              ("\tx" if i % 7 == 0 else "") for i in range(len(lens))]
-    for nb, read_lens in ((1, [150]), (3, [150, 60, 250])):
+    for nb, read_lens, seeds in ((1, [150], [200]), (3, [150, 60, 250], [200, 201, 202]),
+                                 (2, [150, 100], [11, 77])):
         sums, avg = [], []
         for b in range(nb):
-            bam = make_bam(lens, rng.uniform(0.1, 40, len(lens)), seed=200 + b,
+            bam = make_bam(lens, rng.uniform(0.1, 40, len(lens)), seed=seeds[b],
                            read_len=read_lens[b])
             recs, tl, _ = bam_records(bam)
             s, a = oracle.depth_accumulate_ref(recs, tl, 0.97, 75, False, 0)

@@ -40,8 +40,13 @@ def test_index_graph_against_reference(gpu_ctx, ref_lib, N, S, mc, K):
     assert np.array_equal(got["scomp"], sc) and np.array_equal(got["score"], sw)
 
 
-def test_index_graph_rejected_by_batch(gpu_ctx):
+def test_index_graph_through_batch(gpu_ctx):
+    """The batch call runs an index-graph assembly through the single-assembly
+    path: the same graph as rbg_bin_graph."""
     asm = make_assembly(5, 300, 3, seed=7)
     buf, offs = asm.concat()
-    with pytest.raises(api.RbgError):
-        gpu_ctx.bin_batch([(buf, offs, asm.depth, api.default_params(graph_index=1))])
+    e = (buf, offs, asm.depth, api.default_params(graph_index=1))
+    got, _ = gpu_ctx.bin_batch([e])
+    want = gpu_ctx.bin_graph(*e)
+    for k in ("src", "dst", "scomp", "score"):
+        assert np.array_equal(np.asarray(got[0][k]), np.asarray(want[k])), k
