@@ -791,56 +791,78 @@ int rbg_depth_tsv(const rbg_depth_matrix *m, const char *const *bam_names, int32
       if (intra_depth_variance) out += "\t" + n + "-var";
     }
     out += "\n";
-    auto put_float = [&](double v) {
-      char b[64];
-      const int k = std::snprintf(b, sizeof b, "%g", (double)(float)v);
-      out.append(b, (size_t)k);
+    // rows [r0, r1) into `dst`
+    auto rows = [&](int64_t r0, int64_t r1, std::string &dst) {
+      auto put_float = [&](double v) {
+        char b[64];
+        const int k = std::snprintf(b, sizeof b, "%g", (double)(float)v);
+        dst.append(b, (size_t)k);
+      };
+      std::vector<double> mv((size_t)nb);
+      for (int64_t r = r0; r < r1; ++r) {
+        const int32_t t = m->tid[r], cl = m->lens[r];
+        double weighted = 0.0;
+        uint64_t total_len = 0;
+        for (int b = 0; b < nb; ++b) {
+          // corrected length: 2 min(edge, avg_read / 3) bases fewer, unless that
+          // is the whole contig or edges are included
+          const int x = 2 * std::min(edge_all, (int)m->avg_read[b] / 3);
+          const int corr = (p->include_edge_bases || x >= cl) ? cl : cl - x;
+          const uint64_t sum = m->sums[(size_t)b * (size_t)nt + (size_t)t];
+          double mean;
+          if (intra_depth_variance) {
+            const int e = p->include_edge_bases ? 0 : std::min(p->max_edge_bases, (int)m->avg_read[b] / 3);
+            const int32_t adj = (cl > 2 * e + 1) ? (cl - 2 * e) : cl;
+            mean = (double)(adj > 2 ? (float)((double)sum / (double)adj) : 0.0f);
+          } else {
+            mean = corr > 0 ? (double)(sum / (uint64_t)corr) : 0.0;   // integer quotient
+          }
+          if (mean > 1000000) mean = 0;
+          total_len += (uint64_t)(int64_t)corr;
+          // with the variance columns the mean is a float and its product with
+          // the corrected length is a float product, as the reference forms it
+          weighted += intra_depth_variance ? (double)((float)mean * (float)corr) : mean * corr;
+          mv[b] = mean;
+        }
+        double total = total_len > 0 ? weighted / (double)total_len : 0.0;
+        total *= nb;
+        const char *name = m->names + m->name_off[r];
+        dst.append(name, std::strcspn(name, " \t"));
+        dst += '\t';
+        dst += std::to_string(cl);
+        dst += '\t';
+        put_float(total);
+        for (int b = 0; b < nb; ++b) {
+          dst += '\t';
+          put_float(mv[b]);
+          if (intra_depth_variance) {
+            dst += '\t';
+            put_float(0.0);
+          }
+        }
+        dst += '\n';
+      }
     };
-    for (int64_t r = 0; r < m->n_rows; ++r) {
-      const int32_t t = m->tid[r], cl = m->lens[r];
-      double weighted = 0.0;
-      uint64_t total_len = 0;
-      double means[512];
-      std::vector<double> many;
-      double *mv = nb <= 512 ? means : (many.resize((size_t)nb), many.data());
-      for (int b = 0; b < nb; ++b) {
-        // corrected length: 2 min(edge, avg_read / 3) bases fewer, unless that
-        // is the whole contig or edges are included
-        const int x = 2 * std::min(edge_all, (int)m->avg_read[b] / 3);
-        const int corr = (p->include_edge_bases || x >= cl) ? cl : cl - x;
-        const uint64_t sum = m->sums[(size_t)b * (size_t)nt + (size_t)t];
-        double mean;
-        if (intra_depth_variance) {
-          const int e = p->include_edge_bases ? 0 : std::min(p->max_edge_bases, (int)m->avg_read[b] / 3);
-          const int32_t adj = (cl > 2 * e + 1) ? (cl - 2 * e) : cl;
-          mean = (double)(adj > 2 ? (float)((double)sum / (double)adj) : 0.0f);
-        } else {
-          mean = corr > 0 ? (double)(sum / (uint64_t)corr) : 0.0;   // integer quotient
-        }
-        if (mean > 1000000) mean = 0;
-        total_len += (uint64_t)(int64_t)corr;
-        // with the variance columns the mean is a float and its product with
-        // the corrected length is a float product, as the reference forms it
-        weighted += intra_depth_variance ? (double)((float)mean * (float)corr) : mean * corr;
-        mv[b] = mean;
-      }
-      double total = total_len > 0 ? weighted / (double)total_len : 0.0;
-      total *= nb;
-      const char *name = m->names + m->name_off[r];
-      out.append(name, std::strcspn(name, " \t"));
-      out += '\t';
-      out += std::to_string(cl);
-      out += '\t';
-      put_float(total);
-      for (int b = 0; b < nb; ++b) {
-        out += '\t';
-        put_float(mv[b]);
-        if (intra_depth_variance) {
-          out += '\t';
-          put_float(0.0);
-        }
-      }
-      out += '\n';
+    // contiguous row ranges formatted on host threads, joined in row order
+    const int64_t cells = m->n_rows * (int64_t)(nb + 1);
+    const int nth = (int)std::max<int64_t>(1, std::min<int64_t>(host_threads(p), cells / 20000));
+    if (nth <= 1) {
+      rows(0, m->n_rows, out);
+    } else {
+      std::vector<std::string> part((size_t)nth);
+      std::vector<std::thread> pool;
+      std::atomic<int> nomem{0};
+      for (int i = 0; i < nth; ++i)
+        pool.emplace_back([&, i] {
+          try {
+            rows(m->n_rows * i / nth, m->n_rows * (i + 1) / nth, part[(size_t)i]);
+          } catch (const std::bad_alloc &) {
+            nomem = 1;
+          }
+        });
+      for (auto &th : pool) th.join();
+      if (nomem) return RBG_ERR_NOMEM;
+      for (auto &x : part) out += x;
     }
     char *buf = (char *)malloc(out.size() + 1);
     if (!buf) return RBG_ERR_NOMEM;

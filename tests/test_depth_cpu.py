@@ -159,3 +159,33 @@ def test_depth_table_matches_reference_printer():
                 got = C.string_at(buf, ln.value)
                 L.rbg_free_tsv(buf)
                 assert got == want, (nb, variance, inc, edge, min_len)
+
+
+def test_depth_table_large_threaded():
+    """A table large enough to be formatted on several host threads (30,000
+    contigs x 4 BAMs): still the reference printer's bytes."""
+    import ctypes as C
+    from rabbitbin_b200 import api
+    if oracle.ref_depth() is None:
+        pytest.skip("reference harness not built")
+    L = api.lib()
+    rng = np.random.default_rng(21)
+    n, nb = 30000, 4
+    tl = rng.integers(0, 60000, n).astype(np.uint32)
+    sums = (rng.random((nb, n)) ** 3 * tl * 40).astype(np.uint64)
+    sums[:, ::97] = 0
+    sums[1, 5] = np.uint64(2 ** 45)                         # a mean above 1e6
+    avg = [150, 101, 250, 33]
+    names = [f"k141_{i} flag=1" if i % 3 else f"k141_{i}" for i in range(n)]
+    bams = [f"/run/s{b}.bam" for b in range(nb)]
+    for variance in (False, True):
+        want = oracle.depth_tsv_ref(sums, avg, tl, names, bams, variance, False, 75, 1500)
+        m, keep = _matrix(api, sums, avg, tl, names, 1500, nb)
+        p = api.default_depth_params(min_contig_length=1500, threads=6)
+        bn = (C.c_char_p * nb)(*[x.encode() for x in bams])
+        buf, ln = C.c_void_p(), C.c_int64()
+        assert L.rbg_depth_tsv(C.byref(m), bn, nb, C.byref(p), int(variance), C.byref(buf),
+                               C.byref(ln)) == 0
+        got = C.string_at(buf, ln.value)
+        L.rbg_free_tsv(buf)
+        assert got == want, variance
