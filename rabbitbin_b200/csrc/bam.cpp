@@ -418,10 +418,17 @@ Prefix host_prefix(const FileView &f, const std::vector<Blk> &B, const std::vect
 // and inflated, walked and summed on the device.  Returns false when a block
 // did not start on a record (a writer that lets records cross blocks): the
 // caller then clears the sums and takes the host route.
-bool run_sample_device(rbg_ctx *c, const FileView &f, const std::vector<Blk> &B,
+// The BAM's status goes to its 16-byte slot on the device (flags, then the
+// record count; zeroed by the caller): bit 0 a block that does not inflate or
+// fails its CRC32, bit 1 a block that does not start on a record.  Nothing
+// waits for the device here, so the next BAM's host work overlaps this one's
+// kernels; `timed` (per slot: its launch times are not read yet) and
+// `kernel_ms` carry over from BAM to BAM.
+void run_sample_device(rbg_ctx *c, const FileView &f, const std::vector<Blk> &B,
                        const std::vector<uint64_t> &uoff, int64_t hdr_end, const depth::Params &P,
                        const rbg_depth_params *p, const uint32_t *d_tlen, unsigned long long *sum,
-                       unsigned long long *sum_u, int threads, SampleOut &so) {
+                       unsigned long long *sum_u, int threads, uint8_t *slot_dev, bool timed[2],
+                       double &kernel_ms) {
   DepthBufs &D = *c->depthb;
   cudaStream_t s = c->stream;
   for (int i = 0; i < 2; ++i) {
@@ -433,11 +440,8 @@ bool run_sample_device(rbg_ctx *c, const FileView &f, const std::vector<Blk> &B,
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
   const uint64_t budget = (uint64_t)std::max(1, std::min(p->device_chunk_mb, 3072)) << 20;
-  D.flags.ensure(16);
-  CK(cudaMemsetAsync(D.flags.p, 0, 16, s));
-  uint32_t *flags = D.flags.as<uint32_t>();
-  unsigned long long *rec_total = (unsigned long long *)(D.flags.as<uint8_t>() + 8);
-  bool timed[2] = {false, false};
+  uint32_t *flags = (uint32_t *)slot_dev;
+  unsigned long long *rec_total = (unsigned long long *)(slot_dev + 8);
   size_t b0 = 0;
   int slot = 0;
   while (b0 < B.size()) {
@@ -453,7 +457,7 @@ bool run_sample_device(rbg_ctx *c, const FileView &f, const std::vector<Blk> &B,
     if (timed[slot]) {
       float ms = 0;
       CK(cudaEventElapsedTime(&ms, D.k0[slot], D.k1[slot]));
-      so.kernel_ms += ms;
+      kernel_ms += ms;
       timed[slot] = false;
     }
     D.cpin[slot].ensure(cbytes + 16);
@@ -501,22 +505,6 @@ bool run_sample_device(rbg_ctx *c, const FileView &f, const std::vector<Blk> &B,
     b0 = b1;
     slot ^= 1;
   }
-  uint32_t fl[4] = {0, 0, 0, 0};
-  D.hflag.ensure(16);
-  CK(cudaMemcpyAsync(D.hflag.p, D.flags.p, 16, cudaMemcpyDeviceToHost, s));
-  CK(cudaStreamSynchronize(s));
-  std::memcpy(fl, D.hflag.p, 16);
-  for (int i = 0; i < 2; ++i)
-    if (timed[i]) {
-      float ms = 0;
-      CK(cudaEventElapsedTime(&ms, D.k0[i], D.k1[i]));
-      so.kernel_ms += ms;
-    }
-  if (fl[0] & 1u) throw Error(RBG_ERR_ARG, "BGZF block does not inflate to its stated size or fails its CRC32");
-  uint64_t recs = 0;
-  std::memcpy(&recs, (uint8_t *)fl + 8, 8);
-  so.records = (int64_t)recs;
-  return (fl[0] & 2u) == 0;
 }
 
 void bam_depth(rbg_ctx *c, const std::vector<FileView> &files, const rbg_depth_params *p,
@@ -537,49 +525,95 @@ void bam_depth(rbg_ctx *c, const std::vector<FileView> &files, const rbg_depth_p
   double walk_ms = 0, kernel_ms = 0;
   int64_t records = 0, cbytes = 0, ubytes = 0;
   int32_t device_bams = 0;
-  for (int b = 0; b < nb; ++b) {
-    std::vector<Blk> B;
+  bool have_h0 = false;
+  auto set_h0 = [&](const Header &h) {
+    h0 = h;
+    have_h0 = true;
+    const int32_t nt = (int32_t)h0.tlen.size();
+    D.tlen.ensure(std::max<size_t>(1, (size_t)nt) * 4);
+    if (nt) CK(cudaMemcpyAsync(D.tlen.p, h0.tlen.data(), (size_t)nt * 4, cudaMemcpyHostToDevice, s));
+    D.sums.ensure(std::max<size_t>(1, (size_t)ncols * nt) * 8);
+    CK(cudaMemsetAsync(D.sums.p, 0, std::max<size_t>(1, (size_t)ncols * nt) * 8, s));
+  };
+  auto index_file = [&](int b, std::vector<Blk> &B, std::vector<uint64_t> &uoff) {
     index_blocks(files[b].p, files[b].n, B);
-    std::vector<uint64_t> uoff(B.size() + 1, 0);
+    uoff.assign(B.size() + 1, 0);
     for (size_t i = 0; i < B.size(); ++i) uoff[i + 1] = uoff[i] + B[i].isize;
-    cbytes += (int64_t)files[b].n;
-    ubytes += (int64_t)uoff.back();
-    unsigned long long *sums_all = nullptr;
-    if (p->device_inflate) {
+  };
+  auto set_edge = [&](int b, int32_t a) {
+    avg[b] = a;
+    edge_col[b] = p->include_edge_bases ? 0 : std::min(p->max_edge_bases, a / 3);
+    if (dual) edge_col[nb + b] = edge_col[b];
+  };
+  std::vector<int> host_route;
+  if (p->device_inflate) {
+    // every BAM through the device route without waiting in between, then one
+    // read-back of all their status slots
+    D.flags.ensure((size_t)16 * nb);
+    CK(cudaMemsetAsync(D.flags.p, 0, (size_t)16 * nb, s));
+    bool timed[2] = {false, false};
+    std::vector<int32_t> pre_avg(nb, 0);
+    for (int b = 0; b < nb; ++b) {
+      std::vector<Blk> B;
+      std::vector<uint64_t> uoff;
+      index_file(b, B, uoff);
+      cbytes += (int64_t)files[b].n;
+      ubytes += (int64_t)uoff.back();
       const auto t0 = Clock::now();
       Prefix pre = host_prefix(files[b], B, uoff, threads);
       walk_ms += ms_since(t0);
-      if (b == 0) {
-        h0 = pre.h;
-        const int32_t nt = (int32_t)h0.tlen.size();
-        D.tlen.ensure(std::max<size_t>(1, (size_t)nt) * 4);
-        if (nt) CK(cudaMemcpyAsync(D.tlen.p, h0.tlen.data(), (size_t)nt * 4, cudaMemcpyHostToDevice, s));
-        D.sums.ensure(std::max<size_t>(1, (size_t)ncols * nt) * 8);
-        CK(cudaMemsetAsync(D.sums.p, 0, std::max<size_t>(1, (size_t)ncols * nt) * 8, s));
-      } else if (pre.h.tlen != h0.tlen) {
-        throw Error(RBG_ERR_ARG, "BAM files carry different contigs");
-      }
+      if (!have_h0) set_h0(pre.h);
+      else if (pre.h.tlen != h0.tlen) throw Error(RBG_ERR_ARG, "BAM files carry different contigs");
       const int32_t nt = (int32_t)h0.tlen.size();
-      sums_all = D.sums.as<unsigned long long>();
+      unsigned long long *sums_all = D.sums.as<unsigned long long>();
       depth::Params P{p->percent_identity,
                       p->include_edge_bases ? 0 : std::min(p->max_edge_bases, pre.avg / 3),
                       p->min_map_qual, p->dual_map_qual, nt};
-      SampleOut so;
-      if (run_sample_device(c, files[b], B, uoff, pre.hdr_end, P, p, D.tlen.as<uint32_t>(),
-                            sums_all + (size_t)b * nt, sums_all + (size_t)(nb + b) * nt, threads,
-                            so)) {
-        avg[b] = pre.avg;
-        records += so.records;
-        kernel_ms += so.kernel_ms;
-        edge_col[b] = P.edge;
-        if (dual) edge_col[nb + b] = edge_col[b];
-        ++device_bams;
+      run_sample_device(c, files[b], B, uoff, pre.hdr_end, P, p, D.tlen.as<uint32_t>(),
+                        sums_all + (size_t)b * nt, sums_all + (size_t)(nb + b) * nt, threads,
+                        D.flags.as<uint8_t>() + (size_t)16 * b, timed, kernel_ms);
+      pre_avg[b] = pre.avg;
+    }
+    D.hflag.ensure((size_t)16 * nb);
+    CK(cudaMemcpyAsync(D.hflag.p, D.flags.p, (size_t)16 * nb, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (int i = 0; i < 2; ++i)
+      if (timed[i]) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, D.k0[i], D.k1[i]));
+        kernel_ms += ms;
+      }
+    const int32_t nt = (int32_t)h0.tlen.size();
+    unsigned long long *sums_all = D.sums.as<unsigned long long>();
+    for (int b = 0; b < nb; ++b) {
+      const uint8_t *slot = D.hflag.as<uint8_t>() + (size_t)16 * b;
+      uint32_t fl;
+      uint64_t recs;
+      std::memcpy(&fl, slot, 4);
+      std::memcpy(&recs, slot + 8, 8);
+      if (fl & 1u)
+        throw Error(RBG_ERR_ARG, "BGZF block does not inflate to its stated size or fails its CRC32");
+      if (fl & 2u) {
+        // a block did not start on a record: this BAM takes the host route
+        CK(cudaMemsetAsync(sums_all + (size_t)b * nt, 0, (size_t)nt * 8, s));
+        if (dual) CK(cudaMemsetAsync(sums_all + (size_t)(nb + b) * nt, 0, (size_t)nt * 8, s));
+        host_route.push_back(b);
         continue;
       }
-      // a block did not start on a record: this BAM takes the host route
-      kernel_ms += so.kernel_ms;
-      CK(cudaMemsetAsync(sums_all + (size_t)b * nt, 0, (size_t)nt * 8, s));
-      if (dual) CK(cudaMemsetAsync(sums_all + (size_t)(nb + b) * nt, 0, (size_t)nt * 8, s));
+      set_edge(b, pre_avg[b]);
+      records += (int64_t)recs;
+      ++device_bams;
+    }
+  } else {
+    for (int b = 0; b < nb; ++b) host_route.push_back(b);
+  }
+  for (int b : host_route) {
+    std::vector<Blk> B;
+    std::vector<uint64_t> uoff;
+    index_file(b, B, uoff);
+    if (!p->device_inflate) {
+      cbytes += (int64_t)files[b].n;
+      ubytes += (int64_t)uoff.back();
     }
     // header: inflate blocks one by one until it is complete
     std::vector<uint8_t> hb;
@@ -592,27 +626,17 @@ void bam_depth(rbg_ctx *c, const std::vector<FileView> &files, const rbg_depth_p
       inflate_blocks(files[b].p, B, uoff, hblk, hblk + 1, hb.data() + uoff[hblk], 1);
       ++hblk;
     }
-    if (b == 0) {
-      h0 = h;
-      const int32_t nt = (int32_t)h0.tlen.size();
-      D.tlen.ensure(std::max<size_t>(1, (size_t)nt) * 4);
-      if (nt) CK(cudaMemcpyAsync(D.tlen.p, h0.tlen.data(), (size_t)nt * 4, cudaMemcpyHostToDevice, s));
-      D.sums.ensure(std::max<size_t>(1, (size_t)ncols * nt) * 8);
-      CK(cudaMemsetAsync(D.sums.p, 0, std::max<size_t>(1, (size_t)ncols * nt) * 8, s));
-    } else if (h.tlen != h0.tlen) {
-      throw Error(RBG_ERR_ARG, "BAM files carry different contigs");
-    }
+    if (!have_h0) set_h0(h);
+    else if (h.tlen != h0.tlen) throw Error(RBG_ERR_ARG, "BAM files carry different contigs");
     const int32_t nt = (int32_t)h0.tlen.size();
     std::vector<uint8_t> carry(hb.begin() + hlen, hb.end());
     BgzfSource src(files[b].p, B, uoff, hblk, threads);
     unsigned long long *sums = D.sums.as<unsigned long long>();
     const SampleOut so = run_sample(c, src, std::move(carry), p, D.tlen.as<uint32_t>(), nt,
                                     sums + (size_t)b * nt, sums + (size_t)(nb + b) * nt, walk_ms);
-    avg[b] = so.avg_read;
+    set_edge(b, so.avg_read);
     records += so.records;
     kernel_ms += so.kernel_ms;
-    edge_col[b] = p->include_edge_bases ? 0 : std::min(p->max_edge_bases, so.avg_read / 3);
-    if (dual) edge_col[nb + b] = edge_col[b];
   }
   const int32_t nt = (int32_t)h0.tlen.size();
   std::vector<int32_t> kept;
